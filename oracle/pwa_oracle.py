@@ -1,0 +1,439 @@
+"""CPU FP64 oracle of TF-PWA's amplitude-fit hot path (numpy restatement).
+
+TEST INFRASTRUCTURE ONLY.  This module is the checker for the CUDA engine:
+tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py``
+may import it; the product path never does.
+
+It restates, function by function, the reference's algorithm on the same
+per-event inputs (invariant masses and helicity / alignment angles):
+
+* small-d weights and d(beta): ``tf_pwa/dfun.py:118-173``
+* exp(i m theta) and conjugated D: ``tf_pwa/dfun.py:176-218``
+* D gathered to [lambda_a, lambda_b - lambda_c] with zeros outside |.|<=j:
+  ``tf_pwa/dfun.py:63-115,241-266``
+* CG coefficients with sympy, as ``tf_pwa/cg.py:18-26``; vertex CG matrix
+  ``tf_pwa/amp/core.py:851-900``
+* relative momenta q (clamped) and q^2 (unclamped): ``tf_pwa/amp/core.py:311-334``
+* Blatt-Weisskopf polynomial / B'_l(q^2): ``tf_pwa/breit_wigner.py:268-355``
+* barrier factor q^l B'_l of each LS: ``tf_pwa/amp/core.py:1072-1097``
+* helicity coupling H = sum_ls g_ls bf_ls CG_ls: ``tf_pwa/amp/core.py:931-947,1025-1043``
+* decay amplitude H * D*: ``tf_pwa/amp/core.py:1149-1164``
+* lineshapes BWR / BW with running width Gamma(m): ``tf_pwa/breit_wigner.py:56-91,231-245``,
+  particle model ``tf_pwa/amp/core.py:349-418``
+* chain contraction with totals and alignment D's: ``tf_pwa/amp/core.py:1392-1445,1563-1604``
+* sum over chains and |A|^2: ``tf_pwa/amp/core.py:1696-1728,1919-1931``
+* clip_log and the weighted NLL with alpha scaling and normalised MC
+  weights: ``tf_pwa/model/model.py:283-292,407-449,603-641,1126-1229``
+
+Gradients: couplings enter linearly (A = sum_k c_k F_k), so their gradient
+is exact here; masses and widths use a 4-point central difference of this
+FP64 function.
+"""
+import math
+from functools import lru_cache
+
+import numpy as np
+
+_EPS_CLIP = 1e-6
+
+
+# ----------------------------------------------------------- D functions
+@lru_cache(maxsize=None)
+def d_weight(j2):
+    """Wigner weights w[l, m1, m2] for spin j = j2/2 (dfun.py:118-143)."""
+    j = j2
+    ret = np.zeros((j + 1, j + 1, j + 1))
+    f = lambda x: math.factorial(x >> 1)  # noqa: E731
+    for m in range(-j, j + 1, 2):
+        for n in range(-j, j + 1, 2):
+            for k in range(max(0, n - m), min(j - m, j + n) + 1, 2):
+                l = (2 * k + (m - n)) // 2
+                sign = (-1) ** ((k + m - n) // 2)
+                v = sign * math.sqrt(1.0 * f(j + m) * f(j - m) * f(j + n) * f(j - n))
+                v /= f(j - m - k) * f(j + n - k) * f(k + m - n) * f(k)
+                ret[l][(m + j) // 2][(n + j) // 2] = v
+    return ret
+
+
+def small_d(beta, j2):
+    """(N, j2+1, j2+1) d^j_{m1 m2}(beta) (dfun.py:146-173)."""
+    a = np.arange(j2 + 1, dtype=np.float64)[None, :]
+    s = np.sin(0.5 * beta)[:, None]
+    c = np.cos(0.5 * beta)[:, None]
+    sc = s ** a * c ** (j2 - a)
+    w = d_weight(j2).reshape(j2 + 1, -1)
+    return (sc @ w).reshape(-1, j2 + 1, j2 + 1)
+
+
+def D_conj(alpha, beta, gamma, j2):
+    """e^{i m1 alpha} d^j_{m1 m2}(beta) e^{i m2 gamma} (dfun.py:196-218)."""
+    m = np.arange(-j2 / 2, j2 / 2 + 1, 1)[None, :]
+    d = small_d(beta, j2)
+    ea = np.exp(1j * m * alpha[:, None])[:, :, None]
+    eg = np.exp(1j * m * gamma[:, None])[:, None, :]
+    return ea * eg * d
+
+
+def D_lambda(alpha, beta, gamma, ja, la, lb, lc=(0,)):
+    """D* gathered to (N, la, lb, lc): element [lambda_a, lambda_b - lambda_c],
+    zero where |lambda_b - lambda_c| > ja (dfun.py:63-115)."""
+    j2 = int(round(2 * ja))
+    D = D_conj(alpha, beta, gamma, j2).reshape(-1, (j2 + 1) ** 2)
+    D = np.concatenate([D, np.zeros((D.shape[0], 1), D.dtype)], axis=1)
+    idx = []
+    for a in la:
+        for b in lb:
+            for c in lc:
+                dl = b - c
+                if abs(dl) <= ja:
+                    idx.append(int(round(a + ja)) * (j2 + 1) + int(round(dl + ja)))
+                else:
+                    idx.append((j2 + 1) ** 2)
+    return D[:, idx].reshape(-1, len(la), len(lb), len(lc))
+
+
+# ----------------------------------------------------------- CG
+@lru_cache(maxsize=None)
+def cg_coef(jb, jc, mb, mc, ja, ma):
+    """<jb mb; jc mc | ja ma> from sympy, as in tf_pwa/cg.py:18-26."""
+    from sympy import Rational
+    from sympy.physics.quantum.cg import CG
+
+    r = lambda x: Rational(int(round(2 * x)), 2)  # noqa: E731
+    return float(CG(r(jb), r(mb), r(jc), r(mc), r(ja), r(ma)).doit().evalf())
+
+
+def cg_matrix(ja, jb, jc, ls, hb, hc):
+    ret = np.zeros((len(ls), len(hb), len(hc)))
+    for i, (l, s) in enumerate(ls):
+        for ib, lb in enumerate(hb):
+            for ic, lc in enumerate(hc):
+                ret[i, ib, ic] = (
+                    np.sqrt(2 * l + 1) / np.sqrt(2 * ja + 1)
+                    * cg_coef(jb, jc, lb, -lc, s, lb - lc)
+                    * cg_coef(l, s, 0, lb - lc, ja, lb - lc)
+                )
+    return ret
+
+
+# ----------------------------------------------------------- lineshapes
+def rel_p(m0, m1, m2):
+    """|q| with the mass clamped at threshold (core.py:311-321)."""
+    s, d = m1 + m2, m1 - m2
+    m_eff = np.where(m0 > s, m0, s)
+    p = (m_eff - s) * (m_eff + s) * (m_eff - d) * (m_eff + d)
+    return np.sqrt(p) / (2 * m_eff)
+
+
+def rel_p2(m0, m1, m2):
+    """|q|^2, unclamped (core.py:324-334)."""
+    s, d = m1 + m2, m1 - m2
+    p = (m0 - s) * (m0 + s) * (m0 - d) * (m0 + d)
+    return p / (2 * m0) ** 2
+
+
+@lru_cache(maxsize=None)
+def bprime_coef(l):
+    """|theta_l(i w)|^2 coefficients, highest power first (breit_wigner.py:319-390)."""
+    table = {
+        0: [1.0],
+        1: [1.0, 1.0],
+        2: [1.0, 3.0, 9.0],
+        3: [1.0, 6.0, 45.0, 225.0],
+        4: [1.0, 10.0, 135.0, 1575.0, 11025.0],
+        5: [1.0, 15.0, 315.0, 6300.0, 99225.0, 893025.0],
+    }
+    if l in table:
+        return table[l]
+    import sympy as sym
+
+    x = sym.Symbol("x")
+    th = sum(sym.Rational(math.factorial(l + k), math.factorial(l - k) * math.factorial(k) * 2 ** k)
+             * x ** (l - k) for k in range(l + 1))
+    w = sym.Symbol("w", real=True)
+    h = th.subs({x: sym.I * w})
+    poly = sym.Poly(sym.expand(h * sym.conjugate(h)), w).as_dict()
+    return [float(poly.get((2 * l - 2 * i,), 0)) for i in range(l + 1)]
+
+
+def bprime_poly(l, z):
+    r = np.zeros_like(z)
+    for c in bprime_coef(l):
+        r = r * z + c
+    return r
+
+
+def bprime_q2(l, q2, q02, d):
+    bp = bprime_poly(l, q02 * d * d) / bprime_poly(l, q2 * d * d)
+    return np.sqrt(np.where(bp > 0, bp, 1.0))
+
+
+def bprime(l, q, q0, d):
+    return np.sqrt(bprime_poly(l, (q0 * d) ** 2)) / np.sqrt(bprime_poly(l, (q * d) ** 2))
+
+
+def gamma_running(m, g0, q, q0, L, m0, d):
+    qq0 = np.where(q0 > 1e-15, (q / q0) ** (2 * L + 1), 1.0)
+    return g0 * qq0 * (m0 / m) * bprime(L, q, q0, d) ** 2
+
+
+def bwr(m, m0, g0, q, q0, L, d):
+    g = gamma_running(m, g0, q, q0, L, m0, d)
+    x = m0 * m0 - m * m
+    y = m0 * g
+    s = x * x + y * y
+    return x / s + 1j * y / s
+
+
+def bw(m, m0, g0):
+    x = m0 * m0 - m * m
+    y = m0 * g0
+    s = x * x + y * y
+    return x / s + 1j * y / s
+
+
+# ----------------------------------------------------------- model
+class OracleModel:
+    """Amplitude of a decay group on per-event fields.
+
+    ``group`` is the topology object of the engine's model compiler (chains,
+    decays, spins, LS lists -- cross-checked against the reference), ``plan``
+    maps every chain vertex to its input columns."""
+
+    def __init__(self, group, plan):
+        self.group = group
+        self.plan = plan
+        self.letters = {}
+        gen = iter("abcdefghijklmnopqrstuvwxyz")
+        self.letters[group.top] = next(gen)
+        for o in group.outs:
+            self.letters[o] = next(gen)
+        for c in group:
+            for p in c.inner:
+                if p not in self.letters:
+                    self.letters[p] = next(gen)
+
+    # --- parameters ------------------------------------------------------
+    @staticmethod
+    def complex_of(vm_vals, polar, name):
+        r = vm_vals[name + "r"]
+        i = vm_vals[name + "i"]
+        if polar.get(name, True):
+            return r * np.cos(i) + 1j * r * np.sin(i)
+        return r + 1j * i
+
+    def couplings(self, vals, polar):
+        """Per chain: total, per decay g_ls vectors (all complex)."""
+        out = []
+        from_names = {}
+        for c in self.group:
+            tot = self.complex_of(vals, polar, c.params_head + "_total_0")
+            gl = []
+            for d in c:
+                n = len(d.get_ls_list())
+                gl.append(np.array([self.complex_of(vals, polar, f"{d.params_head}_g_ls_{i}")
+                                    for i in range(n)]))
+            out.append((tot, gl))
+        return out
+
+    @staticmethod
+    def mass_of(vals, p):
+        n = f"{p.params_head}_mass"
+        return vals.get(n, p.mass)
+
+    @staticmethod
+    def width_of(vals, p):
+        n = f"{p.params_head}_width"
+        return vals.get(n, p.width)
+
+    # --- per decay --------------------------------------------------------
+    def data_mass(self, x, cf, p, chain):
+        if p in chain.inner:
+            return x[cf["mass"][p]]
+        return np.full(x.shape[1], p.mass)
+
+    def decay_amp(self, x, cf, chain, k, d, vals, gls):
+        """(N, n_a, n_b, n_c) complex amplitude of vertex d (core.py:1149-1164)."""
+        a, (b, c) = d.core, d.outs
+        f = cf["decays"][k]
+        alpha, beta = x[f["alpha"]], x[f["beta"]]
+        Dc = D_lambda(alpha, beta, np.zeros_like(alpha), a.J, a.spins, b.spins, c.spins)
+        # q^2 from data masses, q0^2 from nominal (possibly floating) masses
+        m0d = self.data_mass(x, cf, a, chain)
+        m1d = self.data_mass(x, cf, b, chain)
+        m2d = self.data_mass(x, cf, c, chain)
+        q2 = rel_p2(m0d, m1d, m2d)
+        m0n = self.mass_of(vals, a) if a in chain.inner else a.mass
+        m1n = self.mass_of(vals, b) if b in chain.inner else b.mass
+        m2n = self.mass_of(vals, c) if c in chain.inner else c.mass
+        q02 = rel_p2(m0n, m1n, m2n)
+        ls = d.get_ls_list()
+        if d.has_barrier_factor:
+            q02u = 1.0 if d.no_q0 else q02
+            bfs = []
+            for l, s in ls:
+                if d.has_bprime:
+                    bp = bprime_q2(l, q2, q02u, d.d)
+                    t = q2 ** (l / 2) * bp if d.has_ql else np.ones_like(q2) * bp
+                    if d.barrier_factor_norm:
+                        t = t / np.abs(q02u) ** (l / 2)
+                else:
+                    t = q2 ** (l / 2) if d.has_ql else np.ones_like(q2)
+                bfs.append(t)
+            mdep = gls[None, :] * np.stack(bfs, -1)
+        else:
+            mdep = np.broadcast_to(gls[None, :], (x.shape[1], len(ls)))
+        cg = cg_matrix(a.J, b.J, c.J, ls, b.spins, c.spins)
+        H = np.einsum("nl,lbc->nbc", mdep, cg)
+        return H[:, None, :, :] * Dc
+
+    def lineshape(self, x, cf, chain, p, vals):
+        """Particle.get_amp (core.py:399-418)."""
+        kind = p.lineshape_kind()
+        m = x[cf["mass"][p]]
+        if kind == "one":
+            return np.ones_like(m) + 0j
+        m0 = self.mass_of(vals, p)
+        g0 = self.width_of(vals, p)
+        if kind == "BW":
+            ret = bw(m, m0, g0)
+        else:
+            d = chain.decay_of(p)
+            b, c = d.outs
+            m1d, m2d = self.data_mass(x, cf, b, chain), self.data_mass(x, cf, c, chain)
+            q = rel_p(m, m1d, m2d)
+            m1n = self.mass_of(vals, b) if b in chain.inner else b.mass
+            m2n = self.mass_of(vals, c) if c in chain.inner else c.mass
+            q0 = rel_p(m0, m1n, m2n)
+            L = p.bw_l if p.bw_l is not None else min(d.get_l_list())
+            ret = bwr(m, m0, g0, q, q0, L, p.d)
+        if p.width_norm:
+            ret = g0 * ret
+        return ret
+
+    def chain_amp(self, x, ci, vals, coup):
+        chain = self.group[ci]
+        cf = self.plan.chains[ci]
+        tot, gl = coup[ci]
+        L = self.letters
+        ops, idx = [], []
+        for k, d in enumerate(chain):
+            ops.append(self.decay_amp(x, cf, chain, k, d, vals, gl[k]))
+            idx.append("..." + "".join(L[p] for p in (d.core,) + d.outs))
+        rs = np.ones(x.shape[1], dtype=np.complex128)
+        for p in chain.inner:
+            rs = rs * self.lineshape(x, cf, chain, p, vals)
+        ops.append(tot * rs)
+        idx.append("...")
+        final = "..." + "".join(L[p] for p in [self.group.top] + list(self.group.outs))
+        for k, d in enumerate(chain):
+            for o in d.outs:
+                if o in cf["aligned"] and o.J != 0:
+                    fa, fb, fg = cf["aligned"][o]
+                    dt = D_lambda(x[fa], x[fb], x[fg], o.J, o.spins, o.spins)[..., 0]
+                    ops.append(dt)
+                    idx.append("..." + L[o] + L[o].upper())
+                    final = final.replace(L[o], L[o].upper())
+        return np.einsum(",".join(idx) + "->" + final, *ops)
+
+    def amp(self, x, vals, polar=None):
+        polar = polar or {}
+        coup = self.couplings(vals, polar)
+        return sum(self.chain_amp(x, ci, vals, coup) for ci in range(len(self.group)))
+
+    def pdf(self, x, vals, polar=None):
+        a = self.amp(x, vals, polar)
+        return np.sum(np.abs(a.reshape(a.shape[0], -1)) ** 2, axis=1)
+
+
+# ----------------------------------------------------------- NLL
+def clip_log(x, eps=_EPS_CLIP):
+    """tf_pwa/model/model.py:283-292."""
+    xc = np.where(x > eps, x, eps)
+    dx = x - eps
+    return np.where(x > eps, np.log(xc), np.log(eps) + dx / eps - (dx / eps) ** 2 / 2.0)
+
+
+def weights(w_data, w_bg=None):
+    """alpha-scaled data weights (model.py:603-641): data weights followed by
+    background weights, times sum(w)/sum(w^2)."""
+    w = np.asarray(w_data, np.float64)
+    if w_bg is not None:
+        w = np.concatenate([w, np.asarray(w_bg, np.float64)])
+    return w * (w.sum() / (w * w).sum())
+
+
+def nll_value(f_data, w_data, f_mc, w_mc):
+    """-sum w clip_log f + (sum w) ln(sum w_mc f_mc / sum w_mc) (model.py:407-449)."""
+    wm = w_mc / w_mc.sum()
+    sw = w_data.sum()
+    return -np.sum(w_data * clip_log(f_data)) + sw * np.log(np.sum(wm * f_mc))
+
+
+class OracleNLL:
+    def __init__(self, model, x_data, w_data, x_mc, w_mc, names, polar, vals):
+        self.m = model
+        self.xd, self.wd = x_data, w_data
+        self.xm, self.wm = x_mc, w_mc
+        self.names = list(names)         # trainable names, in order
+        self.polar = polar
+        self.base = dict(vals)
+
+    def _vals(self, p):
+        v = dict(self.base)
+        v.update(dict(zip(self.names, p)))
+        return v
+
+    def nll(self, p):
+        v = self._vals(p)
+        return nll_value(self.m.pdf(self.xd, v, self.polar), self.wd,
+                         self.m.pdf(self.xm, v, self.polar), self.wm)
+
+    def grad(self, p, rel_step=1e-4):
+        """Exact derivative for coupling parameters (via the linear column
+        decomposition evaluated by differentiating r, phi analytically) and
+        4-point central differences for masses and widths."""
+        p = np.asarray(p, np.float64)
+        g = np.zeros_like(p)
+        v0 = self._vals(p)
+        fd0 = self.m.pdf(self.xd, v0, self.polar)
+        fm0 = self.m.pdf(self.xm, v0, self.polar)
+        Ad = self.m.amp(self.xd, v0, self.polar).reshape(len(fd0), -1)
+        Am = self.m.amp(self.xm, v0, self.polar).reshape(len(fm0), -1)
+        wm = self.wm / self.wm.sum()
+        sw = self.wd.sum()
+        I = np.sum(wm * fm0)
+        dclip = np.where(fd0 > _EPS_CLIP, 1.0 / np.where(fd0 > _EPS_CLIP, fd0, 1.0),
+                         1.0 / _EPS_CLIP - (fd0 - _EPS_CLIP) / _EPS_CLIP ** 2)
+        for k, n in enumerate(self.names):
+            base = n[:-1]
+            if n.endswith(("r", "i")) and base + "r" in v0 and base + "i" in v0 and (
+                    "_g_ls_" in base or "_total_" in base):
+                # dA/dtheta: A is linear in the complex coupling c = c(r, phi)
+                c = self.m.complex_of(v0, self.polar, base)
+                polar = self.polar.get(base, True)
+                r, ph = v0[base + "r"], v0[base + "i"]
+                if polar:
+                    dc = np.exp(1j * ph) if n.endswith("r") else 1j * c
+                else:
+                    dc = 1.0 if n.endswith("r") else 1j
+                # A = c * B + rest with B = dA/dc: evaluate B by setting c := 1
+                # and subtracting the c := 0 amplitude.
+                v1 = dict(v0)
+                v1[base + "r"], v1[base + "i"] = (1.0, 0.0)
+                v2 = dict(v0)
+                v2[base + "r"], v2[base + "i"] = (0.0, 0.0)
+                Bd = (self.m.amp(self.xd, v1, self.polar) - self.m.amp(self.xd, v2, self.polar)).reshape(Ad.shape)
+                Bm = (self.m.amp(self.xm, v1, self.polar) - self.m.amp(self.xm, v2, self.polar)).reshape(Am.shape)
+                dfd = 2 * np.real(np.sum(np.conj(Ad) * Bd * dc, axis=1))
+                dfm = 2 * np.real(np.sum(np.conj(Am) * Bm * dc, axis=1))
+                g[k] = -np.sum(self.wd * dclip * dfd) + sw * np.sum(wm * dfm) / I
+            else:
+                h = rel_step * max(abs(p[k]), 1e-3)
+                fs = []
+                for s in (-2, -1, 1, 2):
+                    q = p.copy()
+                    q[k] += s * h
+                    fs.append(self.nll(q))
+                g[k] = (fs[0] - 8 * fs[1] + 8 * fs[2] - fs[3]) / (12 * h)
+        return g

@@ -1,0 +1,180 @@
+"""Generate golden vectors by running the REFERENCE package's own code.
+
+Run in a container that has the reference checkout (it is not needed
+anywhere else; the outputs are committed):
+
+    python tests/golden/make_golden.py /path/to/reference
+
+TensorFlow is not installed, so the reference runs on the torch-backed
+TF-API stand-in in ``tests/golden/tfshim`` (GradientTape = torch autograd,
+float64).  For each workload config this script
+
+1. draws seeded flat phase-space momenta (the engine's own generator) for
+   data, an optional background sample and MC, writes them as the
+   reference's ``E px py pz`` text files;
+2. builds ``tf_pwa.config_loader.ConfigLoader`` on that config, sets seeded
+   parameters, and records: the reference's per-event input fields
+   (invariant masses, helicity and alignment angles from ``cal_angle``),
+   the per-event |A|^2 of data and MC (``AbsPDF.__call__``), and
+   ``FCN.nll_grad`` (NLL and its GradientTape gradient) -- plus, for the
+   small model, ``FCN.nll_grad_hessian``;
+3. saves everything to ``tests/golden/<name>.npz`` and the parameter
+   names/order, LS lists and CG matrices to ``tests/golden/<name>.json``.
+"""
+import json
+import os
+import shutil
+import sys
+import tempfile
+import warnings
+
+import numpy as np
+import yaml
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+
+CASES = {
+    # name: (config file, n_data, n_bg, n_mc, seed, hessian, extra data keys)
+    "d2kpipi": ("d2kpipi.yml", 400, 0, 1500, 11, True, {}),
+    "d2kpipi_float": ("d2kpipi_float.yml", 400, 0, 1500, 12, True, {}),
+    "lc2pkpi": ("lc2pkpi.yml", 400, 40, 1500, 13, False, {"bg_weight": 0.1}),
+    "toy_vvp": ("toy_vvp.yml", 300, 30, 1200, 14, False, {"bg_weight": 0.1}),
+}
+
+
+def load_pkg():
+    import importlib.util
+
+    d = os.path.join(REPO, "tf-pwa_b200")
+    spec = importlib.util.spec_from_file_location(
+        "tf_pwa_b200", os.path.join(d, "__init__.py"), submodule_search_locations=[d])
+    m = importlib.util.module_from_spec(spec)
+    sys.modules["tf_pwa_b200"] = m
+    spec.loader.exec_module(m)
+
+
+def main(ref_root):
+    sys.path[:0] = [os.path.join(HERE, "tfshim"), ref_root]
+    warnings.filterwarnings("ignore")
+    load_pkg()
+    from tf_pwa_b200.decay_config import DecayConfig, float_particles, init_params, load_yaml
+    from tf_pwa_b200.phasespace import generate_phsp
+    from tf_pwa_b200.plan import Plan
+    from tf_pwa_b200.variables import VarsManager
+    from tf_pwa.config_loader import ConfigLoader
+
+    cfg_dir = os.path.join(REPO, "tf-pwa_b200", "configs")
+    only = sys.argv[2:] or list(CASES)
+    for name in only:
+        cfg_file, nd, nb, nm, seed, do_hess, extra = CASES[name]
+        rng = np.random.default_rng(seed)
+        dic = load_yaml(os.path.join(cfg_dir, cfg_file))
+        dc = DecayConfig(dic)
+        group = dc.decay_group
+        plan = Plan(group)
+        order = dic["data"].get("dat_order")
+        top = group.top
+        masses = [dc.particle_property[o]["mass"] for o in order]
+        M = dc.particle_property[str(top)]["mass"]
+        tmp = tempfile.mkdtemp()
+        p4 = {}
+        for kind, n in (("data", nd), ("bg", nb), ("phsp", nm)):
+            if n == 0:
+                continue
+            ps = generate_phsp(M, masses, n, rng=rng)
+            arr = np.stack(ps, 1)  # (n, n_final, 4)
+            p4[kind] = arr
+            np.savetxt(os.path.join(tmp, kind + ".dat"), arr.reshape(-1, 4), fmt="%.17g")
+        dic2 = dict(dic)
+        dic2["data"] = dict(dic.get("data", {}))
+        dic2["data"].update({"data": [os.path.join(tmp, "data.dat")],
+                             "phsp": [os.path.join(tmp, "phsp.dat")]})
+        if nb:
+            dic2["data"]["bg"] = [os.path.join(tmp, "bg.dat")]
+        dic2["data"].update(extra)
+        cfg_path = os.path.join(tmp, "config.yml")
+        with open(cfg_path, "w") as f:
+            yaml.safe_dump(dic2, f)
+        ref = ConfigLoader(cfg_path)
+        amp = ref.get_amplitude()
+        vm = amp.vm
+        # seeded parameter values: |g| ~ U(0.5, 2), phase ~ U(-pi, pi);
+        # masses/widths at their nominal values shifted by a few percent
+        params = {}
+        for k in vm.trainable_vars:
+            if k.endswith("r") and ("_g_ls_" in k or "_total_" in k):
+                params[k] = float(rng.uniform(0.5, 2.0))
+            elif k.endswith("i") and ("_g_ls_" in k or "_total_" in k):
+                params[k] = float(rng.uniform(-np.pi, np.pi))
+            else:
+                params[k] = float(vm.get(k)) * float(rng.uniform(0.97, 1.03))
+        vm.set_all(params)
+        all_vals = {k: float(vm.get(k)) for k in vm.variables}
+        datas = {k: ref.get_data(k) for k in ("data", "phsp", "bg") if (k != "bg" or nb)}
+        fields = {}
+        for kind, lst in datas.items():
+            d = lst[0]
+            cols = np.zeros((plan.n_fields, len(d["weight"])))
+            topo_keys = list(d["decay"].keys())
+            for fi, fname in enumerate(plan.fields):
+                parts = fname.split("/")
+                if parts[0] == "m":
+                    node = [k for k in d["particle"] if str(k) == parts[1]][0]
+                    cols[fi] = np.asarray(d["particle"][node]["m"])
+                    continue
+                tidx = int(parts[0])
+                my_topo = plan.topos[tidx]
+                tstr = "[" + ", ".join(my_topo.decay_name(dd) for dd in my_topo.chain) + "]"
+                tkey = [k for k in topo_keys if str(k) == tstr]
+                assert tkey, (tstr, [str(k) for k in topo_keys])
+                dd = d["decay"][tkey[0]]
+                dkey = [k for k in dd if str(k) == parts[1]][0]
+                pkey = [k for k in dd[dkey] if str(k) == parts[2]][0]
+                if parts[3] == "aligned":
+                    cols[fi] = np.asarray(dd[dkey][pkey]["aligned_angle"][parts[4]])
+                else:
+                    cols[fi] = np.asarray(dd[dkey][pkey]["ang"][parts[3]])
+            fields[kind] = cols
+            # helicity gamma must be zero (not stored as a field)
+            for tkey in topo_keys:
+                for dkey, dv in d["decay"][tkey].items():
+                    for pkey, pv in dv.items():
+                        if isinstance(pv, dict) and "ang" in pv:
+                            assert np.all(np.asarray(pv["ang"]["gamma"]) == 0)
+        f_vals = {k: np.asarray(amp(datas[k][0])) for k in datas}
+        fcn = ref.get_fcn()
+        nll, grad = fcn.nll_grad()
+        out = dict(
+            fields_data=fields["data"], fields_mc=fields["phsp"],
+            f_data=f_vals["data"], f_mc=f_vals["phsp"],
+            p4_data=p4["data"], p4_mc=p4["phsp"],
+            nll=np.float64(nll), grad=np.asarray(grad, np.float64),
+            weight_data=np.asarray(fcn.weight, np.float64),
+        )
+        if nb:
+            out.update(fields_bg=fields["bg"], f_bg=f_vals["bg"], p4_bg=p4["bg"])
+        if do_hess:
+            n2, g2, h2 = fcn.nll_grad_hessian()
+            out.update(hess=np.asarray(h2, np.float64), hess_grad=np.asarray(g2, np.float64),
+                       hess_nll=np.float64(n2))
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+        meta = {
+            "config": cfg_file,
+            "extra_data": extra,
+            "trainable": list(vm.trainable_vars),
+            "variables": all_vals,
+            "fields": plan.fields,
+            "chains": [str(c) for c in amp.decay_group],
+            "ls": [[list(map(list, dd.get_ls_list())) for dd in c] for c in amp.decay_group],
+            "cg": [[np.asarray(dd.get_cg_matrix()).tolist() for dd in c] for c in amp.decay_group],
+            "seed": seed,
+        }
+        with open(os.path.join(HERE, name + ".json"), "w") as f:
+            json.dump(meta, f, indent=1)
+        shutil.rmtree(tmp)
+        print(name, "nll", float(nll), "n_trainable", len(vm.trainable_vars))
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

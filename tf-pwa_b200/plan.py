@@ -1,0 +1,123 @@
+"""Event-field layout of a model: which per-event inputs the hot path reads.
+
+The engine consumes structure-of-arrays event data.  Each column ("field") is
+one per-event quantity produced once per dataset by the kinematics step:
+
+* ``m/<node>``: invariant mass of an intermediate node, e.g. ``m/(B, C)``;
+* ``<t>/<decay>/<particle>/{alpha,beta,gamma}``: helicity angles of a
+  particle in its mother's frame, for topology ``t``;
+* ``<t>/<decay>/<final>/aligned/{alpha,beta,gamma}``: Wigner alignment
+  angles of a final particle with spin in a non-reference chain.
+
+Node and decay names follow the reference's standard topology
+(``tf_pwa/particle.py:698-717``): an inner node is named by its sorted final
+particles, ``(B, C)``; topologies are enumerated as in
+``tf_pwa/particle.py:902-921`` (first chain of each topology, in chain
+order).  Angles are the ones ``tf_pwa/cal_angle.py:262-490`` attaches to the
+standard topology; a chain reads the angles of its own decay's ``outs[0]``
+(``tf_pwa/amp/core.py:1149-1164``) and alignment angles of its finals
+(``tf_pwa/amp/core.py:1414-1429``).  Helicity ``gamma`` is identically zero
+for two-body helicity angles and is not stored.
+"""
+from .particles import DecayChain
+
+
+def node_name(finals):
+    return "({})".format(", ".join(sorted(str(i) for i in finals)))
+
+
+class ChainTopology:
+    """Standard-topology view of one chain: node names for every particle."""
+
+    def __init__(self, chain):
+        self.chain = chain
+        self.node = {}
+        for p in chain.outs:
+            self.node[p] = str(p)
+        for p in chain.inner:
+            self.node[p] = node_name(chain.final_set(p))
+        self.node[chain.top] = str(chain.top)
+        self.id = tuple(sorted(node_name(chain.final_set(p)) for p in chain.inner))
+
+    def decay_name(self, d):
+        return "{}->{}".format(self.node[d.core], "+".join(self.node[o] for o in d.outs))
+
+    def decay_key(self, d):
+        return (self.node[d.core], tuple(sorted(self.node[o] for o in d.outs)))
+
+
+class Plan:
+    """Field layout + per-chain references into it."""
+
+    def __init__(self, group):
+        self.group = group
+        self.topos = []          # list of ChainTopology (first chain of each)
+        self.chain_topo = []     # per chain: index into self.topos
+        for c in group:
+            t = ChainTopology(c)
+            for k, t0 in enumerate(self.topos):
+                if t0.id == t.id:
+                    self.chain_topo.append(k)
+                    break
+            else:
+                self.chain_topo.append(len(self.topos))
+                self.topos.append(t)
+        self.fields = []
+        self._index = {}
+        self.align_ref = self._alignment_reference()
+        self.chains = [self._chain_fields(i, c) for i, c in enumerate(group)]
+
+    def field(self, name):
+        if name not in self._index:
+            self._index[name] = len(self.fields)
+            self.fields.append(name)
+        return self._index[name]
+
+    def _std_decay_name(self, tidx, key):
+        t = self.topos[tidx]
+        for d in t.chain:
+            if t.decay_key(d) == key:
+                return t.decay_name(d)
+        raise KeyError(key)
+
+    def _alignment_reference(self):
+        """Reference topology of every final particle (rule 1 of
+        ``tf_pwa/cal_angle.py:346-378``): the first topology in which it is a
+        direct daughter of the top, else the first topology."""
+        ref = {}
+        top = self.group.top
+        for k, t in enumerate(self.topos):
+            for d in t.chain:
+                if d.core == top:
+                    for o in d.outs:
+                        if o in self.group.outs and str(o) not in ref:
+                            ref[str(o)] = k
+        for o in self.group.outs:
+            ref.setdefault(str(o), 0)
+        return ref
+
+    def _chain_fields(self, ci, chain):
+        tidx = self.chain_topo[ci]
+        t = ChainTopology(chain)
+        out = {"topo": tidx, "decays": [], "aligned": {}, "mass": {}}
+        for p in chain.inner:
+            out["mass"][p] = self.field("m/" + t.node[p])
+        for d in chain:
+            std = self._std_decay_name(tidx, t.decay_key(d))
+            b = t.node[d.outs[0]]
+            out["decays"].append({
+                "alpha": self.field(f"{tidx}/{std}/{b}/alpha"),
+                "beta": self.field(f"{tidx}/{std}/{b}/beta"),
+            })
+        for d in chain:
+            std = self._std_decay_name(tidx, t.decay_key(d))
+            for o in d.outs:
+                if o in chain.outs and o.J != 0 and self.align_ref[str(o)] != tidx:
+                    base = f"{tidx}/{std}/{t.node[o]}/aligned"
+                    out["aligned"][o] = tuple(
+                        self.field(f"{base}/{a}") for a in ("alpha", "beta", "gamma"))
+        return out
+
+    @property
+    def n_fields(self):
+        return len(self.fields)

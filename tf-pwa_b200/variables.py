@@ -1,0 +1,126 @@
+"""Fit-parameter manager with the reference's names, order and conventions.
+
+Mirrors the behaviour of ``tf_pwa/variable.py`` that callers of the fit API
+observe: every real parameter has a name, ``trainable_vars`` lists the free
+ones in creation order (``tf_pwa/variable.py:120-160``), complex parameters
+are stored as ``<name>r``/``<name>i`` pairs in polar form by default
+(``tf_pwa/variable.py:162-197``, value r*exp(i*phi) as in
+``tf_pwa/variable.py:1715-1765``), ``set_fix``/``set_all``/``get_all_dic``
+behave as in ``tf_pwa/variable.py:415-440,684-697``.
+"""
+import contextlib
+import warnings
+
+import numpy as np
+
+
+class VarsManager:
+    def __init__(self, name="", polar=True, rng=None):
+        self.name = name
+        self.polar = polar
+        self.variables = {}        # name -> float
+        self.trainable_vars = []   # free names, in order
+        self.complex_vars = {}     # complex name -> polar flag
+        self.bnd_dic = {}
+        self.same_list = []
+        self._rng = rng if rng is not None else np.random.default_rng()
+
+    # -- creation ---------------------------------------------------------
+    def add_real_var(self, name, value=None, range_=None, trainable=True):
+        if name in self.variables and name in self.trainable_vars:
+            self.trainable_vars.remove(name)
+        if value is None:
+            lo, hi = (0.0, 1.0) if range_ is None else range_
+            value = float(self._rng.uniform(lo, hi))
+        self.variables[name] = float(value)
+        if trainable:
+            self.trainable_vars.append(name)
+
+    def add_complex_var(self, name, polar=None, trainable=True, fix_vals=(1.0, 0.0)):
+        if polar is None:
+            polar = self.polar
+        if trainable:
+            if polar:
+                self.add_real_var(name + "r", range_=(0, 2.0))
+                self.add_real_var(name + "i", range_=(-np.pi, np.pi))
+            else:
+                self.add_real_var(name + "r", range_=(-1, 1))
+                self.add_real_var(name + "i", range_=(-1, 1))
+        else:
+            self.add_real_var(name + "r", value=fix_vals[0], trainable=False)
+            self.add_real_var(name + "i", value=fix_vals[1], trainable=False)
+        self.complex_vars[name] = polar
+
+    # -- fixing ------------------------------------------------------------
+    def set_fix(self, name, value=None, unfix=False):
+        if value is not None:
+            self.variables[name] = float(value)
+        if unfix:
+            if name in self.trainable_vars:
+                warnings.warn(f"{name} has been freed already!")
+            else:
+                self.trainable_vars.append(name)
+        else:
+            if name in self.trainable_vars:
+                self.trainable_vars.remove(name)
+
+    def is_fixed(self, name):
+        return name not in self.trainable_vars
+
+    # -- values ------------------------------------------------------------
+    def get(self, name):
+        return self.variables[name]
+
+    def set(self, name, value):
+        if name not in self.variables:
+            warnings.warn(f"{name} not found")
+            return
+        self.variables[name] = float(value)
+
+    def set_all(self, vals):
+        if isinstance(vals, dict):
+            for k, v in vals.items():
+                self.set(k, v)
+        else:
+            vals = list(vals)
+            if len(vals) != len(self.trainable_vars):
+                raise ValueError(
+                    f"expected {len(self.trainable_vars)} values, got {len(vals)}")
+            for k, v in zip(self.trainable_vars, vals):
+                self.variables[k] = float(v)
+
+    def get_all_val(self):
+        return [self.variables[k] for k in self.trainable_vars]
+
+    def get_all_dic(self, trainable_only=False):
+        if trainable_only:
+            return {k: self.variables[k] for k in self.trainable_vars}
+        return dict(self.variables)
+
+    def complex_value(self, name):
+        r = self.variables[name + "r"]
+        i = self.variables[name + "i"]
+        if self.complex_vars.get(name, self.polar):
+            return r * np.cos(i) + 1j * r * np.sin(i)
+        return r + 1j * i
+
+    @contextlib.contextmanager
+    def temp_params(self, vals):
+        old = dict(self.variables)
+        self.set_all(vals)
+        try:
+            yield
+        finally:
+            self.variables = old
+
+    def std_polar_all(self):
+        """Fold polar parameters to r > 0, phi in (-pi, pi]
+        (``tf_pwa/variable.py`` std_polar)."""
+        for name, polar in self.complex_vars.items():
+            if not polar:
+                continue
+            r, p = self.variables[name + "r"], self.variables[name + "i"]
+            if r < 0:
+                r, p = -r, p + np.pi
+            p = (p + np.pi) % (2 * np.pi) - np.pi
+            self.variables[name + "r"], self.variables[name + "i"] = r, p
