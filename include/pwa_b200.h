@@ -1,0 +1,100 @@
+/*
+ * C ABI of the B200 amplitude-fit engine (libpwa_b200.so).
+ *
+ * The reference package (TF-PWA) is pure Python/TensorFlow and has no FFI of
+ * its own; these entry points sit under the Python classes that replace the
+ * reference's hot path, one for each piece of work that path does:
+ *
+ *   pwa_plan_create    compile a decay model          tf_pwa/amp/amp.py:43-64
+ *                      (AbsPDF construction / init_params of the amplitude)
+ *   pwa_upload_events  keep data + MC events resident  tf_pwa/model/model.py:1126-1164
+ *                      (FCN.__init__: weights, batches, MC weights)
+ *   pwa_eval           NLL + gradient sums             tf_pwa/model/model.py:407-449,1207-1229
+ *                      (BaseModel.nll_grad_batch / FCN.nll_grad)
+ *   pwa_eval_pdf       per-event sum |A|^2             tf_pwa/amp/amp.py:120-129
+ *                      (AbsPDF.__call__ -> DecayGroup.sum_amp, core.py:1919-1931)
+ *   pwa_build_gram     cached MC integral matrix       tf_pwa/model/opt_int.py:128-296
+ *                      (ModelCachedInt.build_cached_int)
+ *   pwa_compile_only / pwa_last_error / pwa_plan_info / pwa_plan_destroy
+ *                      build check and bookkeeping (no reference counterpart)
+ *
+ * Conventions: plain pointers and sizes only; every call returns 0 on success
+ * or a PWA_ERR_* code, with a message in pwa_last_error().  Nothing throws
+ * across the ABI.  Calls on one handle must not overlap; different handles
+ * are independent.  `stream` is a cudaStream_t (0 = legacy default stream).
+ */
+#ifndef PWA_B200_H
+#define PWA_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct pwa_plan pwa_plan;
+
+enum {
+  PWA_OK = 0,
+  PWA_ERR_ARG = 1,      /* invalid argument / size */
+  PWA_ERR_COMPILE = 2,  /* NVRTC compilation or module load failed */
+  PWA_ERR_CUDA = 3,     /* CUDA runtime error */
+  PWA_ERR_STATE = 4,    /* call order (e.g. eval before upload) */
+  PWA_ERR_OOM = 5       /* device allocation failed */
+};
+
+enum { PWA_PLAIN_F64 = 0, PWA_MIXED_F32 = 1 };
+
+/* Compile a model.  `src` is the generated model source (model_event /
+ * model_columns and the Consts layout); the library prepends its device
+ * headers and compiles for sm_100a on the current device.
+ * n_mass / n_angle: number of FP64 mass / angle columns of an event;
+ * ncol, nout, nshape, nconst: model sizes matching the source.
+ * tpb: threads per block of the fused kernels (32..1024, multiple of 32). */
+int pwa_plan_create(const char* src, size_t src_len, int n_mass, int n_angle, int ncol, int nout,
+                    int nshape, int nconst, int tpb, pwa_plan** out);
+
+int pwa_plan_destroy(pwa_plan* h);
+
+/* Compile the model module for `arch` (e.g. "sm_100a") without a device and
+ * return the NVRTC/ptxas log (register and spill report) in log_buf.  Used
+ * by the build step to check generated models on a machine without a GPU. */
+int pwa_compile_only(const char* src, size_t src_len, int tpb, const char* arch, char* log_buf,
+                     size_t log_len);
+
+/* Events: xm[n_mass][n_data+n_mc], xa[n_angle][n_data+n_mc], w[n_data+n_mc]
+ * (row-major; data rows first, then MC).  Data weights are the final
+ * (alpha-scaled) weights; MC weights are normalised to sum 1 by the caller.
+ * `on_device` = 1 when the pointers are device memory. */
+int pwa_upload_events(pwa_plan* h, const double* xm, const double* xa, const double* w,
+                      long long n_data, long long n_mc, int on_device, void* stream);
+
+/* One evaluation.  consts[nconst] per the model's Consts layout.
+ * out[2*nacc] (host): data sums then MC sums, nacc = 1 + 2*ncol + nshape:
+ *   [0] sum w clip_log(f) (data) / sum w f (MC)
+ *   [1+2k], [2+2k]  Re/Im sum fac * G_k,   G_k = sum_o conj(A_o) F_k,o
+ *   [1+2ncol+s]     sum fac * d f / d shape_s
+ * fac = w * clip_log'(f) for data, w for MC.  precision: PWA_PLAIN_F64 or
+ * PWA_MIXED_F32 (FP32 amplitudes, FP64 sums).  mc = 0 skips the MC set. */
+int pwa_eval(pwa_plan* h, const double* consts, int precision, int mc, void* stream, double* out);
+
+/* Per-event sum |A|^2 of events [beg, end) of the uploaded set into
+ * out_dev (device, end-beg doubles). */
+int pwa_eval_pdf(pwa_plan* h, const double* consts, int precision, long long beg, long long end,
+                 double* out_dev, void* stream);
+
+/* Gram matrix of the MC set, M_kl = sum_i w_i sum_o conj(F_ik,o) F_il,o,
+ * in FP64; out[2*ncol*ncol] host, (re, im) row-major. */
+int pwa_build_gram(pwa_plan* h, const double* consts, void* stream, double* out);
+
+/* info[0..7]: registers/thread of eval_f64, eval_f32, local bytes f64, f32,
+ * blocks, blocks_data, nacc, threads per block. */
+int pwa_plan_info(pwa_plan* h, long long* info);
+
+const char* pwa_last_error(pwa_plan* h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PWA_B200_H */

@@ -1,0 +1,46 @@
+"""Model compiler against the reference: parameter names and order, chain
+order, LS lists and CG matrices recorded from the reference package."""
+import numpy as np
+import pytest
+
+from common import load_golden, load_model
+
+CASES = ["d2kpipi", "d2kpipi_float", "lc2pkpi", "toy_vvp"]
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_params_chains_ls_cg(name):
+    g, meta = load_golden(name)
+    dc, vm, plan = load_model(meta["config"])
+    assert vm.trainable_vars == meta["trainable"]
+    assert list(vm.variables.keys()) == list(meta["variables"].keys())
+    assert [str(c) for c in dc.decay_group] == meta["chains"]
+    for c, ls_ref, cg_ref in zip(dc.decay_group, meta["ls"], meta["cg"]):
+        for d, l1, c1 in zip(c, ls_ref, cg_ref):
+            assert [list(x) for x in d.get_ls_list()] == l1
+            np.testing.assert_allclose(d.cg(), np.array(c1), atol=1e-14)
+
+
+def test_cg_against_sympy():
+    from sympy import Rational
+    from sympy.physics.quantum.cg import CG
+
+    from tf_pwa_b200.particles import clebsch_gordan, spin_range, two
+
+    for j1 in (0, 0.5, 1, 1.5, 2):
+        for j2 in (0, 0.5, 1, 1.5):
+            for j in spin_range(abs(j1 - j2), j1 + j2):
+                for m1 in spin_range(-j1, j1):
+                    for m2 in spin_range(-j2, j2):
+                        if abs(m1 + m2) > j:
+                            continue
+                        r = lambda x: Rational(two(x), 2)  # noqa: E731
+                        ref = float(CG(r(j1), r(m1), r(j2), r(m2), r(j), r(m1 + m2)).doit().evalf())
+                        assert abs(clebsch_gordan(j1, m1, j2, m2, j, m1 + m2) - ref) < 1e-14
+
+
+def test_bprime_coefficients():
+    from tf_pwa_b200.particles import bprime_coeff
+
+    assert bprime_coeff(2) == [1.0, 3.0, 9.0]
+    assert bprime_coeff(5) == [1.0, 15.0, 315.0, 6300.0, 99225.0, 893025.0]

@@ -1,0 +1,232 @@
+// Kernels around the generated ``model_event``/``model_columns`` functions.
+//
+// Compiled together with the model code by NVRTC (sm_100a).  Events live in
+// HBM as structure-of-arrays columns: XM[n_mass][ld] (FP64 invariant
+// masses), XA[n_angle][ld] (angles, FP64 or FP32), W[ld] (FP64 weights);
+// data events occupy [0, n_data), MC events [n_data, n_all).
+//
+// pwa_eval_*  one persistent launch over data and MC: blocks
+//             [0, blocks_data) walk the data events, the rest the MC events
+//             (grid-stride).  Every thread accumulates in FP64
+//               data:  sum w clip_log(f),  sum w clip_log'(f) G_k, ... d-shape
+//               MC:    sum w f,            sum w G_k,             ... d-shape
+//             (the NLL of tf_pwa/model/model.py:407-449 and its gradient
+//             pieces), reduces them with warp shuffles and one shared-memory
+//             stage, and writes one row of block partials.
+// pwa_reduce  sums the block partials in a fixed order (one warp per
+//             accumulator), so results are bitwise reproducible.
+// pwa_pdf_*   per-event sum |A|^2 (the forward amplitude, AbsPDF.__call__).
+// pwa_columns_f64  per-event partial-wave columns F_k for the Gram cache.
+// pwa_gram_f64     block partials of M_kl = sum_i w_i sum_o conj(F_ik,o) F_il,o.
+#pragma once
+
+#ifndef PWA_TPB
+#define PWA_TPB 128
+#endif
+
+template <typename R>
+__device__ __forceinline__ void eval_body(const Consts& C, const R* __restrict__ XA,
+                                          const double* __restrict__ XM,
+                                          const double* __restrict__ W, long long n_data,
+                                          long long n_all, long long ld, int blocks_data,
+                                          double* __restrict__ partials) {
+  const bool is_data = (int)blockIdx.x < blocks_data;
+  const long long beg = is_data ? 0 : n_data;
+  const long long end = is_data ? n_data : n_all;
+  const int nb = is_data ? blocks_data : (int)gridDim.x - blocks_data;
+  const int b = is_data ? (int)blockIdx.x : (int)blockIdx.x - blocks_data;
+  double acc[PWA_NACC];
+#pragma unroll
+  for (int j = 0; j < PWA_NACC; ++j) acc[j] = 0.0;
+  for (long long i = beg + (long long)b * PWA_TPB + threadIdx.x; i < end;
+       i += (long long)nb * PWA_TPB) {
+    double f;
+    cpx<R> G[PWA_NCOL];
+    double ds[PWA_NSHAPE > 0 ? PWA_NSHAPE : 1];
+    model_event<R>(C, XA, XM, ld, i, &f, G, ds);
+    const double w = __ldg(W + i);
+    double fac;
+    if (is_data) {
+      double dl;
+      const double cl = clip_log(f, &dl);
+      acc[0] = fma(w, cl, acc[0]);
+      fac = w * dl;
+    } else {
+      acc[0] = fma(w, f, acc[0]);
+      fac = w;
+    }
+#pragma unroll
+    for (int k = 0; k < PWA_NCOL; ++k) {
+      acc[1 + 2 * k] = fma(fac, double(G[k].re), acc[1 + 2 * k]);
+      acc[2 + 2 * k] = fma(fac, double(G[k].im), acc[2 + 2 * k]);
+    }
+#pragma unroll
+    for (int s = 0; s < PWA_NSHAPE; ++s)
+      acc[1 + 2 * PWA_NCOL + s] = fma(fac, ds[s], acc[1 + 2 * PWA_NCOL + s]);
+  }
+  __shared__ double red[PWA_TPB / 32][PWA_NACC];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int j = 0; j < PWA_NACC; ++j) {
+    const double v = warp_sum(acc[j]);
+    if (lane == 0) red[warp][j] = v;
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < PWA_NACC; j += PWA_TPB) {
+    double s = 0.0;
+#pragma unroll
+    for (int w2 = 0; w2 < PWA_TPB / 32; ++w2) s += red[w2][j];
+    partials[(long long)blockIdx.x * PWA_NACC + j] = s;
+  }
+}
+
+extern "C" __global__ void __launch_bounds__(PWA_TPB)
+    pwa_eval_f64(const Consts C, const double* __restrict__ XA, const double* __restrict__ XM,
+                 const double* __restrict__ W, long long n_data, long long n_all, long long ld,
+                 int blocks_data, double* __restrict__ partials) {
+  eval_body<double>(C, XA, XM, W, n_data, n_all, ld, blocks_data, partials);
+}
+
+extern "C" __global__ void __launch_bounds__(PWA_TPB)
+    pwa_eval_f32(const Consts C, const float* __restrict__ XA, const double* __restrict__ XM,
+                 const double* __restrict__ W, long long n_data, long long n_all, long long ld,
+                 int blocks_data, double* __restrict__ partials) {
+  eval_body<float>(C, XA, XM, W, n_data, n_all, ld, blocks_data, partials);
+}
+
+// out[0..nacc) = data sums, out[nacc..2 nacc) = MC sums.  One warp per
+// accumulator; each lane strides over the blocks, then a fixed shuffle tree.
+extern "C" __global__ void pwa_reduce(const double* __restrict__ partials, int nacc,
+                                      int blocks_data, int nblocks, double* __restrict__ out) {
+  const int lane = threadIdx.x & 31;
+  const int warps = blockDim.x >> 5;
+  for (int j = (int)(threadIdx.x >> 5); j < 2 * nacc; j += warps) {
+    const int which = j / nacc, jj = j % nacc;
+    const int b0 = which ? blocks_data : 0, b1 = which ? nblocks : blocks_data;
+    double s = 0.0;
+    for (int b = b0 + lane; b < b1; b += 32) s += partials[(long long)b * nacc + jj];
+    s = warp_sum(s);
+    if (lane == 0) out[j] = s;
+  }
+}
+
+template <typename R>
+__device__ __forceinline__ void pdf_body(const Consts& C, const R* __restrict__ XA,
+                                         const double* __restrict__ XM, long long beg,
+                                         long long end, long long ld, double* __restrict__ out) {
+  for (long long i = beg + (long long)blockIdx.x * blockDim.x + threadIdx.x; i < end;
+       i += (long long)gridDim.x * blockDim.x) {
+    double f;
+    cpx<R> G[PWA_NCOL];
+    double ds[PWA_NSHAPE > 0 ? PWA_NSHAPE : 1];
+    model_event<R>(C, XA, XM, ld, i, &f, G, ds);
+    out[i - beg] = f;
+  }
+}
+
+extern "C" __global__ void __launch_bounds__(PWA_TPB)
+    pwa_pdf_f64(const Consts C, const double* __restrict__ XA, const double* __restrict__ XM,
+                long long beg, long long end, long long ld, double* __restrict__ out) {
+  pdf_body<double>(C, XA, XM, beg, end, ld, out);
+}
+
+extern "C" __global__ void __launch_bounds__(PWA_TPB)
+    pwa_pdf_f32(const Consts C, const float* __restrict__ XA, const double* __restrict__ XM,
+                long long beg, long long end, long long ld, double* __restrict__ out) {
+  pdf_body<float>(C, XA, XM, beg, end, ld, out);
+}
+
+// Per-event columns F[i][k][o] (complex128 as re,im pairs), event range
+// [beg, end) written densely from row 0.
+extern "C" __global__ void __launch_bounds__(PWA_TPB)
+    pwa_columns_f64(const Consts C, const double* __restrict__ XA,
+                    const double* __restrict__ XM, long long beg, long long end, long long ld,
+                    double* __restrict__ F) {
+  for (long long i = beg + (long long)blockIdx.x * blockDim.x + threadIdx.x; i < end;
+       i += (long long)gridDim.x * blockDim.x) {
+    cpx<double> Fk[PWA_NCOL * PWA_NOUT];
+    model_columns<double>(C, XA, XM, ld, i, Fk);
+    double* row = F + (i - beg) * (2LL * PWA_NCOL * PWA_NOUT);
+#pragma unroll
+    for (int k = 0; k < PWA_NCOL * PWA_NOUT; ++k) {
+      row[2 * k] = Fk[k].re;
+      row[2 * k + 1] = Fk[k].im;
+    }
+  }
+}
+
+// Block partials of the weighted Gram matrix over rows of F (n rows of
+// NCOL*NOUT complex).  Each thread owns (k,l) pairs; events are staged
+// through shared memory in tiles of PWA_TPB rows.
+extern "C" __global__ void __launch_bounds__(PWA_TPB)
+    pwa_gram_f64(const double* __restrict__ F, const double* __restrict__ W, long long n,
+                 double* __restrict__ partials) {
+  constexpr int NC = PWA_NCOL, NO = PWA_NOUT, ROW = 2 * NC * NO;
+  constexpr int TILE = (PWA_TPB * 8 + ROW - 1) / ROW > 0 ? (PWA_TPB * 8 + ROW - 1) / ROW : 1;
+  __shared__ double tile[TILE * ROW];
+  __shared__ double wt[TILE];
+  double accr[(NC * NC + PWA_TPB - 1) / PWA_TPB];
+  double acci[(NC * NC + PWA_TPB - 1) / PWA_TPB];
+  constexpr int PER = (NC * NC + PWA_TPB - 1) / PWA_TPB;
+#pragma unroll
+  for (int p = 0; p < PER; ++p) accr[p] = acci[p] = 0.0;
+  for (long long t0 = (long long)blockIdx.x * TILE; t0 < n; t0 += (long long)gridDim.x * TILE) {
+    const int rows = (int)((n - t0) < TILE ? (n - t0) : TILE);
+    __syncthreads();
+    for (int j = threadIdx.x; j < rows * ROW; j += PWA_TPB) tile[j] = F[t0 * ROW + j];
+    for (int j = threadIdx.x; j < rows; j += PWA_TPB) wt[j] = W[t0 + j];
+    __syncthreads();
+#pragma unroll
+    for (int p = 0; p < PER; ++p) {
+      const int kl = threadIdx.x + p * PWA_TPB;
+      if (kl < NC * NC) {
+        const int k = kl / NC, l = kl % NC;
+        double sr = 0.0, si = 0.0;
+        for (int r = 0; r < rows; ++r) {
+          double tr = 0.0, ti = 0.0;
+#pragma unroll
+          for (int o = 0; o < NO; ++o) {
+            const double ar = tile[r * ROW + 2 * (k * NO + o)], ai = tile[r * ROW + 2 * (k * NO + o) + 1];
+            const double br = tile[r * ROW + 2 * (l * NO + o)], bi = tile[r * ROW + 2 * (l * NO + o) + 1];
+            // conj(a) * b
+            tr += ar * br + ai * bi;
+            ti += ar * bi - ai * br;
+          }
+          sr = fma(wt[r], tr, sr);
+          si = fma(wt[r], ti, si);
+        }
+        accr[p] += sr;
+        acci[p] += si;
+      }
+    }
+  }
+#pragma unroll
+  for (int p = 0; p < PER; ++p) {
+    const int kl = threadIdx.x + p * PWA_TPB;
+    if (kl < NC * NC) {
+      partials[(long long)blockIdx.x * 2 * NC * NC + 2 * kl] = accr[p];
+      partials[(long long)blockIdx.x * 2 * NC * NC + 2 * kl + 1] = acci[p];
+    }
+  }
+}
+
+// Column-wise deterministic sum of nrows rows of width ncols.
+extern "C" __global__ void pwa_sum_rows(const double* __restrict__ in, int nrows, int ncols,
+                                        double* __restrict__ out) {
+  const int lane = threadIdx.x & 31;
+  const int warps = blockDim.x >> 5;
+  for (int j = (int)(blockIdx.x * warps + (threadIdx.x >> 5)); j < ncols; j += gridDim.x * warps) {
+    double s = 0.0;
+    for (int r = lane; r < nrows; r += 32) s += in[(long long)r * ncols + j];
+    s = warp_sum(s);
+    if (lane == 0) out[j] = s;
+  }
+}
+
+// FP64 -> FP32 copy of the angle columns for the mixed-precision kernels.
+extern "C" __global__ void pwa_to_f32(const double* __restrict__ in, float* __restrict__ out,
+                                      long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = (float)in[i];
+}

@@ -1,0 +1,412 @@
+// Host runtime of the B200 amplitude-fit engine: the C ABI of
+// include/pwa_b200.h.
+//
+// A plan owns one NVRTC-compiled module (device headers of this library +
+// the generated model code), the resident event columns, the block-partial
+// scratch and a pinned host buffer for the per-evaluation result.
+//
+// Launch geometry: the fused evaluation kernel runs persistent blocks,
+// (blocks per SM from the occupancy API) x (number of SMs), split between
+// the data and the MC event sets in proportion to their sizes.
+#include <cuda_runtime.h>
+#include <nvrtc.h>
+
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/pwa_b200.h"
+
+namespace {
+
+#include "_embedded.inc"  // kDeviceHeader, kKernelsHeader (text of the .cuh files)
+
+struct Kernels {
+  cudaKernel_t eval_f64 = nullptr, eval_f32 = nullptr, reduce = nullptr, pdf_f64 = nullptr,
+               pdf_f32 = nullptr, columns_f64 = nullptr, gram_f64 = nullptr, sum_rows = nullptr,
+               to_f32 = nullptr;
+};
+
+}  // namespace
+
+struct pwa_plan {
+  std::string err;
+  cudaLibrary_t lib = nullptr;
+  Kernels k;
+  int n_mass = 0, n_angle = 0, ncol = 0, nout = 0, nshape = 0, nconst = 0, nacc = 0, tpb = 128;
+  int regs[2] = {0, 0};
+  long long local_bytes[2] = {0, 0};
+  int device = 0, sms = 0;
+  int nblocks = 0, blocks_data = 0;
+  // events
+  double* xm = nullptr;
+  double* xa = nullptr;
+  float* xa32 = nullptr;
+  double* w = nullptr;
+  long long n_data = 0, n_mc = 0, ld = 0, cap = 0;
+  // scratch
+  double* partials = nullptr;
+  long long partials_cap = 0;
+  double* d_out = nullptr;
+  double* h_out = nullptr;
+};
+
+namespace {
+
+int set_err(pwa_plan* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  return code;
+}
+
+#define CU(call)                                                                       \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess)                                                             \
+      return set_err(h, PWA_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+int ensure_partials(pwa_plan* h, long long n) {
+  if (n <= h->partials_cap) return PWA_OK;
+  if (h->partials) cudaFree(h->partials);
+  h->partials = nullptr;
+  h->partials_cap = 0;
+  if (cudaMalloc(&h->partials, sizeof(double) * n) != cudaSuccess)
+    return set_err(h, PWA_ERR_OOM, "cudaMalloc partials failed");
+  h->partials_cap = n;
+  return PWA_OK;
+}
+
+void free_events(pwa_plan* h) {
+  if (h->xm) cudaFree(h->xm);
+  if (h->xa) cudaFree(h->xa);
+  if (h->xa32) cudaFree(h->xa32);
+  if (h->w) cudaFree(h->w);
+  h->xm = h->xa = h->w = nullptr;
+  h->xa32 = nullptr;
+  h->cap = 0;
+}
+
+
+std::string full_source(const char* src, size_t src_len, int tpb) {
+  std::string full;
+  full.reserve(src_len + 65536);
+  full += "#define PWA_TPB " + std::to_string(tpb) + "\n";
+  full += kDeviceHeader;
+  full += "\n";
+  full.append(src, src_len);
+  full += "\n";
+  full += kKernelsHeader;
+  return full;
+}
+
+// NVRTC compile of the full module for `arch` (e.g. "sm_100a").
+int compile_cubin(const char* src, size_t src_len, int tpb, const std::string& arch, bool verbose,
+                  std::vector<char>* cubin, std::string* log) {
+  const std::string full = full_source(src, src_len, tpb);
+  nvrtcProgram prog;
+  if (nvrtcCreateProgram(&prog, full.c_str(), "pwa_model.cu", 0, nullptr, nullptr) !=
+      NVRTC_SUCCESS) {
+    *log = "nvrtcCreateProgram failed";
+    return PWA_ERR_COMPILE;
+  }
+  const std::string a = "--gpu-architecture=" + arch;
+  std::vector<const char*> opts = {a.c_str(), "-std=c++17", "-lineinfo"};
+  if (verbose) opts.push_back("--ptxas-options=-v");
+  nvrtcResult r = nvrtcCompileProgram(prog, (int)opts.size(), opts.data());
+  size_t log_size = 0;
+  nvrtcGetProgramLogSize(prog, &log_size);
+  log->assign(log_size, '\0');
+  if (log_size) nvrtcGetProgramLog(prog, &(*log)[0]);
+  if (r != NVRTC_SUCCESS) {
+    nvrtcDestroyProgram(&prog);
+    return PWA_ERR_COMPILE;
+  }
+  size_t n = 0;
+  if (nvrtcGetCUBINSize(prog, &n) != NVRTC_SUCCESS || n == 0) {
+    nvrtcDestroyProgram(&prog);
+    *log += "\nno cubin produced";
+    return PWA_ERR_COMPILE;
+  }
+  cubin->resize(n);
+  nvrtcGetCUBIN(prog, cubin->data());
+  nvrtcDestroyProgram(&prog);
+  return PWA_OK;
+}
+
+int launch(pwa_plan* h, cudaKernel_t k, dim3 grid, dim3 block, void** args, cudaStream_t s) {
+  cudaError_t e = cudaLaunchKernel((const void*)k, grid, block, args, 0, s);
+  if (e != cudaSuccess)
+    return set_err(h, PWA_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+  return PWA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pwa_compile_only(const char* src, size_t src_len, int tpb, const char* arch, char* log_buf,
+                     size_t log_len) {
+  if (!src || !arch || tpb < 32 || tpb > 1024 || tpb % 32) return PWA_ERR_ARG;
+  std::vector<char> cubin;
+  std::string log;
+  int rc = compile_cubin(src, src_len, tpb, arch, true, &cubin, &log);
+  if (log_buf && log_len) {
+    std::strncpy(log_buf, log.c_str(), log_len - 1);
+    log_buf[log_len - 1] = '\0';
+  }
+  return rc;
+}
+
+int pwa_plan_create(const char* src, size_t src_len, int n_mass, int n_angle, int ncol, int nout,
+                    int nshape, int nconst, int tpb, pwa_plan** out) {
+  if (!out) return PWA_ERR_ARG;
+  *out = nullptr;
+  pwa_plan* h = new pwa_plan();
+  if (!src || ncol <= 0 || nout <= 0 || nconst <= 0 || n_mass < 0 || n_angle < 0 || nshape < 0 ||
+      tpb < 32 || tpb > 1024 || tpb % 32) {
+    *out = h;
+    return set_err(h, PWA_ERR_ARG, "invalid plan sizes");
+  }
+  h->n_mass = n_mass;
+  h->n_angle = n_angle;
+  h->ncol = ncol;
+  h->nout = nout;
+  h->nshape = nshape;
+  h->nconst = nconst;
+  h->nacc = 1 + 2 * ncol + nshape;
+  h->tpb = tpb;
+  *out = h;
+  CU(cudaGetDevice(&h->device));
+  CU(cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, h->device));
+  int major = 0, minor = 0;
+  CU(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, h->device));
+  CU(cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, h->device));
+
+  std::vector<char> cubin;
+  std::string log;
+  std::string arch = "sm_" + std::to_string(major * 10 + minor) + (major == 10 && minor == 0 ? "a" : "");
+  if (compile_cubin(src, src_len, tpb, arch, false, &cubin, &log) != PWA_OK)
+    return set_err(h, PWA_ERR_COMPILE, "NVRTC: " + log);
+  CU(cudaLibraryLoadData(&h->lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0));
+  struct {
+    const char* name;
+    cudaKernel_t* slot;
+  } ks[] = {{"pwa_eval_f64", &h->k.eval_f64},       {"pwa_eval_f32", &h->k.eval_f32},
+            {"pwa_reduce", &h->k.reduce},           {"pwa_pdf_f64", &h->k.pdf_f64},
+            {"pwa_pdf_f32", &h->k.pdf_f32},         {"pwa_columns_f64", &h->k.columns_f64},
+            {"pwa_gram_f64", &h->k.gram_f64},       {"pwa_sum_rows", &h->k.sum_rows},
+            {"pwa_to_f32", &h->k.to_f32}};
+  for (auto& e : ks) CU(cudaLibraryGetKernel(e.slot, h->lib, e.name));
+  for (int p = 0; p < 2; ++p) {
+    cudaFuncAttributes a;
+    CU(cudaFuncGetAttributes(&a, (const void*)(p ? h->k.eval_f32 : h->k.eval_f64)));
+    h->regs[p] = a.numRegs;
+    h->local_bytes[p] = (long long)a.localSizeBytes;
+  }
+  CU(cudaMalloc(&h->d_out, sizeof(double) * 2 * h->nacc));
+  CU(cudaMallocHost(&h->h_out, sizeof(double) * 2 * (h->nacc > ncol * ncol ? h->nacc : ncol * ncol)));
+  return PWA_OK;
+}
+
+int pwa_plan_destroy(pwa_plan* h) {
+  if (!h) return PWA_OK;
+  free_events(h);
+  if (h->partials) cudaFree(h->partials);
+  if (h->d_out) cudaFree(h->d_out);
+  if (h->h_out) cudaFreeHost(h->h_out);
+  if (h->lib) cudaLibraryUnload(h->lib);
+  delete h;
+  return PWA_OK;
+}
+
+int pwa_upload_events(pwa_plan* h, const double* xm, const double* xa, const double* w,
+                      long long n_data, long long n_mc, int on_device, void* stream) {
+  if (!h) return PWA_ERR_ARG;
+  if (!h->lib) return set_err(h, PWA_ERR_STATE, "plan not compiled");
+  if (n_data < 0 || n_mc < 0 || n_data + n_mc <= 0 || !w || (h->n_mass && !xm) ||
+      (h->n_angle && !xa))
+    return set_err(h, PWA_ERR_ARG, "invalid event arrays");
+  cudaStream_t s = (cudaStream_t)stream;
+  const long long n = n_data + n_mc;
+  const long long ld = (n + 31) / 32 * 32;  // 256-byte aligned columns
+  if (ld > h->cap) {
+    free_events(h);
+    size_t bm = sizeof(double) * (size_t)ld * (h->n_mass > 0 ? h->n_mass : 1);
+    size_t ba = sizeof(double) * (size_t)ld * (h->n_angle > 0 ? h->n_angle : 1);
+    if (cudaMalloc(&h->xm, bm) != cudaSuccess || cudaMalloc(&h->xa, ba) != cudaSuccess ||
+        cudaMalloc(&h->xa32, ba / 2) != cudaSuccess ||
+        cudaMalloc(&h->w, sizeof(double) * ld) != cudaSuccess) {
+      free_events(h);
+      return set_err(h, PWA_ERR_OOM, "cudaMalloc of event columns failed");
+    }
+    h->cap = ld;
+  }
+  h->ld = ld;
+  h->n_data = n_data;
+  h->n_mc = n_mc;
+  const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  if (h->n_mass)
+    CU(cudaMemcpy2DAsync(h->xm, sizeof(double) * ld, xm, sizeof(double) * n, sizeof(double) * n,
+                         h->n_mass, kind, s));
+  if (h->n_angle)
+    CU(cudaMemcpy2DAsync(h->xa, sizeof(double) * ld, xa, sizeof(double) * n, sizeof(double) * n,
+                         h->n_angle, kind, s));
+  CU(cudaMemcpyAsync(h->w, w, sizeof(double) * n, kind, s));
+  if (h->n_angle) {
+    long long tot = ld * h->n_angle;
+    void* args[] = {&h->xa, &h->xa32, &tot};
+    int rc = launch(h, h->k.to_f32, dim3(h->sms * 4), dim3(256), args, s);
+    if (rc) return rc;
+  }
+  // persistent grid: occupancy-limited blocks on every SM, split by set size
+  int per_sm = 0;
+  CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)h->k.eval_f64, h->tpb, 0));
+  if (per_sm < 1) per_sm = 1;
+  long long want = (long long)per_sm * h->sms;
+  long long need = (n + h->tpb - 1) / h->tpb;
+  long long nb = want < need ? want : need;
+  if (nb < 2) nb = 2;
+  long long bd = n_mc == 0 ? nb : (n_data == 0 ? 0 : (nb * n_data + n / 2) / n);
+  if (n_data > 0 && bd < 1) bd = 1;
+  if (n_mc > 0 && bd > nb - 1) bd = nb - 1;
+  h->nblocks = (int)nb;
+  h->blocks_data = (int)bd;
+  int rc = ensure_partials(h, (long long)h->nblocks * h->nacc);
+  if (rc) return rc;
+  CU(cudaStreamSynchronize(s));
+  return PWA_OK;
+}
+
+int pwa_eval(pwa_plan* h, const double* consts, int precision, int mc, void* stream, double* out) {
+  if (!h) return PWA_ERR_ARG;
+  if (!h->w) return set_err(h, PWA_ERR_STATE, "no events uploaded");
+  if (!consts || !out || (precision != PWA_PLAIN_F64 && precision != PWA_MIXED_F32))
+    return set_err(h, PWA_ERR_ARG, "invalid eval arguments");
+  cudaStream_t s = (cudaStream_t)stream;
+  std::vector<double> cbuf(consts, consts + h->nconst);
+  long long n_all = mc ? h->n_data + h->n_mc : h->n_data;
+  int nblocks = mc ? h->nblocks : h->blocks_data;
+  if (!mc && h->n_mc == 0) nblocks = h->nblocks;
+  int bd = mc ? h->blocks_data : nblocks;
+  const void* xa = precision == PWA_PLAIN_F64 ? (const void*)h->xa : (const void*)h->xa32;
+  long long nd = h->n_data, ld = h->ld;
+  void* args[] = {cbuf.data(), (void*)&xa, &h->xm, &h->w, &nd, &n_all, &ld, &bd, &h->partials};
+  int rc = launch(h, precision == PWA_PLAIN_F64 ? h->k.eval_f64 : h->k.eval_f32, dim3(nblocks),
+                  dim3(h->tpb), args, s);
+  if (rc) return rc;
+  int nacc = h->nacc;
+  void* args2[] = {&h->partials, &nacc, &bd, &nblocks, &h->d_out};
+  rc = launch(h, h->k.reduce, dim3(1), dim3(1024), args2, s);
+  if (rc) return rc;
+  CU(cudaMemcpyAsync(h->h_out, h->d_out, sizeof(double) * 2 * nacc, cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  std::memcpy(out, h->h_out, sizeof(double) * 2 * nacc);
+  if (!mc)
+    for (int j = 0; j < nacc; ++j) out[nacc + j] = 0.0;
+  return PWA_OK;
+}
+
+int pwa_eval_pdf(pwa_plan* h, const double* consts, int precision, long long beg, long long end,
+                 double* out_dev, void* stream) {
+  if (!h) return PWA_ERR_ARG;
+  if (!h->w) return set_err(h, PWA_ERR_STATE, "no events uploaded");
+  if (!consts || !out_dev || beg < 0 || end < beg || end > h->n_data + h->n_mc)
+    return set_err(h, PWA_ERR_ARG, "invalid pdf arguments");
+  if (end == beg) return PWA_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  std::vector<double> cbuf(consts, consts + h->nconst);
+  const void* xa = precision == PWA_PLAIN_F64 ? (const void*)h->xa : (const void*)h->xa32;
+  long long ld = h->ld;
+  void* args[] = {cbuf.data(), (void*)&xa, &h->xm, &beg, &end, &ld, &out_dev};
+  long long nb = (end - beg + h->tpb - 1) / h->tpb;
+  if (nb > 8LL * h->sms) nb = 8LL * h->sms;
+  int rc = launch(h, precision == PWA_PLAIN_F64 ? h->k.pdf_f64 : h->k.pdf_f32, dim3((int)nb),
+                  dim3(h->tpb), args, s);
+  if (rc) return rc;
+  CU(cudaStreamSynchronize(s));
+  return PWA_OK;
+}
+
+int pwa_build_gram(pwa_plan* h, const double* consts, void* stream, double* out) {
+  if (!h) return PWA_ERR_ARG;
+  if (!h->w || h->n_mc <= 0) return set_err(h, PWA_ERR_STATE, "no MC events uploaded");
+  if (!consts || !out) return set_err(h, PWA_ERR_ARG, "invalid gram arguments");
+  cudaStream_t s = (cudaStream_t)stream;
+  std::vector<double> cbuf(consts, consts + h->nconst);
+  const long long row = 2LL * h->ncol * h->nout;
+  // chunked: columns of at most `chunk` events at a time
+  long long chunk = (256LL << 20) / (8 * row);
+  if (chunk < 1024) chunk = 1024;
+  if (chunk > h->n_mc) chunk = h->n_mc;
+  double* F = nullptr;
+  if (cudaMalloc(&F, sizeof(double) * row * chunk) != cudaSuccess)
+    return set_err(h, PWA_ERR_OOM, "cudaMalloc gram columns failed");
+  const int gb = h->sms * 2;
+  const long long nkk = 2LL * h->ncol * h->ncol;
+  double* gpart = nullptr;
+  double* gsum = nullptr;
+  double* gtot = nullptr;
+  if (cudaMalloc(&gpart, sizeof(double) * nkk * gb) != cudaSuccess ||
+      cudaMalloc(&gsum, sizeof(double) * nkk) != cudaSuccess ||
+      cudaMalloc(&gtot, sizeof(double) * nkk) != cudaSuccess) {
+    cudaFree(F);
+    if (gpart) cudaFree(gpart);
+    if (gsum) cudaFree(gsum);
+    return set_err(h, PWA_ERR_OOM, "cudaMalloc gram partials failed");
+  }
+  int rc = PWA_OK;
+  std::vector<double> acc(nkk, 0.0), part(nkk);
+  long long ld = h->ld;
+  for (long long b0 = h->n_data; b0 < h->n_data + h->n_mc && rc == PWA_OK; b0 += chunk) {
+    long long b1 = b0 + chunk < h->n_data + h->n_mc ? b0 + chunk : h->n_data + h->n_mc;
+    long long cnt = b1 - b0;
+    void* a1[] = {cbuf.data(), &h->xa, &h->xm, &b0, &b1, &ld, &F};
+    long long nb = (cnt + h->tpb - 1) / h->tpb;
+    if (nb > 8LL * h->sms) nb = 8LL * h->sms;
+    rc = launch(h, h->k.columns_f64, dim3((int)nb), dim3(h->tpb), a1, s);
+    if (rc) break;
+    double* wptr = h->w + b0;
+    void* a2[] = {&F, &wptr, &cnt, &gpart};
+    rc = launch(h, h->k.gram_f64, dim3(gb), dim3(h->tpb), a2, s);
+    if (rc) break;
+    int nrows = gb, ncols = (int)nkk;
+    void* a3[] = {&gpart, &nrows, &ncols, &gsum};
+    rc = launch(h, h->k.sum_rows, dim3(16), dim3(256), a3, s);
+    if (rc) break;
+    if (cudaMemcpyAsync(part.data(), gsum, sizeof(double) * nkk, cudaMemcpyDeviceToHost, s) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+      rc = set_err(h, PWA_ERR_CUDA, "gram copy failed");
+      break;
+    }
+    for (long long j = 0; j < nkk; ++j) acc[j] += part[j];
+  }
+  cudaFree(F);
+  cudaFree(gpart);
+  cudaFree(gsum);
+  cudaFree(gtot);
+  if (rc) return rc;
+  std::memcpy(out, acc.data(), sizeof(double) * nkk);
+  return PWA_OK;
+}
+
+int pwa_plan_info(pwa_plan* h, long long* info) {
+  if (!h || !info) return PWA_ERR_ARG;
+  info[0] = h->regs[0];
+  info[1] = h->regs[1];
+  info[2] = h->local_bytes[0];
+  info[3] = h->local_bytes[1];
+  info[4] = h->nblocks;
+  info[5] = h->blocks_data;
+  info[6] = h->nacc;
+  info[7] = h->tpb;
+  return PWA_OK;
+}
+
+const char* pwa_last_error(pwa_plan* h) {
+  if (!h) return "null plan handle";
+  return h->err.c_str();
+}
+
+}  // extern "C"

@@ -1,0 +1,434 @@
+"""Python side of the engine: ctypes binding of ``libpwa_b200.so``, the
+per-evaluation constant block, and the chain rule from the kernel's FP64
+sums to the NLL and its gradient.
+
+NLL (``tf_pwa/model/model.py:407-449``)::
+
+    NLL = -sum_data w clip_log(f) + (sum_data w) * ln( sum_MC w~ f )
+
+with data weights alpha-scaled (``model.py:603-641``) and MC weights
+normalised to 1 (``model.py:1155-1161``).  The kernel returns, per event set,
+S0 = sum w t(f), Gk = sum fac * G_k and the lineshape sums; the derivative of
+f with respect to a real parameter theta is
+
+    df/dtheta = 2 Re sum_k J_k(theta) G_k + (lineshape term),
+
+J_k = dc_k/dtheta + c_k * kappa_k(theta), c_k the product of the column's
+complex couplings (chain total and one g_ls per vertex) and kappa_k the
+derivative of the column's log barrier factors through q0 (nominal masses).
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from .codegen import ModelCode
+from .particles import bprime_coeff
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpwa_b200.so")
+
+PLAIN_F64 = 0
+MIXED_F32 = 1
+
+_lib = None
+
+
+def load_library(path=LIB_PATH):
+    """Load the native library; raises if it is missing (no CPU fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(
+            f"{path} not found: build it first (python -c 'import __graft_entry__ as g; g.build()')")
+    lib = ctypes.CDLL(path)
+    vp, cp, i, ll, dp, sz = (ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_longlong,
+                             ctypes.POINTER(ctypes.c_double), ctypes.c_size_t)
+    lib.pwa_plan_create.argtypes = [cp, sz, i, i, i, i, i, i, i, ctypes.POINTER(vp)]
+    lib.pwa_plan_destroy.argtypes = [vp]
+    lib.pwa_compile_only.argtypes = [cp, sz, i, cp, cp, sz]
+    lib.pwa_upload_events.argtypes = [vp, vp, vp, vp, ll, ll, i, vp]
+    lib.pwa_eval.argtypes = [vp, dp, i, i, vp, dp]
+    lib.pwa_eval_pdf.argtypes = [vp, dp, i, ll, ll, vp, vp]
+    lib.pwa_build_gram.argtypes = [vp, dp, vp, dp]
+    lib.pwa_plan_info.argtypes = [vp, ctypes.POINTER(ll)]
+    lib.pwa_last_error.argtypes = [vp]
+    lib.pwa_last_error.restype = cp
+    for f in ("pwa_plan_create", "pwa_plan_destroy", "pwa_compile_only", "pwa_upload_events",
+              "pwa_eval", "pwa_eval_pdf", "pwa_build_gram", "pwa_plan_info"):
+        getattr(lib, f).restype = i
+    _lib = lib
+    return lib
+
+
+EXPORTED = ("pwa_plan_create", "pwa_plan_destroy", "pwa_compile_only", "pwa_upload_events",
+            "pwa_eval", "pwa_eval_pdf", "pwa_build_gram", "pwa_plan_info", "pwa_last_error")
+
+
+class PWAError(RuntimeError):
+    pass
+
+
+def _dptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+# ----------------------------------------------------------- host formulae
+def rel_p2(m0, m1, m2):
+    s, d = m1 + m2, m1 - m2
+    return (m0 - s) * (m0 + s) * (m0 - d) * (m0 + d) / (2 * m0) ** 2
+
+
+def rel_p(m0, m1, m2):
+    s, d = m1 + m2, m1 - m2
+    me = m0 if np.real(m0) > np.real(s) else s
+    p = (me - s) * (me + s) * (me - d) * (me + d)
+    return np.sqrt(p) / (2 * me)
+
+
+def poly(l, z):
+    r = 0.0
+    for c in bprime_coeff(l):
+        r = r * z + c
+    return r
+
+
+class Engine:
+    """A compiled model bound to a device: events, constants, evaluation."""
+
+    def __init__(self, group, plan, vm, tpb=128, compile=True):
+        self.group = group
+        self.plan = plan
+        self.vm = vm
+        self.code = ModelCode(group, plan)
+        self.src = self.code.source()
+        self.tpb = tpb
+        self.h = None
+        self._n_data = self._n_mc = 0
+        self._sw = None
+        self._gram = None
+        self._prepare_structure()
+        if compile:
+            self._create()
+
+    # ------------------------------------------------------------- native
+    def _create(self):
+        lib = load_library()
+        c = self.code
+        h = ctypes.c_void_p()
+        src = self.src.encode()
+        rc = lib.pwa_plan_create(src, len(src), len(c.mass_fields), len(c.angle_fields), c.ncol,
+                                 c.nout, c.nshape, len(c.consts), self.tpb, ctypes.byref(h))
+        if rc != 0:
+            msg = lib.pwa_last_error(h).decode(errors="replace")
+            lib.pwa_plan_destroy(h)
+            raise PWAError(f"pwa_plan_create failed ({rc}): {msg}")
+        self.h = h
+
+    def close(self):
+        if self.h is not None:
+            load_library().pwa_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc, what):
+        if rc != 0:
+            msg = load_library().pwa_last_error(self.h).decode(errors="replace")
+            raise PWAError(f"{what} failed ({rc}): {msg}")
+
+    def info(self):
+        arr = (ctypes.c_longlong * 8)()
+        self._check(load_library().pwa_plan_info(self.h, arr), "pwa_plan_info")
+        keys = ("regs_f64", "regs_f32", "local_f64", "local_f32", "blocks", "blocks_data",
+                "nacc", "tpb")
+        return dict(zip(keys, list(arr)))
+
+    def compile_check(self, arch="sm_100a"):
+        """NVRTC compile without a device; returns the ptxas log."""
+        buf = ctypes.create_string_buffer(1 << 16)
+        src = self.src.encode()
+        rc = load_library().pwa_compile_only(src, len(src), self.tpb, arch.encode(), buf, len(buf))
+        log = buf.value.decode(errors="replace")
+        if rc != 0:
+            raise PWAError(f"compile failed: {log}")
+        return log
+
+    # ------------------------------------------------------------- events
+    def split_fields(self, x):
+        """(n_fields, N) plan-ordered columns -> (mass columns, angle columns)."""
+        c = self.code
+        x = np.asarray(x, np.float64)
+        xm = np.ascontiguousarray(x[c.mass_fields]) if c.mass_fields else np.zeros((0, x.shape[1]))
+        xa = np.ascontiguousarray(x[c.angle_fields]) if c.angle_fields else np.zeros((0, x.shape[1]))
+        return xm, xa
+
+    def upload(self, x_data, w_data, x_mc=None, w_mc=None, stream=None):
+        """Make data (+ MC) events resident.  x_*: (n_fields, N) columns in
+        plan order; w_data: final data weights; w_mc: raw MC weights
+        (normalised here to sum 1)."""
+        xd = np.asarray(x_data, np.float64)
+        wd = np.asarray(w_data, np.float64)
+        nd = xd.shape[1]
+        if x_mc is None:
+            x = xd
+            w = wd
+            nm = 0
+        else:
+            xmc = np.asarray(x_mc, np.float64)
+            nm = xmc.shape[1]
+            wm = np.ones(nm) if w_mc is None else np.asarray(w_mc, np.float64)
+            wm = wm / wm.sum()
+            x = np.concatenate([xd, xmc], axis=1)
+            w = np.concatenate([wd, wm])
+        xm, xa = self.split_fields(x)
+        w = np.ascontiguousarray(w)
+        self._check(load_library().pwa_upload_events(
+            self.h, xm.ctypes.data, xa.ctypes.data, w.ctypes.data, nd, nm, 0,
+            stream or 0), "pwa_upload_events")
+        self._n_data, self._n_mc = nd, nm
+        self._sw = float(wd.sum())
+        self._gram = None
+
+    def upload_device(self, xm_ptr, xa_ptr, w_ptr, n_data, n_mc, sw, stream=None):
+        """Events already on the device (pointers to FP64 row-major columns)."""
+        self._check(load_library().pwa_upload_events(
+            self.h, xm_ptr, xa_ptr, w_ptr, n_data, n_mc, 1, stream or 0), "pwa_upload_events")
+        self._n_data, self._n_mc = n_data, n_mc
+        self._sw = float(sw)
+        self._gram = None
+
+    # ---------------------------------------------------------- structure
+    def _prepare_structure(self):
+        g = self.group
+        self.coupling_names = []   # complex names per column factor
+        self.col_factors = []
+        for ci, lsi in self.code.columns:
+            c = g[ci]
+            names = [c.params_head + "_total_0"]
+            for vi, d in enumerate(c):
+                names.append(f"{d.params_head}_g_ls_{lsi[vi]}")
+            self.col_factors.append(names)
+            for n in names:
+                if n not in self.coupling_names:
+                    self.coupling_names.append(n)
+        self.res_info = {}
+        for p in g.resonances:
+            chains = [c for c in g if p in c.inner]
+            dp = chains[0].decay_of(p)
+            self.res_info[p] = (dp, chains[0])
+        self.shape_index = {}
+        for si, p in enumerate(self.code.shape_res):
+            self.shape_index[(p, "m")] = 2 * si
+            self.shape_index[(p, "g")] = 2 * si + 1
+
+    def _nominal(self, p, vals, chain):
+        if p in chain.inner:
+            return vals.get(f"{p.params_head}_mass", p.mass)
+        return p.mass
+
+    def complex_val(self, vals, name):
+        r, i = vals[name + "r"], vals[name + "i"]
+        if self.vm.complex_vars.get(name, True):
+            return r * np.cos(i) + 1j * r * np.sin(i)
+        return r + 1j * i
+
+    def _vertex_consts(self, d, chain, vals, m_override=None):
+        """{l: (Pz0_l, norm_l)} of vertex d, masses optionally overridden."""
+        a, (b, c) = d.core, d.outs
+        mv = lambda p: (m_override[p] if m_override and p in m_override else self._nominal(p, vals, chain))  # noqa: E731
+        q02 = rel_p2(mv(a), mv(b), mv(c))
+        if d.no_q0:
+            q02 = 1.0 + 0 * q02
+        out = {}
+        for l in sorted(set(d.get_l_list())):
+            pz0 = poly(l, q02 * d.d * d.d) if d.has_bprime else 1.0
+            norm = 1.0 / np.abs(q02) ** (l / 2) if d.barrier_factor_norm else 1.0
+            if isinstance(q02, complex) or np.iscomplexobj(q02):
+                norm = 1.0 / np.sqrt(q02 * q02) ** (l / 2) if d.barrier_factor_norm else 1.0
+            out[l] = (pz0, norm)
+        return out
+
+    def _lineshape_K(self, p, vals, m0=None):
+        kind = p.lineshape_kind()
+        dp, chain = self.res_info[p]
+        m0 = self._nominal(p, vals, chain) if m0 is None else m0
+        g0 = vals.get(f"{p.params_head}_width", p.width)
+        if kind == "BW":
+            return m0 * g0, 1.0
+        b, c = dp.outs
+        L = p.bw_l if p.bw_l is not None else min(dp.get_l_list())
+        q0 = rel_p(m0, self._nominal(b, vals, chain), self._nominal(c, vals, chain))
+        pz0 = poly(L, (q0 * p.d) ** 2)
+        if np.real(q0) > 1e-15:
+            return m0 * m0 * g0 * pz0 / q0 ** (2 * L + 1), 1.0
+        return m0 * m0 * g0 * pz0, 0.0
+
+    def consts(self, vals):
+        """Constant block of one evaluation from the parameter dict."""
+        c = self.code
+        C = np.zeros(len(c.consts))
+        idx = c.consts.index
+        cv = {n: self.complex_val(vals, n) for n in self.coupling_names}
+        self._ck = np.array([np.prod([cv[n] for n in f]) for f in self.col_factors])
+        self._cv = cv
+        C[0:2 * c.ncol:2] = self._ck.real
+        C[1:2 * c.ncol:2] = self._ck.imag
+        for p, kind in c.res:
+            if kind == "one":
+                continue
+            dp, chain = self.res_info[p]
+            m0 = self._nominal(p, vals, chain)
+            C[idx[f"{p}.m0sq"]] = m0 * m0
+            if kind == "BWR":
+                K, useq = self._lineshape_K(p, vals)
+                C[idx[f"{p}.K"]] = K
+                C[idx[f"{p}.useq"]] = useq
+            else:
+                C[idx[f"{p}.y"]] = m0 * vals.get(f"{p.params_head}_width", p.width)
+        for d in c.vertices:
+            chain = [ch for ch in self.group if d in ch.decays][0]
+            vc = self._vertex_consts(d, chain, vals)
+            for l, (pz0, norm) in vc.items():
+                if d.has_barrier_factor and d.has_bprime:
+                    C[idx[f"{d}.Pz0_{l}"]] = pz0
+                if d.has_barrier_factor and d.barrier_factor_norm:
+                    C[idx[f"{d}.norm_{l}"]] = norm
+        for p in c.shape_res:
+            dp, chain = self.res_info[p]
+            m0 = self._nominal(p, vals, chain)
+            g0 = vals.get(f"{p.params_head}_width", p.width)
+            h = 1e-20
+            Kc, _ = self._lineshape_K(p, vals, m0=m0 + 1j * h)
+            K0, _ = self._lineshape_K(p, vals, m0=m0)
+            C[idx[f"{p}.kappa_m"]] = np.imag(Kc) / h / np.real(K0) if np.real(K0) != 0 else 0.0
+            C[idx[f"{p}.inv_g0"]] = 1.0 / g0 if g0 else 0.0
+        return C
+
+    # ------------------------------------------------------------ jacobian
+    def jacobian(self, vals, names):
+        """J[p, k] (complex) and shape selectors D[p, s] for parameters
+        ``names`` at ``vals`` (call after consts())."""
+        c = self.code
+        P = len(names)
+        J = np.zeros((P, c.ncol), np.complex128)
+        D = np.zeros((P, max(c.nshape, 1)))
+        cv = self._cv
+        for pi, n in enumerate(names):
+            base = n[:-1]
+            if base in cv:
+                r, ph = vals[base + "r"], vals[base + "i"]
+                polar = self.vm.complex_vars.get(base, True)
+                if polar:
+                    dz = np.exp(1j * ph) if n.endswith("r") else 1j * cv[base]
+                else:
+                    dz = 1.0 if n.endswith("r") else 1j
+                for k, f in enumerate(self.col_factors):
+                    cnt = f.count(base)
+                    if cnt == 0:
+                        continue
+                    others = np.prod([cv[x] for x in f if x != base]) if len(f) > cnt else 1.0
+                    J[pi, k] += cnt * others * cv[base] ** (cnt - 1) * dz
+                continue
+            # masses / widths
+            hit = None
+            for p in self.group.resonances:
+                if n == f"{p.params_head}_mass":
+                    hit = (p, "m")
+                elif n == f"{p.params_head}_width":
+                    hit = (p, "g")
+            if hit is None:
+                raise KeyError(f"unknown parameter {n}")
+            p, kind = hit
+            if (p, kind) in self.shape_index:
+                D[pi, self.shape_index[(p, kind)]] = 1.0
+            if kind == "m":
+                # barrier factors through q0^2 of every vertex touching p
+                for k, (ci, lsi) in enumerate(c.columns):
+                    chain = self.group[ci]
+                    if p not in chain.inner:
+                        continue
+                    kap = 0.0
+                    for vi, d in enumerate(chain):
+                        if p not in (d.core,) + d.outs or not d.has_barrier_factor:
+                            continue
+                        l = d.get_ls_list()[lsi[vi]][0]
+                        hh = 1e-20
+                        m0 = self._nominal(p, vals, chain)
+                        vc = self._vertex_consts(d, chain, vals, {p: m0 + 1j * hh})
+                        v0 = self._vertex_consts(d, chain, vals)
+                        # bf_l ~ sqrt(Pz0_l) * norm_l
+                        if d.has_bprime:
+                            kap += 0.5 * np.imag(vc[l][0]) / hh / np.real(v0[l][0])
+                        if d.barrier_factor_norm:
+                            kap += np.imag(vc[l][1]) / hh / np.real(v0[l][1])
+                    J[pi, k] += self._ck[k] * kap
+        return J, D
+
+    # ------------------------------------------------------------ evaluate
+    def eval_sums(self, C, precision=PLAIN_F64, mc=True, stream=None):
+        nacc = self.code.nacc
+        out = np.zeros(2 * nacc)
+        C = np.ascontiguousarray(C, np.float64)
+        self._check(load_library().pwa_eval(self.h, _dptr(C), precision, 1 if mc else 0,
+                                            stream or 0, _dptr(out)), "pwa_eval")
+        return out[:nacc], out[nacc:]
+
+    def build_gram(self, C, stream=None):
+        K = self.code.ncol
+        out = np.zeros(2 * K * K)
+        C = np.ascontiguousarray(C, np.float64)
+        self._check(load_library().pwa_build_gram(self.h, _dptr(C), stream or 0, _dptr(out)),
+                    "pwa_build_gram")
+        M = out[0::2] + 1j * out[1::2]
+        return M.reshape(K, K)
+
+    def pdf_device(self, C, beg, end, out_ptr, precision=PLAIN_F64, stream=None):
+        C = np.ascontiguousarray(C, np.float64)
+        self._check(load_library().pwa_eval_pdf(self.h, _dptr(C), precision, beg, end, out_ptr,
+                                                stream or 0), "pwa_eval_pdf")
+
+    def nll_grad(self, vals, names, precision=PLAIN_F64, use_gram=False, stream=None):
+        """NLL and gradient w.r.t. ``names`` (real parameter names)."""
+        C = self.consts(vals)
+        J, D = self.jacobian(vals, names)
+        nacc = self.code.nacc
+        K = self.code.ncol
+        if use_gram:
+            if self._gram is None:
+                raise PWAError("gram matrix not built")
+            sd, _ = self.eval_sums(C, precision, mc=False, stream=stream)
+            ck = self._ck
+            M = self._gram
+            I = float(np.real(np.conj(ck) @ M @ ck))
+            # G^mc_k = sum_i w conj(A_i) F_ik = sum_l conj(c_l) M_lk
+            Gm = np.conj(ck) @ M
+            sm = np.zeros(nacc)
+            sm[0] = I
+            sm[1:1 + 2 * K:2] = Gm.real
+            sm[2:2 + 2 * K:2] = Gm.imag
+        else:
+            sd, sm = self.eval_sums(C, precision, mc=True, stream=stream)
+        sw = self._sw
+        Gd = sd[1:1 + 2 * K:2] + 1j * sd[2:2 + 2 * K:2]
+        Gm = sm[1:1 + 2 * K:2] + 1j * sm[2:2 + 2 * K:2]
+        I = sm[0]
+        gd = 2 * np.real(J @ Gd)
+        gm = 2 * np.real(J @ Gm)
+        if self.code.nshape:
+            gd = gd + D @ sd[1 + 2 * K:]
+            gm = gm + D @ sm[1 + 2 * K:]
+        nll = -sd[0] + sw * np.log(I)
+        grad = -gd + sw * gm / I
+        return float(nll), grad
+
+    def set_gram(self, vals):
+        """Build the MC Gram matrix at the current masses/widths."""
+        C = self.consts(vals)
+        self._gram = self.build_gram(C)
+        return self._gram
