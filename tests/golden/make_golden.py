@@ -79,10 +79,10 @@ def main(ref_root):
         M = dc.particle_property[str(top)]["mass"]
         tmp = tempfile.mkdtemp()
         p4 = {}
-        for kind, n in (("data", nd), ("bg", nb), ("phsp", nm)):
+        for kk, (kind, n) in enumerate((("data", nd), ("bg", nb), ("phsp", nm))):
             if n == 0:
                 continue
-            ps = generate_phsp(M, masses, n, rng=rng)
+            ps = generate_phsp(M, masses, n, seed=1000 * seed + kk)
             arr = np.stack(ps, 1)  # (n, n_final, 4)
             p4[kind] = arr
             np.savetxt(os.path.join(tmp, kind + ".dat"), arr.reshape(-1, 4), fmt="%.17g")
