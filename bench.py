@@ -1,0 +1,393 @@
+"""Benchmark: NLL + gradient evaluations per second of the Lambda_c+ -> p K- pi+
+three-chain helicity model at 1e6 signal (+1e5 background rows, weight -0.1)
+data events and 1e6 MC events on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  ``value`` is device-timed evaluations/s of the
+headline (mixed) form: FP32 amplitudes, FP64 log-sum and reductions, MC
+integral from the FP64 Gram matrix (masses/widths fixed); inputs resident in
+HBM, L2 flushed before every timed step.  ``plain_f64`` is the same metric
+for the all-FP64 kernels.  ``e2e`` times the public call ``FCN.nll_grad(x)``
+with host parameters in and host NLL/gradient out.  ``roofline`` covers the
+dominant kernel (the fused data-term kernel), timed with CUDA events on the
+stream it is launched on.  ``cpu_baseline`` times the FP64 CPU oracle on a
+bounded sample of the same workload with all host cores.
+
+Multi-GPU (torchrun, one process per GPU): every rank holds its own full
+workload shard (weak scaling); the per-evaluation FP64 sums are combined
+with one NCCL all-reduce before the host forms NLL and gradient.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+CONFIG = "lc2pkpi.yml"
+N_SIG, N_BG, N_MC = 1_000_000, 100_000, 1_000_000
+BG_WEIGHT = 0.1
+METRIC = "NLL+grad evals/s @1M data+1M MC"
+WORKLOAD = ("Lambda_c+ -> p K- pi+ (Lambda(1520), K*(892), Delta(1232); 3 chains, 8 LS "
+            "columns, 4 helicity combinations), 1e6 accept-reject signal + 1e5 flat background "
+            "(w=-0.1) data rows, 1e6 flat MC")
+
+
+def _pkg():
+    sys.path.insert(0, ROOT)
+    import __graft_entry__ as g
+
+    return g._pkg()
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ----------------------------------------------------------------- clocks
+class Clocks:
+    def __init__(self, path):
+        self.path = path
+        self.proc = None
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv",
+                                          "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self, gpu_index=0):
+        if self.proc is None:
+            return None
+        time.sleep(0.3)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path).read().splitlines()[1:]:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9 or parts[0] != str(gpu_index):
+                continue
+            try:
+                sm.append(float(parts[1].split()[0]))
+                mx = float(parts[2].split()[0])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------- cpu oracle
+_W = {}
+
+
+def _oracle_init(cfg):
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import conftest  # noqa: F401  (package loader)
+    from common import load_model
+    from oracle.pwa_oracle import OracleModel
+
+    dc, vm, plan = load_model(cfg)
+    _W["m"] = OracleModel(dc.decay_group, plan)
+
+
+def _oracle_chunk(args):
+    """Sums of one chunk: data log-term and MC integral with the derivative
+    of each w.r.t. every free complex coupling (what the reference's
+    GradientTape pass produces)."""
+    xd, wd, xm, wm, vals, names = args
+    from oracle.pwa_oracle import clip_log
+
+    m = _W["m"]
+    out = {}
+    for tag, x, w in (("d", xd, wd), ("m", xm, wm)):
+        A = m.amp(x, vals).reshape(x.shape[1], -1)
+        f = np.sum(np.abs(A) ** 2, 1)
+        grads = []
+        for n in names:
+            base = n[:-1]
+            v1, v2 = dict(vals), dict(vals)
+            v1[base + "r"], v1[base + "i"] = 1.0, 0.0
+            v2[base + "r"], v2[base + "i"] = 0.0, 0.0
+            B = (m.amp(x, v1) - m.amp(x, v2)).reshape(A.shape)
+            grads.append(np.sum(np.conj(A) * B, 1))
+        if tag == "d":
+            out["d"] = (np.sum(w * clip_log(f)), [np.sum(w / f * g) for g in grads])
+        else:
+            out["m"] = (np.sum(w * f), [np.sum(w * g) for g in grads])
+    return out
+
+
+class CpuOracle:
+    """FP64 oracle NLL + gradient on a bounded sample, all host cores
+    (spawned worker processes, one chunk of events each)."""
+
+    def __init__(self, n_sample, seed=5):
+        import multiprocessing as mp
+
+        _pkg()
+        from tf_pwa_b200.api import ConfigLoader
+        from tf_pwa_b200.kinematics import event_fields, p4_dict
+        from tf_pwa_b200.phasespace import generate_phsp
+        from tf_pwa_b200.workload import config_path, seeded_params
+
+        cl = ConfigLoader(config_path(CONFIG), seed=seed)
+        vals = seeded_params(cl.vm, seed)
+        pp = cl.decay_config.particle_property
+        order = cl.get_dat_order()
+        M = pp[str(cl.decay_group.top)]["mass"]
+        ms = [pp[o]["mass"] for o in order]
+        gen = lambda s: event_fields(cl.plan, p4_dict(np.stack(  # noqa: E731
+            generate_phsp(M, ms, n_sample, seed=s), 1), order)).numpy()
+        xd, xm = gen(seed), gen(seed + 1)
+        names = sorted({n[:-1] + "r" for n in cl.vm.trainable_vars})
+        self.cores = os.cpu_count() or 1
+        chunks = [c for c in np.array_split(np.arange(n_sample), self.cores) if len(c)]
+        self.args = [(xd[:, c], np.ones(len(c)), xm[:, c], np.ones(len(c)) / n_sample, vals,
+                      names) for c in chunks]
+        self.n = n_sample
+        self.pool = mp.get_context("spawn").Pool(len(self.args), initializer=_oracle_init,
+                                                 initargs=(CONFIG,))
+        self.pool.map(_oracle_chunk, self.args)  # warm
+
+    def step(self):
+        t0 = time.perf_counter()
+        self.pool.map(_oracle_chunk, self.args)
+        return time.perf_counter() - t0
+
+    def scale(self):
+        """sample -> full workload (data + MC events)."""
+        return (N_SIG + N_BG + N_MC) / (2.0 * self.n)
+
+    def describe(self, t):
+        return (f"{self.n} data + {self.n} MC events of the same model per step, FP64 numpy "
+                f"oracle (forward + per-coupling derivative columns), {len(self.args)} spawned "
+                f"workers, {t:.3f} s per step, scaled x{self.scale():.1f} to the full workload")
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
+
+
+def cpu_baseline(n_sample, steps=3):
+    o = CpuOracle(n_sample)
+    try:
+        t = float(np.mean([o.step() for _ in range(steps)]))
+    finally:
+        o.close()
+    return {"value": 1.0 / (t * o.scale()), "unit": "evals/s", "cores": len(o.args),
+            "kind": "port", "sample": o.describe(t)}
+
+
+# ------------------------------------------------------------ reference arm
+def run_reference(args, rank):
+    """The reference's CPU path on the host cores.  TensorFlow is not
+    installed, so the reference package cannot run; its FP64 restatement
+    (the oracle) stands in, on a bounded per-step sample."""
+    if rank != 0:
+        return
+    o = CpuOracle(int(os.environ.get("PWA_REF_SAMPLE", "8000")))
+    try:
+        for _ in range(max(args.warmup, 1)):
+            o.step()
+        ts = [o.step() for _ in range(args.steps)]
+    finally:
+        o.close()
+    t = float(np.mean(ts)) * o.scale()
+    v = 1.0 / t
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "evals/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * t, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "precision": "FP64 CPU (numpy oracle standing in "
+                       "for the reference's TensorFlow CPU path, which is not installed)"},
+            "cpu_baseline": {"value": v, "unit": "evals/s", "cores": len(o.args), "kind": "port",
+                             "sample": o.describe(float(np.mean(ts)))},
+            "e2e": {"value": v, "unit": "evals/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------- our arm
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours")
+    ap.add_argument("--cpu-sample", type=int, default=int(os.environ.get("PWA_CPU_SAMPLE", "2000")))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank)
+    args.warmup = max(args.warmup, 3)
+
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    _pkg()
+    from tf_pwa_b200.engine import MIXED_F32, PLAIN_F64
+    from tf_pwa_b200.api import FCN
+    from tf_pwa_b200.workload import make_dataset
+
+    t_setup = time.perf_counter()
+    cl, data, bg, mc = make_dataset(CONFIG, N_SIG, N_MC, n_bg=N_BG, bg_weight=BG_WEIGHT,
+                                    seed=1 + rank, device="cuda")
+    t_data = time.perf_counter() - t_setup
+    reduce_fn = None
+    if dist is not None:
+        def reduce_fn(vec):
+            t = torch.as_tensor(vec, device="cuda")
+            dist.all_reduce(t)
+            return t.cpu().numpy()
+    fcn = FCN(cl, data, mc, bg=bg, precision="mixed")         # Gram MC term
+    fcn_plain = FCN(cl, data, mc, bg=bg, precision="plain")
+    for f in (fcn, fcn_plain):
+        f.eng.dist_reduce = reduce_fn
+        f.eng.mc_share = 1.0 / world  # equal MC shards
+    x0 = np.array(cl.vm.get_all_val())
+    names = list(cl.vm.trainable_vars)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    def timed(step_fn, k):
+        """k steps, L2 flushed before each; device time from CUDA events."""
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(k)]
+        barrier()
+        for i in range(k):
+            flush.zero_()
+            ev[i][0].record()
+            step_fn()
+            ev[i][1].record()
+        barrier()
+        t = sum(a.elapsed_time(b) for a, b in ev) / 1e3
+        if dist is not None:
+            tt = torch.tensor([t], device="cuda", dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t = float(tt.item())
+        return t
+
+    vals = cl.vm.get_all_dic()
+    eng, eng_p = fcn.eng, fcn_plain.eng
+    # warm-up
+    for _ in range(args.warmup):
+        fcn.nll_grad(x0)
+        fcn_plain.nll_grad(x0)
+    from tf_pwa_b200.workload import _phsp_fields  # noqa: F401
+
+    clocks = Clocks(os.path.join(ROOT, "gpurun_out", f"clocks_rank{rank}.csv")
+                    if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else f"/tmp/clocks{rank}.csv")
+    clocks.start()
+    # headline: one engine evaluation (kernels + host chain rule) per step
+    t_mixed = timed(lambda: eng.nll_grad(vals, names, MIXED_F32, use_gram=True), args.steps)
+    t_plain = timed(lambda: eng_p.nll_grad(vals, names, PLAIN_F64), args.steps)
+    # e2e through the public API with host parameters
+    t_e2e = timed(lambda: fcn.nll_grad(x0), args.steps)
+    # roofline: the fused data-term kernel alone (enqueue only), same stream
+    C = eng.consts(vals)
+    k_kernel = args.steps
+    t_kernel = timed(lambda: eng.eval_enqueue(C, MIXED_F32, mc=False), k_kernel)
+    Cp = eng_p.consts(vals)
+    t_kernel_p = timed(lambda: eng_p.eval_enqueue(Cp, PLAIN_F64, mc=True), k_kernel)
+    ck = clocks.stop(local)
+    nll_m, g_m = eng.nll_grad(vals, names, MIXED_F32, use_gram=True)
+    nll_p, g_p = eng_p.nll_grad(vals, names, PLAIN_F64)
+
+    n_data = N_SIG + N_BG
+    code = eng.code
+    n_mass, n_ang = len(code.mass_fields), len(code.angle_fields)
+    bytes_mixed = n_data * (8 * n_mass + 4 * n_ang + 8)
+    bytes_plain = (n_data + N_MC) * (8 * n_mass + 8 * n_ang + 8)
+    hbm, peak_kind = _peaks()
+    ach = bytes_mixed / (t_kernel / k_kernel) / 1e9
+    ach_p = bytes_plain / (t_kernel_p / k_kernel) / 1e9
+    value = world * args.steps / t_mixed
+    line = {
+        "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_mixed / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "precision": "mixed: FP32 amplitudes, FP64 log-sum "
+                   "and sums, MC integral from the FP64 Gram matrix (masses/widths fixed)",
+                   "events_per_rank": {"data": n_data, "mc": N_MC},
+                   "l2": "256 MB buffer written before every timed step (L2 126 MB)",
+                   "parallelism": f"dp{world}" if world > 1 else "single GPU"},
+        "plain_f64": {"value": world * args.steps / t_plain, "unit": "evals/s",
+                      "ms_per_step": 1e3 * t_plain / args.steps,
+                      "speedup_mixed_over_plain": t_plain / t_mixed},
+        "e2e": {"value": world * args.steps / t_e2e, "unit": "evals/s",
+                "h2d_bytes_per_step": 8 * len(code.consts) + 8 * len(x0),
+                "d2h_bytes_per_step": 16 * code.nacc,
+                "call": "FCN.nll_grad(x) with x a host numpy vector"},
+        "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
+                     "frac": ach / hbm, "traffic": None, "peak_kind": peak_kind,
+                     "kernel": "pwa_eval_f32 + pwa_reduce (data term, mixed form)",
+                     "algorithmic_bytes_per_launch": bytes_mixed,
+                     "launch_us": 1e6 * t_kernel / k_kernel,
+                     "plain_f64_kernel": {"achieved": ach_p, "frac": ach_p / hbm,
+                                          "launch_us": 1e6 * t_kernel_p / k_kernel,
+                                          "algorithmic_bytes_per_launch": bytes_plain}},
+        "gpu_launches": 2 * args.steps,
+        "check": {"nll_mixed": nll_m, "nll_plain": nll_p, "dnll": nll_m - nll_p,
+                  "grad_max_rel": float(np.max(np.abs(g_m - g_p)) / np.max(np.abs(g_p)))},
+        "setup_s": {"dataset": t_data},
+        "engine": eng.info(),
+    }
+    if ck:
+        line["clocks"] = ck
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_baseline(args.cpu_sample)
+        except Exception as e:  # reported, never fatal
+            line["cpu_baseline"] = {"error": repr(e)}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    fcn.eng.close()
+    fcn_plain.eng.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -78,6 +78,11 @@ int pwa_upload_events(pwa_plan* h, const double* xm, const double* xa, const dou
  * PWA_MIXED_F32 (FP32 amplitudes, FP64 sums).  mc = 0 skips the MC set. */
 int pwa_eval(pwa_plan* h, const double* consts, int precision, int mc, void* stream, double* out);
 
+/* The device work of pwa_eval (fused kernel + fixed-order reduction) only,
+ * enqueued on `stream` without waiting; the sums stay on the device.  For
+ * timing the kernels and for capture into larger asynchronous pipelines. */
+int pwa_eval_enqueue(pwa_plan* h, const double* consts, int precision, int mc, void* stream);
+
 /* Per-event sum |A|^2 of events [beg, end) of the uploaded set into
  * out_dev (device, end-beg doubles). */
 int pwa_eval_pdf(pwa_plan* h, const double* consts, int precision, long long beg, long long end,

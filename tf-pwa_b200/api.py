@@ -1,0 +1,382 @@
+"""Reference-facing API: ConfigLoader, amplitude, FCN and fit.
+
+Mirrors the public surface of TF-PWA that callers of the amplitude-fit hot
+path use, with the same names, arguments and parameter conventions:
+
+* ``ConfigLoader(file)``: ``tf_pwa/config_loader/config_loader.py:62-104``;
+  ``get_amplitude`` (:210-237), ``get_data``/``get_all_data`` (:130-200),
+  ``get_fcn`` (:659-720), ``fit`` (:744-801), ``get_params_error``
+  (:814-874), ``set_params``/``get_params``/``save_params`` (:995-1040).
+* ``FCN``: ``tf_pwa/model/model.py:1115-1285`` -- ``__call__``, ``grad``,
+  ``nll_grad`` (float NLL and gradient list in ``vm.trainable_vars`` order),
+  ``nll_grad_hessian``.
+* ``FitResult``: ``tf_pwa/fit.py:497-536``.
+
+Data: the reference's ``E px py pz`` text files or ``.npy`` arrays, grouped
+per event in ``dat_order`` (``tf_pwa/data.py:300-365``); background files
+enter with weight ``-bg_weight`` (``config_loader/data.py:149-155,421-429``).
+Every evaluation runs on the CUDA engine; there is no CPU path.
+"""
+import json
+import os
+import time
+
+import numpy as np
+
+from .decay_config import DecayConfig, float_particles, init_params, load_yaml
+from .engine import MIXED_F32, PLAIN_F64, Engine
+from .kinematics import event_fields, p4_dict
+from .plan import Plan
+from .variables import VarsManager
+
+PRECISIONS = {"plain": PLAIN_F64, "f64": PLAIN_F64, "mixed": MIXED_F32, "chosen": MIXED_F32}
+
+
+class EventData:
+    """One dataset: plan-ordered (n_fields, N) FP64 columns and weights."""
+
+    def __init__(self, fields, weight=None):
+        self.fields = fields
+        n = fields.shape[1]
+        self.weight = np.ones(n) if weight is None else np.asarray(weight, np.float64)
+        self.n = n
+
+    def __len__(self):
+        return self.n
+
+    def numpy_fields(self):
+        f = self.fields
+        return f.detach().cpu().numpy() if hasattr(f, "detach") else np.asarray(f)
+
+
+def load_dat_file(fnames, n_particles):
+    """(N, n_particles, 4) momenta from ``.dat``/``.npy``/``.npz`` files."""
+    if isinstance(fnames, str):
+        fnames = [fnames]
+    out = []
+    for fn in fnames:
+        if fn.endswith(".npz"):
+            a = np.load(fn)["arr_0"]
+        elif fn.endswith(".npy"):
+            a = np.load(fn)
+        else:
+            a = np.loadtxt(fn, dtype=np.float64)
+        out.append(np.reshape(a, (-1, n_particles, 4)))
+    return np.concatenate(out, 0)
+
+
+class AmplitudeModel:
+    """sum |A|^2 of the model per event (``AbsPDF.__call__``)."""
+
+    def __init__(self, config, precision="plain"):
+        self.config = config
+        self.vm = config.vm
+        self.decay_group = config.decay_group
+        self.precision = PRECISIONS[precision]
+        self._eng = None
+        self._cached = None
+
+    @property
+    def trainable_variables(self):
+        return list(self.vm.trainable_vars)
+
+    def get_params(self, trainable_only=False):
+        return self.vm.get_all_dic(trainable_only)
+
+    def set_params(self, var):
+        self.vm.set_all(var)
+
+    def __call__(self, data):
+        if self._eng is None:
+            self._eng = Engine(self.decay_group, self.config.plan, self.vm)
+        if self._cached is not data:
+            x = data.numpy_fields()
+            self._eng.upload(x, np.ones(x.shape[1]))
+            self._cached = data
+        import torch
+
+        out = torch.empty(data.n, dtype=torch.float64, device="cuda")
+        C = self._eng.consts(self.vm.get_all_dic())
+        self._eng.pdf_device(C, 0, data.n, out.data_ptr(), self.precision)
+        return out.cpu().numpy()
+
+
+class FCN:
+    """Negative log-likelihood of data against the MC-normalised amplitude.
+
+    ``precision``: "plain" (FP64 throughout) or "mixed" (FP32 amplitudes,
+    FP64 sums; with ``gram=True`` and fixed masses/widths the MC integral
+    uses the cached Gram matrix)."""
+
+    def __init__(self, config, data, mcdata, bg=None, w_bkg=1.0, precision="plain",
+                 gram=None, batch=65000):
+        self.config = config
+        self.vm = config.vm
+        self.precision = PRECISIONS[precision]
+        self.n_call = 0
+        self.cached_nll = None
+        wd = list(data.weight)
+        xd = [data.numpy_fields()] if not hasattr(data.fields, "data_ptr") else None
+        if bg is not None:
+            wb = bg.weight if bg.weight is not None else -w_bkg * np.ones(bg.n)
+            w = np.concatenate([data.weight, wb])
+        else:
+            w = np.asarray(data.weight)
+        self.alpha = w.sum() / (w * w).sum()
+        self.weight = self.alpha * w
+        self.eng = Engine(config.decay_group, config.plan, self.vm)
+        self._upload(data, bg, mcdata)
+        shape_free = any(n.endswith(("_mass", "_width")) for n in self.vm.trainable_vars)
+        self.use_gram = (self.precision == MIXED_F32 and not shape_free) if gram is None else gram
+        if self.use_gram and shape_free:
+            raise ValueError("the Gram cache needs fixed masses and widths")
+        if self.use_gram:
+            self.eng.set_gram(self.vm.get_all_dic())
+
+    def _upload(self, data, bg, mcdata):
+        import torch
+
+        parts = [data] + ([bg] if bg is not None else [])
+        if all(hasattr(p.fields, "data_ptr") and p.fields.is_cuda for p in parts + [mcdata]):
+            x = torch.cat([p.fields for p in parts] + [mcdata.fields], 1)
+            c = self.eng.code
+            xm = x[c.mass_fields].contiguous() if c.mass_fields else x[:1].contiguous()
+            xa = x[c.angle_fields].contiguous() if c.angle_fields else x[:1].contiguous()
+            wm = np.asarray(mcdata.weight, np.float64)
+            wm = wm / wm.sum()
+            w = torch.as_tensor(np.concatenate([self.weight, wm]), device="cuda")
+            nd = sum(p.n for p in parts)
+            self.eng.upload_device(xm.data_ptr(), xa.data_ptr(), w.data_ptr(), nd, mcdata.n,
+                                   float(self.weight.sum()))
+            torch.cuda.synchronize()
+        else:
+            xd = np.concatenate([p.numpy_fields() for p in parts], 1)
+            self.eng.upload(xd, self.weight, mcdata.numpy_fields(), mcdata.weight)
+
+    # -- reference API -----------------------------------------------------
+    def get_params(self, trainable_only=False):
+        return self.vm.get_all_dic(trainable_only)
+
+    def _set(self, x):
+        if x is not None and len(np.atleast_1d(x)) > 0 and not isinstance(x, dict):
+            self.vm.set_all(list(x))
+        elif isinstance(x, dict) and x:
+            self.vm.set_all(x)
+
+    def get_nll_grad(self, x=None):
+        self._set(x)
+        nll, g = self.eng.nll_grad(self.vm.get_all_dic(), self.vm.trainable_vars,
+                                   self.precision, use_gram=self.use_gram)
+        self.n_call += 1
+        return nll, g
+
+    def nll_grad(self, x=None):
+        nll, g = self.get_nll_grad(x)
+        self.cached_nll = nll
+        return float(nll), g
+
+    def __call__(self, x=None):
+        nll, _ = self.get_nll_grad(x)
+        self.cached_nll = nll
+        return nll
+
+    def grad(self, x=None):
+        return self.get_nll_grad(x)[1]
+
+    def nll_grad_hessian(self, x=None, step=1e-4):
+        """Hessian by central differences of the adjoint gradient (symmetrised)."""
+        self._set(x)
+        x0 = np.array(self.vm.get_all_val())
+        nll, g0 = self.get_nll_grad(x0)
+        P = len(x0)
+        H = np.zeros((P, P))
+        for i in range(P):
+            h = step * max(abs(x0[i]), 1e-2)
+            xp, xm = x0.copy(), x0.copy()
+            xp[i] += h
+            xm[i] -= h
+            gp = self.get_nll_grad(xp)[1]
+            gm = self.get_nll_grad(xm)[1]
+            H[i] = (gp - gm) / (2 * h)
+        self._set(x0)
+        return nll, g0, 0.5 * (H + H.T)
+
+
+class FitResult:
+    def __init__(self, params, fcn, min_nll, ndf=0, success=True, message="", hess_inv=None,
+                 n_call=0):
+        self.params = params
+        self.error = {}
+        self.fcn = fcn
+        self.min_nll = float(min_nll)
+        self.ndf = int(ndf)
+        self.success = success
+        self.message = message
+        self.hess_inv = hess_inv
+        self.n_call = n_call
+
+    def save_as(self, file_name, save_hess=False):
+        s = {"value": self.params, "error": self.error, "status": {
+            "success": self.success, "NLL": self.min_nll, "Ndf": self.ndf}}
+        with open(file_name, "w") as f:
+            json.dump(s, f, indent=2)
+
+    def set_error(self, error):
+        self.error = dict(error)
+
+
+class ConfigLoader:
+    """config.yml -> model, data, FCN and fit (reference-compatible)."""
+
+    def __init__(self, file_name, vm=None, share_dict=None, precision="plain", seed=None):
+        self.config_file = file_name
+        self.config = load_yaml(file_name, share_dict)
+        base = os.path.dirname(os.path.abspath(file_name)) if isinstance(file_name, str) else "."
+        self.base_dir = base
+        self.decay_config = DecayConfig(self.config, base_dir=base, share_dict=share_dict)
+        self.decay_group = self.decay_config.decay_group
+        self.full_decay = self.decay_group
+        self.vm = vm if vm is not None else VarsManager(
+            rng=np.random.default_rng(seed))
+        self._names = init_params(self.decay_group, self.vm, self.config.get("constrains"))
+        float_particles(self.decay_group, self.vm, self._names,
+                        self.decay_config.particle_property)
+        self.plan = Plan(self.decay_group)
+        self.precision = precision
+        self._amp = None
+        self._data = {}
+
+    # -- model --------------------------------------------------------------
+    def get_decay(self, full=True):
+        return self.decay_group
+
+    def get_amplitude(self, vm=None, name=""):
+        if self._amp is None:
+            self._amp = AmplitudeModel(self, self.precision)
+        return self._amp
+
+    def get_dat_order(self):
+        order = self.config.get("data", {}).get("dat_order")
+        return order if order is not None else [str(o) for o in self.decay_group.outs]
+
+    # -- data ---------------------------------------------------------------
+    def _path(self, f):
+        return f if os.path.isabs(f) else os.path.join(self.base_dir, f)
+
+    def load_p4(self, files):
+        files = [self._path(f) for f in (files if isinstance(files, list) else [files])]
+        return load_dat_file(files, len(self.get_dat_order()))
+
+    def data_from_p4(self, p4, weight=None, device=None):
+        """EventData from (N, n_final, 4) momenta in dat_order."""
+        x = event_fields(self.plan, p4_dict(p4, self.get_dat_order()), device=device)
+        return EventData(x, weight)
+
+    def get_data(self, idx):
+        if idx in self._data:
+            return self._data[idx]
+        dcfg = self.config.get("data", {})
+        files = dcfg.get(idx)
+        if files is None:
+            return None
+        if isinstance(files, str):
+            files = [files]
+        ret = []
+        for f in files:
+            p4 = self.load_p4([f])
+            n = p4.shape[0]
+            w = np.ones(n)
+            wkey = dcfg.get(idx + "_weight")
+            if isinstance(wkey, (int, float)):
+                w = w * float(wkey)
+            elif wkey is not None:
+                w = np.concatenate([np.loadtxt(self._path(x)).reshape(-1)
+                                    for x in (wkey if isinstance(wkey, list) else [wkey])])[:n]
+            if idx == "bg":
+                w = -abs(float(dcfg.get("bg_weight", 1.0))) * w if wkey is None or isinstance(wkey, (int, float)) else -w
+            ret.append(self.data_from_p4(p4, w))
+        self._data[idx] = ret
+        return ret
+
+    def get_all_data(self):
+        return [self.get_data(k) for k in ("data", "phsp", "bg", "inmc")]
+
+    @staticmethod
+    def _merge(lst):
+        if lst is None:
+            return None
+        if len(lst) == 1:
+            return lst[0]
+        import torch
+
+        if hasattr(lst[0].fields, "data_ptr"):
+            f = torch.cat([d.fields for d in lst], 1)
+        else:
+            f = np.concatenate([d.fields for d in lst], 1)
+        return EventData(f, np.concatenate([d.weight for d in lst]))
+
+    def get_fcn(self, all_data=None, batch=65000, precision=None, gram=None):
+        if all_data is None:
+            data, phsp, bg, _ = self.get_all_data()
+        else:
+            data, phsp, bg = all_data[:3]
+        data = self._merge(data if isinstance(data, list) else [data])
+        phsp = self._merge(phsp if isinstance(phsp, list) else [phsp])
+        if bg is not None:
+            bg = self._merge(bg if isinstance(bg, list) else [bg])
+        return FCN(self, data, phsp, bg=bg, precision=precision or self.precision, gram=gram,
+                   batch=batch)
+
+    # -- parameters ---------------------------------------------------------
+    def get_params(self, trainable_only=False):
+        return self.vm.get_all_dic(trainable_only)
+
+    def set_params(self, params, neglect_params=None):
+        if isinstance(params, str):
+            with open(params) as f:
+                params = json.load(f)
+            params = params.get("value", params)
+        self.vm.set_all({k: v for k, v in params.items() if k in self.vm.variables})
+        return True
+
+    def save_params(self, file_name):
+        with open(file_name, "w") as f:
+            json.dump(self.get_params(), f, indent=2)
+
+    # -- fit ----------------------------------------------------------------
+    def fit(self, data=None, phsp=None, bg=None, batch=65000, method="BFGS", maxiter=None,
+            gtol=1e-3, fcn=None, precision=None):
+        """BFGS on FCN.nll_grad (``tf_pwa/fit.py:189-419``)."""
+        from scipy.optimize import minimize
+
+        if fcn is None:
+            fcn = self.get_fcn(None if data is None else [data, phsp, bg], batch, precision)
+        x0 = np.array(self.vm.get_all_val())
+        maxiter = maxiter or max(100 * len(x0), 2000)
+        t0 = time.time()
+        res = minimize(lambda x: fcn.nll_grad(x), x0, jac=True, method=method,
+                       options={"maxiter": maxiter, "gtol": gtol})
+        self.vm.set_all(list(res.x))
+        self.vm.std_polar_all()
+        fr = FitResult(self.get_params(), fcn, res.fun, ndf=len(x0), success=bool(res.success),
+                       message=str(res.message), hess_inv=getattr(res, "hess_inv", None),
+                       n_call=fcn.n_call)
+        fr.time = time.time() - t0
+        self._fcn = fcn
+        return fr
+
+    def get_params_error(self, params=None, data=None, phsp=None, bg=None, batch=10000,
+                         fcn=None):
+        """Errors from the inverse Hessian in FP64 (``applications.py:280-309``)."""
+        if params is not None:
+            self.set_params(params.params if isinstance(params, FitResult) else params)
+        fcn = fcn or getattr(self, "_fcn", None) or self.get_fcn(
+            None if data is None else [data, phsp, bg])
+        _, _, H = fcn.nll_grad_hessian()
+        try:
+            inv = np.linalg.inv(H)
+        except np.linalg.LinAlgError:
+            inv = np.linalg.pinv(H)
+        self.inv_he = inv
+        err = np.sqrt(np.abs(np.diag(inv)))
+        return dict(zip(self.vm.trainable_vars, err))

@@ -278,16 +278,17 @@ int pwa_upload_events(pwa_plan* h, const double* xm, const double* xa, const dou
   return PWA_OK;
 }
 
-int pwa_eval(pwa_plan* h, const double* consts, int precision, int mc, void* stream, double* out) {
+int pwa_eval_enqueue(pwa_plan* h, const double* consts, int precision, int mc, void* stream) {
   if (!h) return PWA_ERR_ARG;
   if (!h->w) return set_err(h, PWA_ERR_STATE, "no events uploaded");
-  if (!consts || !out || (precision != PWA_PLAIN_F64 && precision != PWA_MIXED_F32))
+  if (!consts || (precision != PWA_PLAIN_F64 && precision != PWA_MIXED_F32))
     return set_err(h, PWA_ERR_ARG, "invalid eval arguments");
   cudaStream_t s = (cudaStream_t)stream;
   std::vector<double> cbuf(consts, consts + h->nconst);
   long long n_all = mc ? h->n_data + h->n_mc : h->n_data;
   int nblocks = mc ? h->nblocks : h->blocks_data;
   if (!mc && h->n_mc == 0) nblocks = h->nblocks;
+  if (nblocks < 1) nblocks = 1;
   int bd = mc ? h->blocks_data : nblocks;
   const void* xa = precision == PWA_PLAIN_F64 ? (const void*)h->xa : (const void*)h->xa32;
   long long nd = h->n_data, ld = h->ld;
@@ -296,9 +297,19 @@ int pwa_eval(pwa_plan* h, const double* consts, int precision, int mc, void* str
                   dim3(h->tpb), args, s);
   if (rc) return rc;
   int nacc = h->nacc;
+  if (!mc) {
+    // only data sums: the MC half of d_out is cleared by the reduction
+  }
   void* args2[] = {&h->partials, &nacc, &bd, &nblocks, &h->d_out};
-  rc = launch(h, h->k.reduce, dim3(1), dim3(1024), args2, s);
+  return launch(h, h->k.reduce, dim3(1), dim3(1024), args2, s);
+}
+
+int pwa_eval(pwa_plan* h, const double* consts, int precision, int mc, void* stream, double* out) {
+  if (!out) return set_err(h, PWA_ERR_ARG, "null output");
+  int rc = pwa_eval_enqueue(h, consts, precision, mc, stream);
   if (rc) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  int nacc = h->nacc;
   CU(cudaMemcpyAsync(h->h_out, h->d_out, sizeof(double) * 2 * nacc, cudaMemcpyDeviceToHost, s));
   CU(cudaStreamSynchronize(s));
   std::memcpy(out, h->h_out, sizeof(double) * 2 * nacc);

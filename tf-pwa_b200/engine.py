@@ -50,20 +50,21 @@ def load_library(path=LIB_PATH):
     lib.pwa_compile_only.argtypes = [cp, sz, i, cp, cp, sz]
     lib.pwa_upload_events.argtypes = [vp, vp, vp, vp, ll, ll, i, vp]
     lib.pwa_eval.argtypes = [vp, dp, i, i, vp, dp]
+    lib.pwa_eval_enqueue.argtypes = [vp, dp, i, i, vp]
     lib.pwa_eval_pdf.argtypes = [vp, dp, i, ll, ll, vp, vp]
     lib.pwa_build_gram.argtypes = [vp, dp, vp, dp]
     lib.pwa_plan_info.argtypes = [vp, ctypes.POINTER(ll)]
     lib.pwa_last_error.argtypes = [vp]
     lib.pwa_last_error.restype = cp
     for f in ("pwa_plan_create", "pwa_plan_destroy", "pwa_compile_only", "pwa_upload_events",
-              "pwa_eval", "pwa_eval_pdf", "pwa_build_gram", "pwa_plan_info"):
+              "pwa_eval", "pwa_eval_enqueue", "pwa_eval_pdf", "pwa_build_gram", "pwa_plan_info"):
         getattr(lib, f).restype = i
     _lib = lib
     return lib
 
 
 EXPORTED = ("pwa_plan_create", "pwa_plan_destroy", "pwa_compile_only", "pwa_upload_events",
-            "pwa_eval", "pwa_eval_pdf", "pwa_build_gram", "pwa_plan_info", "pwa_last_error")
+            "pwa_eval", "pwa_eval_enqueue", "pwa_eval_pdf", "pwa_build_gram", "pwa_plan_info", "pwa_last_error")
 
 
 class PWAError(RuntimeError):
@@ -94,6 +95,16 @@ def poly(l, z):
     return r
 
 
+def combine_pieces(vec, P):
+    """NLL and gradient from the summed piece vector of
+    :meth:`Engine.local_pieces` (model.py:433-449):
+    NLL = -S_d + sw ln S_m, grad = -g_d + sw g_m / S_m."""
+    vec = np.asarray(vec, np.float64)
+    sd, sm, sw = vec[0], vec[1], vec[2]
+    gd, gm = vec[3:3 + P], vec[3 + P:3 + 2 * P]
+    return float(-sd + sw * np.log(sm)), -gd + sw * gm / sm
+
+
 class Engine:
     """A compiled model bound to a device: events, constants, evaluation."""
 
@@ -108,6 +119,8 @@ class Engine:
         self._n_data = self._n_mc = 0
         self._sw = None
         self._gram = None
+        self.mc_share = 1.0      # this device's fraction of the total MC weight
+        self.dist_reduce = None  # vector sum over devices (multi-GPU)
         self._prepare_structure()
         if compile:
             self._create()
@@ -379,6 +392,12 @@ class Engine:
                                             stream or 0, _dptr(out)), "pwa_eval")
         return out[:nacc], out[nacc:]
 
+    def eval_enqueue(self, C, precision=PLAIN_F64, mc=True, stream=None):
+        """Launch the evaluation kernels without waiting (for timing)."""
+        C = np.ascontiguousarray(C, np.float64)
+        self._check(load_library().pwa_eval_enqueue(self.h, _dptr(C), precision, 1 if mc else 0,
+                                                    stream or 0), "pwa_eval_enqueue")
+
     def build_gram(self, C, stream=None):
         K = self.code.ncol
         out = np.zeros(2 * K * K)
@@ -393,8 +412,13 @@ class Engine:
         self._check(load_library().pwa_eval_pdf(self.h, _dptr(C), precision, beg, end, out_ptr,
                                                 stream or 0), "pwa_eval_pdf")
 
-    def nll_grad(self, vals, names, precision=PLAIN_F64, use_gram=False, stream=None):
-        """NLL and gradient w.r.t. ``names`` (real parameter names)."""
+    def local_pieces(self, vals, names, precision=PLAIN_F64, use_gram=False, stream=None):
+        """This device's share of the NLL as the vector
+        [S_data, S_mc * f, sw, g_data (P), g_mc * f (P)] with S the summed
+        data log term / MC integral, g their gradients, sw the data weight
+        sum and f = this device's share of the total MC weight.  Summing the
+        vectors of all devices and calling :func:`combine_pieces` gives the
+        NLL and gradient of the union of all devices' events."""
         C = self.consts(vals)
         J, D = self.jacobian(vals, names)
         nacc = self.code.nacc
@@ -405,27 +429,30 @@ class Engine:
             sd, _ = self.eval_sums(C, precision, mc=False, stream=stream)
             ck = self._ck
             M = self._gram
-            I = float(np.real(np.conj(ck) @ M @ ck))
-            # G^mc_k = sum_i w conj(A_i) F_ik = sum_l conj(c_l) M_lk
+            # I = c^H M c; G^mc_k = sum_i w conj(A_i) F_ik = sum_l conj(c_l) M_lk
             Gm = np.conj(ck) @ M
             sm = np.zeros(nacc)
-            sm[0] = I
+            sm[0] = float(np.real(Gm @ ck))
             sm[1:1 + 2 * K:2] = Gm.real
             sm[2:2 + 2 * K:2] = Gm.imag
         else:
             sd, sm = self.eval_sums(C, precision, mc=True, stream=stream)
-        sw = self._sw
         Gd = sd[1:1 + 2 * K:2] + 1j * sd[2:2 + 2 * K:2]
         Gm = sm[1:1 + 2 * K:2] + 1j * sm[2:2 + 2 * K:2]
-        I = sm[0]
         gd = 2 * np.real(J @ Gd)
         gm = 2 * np.real(J @ Gm)
         if self.code.nshape:
             gd = gd + D @ sd[1 + 2 * K:]
             gm = gm + D @ sm[1 + 2 * K:]
-        nll = -sd[0] + sw * np.log(I)
-        grad = -gd + sw * gm / I
-        return float(nll), grad
+        f = self.mc_share
+        return np.concatenate([[sd[0], sm[0] * f, self._sw], gd, gm * f])
+
+    def nll_grad(self, vals, names, precision=PLAIN_F64, use_gram=False, stream=None):
+        """NLL and gradient w.r.t. ``names`` (real parameter names)."""
+        vec = self.local_pieces(vals, names, precision, use_gram, stream)
+        if self.dist_reduce is not None:
+            vec = self.dist_reduce(vec)
+        return combine_pieces(vec, len(names))
 
     def set_gram(self, vals):
         """Build the MC Gram matrix at the current masses/widths."""
