@@ -49,10 +49,11 @@ enum { PWA_PLAIN_F64 = 0, PWA_MIXED_F32 = 1 };
  * model_columns and the Consts layout); the library prepends its device
  * headers and compiles for sm_100a on the current device.
  * n_mass / n_angle: number of FP64 mass / angle columns of an event;
- * ncol, nout, nshape, nconst: model sizes matching the source.
+ * ncol, nout, nshape, nconst, nf: model sizes matching the source (nf =
+ * structurally non-zero (column, helicity) pairs, PWA_NF of the source).
  * tpb: threads per block of the fused kernels (32..1024, multiple of 32). */
 int pwa_plan_create(const char* src, size_t src_len, int n_mass, int n_angle, int ncol, int nout,
-                    int nshape, int nconst, int tpb, pwa_plan** out);
+                    int nshape, int nconst, int nf, int tpb, pwa_plan** out);
 
 int pwa_plan_destroy(pwa_plan* h);
 
@@ -91,6 +92,42 @@ int pwa_eval_pdf(pwa_plan* h, const double* consts, int precision, long long beg
 /* Gram matrix of the MC set, M_kl = sum_i w_i sum_o conj(F_ik,o) F_il,o,
  * in FP64; out[2*ncol*ncol] host, (re, im) row-major. */
 int pwa_build_gram(pwa_plan* h, const double* consts, void* stream, double* out);
+
+/* ---- fixed masses/widths: cached partial-wave columns -------------------
+ * The reference's cached-integral / cached-amplitude modes
+ * (tf_pwa/model/opt_int.py:128-558) keep per-event amplitude factors while
+ * masses and widths are fixed.  pwa_cache_data evaluates the columns
+ * F_k,o of all data events once (FP64) and keeps them as FP32 complex;
+ * pwa_build_gram (above) keeps the MC Gram matrix.  Each evaluation then
+ * streams the column cache once with FP64 arithmetic. */
+int pwa_cache_data(pwa_plan* h, const double* consts, void* stream);
+
+/* Data-term kernels on the cache with column couplings ck[2*ncol]
+ * (re, im); sums (1 + 2*ncol doubles) stay on the device. */
+int pwa_eval_cached_enqueue(pwa_plan* h, const double* ck, void* stream);
+
+/* Parameter layout for the C-side chain rule (fit parameter vector of
+ * n_vars reals, tf_pwa/variable.py order): coupling j is the complex number
+ * (vars[coup_r[j]], vars[coup_i[j]]), polar (r e^{i phi}) when
+ * coup_polar[j]; column k is the product of couplings col_fac[k*nfac+f]
+ * (-1 = unused slot); the gradient is taken w.r.t. vars[train_idx[t]]. */
+int pwa_set_param_layout(pwa_plan* h, int n_vars, int n_coup, const int* coup_r,
+                         const int* coup_i, const int* coup_polar, int nfac, const int* col_fac,
+                         int n_train, const int* train_idx);
+
+/* This device's NLL pieces from the cache + Gram: out[3 + 2*n_train] =
+ * [S_data, S_mc*mc_share, sw, g_data[n_train], g_mc*mc_share[n_train]];
+ * summing the vectors of several devices and forming
+ * NLL = -S_d + sw ln S_m, grad = -g_d + sw g_m / S_m gives the NLL of the
+ * union of their events (tf_pwa/model/model.py:433-449).  sw = sum of the
+ * final data weights. */
+int pwa_pieces_cached(pwa_plan* h, const double* vars, double sw, double mc_share, void* stream,
+                      double* out);
+
+/* NLL and gradient (FCN.nll_grad, tf_pwa/model/model.py:1223-1229) on one
+ * device from the cache: vars[n_vars] in, *out_nll and out_grad[n_train]. */
+int pwa_nll_grad_cached(pwa_plan* h, const double* vars, double sw, void* stream,
+                        double* out_nll, double* out_grad);
 
 /* info[0..7]: registers/thread of eval_f64, eval_f32, local bytes f64, f32,
  * blocks, blocks_data, nacc, threads per block. */

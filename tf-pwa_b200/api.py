@@ -131,7 +131,11 @@ class FCN:
         if self.use_gram and shape_free:
             raise ValueError("the Gram cache needs fixed masses and widths")
         if self.use_gram:
-            self.eng.set_gram(self.vm.get_all_dic())
+            vals = self.vm.get_all_dic()
+            self.eng.set_gram(vals)
+            self.eng.cache_data(vals)
+            self._var_names = list(self.vm.variables.keys())
+            self.eng.set_param_layout(self._var_names, self.vm.trainable_vars)
 
     def _upload(self, data, bg, mcdata):
         import torch
@@ -165,8 +169,12 @@ class FCN:
 
     def get_nll_grad(self, x=None):
         self._set(x)
-        nll, g = self.eng.nll_grad(self.vm.get_all_dic(), self.vm.trainable_vars,
-                                   self.precision, use_gram=self.use_gram)
+        if self.use_gram:
+            v = self.vm.variables
+            nll, g = self.eng.nll_grad_cached([v[k] for k in self._var_names])
+        else:
+            nll, g = self.eng.nll_grad(self.vm.get_all_dic(), self.vm.trainable_vars,
+                                       self.precision)
         self.n_call += 1
         return nll, g
 

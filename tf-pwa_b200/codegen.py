@@ -418,6 +418,11 @@ class ModelCode:
                  "    long long ld, long long i, cpx<R>* __restrict__ F) {")
         L.append("\n".join(cols_body))
         L.append("}\n")
+        fl = sorted(self._fset)
+        self.nf = len(fl)
+        L.append(f"#define PWA_NF {self.nf}")
+        L.append("__device__ constexpr int pwa_fk[PWA_NF] = {" + ", ".join(str(k) for k, _ in fl) + "};")
+        L.append("__device__ constexpr int pwa_fo[PWA_NF] = {" + ", ".join(str(o) for _, o in fl) + "};")
         return "\n".join(L)
 
     def _pre_name(self, ci, k, po):

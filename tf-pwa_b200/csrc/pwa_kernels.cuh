@@ -230,3 +230,94 @@ extern "C" __global__ void pwa_to_f32(const double* __restrict__ in, float* __re
        i += (long long)gridDim.x * blockDim.x)
     out[i] = (float)in[i];
 }
+
+// ---------------------------------------------------------------------------
+// Cached partial-wave columns (masses and widths fixed).
+//
+// pwa_cache_f32 evaluates F_k,o = S_k * F^ang_k,o of events [0, n) in FP64
+// and stores the structurally non-zero (k, o) pairs as FP32 complex in
+// column-major SoA: Fc[j * ldc + i], j over PWA_NF pairs.  Rounding to FP32
+// happens once per stored value (unbiased, per event), so sums over events
+// keep FP64-level systematic accuracy.
+// pwa_eval_cached streams Fc and the weights once per evaluation and does
+// all arithmetic in FP64: A_o = sum_k c_k F_k,o, f = sum_o |A_o|^2,
+// w clip_log(f), and sum_o conj(A_o) F_k,o scaled by w clip_log'(f).
+extern "C" __global__ void __launch_bounds__(PWA_TPB)
+    pwa_cache_f32(const Consts C, const double* __restrict__ XA, const double* __restrict__ XM,
+                  long long n, long long ld, long long ldc, float2* __restrict__ Fc) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    cpx<double> F[PWA_NCOL * PWA_NOUT];
+    model_columns<double>(C, XA, XM, ld, i, F);
+#pragma unroll
+    for (int j = 0; j < PWA_NF; ++j) {
+      const cpx<double> v = F[pwa_fk[j] * PWA_NOUT + pwa_fo[j]];
+      Fc[(long long)j * ldc + i] = make_float2((float)v.re, (float)v.im);
+    }
+  }
+}
+
+struct CCoup {
+  double v[2 * PWA_NCOL];
+};
+
+extern "C" __global__ void __launch_bounds__(PWA_TPB)
+    pwa_eval_cached(const CCoup c, const float2* __restrict__ Fc, const double* __restrict__ W,
+                    long long n, long long ldc, double* __restrict__ partials) {
+  constexpr int NA = 1 + 2 * PWA_NCOL;
+  double acc[NA];
+#pragma unroll
+  for (int j = 0; j < NA; ++j) acc[j] = 0.0;
+  for (long long i = (long long)blockIdx.x * PWA_TPB + threadIdx.x; i < n;
+       i += (long long)gridDim.x * PWA_TPB) {
+    float2 fv[PWA_NF];
+#pragma unroll
+    for (int j = 0; j < PWA_NF; ++j) fv[j] = __ldg(Fc + (long long)j * ldc + i);
+    const double w = __ldg(W + i);
+    double ar[PWA_NOUT], ai[PWA_NOUT];
+#pragma unroll
+    for (int o = 0; o < PWA_NOUT; ++o) ar[o] = ai[o] = 0.0;
+#pragma unroll
+    for (int j = 0; j < PWA_NF; ++j) {
+      const int k = pwa_fk[j], o = pwa_fo[j];
+      const double fr = fv[j].x, fi = fv[j].y;
+      const double cr = c.v[2 * k], ci = c.v[2 * k + 1];
+      ar[o] = fma(cr, fr, fma(-ci, fi, ar[o]));
+      ai[o] = fma(cr, fi, fma(ci, fr, ai[o]));
+    }
+    double f = 0.0;
+#pragma unroll
+    for (int o = 0; o < PWA_NOUT; ++o) f = fma(ar[o], ar[o], fma(ai[o], ai[o], f));
+    double dl;
+    const double cl = clip_log(f, &dl);
+    acc[0] = fma(w, cl, acc[0]);
+    const double fac = w * dl;
+    // fac * conj(A_o), then acc_k += fac conj(A_o) F_k,o
+#pragma unroll
+    for (int o = 0; o < PWA_NOUT; ++o) {
+      ar[o] *= fac;
+      ai[o] *= -fac;
+    }
+#pragma unroll
+    for (int j = 0; j < PWA_NF; ++j) {
+      const int k = pwa_fk[j], o = pwa_fo[j];
+      const double fr = fv[j].x, fi = fv[j].y;
+      acc[1 + 2 * k] = fma(ar[o], fr, fma(-ai[o], fi, acc[1 + 2 * k]));
+      acc[2 + 2 * k] = fma(ar[o], fi, fma(ai[o], fr, acc[2 + 2 * k]));
+    }
+  }
+  __shared__ double red[PWA_TPB / 32][NA];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int j = 0; j < NA; ++j) {
+    const double v = warp_sum(acc[j]);
+    if (lane == 0) red[warp][j] = v;
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < NA; j += PWA_TPB) {
+    double s = 0.0;
+#pragma unroll
+    for (int w2 = 0; w2 < PWA_TPB / 32; ++w2) s += red[w2][j];
+    partials[(long long)blockIdx.x * NA + j] = s;
+  }
+}

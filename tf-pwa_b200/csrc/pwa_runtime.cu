@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 #include <nvrtc.h>
 
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -25,7 +26,7 @@ namespace {
 struct Kernels {
   cudaKernel_t eval_f64 = nullptr, eval_f32 = nullptr, reduce = nullptr, pdf_f64 = nullptr,
                pdf_f32 = nullptr, columns_f64 = nullptr, gram_f64 = nullptr, sum_rows = nullptr,
-               to_f32 = nullptr;
+               to_f32 = nullptr, cache_f32 = nullptr, eval_cached = nullptr;
 };
 
 }  // namespace
@@ -45,6 +46,16 @@ struct pwa_plan {
   float* xa32 = nullptr;
   double* w = nullptr;
   long long n_data = 0, n_mc = 0, ld = 0, cap = 0;
+  // cached partial-wave columns of the data events (FP32 complex, SoA)
+  int nf = 0;
+  float2* fcache = nullptr;
+  long long ldc = 0, fcache_n = 0;
+  int cached_blocks = 0;
+  std::vector<double> gram;  // MC Gram matrix, (re, im) row-major ncol x ncol
+  bool gram_valid = false;
+  // parameter layout for the C-side chain rule
+  int n_vars = 0, n_coup = 0, nfac = 0, n_train = 0;
+  std::vector<int> coup_r, coup_i, coup_polar, col_fac, train_idx;
   // scratch
   double* partials = nullptr;
   long long partials_cap = 0;
@@ -159,12 +170,12 @@ int pwa_compile_only(const char* src, size_t src_len, int tpb, const char* arch,
 }
 
 int pwa_plan_create(const char* src, size_t src_len, int n_mass, int n_angle, int ncol, int nout,
-                    int nshape, int nconst, int tpb, pwa_plan** out) {
+                    int nshape, int nconst, int nf, int tpb, pwa_plan** out) {
   if (!out) return PWA_ERR_ARG;
   *out = nullptr;
   pwa_plan* h = new pwa_plan();
   if (!src || ncol <= 0 || nout <= 0 || nconst <= 0 || n_mass < 0 || n_angle < 0 || nshape < 0 ||
-      tpb < 32 || tpb > 1024 || tpb % 32) {
+      nf <= 0 || nf > ncol * nout || tpb < 32 || tpb > 1024 || tpb % 32) {
     *out = h;
     return set_err(h, PWA_ERR_ARG, "invalid plan sizes");
   }
@@ -175,6 +186,7 @@ int pwa_plan_create(const char* src, size_t src_len, int n_mass, int n_angle, in
   h->nshape = nshape;
   h->nconst = nconst;
   h->nacc = 1 + 2 * ncol + nshape;
+  h->nf = nf;
   h->tpb = tpb;
   *out = h;
   CU(cudaGetDevice(&h->device));
@@ -196,7 +208,8 @@ int pwa_plan_create(const char* src, size_t src_len, int n_mass, int n_angle, in
             {"pwa_reduce", &h->k.reduce},           {"pwa_pdf_f64", &h->k.pdf_f64},
             {"pwa_pdf_f32", &h->k.pdf_f32},         {"pwa_columns_f64", &h->k.columns_f64},
             {"pwa_gram_f64", &h->k.gram_f64},       {"pwa_sum_rows", &h->k.sum_rows},
-            {"pwa_to_f32", &h->k.to_f32}};
+            {"pwa_to_f32", &h->k.to_f32},           {"pwa_cache_f32", &h->k.cache_f32},
+            {"pwa_eval_cached", &h->k.eval_cached}};
   for (auto& e : ks) CU(cudaLibraryGetKernel(e.slot, h->lib, e.name));
   for (int p = 0; p < 2; ++p) {
     cudaFuncAttributes a;
@@ -213,6 +226,7 @@ int pwa_plan_destroy(pwa_plan* h) {
   if (!h) return PWA_OK;
   free_events(h);
   if (h->partials) cudaFree(h->partials);
+  if (h->fcache) cudaFree(h->fcache);
   if (h->d_out) cudaFree(h->d_out);
   if (h->h_out) cudaFreeHost(h->h_out);
   if (h->lib) cudaLibraryUnload(h->lib);
@@ -245,6 +259,8 @@ int pwa_upload_events(pwa_plan* h, const double* xm, const double* xa, const dou
   h->ld = ld;
   h->n_data = n_data;
   h->n_mc = n_mc;
+  h->fcache_n = 0;
+  h->gram_valid = false;
   const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
   if (h->n_mass)
     CU(cudaMemcpy2DAsync(h->xm, sizeof(double) * ld, xm, sizeof(double) * n, sizeof(double) * n,
@@ -342,7 +358,7 @@ int pwa_eval_pdf(pwa_plan* h, const double* consts, int precision, long long beg
 int pwa_build_gram(pwa_plan* h, const double* consts, void* stream, double* out) {
   if (!h) return PWA_ERR_ARG;
   if (!h->w || h->n_mc <= 0) return set_err(h, PWA_ERR_STATE, "no MC events uploaded");
-  if (!consts || !out) return set_err(h, PWA_ERR_ARG, "invalid gram arguments");
+  if (!consts) return set_err(h, PWA_ERR_ARG, "invalid gram arguments");
   cudaStream_t s = (cudaStream_t)stream;
   std::vector<double> cbuf(consts, consts + h->nconst);
   const long long row = 2LL * h->ncol * h->nout;
@@ -398,7 +414,198 @@ int pwa_build_gram(pwa_plan* h, const double* consts, void* stream, double* out)
   cudaFree(gsum);
   cudaFree(gtot);
   if (rc) return rc;
-  std::memcpy(out, acc.data(), sizeof(double) * nkk);
+  h->gram = acc;
+  h->gram_valid = true;
+  if (out) std::memcpy(out, acc.data(), sizeof(double) * nkk);
+  return PWA_OK;
+}
+
+
+int pwa_cache_data(pwa_plan* h, const double* consts, void* stream) {
+  if (!h) return PWA_ERR_ARG;
+  if (!h->w || h->n_data <= 0) return set_err(h, PWA_ERR_STATE, "no data events uploaded");
+  if (!consts) return set_err(h, PWA_ERR_ARG, "null consts");
+  cudaStream_t s = (cudaStream_t)stream;
+  const long long n = h->n_data;
+  const long long ldc = (n + 31) / 32 * 32;
+  if (h->fcache == nullptr || ldc > h->ldc) {
+    if (h->fcache) cudaFree(h->fcache);
+    h->fcache = nullptr;
+    if (cudaMalloc(&h->fcache, sizeof(float2) * (size_t)ldc * h->nf) != cudaSuccess)
+      return set_err(h, PWA_ERR_OOM, "cudaMalloc of the column cache failed");
+    h->ldc = ldc;
+  }
+  std::vector<double> cbuf(consts, consts + h->nconst);
+  long long ld = h->ld, ldcv = h->ldc;
+  void* args[] = {cbuf.data(), &h->xa, &h->xm, (void*)&n, &ld, &ldcv, &h->fcache};
+  long long nb = (n + h->tpb - 1) / h->tpb;
+  if (nb > 16LL * h->sms) nb = 16LL * h->sms;
+  int rc = launch(h, h->k.cache_f32, dim3((int)nb), dim3(h->tpb), args, s);
+  if (rc) return rc;
+  int per_sm = 0;
+  CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)h->k.eval_cached, h->tpb, 0));
+  if (per_sm < 1) per_sm = 1;
+  long long want = (long long)per_sm * h->sms, need = (n + h->tpb - 1) / h->tpb;
+  h->cached_blocks = (int)(want < need ? want : need);
+  rc = ensure_partials(h, (long long)h->cached_blocks * (1 + 2 * h->ncol));
+  if (rc) return rc;
+  CU(cudaStreamSynchronize(s));
+  h->fcache_n = n;
+  return PWA_OK;
+}
+
+int pwa_eval_cached_enqueue(pwa_plan* h, const double* ck, void* stream) {
+  if (!h) return PWA_ERR_ARG;
+  if (h->fcache_n <= 0) return set_err(h, PWA_ERR_STATE, "no column cache (call pwa_cache_data)");
+  if (!ck) return set_err(h, PWA_ERR_ARG, "null couplings");
+  cudaStream_t s = (cudaStream_t)stream;
+  std::vector<double> cbuf(ck, ck + 2 * h->ncol);
+  long long n = h->fcache_n, ldc = h->ldc;
+  void* args[] = {cbuf.data(), &h->fcache, &h->w, &n, &ldc, &h->partials};
+  int rc = launch(h, h->k.eval_cached, dim3(h->cached_blocks), dim3(h->tpb), args, s);
+  if (rc) return rc;
+  int na = 1 + 2 * h->ncol, nb = h->cached_blocks;
+  void* args2[] = {&h->partials, &na, &nb, &nb, &h->d_out};
+  return launch(h, h->k.reduce, dim3(1), dim3(1024), args2, s);
+}
+
+int pwa_set_param_layout(pwa_plan* h, int n_vars, int n_coup, const int* coup_r,
+                         const int* coup_i, const int* coup_polar, int nfac, const int* col_fac,
+                         int n_train, const int* train_idx) {
+  if (!h) return PWA_ERR_ARG;
+  if (n_vars <= 0 || n_coup <= 0 || nfac <= 0 || n_train < 0 || !coup_r || !coup_i ||
+      !coup_polar || !col_fac || (n_train && !train_idx))
+    return set_err(h, PWA_ERR_ARG, "invalid parameter layout");
+  for (int j = 0; j < n_coup; ++j)
+    if (coup_r[j] < 0 || coup_r[j] >= n_vars || coup_i[j] < 0 || coup_i[j] >= n_vars)
+      return set_err(h, PWA_ERR_ARG, "coupling index out of range");
+  for (int k = 0; k < h->ncol * nfac; ++k)
+    if (col_fac[k] < -1 || col_fac[k] >= n_coup)
+      return set_err(h, PWA_ERR_ARG, "column factor index out of range");
+  for (int t = 0; t < n_train; ++t)
+    if (train_idx[t] < 0 || train_idx[t] >= n_vars)
+      return set_err(h, PWA_ERR_ARG, "trainable index out of range");
+  h->n_vars = n_vars;
+  h->n_coup = n_coup;
+  h->nfac = nfac;
+  h->n_train = n_train;
+  h->coup_r.assign(coup_r, coup_r + n_coup);
+  h->coup_i.assign(coup_i, coup_i + n_coup);
+  h->coup_polar.assign(coup_polar, coup_polar + n_coup);
+  h->col_fac.assign(col_fac, col_fac + h->ncol * nfac);
+  h->train_idx.assign(train_idx, train_idx + n_train);
+  return PWA_OK;
+}
+
+namespace {
+struct cplx {
+  double r, i;
+};
+inline cplx cmulh(cplx a, cplx b) { return {a.r * b.r - a.i * b.i, a.r * b.i + a.i * b.r}; }
+}  // namespace
+
+int pwa_pieces_cached(pwa_plan* h, const double* vars, double sw, double mc_share, void* stream,
+                      double* out) {
+  if (!h) return PWA_ERR_ARG;
+  if (!vars || !out) return set_err(h, PWA_ERR_ARG, "null argument");
+  if (h->n_coup == 0) return set_err(h, PWA_ERR_STATE, "parameter layout not set");
+  if (!h->gram_valid) return set_err(h, PWA_ERR_STATE, "MC Gram matrix not built");
+  const int K = h->ncol, P = h->n_train;
+  // couplings and column products
+  std::vector<cplx> z(h->n_coup);
+  for (int j = 0; j < h->n_coup; ++j) {
+    const double r = vars[h->coup_r[j]], p = vars[h->coup_i[j]];
+    z[j] = h->coup_polar[j] ? cplx{r * std::cos(p), r * std::sin(p)} : cplx{r, p};
+  }
+  std::vector<double> ck(2 * K);
+  for (int k = 0; k < K; ++k) {
+    cplx c{1.0, 0.0};
+    for (int f = 0; f < h->nfac; ++f) {
+      const int j = h->col_fac[k * h->nfac + f];
+      if (j >= 0) c = cmulh(c, z[j]);
+    }
+    ck[2 * k] = c.r;
+    ck[2 * k + 1] = c.i;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  int rc = pwa_eval_cached_enqueue(h, ck.data(), stream);
+  if (rc) return rc;
+  const int na = 1 + 2 * K;
+  CU(cudaMemcpyAsync(h->h_out, h->d_out, sizeof(double) * na, cudaMemcpyDeviceToHost, s));
+  // MC term from the Gram matrix while the kernels run: I = c^H M c,
+  // Gm_k = sum_l conj(c_l) M_lk
+  std::vector<cplx> Gm(K, cplx{0, 0});
+  double I = 0.0;
+  for (int k = 0; k < K; ++k) {
+    cplx acc{0, 0};
+    for (int l = 0; l < K; ++l) {
+      const cplx m{h->gram[2 * (l * K + k)], h->gram[2 * (l * K + k) + 1]};
+      const cplx cl{ck[2 * l], -ck[2 * l + 1]};
+      const cplx t = cmulh(cl, m);
+      acc.r += t.r;
+      acc.i += t.i;
+    }
+    Gm[k] = acc;
+    I += acc.r * ck[2 * k] - acc.i * ck[2 * k + 1];
+  }
+  CU(cudaStreamSynchronize(s));
+  const double* sd = h->h_out;
+  // chain rule: d f / d theta = 2 Re sum_k J_k G_k
+  out[0] = sd[0];
+  out[1] = I * mc_share;
+  out[2] = sw;
+  for (int t = 0; t < P; ++t) {
+    const int v = h->train_idx[t];
+    int j = -1, comp = 0;
+    for (int q = 0; q < h->n_coup && j < 0; ++q) {
+      if (h->coup_r[q] == v) j = q, comp = 0;
+      else if (h->coup_i[q] == v) j = q, comp = 1;
+    }
+    if (j < 0) return set_err(h, PWA_ERR_ARG, "trainable variable is not a coupling (cached mode)");
+    const double r = vars[h->coup_r[j]], p = vars[h->coup_i[j]];
+    cplx dz;
+    if (h->coup_polar[j])
+      dz = comp == 0 ? cplx{std::cos(p), std::sin(p)} : cplx{-r * std::sin(p), r * std::cos(p)};
+    else
+      dz = comp == 0 ? cplx{1, 0} : cplx{0, 1};
+    double gd = 0.0, gm = 0.0;
+    for (int k = 0; k < K; ++k) {
+      int cnt = 0;
+      cplx others{1.0, 0.0};
+      for (int f = 0; f < h->nfac; ++f) {
+        const int q = h->col_fac[k * h->nfac + f];
+        if (q < 0) continue;
+        if (q == j && cnt == 0) {
+          ++cnt;
+          continue;
+        }
+        if (q == j) ++cnt;
+        others = cmulh(others, z[q]);
+      }
+      if (!cnt) continue;
+      cplx J = cmulh(others, dz);
+      J.r *= cnt;
+      J.i *= cnt;
+      const cplx Gd{sd[1 + 2 * k], sd[2 + 2 * k]};
+      gd += 2.0 * (J.r * Gd.r - J.i * Gd.i);
+      gm += 2.0 * (J.r * Gm[k].r - J.i * Gm[k].i);
+    }
+    out[3 + t] = gd;
+    out[3 + P + t] = gm * mc_share;
+  }
+  return PWA_OK;
+}
+
+int pwa_nll_grad_cached(pwa_plan* h, const double* vars, double sw, void* stream,
+                        double* out_nll, double* out_grad) {
+  if (!h) return PWA_ERR_ARG;
+  if (!out_nll || (!out_grad && h->n_train)) return set_err(h, PWA_ERR_ARG, "null output");
+  const int P = h->n_train;
+  std::vector<double> v(3 + 2 * P);
+  int rc = pwa_pieces_cached(h, vars, sw, 1.0, stream, v.data());
+  if (rc) return rc;
+  *out_nll = -v[0] + v[2] * std::log(v[1]);
+  for (int t = 0; t < P; ++t) out_grad[t] = -v[3 + t] + v[2] * v[3 + P + t] / v[1];
   return PWA_OK;
 }
 

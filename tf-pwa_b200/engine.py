@@ -45,7 +45,13 @@ def load_library(path=LIB_PATH):
     lib = ctypes.CDLL(path)
     vp, cp, i, ll, dp, sz = (ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_longlong,
                              ctypes.POINTER(ctypes.c_double), ctypes.c_size_t)
-    lib.pwa_plan_create.argtypes = [cp, sz, i, i, i, i, i, i, i, ctypes.POINTER(vp)]
+    lib.pwa_plan_create.argtypes = [cp, sz, i, i, i, i, i, i, i, i, ctypes.POINTER(vp)]
+    ip = ctypes.POINTER(ctypes.c_int)
+    lib.pwa_cache_data.argtypes = [vp, dp, vp]
+    lib.pwa_eval_cached_enqueue.argtypes = [vp, dp, vp]
+    lib.pwa_set_param_layout.argtypes = [vp, i, i, ip, ip, ip, i, ip, i, ip]
+    lib.pwa_pieces_cached.argtypes = [vp, dp, ctypes.c_double, ctypes.c_double, vp, dp]
+    lib.pwa_nll_grad_cached.argtypes = [vp, dp, ctypes.c_double, vp, dp, dp]
     lib.pwa_plan_destroy.argtypes = [vp]
     lib.pwa_compile_only.argtypes = [cp, sz, i, cp, cp, sz]
     lib.pwa_upload_events.argtypes = [vp, vp, vp, vp, ll, ll, i, vp]
@@ -56,15 +62,18 @@ def load_library(path=LIB_PATH):
     lib.pwa_plan_info.argtypes = [vp, ctypes.POINTER(ll)]
     lib.pwa_last_error.argtypes = [vp]
     lib.pwa_last_error.restype = cp
-    for f in ("pwa_plan_create", "pwa_plan_destroy", "pwa_compile_only", "pwa_upload_events",
-              "pwa_eval", "pwa_eval_enqueue", "pwa_eval_pdf", "pwa_build_gram", "pwa_plan_info"):
+    for f in EXPORTED:
+        if f == "pwa_last_error":
+            continue
         getattr(lib, f).restype = i
     _lib = lib
     return lib
 
 
 EXPORTED = ("pwa_plan_create", "pwa_plan_destroy", "pwa_compile_only", "pwa_upload_events",
-            "pwa_eval", "pwa_eval_enqueue", "pwa_eval_pdf", "pwa_build_gram", "pwa_plan_info", "pwa_last_error")
+            "pwa_eval", "pwa_eval_enqueue", "pwa_eval_pdf", "pwa_build_gram", "pwa_cache_data",
+            "pwa_eval_cached_enqueue", "pwa_set_param_layout", "pwa_pieces_cached",
+            "pwa_nll_grad_cached", "pwa_plan_info", "pwa_last_error")
 
 
 class PWAError(RuntimeError):
@@ -132,7 +141,7 @@ class Engine:
         h = ctypes.c_void_p()
         src = self.src.encode()
         rc = lib.pwa_plan_create(src, len(src), len(c.mass_fields), len(c.angle_fields), c.ncol,
-                                 c.nout, c.nshape, len(c.consts), self.tpb, ctypes.byref(h))
+                                 c.nout, c.nshape, len(c.consts), c.nf, self.tpb, ctypes.byref(h))
         if rc != 0:
             msg = lib.pwa_last_error(h).decode(errors="replace")
             lib.pwa_plan_destroy(h)
@@ -453,6 +462,64 @@ class Engine:
         if self.dist_reduce is not None:
             vec = self.dist_reduce(vec)
         return combine_pieces(vec, len(names))
+
+    # -------------------------------------------------- cached (fixed shapes)
+    def _ivec(self, a):
+        a = np.ascontiguousarray(np.asarray(a, np.int32))
+        return a, a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+    def set_param_layout(self, var_names, train_names):
+        """Hand the coupling structure to the library for its chain rule."""
+        idx = {n: i for i, n in enumerate(var_names)}
+        r = [idx[n + "r"] for n in self.coupling_names]
+        im = [idx[n + "i"] for n in self.coupling_names]
+        pol = [1 if self.vm.complex_vars.get(n, True) else 0 for n in self.coupling_names]
+        cidx = {n: j for j, n in enumerate(self.coupling_names)}
+        nfac = max(len(f) for f in self.col_factors)
+        cf = -np.ones((self.code.ncol, nfac), np.int32)
+        for k, f in enumerate(self.col_factors):
+            for q, n in enumerate(f):
+                cf[k, q] = cidx[n]
+        tr = [idx[n] for n in train_names]
+        self._layout = [self._ivec(x) for x in (r, im, pol, cf.reshape(-1), tr)]
+        self._var_names = list(var_names)
+        self._n_train = len(tr)
+        (a, pa), (b, pb), (c, pc), (d, pd), (e, pe) = self._layout
+        self._check(load_library().pwa_set_param_layout(
+            self.h, len(var_names), len(r), pa, pb, pc, nfac, pd, len(tr), pe),
+            "pwa_set_param_layout")
+
+    def cache_data(self, vals):
+        """Evaluate and keep the data events' partial-wave columns."""
+        C = np.ascontiguousarray(self.consts(vals))
+        self._check(load_library().pwa_cache_data(self.h, _dptr(C), 0), "pwa_cache_data")
+
+    def pieces_cached(self, var_values, mc_share=None, stream=None):
+        v = np.ascontiguousarray(var_values, np.float64)
+        out = np.zeros(3 + 2 * self._n_train)
+        share = self.mc_share if mc_share is None else mc_share
+        self._check(load_library().pwa_pieces_cached(self.h, _dptr(v), self._sw, share,
+                                                     stream or 0, _dptr(out)),
+                    "pwa_pieces_cached")
+        return out
+
+    def nll_grad_cached(self, var_values, stream=None):
+        """NLL and gradient from the column cache + Gram matrix (C++ path)."""
+        if self.dist_reduce is not None:
+            vec = self.dist_reduce(self.pieces_cached(var_values, stream=stream))
+            return combine_pieces(vec, self._n_train)
+        v = np.ascontiguousarray(var_values, np.float64)
+        nll = ctypes.c_double()
+        g = np.zeros(self._n_train)
+        self._check(load_library().pwa_nll_grad_cached(self.h, _dptr(v), self._sw, stream or 0,
+                                                       ctypes.byref(nll), _dptr(g)),
+                    "pwa_nll_grad_cached")
+        return nll.value, g
+
+    def eval_cached_enqueue(self, ck, stream=None):
+        ck = np.ascontiguousarray(ck, np.float64)
+        self._check(load_library().pwa_eval_cached_enqueue(self.h, _dptr(ck), stream or 0),
+                    "pwa_eval_cached_enqueue")
 
     def set_gram(self, vals):
         """Build the MC Gram matrix at the current masses/widths."""
