@@ -129,6 +129,23 @@ int pwa_pieces_cached(pwa_plan* h, const double* vars, double sw, double mc_shar
 int pwa_nll_grad_cached(pwa_plan* h, const double* vars, double sw, void* stream,
                         double* out_nll, double* out_grad);
 
+/* Allocation-free variant of pwa_eval's device work (plain FP64 kernels),
+ * with no counterpart in the reference.  For callers that cannot call
+ * cudaMalloc while they run (inside a stream capture, or under a framework
+ * that owns all device memory).  The caller passes device inputs xm
+ * [n_mass][ld], xa [n_angle][ld], w [ld] (data rows first, then MC, same
+ * meaning as pwa_upload_events) and a device output out[2*nacc] (data sums,
+ * then MC sums, as pwa_eval).  Block partials live in a fixed device array
+ * inside the library (1184 blocks x 256 accumulators of FP64, 2.4 MB held
+ * by every GPU that loads the library until exit); models with more than
+ * 256 accumulators are rejected with PWA_ERR_ARG.  Allocates nothing and
+ * does not wait.  The first call on a device looks up the array's device
+ * address; make that first call before any stream capture.  Calls share the
+ * array: calls that overlap on the GPU race. */
+int pwa_eval_noalloc(pwa_plan* h, const double* consts, const double* xm, const double* xa,
+                     const double* w, long long n_data, long long n_mc, long long ld,
+                     double* out, void* stream);
+
 /* info[0..7]: registers/thread of eval_f64, eval_f32, local bytes f64, f32,
  * blocks, blocks_data, nacc, threads per block. */
 int pwa_plan_info(pwa_plan* h, long long* info);

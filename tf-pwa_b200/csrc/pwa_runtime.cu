@@ -13,6 +13,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <mutex>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -628,3 +629,88 @@ const char* pwa_last_error(pwa_plan* h) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free evaluation.
+//
+// Callers that may not allocate device memory while they run -- code inside
+// a CUDA stream capture, or a host framework that owns every device byte
+// through its own arena and forbids cudaMalloc from plug-ins -- still need
+// the fused evaluation's block partials somewhere.  pwa_eval_noalloc keeps
+// them in this fixed, file-scope device array instead of the plan's
+// cudaMalloc'd scratch.  The array is part of this library's device image:
+// every GPU that loads the library holds it (2.4 MB) until the process
+// exits.  All calls share it, so calls whose kernels overlap on a GPU race;
+// serialise them (one stream, or events between streams).
+#define PWA_NOALLOC_MAX_BLOCKS 1184
+#define PWA_NOALLOC_MAX_NACC 256
+static __device__ __align__(256) double
+    g_pwa_noalloc_scratch[PWA_NOALLOC_MAX_BLOCKS * PWA_NOALLOC_MAX_NACC];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+double* g_noalloc_ptr[kMaxDevices] = {nullptr};
+
+// Device address of the scratch array for `dev` (the current device).  The
+// name g_pwa_noalloc_scratch is only a host-side stand-in in host code; its
+// device address comes from cudaGetSymbolAddress, once per device.
+int noalloc_scratch(pwa_plan* h, int dev, double** out) {
+  if (dev < 0 || dev >= kMaxDevices) return set_err(h, PWA_ERR_ARG, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_pwa_noalloc_scratch);
+    if (e != cudaSuccess)
+      return set_err(h, PWA_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    g_noalloc_ptr[dev] = (double*)p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return PWA_OK;
+}
+}  // namespace
+
+extern "C" int pwa_eval_noalloc(pwa_plan* h, const double* consts, const double* xm,
+                                const double* xa, const double* w, long long n_data,
+                                long long n_mc, long long ld, double* out, void* stream) {
+  if (!h) return PWA_ERR_ARG;
+  if (!h->lib) return set_err(h, PWA_ERR_STATE, "plan not compiled");
+  if (!consts || !w || !out || (h->n_mass && !xm) || (h->n_angle && !xa))
+    return set_err(h, PWA_ERR_ARG, "null argument");
+  if (n_data < 0 || n_mc < 0 || n_data + n_mc <= 0 || ld < n_data + n_mc)
+    return set_err(h, PWA_ERR_ARG, "invalid event counts or leading dimension");
+  if (h->nacc > PWA_NOALLOC_MAX_NACC)
+    return set_err(h, PWA_ERR_ARG,
+                   "model needs " + std::to_string(h->nacc) + " accumulators; pwa_eval_noalloc "
+                   "supports at most " + std::to_string(PWA_NOALLOC_MAX_NACC));
+  int dev = 0;
+  CU(cudaGetDevice(&dev));
+  double* scratch = nullptr;
+  int rc = noalloc_scratch(h, dev, &scratch);
+  if (rc) return rc;
+  int per_sm = 0;
+  CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)h->k.eval_f64, h->tpb, 0));
+  if (per_sm < 1) per_sm = 1;
+  const long long n = n_data + n_mc;
+  long long nb = (long long)per_sm * h->sms;
+  const long long need = (n + h->tpb - 1) / h->tpb;
+  if (nb > need) nb = need;
+  if (nb > PWA_NOALLOC_MAX_BLOCKS) nb = PWA_NOALLOC_MAX_BLOCKS;
+  if (nb < 2) nb = 2;
+  long long bd = n_mc == 0 ? nb : (n_data == 0 ? 0 : (nb * n_data + n / 2) / n);
+  if (n_data > 0 && bd < 1) bd = 1;
+  if (n_mc > 0 && bd > nb - 1) bd = nb - 1;
+  int nblocks = (int)nb, blocks_data = (int)bd;
+  // nothing in the scratch must start at zero: every launched block writes
+  // its whole partial row before pwa_reduce reads it
+  cudaStream_t s = (cudaStream_t)stream;
+  std::vector<double> cbuf(consts, consts + h->nconst);
+  long long n_all = n;
+  void* args[] = {cbuf.data(), (void*)&xa, (void*)&xm, (void*)&w, &n_data, &n_all, &ld,
+                  &blocks_data, &scratch};
+  rc = launch(h, h->k.eval_f64, dim3(nblocks), dim3(h->tpb), args, s);
+  if (rc) return rc;
+  int nacc = h->nacc;
+  void* args2[] = {&scratch, &nacc, &blocks_data, &nblocks, &out};
+  return launch(h, h->k.reduce, dim3(1), dim3(1024), args2, s);
+}
