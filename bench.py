@@ -241,6 +241,9 @@ def main():
     ap.add_argument("--impl", default="ours")
     ap.add_argument("--cpu-sample", type=int, default=int(os.environ.get("PWA_CPU_SAMPLE", "2000")))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--n-sig", type=int, default=N_SIG, help="signal data events per GPU")
+    ap.add_argument("--n-bg", type=int, default=N_BG, help="background data rows per GPU")
+    ap.add_argument("--n-mc", type=int, default=N_MC, help="MC events per GPU")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -266,7 +269,8 @@ def main():
     from tf_pwa_b200.workload import make_dataset
 
     t_setup = time.perf_counter()
-    cl, data, bg, mc = make_dataset(CONFIG, N_SIG, N_MC, n_bg=N_BG, bg_weight=BG_WEIGHT,
+    n_sig, n_bg, n_mc = args.n_sig, args.n_bg, args.n_mc
+    cl, data, bg, mc = make_dataset(CONFIG, n_sig, n_mc, n_bg=n_bg, bg_weight=BG_WEIGHT,
                                     seed=1 + rank, device="cuda")
     t_data = time.perf_counter() - t_setup
     reduce_fn = None
@@ -335,11 +339,11 @@ def main():
     nll_m, g_m = eng.nll_grad_cached(var_vec)
     nll_p, g_p = eng_p.nll_grad(vals, names, PLAIN_F64)
 
-    n_data = N_SIG + N_BG
+    n_data = n_sig + n_bg
     code = eng.code
     n_mass, n_ang = len(code.mass_fields), len(code.angle_fields)
     bytes_mixed = n_data * (8 * code.nf + 8)
-    bytes_plain = (n_data + N_MC) * (8 * n_mass + 8 * n_ang + 8)
+    bytes_plain = (n_data + n_mc) * (8 * n_mass + 8 * n_ang + 8)
     hbm, peak_kind = _peaks()
     ach = bytes_mixed / (t_kernel / k_kernel) / 1e9
     ach_p = bytes_plain / (t_kernel_p / k_kernel) / 1e9
@@ -352,7 +356,7 @@ def main():
         "config": {"workload": WORKLOAD, "precision": "mixed: per-event partial-wave columns "
                    "cached as FP32 (computed in FP64), FP64 amplitude sum, log and reductions; "
                    "MC integral from the FP64 Gram matrix (masses/widths fixed)",
-                   "events_per_rank": {"data": n_data, "mc": N_MC},
+                   "events_per_rank": {"data": n_data, "mc": n_mc},
                    "l2": "256 MB buffer written before every timed step (L2 126 MB)",
                    "parallelism": f"dp{world}" if world > 1 else "single GPU"},
         "plain_f64": {"value": world * args.steps / t_plain, "unit": "evals/s",
