@@ -234,25 +234,35 @@ extern "C" __global__ void pwa_to_f32(const double* __restrict__ in, float* __re
 // ---------------------------------------------------------------------------
 // Cached partial-wave columns (masses and widths fixed).
 //
-// pwa_cache_f32 evaluates F_k,o = S_k * F^ang_k,o of events [0, n) in FP64
-// and stores the structurally non-zero (k, o) pairs as FP32 complex in
-// column-major SoA: Fc[j * ldc + i], j over PWA_NF pairs.  Rounding to FP32
-// happens once per stored value (unbiased, per event), so sums over events
-// keep FP64-level systematic accuracy.
-// pwa_eval_cached streams Fc and the weights once per evaluation and does
-// all arithmetic in FP64: A_o = sum_k c_k F_k,o, f = sum_o |A_o|^2,
-// w clip_log(f), and sum_o conj(A_o) F_k,o scaled by w clip_log'(f).
+// Layout (tile-major, PWA_TPB events per tile, zero-padded last tile):
+//   Fc[(t * PWA_NF + j) * PWA_TPB + e]  float2 (re, im) of pair j of event
+//                                       t*PWA_TPB + e, j over the structurally
+//                                       non-zero (column k, helicity o) pairs;
+//   Wc[t * PWA_TPB + e]                 FP64 weight (0 for padding).
+// A tile is one contiguous block, so one bulk copy moves it to shared memory.
+// Values are computed in FP64 and rounded to FP32 once per stored value
+// (unbiased per-event rounding, no systematic bias in sums over events).
 extern "C" __global__ void __launch_bounds__(PWA_TPB)
     pwa_cache_f32(const Consts C, const double* __restrict__ XA, const double* __restrict__ XM,
-                  long long n, long long ld, long long ldc, float2* __restrict__ Fc) {
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+                  const double* __restrict__ W, long long n, long long ntiles, long long ld,
+                  float2* __restrict__ Fc, double* __restrict__ Wc) {
+  const long long total = ntiles * PWA_TPB;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
        i += (long long)gridDim.x * blockDim.x) {
-    cpx<double> F[PWA_NCOL * PWA_NOUT];
-    model_columns<double>(C, XA, XM, ld, i, F);
+    const long long t = i / PWA_TPB, e = i % PWA_TPB;
+    if (i < n) {
+      cpx<double> F[PWA_NCOL * PWA_NOUT];
+      model_columns<double>(C, XA, XM, ld, i, F);
 #pragma unroll
-    for (int j = 0; j < PWA_NF; ++j) {
-      const cpx<double> v = F[pwa_fk[j] * PWA_NOUT + pwa_fo[j]];
-      Fc[(long long)j * ldc + i] = make_float2((float)v.re, (float)v.im);
+      for (int j = 0; j < PWA_NF; ++j) {
+        const cpx<double> v = F[pwa_fk[j] * PWA_NOUT + pwa_fo[j]];
+        Fc[(t * PWA_NF + j) * PWA_TPB + e] = make_float2((float)v.re, (float)v.im);
+      }
+      Wc[i] = W[i];
+    } else {
+#pragma unroll
+      for (int j = 0; j < PWA_NF; ++j) Fc[(t * PWA_NF + j) * PWA_TPB + e] = make_float2(0.f, 0.f);
+      Wc[i] = 0.0;
     }
   }
 }
@@ -261,26 +271,74 @@ struct CCoup {
   double v[2 * PWA_NCOL];
 };
 
+#ifndef PWA_STAGES
+#define PWA_STAGES 3
+#endif
+#define PWA_CACHE_NA (1 + 2 * PWA_NCOL)
+#define PWA_WAIT_LIMIT (1u << 22)
+
+// Persistent streaming kernel over the column cache.  Thread 0 keeps
+// PWA_STAGES tiles in flight with cp.async.bulk into a shared-memory ring
+// (full-barrier per stage with transaction bytes); every thread evaluates
+// one event of the current tile from shared memory in FP64; a block
+// barrier frees the stage for the next copy.  Block partials go to
+// `partials`; the last block to finish (atomic ticket) sums them in a fixed
+// order and writes out[0 .. NA), out[NA] = error flag (0 = ok, 1 = a
+// barrier wait gave up) and out[NA+1] = seq (the caller's call number, to
+// detect a stale result); `out` may be mapped host memory.
 extern "C" __global__ void __launch_bounds__(PWA_TPB)
-    pwa_eval_cached(const CCoup c, const float2* __restrict__ Fc, const double* __restrict__ W,
-                    long long n, long long ldc, double* __restrict__ partials) {
-  constexpr int NA = 1 + 2 * PWA_NCOL;
+    pwa_eval_cached(const CCoup c, const float2* __restrict__ Fc, const double* __restrict__ Wc,
+                    long long ntiles, double* __restrict__ partials,
+                    unsigned int* __restrict__ ticket, double* __restrict__ out, double seq) {
+  constexpr int NA = PWA_CACHE_NA;
+  constexpr unsigned TILE_F = PWA_NF * PWA_TPB * sizeof(float2);
+  constexpr unsigned TILE_W = PWA_TPB * sizeof(double);
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  float2* sF = (float2*)smem_raw;                                    // [STAGES][NF][TPB]
+  double* sW = (double*)(smem_raw + PWA_STAGES * TILE_F);            // [STAGES][TPB]
+  __shared__ __align__(8) unsigned long long full[PWA_STAGES];
+  __shared__ double red[PWA_TPB / 32][NA];
+  __shared__ int s_last, s_err;
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    s_err = 0;
+    for (int st = 0; st < PWA_STAGES; ++st) mbar_init(&full[st], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  const long long G = gridDim.x, b0 = blockIdx.x;
+  if (tid == 0) {
+    for (int st = 0; st < PWA_STAGES; ++st) {
+      const long long t = b0 + st * G;
+      if (t < ntiles) {
+        mbar_expect_tx(&full[st], TILE_F + TILE_W);
+        bulk_g2s(sF + (long long)st * PWA_NF * PWA_TPB, Fc + t * PWA_NF * PWA_TPB, TILE_F, &full[st]);
+        bulk_g2s(sW + st * PWA_TPB, Wc + t * PWA_TPB, TILE_W, &full[st]);
+      }
+    }
+  }
   double acc[NA];
 #pragma unroll
   for (int j = 0; j < NA; ++j) acc[j] = 0.0;
-  for (long long i = (long long)blockIdx.x * PWA_TPB + threadIdx.x; i < n;
-       i += (long long)gridDim.x * PWA_TPB) {
-    float2 fv[PWA_NF];
-#pragma unroll
-    for (int j = 0; j < PWA_NF; ++j) fv[j] = __ldg(Fc + (long long)j * ldc + i);
-    const double w = __ldg(W + i);
+  int it = 0;
+  for (long long t = b0; t < ntiles; t += G, ++it) {
+    const int st = it % PWA_STAGES;
+    const unsigned par = (unsigned)((it / PWA_STAGES) & 1);
+    if (!mbar_wait(&full[st], par, PWA_WAIT_LIMIT)) {
+      s_err = 1;  // benign race: any thread may set it
+    }
+    __syncthreads();
+    if (s_err) break;
+    const float2* F = sF + (long long)st * PWA_NF * PWA_TPB;
+    const double w = sW[st * PWA_TPB + tid];
     double ar[PWA_NOUT], ai[PWA_NOUT];
 #pragma unroll
     for (int o = 0; o < PWA_NOUT; ++o) ar[o] = ai[o] = 0.0;
 #pragma unroll
     for (int j = 0; j < PWA_NF; ++j) {
       const int k = pwa_fk[j], o = pwa_fo[j];
-      const double fr = fv[j].x, fi = fv[j].y;
+      const float2 v = F[j * PWA_TPB + tid];
+      const double fr = v.x, fi = v.y;
       const double cr = c.v[2 * k], ci = c.v[2 * k + 1];
       ar[o] = fma(cr, fr, fma(-ci, fi, ar[o]));
       ai[o] = fma(cr, fi, fma(ci, fr, ai[o]));
@@ -292,7 +350,6 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB)
     const double cl = clip_log(f, &dl);
     acc[0] = fma(w, cl, acc[0]);
     const double fac = w * dl;
-    // fac * conj(A_o), then acc_k += fac conj(A_o) F_k,o
 #pragma unroll
     for (int o = 0; o < PWA_NOUT; ++o) {
       ar[o] *= fac;
@@ -301,23 +358,66 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB)
 #pragma unroll
     for (int j = 0; j < PWA_NF; ++j) {
       const int k = pwa_fk[j], o = pwa_fo[j];
-      const double fr = fv[j].x, fi = fv[j].y;
+      const float2 v = F[j * PWA_TPB + tid];
+      const double fr = v.x, fi = v.y;
       acc[1 + 2 * k] = fma(ar[o], fr, fma(-ai[o], fi, acc[1 + 2 * k]));
       acc[2 + 2 * k] = fma(ar[o], fi, fma(ai[o], fr, acc[2 + 2 * k]));
     }
+    __syncthreads();  // stage st fully consumed
+    if (tid == 0) {
+      const long long tn = t + (long long)PWA_STAGES * G;
+      if (tn < ntiles) {
+        fence_proxy_async_smem();
+        mbar_expect_tx(&full[st], TILE_F + TILE_W);
+        bulk_g2s(sF + (long long)st * PWA_NF * PWA_TPB, Fc + tn * PWA_NF * PWA_TPB, TILE_F,
+                 &full[st]);
+        bulk_g2s(sW + st * PWA_TPB, Wc + tn * PWA_TPB, TILE_W, &full[st]);
+      }
+    }
   }
-  __shared__ double red[PWA_TPB / 32][NA];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (s_err) {
+    // drain: wait (bounded) for every copy this block issued before exiting
+    const int issued = it + PWA_STAGES;
+    if (tid == 0)
+      for (int k2 = it; k2 < issued; ++k2) {
+        const long long t2 = b0 + (long long)k2 * G;
+        if (t2 < ntiles) mbar_wait(&full[k2 % PWA_STAGES], (unsigned)((k2 / PWA_STAGES) & 1), PWA_WAIT_LIMIT);
+      }
+  }
+  const int lane = tid & 31, warp = tid >> 5;
 #pragma unroll
   for (int j = 0; j < NA; ++j) {
     const double v = warp_sum(acc[j]);
     if (lane == 0) red[warp][j] = v;
   }
   __syncthreads();
-  for (int j = threadIdx.x; j < NA; j += PWA_TPB) {
+  for (int j = tid; j < NA; j += PWA_TPB) {
     double s = 0.0;
 #pragma unroll
     for (int w2 = 0; w2 < PWA_TPB / 32; ++w2) s += red[w2][j];
     partials[(long long)blockIdx.x * NA + j] = s;
+  }
+  if (tid == 0 && s_err) atomicOr((unsigned int*)(ticket + 1), 1u);
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) s_last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  // last block: fixed-order sums over blocks, one warp per accumulator
+  for (int j = warp; j < NA; j += PWA_TPB / 32) {
+    double s = 0.0;
+    for (int bb = lane; bb < (int)gridDim.x; bb += 32) s += __ldcg(partials + (long long)bb * NA + j);
+    s = warp_sum(s);
+    if (lane == 0) out[j] = s;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    const unsigned e = atomicOr((unsigned int*)(ticket + 1), 0u);
+    out[NA] = (double)e;
+    out[NA + 1] = seq;
+    ticket[0] = 0u;
+    ticket[1] = 0u;
+    __threadfence_system();
   }
 }

@@ -50,8 +50,14 @@ struct pwa_plan {
   // cached partial-wave columns of the data events (FP32 complex, SoA)
   int nf = 0;
   float2* fcache = nullptr;
-  long long ldc = 0, fcache_n = 0;
+  double* wcache = nullptr;
+  long long ntiles = 0, ntiles_cap = 0, fcache_n = 0;
   int cached_blocks = 0;
+  size_t cached_smem = 0;
+  unsigned int* ticket = nullptr;  // [0] finished-block count, [1] error flag
+  double* h_map = nullptr;         // mapped pinned result of the cached kernel
+  double* d_map = nullptr;         // its device address
+  double seq = 0.0;
   std::vector<double> gram;  // MC Gram matrix, (re, im) row-major ncol x ncol
   bool gram_valid = false;
   // parameter layout for the C-side chain rule
@@ -219,6 +225,10 @@ int pwa_plan_create(const char* src, size_t src_len, int n_mass, int n_angle, in
     h->local_bytes[p] = (long long)a.localSizeBytes;
   }
   CU(cudaMalloc(&h->d_out, sizeof(double) * 2 * h->nacc));
+  CU(cudaMalloc(&h->ticket, 2 * sizeof(unsigned int)));
+  CU(cudaMemset(h->ticket, 0, 2 * sizeof(unsigned int)));
+  CU(cudaHostAlloc(&h->h_map, sizeof(double) * (2 * ncol + 4), cudaHostAllocMapped));
+  CU(cudaHostGetDevicePointer((void**)&h->d_map, h->h_map, 0));
   CU(cudaMallocHost(&h->h_out, sizeof(double) * 2 * (h->nacc > ncol * ncol ? h->nacc : ncol * ncol)));
   return PWA_OK;
 }
@@ -228,6 +238,9 @@ int pwa_plan_destroy(pwa_plan* h) {
   free_events(h);
   if (h->partials) cudaFree(h->partials);
   if (h->fcache) cudaFree(h->fcache);
+  if (h->wcache) cudaFree(h->wcache);
+  if (h->ticket) cudaFree(h->ticket);
+  if (h->h_map) cudaFreeHost(h->h_map);
   if (h->d_out) cudaFree(h->d_out);
   if (h->h_out) cudaFreeHost(h->h_out);
   if (h->lib) cudaLibraryUnload(h->lib);
@@ -428,26 +441,41 @@ int pwa_cache_data(pwa_plan* h, const double* consts, void* stream) {
   if (!consts) return set_err(h, PWA_ERR_ARG, "null consts");
   cudaStream_t s = (cudaStream_t)stream;
   const long long n = h->n_data;
-  const long long ldc = (n + 31) / 32 * 32;
-  if (h->fcache == nullptr || ldc > h->ldc) {
+  const long long tile = h->tpb;
+  const long long ntiles = (n + tile - 1) / tile;
+  if (h->fcache == nullptr || ntiles > h->ntiles_cap) {
     if (h->fcache) cudaFree(h->fcache);
+    if (h->wcache) cudaFree(h->wcache);
     h->fcache = nullptr;
-    if (cudaMalloc(&h->fcache, sizeof(float2) * (size_t)ldc * h->nf) != cudaSuccess)
+    h->wcache = nullptr;
+    h->ntiles_cap = 0;
+    if (cudaMalloc(&h->fcache, sizeof(float2) * (size_t)ntiles * tile * h->nf) != cudaSuccess ||
+        cudaMalloc(&h->wcache, sizeof(double) * (size_t)ntiles * tile) != cudaSuccess)
       return set_err(h, PWA_ERR_OOM, "cudaMalloc of the column cache failed");
-    h->ldc = ldc;
+    h->ntiles_cap = ntiles;
   }
+  h->ntiles = ntiles;
   std::vector<double> cbuf(consts, consts + h->nconst);
-  long long ld = h->ld, ldcv = h->ldc;
-  void* args[] = {cbuf.data(), &h->xa, &h->xm, (void*)&n, &ld, &ldcv, &h->fcache};
-  long long nb = (n + h->tpb - 1) / h->tpb;
+  long long ld = h->ld, nt = ntiles;
+  void* args[] = {cbuf.data(), &h->xa, &h->xm, &h->w, (void*)&n, &nt, &ld, &h->fcache,
+                  &h->wcache};
+  long long nb = (ntiles * tile + h->tpb - 1) / h->tpb;
   if (nb > 16LL * h->sms) nb = 16LL * h->sms;
   int rc = launch(h, h->k.cache_f32, dim3((int)nb), dim3(h->tpb), args, s);
   if (rc) return rc;
+  // streaming kernel: PWA_STAGES tiles of (nf float2 + 1 double) per event in
+  // shared memory per block
+  const int stages = 3;
+  h->cached_smem = (size_t)stages * tile * (h->nf * sizeof(float2) + sizeof(double));
+  CU(cudaFuncSetAttribute((const void*)h->k.eval_cached,
+                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->cached_smem));
   int per_sm = 0;
-  CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)h->k.eval_cached, h->tpb, 0));
-  if (per_sm < 1) per_sm = 1;
-  long long want = (long long)per_sm * h->sms, need = (n + h->tpb - 1) / h->tpb;
-  h->cached_blocks = (int)(want < need ? want : need);
+  CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)h->k.eval_cached, h->tpb,
+                                                   h->cached_smem));
+  if (per_sm < 1)
+    return set_err(h, PWA_ERR_ARG, "column tile does not fit in shared memory");
+  long long want = (long long)per_sm * h->sms;
+  h->cached_blocks = (int)(want < ntiles ? want : ntiles);
   rc = ensure_partials(h, (long long)h->cached_blocks * (1 + 2 * h->ncol));
   if (rc) return rc;
   CU(cudaStreamSynchronize(s));
@@ -461,13 +489,30 @@ int pwa_eval_cached_enqueue(pwa_plan* h, const double* ck, void* stream) {
   if (!ck) return set_err(h, PWA_ERR_ARG, "null couplings");
   cudaStream_t s = (cudaStream_t)stream;
   std::vector<double> cbuf(ck, ck + 2 * h->ncol);
-  long long n = h->fcache_n, ldc = h->ldc;
-  void* args[] = {cbuf.data(), &h->fcache, &h->w, &n, &ldc, &h->partials};
-  int rc = launch(h, h->k.eval_cached, dim3(h->cached_blocks), dim3(h->tpb), args, s);
-  if (rc) return rc;
-  int na = 1 + 2 * h->ncol, nb = h->cached_blocks;
-  void* args2[] = {&h->partials, &na, &nb, &nb, &h->d_out};
-  return launch(h, h->k.reduce, dim3(1), dim3(1024), args2, s);
+  long long nt = h->ntiles;
+  h->seq += 1.0;
+  double seq = h->seq;
+  void* args[] = {cbuf.data(), &h->fcache, &h->wcache, &nt, &h->partials, &h->ticket, &h->d_map,
+                  &seq};
+  cudaError_t e = cudaLaunchKernel((const void*)h->k.eval_cached, dim3(h->cached_blocks),
+                                   dim3(h->tpb), args, h->cached_smem, s);
+  if (e != cudaSuccess)
+    return set_err(h, PWA_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+  return PWA_OK;
+}
+
+// Result of the last cached launch (after the stream has been synchronised):
+// checks the error flag and the call number.
+int cached_result(pwa_plan* h, const double** sums) {
+  const int na = 1 + 2 * h->ncol;
+  const volatile double* m = h->h_map;
+  if (m[na + 1] != h->seq) {
+    cudaMemset(h->ticket, 0, 2 * sizeof(unsigned int));
+    return set_err(h, PWA_ERR_CUDA, "cached evaluation did not complete (stale result)");
+  }
+  if (m[na] != 0.0) return set_err(h, PWA_ERR_CUDA, "cached evaluation: a barrier wait timed out");
+  *sums = h->h_map;
+  return PWA_OK;
 }
 
 int pwa_set_param_layout(pwa_plan* h, int n_vars, int n_coup, const int* coup_r,
@@ -531,8 +576,6 @@ int pwa_pieces_cached(pwa_plan* h, const double* vars, double sw, double mc_shar
   cudaStream_t s = (cudaStream_t)stream;
   int rc = pwa_eval_cached_enqueue(h, ck.data(), stream);
   if (rc) return rc;
-  const int na = 1 + 2 * K;
-  CU(cudaMemcpyAsync(h->h_out, h->d_out, sizeof(double) * na, cudaMemcpyDeviceToHost, s));
   // MC term from the Gram matrix while the kernels run: I = c^H M c,
   // Gm_k = sum_l conj(c_l) M_lk
   std::vector<cplx> Gm(K, cplx{0, 0});
@@ -550,7 +593,9 @@ int pwa_pieces_cached(pwa_plan* h, const double* vars, double sw, double mc_shar
     I += acc.r * ck[2 * k] - acc.i * ck[2 * k + 1];
   }
   CU(cudaStreamSynchronize(s));
-  const double* sd = h->h_out;
+  const double* sd = nullptr;
+  rc = cached_result(h, &sd);
+  if (rc) return rc;
   // chain rule: d f / d theta = 2 Re sum_k J_k G_k
   out[0] = sd[0];
   out[1] = I * mc_share;
