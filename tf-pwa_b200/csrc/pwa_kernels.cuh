@@ -268,7 +268,8 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB)
 }
 
 struct CCoup {
-  double v[2 * PWA_NCOL];
+  float hi[2 * PWA_NCOL];  // column couplings c_k = hi + lo, (re, im) pairs
+  float lo[2 * PWA_NCOL];
 };
 
 #ifndef PWA_STAGES
@@ -280,7 +281,8 @@ struct CCoup {
 // Persistent streaming kernel over the column cache.  Thread 0 keeps
 // PWA_STAGES tiles in flight with cp.async.bulk into a shared-memory ring
 // (full-barrier per stage with transaction bytes); every thread evaluates
-// one event of the current tile from shared memory in FP64; a block
+// one event of the current tile from shared memory (A, G_k with FP32
+// FMAs on exactly split couplings; f, log and all sums in FP64); a block
 // barrier frees the stage for the next copy.  Block partials go to
 // `partials`; the last block to finish (atomic ticket) sums them in a fixed
 // order and writes out[0 .. NA), out[NA] = error flag (0 = ok, 1 = a
@@ -331,37 +333,51 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB)
     if (s_err) break;
     const float2* F = sF + (long long)st * PWA_NF * PWA_TPB;
     const double w = sW[st * PWA_TPB + tid];
-    double ar[PWA_NOUT], ai[PWA_NOUT];
+    // A_o = sum_k c_k F_k,o in FP32 with the couplings split c = hi + lo
+    // (hi, lo FP32): the constants carry no FP32 rounding, so the remaining
+    // error is per-event rounding (random), not a bias shared by all events.
+    float ar[PWA_NOUT], ai[PWA_NOUT];
 #pragma unroll
-    for (int o = 0; o < PWA_NOUT; ++o) ar[o] = ai[o] = 0.0;
+    for (int o = 0; o < PWA_NOUT; ++o) ar[o] = ai[o] = 0.f;
 #pragma unroll
     for (int j = 0; j < PWA_NF; ++j) {
       const int k = pwa_fk[j], o = pwa_fo[j];
       const float2 v = F[j * PWA_TPB + tid];
-      const double fr = v.x, fi = v.y;
-      const double cr = c.v[2 * k], ci = c.v[2 * k + 1];
-      ar[o] = fma(cr, fr, fma(-ci, fi, ar[o]));
-      ai[o] = fma(cr, fi, fma(ci, fr, ai[o]));
+      const float crh = c.hi[2 * k], cih = c.hi[2 * k + 1];
+      const float crl = c.lo[2 * k], cil = c.lo[2 * k + 1];
+      ar[o] = fmaf(crl, v.x, fmaf(-cil, v.y, ar[o]));
+      ai[o] = fmaf(crl, v.y, fmaf(cil, v.x, ai[o]));
+      ar[o] = fmaf(crh, v.x, fmaf(-cih, v.y, ar[o]));
+      ai[o] = fmaf(crh, v.y, fmaf(cih, v.x, ai[o]));
     }
-    double f = 0.0;
+    float ff = 0.f;
 #pragma unroll
-    for (int o = 0; o < PWA_NOUT; ++o) f = fma(ar[o], ar[o], fma(ai[o], ai[o], f));
+    for (int o = 0; o < PWA_NOUT; ++o) ff = fmaf(ar[o], ar[o], fmaf(ai[o], ai[o], ff));
+    const double f = (double)ff;
     double dl;
     const double cl = clip_log(f, &dl);
     acc[0] = fma(w, cl, acc[0]);
-    const double fac = w * dl;
+    const float fac = (float)(w * dl);
 #pragma unroll
     for (int o = 0; o < PWA_NOUT; ++o) {
       ar[o] *= fac;
       ai[o] *= -fac;
     }
+    // per-event sensitivities in FP32, summed over events in FP64
+    float gr[PWA_NCOL], gi[PWA_NCOL];
+#pragma unroll
+    for (int k = 0; k < PWA_NCOL; ++k) gr[k] = gi[k] = 0.f;
 #pragma unroll
     for (int j = 0; j < PWA_NF; ++j) {
       const int k = pwa_fk[j], o = pwa_fo[j];
       const float2 v = F[j * PWA_TPB + tid];
-      const double fr = v.x, fi = v.y;
-      acc[1 + 2 * k] = fma(ar[o], fr, fma(-ai[o], fi, acc[1 + 2 * k]));
-      acc[2 + 2 * k] = fma(ar[o], fi, fma(ai[o], fr, acc[2 + 2 * k]));
+      gr[k] = fmaf(ar[o], v.x, fmaf(-ai[o], v.y, gr[k]));
+      gi[k] = fmaf(ar[o], v.y, fmaf(ai[o], v.x, gi[k]));
+    }
+#pragma unroll
+    for (int k = 0; k < PWA_NCOL; ++k) {
+      acc[1 + 2 * k] += (double)gr[k];
+      acc[2 + 2 * k] += (double)gi[k];
     }
     __syncthreads();  // stage st fully consumed
     if (tid == 0) {

@@ -488,7 +488,13 @@ int pwa_eval_cached_enqueue(pwa_plan* h, const double* ck, void* stream) {
   if (h->fcache_n <= 0) return set_err(h, PWA_ERR_STATE, "no column cache (call pwa_cache_data)");
   if (!ck) return set_err(h, PWA_ERR_ARG, "null couplings");
   cudaStream_t s = (cudaStream_t)stream;
-  std::vector<double> cbuf(ck, ck + 2 * h->ncol);
+  // couplings as FP32 hi + lo pairs (layout of CCoup in pwa_kernels.cuh)
+  std::vector<float> cbuf(4 * h->ncol);
+  for (int k = 0; k < 2 * h->ncol; ++k) {
+    const float hi = (float)ck[k];
+    cbuf[k] = hi;
+    cbuf[2 * h->ncol + k] = (float)(ck[k] - (double)hi);
+  }
   long long nt = h->ntiles;
   h->seq += 1.0;
   double seq = h->seq;
