@@ -333,6 +333,15 @@ def main():
     ck = np.stack([eng._ck.real, eng._ck.imag], 1).reshape(-1)
     k_kernel = args.steps
     t_kernel = timed(lambda: eng.eval_cached_enqueue(ck), k_kernel)
+    variants = {}
+    for var in (0, 1):
+        eng.set_cached_variant(var)
+        variants[var] = {"kernel_us": 1e6 * timed(lambda: eng.eval_cached_enqueue(ck), k_kernel)
+                         / k_kernel,
+                         "step_us": 1e6 * timed(lambda: eng.nll_grad_cached(var_vec), args.steps)
+                         / args.steps,
+                         "nll": eng.nll_grad_cached(var_vec)[0]}
+    eng.set_cached_variant(0)
     Cp = eng_p.consts(vals)
     t_kernel_p = timed(lambda: eng_p.eval_enqueue(Cp, PLAIN_F64, mc=True), k_kernel)
     ck_clocks = clocks.stop(local)
@@ -374,7 +383,8 @@ def main():
                      "plain_f64_kernel": {"achieved": ach_p, "frac": ach_p / hbm,
                                           "launch_us": 1e6 * t_kernel_p / k_kernel,
                                           "algorithmic_bytes_per_launch": bytes_plain}},
-        "gpu_launches": 2 * args.steps,
+        "gpu_launches": args.steps,
+        "cached_variants": variants,
         "check": {"nll_mixed": nll_m, "nll_plain": nll_p, "dnll": nll_m - nll_p,
                   "grad_max_rel": float(np.max(np.abs(g_m - g_p)) / np.max(np.abs(g_p)))},
         "setup_s": {"dataset": t_data},

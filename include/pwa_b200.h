@@ -102,6 +102,10 @@ int pwa_build_gram(pwa_plan* h, const double* consts, void* stream, double* out)
  * streams the column cache once with FP64 arithmetic. */
 int pwa_cache_data(pwa_plan* h, const double* consts, void* stream);
 
+/* Kernel used for the cached data term: 0 = shared-memory ring fed by bulk
+ * copies, 1 = direct loads with four blocks per SM (default 0). */
+int pwa_set_cached_variant(pwa_plan* h, int variant);
+
 /* Data-term kernels on the cache with column couplings ck[2*ncol]
  * (re, im); sums (1 + 2*ncol doubles) stay on the device. */
 int pwa_eval_cached_enqueue(pwa_plan* h, const double* ck, void* stream);

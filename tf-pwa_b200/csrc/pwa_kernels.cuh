@@ -268,8 +268,7 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB)
 }
 
 struct CCoup {
-  float hi[2 * PWA_NCOL];  // column couplings c_k = hi + lo, (re, im) pairs
-  float lo[2 * PWA_NCOL];
+  double v[2 * PWA_NCOL];  // column couplings c_k, (re, im) pairs
 };
 
 #ifndef PWA_STAGES
@@ -281,8 +280,7 @@ struct CCoup {
 // Persistent streaming kernel over the column cache.  Thread 0 keeps
 // PWA_STAGES tiles in flight with cp.async.bulk into a shared-memory ring
 // (full-barrier per stage with transaction bytes); every thread evaluates
-// one event of the current tile from shared memory (A, G_k with FP32
-// FMAs on exactly split couplings; f, log and all sums in FP64); a block
+// one event of the current tile from shared memory in FP64; a block
 // barrier frees the stage for the next copy.  Block partials go to
 // `partials`; the last block to finish (atomic ticket) sums them in a fixed
 // order and writes out[0 .. NA), out[NA] = error flag (0 = ok, 1 = a
@@ -333,51 +331,37 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB)
     if (s_err) break;
     const float2* F = sF + (long long)st * PWA_NF * PWA_TPB;
     const double w = sW[st * PWA_TPB + tid];
-    // A_o = sum_k c_k F_k,o in FP32 with the couplings split c = hi + lo
-    // (hi, lo FP32): the constants carry no FP32 rounding, so the remaining
-    // error is per-event rounding (random), not a bias shared by all events.
-    float ar[PWA_NOUT], ai[PWA_NOUT];
+    double ar[PWA_NOUT], ai[PWA_NOUT];
 #pragma unroll
-    for (int o = 0; o < PWA_NOUT; ++o) ar[o] = ai[o] = 0.f;
+    for (int o = 0; o < PWA_NOUT; ++o) ar[o] = ai[o] = 0.0;
 #pragma unroll
     for (int j = 0; j < PWA_NF; ++j) {
       const int k = pwa_fk[j], o = pwa_fo[j];
       const float2 v = F[j * PWA_TPB + tid];
-      const float crh = c.hi[2 * k], cih = c.hi[2 * k + 1];
-      const float crl = c.lo[2 * k], cil = c.lo[2 * k + 1];
-      ar[o] = fmaf(crl, v.x, fmaf(-cil, v.y, ar[o]));
-      ai[o] = fmaf(crl, v.y, fmaf(cil, v.x, ai[o]));
-      ar[o] = fmaf(crh, v.x, fmaf(-cih, v.y, ar[o]));
-      ai[o] = fmaf(crh, v.y, fmaf(cih, v.x, ai[o]));
+      const double fr = v.x, fi = v.y;
+      const double cr = c.v[2 * k], ci = c.v[2 * k + 1];
+      ar[o] = fma(cr, fr, fma(-ci, fi, ar[o]));
+      ai[o] = fma(cr, fi, fma(ci, fr, ai[o]));
     }
-    float ff = 0.f;
+    double f = 0.0;
 #pragma unroll
-    for (int o = 0; o < PWA_NOUT; ++o) ff = fmaf(ar[o], ar[o], fmaf(ai[o], ai[o], ff));
-    const double f = (double)ff;
+    for (int o = 0; o < PWA_NOUT; ++o) f = fma(ar[o], ar[o], fma(ai[o], ai[o], f));
     double dl;
     const double cl = clip_log(f, &dl);
     acc[0] = fma(w, cl, acc[0]);
-    const float fac = (float)(w * dl);
+    const double fac = w * dl;
 #pragma unroll
     for (int o = 0; o < PWA_NOUT; ++o) {
       ar[o] *= fac;
       ai[o] *= -fac;
     }
-    // per-event sensitivities in FP32, summed over events in FP64
-    float gr[PWA_NCOL], gi[PWA_NCOL];
-#pragma unroll
-    for (int k = 0; k < PWA_NCOL; ++k) gr[k] = gi[k] = 0.f;
 #pragma unroll
     for (int j = 0; j < PWA_NF; ++j) {
       const int k = pwa_fk[j], o = pwa_fo[j];
       const float2 v = F[j * PWA_TPB + tid];
-      gr[k] = fmaf(ar[o], v.x, fmaf(-ai[o], v.y, gr[k]));
-      gi[k] = fmaf(ar[o], v.y, fmaf(ai[o], v.x, gi[k]));
-    }
-#pragma unroll
-    for (int k = 0; k < PWA_NCOL; ++k) {
-      acc[1 + 2 * k] += (double)gr[k];
-      acc[2 + 2 * k] += (double)gi[k];
+      const double fr = v.x, fi = v.y;
+      acc[1 + 2 * k] = fma(ar[o], fr, fma(-ai[o], fi, acc[1 + 2 * k]));
+      acc[2 + 2 * k] = fma(ar[o], fi, fma(ai[o], fr, acc[2 + 2 * k]));
     }
     __syncthreads();  // stage st fully consumed
     if (tid == 0) {
@@ -431,6 +415,108 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB)
   if (tid == 0) {
     const unsigned e = atomicOr((unsigned int*)(ticket + 1), 0u);
     out[NA] = (double)e;
+    out[NA + 1] = seq;
+    ticket[0] = 0u;
+    ticket[1] = 0u;
+    __threadfence_system();
+  }
+}
+
+// Direct-load variant of pwa_eval_cached: no shared-memory staging; each
+// thread loads its event's pairs straight from the tile-major cache (a warp
+// reads 256 contiguous bytes per pair) and the register budget is capped so
+// that four blocks (16 warps) share an SM.  A, f, log and all cross-event
+// sums in FP64; the per-event sensitivities G_k in FP32 (per-event rounding
+// only, summed in FP64).  Same outputs and protocol as pwa_eval_cached.
+extern "C" __global__ void __launch_bounds__(PWA_TPB, 4)
+    pwa_eval_cached_direct(const CCoup c, const float2* __restrict__ Fc,
+                           const double* __restrict__ Wc, long long ntiles,
+                           double* __restrict__ partials, unsigned int* __restrict__ ticket,
+                           double* __restrict__ out, double seq) {
+  constexpr int NA = PWA_CACHE_NA;
+  __shared__ double red[PWA_TPB / 32][NA];
+  __shared__ int s_last;
+  const int tid = threadIdx.x;
+  double acc0 = 0.0;
+  double accg[2 * PWA_NCOL];
+#pragma unroll
+  for (int j = 0; j < 2 * PWA_NCOL; ++j) accg[j] = 0.0;
+  for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const float2* F = Fc + t * PWA_NF * PWA_TPB + tid;
+    float2 v[PWA_NF];
+#pragma unroll
+    for (int j = 0; j < PWA_NF; ++j) v[j] = __ldcs(F + j * PWA_TPB);
+    const double w = __ldcs(Wc + t * PWA_TPB + tid);
+    double ar[PWA_NOUT], ai[PWA_NOUT];
+#pragma unroll
+    for (int o = 0; o < PWA_NOUT; ++o) ar[o] = ai[o] = 0.0;
+#pragma unroll
+    for (int j = 0; j < PWA_NF; ++j) {
+      const int k = pwa_fk[j], o = pwa_fo[j];
+      const double cr = c.v[2 * k], ci = c.v[2 * k + 1];
+      ar[o] = fma(cr, (double)v[j].x, fma(-ci, (double)v[j].y, ar[o]));
+      ai[o] = fma(cr, (double)v[j].y, fma(ci, (double)v[j].x, ai[o]));
+    }
+    double f = 0.0;
+#pragma unroll
+    for (int o = 0; o < PWA_NOUT; ++o) f = fma(ar[o], ar[o], fma(ai[o], ai[o], f));
+    double dl;
+    const double cl = clip_log(f, &dl);
+    acc0 = fma(w, cl, acc0);
+    const double fac = w * dl;
+    float br[PWA_NOUT], bi[PWA_NOUT];
+#pragma unroll
+    for (int o = 0; o < PWA_NOUT; ++o) {
+      br[o] = (float)(fac * ar[o]);
+      bi[o] = (float)(-fac * ai[o]);
+    }
+    float gr[PWA_NCOL], gi[PWA_NCOL];
+#pragma unroll
+    for (int k = 0; k < PWA_NCOL; ++k) gr[k] = gi[k] = 0.f;
+#pragma unroll
+    for (int j = 0; j < PWA_NF; ++j) {
+      const int k = pwa_fk[j], o = pwa_fo[j];
+      gr[k] = fmaf(br[o], v[j].x, fmaf(-bi[o], v[j].y, gr[k]));
+      gi[k] = fmaf(br[o], v[j].y, fmaf(bi[o], v[j].x, gi[k]));
+    }
+#pragma unroll
+    for (int k = 0; k < PWA_NCOL; ++k) {
+      accg[2 * k] += (double)gr[k];
+      accg[2 * k + 1] += (double)gi[k];
+    }
+  }
+  const int lane = tid & 31, warp = tid >> 5;
+  {
+    const double v0 = warp_sum(acc0);
+    if (lane == 0) red[warp][0] = v0;
+  }
+#pragma unroll
+  for (int j = 0; j < 2 * PWA_NCOL; ++j) {
+    const double v2 = warp_sum(accg[j]);
+    if (lane == 0) red[warp][1 + j] = v2;
+  }
+  __syncthreads();
+  for (int j = tid; j < NA; j += PWA_TPB) {
+    double s2 = 0.0;
+#pragma unroll
+    for (int w2 = 0; w2 < PWA_TPB / 32; ++w2) s2 += red[w2][j];
+    partials[(long long)blockIdx.x * NA + j] = s2;
+  }
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) s_last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  for (int j = warp; j < NA; j += PWA_TPB / 32) {
+    double s2 = 0.0;
+    for (int bb = lane; bb < (int)gridDim.x; bb += 32) s2 += __ldcg(partials + (long long)bb * NA + j);
+    s2 = warp_sum(s2);
+    if (lane == 0) out[j] = s2;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    out[NA] = (double)atomicOr((unsigned int*)(ticket + 1), 0u);
     out[NA + 1] = seq;
     ticket[0] = 0u;
     ticket[1] = 0u;

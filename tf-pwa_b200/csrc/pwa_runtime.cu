@@ -27,7 +27,8 @@ namespace {
 struct Kernels {
   cudaKernel_t eval_f64 = nullptr, eval_f32 = nullptr, reduce = nullptr, pdf_f64 = nullptr,
                pdf_f32 = nullptr, columns_f64 = nullptr, gram_f64 = nullptr, sum_rows = nullptr,
-               to_f32 = nullptr, cache_f32 = nullptr, eval_cached = nullptr;
+               to_f32 = nullptr, cache_f32 = nullptr, eval_cached = nullptr,
+               eval_cached_direct = nullptr;
 };
 
 }  // namespace
@@ -52,7 +53,8 @@ struct pwa_plan {
   float2* fcache = nullptr;
   double* wcache = nullptr;
   long long ntiles = 0, ntiles_cap = 0, fcache_n = 0;
-  int cached_blocks = 0;
+  int cached_blocks = 0, cached_blocks_direct = 0;
+  int cached_variant = 0;  // 0: shared-memory ring (bulk copies), 1: direct loads
   size_t cached_smem = 0;
   unsigned int* ticket = nullptr;  // [0] finished-block count, [1] error flag
   double* h_map = nullptr;         // mapped pinned result of the cached kernel
@@ -216,7 +218,8 @@ int pwa_plan_create(const char* src, size_t src_len, int n_mass, int n_angle, in
             {"pwa_pdf_f32", &h->k.pdf_f32},         {"pwa_columns_f64", &h->k.columns_f64},
             {"pwa_gram_f64", &h->k.gram_f64},       {"pwa_sum_rows", &h->k.sum_rows},
             {"pwa_to_f32", &h->k.to_f32},           {"pwa_cache_f32", &h->k.cache_f32},
-            {"pwa_eval_cached", &h->k.eval_cached}};
+            {"pwa_eval_cached", &h->k.eval_cached},
+            {"pwa_eval_cached_direct", &h->k.eval_cached_direct}};
   for (auto& e : ks) CU(cudaLibraryGetKernel(e.slot, h->lib, e.name));
   for (int p = 0; p < 2; ++p) {
     cudaFuncAttributes a;
@@ -476,7 +479,15 @@ int pwa_cache_data(pwa_plan* h, const double* consts, void* stream) {
     return set_err(h, PWA_ERR_ARG, "column tile does not fit in shared memory");
   long long want = (long long)per_sm * h->sms;
   h->cached_blocks = (int)(want < ntiles ? want : ntiles);
-  rc = ensure_partials(h, (long long)h->cached_blocks * (1 + 2 * h->ncol));
+  int per_sm2 = 0;
+  CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, (const void*)h->k.eval_cached_direct,
+                                                   h->tpb, 0));
+  if (per_sm2 < 1) per_sm2 = 1;
+  long long want2 = (long long)per_sm2 * h->sms;
+  h->cached_blocks_direct = (int)(want2 < ntiles ? want2 : ntiles);
+  const int mb = h->cached_blocks > h->cached_blocks_direct ? h->cached_blocks
+                                                            : h->cached_blocks_direct;
+  rc = ensure_partials(h, (long long)mb * (1 + 2 * h->ncol));
   if (rc) return rc;
   CU(cudaStreamSynchronize(s));
   h->fcache_n = n;
@@ -488,20 +499,18 @@ int pwa_eval_cached_enqueue(pwa_plan* h, const double* ck, void* stream) {
   if (h->fcache_n <= 0) return set_err(h, PWA_ERR_STATE, "no column cache (call pwa_cache_data)");
   if (!ck) return set_err(h, PWA_ERR_ARG, "null couplings");
   cudaStream_t s = (cudaStream_t)stream;
-  // couplings as FP32 hi + lo pairs (layout of CCoup in pwa_kernels.cuh)
-  std::vector<float> cbuf(4 * h->ncol);
-  for (int k = 0; k < 2 * h->ncol; ++k) {
-    const float hi = (float)ck[k];
-    cbuf[k] = hi;
-    cbuf[2 * h->ncol + k] = (float)(ck[k] - (double)hi);
-  }
+  std::vector<double> cbuf(ck, ck + 2 * h->ncol);
   long long nt = h->ntiles;
   h->seq += 1.0;
   double seq = h->seq;
   void* args[] = {cbuf.data(), &h->fcache, &h->wcache, &nt, &h->partials, &h->ticket, &h->d_map,
                   &seq};
-  cudaError_t e = cudaLaunchKernel((const void*)h->k.eval_cached, dim3(h->cached_blocks),
-                                   dim3(h->tpb), args, h->cached_smem, s);
+  cudaError_t e =
+      h->cached_variant == 1
+          ? cudaLaunchKernel((const void*)h->k.eval_cached_direct, dim3(h->cached_blocks_direct),
+                             dim3(h->tpb), args, 0, s)
+          : cudaLaunchKernel((const void*)h->k.eval_cached, dim3(h->cached_blocks), dim3(h->tpb),
+                             args, h->cached_smem, s);
   if (e != cudaSuccess)
     return set_err(h, PWA_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
   return PWA_OK;
@@ -518,6 +527,13 @@ int cached_result(pwa_plan* h, const double** sums) {
   }
   if (m[na] != 0.0) return set_err(h, PWA_ERR_CUDA, "cached evaluation: a barrier wait timed out");
   *sums = h->h_map;
+  return PWA_OK;
+}
+
+int pwa_set_cached_variant(pwa_plan* h, int variant) {
+  if (!h) return PWA_ERR_ARG;
+  if (variant != 0 && variant != 1) return set_err(h, PWA_ERR_ARG, "variant must be 0 or 1");
+  h->cached_variant = variant;
   return PWA_OK;
 }
 

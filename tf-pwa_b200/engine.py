@@ -52,6 +52,7 @@ def load_library(path=LIB_PATH):
     lib.pwa_set_param_layout.argtypes = [vp, i, i, ip, ip, ip, i, ip, i, ip]
     lib.pwa_pieces_cached.argtypes = [vp, dp, ctypes.c_double, ctypes.c_double, vp, dp]
     lib.pwa_nll_grad_cached.argtypes = [vp, dp, ctypes.c_double, vp, dp, dp]
+    lib.pwa_set_cached_variant.argtypes = [vp, i]
     lib.pwa_eval_noalloc.argtypes = [vp, dp, vp, vp, vp, ll, ll, ll, vp, vp]
     lib.pwa_plan_destroy.argtypes = [vp]
     lib.pwa_compile_only.argtypes = [cp, sz, i, cp, cp, sz]
@@ -74,7 +75,7 @@ def load_library(path=LIB_PATH):
 EXPORTED = ("pwa_plan_create", "pwa_plan_destroy", "pwa_compile_only", "pwa_upload_events",
             "pwa_eval", "pwa_eval_enqueue", "pwa_eval_pdf", "pwa_build_gram", "pwa_cache_data",
             "pwa_eval_cached_enqueue", "pwa_set_param_layout", "pwa_pieces_cached",
-            "pwa_nll_grad_cached", "pwa_eval_noalloc", "pwa_plan_info", "pwa_last_error")
+            "pwa_nll_grad_cached", "pwa_set_cached_variant", "pwa_eval_noalloc", "pwa_plan_info", "pwa_last_error")
 
 
 class PWAError(RuntimeError):
@@ -516,6 +517,10 @@ class Engine:
                                                        ctypes.byref(nll), _dptr(g)),
                     "pwa_nll_grad_cached")
         return nll.value, g
+
+    def set_cached_variant(self, variant):
+        self._check(load_library().pwa_set_cached_variant(self.h, int(variant)),
+                    "pwa_set_cached_variant")
 
     def eval_cached_enqueue(self, ck, stream=None):
         ck = np.ascontiguousarray(ck, np.float64)
