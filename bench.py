@@ -341,7 +341,7 @@ def main():
                          "step_us": 1e6 * timed(lambda: eng.nll_grad_cached(var_vec), args.steps)
                          / args.steps,
                          "nll": eng.nll_grad_cached(var_vec)[0]}
-    eng.set_cached_variant(0)
+    eng.set_cached_variant(1)
     Cp = eng_p.consts(vals)
     t_kernel_p = timed(lambda: eng_p.eval_enqueue(Cp, PLAIN_F64, mc=True), k_kernel)
     ck_clocks = clocks.stop(local)

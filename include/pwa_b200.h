@@ -103,7 +103,7 @@ int pwa_build_gram(pwa_plan* h, const double* consts, void* stream, double* out)
 int pwa_cache_data(pwa_plan* h, const double* consts, void* stream);
 
 /* Kernel used for the cached data term: 0 = shared-memory ring fed by bulk
- * copies, 1 = direct loads with four blocks per SM (default 0). */
+ * copies, 1 = direct loads with four blocks per SM (default 1). */
 int pwa_set_cached_variant(pwa_plan* h, int variant);
 
 /* Data-term kernels on the cache with column couplings ck[2*ncol]

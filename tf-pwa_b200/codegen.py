@@ -1,24 +1,30 @@
 """Model compiler back end: emits the CUDA source of a decay model.
 
-The generated code is one ``model_event<R>()`` device function that, for one
-event, evaluates every partial-wave column F_k of the amplitude, the full
-amplitude A = sum_k c_k F_k, |A|^2 summed over external helicities, and the
-column sensitivities G_k = sum_lambda conj(A_lambda) F_k,lambda from which
-the NLL gradient follows.  Constants (CG products, Wigner-d weights,
-Blatt-Weisskopf coefficients, helicity bookkeeping) are folded into the code;
-per-evaluation quantities (couplings, q0 factors, lineshape constants) are
-read from a ``Consts`` kernel argument laid out by :class:`ConstLayout`.
+Three device functions are generated per model, all straight-line code with
+every constant folded (CG products, Wigner-d weights, Blatt-Weisskopf
+polynomial coefficients, helicity bookkeeping):
 
-The mathematics is the reference's (see ``csrc/pwa_device.cuh`` and the
-restated chain contraction of ``tf_pwa/amp/core.py:1392-1445``): a chain's
-amplitude is the product of its vertices' H(LS) * D*(angles of outs[0]),
-summed over inner helicities, times the lineshapes, the chain total, and the
-alignment D* of spinning final particles.
+``model_amp<R>``      forward pass: the amplitude A_o of every external
+                      helicity combination o, with the couplings contracted
+                      vertex by vertex (H = sum_ls g_ls bf_ls CG_ls, vertex
+                      tensor H * D*, sum over inner helicities, lineshapes,
+                      chain total, alignment D* of spinning finals).
+``model_adj<R>``      adjoint pass: given Abar_o = fac * conj(A_o), recompute
+                      each chain's angular factors and accumulate the column
+                      sensitivities G_k = S_k sum_o Abar_o F^ang_k,o and the
+                      lineshape-parameter sensitivities.  Nothing from the
+                      forward pass is kept, so registers stay per chain.
+``model_columns<R>``  the partial-wave columns F_k,o = S_k F^ang_k,o one
+                      column at a time (for the column cache and the Gram
+                      matrix).
+
+A chain's amplitude is sum_k c_k F_k with c_k = total * prod_vertices g_ls;
+S_k = BW(m) * prod_vertices bf_{l_k}; F^ang_k,o = sum over inner helicities of
+prod_vertices CG_{ls_k}[lb, lc] D*^{Ja}_{la, lb-lc} (then aligned).  The
+mathematics is the reference's chain contraction
+(``tf_pwa/amp/core.py:1149-1164,1392-1445``).
 """
 import itertools
-import math
-
-import numpy as np
 
 from .particles import bprime_coeff, small_d_weight, two
 
@@ -37,6 +43,10 @@ def _lit(v):
     if "e" not in r and "." not in r and "inf" not in r and "nan" not in r:
         r += ".0"
     return f"R({r})"
+
+
+def _key(t):
+    return [float(x) for x in t]
 
 
 class ConstLayout:
@@ -59,7 +69,7 @@ class ConstLayout:
 class ModelCode:
     """Everything the engine needs to know about the compiled model."""
 
-    def __init__(self, group, plan, vm_names=None):
+    def __init__(self, group, plan):
         self.group = group
         self.plan = plan
         self.consts = ConstLayout()
@@ -67,24 +77,42 @@ class ModelCode:
         self.chain_columns = []    # per chain: list of global column ids
         for ci, c in enumerate(group):
             ids = []
-            ranges = [range(len(d.get_ls_list())) for d in c]
-            for lsi in itertools.product(*ranges):
+            for lsi in itertools.product(*[range(len(d.get_ls_list())) for d in c]):
                 ids.append(len(self.columns))
                 self.columns.append((ci, lsi))
             self.chain_columns.append(ids)
         self.outs = [group.top] + list(group.outs)
         self.out_hel = list(itertools.product(*[p.spins for p in self.outs]))
+        self.out_index = {o: j for j, o in enumerate(self.out_hel)}
         self.nout = len(self.out_hel)
-        # field split: masses (always FP64 storage) and angles
         self.mass_fields = [i for i, f in enumerate(plan.fields) if f.startswith("m/")]
         self.angle_fields = [i for i, f in enumerate(plan.fields) if not f.startswith("m/")]
         self.mass_slot = {f: k for k, f in enumerate(self.mass_fields)}
         self.angle_slot = {f: k for k, f in enumerate(self.angle_fields)}
-        # consts: couplings first
+        # constants: column couplings c_k, vertex couplings, chain totals
         for k in range(len(self.columns)):
             self.consts.add(f"c{k}.re")
             self.consts.add(f"c{k}.im")
-        # resonances with shape
+        self.vertices = []
+        seen = set()
+        for c in group:
+            for d in c:
+                if d in seen:
+                    continue
+                seen.add(d)
+                self.vertices.append(d)
+                for i in range(len(d.get_ls_list())):
+                    self.consts.add(f"{d}.g{i}.re")
+                    self.consts.add(f"{d}.g{i}.im")
+                if d.has_barrier_factor and d.has_bprime:
+                    for l in sorted(set(d.get_l_list())):
+                        self.consts.add(f"{d}.Pz0_{l}")
+                if d.has_barrier_factor and d.barrier_factor_norm:
+                    for l in sorted(set(d.get_l_list())):
+                        self.consts.add(f"{d}.norm_{l}")
+        for ci in range(len(group)):
+            self.consts.add(f"t{ci}.re")
+            self.consts.add(f"t{ci}.im")
         self.res = []
         for p in group.resonances:
             kind = p.lineshape_kind()
@@ -98,22 +126,6 @@ class ModelCode:
             elif kind == "BW":
                 self.consts.add(f"{p}.m0sq")
                 self.consts.add(f"{p}.y")
-        # barrier factor constants per decay vertex
-        self.vertices = []
-        seen = set()
-        for c in group:
-            for d in c:
-                if d in seen:
-                    continue
-                seen.add(d)
-                self.vertices.append(d)
-                if d.has_barrier_factor and d.has_bprime:
-                    for l in sorted(set(d.get_l_list())):
-                        self.consts.add(f"{d}.Pz0_{l}")
-                if d.has_barrier_factor and d.barrier_factor_norm:
-                    for l in sorted(set(d.get_l_list())):
-                        self.consts.add(f"{d}.norm_{l}")
-        # shape derivatives: per resonance that may float, d ln(m0*Gamma)/dm0
         self.shape_res = []
         for p, kind in self.res:
             if kind in ("BWR", "BW"):
@@ -123,163 +135,21 @@ class ModelCode:
         self.nshape = 2 * len(self.shape_res)
         self.ncol = len(self.columns)
         self.nacc = 1 + 2 * self.ncol + self.nshape
+        self._analyse()
 
-    # ------------------------------------------------------------ emission
-    def source(self):
-        self._fset = set()
-        L = []
-        L.append(_HEADER.format(ncol=self.ncol, nout=self.nout, nshape=self.nshape,
-                                nacc=self.nacc, nconst=max(len(self.consts), 1)))
-        L.append("template <typename R>\n__device__ __forceinline__ void model_event(\n"
-                 "    const Consts& C, const R* __restrict__ XA, const double* __restrict__ XM,\n"
-                 "    long long ld, long long i, double* __restrict__ fout,\n"
-                 "    cpx<R>* __restrict__ G, double* __restrict__ dshape) {")
-        body = []
-        e = body.append
-        cidx = self.consts.index
-
-        def cst(name):
-            return f"R(C.v[{cidx[name]}])"
-
-        # --- load fields
-        for f in self.mass_fields:
-            e(f"  const double xm{f} = __ldg(XM + (long long){self.mass_slot[f]} * ld + i);")
-        for f in self.angle_fields:
-            e(f"  const R xa{f} = __ldg(XA + (long long){self.angle_slot[f]} * ld + i);")
-
-        # --- per chain
+    # ------------------------------------------------------------ analysis
+    def _analyse(self):
+        """Helicity assignments of every chain and the CG coefficient of
+        every (column, assignment)."""
+        self.chain_assign = []
         for ci, c in enumerate(self.group):
-            cf = self.plan.chains[ci]
-            e(f"  // chain {ci}: {c}")
-
-            def dmass(p, dbl=False):
-                if p in c.inner:
-                    return f"xm{cf['mass'][p]}" if dbl else f"R(xm{cf['mass'][p]})"
-                return repr(float(p.mass)) if dbl else _lit(p.mass)
-
-            # vertices: q^2 (FP64 from FP64 masses), barrier factors, D elements
-            for vi, d in enumerate(c):
-                a, (b, cc) = d.core, d.outs
-                tag = f"c{ci}v{vi}"
-                fa = cf["decays"][vi]
-                if d.has_barrier_factor:
-                    e(f"  const double q2d_{tag} = rel_p2<double>({dmass(a, True)}, {dmass(b, True)}, {dmass(cc, True)});")
-                    e(f"  const R q2_{tag} = R(q2d_{tag});")
-                    for l in sorted(set(d.get_l_list())):
-                        terms = []
-                        if d.has_ql:
-                            if l == 0:
-                                ql = "R(1)"
-                            elif l % 2 == 0:
-                                ql = "*".join([f"q2_{tag}"] * (l // 2))
-                            else:
-                                ql = "*".join([f"psqrt(q2_{tag})"] + [f"q2_{tag}"] * (l // 2))
-                        else:
-                            ql = "R(1)"
-                        if d.has_bprime:
-                            co = bprime_coeff(l)
-                            z = f"(q2_{tag} * {_lit(d.d * d.d)})"
-                            poly = _lit(co[0])
-                            for cc_ in co[1:]:
-                                poly = f"fma({poly}, {z}, {_lit(cc_)})"
-                            e(f"  R bp_{tag}_{l} = {cst(f'{d}.Pz0_{l}')} / ({poly});")
-                            e(f"  bp_{tag}_{l} = bp_{tag}_{l} > R(0) ? bp_{tag}_{l} : R(1);")
-                            bf = f"({ql}) * psqrt(bp_{tag}_{l})"
-                        else:
-                            bf = ql
-                        if d.barrier_factor_norm:
-                            bf = f"({bf}) * {cst(f'{d}.norm_{l}')}"
-                        e(f"  const R bf_{tag}_{l} = {bf};")
-                # D*^{Ja}_{la, lb-lc}(alpha, beta, 0)
-                j2 = two(a.J)
-                need = set()
-                for la in a.spins:
-                    for lb in b.spins:
-                        for lc in cc.spins:
-                            dl = lb - lc
-                            if abs(dl) <= a.J + 1e-9:
-                                need.add((two(la), two(dl)))
-                e(f"  R sp_{tag}[{j2 + 1}], cp_{tag}[{j2 + 1}];")
-                e(f"  half_angle_sc_powers<R, {j2}>(xa{fa['beta']}, sp_{tag}, cp_{tag});")
-                need_alpha = any(n1 != 0 for n1, _ in need)
-                if need_alpha:
-                    e(f"  cpx<R> ea_{tag}[{2 * j2 + 1}];")
-                    e(f"  half_angle_powers<R, {j2}>(xa{fa['alpha']}, ea_{tag});")
-                w = small_d_weight(j2)
-                for n1, n2 in sorted(need):
-                    i1, i2 = (n1 + j2) // 2, (n2 + j2) // 2
-                    terms = [f"{_lit(w[l][i1][i2])} * sp_{tag}[{l}] * cp_{tag}[{j2 - l}]"
-                             for l in range(j2 + 1) if w[l][i1][i2] != 0]
-                    dexpr = " + ".join(terms) if terms else "R(0)"
-                    nm = f"D_{tag}_{n1 + j2}_{n2 + j2}"
-                    if need_alpha and n1 != 0:
-                        e(f"  const cpx<R> {nm} = cscale(ea_{tag}[{n1 + j2}], {dexpr});")
-                    else:
-                        e(f"  const cpx<R> {nm} = cmk<R>({dexpr}, R(0));")
-            # alignment D for spinning finals: e^{i l a} d_{l l'}(b) e^{i l' g}
-            for o, (fa_, fb_, fg_) in cf["aligned"].items():
-                tag = f"c{ci}al{self.group.outs.index(o)}"
-                j2 = two(o.J)
-                e(f"  R sp_{tag}[{j2 + 1}], cp_{tag}[{j2 + 1}];")
-                e(f"  half_angle_sc_powers<R, {j2}>(xa{fb_}, sp_{tag}, cp_{tag});")
-                e(f"  cpx<R> ea_{tag}[{2 * j2 + 1}], eg_{tag}[{2 * j2 + 1}];")
-                e(f"  half_angle_powers<R, {j2}>(xa{fa_}, ea_{tag});")
-                e(f"  half_angle_powers<R, {j2}>(xa{fg_}, eg_{tag});")
-                w = small_d_weight(j2)
-                for l1 in o.spins:
-                    for l2 in o.spins:
-                        n1, n2 = two(l1), two(l2)
-                        i1, i2 = (n1 + j2) // 2, (n2 + j2) // 2
-                        terms = [f"{_lit(w[l][i1][i2])} * sp_{tag}[{l}] * cp_{tag}[{j2 - l}]"
-                                 for l in range(j2 + 1) if w[l][i1][i2] != 0]
-                        dexpr = " + ".join(terms) if terms else "R(0)"
-                        e(f"  const cpx<R> Dal_{tag}_{n1 + j2}_{n2 + j2} = cscale(cmul(ea_{tag}[{n1 + j2}], eg_{tag}[{n2 + j2}]), {dexpr});")
-            # lineshapes of the chain's inner particles
-            bw_names = []
-            for p in c.inner:
-                kind = p.lineshape_kind()
-                tag = f"c{ci}r{c.inner.index(p)}"
-                m = f"xm{cf['mass'][p]}"
-                if kind == "one":
-                    continue
-                bw_names.append(f"bw_{tag}")
-                e(f"  const double xx_{tag} = {repr(0.0)} + C.v[{cidx[f'{p}.m0sq']}] - {m} * {m};")
-                if kind == "BWR":
-                    dp = c.decay_of(p)
-                    b, cc = dp.outs
-                    L_ = p.bw_l if p.bw_l is not None else min(dp.get_l_list())
-                    e(f"  const R q_{tag} = R(rel_p<double>({m}, {dmass(b, True)}, {dmass(cc, True)}));")
-                    co = bprime_coeff(L_)
-                    z = f"(q_{tag} * q_{tag} * {_lit(p.d * p.d)})"
-                    poly = _lit(co[0])
-                    for cc_ in co[1:]:
-                        poly = f"fma({poly}, {z}, {_lit(cc_)})"
-                    qp = "*".join([f"q_{tag}"] * (2 * L_ + 1))
-                    e(f"  const R qp_{tag} = {cst(f'{p}.useq')} != R(0) ? ({qp}) : R(1);")
-                    e(f"  const R y_{tag} = {cst(f'{p}.K')} * qp_{tag} / (R({m}) * ({poly}));")
-                else:
-                    e(f"  const R y_{tag} = {cst(f'{p}.y')};")
-                e(f"  const R xr_{tag} = R(xx_{tag});")
-                e(f"  const R s_{tag} = xr_{tag} * xr_{tag} + y_{tag} * y_{tag};")
-                e(f"  const cpx<R> bw_{tag} = cmk<R>(xr_{tag} / s_{tag}, y_{tag} / s_{tag});")
-            # chain lineshape product
-            if bw_names:
-                e(f"  cpx<R> BW_c{ci} = {bw_names[0]};")
-                for nm in bw_names[1:]:
-                    e(f"  BW_c{ci} = cmul(BW_c{ci}, {nm});")
-            else:
-                e(f"  const cpx<R> BW_c{ci} = cmk<R>(R(1), R(0));")
-
-            # angular columns F^ang_k[out]
-            cols = self.chain_columns[ci]
             parts = [c.top] + c.inner + list(c.outs)
             cgs = [d.cg() for d in c]
-            terms = {}  # (k, out) -> list of (coef, product expr)
-            prods = {}
+            rows = []
             for hel in itertools.product(*[p.spins for p in parts]):
                 hmap = dict(zip(parts, hel))
-                ok = True
                 facs = []
+                ok = True
                 for vi, d in enumerate(c):
                     a, (b, cc) = d.core, d.outs
                     dl = hmap[b] - hmap[cc]
@@ -287,144 +157,397 @@ class ModelCode:
                         ok = False
                         break
                     j2 = two(a.J)
-                    facs.append(f"D_c{ci}v{vi}_{two(hmap[a]) + j2}_{two(dl) + j2}")
+                    facs.append((vi, two(hmap[a]) + j2, two(dl) + j2,
+                                 b.spins.index(hmap[b]), cc.spins.index(hmap[cc])))
                 if not ok:
                     continue
-                # pre-alignment output helicities (chain's own final helicities)
                 pre_out = (hmap[c.top],) + tuple(hmap[o] for o in self.group.outs)
-                for kk, k in enumerate(cols):
+                coefs = {}
+                for k in self.chain_columns[ci]:
                     lsi = self.columns[k][1]
-                    coef = 1.0
-                    for vi, d in enumerate(c):
-                        a, (b, cc) = d.core, d.outs
-                        ib = b.spins.index(hmap[b])
-                        ic = cc.spins.index(hmap[cc])
-                        coef *= cgs[vi][lsi[vi], ib, ic]
-                    if coef == 0.0:
-                        continue
-                    key = tuple(facs)
-                    if key not in prods:
-                        pn = f"P_c{ci}_{len(prods)}"
-                        prods[key] = pn
-                        if len(facs) == 1:
-                            e(f"  const cpx<R> {pn} = {facs[0]};")
+                    cf = 1.0
+                    for (vi, _, _, ib, ic) in facs:
+                        cf *= cgs[vi][lsi[vi], ib, ic]
+                    if cf != 0.0:
+                        coefs[k] = cf
+                if coefs:
+                    rows.append((tuple(facs), pre_out, coefs))
+            self.chain_assign.append(rows)
+        # structurally non-zero (column, output) pairs after alignment
+        self._fset = set()
+        for ci in range(len(self.group)):
+            aligned = self._aligned_finals(ci)
+            for facs, pre, coefs in self.chain_assign[ci]:
+                outs = [pre]
+                for oi in aligned:
+                    new = []
+                    for o in outs:
+                        for l2 in self.outs[oi].spins:
+                            t = list(o)
+                            t[oi] = l2
+                            new.append(tuple(t))
+                    outs = new
+                for k in coefs:
+                    for o in outs:
+                        self._fset.add((k, self.out_index[o]))
+        self.nf = len(self._fset)
+
+    # ------------------------------------------------------------ helpers
+    def _cst(self, name):
+        return f"R(C.v[{self.consts.index[name]}])"
+
+    def _cpx(self, base):
+        return f"cmk<R>({self._cst(base + '.re')}, {self._cst(base + '.im')})"
+
+    def _aligned_finals(self, ci):
+        cf = self.plan.chains[ci]
+        return [self.group.outs.index(o) + 1 for o in self.group.outs if o in cf["aligned"]]
+
+    @staticmethod
+    def _d_name(ci, vi, ia, idl):
+        return f"D_c{ci}v{vi}_{ia}_{idl}"
+
+    @staticmethod
+    def _pre_name(ci, po, pfx):
+        return f"{pfx}_c{ci}_" + "_".join(str(two(x) + 8) for x in po)
+
+    def _scale_k(self, ci, k):
+        c = self.group[ci]
+        lsi = self.columns[k][1]
+        sc = []
+        for vi, d in enumerate(c):
+            if d.has_barrier_factor:
+                l = d.get_ls_list()[lsi[vi]][0]
+                sc.append(f"bf_c{ci}v{vi}_{l}")
+        return " * ".join(sc) if sc else "R(1)"
+
+    def _first_chain(self, p):
+        for ci, c in enumerate(self.group):
+            if p in c.inner:
+                return ci
+        return -1
+
+    def _emit_loads(self, e):
+        for f in self.mass_fields:
+            e(f"  const double xm{f} = __ldg(XM + (long long){self.mass_slot[f]} * ld + i);")
+        for f in self.angle_fields:
+            e(f"  const R xa{f} = __ldg(XA + (long long){self.angle_slot[f]} * ld + i);")
+
+    def _emit_chain_common(self, e, ci):
+        """Masses, q^2, barrier factors, D elements, alignment D and
+        lineshapes of chain ci (names prefixed by the chain)."""
+        c = self.group[ci]
+        cf = self.plan.chains[ci]
+        cst = self._cst
+
+        def dmass(p):
+            if p in c.inner:
+                return f"xm{cf['mass'][p]}"
+            return repr(float(p.mass))
+
+        for vi, d in enumerate(c):
+            a, (b, cc) = d.core, d.outs
+            tag = f"c{ci}v{vi}"
+            fa = cf["decays"][vi]
+            if d.has_barrier_factor:
+                e(f"  const R q2_{tag} = R(rel_p2<double>({dmass(a)}, {dmass(b)}, {dmass(cc)}));")
+                for l in sorted(set(d.get_l_list())):
+                    if d.has_ql:
+                        if l == 0:
+                            ql = "R(1)"
+                        elif l % 2 == 0:
+                            ql = "*".join([f"q2_{tag}"] * (l // 2))
                         else:
-                            expr = facs[0]
-                            for fnm in facs[1:]:
-                                expr = f"cmul({expr}, {fnm})"
-                            e(f"  const cpx<R> {pn} = {expr};")
-                    terms.setdefault((k, pre_out), []).append((coef, prods[key]))
-            # emit pre-alignment columns
-            pre_outs = sorted({po for (_, po) in terms}, key=lambda t: [float(x) for x in t])
-            for k in cols:
-                for po in pre_outs:
-                    lst = terms.get((k, po))
-                    nm = self._pre_name(ci, k, po)
-                    if not lst:
-                        continue
-                    e(f"  cpx<R> {nm} = cmk<R>(R(0), R(0));")
-                    for coef, pn in lst:
-                        e(f"  cfma({nm}, {_lit(coef)}, {pn});")
-            # alignment: contract each aligned final's helicity index
-            aligned = [o for o in self.group.outs if o in cf["aligned"]]
-            cur = {(k, po): self._pre_name(ci, k, po) for k in cols for po in pre_outs
-                   if (k, po) in terms}
-            for o in aligned:
-                oi = 1 + self.group.outs.index(o)
-                tag = f"c{ci}al{oi - 1}"
-                j2 = two(o.J)
-                new = {}
-                for k in cols:
-                    for out in self.out_hel:
-                        # out[oi] is the aligned helicity; sum over source helicity
-                        srcs = []
-                        for l1 in o.spins:
-                            src = list(out)
-                            src[oi] = l1
-                            src = tuple(src)
-                            if (k, src) in cur:
-                                srcs.append((cur[(k, src)], f"Dal_{tag}_{two(l1) + j2}_{two(out[oi]) + j2}"))
-                        if not srcs:
-                            continue
-                        nm = f"Fa_c{ci}_{oi}_{k}_{self.out_hel.index(out)}"
-                        e(f"  cpx<R> {nm} = cmk<R>(R(0), R(0));")
-                        for s_, dn in srcs:
-                            e(f"  cfmac({nm}, {s_}, {dn});")
-                        new[(k, out)] = nm
-                cur = new
-            # final per-column angular values F[k][out] and per-event scale
-            for k in cols:
-                lsi = self.columns[k][1]
-                sc = []
-                for vi, d in enumerate(c):
-                    if d.has_barrier_factor:
-                        l = d.get_ls_list()[lsi[vi]][0]
-                        sc.append(f"bf_c{ci}v{vi}_{l}")
-                scale = " * ".join(sc) if sc else "R(1)"
-                e(f"  const cpx<R> S{k} = cscale(BW_c{ci}, {scale});")
-                # e_k = c_k * scale_k
-                e(f"  const cpx<R> E{k} = cmul(cmk<R>({cst(f'c{k}.re')}, {cst(f'c{k}.im')}), S{k});")
-                for oj, out in enumerate(self.out_hel):
-                    nm = cur.get((k, out))
-                    if nm is not None:
-                        e(f"  const cpx<R> F{k}_{oj} = {nm};")
-                        self._fset.add((k, oj))
-            self._cur_chain = None
-        # --- columns variant: F[k][o] = S_k * F^ang_k[o]
-        cols_body = list(body)
-        for k in range(self.ncol):
-            for oj in range(self.nout):
-                if (k, oj) in self._fset:
-                    cols_body.append(f"  F[{k * self.nout + oj}] = cmul(S{k}, F{k}_{oj});")
+                            ql = "*".join([f"psqrt(q2_{tag})"] + [f"q2_{tag}"] * (l // 2))
+                    else:
+                        ql = "R(1)"
+                    if d.has_bprime:
+                        co = bprime_coeff(l)
+                        z = f"(q2_{tag} * {_lit(d.d * d.d)})"
+                        poly = _lit(co[0])
+                        for cc_ in co[1:]:
+                            poly = f"fma({poly}, {z}, {_lit(cc_)})"
+                        e(f"  R bp_{tag}_{l} = {cst(f'{d}.Pz0_{l}')} / ({poly});")
+                        e(f"  bp_{tag}_{l} = bp_{tag}_{l} > R(0) ? bp_{tag}_{l} : R(1);")
+                        bf = f"({ql}) * psqrt(bp_{tag}_{l})"
+                    else:
+                        bf = ql
+                    if d.barrier_factor_norm:
+                        bf = f"({bf}) * {cst(f'{d}.norm_{l}')}"
+                    e(f"  const R bf_{tag}_{l} = {bf};")
+            # D*^{Ja}_{la, lb-lc}(alpha, beta, 0); indices are 2m + 2J
+            j2 = two(a.J)
+            need = set()
+            for la in a.spins:
+                for lb in b.spins:
+                    for lc in cc.spins:
+                        dl = lb - lc
+                        if abs(dl) <= a.J + 1e-9:
+                            need.add((two(la) + j2, two(dl) + j2))
+            e(f"  R sp_{tag}[{j2 + 1}], cp_{tag}[{j2 + 1}];")
+            e(f"  half_angle_sc_powers<R, {j2}>(xa{fa['beta']}, sp_{tag}, cp_{tag});")
+            need_alpha = any(i1 != j2 for i1, _ in need)
+            if need_alpha:
+                e(f"  cpx<R> ea_{tag}[{2 * j2 + 1}];")
+                e(f"  half_angle_powers<R, {j2}>(xa{fa['alpha']}, ea_{tag});")
+            w = small_d_weight(j2)
+            for i1, i2 in sorted(need):
+                k1, k2 = i1 // 2, i2 // 2
+                terms = [f"{_lit(w[l][k1][k2])} * sp_{tag}[{l}] * cp_{tag}[{j2 - l}]"
+                         for l in range(j2 + 1) if w[l][k1][k2] != 0]
+                dexpr = " + ".join(terms) if terms else "R(0)"
+                nm = self._d_name(ci, vi, i1, i2)
+                if need_alpha and i1 != j2:
+                    e(f"  const cpx<R> {nm} = cscale(ea_{tag}[{i1}], {dexpr});")
                 else:
-                    cols_body.append(f"  F[{k * self.nout + oj}] = cmk<R>(R(0), R(0));")
-        # --- amplitude, |A|^2
+                    e(f"  const cpx<R> {nm} = cmk<R>({dexpr}, R(0));")
+        for o, (fa_, fb_, fg_) in cf["aligned"].items():
+            oi = self.group.outs.index(o)
+            tag = f"c{ci}al{oi}"
+            j2 = two(o.J)
+            e(f"  R sp_{tag}[{j2 + 1}], cp_{tag}[{j2 + 1}];")
+            e(f"  half_angle_sc_powers<R, {j2}>(xa{fb_}, sp_{tag}, cp_{tag});")
+            e(f"  cpx<R> ea_{tag}[{2 * j2 + 1}], eg_{tag}[{2 * j2 + 1}];")
+            e(f"  half_angle_powers<R, {j2}>(xa{fa_}, ea_{tag});")
+            e(f"  half_angle_powers<R, {j2}>(xa{fg_}, eg_{tag});")
+            w = small_d_weight(j2)
+            for l1 in o.spins:
+                for l2 in o.spins:
+                    n1, n2 = two(l1) + j2, two(l2) + j2
+                    terms = [f"{_lit(w[l][n1 // 2][n2 // 2])} * sp_{tag}[{l}] * cp_{tag}[{j2 - l}]"
+                             for l in range(j2 + 1) if w[l][n1 // 2][n2 // 2] != 0]
+                    dexpr = " + ".join(terms) if terms else "R(0)"
+                    e(f"  const cpx<R> Dal_{tag}_{n1}_{n2} = cscale(cmul(ea_{tag}[{n1}], eg_{tag}[{n2}]), {dexpr});")
+        bw_names = []
+        for p in c.inner:
+            kind = p.lineshape_kind()
+            if kind == "one":
+                continue
+            tag = f"c{ci}r{c.inner.index(p)}"
+            m = f"xm{cf['mass'][p]}"
+            bw_names.append(f"bw_{tag}")
+            e(f"  const R xr_{tag} = R(C.v[{self.consts.index[f'{p}.m0sq']}] - {m} * {m});")
+            if kind == "BWR":
+                dp = c.decay_of(p)
+                b, cc = dp.outs
+                L_ = p.bw_l if p.bw_l is not None else min(dp.get_l_list())
+                e(f"  const R q_{tag} = R(rel_p<double>({m}, {dmass(b)}, {dmass(cc)}));")
+                co = bprime_coeff(L_)
+                z = f"(q_{tag} * q_{tag} * {_lit(p.d * p.d)})"
+                poly = _lit(co[0])
+                for cc_ in co[1:]:
+                    poly = f"fma({poly}, {z}, {_lit(cc_)})"
+                qp = "*".join([f"q_{tag}"] * (2 * L_ + 1))
+                e(f"  const R qp_{tag} = {cst(f'{p}.useq')} != R(0) ? ({qp}) : R(1);")
+                e(f"  const R y_{tag} = {cst(f'{p}.K')} * qp_{tag} / (R({m}) * ({poly}));")
+            else:
+                e(f"  const R y_{tag} = {cst(f'{p}.y')};")
+            e(f"  const R s_{tag} = xr_{tag} * xr_{tag} + y_{tag} * y_{tag};")
+            e(f"  const cpx<R> bw_{tag} = cmk<R>(xr_{tag} / s_{tag}, y_{tag} / s_{tag});")
+        if bw_names:
+            e(f"  cpx<R> BW_c{ci} = {bw_names[0]};")
+            for nm in bw_names[1:]:
+                e(f"  BW_c{ci} = cmul(BW_c{ci}, {nm});")
+        else:
+            e(f"  const cpx<R> BW_c{ci} = cmk<R>(R(1), R(0));")
+
+    def _emit_align_forward(self, e, ci, cur, pfx):
+        """Contract each aligned final's helicity with D*(aligned angles)."""
+        for oi in self._aligned_finals(ci):
+            o = self.outs[oi]
+            j2 = two(o.J)
+            tag = f"c{ci}al{oi - 1}"
+            targets = set()
+            for po in cur:
+                for l2 in o.spins:
+                    t = list(po)
+                    t[oi] = l2
+                    targets.add(tuple(t))
+            new = {}
+            for to in sorted(targets, key=_key):
+                nm = self._pre_name(ci, to, f"{pfx}{oi}")
+                e(f"  cpx<R> {nm} = cmk<R>(R(0), R(0));")
+                for l1 in o.spins:
+                    s_ = list(to)
+                    s_[oi] = l1
+                    s_ = tuple(s_)
+                    if s_ in cur:
+                        e(f"  cfmac({nm}, {cur[s_]}, Dal_{tag}_{two(l1) + j2}_{two(to[oi]) + j2});")
+                new[to] = nm
+            cur = new
+        return cur
+
+    # ------------------------------------------------------------ forward
+    def _emit_forward(self, e):
         for oj in range(self.nout):
             e(f"  cpx<R> A{oj} = cmk<R>(R(0), R(0));")
-            for k in range(self.ncol):
-                if (k, oj) in self._fset:
-                    e(f"  cfmac(A{oj}, E{k}, F{k}_{oj});")
-        e("  R fsum = R(0);")
-        for oj in range(self.nout):
-            e(f"  fsum += cabs2(A{oj});")
-        e("  *fout = double(fsum);")
-        # --- sensitivities: G_k = S_k * sum_out conj(A_out) F_k[out]
-        for k in range(self.ncol):
-            e(f"  cpx<R> H{k} = cmk<R>(R(0), R(0));")
-            for oj in range(self.nout):
-                if (k, oj) in self._fset:
-                    e(f"  {{ const cpx<R> t = cmulc(F{k}_{oj}, A{oj}); H{k} = cadd(H{k}, t); }}")
-            e(f"  G[{k}] = cmul(S{k}, H{k});")
-        # --- shape derivatives for each resonance with a lineshape
+        for ci, c in enumerate(self.group):
+            e(f"  {{ // chain {ci}: {c}")
+            self._emit_chain_common(e, ci)
+            hnames = {}
+            for vi, d in enumerate(c):
+                b, cc = d.outs
+                cg = d.cg()
+                ls = d.get_ls_list()
+                for ib in range(len(b.spins)):
+                    for ic in range(len(cc.spins)):
+                        terms = [(i, cg[i, ib, ic]) for i in range(len(ls)) if cg[i, ib, ic] != 0]
+                        if not terms:
+                            continue
+                        nm = f"H_c{ci}v{vi}_{ib}_{ic}"
+                        hnames[(vi, ib, ic)] = nm
+                        e(f"  cpx<R> {nm} = cmk<R>(R(0), R(0));")
+                        for i, cgv in terms:
+                            l = ls[i][0]
+                            bfv = f"bf_c{ci}v{vi}_{l} * " if d.has_barrier_factor else ""
+                            e(f"  cfma({nm}, {bfv}{_lit(cgv)}, {self._cpx(f'{d}.g{i}')});")
+            pre = {}
+            for facs, po, coefs in self.chain_assign[ci]:
+                if any((vi, ib, ic) not in hnames for (vi, _, _, ib, ic) in facs):
+                    continue
+                vs = [f"cmul({hnames[(vi, ib, ic)]}, {self._d_name(ci, vi, ia, idl)})"
+                      for (vi, ia, idl, ib, ic) in facs]
+                nm = pre.get(po)
+                if nm is None:
+                    nm = self._pre_name(ci, po, "Ap")
+                    pre[po] = nm
+                    e(f"  cpx<R> {nm} = cmk<R>(R(0), R(0));")
+                if len(vs) == 1:
+                    e(f"  {nm} = cadd({nm}, {vs[0]});")
+                else:
+                    prod = vs[0]
+                    for v in vs[1:-1]:
+                        prod = f"cmul({prod}, {v})"
+                    e(f"  cfmac({nm}, {prod}, {vs[-1]});")
+            cur = self._emit_align_forward(e, ci, pre, "Aa")
+            e(f"  const cpx<R> E_c{ci} = cmul({self._cpx(f't{ci}')}, BW_c{ci});")
+            for o, nm in cur.items():
+                e(f"  cfmac(A{self.out_index[o]}, E_c{ci}, {nm});")
+            e("  }")
+
+    # ------------------------------------------------------------ adjoint
+    def _emit_adjoint(self, e):
         for si, p in enumerate(self.shape_res):
-            # S_R = sum over columns of chains containing p of e_k H_k
-            e(f"  {{ cpx<R> SR = cmk<R>(R(0), R(0));")
-            tag = None
-            for ci, c in enumerate(self.group):
-                if p in c.inner:
+            e(f"  cpx<R> SR{si} = cmk<R>(R(0), R(0)), dm{si} = SR{si}, dg{si} = SR{si};")
+        for ci, c in enumerate(self.group):
+            e(f"  {{ // chain {ci}: {c}")
+            self._emit_chain_common(e, ci)
+            cur = {o: f"Ab[{j}]" for o, j in self.out_index.items()}
+            for oi in reversed(self._aligned_finals(ci)):
+                o = self.outs[oi]
+                j2 = two(o.J)
+                tag = f"c{ci}al{oi - 1}"
+                keys = set()
+                for to in cur:
+                    for l1 in o.spins:
+                        t = list(to)
+                        t[oi] = l1
+                        keys.add(tuple(t))
+                new = {}
+                for po in sorted(keys, key=_key):
+                    nm = self._pre_name(ci, po, f"Bb{oi}")
+                    e(f"  cpx<R> {nm} = cmk<R>(R(0), R(0));")
+                    for l2 in o.spins:
+                        t = list(po)
+                        t[oi] = l2
+                        t = tuple(t)
+                        if t in cur:
+                            e(f"  cfmac({nm}, {cur[t]}, Dal_{tag}_{two(po[oi]) + j2}_{two(l2) + j2});")
+                    new[po] = nm
+                cur = new
+            cols = self.chain_columns[ci]
+            for k in cols:
+                e(f"  cpx<R> Gk{k} = cmk<R>(R(0), R(0));")
+            for facs, po, coefs in self.chain_assign[ci]:
+                if po not in cur:
+                    continue
+                ds = [self._d_name(ci, vi, ia, idl) for (vi, ia, idl, _, _) in facs]
+                prod = ds[0]
+                for dn in ds[1:]:
+                    prod = f"cmul({prod}, {dn})"
+                e(f"  {{ const cpx<R> rr = cmul({prod}, {cur[po]});")
+                for k, cfv in coefs.items():
+                    e(f"    cfma(Gk{k}, {_lit(cfv)}, rr);")
+                e("  }")
+            for k in cols:
+                e(f"  {{ const cpx<R> g = cmul(cscale(BW_c{ci}, {self._scale_k(ci, k)}), Gk{k});")
+                e(f"    accg[{2 * k}] += double(g.re); accg[{2 * k + 1}] += double(g.im);")
+                for si, p in enumerate(self.shape_res):
+                    if p in c.inner:
+                        e(f"    cfmac(SR{si}, {self._cpx(f'c{k}')}, g);")
+                e("  }")
+            for si, p in enumerate(self.shape_res):
+                if p in c.inner and self._first_chain(p) == ci:
                     tag = f"c{ci}r{c.inner.index(p)}"
-                    for k in self.chain_columns[ci]:
-                        e(f"    cfmac(SR, E{k}, H{k});")
-            # dlnBW/dm0 = -BW (2 m0 - i y kappa_m); dlnBW/dg0 = i BW y / g0
-            e(f"    const R m0 = psqrt({cst(f'{p}.m0sq')});")
-            e(f"    const cpx<R> dm = cmul(bw_{tag}, cmk<R>(R(-2) * m0, y_{tag} * {cst(f'{p}.kappa_m')}));")
-            e(f"    const cpx<R> dg = cmul(bw_{tag}, cmk<R>(R(0), y_{tag} * {cst(f'{p}.inv_g0')}));")
-            e(f"    const cpx<R> a1 = cmul(SR, dm), a2 = cmul(SR, dg);")
-            e(f"    dshape[{2 * si}] = 2.0 * double(a1.re); dshape[{2 * si + 1}] = 2.0 * double(a2.re); }}")
-        L.append("\n".join(body))
+                    e(f"  {{ const R m0 = psqrt({self._cst(f'{p}.m0sq')});")
+                    e(f"    dm{si} = cmul(bw_{tag}, cmk<R>(R(-2) * m0, y_{tag} * {self._cst(f'{p}.kappa_m')}));")
+                    e(f"    dg{si} = cmul(bw_{tag}, cmk<R>(R(0), y_{tag} * {self._cst(f'{p}.inv_g0')})); }}")
+            e("  }")
+        for si, p in enumerate(self.shape_res):
+            e(f"  accs[{2 * si}] += 2.0 * double(cmul(SR{si}, dm{si}).re);")
+            e(f"  accs[{2 * si + 1}] += 2.0 * double(cmul(SR{si}, dg{si}).re);")
+
+    # ------------------------------------------------------------ columns
+    def _emit_columns(self, e):
+        for j in range(self.ncol * self.nout):
+            e(f"  F[{j}] = cmk<R>(R(0), R(0));")
+        for ci, c in enumerate(self.group):
+            e(f"  {{ // chain {ci}: {c}")
+            self._emit_chain_common(e, ci)
+            for k in self.chain_columns[ci]:
+                e("  {")
+                pre = {}
+                for facs, po, coefs in self.chain_assign[ci]:
+                    if k not in coefs:
+                        continue
+                    ds = [self._d_name(ci, vi, ia, idl) for (vi, ia, idl, _, _) in facs]
+                    prod = ds[0]
+                    for dn in ds[1:]:
+                        prod = f"cmul({prod}, {dn})"
+                    nm = pre.get(po)
+                    if nm is None:
+                        nm = self._pre_name(ci, po, "Fp")
+                        pre[po] = nm
+                        e(f"  cpx<R> {nm} = cmk<R>(R(0), R(0));")
+                    e(f"  cfma({nm}, {_lit(coefs[k])}, {prod});")
+                cur = self._emit_align_forward(e, ci, pre, "Fa")
+                e(f"  const cpx<R> S = cscale(BW_c{ci}, {self._scale_k(ci, k)});")
+                for o, nm in cur.items():
+                    e(f"  F[{k * self.nout + self.out_index[o]}] = cmul(S, {nm});")
+                e("  }")
+            e("  }")
+
+    # ------------------------------------------------------------ emission
+    def source(self):
+        L = [_HEADER.format(ncol=self.ncol, nout=self.nout, nshape=self.nshape, nacc=self.nacc,
+                            nconst=max(len(self.consts), 1))]
+        sig = ("    const Consts& C, const R* __restrict__ XA, const double* __restrict__ XM,\n"
+               "    long long ld, long long i")
+        body = []
+        self._emit_loads(body.append)
+        self._emit_forward(body.append)
+        L.append(f"template <typename R>\n__device__ __forceinline__ void model_amp(\n{sig},\n"
+                 "    cpx<R>* __restrict__ A) {")
+        L += body
+        L += [f"  A[{oj}] = A{oj};" for oj in range(self.nout)]
         L.append("}\n")
-        L.append("template <typename R>\n__device__ __forceinline__ void model_columns(\n"
-                 "    const Consts& C, const R* __restrict__ XA, const double* __restrict__ XM,\n"
-                 "    long long ld, long long i, cpx<R>* __restrict__ F) {")
-        L.append("\n".join(cols_body))
+        body = []
+        self._emit_loads(body.append)
+        self._emit_adjoint(body.append)
+        L.append(f"template <typename R>\n__device__ __forceinline__ void model_adj(\n{sig},\n"
+                 "    const cpx<R>* __restrict__ Ab, double* __restrict__ accg,\n"
+                 "    double* __restrict__ accs) {")
+        L += body
+        L.append("}\n")
+        body = []
+        self._emit_loads(body.append)
+        self._emit_columns(body.append)
+        L.append(f"template <typename R>\n__device__ __forceinline__ void model_columns(\n{sig},\n"
+                 "    cpx<R>* __restrict__ F) {")
+        L += body
         L.append("}\n")
         fl = sorted(self._fset)
-        self.nf = len(fl)
         L.append(f"#define PWA_NF {self.nf}")
         L.append("__device__ constexpr int pwa_fk[PWA_NF] = {" + ", ".join(str(k) for k, _ in fl) + "};")
         L.append("__device__ constexpr int pwa_fo[PWA_NF] = {" + ", ".join(str(o) for _, o in fl) + "};")
         return "\n".join(L)
-
-    def _pre_name(self, ci, k, po):
-        tag = "_".join(str(two(x) + 8) for x in po)
-        return f"Fp_c{ci}_{k}_{tag}"

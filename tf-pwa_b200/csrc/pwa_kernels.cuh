@@ -1,4 +1,5 @@
-// Kernels around the generated ``model_event``/``model_columns`` functions.
+// Kernels around the generated ``model_amp`` / ``model_adj`` /
+// ``model_columns`` functions.
 //
 // Compiled together with the model code by NVRTC (sm_100a).  Events live in
 // HBM as structure-of-arrays columns: XM[n_mass][ld] (FP64 invariant
@@ -40,10 +41,11 @@ __device__ __forceinline__ void eval_body(const Consts& C, const R* __restrict__
   for (int j = 0; j < PWA_NACC; ++j) acc[j] = 0.0;
   for (long long i = beg + (long long)b * PWA_TPB + threadIdx.x; i < end;
        i += (long long)nb * PWA_TPB) {
-    double f;
-    cpx<R> G[PWA_NCOL];
-    double ds[PWA_NSHAPE > 0 ? PWA_NSHAPE : 1];
-    model_event<R>(C, XA, XM, ld, i, &f, G, ds);
+    cpx<R> A[PWA_NOUT];
+    model_amp<R>(C, XA, XM, ld, i, A);
+    double f = 0.0;
+#pragma unroll
+    for (int o = 0; o < PWA_NOUT; ++o) f += double(cabs2(A[o]));
     const double w = __ldg(W + i);
     double fac;
     if (is_data) {
@@ -55,14 +57,10 @@ __device__ __forceinline__ void eval_body(const Consts& C, const R* __restrict__
       acc[0] = fma(w, f, acc[0]);
       fac = w;
     }
+    cpx<R> Ab[PWA_NOUT];
 #pragma unroll
-    for (int k = 0; k < PWA_NCOL; ++k) {
-      acc[1 + 2 * k] = fma(fac, double(G[k].re), acc[1 + 2 * k]);
-      acc[2 + 2 * k] = fma(fac, double(G[k].im), acc[2 + 2 * k]);
-    }
-#pragma unroll
-    for (int s = 0; s < PWA_NSHAPE; ++s)
-      acc[1 + 2 * PWA_NCOL + s] = fma(fac, ds[s], acc[1 + 2 * PWA_NCOL + s]);
+    for (int o = 0; o < PWA_NOUT; ++o) Ab[o] = cmk<R>(R(fac * double(A[o].re)), R(-fac * double(A[o].im)));
+    model_adj<R>(C, XA, XM, ld, i, Ab, acc + 1, acc + 1 + 2 * PWA_NCOL);
   }
   __shared__ double red[PWA_TPB / 32][PWA_NACC];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -80,14 +78,17 @@ __device__ __forceinline__ void eval_body(const Consts& C, const R* __restrict__
   }
 }
 
-extern "C" __global__ void __launch_bounds__(PWA_TPB)
+#ifndef PWA_EVAL_MINB
+#define PWA_EVAL_MINB 3
+#endif
+extern "C" __global__ void __launch_bounds__(PWA_TPB, PWA_EVAL_MINB)
     pwa_eval_f64(const Consts C, const double* __restrict__ XA, const double* __restrict__ XM,
                  const double* __restrict__ W, long long n_data, long long n_all, long long ld,
                  int blocks_data, double* __restrict__ partials) {
   eval_body<double>(C, XA, XM, W, n_data, n_all, ld, blocks_data, partials);
 }
 
-extern "C" __global__ void __launch_bounds__(PWA_TPB)
+extern "C" __global__ void __launch_bounds__(PWA_TPB, PWA_EVAL_MINB)
     pwa_eval_f32(const Consts C, const float* __restrict__ XA, const double* __restrict__ XM,
                  const double* __restrict__ W, long long n_data, long long n_all, long long ld,
                  int blocks_data, double* __restrict__ partials) {
@@ -116,10 +117,11 @@ __device__ __forceinline__ void pdf_body(const Consts& C, const R* __restrict__ 
                                          long long end, long long ld, double* __restrict__ out) {
   for (long long i = beg + (long long)blockIdx.x * blockDim.x + threadIdx.x; i < end;
        i += (long long)gridDim.x * blockDim.x) {
-    double f;
-    cpx<R> G[PWA_NCOL];
-    double ds[PWA_NSHAPE > 0 ? PWA_NSHAPE : 1];
-    model_event<R>(C, XA, XM, ld, i, &f, G, ds);
+    cpx<R> A[PWA_NOUT];
+    model_amp<R>(C, XA, XM, ld, i, A);
+    double f = 0.0;
+#pragma unroll
+    for (int o = 0; o < PWA_NOUT; ++o) f += double(cabs2(A[o]));
     out[i - beg] = f;
   }
 }

@@ -54,7 +54,7 @@ struct pwa_plan {
   double* wcache = nullptr;
   long long ntiles = 0, ntiles_cap = 0, fcache_n = 0;
   int cached_blocks = 0, cached_blocks_direct = 0;
-  int cached_variant = 0;  // 0: shared-memory ring (bulk copies), 1: direct loads
+  int cached_variant = 1;  // 0: shared-memory ring (bulk copies), 1: direct loads
   size_t cached_smem = 0;
   unsigned int* ticket = nullptr;  // [0] finished-block count, [1] error flag
   double* h_map = nullptr;         // mapped pinned result of the cached kernel

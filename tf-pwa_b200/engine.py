@@ -303,6 +303,17 @@ class Engine:
         self._cv = cv
         C[0:2 * c.ncol:2] = self._ck.real
         C[1:2 * c.ncol:2] = self._ck.imag
+        for d in c.vertices:
+            for i in range(len(d.get_ls_list())):
+                z = cv.get(f"{d.params_head}_g_ls_{i}")
+                if z is None:
+                    z = self.complex_val(vals, f"{d.params_head}_g_ls_{i}")
+                C[idx[f"{d}.g{i}.re"]] = z.real
+                C[idx[f"{d}.g{i}.im"]] = z.imag
+        for ci, ch in enumerate(self.group):
+            z = cv[ch.params_head + "_total_0"]
+            C[idx[f"t{ci}.re"]] = z.real
+            C[idx[f"t{ci}.im"]] = z.imag
         for p, kind in c.res:
             if kind == "one":
                 continue
