@@ -191,6 +191,19 @@ class ModelCode:
                     for o in outs:
                         self._fset.add((k, self.out_index[o]))
         self.nf = len(self._fset)
+        # stash slots: one (sin, cos) pair per half angle of every chain
+        self._slot = {}
+        for ci, c in enumerate(self.group):
+            cf = self.plan.chains[ci]
+            for vi, d in enumerate(c):
+                self._slot[(ci, f"c{ci}v{vi}b")] = len(self._slot)
+                self._slot[(ci, f"c{ci}v{vi}a")] = len(self._slot)
+            for o in cf["aligned"]:
+                oi = self.group.outs.index(o)
+                for a in "bag":
+                    self._slot[(ci, f"c{ci}al{oi}{a}")] = len(self._slot)
+        self.nstash = 2 * len(self._slot)
+        self._mode = "plain"
 
     # ------------------------------------------------------------ helpers
     def _cst(self, name):
@@ -232,6 +245,20 @@ class ModelCode:
             e(f"  const double xm{f} = __ldg(XM + (long long){self.mass_slot[f]} * ld + i);")
         for f in self.angle_fields:
             e(f"  const R xa{f} = __ldg(XA + (long long){self.angle_slot[f]} * ld + i);")
+
+    def _trig(self, e, ci, key, angle):
+        """sin/cos of half an angle: computed (and stashed in the forward
+        pass) or read back from the stash (adjoint pass)."""
+        nm = f"{key}"
+        slot = self._slot[(ci, key)]
+        if self._mode == "load":
+            e(f"  const R s_{nm} = st[{2 * slot} * PWA_TPB], c_{nm} = st[{2 * slot + 1} * PWA_TPB];")
+        else:
+            e(f"  R s_{nm}, c_{nm};")
+            e(f"  psincos(R(0.5) * {angle}, &s_{nm}, &c_{nm});")
+            if self._mode == "store":
+                e(f"  if (STASH) {{ st[{2 * slot} * PWA_TPB] = s_{nm}; st[{2 * slot + 1} * PWA_TPB] = c_{nm}; }}")
+        return f"s_{nm}", f"c_{nm}"
 
     def _emit_chain_common(self, e, ci):
         """Masses, q^2, barrier factors, D elements, alignment D and
@@ -285,11 +312,13 @@ class ModelCode:
                         if abs(dl) <= a.J + 1e-9:
                             need.add((two(la) + j2, two(dl) + j2))
             e(f"  R sp_{tag}[{j2 + 1}], cp_{tag}[{j2 + 1}];")
-            e(f"  half_angle_sc_powers<R, {j2}>(xa{fa['beta']}, sp_{tag}, cp_{tag});")
+            sb, cb = self._trig(e, ci, f"{tag}b", f"xa{fa['beta']}")
+            e(f"  sc_powers<R, {j2}>({sb}, {cb}, sp_{tag}, cp_{tag});")
             need_alpha = any(i1 != j2 for i1, _ in need)
             if need_alpha:
                 e(f"  cpx<R> ea_{tag}[{2 * j2 + 1}];")
-                e(f"  half_angle_powers<R, {j2}>(xa{fa['alpha']}, ea_{tag});")
+                sa, ca = self._trig(e, ci, f"{tag}a", f"xa{fa['alpha']}")
+                e(f"  half_angle_powers_sc<R, {j2}>({sa}, {ca}, ea_{tag});")
             w = small_d_weight(j2)
             for i1, i2 in sorted(need):
                 k1, k2 = i1 // 2, i2 // 2
@@ -306,10 +335,13 @@ class ModelCode:
             tag = f"c{ci}al{oi}"
             j2 = two(o.J)
             e(f"  R sp_{tag}[{j2 + 1}], cp_{tag}[{j2 + 1}];")
-            e(f"  half_angle_sc_powers<R, {j2}>(xa{fb_}, sp_{tag}, cp_{tag});")
+            sb, cb = self._trig(e, ci, f"{tag}b", f"xa{fb_}")
+            e(f"  sc_powers<R, {j2}>({sb}, {cb}, sp_{tag}, cp_{tag});")
             e(f"  cpx<R> ea_{tag}[{2 * j2 + 1}], eg_{tag}[{2 * j2 + 1}];")
-            e(f"  half_angle_powers<R, {j2}>(xa{fa_}, ea_{tag});")
-            e(f"  half_angle_powers<R, {j2}>(xa{fg_}, eg_{tag});")
+            sa, ca = self._trig(e, ci, f"{tag}a", f"xa{fa_}")
+            e(f"  half_angle_powers_sc<R, {j2}>({sa}, {ca}, ea_{tag});")
+            sg, cg = self._trig(e, ci, f"{tag}g", f"xa{fg_}")
+            e(f"  half_angle_powers_sc<R, {j2}>({sg}, {cg}, eg_{tag});")
             w = small_d_weight(j2)
             for l1 in o.spins:
                 for l2 in o.spins:
@@ -521,25 +553,41 @@ class ModelCode:
     def source(self):
         L = [_HEADER.format(ncol=self.ncol, nout=self.nout, nshape=self.nshape, nacc=self.nacc,
                             nconst=max(len(self.consts), 1))]
+        # the per-thread stash of half-angle sin/cos (shared memory, stride
+        # PWA_TPB) is used when it fits a 40 KB budget at FP64
+        use = 1 if self.nstash * 128 * 8 <= 40 * 1024 else 0
+        L.append(f"#define PWA_NSTASH {max(self.nstash, 1)}\n#define PWA_USE_STASH {use}")
         sig = ("    const Consts& C, const R* __restrict__ XA, const double* __restrict__ XM,\n"
                "    long long ld, long long i")
         body = []
+        self._mode = "store"
         self._emit_loads(body.append)
         self._emit_forward(body.append)
-        L.append(f"template <typename R>\n__device__ __forceinline__ void model_amp(\n{sig},\n"
-                 "    cpx<R>* __restrict__ A) {")
+        L.append(f"template <typename R, bool STASH>\n__device__ __forceinline__ void model_amp(\n{sig},\n"
+                 "    cpx<R>* __restrict__ A, R* __restrict__ st) {")
         L += body
         L += [f"  A[{oj}] = A{oj};" for oj in range(self.nout)]
         L.append("}\n")
         body = []
+        self._mode = "load"
         self._emit_loads(body.append)
         self._emit_adjoint(body.append)
-        L.append(f"template <typename R>\n__device__ __forceinline__ void model_adj(\n{sig},\n"
+        L.append(f"template <typename R>\n__device__ __forceinline__ void model_adj_stash(\n{sig},\n"
+                 "    const cpx<R>* __restrict__ Ab, double* __restrict__ accg,\n"
+                 "    double* __restrict__ accs, const R* __restrict__ st) {")
+        L += body
+        L.append("}\n")
+        body = []
+        self._mode = "plain"
+        self._emit_loads(body.append)
+        self._emit_adjoint(body.append)
+        L.append(f"template <typename R>\n__device__ __forceinline__ void model_adj_recompute(\n{sig},\n"
                  "    const cpx<R>* __restrict__ Ab, double* __restrict__ accg,\n"
                  "    double* __restrict__ accs) {")
         L += body
         L.append("}\n")
         body = []
+        self._mode = "plain"
         self._emit_loads(body.append)
         self._emit_columns(body.append)
         L.append(f"template <typename R>\n__device__ __forceinline__ void model_columns(\n{sig},\n"

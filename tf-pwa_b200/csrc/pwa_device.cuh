@@ -100,6 +100,30 @@ __device__ __forceinline__ void half_angle_sc_powers(R b, R* sp, R* cp) {
   }
 }
 
+// The same powers from a given (sin, cos) of the half angle.
+template <typename R, int N>
+__device__ __forceinline__ void half_angle_powers_sc(R s, R c, cpx<R>* out) {
+  const cpx<R> e1 = cmk<R>(c, s);
+  out[N] = cmk<R>(R(1), R(0));
+  cpx<R> p = e1;
+#pragma unroll
+  for (int n = 1; n <= N; ++n) {
+    out[N + n] = p;
+    out[N - n] = cconj(p);
+    p = cmul(p, e1);
+  }
+}
+template <typename R, int N>
+__device__ __forceinline__ void sc_powers(R s, R c, R* sp, R* cp) {
+  sp[0] = R(1);
+  cp[0] = R(1);
+#pragma unroll
+  for (int l = 1; l <= N; ++l) {
+    sp[l] = sp[l - 1] * s;
+    cp[l] = cp[l - 1] * c;
+  }
+}
+
 // q^2 of m0 -> m1 m2 (unclamped)
 template <typename R>
 __device__ __forceinline__ R rel_p2(R m0, R m1, R m2) {

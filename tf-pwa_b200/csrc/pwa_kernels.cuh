@@ -39,10 +39,19 @@ __device__ __forceinline__ void eval_body(const Consts& C, const R* __restrict__
   double acc[PWA_NACC];
 #pragma unroll
   for (int j = 0; j < PWA_NACC; ++j) acc[j] = 0.0;
+#if PWA_USE_STASH
+  // per-thread half-angle sin/cos kept between the forward and adjoint pass
+  __shared__ R stash[PWA_NSTASH * PWA_TPB];
+  R* st = stash + threadIdx.x;
+#endif
   for (long long i = beg + (long long)b * PWA_TPB + threadIdx.x; i < end;
        i += (long long)nb * PWA_TPB) {
     cpx<R> A[PWA_NOUT];
-    model_amp<R>(C, XA, XM, ld, i, A);
+#if PWA_USE_STASH
+    model_amp<R, true>(C, XA, XM, ld, i, A, st);
+#else
+    model_amp<R, false>(C, XA, XM, ld, i, A, nullptr);
+#endif
     double f = 0.0;
 #pragma unroll
     for (int o = 0; o < PWA_NOUT; ++o) f += double(cabs2(A[o]));
@@ -60,7 +69,11 @@ __device__ __forceinline__ void eval_body(const Consts& C, const R* __restrict__
     cpx<R> Ab[PWA_NOUT];
 #pragma unroll
     for (int o = 0; o < PWA_NOUT; ++o) Ab[o] = cmk<R>(R(fac * double(A[o].re)), R(-fac * double(A[o].im)));
-    model_adj<R>(C, XA, XM, ld, i, Ab, acc + 1, acc + 1 + 2 * PWA_NCOL);
+#if PWA_USE_STASH
+    model_adj_stash<R>(C, XA, XM, ld, i, Ab, acc + 1, acc + 1 + 2 * PWA_NCOL, st);
+#else
+    model_adj_recompute<R>(C, XA, XM, ld, i, Ab, acc + 1, acc + 1 + 2 * PWA_NCOL);
+#endif
   }
   __shared__ double red[PWA_TPB / 32][PWA_NACC];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -118,7 +131,7 @@ __device__ __forceinline__ void pdf_body(const Consts& C, const R* __restrict__ 
   for (long long i = beg + (long long)blockIdx.x * blockDim.x + threadIdx.x; i < end;
        i += (long long)gridDim.x * blockDim.x) {
     cpx<R> A[PWA_NOUT];
-    model_amp<R>(C, XA, XM, ld, i, A);
+    model_amp<R, false>(C, XA, XM, ld, i, A, nullptr);
     double f = 0.0;
 #pragma unroll
     for (int o = 0; o < PWA_NOUT; ++o) f += double(cabs2(A[o]));
