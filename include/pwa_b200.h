@@ -133,6 +133,31 @@ int pwa_pieces_cached(pwa_plan* h, const double* vars, double sw, double mc_shar
 int pwa_nll_grad_cached(pwa_plan* h, const double* vars, double sw, void* stream,
                         double* out_nll, double* out_grad);
 
+/* ---- many concurrent fits (serving) ------------------------------------
+ * A pool of column-cache tiles (PWA_TPB events each) holds the data events
+ * of many fits at once; each fit owns one run of tiles.  The fits share the
+ * model, the MC sample and therefore the Gram matrix built by
+ * pwa_build_gram; each has its own couplings.  There is no counterpart in the
+ * reference (which runs one fit per process); these calls serve the
+ * reference's FCN.nll_grad for many fits in one launch. */
+int pwa_pool_reserve(pwa_plan* h, long long n_tiles);
+/* First-fit run of ceil(n_events / tile) tiles; PWA_ERR_OOM when no free run
+ * is large enough (the caller's admission control waits and retries). */
+int pwa_pool_alloc(pwa_plan* h, long long n_events, long long* first_tile, long long* n_tiles);
+int pwa_pool_free(pwa_plan* h, long long first_tile);
+/* Columns of a fit's n data events (device columns as pwa_upload_events,
+ * leading dimension ld, final weights w) into its tile run. */
+int pwa_pool_fill(pwa_plan* h, long long first_tile, const double* consts, const double* xm,
+                  const double* xa, const double* w, long long n, long long ld, void* stream);
+/* One launch for n_req pending evaluations: request r uses tiles
+ * [first_tile[r], first_tile[r] + n_tiles[r]) and the parameter vector
+ * vars[r * n_vars ...]; out[r * (3 + 2*n_train) ...] receives its piece
+ * vector (see pwa_pieces_cached) with data weight sum sw[r].  A request's
+ * result does not depend on the other requests in the launch. */
+int pwa_pieces_multi(pwa_plan* h, int n_req, const long long* first_tile, const long long* n_tiles,
+                     const double* vars, const double* sw, double mc_share, void* stream,
+                     double* out);
+
 /* Allocation-free variant of pwa_eval's device work (plain FP64 kernels),
  * with no counterpart in the reference.  For callers that cannot call
  * cudaMalloc while they run (inside a stream capture, or under a framework

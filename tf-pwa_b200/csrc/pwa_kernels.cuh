@@ -538,3 +538,101 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, 4)
     __threadfence_system();
   }
 }
+
+// ---------------------------------------------------------------------------
+// Many fits in one launch (serving).  Each fit's data-event column cache is a
+// run of tiles in a shared pool (same tile layout as above).  The launch gets
+// a work list of (request, pool tile) pairs covering the tiles of every fit
+// with a pending evaluation; each block evaluates work tiles with that
+// request's couplings and writes one row of per-tile sums.  pwa_reduce_multi
+// then sums each request's rows in the fit's own tile order, so a fit's
+// result does not depend on which other fits share the launch.
+extern "C" __global__ void __launch_bounds__(PWA_TPB, 4)
+    pwa_eval_multi(const double* __restrict__ ck, const int* __restrict__ work_req,
+                   const long long* __restrict__ work_tile, long long n_work,
+                   const float2* __restrict__ Fc, const double* __restrict__ Wc,
+                   double* __restrict__ tile_part) {
+  constexpr int NA = PWA_CACHE_NA;
+  __shared__ double red[PWA_TPB / 32][NA];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (long long wi = blockIdx.x; wi < n_work; wi += gridDim.x) {
+    const int r = work_req[wi];
+    const long long t = work_tile[wi];
+    const double* c = ck + (long long)r * 2 * PWA_NCOL;
+    const float2* F = Fc + t * PWA_NF * PWA_TPB + tid;
+    float2 v[PWA_NF];
+#pragma unroll
+    for (int j = 0; j < PWA_NF; ++j) v[j] = __ldcs(F + j * PWA_TPB);
+    const double w = __ldcs(Wc + t * PWA_TPB + tid);
+    double ar[PWA_NOUT], ai[PWA_NOUT];
+#pragma unroll
+    for (int o = 0; o < PWA_NOUT; ++o) ar[o] = ai[o] = 0.0;
+#pragma unroll
+    for (int j = 0; j < PWA_NF; ++j) {
+      const int k = pwa_fk[j], o = pwa_fo[j];
+      const double cr = __ldg(c + 2 * k), ci = __ldg(c + 2 * k + 1);
+      ar[o] = fma(cr, (double)v[j].x, fma(-ci, (double)v[j].y, ar[o]));
+      ai[o] = fma(cr, (double)v[j].y, fma(ci, (double)v[j].x, ai[o]));
+    }
+    double f = 0.0;
+#pragma unroll
+    for (int o = 0; o < PWA_NOUT; ++o) f = fma(ar[o], ar[o], fma(ai[o], ai[o], f));
+    double dl;
+    const double cl = clip_log(f, &dl);
+    const double fac = w * dl;
+    float br[PWA_NOUT], bi[PWA_NOUT];
+#pragma unroll
+    for (int o = 0; o < PWA_NOUT; ++o) {
+      br[o] = (float)(fac * ar[o]);
+      bi[o] = (float)(-fac * ai[o]);
+    }
+    float gr[PWA_NCOL], gi[PWA_NCOL];
+#pragma unroll
+    for (int k = 0; k < PWA_NCOL; ++k) gr[k] = gi[k] = 0.f;
+#pragma unroll
+    for (int j = 0; j < PWA_NF; ++j) {
+      const int k = pwa_fk[j], o = pwa_fo[j];
+      gr[k] = fmaf(br[o], v[j].x, fmaf(-bi[o], v[j].y, gr[k]));
+      gi[k] = fmaf(br[o], v[j].y, fmaf(bi[o], v[j].x, gi[k]));
+    }
+    {
+      const double s0 = warp_sum(w * cl);
+      if (lane == 0) red[warp][0] = s0;
+    }
+#pragma unroll
+    for (int k = 0; k < PWA_NCOL; ++k) {
+      const double a = warp_sum((double)gr[k]), b = warp_sum((double)gi[k]);
+      if (lane == 0) {
+        red[warp][1 + 2 * k] = a;
+        red[warp][2 + 2 * k] = b;
+      }
+    }
+    __syncthreads();
+    for (int j = tid; j < NA; j += PWA_TPB) {
+      double s = 0.0;
+#pragma unroll
+      for (int w2 = 0; w2 < PWA_TPB / 32; ++w2) s += red[w2][j];
+      tile_part[wi * NA + j] = s;
+    }
+    __syncthreads();
+  }
+}
+
+// out[r * NA + j] = sum over rows [row_beg[r], row_beg[r+1]) of tile_part,
+// in row order (one warp per (request, accumulator), lanes strided, fixed
+// shuffle tree).
+extern "C" __global__ void pwa_reduce_multi(const double* __restrict__ tile_part,
+                                            const long long* __restrict__ row_beg, int n_req,
+                                            double* __restrict__ out) {
+  constexpr int NA = PWA_CACHE_NA;
+  const int lane = threadIdx.x & 31;
+  const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long q = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+       q < (long long)n_req * NA; q += warps) {
+    const int r = (int)(q / NA), j = (int)(q % NA);
+    double s = 0.0;
+    for (long long row = row_beg[r] + lane; row < row_beg[r + 1]; row += 32) s += tile_part[row * NA + j];
+    s = warp_sum(s);
+    if (lane == 0) out[q] = s;
+  }
+}

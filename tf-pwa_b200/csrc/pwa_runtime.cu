@@ -28,7 +28,7 @@ struct Kernels {
   cudaKernel_t eval_f64 = nullptr, eval_f32 = nullptr, reduce = nullptr, pdf_f64 = nullptr,
                pdf_f32 = nullptr, columns_f64 = nullptr, gram_f64 = nullptr, sum_rows = nullptr,
                to_f32 = nullptr, cache_f32 = nullptr, eval_cached = nullptr,
-               eval_cached_direct = nullptr;
+               eval_cached_direct = nullptr, eval_multi = nullptr, reduce_multi = nullptr;
 };
 
 }  // namespace
@@ -62,6 +62,20 @@ struct pwa_plan {
   double seq = 0.0;
   std::vector<double> gram;  // MC Gram matrix, (re, im) row-major ncol x ncol
   bool gram_valid = false;
+  // pool of column-cache tiles shared by many fits (serving)
+  float2* pool_f = nullptr;
+  double* pool_w = nullptr;
+  long long pool_tiles = 0;
+  std::vector<std::pair<long long, long long>> pool_free;  // (first, count), sorted
+  std::vector<std::pair<long long, long long>> pool_used;  // (first, count)
+  // batch scratch of pwa_pieces_multi
+  int* d_work_req = nullptr;
+  long long* d_work_tile = nullptr;
+  long long* d_row_beg = nullptr;
+  double* d_ck = nullptr;
+  double* d_tile_part = nullptr;
+  double* d_multi_out = nullptr;
+  long long multi_cap_work = 0, multi_cap_req = 0;
   // parameter layout for the C-side chain rule
   int n_vars = 0, n_coup = 0, nfac = 0, n_train = 0;
   std::vector<int> coup_r, coup_i, coup_polar, col_fac, train_idx;
@@ -219,7 +233,8 @@ int pwa_plan_create(const char* src, size_t src_len, int n_mass, int n_angle, in
             {"pwa_gram_f64", &h->k.gram_f64},       {"pwa_sum_rows", &h->k.sum_rows},
             {"pwa_to_f32", &h->k.to_f32},           {"pwa_cache_f32", &h->k.cache_f32},
             {"pwa_eval_cached", &h->k.eval_cached},
-            {"pwa_eval_cached_direct", &h->k.eval_cached_direct}};
+            {"pwa_eval_cached_direct", &h->k.eval_cached_direct},
+            {"pwa_eval_multi", &h->k.eval_multi},   {"pwa_reduce_multi", &h->k.reduce_multi}};
   for (auto& e : ks) CU(cudaLibraryGetKernel(e.slot, h->lib, e.name));
   for (int p = 0; p < 2; ++p) {
     cudaFuncAttributes a;
@@ -243,6 +258,14 @@ int pwa_plan_destroy(pwa_plan* h) {
   if (h->fcache) cudaFree(h->fcache);
   if (h->wcache) cudaFree(h->wcache);
   if (h->ticket) cudaFree(h->ticket);
+  if (h->pool_f) cudaFree(h->pool_f);
+  if (h->pool_w) cudaFree(h->pool_w);
+  if (h->d_work_req) cudaFree(h->d_work_req);
+  if (h->d_work_tile) cudaFree(h->d_work_tile);
+  if (h->d_row_beg) cudaFree(h->d_row_beg);
+  if (h->d_ck) cudaFree(h->d_ck);
+  if (h->d_tile_part) cudaFree(h->d_tile_part);
+  if (h->d_multi_out) cudaFree(h->d_multi_out);
   if (h->h_map) cudaFreeHost(h->h_map);
   if (h->d_out) cudaFree(h->d_out);
   if (h->h_out) cudaFreeHost(h->h_out);
@@ -572,34 +595,32 @@ struct cplx {
 inline cplx cmulh(cplx a, cplx b) { return {a.r * b.r - a.i * b.i, a.r * b.i + a.i * b.r}; }
 }  // namespace
 
-int pwa_pieces_cached(pwa_plan* h, const double* vars, double sw, double mc_share, void* stream,
-                      double* out) {
-  if (!h) return PWA_ERR_ARG;
-  if (!vars || !out) return set_err(h, PWA_ERR_ARG, "null argument");
-  if (h->n_coup == 0) return set_err(h, PWA_ERR_STATE, "parameter layout not set");
-  if (!h->gram_valid) return set_err(h, PWA_ERR_STATE, "MC Gram matrix not built");
-  const int K = h->ncol, P = h->n_train;
-  // couplings and column products
-  std::vector<cplx> z(h->n_coup);
+namespace {
+// Column couplings of one parameter vector (layout of pwa_set_param_layout).
+void column_couplings(const pwa_plan* h, const double* vars, std::vector<cplx>* z,
+                      double* ck) {
+  z->resize(h->n_coup);
   for (int j = 0; j < h->n_coup; ++j) {
     const double r = vars[h->coup_r[j]], p = vars[h->coup_i[j]];
-    z[j] = h->coup_polar[j] ? cplx{r * std::cos(p), r * std::sin(p)} : cplx{r, p};
+    (*z)[j] = h->coup_polar[j] ? cplx{r * std::cos(p), r * std::sin(p)} : cplx{r, p};
   }
-  std::vector<double> ck(2 * K);
-  for (int k = 0; k < K; ++k) {
+  for (int k = 0; k < h->ncol; ++k) {
     cplx c{1.0, 0.0};
     for (int f = 0; f < h->nfac; ++f) {
       const int j = h->col_fac[k * h->nfac + f];
-      if (j >= 0) c = cmulh(c, z[j]);
+      if (j >= 0) c = cmulh(c, (*z)[j]);
     }
     ck[2 * k] = c.r;
     ck[2 * k + 1] = c.i;
   }
-  cudaStream_t s = (cudaStream_t)stream;
-  int rc = pwa_eval_cached_enqueue(h, ck.data(), stream);
-  if (rc) return rc;
-  // MC term from the Gram matrix while the kernels run: I = c^H M c,
-  // Gm_k = sum_l conj(c_l) M_lk
+}
+
+// Piece vector from the data sums sd[1 + 2*ncol] of one parameter vector:
+// MC term from the Gram matrix and the chain rule to the trainable variables.
+int pieces_from_sums(pwa_plan* h, const double* vars, const std::vector<cplx>& z,
+                     const double* ck, const double* sd, double sw, double mc_share,
+                     double* out) {
+  const int K = h->ncol, P = h->n_train;
   std::vector<cplx> Gm(K, cplx{0, 0});
   double I = 0.0;
   for (int k = 0; k < K; ++k) {
@@ -614,11 +635,6 @@ int pwa_pieces_cached(pwa_plan* h, const double* vars, double sw, double mc_shar
     Gm[k] = acc;
     I += acc.r * ck[2 * k] - acc.i * ck[2 * k + 1];
   }
-  CU(cudaStreamSynchronize(s));
-  const double* sd = nullptr;
-  rc = cached_result(h, &sd);
-  if (rc) return rc;
-  // chain rule: d f / d theta = 2 Re sum_k J_k G_k
   out[0] = sd[0];
   out[1] = I * mc_share;
   out[2] = sw;
@@ -660,6 +676,202 @@ int pwa_pieces_cached(pwa_plan* h, const double* vars, double sw, double mc_shar
     }
     out[3 + t] = gd;
     out[3 + P + t] = gm * mc_share;
+  }
+  return PWA_OK;
+}
+}  // namespace
+
+int pwa_pieces_cached(pwa_plan* h, const double* vars, double sw, double mc_share, void* stream,
+                      double* out) {
+  if (!h) return PWA_ERR_ARG;
+  if (!vars || !out) return set_err(h, PWA_ERR_ARG, "null argument");
+  if (h->n_coup == 0) return set_err(h, PWA_ERR_STATE, "parameter layout not set");
+  if (!h->gram_valid) return set_err(h, PWA_ERR_STATE, "MC Gram matrix not built");
+  std::vector<cplx> z;
+  std::vector<double> ck(2 * h->ncol);
+  column_couplings(h, vars, &z, ck.data());
+  cudaStream_t s = (cudaStream_t)stream;
+  int rc = pwa_eval_cached_enqueue(h, ck.data(), stream);
+  if (rc) return rc;
+  CU(cudaStreamSynchronize(s));
+  const double* sd = nullptr;
+  rc = cached_result(h, &sd);
+  if (rc) return rc;
+  return pieces_from_sums(h, vars, z, ck.data(), sd, sw, mc_share, out);
+}
+
+// ------------------------------------------------------------------ pool
+int pwa_pool_reserve(pwa_plan* h, long long n_tiles) {
+  if (!h) return PWA_ERR_ARG;
+  if (n_tiles <= 0) return set_err(h, PWA_ERR_ARG, "pool size must be positive");
+  if (h->pool_f) return set_err(h, PWA_ERR_STATE, "pool already reserved");
+  const size_t tile = h->tpb;
+  if (cudaMalloc(&h->pool_f, sizeof(float2) * tile * h->nf * (size_t)n_tiles) != cudaSuccess ||
+      cudaMalloc(&h->pool_w, sizeof(double) * tile * (size_t)n_tiles) != cudaSuccess) {
+    if (h->pool_f) cudaFree(h->pool_f);
+    h->pool_f = nullptr;
+    return set_err(h, PWA_ERR_OOM, "cudaMalloc of the tile pool failed");
+  }
+  h->pool_tiles = n_tiles;
+  h->pool_free.assign(1, {0LL, n_tiles});
+  h->pool_used.clear();
+  return PWA_OK;
+}
+
+int pwa_pool_alloc(pwa_plan* h, long long n_events, long long* first_tile, long long* n_tiles) {
+  if (!h || !first_tile || !n_tiles) return PWA_ERR_ARG;
+  if (!h->pool_f) return set_err(h, PWA_ERR_STATE, "no pool reserved");
+  if (n_events <= 0) return set_err(h, PWA_ERR_ARG, "n_events must be positive");
+  const long long need = (n_events + h->tpb - 1) / h->tpb;
+  for (size_t q = 0; q < h->pool_free.size(); ++q) {
+    auto& fr = h->pool_free[q];
+    if (fr.second >= need) {
+      *first_tile = fr.first;
+      *n_tiles = need;
+      h->pool_used.push_back({fr.first, need});
+      fr.first += need;
+      fr.second -= need;
+      if (fr.second == 0) h->pool_free.erase(h->pool_free.begin() + q);
+      return PWA_OK;
+    }
+  }
+  return set_err(h, PWA_ERR_OOM, "tile pool has no free run of " + std::to_string(need) + " tiles");
+}
+
+int pwa_pool_free(pwa_plan* h, long long first_tile) {
+  if (!h) return PWA_ERR_ARG;
+  for (size_t q = 0; q < h->pool_used.size(); ++q) {
+    if (h->pool_used[q].first != first_tile) continue;
+    const auto run = h->pool_used[q];
+    h->pool_used.erase(h->pool_used.begin() + q);
+    // insert sorted and coalesce neighbours
+    auto it = h->pool_free.begin();
+    while (it != h->pool_free.end() && it->first < run.first) ++it;
+    it = h->pool_free.insert(it, run);
+    size_t i = it - h->pool_free.begin();
+    if (i + 1 < h->pool_free.size() &&
+        h->pool_free[i].first + h->pool_free[i].second == h->pool_free[i + 1].first) {
+      h->pool_free[i].second += h->pool_free[i + 1].second;
+      h->pool_free.erase(h->pool_free.begin() + i + 1);
+    }
+    if (i > 0 && h->pool_free[i - 1].first + h->pool_free[i - 1].second == h->pool_free[i].first) {
+      h->pool_free[i - 1].second += h->pool_free[i].second;
+      h->pool_free.erase(h->pool_free.begin() + i);
+    }
+    return PWA_OK;
+  }
+  return set_err(h, PWA_ERR_ARG, "tile run not allocated");
+}
+
+int pwa_pool_fill(pwa_plan* h, long long first_tile, const double* consts, const double* xm,
+                  const double* xa, const double* w, long long n, long long ld, void* stream) {
+  if (!h) return PWA_ERR_ARG;
+  if (!h->pool_f) return set_err(h, PWA_ERR_STATE, "no pool reserved");
+  if (!consts || !w || (h->n_mass && !xm) || (h->n_angle && !xa) || n <= 0 || ld < n)
+    return set_err(h, PWA_ERR_ARG, "invalid fill arguments");
+  long long ntl = -1;
+  for (const auto& u : h->pool_used)
+    if (u.first == first_tile) ntl = u.second;
+  if (ntl < 0) return set_err(h, PWA_ERR_ARG, "tile run not allocated");
+  if ((n + h->tpb - 1) / h->tpb > ntl) return set_err(h, PWA_ERR_ARG, "events exceed the tile run");
+  cudaStream_t s = (cudaStream_t)stream;
+  std::vector<double> cbuf(consts, consts + h->nconst);
+  float2* fdst = h->pool_f + first_tile * h->nf * (long long)h->tpb;
+  double* wdst = h->pool_w + first_tile * (long long)h->tpb;
+  void* args[] = {cbuf.data(), (void*)&xa, (void*)&xm, (void*)&w, &n, &ntl, &ld, &fdst, &wdst};
+  long long nb = (ntl * h->tpb + h->tpb - 1) / h->tpb;
+  if (nb > 16LL * h->sms) nb = 16LL * h->sms;
+  return launch(h, h->k.cache_f32, dim3((int)nb), dim3(h->tpb), args, s);
+}
+
+int pwa_pieces_multi(pwa_plan* h, int n_req, const long long* first_tile, const long long* n_tiles,
+                     const double* vars, const double* sw, double mc_share, void* stream,
+                     double* out) {
+  if (!h) return PWA_ERR_ARG;
+  if (n_req <= 0 || !first_tile || !n_tiles || !vars || !sw || !out)
+    return set_err(h, PWA_ERR_ARG, "invalid multi-request arguments");
+  if (!h->pool_f) return set_err(h, PWA_ERR_STATE, "no pool reserved");
+  if (h->n_coup == 0) return set_err(h, PWA_ERR_STATE, "parameter layout not set");
+  if (!h->gram_valid) return set_err(h, PWA_ERR_STATE, "MC Gram matrix not built");
+  const int K = h->ncol, NA = 1 + 2 * K, P = h->n_train;
+  long long n_work = 0;
+  std::vector<long long> row_beg(n_req + 1, 0);
+  for (int r = 0; r < n_req; ++r) {
+    if (first_tile[r] < 0 || n_tiles[r] <= 0 || first_tile[r] + n_tiles[r] > h->pool_tiles)
+      return set_err(h, PWA_ERR_ARG, "request tile run outside the pool");
+    row_beg[r] = n_work;
+    n_work += n_tiles[r];
+  }
+  row_beg[n_req] = n_work;
+  // grow scratch (serving set-up; steady state allocates nothing)
+  if (n_work > h->multi_cap_work || n_req > h->multi_cap_req) {
+    const long long cw = n_work > h->multi_cap_work ? 2 * n_work : h->multi_cap_work;
+    const long long cr = n_req > h->multi_cap_req ? 2LL * n_req : h->multi_cap_req;
+    cudaFree(h->d_work_req);
+    cudaFree(h->d_work_tile);
+    cudaFree(h->d_row_beg);
+    cudaFree(h->d_ck);
+    cudaFree(h->d_tile_part);
+    cudaFree(h->d_multi_out);
+    h->d_work_req = nullptr;
+    h->d_work_tile = nullptr;
+    h->d_row_beg = nullptr;
+    h->d_ck = nullptr;
+    h->d_tile_part = nullptr;
+    h->d_multi_out = nullptr;
+    h->multi_cap_work = h->multi_cap_req = 0;
+    if (cudaMalloc(&h->d_work_req, sizeof(int) * cw) != cudaSuccess ||
+        cudaMalloc(&h->d_work_tile, sizeof(long long) * cw) != cudaSuccess ||
+        cudaMalloc(&h->d_row_beg, sizeof(long long) * (cr + 1)) != cudaSuccess ||
+        cudaMalloc(&h->d_ck, sizeof(double) * 2 * K * cr) != cudaSuccess ||
+        cudaMalloc(&h->d_tile_part, sizeof(double) * NA * cw) != cudaSuccess ||
+        cudaMalloc(&h->d_multi_out, sizeof(double) * NA * cr) != cudaSuccess)
+      return set_err(h, PWA_ERR_OOM, "cudaMalloc of the batch scratch failed");
+    h->multi_cap_work = cw;
+    h->multi_cap_req = cr;
+  }
+  std::vector<int> wreq(n_work);
+  std::vector<long long> wtile(n_work);
+  std::vector<double> ck(2 * K * (size_t)n_req);
+  std::vector<std::vector<cplx>> zs(n_req);
+  for (int r = 0; r < n_req; ++r) {
+    for (long long q = 0; q < n_tiles[r]; ++q) {
+      wreq[row_beg[r] + q] = r;
+      wtile[row_beg[r] + q] = first_tile[r] + q;
+    }
+    column_couplings(h, vars + (size_t)r * h->n_vars, &zs[r], ck.data() + 2 * K * (size_t)r);
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  CU(cudaMemcpyAsync(h->d_work_req, wreq.data(), sizeof(int) * n_work, cudaMemcpyHostToDevice, s));
+  CU(cudaMemcpyAsync(h->d_work_tile, wtile.data(), sizeof(long long) * n_work,
+                     cudaMemcpyHostToDevice, s));
+  CU(cudaMemcpyAsync(h->d_row_beg, row_beg.data(), sizeof(long long) * (n_req + 1),
+                     cudaMemcpyHostToDevice, s));
+  CU(cudaMemcpyAsync(h->d_ck, ck.data(), sizeof(double) * ck.size(), cudaMemcpyHostToDevice, s));
+  int per_sm = 0;
+  CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)h->k.eval_multi, h->tpb, 0));
+  if (per_sm < 1) per_sm = 1;
+  long long nb = (long long)per_sm * h->sms;
+  if (nb > n_work) nb = n_work;
+  void* a1[] = {&h->d_ck, &h->d_work_req, &h->d_work_tile, &n_work, &h->pool_f, &h->pool_w,
+                &h->d_tile_part};
+  int rc = launch(h, h->k.eval_multi, dim3((int)nb), dim3(h->tpb), a1, s);
+  if (rc) return rc;
+  long long nq = (long long)n_req * NA;
+  int rb = (int)((nq + 7) / 8);
+  if (rb > 8 * h->sms) rb = 8 * h->sms;
+  void* a2[] = {&h->d_tile_part, &h->d_row_beg, &n_req, &h->d_multi_out};
+  rc = launch(h, h->k.reduce_multi, dim3(rb), dim3(256), a2, s);
+  if (rc) return rc;
+  std::vector<double> sums((size_t)NA * n_req);
+  CU(cudaMemcpyAsync(sums.data(), h->d_multi_out, sizeof(double) * sums.size(),
+                     cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  for (int r = 0; r < n_req; ++r) {
+    rc = pieces_from_sums(h, vars + (size_t)r * h->n_vars, zs[r], ck.data() + 2 * K * (size_t)r,
+                          sums.data() + (size_t)NA * r, sw[r], mc_share,
+                          out + (size_t)r * (3 + 2 * P));
+    if (rc) return rc;
   }
   return PWA_OK;
 }

@@ -53,6 +53,12 @@ def load_library(path=LIB_PATH):
     lib.pwa_pieces_cached.argtypes = [vp, dp, ctypes.c_double, ctypes.c_double, vp, dp]
     lib.pwa_nll_grad_cached.argtypes = [vp, dp, ctypes.c_double, vp, dp, dp]
     lib.pwa_set_cached_variant.argtypes = [vp, i]
+    llp = ctypes.POINTER(ll)
+    lib.pwa_pool_reserve.argtypes = [vp, ll]
+    lib.pwa_pool_alloc.argtypes = [vp, ll, llp, llp]
+    lib.pwa_pool_free.argtypes = [vp, ll]
+    lib.pwa_pool_fill.argtypes = [vp, ll, dp, vp, vp, vp, ll, ll, vp]
+    lib.pwa_pieces_multi.argtypes = [vp, i, llp, llp, dp, dp, ctypes.c_double, vp, dp]
     lib.pwa_eval_noalloc.argtypes = [vp, dp, vp, vp, vp, ll, ll, ll, vp, vp]
     lib.pwa_plan_destroy.argtypes = [vp]
     lib.pwa_compile_only.argtypes = [cp, sz, i, cp, cp, sz]
@@ -75,7 +81,9 @@ def load_library(path=LIB_PATH):
 EXPORTED = ("pwa_plan_create", "pwa_plan_destroy", "pwa_compile_only", "pwa_upload_events",
             "pwa_eval", "pwa_eval_enqueue", "pwa_eval_pdf", "pwa_build_gram", "pwa_cache_data",
             "pwa_eval_cached_enqueue", "pwa_set_param_layout", "pwa_pieces_cached",
-            "pwa_nll_grad_cached", "pwa_set_cached_variant", "pwa_eval_noalloc", "pwa_plan_info", "pwa_last_error")
+            "pwa_nll_grad_cached", "pwa_set_cached_variant", "pwa_pool_reserve",
+            "pwa_pool_alloc", "pwa_pool_free", "pwa_pool_fill", "pwa_pieces_multi",
+            "pwa_eval_noalloc", "pwa_plan_info", "pwa_last_error")
 
 
 class PWAError(RuntimeError):
@@ -537,6 +545,40 @@ class Engine:
         ck = np.ascontiguousarray(ck, np.float64)
         self._check(load_library().pwa_eval_cached_enqueue(self.h, _dptr(ck), stream or 0),
                     "pwa_eval_cached_enqueue")
+
+    # ----------------------------------------------------- serving (pool)
+    def pool_reserve(self, n_tiles):
+        self._check(load_library().pwa_pool_reserve(self.h, int(n_tiles)), "pwa_pool_reserve")
+
+    def pool_alloc(self, n_events):
+        """(first_tile, n_tiles), or None when the pool has no free run."""
+        a, b = ctypes.c_longlong(), ctypes.c_longlong()
+        rc = load_library().pwa_pool_alloc(self.h, int(n_events), ctypes.byref(a), ctypes.byref(b))
+        if rc == 5:  # PWA_ERR_OOM
+            return None
+        self._check(rc, "pwa_pool_alloc")
+        return a.value, b.value
+
+    def pool_free(self, first_tile):
+        self._check(load_library().pwa_pool_free(self.h, int(first_tile)), "pwa_pool_free")
+
+    def pool_fill(self, first_tile, C, xm_ptr, xa_ptr, w_ptr, n, ld, stream=None):
+        C = np.ascontiguousarray(C, np.float64)
+        self._check(load_library().pwa_pool_fill(self.h, int(first_tile), _dptr(C), xm_ptr,
+                                                 xa_ptr, w_ptr, int(n), int(ld), stream or 0),
+                    "pwa_pool_fill")
+
+    def pieces_multi(self, first_tiles, n_tiles, var_rows, sws, mc_share=1.0, stream=None):
+        ft = np.ascontiguousarray(first_tiles, np.int64)
+        nt = np.ascontiguousarray(n_tiles, np.int64)
+        V = np.ascontiguousarray(var_rows, np.float64)
+        sw = np.ascontiguousarray(sws, np.float64)
+        out = np.zeros((len(ft), 3 + 2 * self._n_train))
+        llp = ctypes.POINTER(ctypes.c_longlong)
+        self._check(load_library().pwa_pieces_multi(
+            self.h, len(ft), ft.ctypes.data_as(llp), nt.ctypes.data_as(llp), _dptr(V), _dptr(sw),
+            mc_share, stream or 0, _dptr(out)), "pwa_pieces_multi")
+        return out
 
     def set_gram(self, vals):
         """Build the MC Gram matrix at the current masses/widths."""
