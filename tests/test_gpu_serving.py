@@ -66,20 +66,17 @@ def test_multi_request_equals_cached_path(setup):
 
     cl, data, mc = setup
     job = _jobs(cl, data, [12000])[0]
-    srv = FitServer(cl, mc, 1e9)
-    with srv.lock:
-        srv.pending.append(job)
-    srv._admit()
+    srv = FitServer(cl, mc, 1e9, run=False)
+    srv.pending.append(job)
+    srv._admit(start=False)
     x = job.x0
     nll_s, g_s = srv.eval_alone(job, x)
-    srv._stop = True
+    srv.close()
     fcn = FCN(cl, EventData(job.fields, np.ones(job.n)), mc, precision="mixed")
     nll_c, g_c = fcn.nll_grad(x)
     assert abs(nll_s - nll_c) <= 1e-10 * abs(nll_c)
     np.testing.assert_allclose(g_s, g_c, rtol=1e-8, atol=1e-8 * np.abs(g_c).max())
     fcn.eng.close()
-    job.done.wait(timeout=60)
-    srv.close()
 
 
 def test_admission_under_budget(setup):

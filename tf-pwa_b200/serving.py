@@ -43,10 +43,11 @@ class FitJob:
 
 
 class FitServer:
-    def __init__(self, config, mc, budget_bytes, max_active=256, tpb=128):
+    def __init__(self, config, mc, budget_bytes, max_active=256, tpb=128, run=True):
         """``config``: ConfigLoader of the model (its parameters hold the
         fixed masses/widths and the fixed couplings); ``mc``: EventData of the
-        shared MC sample (device fields)."""
+        shared MC sample (device fields).  ``run=False`` creates the server
+        without its scheduler thread (for direct single evaluations)."""
         self.cl = config
         self.vm = config.vm
         self.eng = Engine(config.decay_group, config.plan, self.vm, tpb=tpb)
@@ -76,8 +77,10 @@ class FitServer:
         self.finished = []
         self.batches = []             # (n_requests, n_tiles, seconds)
         self._stop = False
-        self._thread = threading.Thread(target=self._loop, daemon=True)
-        self._thread.start()
+        self._thread = None
+        if run:
+            self._thread = threading.Thread(target=self._loop, daemon=True)
+            self._thread.start()
 
     # ------------------------------------------------------------ client
     def submit(self, job):
@@ -89,7 +92,8 @@ class FitServer:
     def close(self):
         self._stop = True
         self.requests.put(None)
-        self._thread.join(timeout=30)
+        if self._thread is not None:
+            self._thread.join(timeout=30)
         self.eng.close()
 
     # ------------------------------------------------------------ fits
@@ -117,7 +121,7 @@ class FitServer:
         job.finished = time.perf_counter()
         self.requests.put(("done", job))
 
-    def _admit(self):
+    def _admit(self, start=True):
         with self.lock:
             while self.pending and len(self.active) < self.max_active:
                 job = self.pending[0]
@@ -136,7 +140,8 @@ class FitServer:
                 torch.cuda.synchronize()
                 job.admitted = time.perf_counter()
                 self.active[job.fid] = job
-                threading.Thread(target=self._fit_thread, args=(job,), daemon=True).start()
+                if start:
+                    threading.Thread(target=self._fit_thread, args=(job,), daemon=True).start()
 
     # ------------------------------------------------------------ scheduler
     def _loop(self):
