@@ -40,6 +40,7 @@ CASES = {
     "d2kpipi_float": ("d2kpipi_float.yml", 400, 0, 1500, 12, True, {}),
     "lc2pkpi": ("lc2pkpi.yml", 400, 40, 1500, 13, False, {"bg_weight": 0.1}),
     "toy_vvp": ("toy_vvp.yml", 300, 30, 1200, 14, False, {"bg_weight": 0.1}),
+    "b2dstkpi": ("b2dstkpi.yml", 300, 0, 1200, 15, False, {}),
 }
 
 

@@ -173,6 +173,23 @@ class Tensor(torch.Tensor):
     def __rpow__(self, o):
         return torch.Tensor.__rpow__(self, self._np(o))
 
+    # TF tensors are immutable: ``a += b`` rebinds ``a`` to a new tensor and
+    # never writes through a slice view (LorentzVector.boost relies on this)
+    def __iadd__(self, o):
+        return self.__add__(o)
+
+    def __isub__(self, o):
+        return self.__sub__(o)
+
+    def __imul__(self, o):
+        return self.__mul__(o)
+
+    def __itruediv__(self, o):
+        return self.__truediv__(o)
+
+    def __ipow__(self, o):
+        return self.__pow__(o)
+
     __array_priority__ = 10000
 
     def __bool__(self):

@@ -5,7 +5,7 @@ import pytest
 
 from common import load_golden, load_model
 
-CASES = ["d2kpipi", "d2kpipi_float", "lc2pkpi", "toy_vvp"]
+CASES = ["d2kpipi", "d2kpipi_float", "lc2pkpi", "toy_vvp", "b2dstkpi"]
 
 
 @pytest.mark.parametrize("name", CASES)
