@@ -28,13 +28,26 @@ import time
 import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
-CONFIG = "lc2pkpi.yml"
-N_SIG, N_BG, N_MC = 1_000_000, 100_000, 1_000_000
 BG_WEIGHT = 0.1
-METRIC = "NLL+grad evals/s @1M data+1M MC"
-WORKLOAD = ("Lambda_c+ -> p K- pi+ (Lambda(1520), K*(892), Delta(1232); 3 chains, 8 LS "
-            "columns, 4 helicity combinations), 1e6 accept-reject signal + 1e5 flat background "
-            "(w=-0.1) data rows, 1e6 flat MC")
+# name: (config, signal events, background rows, MC events, metric, description)
+WORKLOADS = {
+    "lc2pkpi": ("lc2pkpi.yml", 1_000_000, 100_000, 1_000_000,
+                "NLL+grad evals/s @1M data+1M MC",
+                "Lambda_c+ -> p K- pi+ (Lambda(1520), K*(892), Delta(1232); 3 chains, 8 LS "
+                "columns, 4 helicity combinations), 1e6 accept-reject signal + 1e5 flat "
+                "background (w=-0.1) data rows, 1e6 flat MC"),
+    "b2dstkpi": ("b2dstkpi.yml", 1_000_000, 0, 4_000_000,
+                 "NLL+grad evals/s @1M data+4M MC",
+                 "B -> D*(2007) (-> D pi_s) K pi, 12 resonances (J = 0..3) in the D*K, D*pi "
+                 "and K pi topologies, 30 LS columns, 1 helicity combination; 1e6 "
+                 "accept-reject data, 4e6 flat MC"),
+}
+CONFIG, N_SIG, N_BG, N_MC, METRIC, WORKLOAD = WORKLOADS["lc2pkpi"]
+
+
+def _select(name):
+    global CONFIG, N_SIG, N_BG, N_MC, METRIC, WORKLOAD
+    CONFIG, N_SIG, N_BG, N_MC, METRIC, WORKLOAD = WORKLOADS[name]
 
 
 def _pkg():
@@ -243,7 +256,7 @@ def run_serving(args):
     _pkg()
     from tf_pwa_b200.serving import serving_benchmark
 
-    r = serving_benchmark(n_fits=args.n_fits)
+    r = serving_benchmark(n_fits=args.n_fits, rate=args.fit_rate)
     line = {"metric": "toy-fit service: per-fit latency p50/p99 and aggregate NLL+grad evals/s",
             "value": r["evals_per_s"], "unit": "evals/s", "n_gpus": 1,
             "higher_is_better": True, "data": "synthetic", "dtype": "f64",
@@ -266,10 +279,17 @@ def main():
     ap.add_argument("--serving", action="store_true",
                     help="run the toy-fit serving workload instead (separate JSON line)")
     ap.add_argument("--n-fits", type=int, default=512)
-    ap.add_argument("--n-sig", type=int, default=N_SIG, help="signal data events per GPU")
-    ap.add_argument("--n-bg", type=int, default=N_BG, help="background data rows per GPU")
-    ap.add_argument("--n-mc", type=int, default=N_MC, help="MC events per GPU")
+    ap.add_argument("--fit-rate", type=float, default=None,
+                    help="serving: Poisson arrival rate, fits/s (default n_fits / 5 s)")
+    ap.add_argument("--workload", default="lc2pkpi", choices=sorted(WORKLOADS))
+    ap.add_argument("--n-sig", type=int, default=None, help="signal data events per GPU")
+    ap.add_argument("--n-bg", type=int, default=None, help="background data rows per GPU")
+    ap.add_argument("--n-mc", type=int, default=None, help="MC events per GPU")
     args = ap.parse_args()
+    _select(args.workload)
+    args.n_sig = N_SIG if args.n_sig is None else args.n_sig
+    args.n_bg = N_BG if args.n_bg is None else args.n_bg
+    args.n_mc = N_MC if args.n_mc is None else args.n_mc
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -361,14 +381,14 @@ def main():
     k_kernel = args.steps
     t_kernel = timed(lambda: eng.eval_cached_enqueue(ck), k_kernel)
     variants = {}
-    for var in (0, 1):
+    for var in (0, 1, 2):
         eng.set_cached_variant(var)
         variants[var] = {"kernel_us": 1e6 * timed(lambda: eng.eval_cached_enqueue(ck), k_kernel)
                          / k_kernel,
                          "step_us": 1e6 * timed(lambda: eng.nll_grad_cached(var_vec), args.steps)
                          / args.steps,
                          "nll": eng.nll_grad_cached(var_vec)[0]}
-    eng.set_cached_variant(1)
+    eng.set_cached_variant(-1)
     Cp = eng_p.consts(vals)
     t_kernel_p = timed(lambda: eng_p.eval_enqueue(Cp, PLAIN_F64, mc=True), k_kernel)
     ck_clocks = clocks.stop(local)
@@ -404,7 +424,9 @@ def main():
                 "call": "FCN.nll_grad(x) with x a host numpy vector"},
         "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
                      "frac": ach / hbm, "traffic": None, "peak_kind": peak_kind,
-                     "kernel": "pwa_eval_cached + pwa_reduce (data term, mixed form)",
+                     "kernel": ("pwa_eval_cached_direct" if code.ncol <= 12 else
+                                "pwa_eval_cached_wred") + " (data term, mixed form; ends with "
+                               "its own fixed-order reduction)",
                      "algorithmic_bytes_per_launch": bytes_mixed,
                      "launch_us": 1e6 * t_kernel / k_kernel,
                      "plain_f64_kernel": {"achieved": ach_p, "frac": ach_p / hbm,

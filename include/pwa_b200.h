@@ -103,7 +103,11 @@ int pwa_build_gram(pwa_plan* h, const double* consts, void* stream, double* out)
 int pwa_cache_data(pwa_plan* h, const double* consts, void* stream);
 
 /* Kernel used for the cached data term: 0 = shared-memory ring fed by bulk
- * copies, 1 = direct loads with four blocks per SM (default 1). */
+ * copies, 1 = direct loads with four blocks per SM and per-thread FP64
+ * column sums, 2 = direct loads with the column sums of each warp's 32
+ * events reduce-scattered in FP32 before FP64 accumulation (register use
+ * independent of the column count), -1 = automatic (default: 1 for up to
+ * 12 columns, else 2). */
 int pwa_set_cached_variant(pwa_plan* h, int variant);
 
 /* Data-term kernels on the cache with column couplings ck[2*ncol]

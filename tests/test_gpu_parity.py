@@ -13,7 +13,7 @@ from common import golden_data, load_golden, load_model
 
 pytestmark = pytest.mark.gpu
 
-CASES = ["d2kpipi", "d2kpipi_float", "lc2pkpi"]
+CASES = ["d2kpipi", "d2kpipi_float", "lc2pkpi", "b2dstkpi"]
 
 
 def _engine(name):
@@ -69,7 +69,7 @@ def test_pdf_matches_reference(name):
     eng.close()
 
 
-@pytest.mark.parametrize("name", ["d2kpipi", "lc2pkpi"])
+@pytest.mark.parametrize("name", ["d2kpipi", "lc2pkpi", "b2dstkpi"])
 def test_gram_mc_term(name):
     """Cached MC integral I = c^H M c and its gradient equal the direct sums."""
     from tf_pwa_b200.engine import PLAIN_F64
@@ -93,7 +93,7 @@ def test_reproducible_bitwise():
     eng.close()
 
 
-@pytest.mark.parametrize("name", ["d2kpipi", "lc2pkpi"])
+@pytest.mark.parametrize("name", ["d2kpipi", "lc2pkpi", "b2dstkpi"])
 def test_cached_columns_fcn(name):
     """Mixed form with fixed masses/widths: FP32 column cache + FP64 Gram,
     NLL/gradient from the C-side chain rule, against the reference."""
@@ -124,3 +124,37 @@ def test_cached_columns_fcn(name):
     n2, g2 = combine_pieces(v, len(meta["trainable"]))
     assert n2 == pytest.approx(nll, rel=1e-14)
     fcn.eng.close()
+
+
+@pytest.mark.parametrize("name", ["lc2pkpi", "b2dstkpi"])
+def test_cached_kernel_variants_agree(name):
+    """The three data-term kernels on the column cache (shared-memory ring,
+    per-thread FP64 column sums, warp reduce-scatter of FP32 column sums)
+    give the same NLL (FP64 amplitude and log in all three) and gradients
+    that differ only by FP32 rounding of per-event / per-warp sums."""
+    from tf_pwa_b200.api import FCN, EventData
+    from common import load_model as lm
+
+    g, meta = load_golden(name)
+    dc, vm, plan = lm(meta["config"])
+    vm.set_all(meta["variables"])
+
+    class _Cfg:
+        pass
+
+    cfg = _Cfg()
+    cfg.vm, cfg.decay_group, cfg.plan = vm, dc.decay_group, plan
+    x, w = golden_data(g, meta)
+    fcn = FCN(cfg, EventData(x, w / (w.sum() / (w * w).sum())), EventData(g["fields_mc"]),
+              precision="mixed")
+    vals = [vm.variables[k] for k in fcn._var_names]
+    res = {}
+    for var in (0, 1, 2):
+        fcn.eng.set_cached_variant(var)
+        res[var] = fcn.eng.nll_grad_cached(vals)
+    fcn.eng.close()
+    n1, g1 = res[1]
+    for var in (0, 2):
+        n, gr = res[var]
+        assert abs(n - n1) <= 1e-12 * abs(n1)
+        np.testing.assert_allclose(gr, g1, rtol=1e-5, atol=1e-6 * np.abs(g1).max())

@@ -149,6 +149,32 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
+// Reduce-scatter across a warp by recursive halving.  Every lane holds P
+// values (P a multiple of 32); at the step with lane offset O, a lane keeps
+// the half of its C live values selected by its lane bit O and adds the
+// partner's copy of that half.  After the five steps lane l holds in
+// v[0 .. P/32) the warp sums of entries P/32 * l .. P/32 * l + P/32 - 1.
+// P - 1 shuffles per lane instead of 5 P for one warp_sum per value.
+template <int C, int O, int P>
+__device__ __forceinline__ void warp_rs_step(float (&v)[P], int lane) {
+  if constexpr (O > 0) {
+    const bool up = (lane & O) != 0;
+#pragma unroll
+    for (int j = 0; j < C / 2; ++j) {
+      const float lo = v[j], hi = v[j + C / 2];
+      const float keep = up ? hi : lo, send = up ? lo : hi;
+      v[j] = keep + __shfl_xor_sync(0xffffffffu, send, O);
+    }
+    warp_rs_step<C / 2, O / 2, P>(v, lane);
+  }
+}
+
+template <int P>
+__device__ __forceinline__ void warp_reduce_scatter(float (&v)[P], int lane) {
+  static_assert(P % 32 == 0, "warp_reduce_scatter: P must be a multiple of 32");
+  warp_rs_step<P, 16, P>(v, lane);
+}
+
 // clip_log and its derivative in FP64
 __device__ __forceinline__ double clip_log(double x, double* dx) {
   const double eps = 1e-6;

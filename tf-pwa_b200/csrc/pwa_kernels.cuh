@@ -540,72 +540,166 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, 4)
 }
 
 // ---------------------------------------------------------------------------
+// Column sensitivities summed over a warp before they reach FP64.  The
+// per-event terms are those of pwa_eval_cached_direct; the FP32 values
+// fac * conj(A) F_k of the warp's 32 events are summed by a reduce-scatter
+// (lane l ends with entries PWA_GPAD / 32 * l ..), so each lane carries
+// PWA_GPAD / 32 FP64 accumulators across tiles instead of 2 * PWA_NCOL:
+// the register footprint no longer grows with the number of columns.
+#define PWA_GPAD ((2 * PWA_NCOL + 31) / 32 * 32)
+
+struct CoupParam {  // couplings from the kernel's parameter block
+  const CCoup& c;
+  __device__ __forceinline__ double operator()(int i) const { return c.v[i]; }
+};
+struct CoupGlobal {  // couplings from global memory (one row per request)
+  const double* __restrict__ c;
+  __device__ __forceinline__ double operator()(int i) const { return __ldg(c + i); }
+};
+
+// One event of a column tile: returns w * clip_log(f) and fills g (entries
+// 2k, 2k + 1 = re, im of fac * conj(A) F_k, zero beyond 2 * PWA_NCOL).
+template <class Coup>
+__device__ __forceinline__ double cached_event(const float2 (&v)[PWA_NF], double w,
+                                               const Coup& cp, float (&g)[PWA_GPAD]) {
+  double ar[PWA_NOUT], ai[PWA_NOUT];
+#pragma unroll
+  for (int o = 0; o < PWA_NOUT; ++o) ar[o] = ai[o] = 0.0;
+#pragma unroll
+  for (int j = 0; j < PWA_NF; ++j) {
+    const int k = pwa_fk[j], o = pwa_fo[j];
+    const double cr = cp(2 * k), ci = cp(2 * k + 1);
+    ar[o] = fma(cr, (double)v[j].x, fma(-ci, (double)v[j].y, ar[o]));
+    ai[o] = fma(cr, (double)v[j].y, fma(ci, (double)v[j].x, ai[o]));
+  }
+  double f = 0.0;
+#pragma unroll
+  for (int o = 0; o < PWA_NOUT; ++o) f = fma(ar[o], ar[o], fma(ai[o], ai[o], f));
+  double dl;
+  const double cl = clip_log(f, &dl);
+  const double fac = w * dl;
+  float br[PWA_NOUT], bi[PWA_NOUT];
+#pragma unroll
+  for (int o = 0; o < PWA_NOUT; ++o) {
+    br[o] = (float)(fac * ar[o]);
+    bi[o] = (float)(-fac * ai[o]);
+  }
+#pragma unroll
+  for (int j = 0; j < PWA_GPAD; ++j) g[j] = 0.f;
+#pragma unroll
+  for (int j = 0; j < PWA_NF; ++j) {
+    const int k = pwa_fk[j], o = pwa_fo[j];
+    g[2 * k] = fmaf(br[o], v[j].x, fmaf(-bi[o], v[j].y, g[2 * k]));
+    g[2 * k + 1] = fmaf(br[o], v[j].y, fmaf(bi[o], v[j].x, g[2 * k + 1]));
+  }
+  return w * cl;
+}
+
+// four blocks per SM (128 registers) while the column sums fit one
+// reduce-scatter row (up to 16 complex columns), three above
+#ifndef PWA_WRED_MINB
+#define PWA_WRED_MINB (PWA_GPAD > 32 ? 3 : 4)
+#endif
+extern "C" __global__ void __launch_bounds__(PWA_TPB, PWA_WRED_MINB)
+    pwa_eval_cached_wred(const CCoup c, const float2* __restrict__ Fc,
+                         const double* __restrict__ Wc, long long ntiles,
+                         double* __restrict__ partials, unsigned int* __restrict__ ticket,
+                         double* __restrict__ out, double seq) {
+  constexpr int NA = PWA_CACHE_NA;
+  constexpr int NG = 2 * PWA_NCOL, MG = PWA_GPAD / 32;
+  __shared__ double red[PWA_TPB / 32][NA];
+  __shared__ int s_last;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const CoupParam cp{c};
+  double acc0 = 0.0;
+  double accg[MG];
+#pragma unroll
+  for (int j = 0; j < MG; ++j) accg[j] = 0.0;
+  for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const float2* F = Fc + t * PWA_NF * PWA_TPB + tid;
+    float2 v[PWA_NF];
+#pragma unroll
+    for (int j = 0; j < PWA_NF; ++j) v[j] = __ldcs(F + j * PWA_TPB);
+    const double w = __ldcs(Wc + t * PWA_TPB + tid);
+    float g[PWA_GPAD];
+    acc0 += cached_event(v, w, cp, g);
+    warp_reduce_scatter<PWA_GPAD>(g, lane);
+#pragma unroll
+    for (int j = 0; j < MG; ++j) accg[j] += (double)g[j];
+  }
+  {
+    const double v0 = warp_sum(acc0);
+    if (lane == 0) red[warp][0] = v0;
+  }
+#pragma unroll
+  for (int j = 0; j < MG; ++j) {
+    const int idx = MG * lane + j;
+    if (idx < NG) red[warp][1 + idx] = accg[j];
+  }
+  __syncthreads();
+  for (int j = tid; j < NA; j += PWA_TPB) {
+    double s2 = 0.0;
+#pragma unroll
+    for (int w2 = 0; w2 < PWA_TPB / 32; ++w2) s2 += red[w2][j];
+    partials[(long long)blockIdx.x * NA + j] = s2;
+  }
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) s_last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  for (int j = warp; j < NA; j += PWA_TPB / 32) {
+    double s2 = 0.0;
+    for (int bb = lane; bb < (int)gridDim.x; bb += 32) s2 += __ldcg(partials + (long long)bb * NA + j);
+    s2 = warp_sum(s2);
+    if (lane == 0) out[j] = s2;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    out[NA] = (double)atomicOr((unsigned int*)(ticket + 1), 0u);
+    out[NA + 1] = seq;
+    ticket[0] = 0u;
+    ticket[1] = 0u;
+    __threadfence_system();
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Many fits in one launch (serving).  Each fit's data-event column cache is a
 // run of tiles in a shared pool (same tile layout as above).  The launch gets
 // a work list of (request, pool tile) pairs covering the tiles of every fit
 // with a pending evaluation; each block evaluates work tiles with that
 // request's couplings and writes one row of per-tile sums.  pwa_reduce_multi
 // then sums each request's rows in the fit's own tile order, so a fit's
-// result does not depend on which other fits share the launch.
-extern "C" __global__ void __launch_bounds__(PWA_TPB, 4)
+// result does not depend on which other fits share the launch.  Per-tile
+// column sums use the warp reduce-scatter of pwa_eval_cached_wred.
+extern "C" __global__ void __launch_bounds__(PWA_TPB, PWA_WRED_MINB)
     pwa_eval_multi(const double* __restrict__ ck, const int* __restrict__ work_req,
                    const long long* __restrict__ work_tile, long long n_work,
                    const float2* __restrict__ Fc, const double* __restrict__ Wc,
                    double* __restrict__ tile_part) {
   constexpr int NA = PWA_CACHE_NA;
+  constexpr int NG = 2 * PWA_NCOL, MG = PWA_GPAD / 32;
   __shared__ double red[PWA_TPB / 32][NA];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (long long wi = blockIdx.x; wi < n_work; wi += gridDim.x) {
     const int r = work_req[wi];
     const long long t = work_tile[wi];
-    const double* c = ck + (long long)r * 2 * PWA_NCOL;
+    const CoupGlobal cp{ck + (long long)r * 2 * PWA_NCOL};
     const float2* F = Fc + t * PWA_NF * PWA_TPB + tid;
     float2 v[PWA_NF];
 #pragma unroll
     for (int j = 0; j < PWA_NF; ++j) v[j] = __ldcs(F + j * PWA_TPB);
     const double w = __ldcs(Wc + t * PWA_TPB + tid);
-    double ar[PWA_NOUT], ai[PWA_NOUT];
+    float g[PWA_GPAD];
+    const double s0 = warp_sum(cached_event(v, w, cp, g));
+    warp_reduce_scatter<PWA_GPAD>(g, lane);
+    if (lane == 0) red[warp][0] = s0;
 #pragma unroll
-    for (int o = 0; o < PWA_NOUT; ++o) ar[o] = ai[o] = 0.0;
-#pragma unroll
-    for (int j = 0; j < PWA_NF; ++j) {
-      const int k = pwa_fk[j], o = pwa_fo[j];
-      const double cr = __ldg(c + 2 * k), ci = __ldg(c + 2 * k + 1);
-      ar[o] = fma(cr, (double)v[j].x, fma(-ci, (double)v[j].y, ar[o]));
-      ai[o] = fma(cr, (double)v[j].y, fma(ci, (double)v[j].x, ai[o]));
-    }
-    double f = 0.0;
-#pragma unroll
-    for (int o = 0; o < PWA_NOUT; ++o) f = fma(ar[o], ar[o], fma(ai[o], ai[o], f));
-    double dl;
-    const double cl = clip_log(f, &dl);
-    const double fac = w * dl;
-    float br[PWA_NOUT], bi[PWA_NOUT];
-#pragma unroll
-    for (int o = 0; o < PWA_NOUT; ++o) {
-      br[o] = (float)(fac * ar[o]);
-      bi[o] = (float)(-fac * ai[o]);
-    }
-    float gr[PWA_NCOL], gi[PWA_NCOL];
-#pragma unroll
-    for (int k = 0; k < PWA_NCOL; ++k) gr[k] = gi[k] = 0.f;
-#pragma unroll
-    for (int j = 0; j < PWA_NF; ++j) {
-      const int k = pwa_fk[j], o = pwa_fo[j];
-      gr[k] = fmaf(br[o], v[j].x, fmaf(-bi[o], v[j].y, gr[k]));
-      gi[k] = fmaf(br[o], v[j].y, fmaf(bi[o], v[j].x, gi[k]));
-    }
-    {
-      const double s0 = warp_sum(w * cl);
-      if (lane == 0) red[warp][0] = s0;
-    }
-#pragma unroll
-    for (int k = 0; k < PWA_NCOL; ++k) {
-      const double a = warp_sum((double)gr[k]), b = warp_sum((double)gi[k]);
-      if (lane == 0) {
-        red[warp][1 + 2 * k] = a;
-        red[warp][2 + 2 * k] = b;
-      }
+    for (int j = 0; j < MG; ++j) {
+      const int idx = MG * lane + j;
+      if (idx < NG) red[warp][1 + idx] = (double)g[j];
     }
     __syncthreads();
     for (int j = tid; j < NA; j += PWA_TPB) {

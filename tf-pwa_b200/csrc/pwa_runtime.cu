@@ -15,6 +15,7 @@
 #include <cstdio>
 #include <mutex>
 #include <cstring>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -28,7 +29,7 @@ struct Kernels {
   cudaKernel_t eval_f64 = nullptr, eval_f32 = nullptr, reduce = nullptr, pdf_f64 = nullptr,
                pdf_f32 = nullptr, columns_f64 = nullptr, gram_f64 = nullptr, sum_rows = nullptr,
                to_f32 = nullptr, cache_f32 = nullptr, eval_cached = nullptr,
-               eval_cached_direct = nullptr, eval_multi = nullptr, reduce_multi = nullptr;
+               eval_cached_direct = nullptr, eval_cached_wred = nullptr, eval_multi = nullptr, reduce_multi = nullptr;
 };
 
 }  // namespace
@@ -53,8 +54,11 @@ struct pwa_plan {
   float2* fcache = nullptr;
   double* wcache = nullptr;
   long long ntiles = 0, ntiles_cap = 0, fcache_n = 0;
-  int cached_blocks = 0, cached_blocks_direct = 0;
-  int cached_variant = 1;  // 0: shared-memory ring (bulk copies), 1: direct loads
+  int cached_blocks = 0, cached_blocks_direct = 0, cached_blocks_wred = 0;
+  // 0: shared-memory ring (bulk copies), 1: direct loads with per-thread FP64
+  // column sums, 2: direct loads with warp reduce-scatter of the column sums;
+  // -1: automatic (1 for up to 12 columns, else 2)
+  int cached_variant = -1;
   size_t cached_smem = 0;
   unsigned int* ticket = nullptr;  // [0] finished-block count, [1] error flag
   double* h_map = nullptr;         // mapped pinned result of the cached kernel
@@ -135,9 +139,24 @@ std::string full_source(const char* src, size_t src_len, int tpb) {
 }
 
 // NVRTC compile of the full module for `arch` (e.g. "sm_100a").
+// Cubins already built in this process, keyed by (arch, full source): plans
+// of the same model (one per fit, per precision, per test) compile once.
+std::mutex g_cubin_mu;
+std::map<std::string, std::vector<char>> g_cubins;
+
 int compile_cubin(const char* src, size_t src_len, int tpb, const std::string& arch, bool verbose,
                   std::vector<char>* cubin, std::string* log) {
   const std::string full = full_source(src, src_len, tpb);
+  const std::string key = arch + '\n' + full;
+  if (!verbose) {
+    std::lock_guard<std::mutex> g(g_cubin_mu);
+    auto it = g_cubins.find(key);
+    if (it != g_cubins.end()) {
+      *cubin = it->second;
+      log->clear();
+      return PWA_OK;
+    }
+  }
   nvrtcProgram prog;
   if (nvrtcCreateProgram(&prog, full.c_str(), "pwa_model.cu", 0, nullptr, nullptr) !=
       NVRTC_SUCCESS) {
@@ -165,6 +184,10 @@ int compile_cubin(const char* src, size_t src_len, int tpb, const std::string& a
   cubin->resize(n);
   nvrtcGetCUBIN(prog, cubin->data());
   nvrtcDestroyProgram(&prog);
+  if (!verbose) {
+    std::lock_guard<std::mutex> g(g_cubin_mu);
+    g_cubins.emplace(key, *cubin);
+  }
   return PWA_OK;
 }
 
@@ -234,6 +257,7 @@ int pwa_plan_create(const char* src, size_t src_len, int n_mass, int n_angle, in
             {"pwa_to_f32", &h->k.to_f32},           {"pwa_cache_f32", &h->k.cache_f32},
             {"pwa_eval_cached", &h->k.eval_cached},
             {"pwa_eval_cached_direct", &h->k.eval_cached_direct},
+            {"pwa_eval_cached_wred", &h->k.eval_cached_wred},
             {"pwa_eval_multi", &h->k.eval_multi},   {"pwa_reduce_multi", &h->k.reduce_multi}};
   for (auto& e : ks) CU(cudaLibraryGetKernel(e.slot, h->lib, e.name));
   for (int p = 0; p < 2; ++p) {
@@ -508,8 +532,14 @@ int pwa_cache_data(pwa_plan* h, const double* consts, void* stream) {
   if (per_sm2 < 1) per_sm2 = 1;
   long long want2 = (long long)per_sm2 * h->sms;
   h->cached_blocks_direct = (int)(want2 < ntiles ? want2 : ntiles);
-  const int mb = h->cached_blocks > h->cached_blocks_direct ? h->cached_blocks
-                                                            : h->cached_blocks_direct;
+  int per_sm3 = 0;
+  CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm3, (const void*)h->k.eval_cached_wred,
+                                                   h->tpb, 0));
+  if (per_sm3 < 1) per_sm3 = 1;
+  long long want3 = (long long)per_sm3 * h->sms;
+  h->cached_blocks_wred = (int)(want3 < ntiles ? want3 : ntiles);
+  int mb = h->cached_blocks > h->cached_blocks_direct ? h->cached_blocks : h->cached_blocks_direct;
+  if (h->cached_blocks_wred > mb) mb = h->cached_blocks_wred;
   rc = ensure_partials(h, (long long)mb * (1 + 2 * h->ncol));
   if (rc) return rc;
   CU(cudaStreamSynchronize(s));
@@ -528,12 +558,14 @@ int pwa_eval_cached_enqueue(pwa_plan* h, const double* ck, void* stream) {
   double seq = h->seq;
   void* args[] = {cbuf.data(), &h->fcache, &h->wcache, &nt, &h->partials, &h->ticket, &h->d_map,
                   &seq};
+  const int variant = h->cached_variant >= 0 ? h->cached_variant : (h->ncol <= 12 ? 1 : 2);
   cudaError_t e =
-      h->cached_variant == 1
-          ? cudaLaunchKernel((const void*)h->k.eval_cached_direct, dim3(h->cached_blocks_direct),
-                             dim3(h->tpb), args, 0, s)
-          : cudaLaunchKernel((const void*)h->k.eval_cached, dim3(h->cached_blocks), dim3(h->tpb),
-                             args, h->cached_smem, s);
+      variant == 1   ? cudaLaunchKernel((const void*)h->k.eval_cached_direct,
+                                        dim3(h->cached_blocks_direct), dim3(h->tpb), args, 0, s)
+      : variant == 2 ? cudaLaunchKernel((const void*)h->k.eval_cached_wred,
+                                        dim3(h->cached_blocks_wred), dim3(h->tpb), args, 0, s)
+                     : cudaLaunchKernel((const void*)h->k.eval_cached, dim3(h->cached_blocks),
+                                        dim3(h->tpb), args, h->cached_smem, s);
   if (e != cudaSuccess)
     return set_err(h, PWA_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
   return PWA_OK;
@@ -555,7 +587,7 @@ int cached_result(pwa_plan* h, const double** sums) {
 
 int pwa_set_cached_variant(pwa_plan* h, int variant) {
   if (!h) return PWA_ERR_ARG;
-  if (variant != 0 && variant != 1) return set_err(h, PWA_ERR_ARG, "variant must be 0 or 1");
+  if (variant < -1 || variant > 2) return set_err(h, PWA_ERR_ARG, "variant must be -1, 0, 1 or 2");
   h->cached_variant = variant;
   return PWA_OK;
 }
