@@ -165,17 +165,27 @@ class CpuOracle:
         _pkg()
         from tf_pwa_b200.api import ConfigLoader
         from tf_pwa_b200.kinematics import event_fields, p4_dict
-        from tf_pwa_b200.phasespace import generate_phsp
         from tf_pwa_b200.workload import config_path, seeded_params
+
+        from oracle.toy_oracle import select
+        from tf_pwa_b200.kincode import KinCode
 
         cl = ConfigLoader(config_path(CONFIG), seed=seed)
         vals = seeded_params(cl.vm, seed)
-        pp = cl.decay_config.particle_property
         order = cl.get_dat_order()
-        M = pp[str(cl.decay_group.top)]["mass"]
-        ms = [pp[o]["mass"] for o in order]
-        gen = lambda s: event_fields(cl.plan, p4_dict(np.stack(  # noqa: E731
-            generate_phsp(M, ms, n_sample, seed=s), 1), order)).numpy()
+        kin = KinCode(cl.plan, order)
+
+        def gen(s):
+            """n_sample flat phase-space events (the generator's CPU oracle)."""
+            ps = []
+            first = 0
+            while sum(len(p) for p in ps) < n_sample:
+                out, p = select(s, first, 4 * n_sample, kin.levels, kin.nfin)
+                ps.append(np.transpose(p[:, :, out >= 0], (2, 0, 1)))
+                first += 4 * n_sample
+            p4 = np.concatenate(ps)[:n_sample]
+            return event_fields(cl.plan, p4_dict(p4, order)).numpy()
+
         xd, xm = gen(seed), gen(seed + 1)
         names = sorted({n[:-1] + "r" for n in cl.vm.trainable_vars})
         self.cores = os.cpu_count() or 1
@@ -316,10 +326,15 @@ def main():
     from tf_pwa_b200.workload import make_dataset
 
     t_setup = time.perf_counter()
+
+    def log(msg):
+        print(f"[bench {time.perf_counter() - t_setup:8.1f}s] {msg}", file=sys.stderr, flush=True)
+
     n_sig, n_bg, n_mc = args.n_sig, args.n_bg, args.n_mc
     cl, data, bg, mc = make_dataset(CONFIG, n_sig, n_mc, n_bg=n_bg, bg_weight=BG_WEIGHT,
                                     seed=1 + rank, device="cuda")
     t_data = time.perf_counter() - t_setup
+    log(f"dataset: {n_sig} signal + {n_bg} background + {n_mc} MC events")
     reduce_fn = None
     if dist is not None:
         def reduce_fn(vec):
@@ -327,7 +342,9 @@ def main():
             dist.all_reduce(t)
             return t.cpu().numpy()
     fcn = FCN(cl, data, mc, bg=bg, precision="mixed")         # Gram MC term
+    log("mixed-form FCN ready (column cache + Gram)")
     fcn_plain = FCN(cl, data, mc, bg=bg, precision="plain")
+    log("plain FCN ready")
     for f in (fcn, fcn_plain):
         f.eng.dist_reduce = reduce_fn
         f.eng.mc_share = 1.0 / world  # equal MC shards

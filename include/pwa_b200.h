@@ -15,6 +15,10 @@
  *                      (AbsPDF.__call__ -> DecayGroup.sum_amp, core.py:1919-1931)
  *   pwa_build_gram     cached MC integral matrix       tf_pwa/model/opt_int.py:128-296
  *                      (ModelCachedInt.build_cached_int)
+ *   pwa_fields_from_p4 momenta -> masses and angles    tf_pwa/cal_angle.py:262-490
+ *                      (cal_angle_from_momentum at data load)
+ *   pwa_toy_select /   flat phase space and toy        tf_pwa/phasespace.py:31-254,
+ *   pwa_toy_fields     accept-reject on sum |A|^2      tf_pwa/applications.py:394-487
  *   pwa_compile_only / pwa_last_error / pwa_plan_info / pwa_plan_destroy
  *                      build check and bookkeeping (no reference counterpart)
  *
@@ -88,6 +92,32 @@ int pwa_eval_enqueue(pwa_plan* h, const double* consts, int precision, int mc, v
  * out_dev (device, end-beg doubles). */
 int pwa_eval_pdf(pwa_plan* h, const double* consts, int precision, long long beg, long long end,
                  double* out_dev, void* stream);
+
+/* Dataset step on the device: final-state four-momenta -> every event field
+ * of the model (invariant masses, helicity angles, alignment angles), as
+ * tf_pwa/cal_angle.py:262-490 (cal_angle_from_momentum) computes them at
+ * data-load time.  p4: device, rows (4 f + c) with stride ld_in (c = E, px,
+ * py, pz; finals in dat_order; parent rest frame); out: device, one row per
+ * field in plan order with stride ld_out.  Enqueued on `stream`. */
+int pwa_fields_from_p4(pwa_plan* h, const double* p4, long long n, long long ld_in, double* out,
+                       long long ld_out, void* stream);
+
+/* Toy / MC generation on the device (tf_pwa/phasespace.py:31-254 flat phase
+ * space; tf_pwa/applications.py:394-487 accept-reject on sum |A|^2).
+ * Candidate e = first + i is drawn from a Philox4x32-10 stream keyed by
+ * `seed`; out[i] (device, n doubles) = sum |A|^2 of a kept signal candidate
+ * (flat = 0; kept when u * fmax < sum |A|^2, or when fmax <= 0 after the
+ * phase-space step alone), 1 for a kept flat candidate (flat = 1; consts
+ * may be null), -1 for a rejected one.  Enqueued on `stream`. */
+int pwa_toy_select(pwa_plan* h, const double* consts, unsigned long long seed, long long first,
+                   long long n, double fmax, int flat, double* out, void* stream);
+
+/* Fields (out: rows in plan order, stride ld_out) and, if p4 is not null,
+ * momenta (rows 4 f + c, stride ld_p4) of candidates idx[0..n) (device
+ * event numbers as passed to pwa_toy_select), regenerated from the same
+ * random stream.  Enqueued on `stream`. */
+int pwa_toy_fields(pwa_plan* h, unsigned long long seed, const long long* idx, long long n,
+                   double* out, long long ld_out, double* p4, long long ld_p4, void* stream);
 
 /* Gram matrix of the MC set, M_kl = sum_i w_i sum_o conj(F_ik,o) F_il,o,
  * in FP64; out[2*ncol*ncol] host, (re, im) row-major. */

@@ -20,7 +20,7 @@ def load_model(config_file):
     vm = VarsManager(rng=np.random.default_rng(0))
     names = init_params(dc.decay_group, vm, dic.get("constrains"))
     float_particles(dc.decay_group, vm, names, dc.particle_property)
-    return dc, vm, Plan(dc.decay_group)
+    return dc, vm, Plan(dc.decay_group, dic.get("data", {}).get("dat_order"))
 
 
 def load_golden(name):

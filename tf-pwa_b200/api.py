@@ -86,9 +86,13 @@ class AmplitudeModel:
     def set_params(self, var):
         self.vm.set_all(var)
 
-    def __call__(self, data):
+    def _engine(self):
         if self._eng is None:
             self._eng = Engine(self.decay_group, self.config.plan, self.vm)
+        return self._eng
+
+    def __call__(self, data):
+        self._engine()
         if self._cached is not data:
             x = data.numpy_fields()
             self._eng.upload(x, np.ones(x.shape[1]))
@@ -250,7 +254,7 @@ class ConfigLoader:
         self._names = init_params(self.decay_group, self.vm, self.config.get("constrains"))
         float_particles(self.decay_group, self.vm, self._names,
                         self.decay_config.particle_property)
-        self.plan = Plan(self.decay_group)
+        self.plan = Plan(self.decay_group, self.config.get("data", {}).get("dat_order"))
         self.precision = precision
         self._amp = None
         self._data = {}
@@ -277,7 +281,15 @@ class ConfigLoader:
         return load_dat_file(files, len(self.get_dat_order()))
 
     def data_from_p4(self, p4, weight=None, device=None):
-        """EventData from (N, n_final, 4) momenta in dat_order."""
+        """EventData from (N, n_final, 4) momenta in dat_order.  With
+        ``device="cuda"`` the engine's kinematics kernel computes the fields
+        on the GPU (one thread per event); otherwise the host code does."""
+        if device is not None and str(device).startswith("cuda"):
+            import torch
+
+            eng = self.get_amplitude()._engine()
+            x = eng.fields_from_p4(torch.as_tensor(p4, dtype=torch.float64, device=device))
+            return EventData(x, weight)
         x = event_fields(self.plan, p4_dict(p4, self.get_dat_order()), device=device)
         return EventData(x, weight)
 

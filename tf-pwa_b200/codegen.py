@@ -26,6 +26,7 @@ mathematics is the reference's chain contraction
 """
 import itertools
 
+from .kincode import KinCode
 from .particles import bprime_coeff, small_d_weight, two
 
 _HEADER = """
@@ -69,9 +70,10 @@ class ConstLayout:
 class ModelCode:
     """Everything the engine needs to know about the compiled model."""
 
-    def __init__(self, group, plan):
+    def __init__(self, group, plan, order=None):
         self.group = group
         self.plan = plan
+        self.kin = KinCode(plan, order if order is not None else plan.order)
         self.consts = ConstLayout()
         self.columns = []          # per column: (chain index, tuple of ls indices)
         self.chain_columns = []    # per chain: list of global column ids
@@ -241,10 +243,13 @@ class ModelCode:
         return -1
 
     def _emit_loads(self, e):
+        # LDG: read-only global loads; false for fields staged in shared memory
         for f in self.mass_fields:
-            e(f"  const double xm{f} = __ldg(XM + (long long){self.mass_slot[f]} * ld + i);")
+            a = f"XM + (long long){self.mass_slot[f]} * ld + i"
+            e(f"  const double xm{f} = LDG ? __ldg({a}) : *({a});")
         for f in self.angle_fields:
-            e(f"  const R xa{f} = __ldg(XA + (long long){self.angle_slot[f]} * ld + i);")
+            a = f"XA + (long long){self.angle_slot[f]} * ld + i"
+            e(f"  const R xa{f} = LDG ? __ldg({a}) : *({a});")
 
     def _trig(self, e, ci, key, angle):
         """sin/cos of half an angle: computed (and stashed in the forward
@@ -563,7 +568,7 @@ class ModelCode:
         self._mode = "store"
         self._emit_loads(body.append)
         self._emit_forward(body.append)
-        L.append(f"template <typename R, bool STASH>\n__device__ __forceinline__ void model_amp(\n{sig},\n"
+        L.append(f"template <typename R, bool STASH, bool LDG = true>\n__device__ __forceinline__ void model_amp(\n{sig},\n"
                  "    cpx<R>* __restrict__ A, R* __restrict__ st) {")
         L += body
         L += [f"  A[{oj}] = A{oj};" for oj in range(self.nout)]
@@ -572,7 +577,7 @@ class ModelCode:
         self._mode = "load"
         self._emit_loads(body.append)
         self._emit_adjoint(body.append)
-        L.append(f"template <typename R>\n__device__ __forceinline__ void model_adj_stash(\n{sig},\n"
+        L.append(f"template <typename R, bool LDG = true>\n__device__ __forceinline__ void model_adj_stash(\n{sig},\n"
                  "    const cpx<R>* __restrict__ Ab, double* __restrict__ accg,\n"
                  "    double* __restrict__ accs, const R* __restrict__ st) {")
         L += body
@@ -581,7 +586,7 @@ class ModelCode:
         self._mode = "plain"
         self._emit_loads(body.append)
         self._emit_adjoint(body.append)
-        L.append(f"template <typename R>\n__device__ __forceinline__ void model_adj_recompute(\n{sig},\n"
+        L.append(f"template <typename R, bool LDG = true>\n__device__ __forceinline__ void model_adj_recompute(\n{sig},\n"
                  "    const cpx<R>* __restrict__ Ab, double* __restrict__ accg,\n"
                  "    double* __restrict__ accs) {")
         L += body
@@ -590,7 +595,7 @@ class ModelCode:
         self._mode = "plain"
         self._emit_loads(body.append)
         self._emit_columns(body.append)
-        L.append(f"template <typename R>\n__device__ __forceinline__ void model_columns(\n{sig},\n"
+        L.append(f"template <typename R, bool LDG = true>\n__device__ __forceinline__ void model_columns(\n{sig},\n"
                  "    cpx<R>* __restrict__ F) {")
         L += body
         L.append("}\n")
@@ -598,4 +603,15 @@ class ModelCode:
         L.append(f"#define PWA_NF {self.nf}")
         L.append("__device__ constexpr int pwa_fk[PWA_NF] = {" + ", ".join(str(k) for k, _ in fl) + "};")
         L.append("__device__ constexpr int pwa_fo[PWA_NF] = {" + ", ".join(str(o) for _, o in fl) + "};")
+        # dataset step: momenta -> fields, and the phase-space generator;
+        # field j goes to XM row pwa_field_slot[j] (pwa_field_mass[j] = 1) or
+        # XA row pwa_field_slot[j]
+        L.append(self.kin.source())
+        L.append(f"#define PWA_NFIELD_MASS {len(self.mass_fields)}")
+        nf = self.plan.n_fields
+        L.append("__device__ constexpr int pwa_field_mass[PWA_NFIELD] = {" + ", ".join(
+            "1" if j in self.mass_slot else "0" for j in range(nf)) + "};")
+        L.append("__device__ constexpr int pwa_field_slot[PWA_NFIELD] = {" + ", ".join(
+            str(self.mass_slot[j] if j in self.mass_slot else self.angle_slot[j])
+            for j in range(nf)) + "};")
         return "\n".join(L)

@@ -230,3 +230,159 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned pari
   }
   return false;
 }
+
+// ------------------------------------------------------------ kinematics
+// FP64 four-vector algebra for the dataset step (four-momenta -> masses,
+// helicity and alignment angles), restating tf_pwa/angle.py
+// (LorentzVector.rest_vector, Vector3.cross_unit / angle_from,
+// EulerAngle.angle_zx_z_getx, SU2M) one event per thread.
+struct LV {
+  double t, x, y, z;
+};
+struct V3 {
+  double x, y, z;
+};
+struct SU2 {  // [[a, b], [c, d]], complex entries as (re, im)
+  double2 a, b, c, d;
+};
+
+__device__ __forceinline__ LV lv_add(LV p, LV q) { return {p.t + q.t, p.x + q.x, p.y + q.y, p.z + q.z}; }
+__device__ __forceinline__ V3 lv_vec(LV p) { return {p.x, p.y, p.z}; }
+__device__ __forceinline__ double v3_dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ V3 v3_cross(V3 a, V3 b) {
+  return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ __forceinline__ V3 v3_unit(V3 a) {
+  const double n = sqrt(v3_dot(a, a));
+  return {a.x / n, a.y / n, a.z / n};
+}
+// unit(a x b); for (anti)parallel a, b the reference falls back to a x (b + 1)
+__device__ __forceinline__ V3 kin_cross_unit(V3 a, V3 b) {
+  V3 c = v3_cross(a, b);
+  if (sqrt(v3_dot(c, c)) < 1e-14) c = v3_cross(a, V3{b.x + 1.0, b.y + 1.0, b.z + 1.0});
+  return v3_unit(c);
+}
+__device__ __forceinline__ double kin_angle_from(V3 v, V3 x, V3 y) {
+  return atan2(v3_dot(v, y), v3_dot(v, x));
+}
+// Euler angles (alpha, beta; gamma = 0) from frame (z1, x1) to axis z2, and
+// the x axis of the new frame
+__device__ __forceinline__ void kin_angle_zx_z_getx(V3 z1, V3 x1, V3 z2, double* alpha,
+                                                    double* beta, V3* x2) {
+  const V3 u_z1 = v3_unit(z1), u_z2 = v3_unit(z2);
+  const V3 u_y1 = kin_cross_unit(z1, x1);
+  const V3 u_x1 = kin_cross_unit(u_y1, z1);
+  const V3 u_yr = kin_cross_unit(z1, z2);
+  const V3 u_xr = kin_cross_unit(u_yr, z1);
+  *alpha = kin_angle_from(u_xr, u_x1, u_y1);
+  *beta = kin_angle_from(u_z2, u_z1, u_xr);
+  *x2 = kin_cross_unit(u_yr, u_z2);
+}
+// alpha folded into [bias, bias + 2 pi)
+__device__ __forceinline__ double kin_fold(double a, double bias) {
+  const double tp = 2.0 * 3.141592653589793, x = a - bias;
+  return x - tp * floor(x / tp) + bias;
+}
+// `o` boosted into the rest frame of `p`
+__device__ __forceinline__ LV kin_rest_vector(LV p, LV o) {
+  const V3 pb = {-p.x / p.t, -p.y / p.t, -p.z / p.t};
+  const double beta2 = v3_dot(pb, pb);
+  const double gamma = 1.0 / sqrt(1.0 - beta2);
+  const double bp = v3_dot(pb, lv_vec(o));
+  const double gamma2 = beta2 > 1e-14 ? (gamma - 1.0) / beta2 : 0.0;
+  const double s = gamma2 * bp + gamma * o.t;
+  return {gamma * (o.t + bp), o.x + s * pb.x, o.y + s * pb.y, o.z + s * pb.z};
+}
+__device__ __forceinline__ double kin_inv_mass(LV p) {
+  return sqrt(fabs(p.t * p.t - (p.x * p.x + p.y * p.y + p.z * p.z)));
+}
+
+__device__ __forceinline__ double2 c2mul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 c2add(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ SU2 su2_mul(const SU2& p, const SU2& q) {
+  return {c2add(c2mul(p.a, q.a), c2mul(p.b, q.c)), c2add(c2mul(p.a, q.b), c2mul(p.b, q.d)),
+          c2add(c2mul(p.c, q.a), c2mul(p.d, q.c)), c2add(c2mul(p.c, q.b), c2mul(p.d, q.d))};
+}
+__device__ __forceinline__ SU2 su2_inv(const SU2& p) {
+  return {p.d, make_double2(-p.b.x, -p.b.y), make_double2(-p.c.x, -p.c.y), p.a};
+}
+// R_y(beta) R_z(alpha)
+__device__ __forceinline__ SU2 su2_rot_yz(double beta, double alpha) {
+  double s, c, sa, ca;
+  sincos(0.5 * beta, &s, &c);
+  sincos(0.5 * alpha, &sa, &ca);
+  const double2 em = make_double2(ca, -sa), ep = make_double2(ca, sa);
+  return {make_double2(c * em.x, c * em.y), make_double2(-s * ep.x, -s * ep.y),
+          make_double2(s * em.x, s * em.y), make_double2(c * ep.x, c * ep.y)};
+}
+// boost along z to the frame where `p` is at rest: diag(e^-w/2, e^w/2)
+__device__ __forceinline__ SU2 su2_boost_z_from_p(LV p) {
+  const V3 pb = {p.x / p.t, p.y / p.t, p.z / p.t};
+  double beta2 = v3_dot(pb, pb);
+  beta2 = beta2 < 1.0 ? beta2 : 0.0;
+  const double a = exp(0.5 * acosh(1.0 / sqrt(1.0 - beta2)));
+  return {make_double2(1.0 / a, 0.0), make_double2(0.0, 0.0), make_double2(0.0, 0.0),
+          make_double2(a, 0.0)};
+}
+__device__ __forceinline__ void su2_euler(const SU2& m, double* alpha, double* beta,
+                                          double* gamma) {
+  double cb = c2mul(m.a, m.d).x + c2mul(m.b, m.c).x;
+  cb = cb < -1.0 ? -1.0 : (cb > 1.0 ? 1.0 : cb);
+  *beta = acos(cb);
+  const double apg = atan2(m.d.y, m.d.x), amg = -atan2(m.c.y, m.c.x);
+  *alpha = apg + amg;
+  *gamma = apg - amg;
+}
+
+// two-body breakup momentum of a -> b c (0 below threshold)
+__device__ __forceinline__ double kin_pdk(double a, double b, double c) {
+  const double x = (a - b - c) * (a + b + c) * (a - b + c) * (a + b - c);
+  return sqrt(x > 0.0 ? x : 0.0) / (2.0 * a);
+}
+// boost p by velocity beta
+__device__ __forceinline__ LV kin_boost(LV p, V3 beta) {
+  const double b2 = v3_dot(beta, beta);
+  const double g = 1.0 / sqrt(1.0 - b2);
+  const double bp = v3_dot(beta, lv_vec(p));
+  const double g2 = b2 > 0.0 ? (g - 1.0) / b2 : 0.0;
+  const double s = g2 * bp + g * p.t;
+  return {g * (p.t + bp), p.x + s * beta.x, p.y + s * beta.y, p.z + s * beta.z};
+}
+
+// ------------------------------------------------------------ random numbers
+// Philox4x32-10 counter-based generator (Salmon, Moraes, Dror, Shaw,
+// "Parallel random numbers: as easy as 1, 2, 3", SC'11): ten rounds of two
+// 32x32->64 multiplies with the published multipliers and Weyl key
+// increments.  Counter = (event index, draw number), key = seed, so any
+// event can be regenerated from its index alone.
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    if (r) {
+      k.x += 0x9E3779B9u;
+      k.y += 0xBB67AE85u;
+    }
+    const unsigned lo0 = 0xD2511F53u * c.x, hi0 = __umulhi(0xD2511F53u, c.x);
+    const unsigned lo1 = 0xCD9E8D57u * c.z, hi1 = __umulhi(0xCD9E8D57u, c.z);
+    c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+  }
+  return c;
+}
+// 53-bit uniform double in [0, 1) from two 32-bit words
+__device__ __forceinline__ double u01_53(unsigned a, unsigned b) {
+  return ((double)(a >> 5) * 67108864.0 + (double)(b >> 6)) * (1.0 / 9007199254740992.0);
+}
+// n uniform doubles of event `i` under `seed` (draw j uses counter word 2 = j/2)
+template <int N>
+__device__ __forceinline__ void event_uniforms(unsigned long long seed, unsigned long long i,
+                                               double (&u)[N]) {
+  const uint2 key = make_uint2((unsigned)seed, (unsigned)(seed >> 32));
+#pragma unroll
+  for (int j = 0; j < (N + 1) / 2; ++j) {
+    const uint4 r = philox4x32_10(make_uint4((unsigned)i, (unsigned)(i >> 32), (unsigned)j, 0u), key);
+    u[2 * j] = u01_53(r.x, r.y);
+    if (2 * j + 1 < N) u[2 * j + 1] = u01_53(r.z, r.w);
+  }
+}

@@ -730,3 +730,100 @@ extern "C" __global__ void pwa_reduce_multi(const double* __restrict__ tile_part
     if (lane == 0) out[q] = s;
   }
 }
+
+// ---------------------------------------------------------------------------
+// Dataset step on the device (model_kin / model_genbod are generated per
+// model).  One event per thread, grid-stride, FP64.
+//
+// pwa_fields_from_p4: final-state momenta, rows (4 f + c) of P4 with stride
+// ld_in (c = E, px, py, pz; finals in dat_order; parent rest frame) -> every
+// plan field, row j of OUT with stride ld_out (plan order).
+extern "C" __global__ void __launch_bounds__(PWA_TPB)
+    pwa_fields_from_p4(const double* __restrict__ P4, long long n, long long ld_in,
+                       double* __restrict__ out, long long ld_out) {
+  for (long long i = (long long)blockIdx.x * PWA_TPB + threadIdx.x; i < n;
+       i += (long long)gridDim.x * PWA_TPB) {
+    LV P[PWA_NFIN];
+#pragma unroll
+    for (int f = 0; f < PWA_NFIN; ++f)
+      P[f] = LV{__ldg(P4 + (4LL * f) * ld_in + i), __ldg(P4 + (4LL * f + 1) * ld_in + i),
+                __ldg(P4 + (4LL * f + 2) * ld_in + i), __ldg(P4 + (4LL * f + 3) * ld_in + i)};
+    double F[PWA_NFIELD];
+    model_kin(P, F);
+#pragma unroll
+    for (int j = 0; j < PWA_NFIELD; ++j) out[(long long)j * ld_out + i] = F[j];
+  }
+}
+
+// Toy selection.  Candidate event e = first + i is drawn from the Philox
+// stream (seed, e): a GENBOD phase-space event accepted with probability
+// weight / max weight; for signal (flat = 0) its fields are formed in shared
+// memory and sum |A|^2 evaluated (FP64); with fmax > 0 the candidate is kept
+// if u fmax < sum |A|^2 (the accept-reject of tf_pwa/applications.py:
+// 428-453).  out[i] = sum |A|^2 of a kept signal candidate, 1 for a kept
+// flat one, -1 otherwise.  fmax <= 0 applies the phase-space step only
+// (a first pass that finds the maximum).
+extern "C" __global__ void __launch_bounds__(PWA_TPB)
+    pwa_toy_select(const Consts C, unsigned long long seed, long long first, long long n,
+                   double fmax, int flat, double* __restrict__ out) {
+  extern __shared__ double sfield[];  // [PWA_NFIELD][PWA_TPB]: XM rows, then XA rows
+  constexpr int NM = PWA_NFIELD_MASS;
+  double* sXM = sfield;
+  double* sXA = sfield + NM * PWA_TPB;
+  const int tid = threadIdx.x;
+  for (long long i = (long long)blockIdx.x * PWA_TPB + tid; i < n;
+       i += (long long)gridDim.x * PWA_TPB) {
+    double U[PWA_NDRAW];
+    event_uniforms(seed, (unsigned long long)(first + i), U);
+    LV P[PWA_NFIN];
+    const double wps = model_genbod(U, P);
+    double res = -1.0;
+    if (U[PWA_NDRAW - 2] < wps) {
+      if (flat) {
+        res = 1.0;
+      } else {
+        double F[PWA_NFIELD];
+        model_kin(P, F);
+#pragma unroll
+        for (int j = 0; j < PWA_NFIELD; ++j)
+          (pwa_field_mass[j] ? sXM : sXA)[pwa_field_slot[j] * PWA_TPB + tid] = F[j];
+        cpx<double> A[PWA_NOUT];
+        model_amp<double, false, false>(C, sXA, sXM, PWA_TPB, tid, A, nullptr);
+        double f = 0.0;
+#pragma unroll
+        for (int o = 0; o < PWA_NOUT; ++o) f += cabs2(A[o]);
+        res = (fmax <= 0.0 || U[PWA_NDRAW - 1] * fmax < f) ? f : -1.0;
+      }
+    }
+    out[i] = res;
+  }
+}
+
+// Fields (and optionally momenta) of selected candidates, regenerated from
+// their event numbers idx[i]: row j of OUT (stride ld_out) in plan order,
+// P4 rows (4 f + c) with stride ld_p4 when P4 is not null.
+extern "C" __global__ void __launch_bounds__(PWA_TPB)
+    pwa_toy_fields(unsigned long long seed, const long long* __restrict__ idx, long long n,
+                   double* __restrict__ out, long long ld_out, double* __restrict__ P4,
+                   long long ld_p4) {
+  for (long long i = (long long)blockIdx.x * PWA_TPB + threadIdx.x; i < n;
+       i += (long long)gridDim.x * PWA_TPB) {
+    double U[PWA_NDRAW];
+    event_uniforms(seed, (unsigned long long)__ldg(idx + i), U);
+    LV P[PWA_NFIN];
+    model_genbod(U, P);
+    double F[PWA_NFIELD];
+    model_kin(P, F);
+#pragma unroll
+    for (int j = 0; j < PWA_NFIELD; ++j) out[(long long)j * ld_out + i] = F[j];
+    if (P4) {
+#pragma unroll
+      for (int f = 0; f < PWA_NFIN; ++f) {
+        P4[(4LL * f) * ld_p4 + i] = P[f].t;
+        P4[(4LL * f + 1) * ld_p4 + i] = P[f].x;
+        P4[(4LL * f + 2) * ld_p4 + i] = P[f].y;
+        P4[(4LL * f + 3) * ld_p4 + i] = P[f].z;
+      }
+    }
+  }
+}

@@ -29,7 +29,8 @@ struct Kernels {
   cudaKernel_t eval_f64 = nullptr, eval_f32 = nullptr, reduce = nullptr, pdf_f64 = nullptr,
                pdf_f32 = nullptr, columns_f64 = nullptr, gram_f64 = nullptr, sum_rows = nullptr,
                to_f32 = nullptr, cache_f32 = nullptr, eval_cached = nullptr,
-               eval_cached_direct = nullptr, eval_cached_wred = nullptr, eval_multi = nullptr, reduce_multi = nullptr;
+               eval_cached_direct = nullptr, eval_cached_wred = nullptr, eval_multi = nullptr, reduce_multi = nullptr,
+               fields_from_p4 = nullptr, toy_select = nullptr, toy_fields = nullptr;
 };
 
 }  // namespace
@@ -39,6 +40,7 @@ struct pwa_plan {
   cudaLibrary_t lib = nullptr;
   Kernels k;
   int n_mass = 0, n_angle = 0, ncol = 0, nout = 0, nshape = 0, nconst = 0, nacc = 0, tpb = 128;
+  bool has_genbod = false;  // the model source carries a phase-space generator
   int regs[2] = {0, 0};
   long long local_bytes[2] = {0, 0};
   int device = 0, sms = 0;
@@ -226,6 +228,8 @@ int pwa_plan_create(const char* src, size_t src_len, int n_mass, int n_angle, in
     return set_err(h, PWA_ERR_ARG, "invalid plan sizes");
   }
   h->n_mass = n_mass;
+  h->has_genbod =
+      std::string(src, src_len).find("#define PWA_HAS_GENBOD 1") != std::string::npos;
   h->n_angle = n_angle;
   h->ncol = ncol;
   h->nout = nout;
@@ -258,6 +262,9 @@ int pwa_plan_create(const char* src, size_t src_len, int n_mass, int n_angle, in
             {"pwa_eval_cached", &h->k.eval_cached},
             {"pwa_eval_cached_direct", &h->k.eval_cached_direct},
             {"pwa_eval_cached_wred", &h->k.eval_cached_wred},
+            {"pwa_fields_from_p4", &h->k.fields_from_p4},
+            {"pwa_toy_select", &h->k.toy_select},
+            {"pwa_toy_fields", &h->k.toy_fields},
             {"pwa_eval_multi", &h->k.eval_multi},   {"pwa_reduce_multi", &h->k.reduce_multi}};
   for (auto& e : ks) CU(cudaLibraryGetKernel(e.slot, h->lib, e.name));
   for (int p = 0; p < 2; ++p) {
@@ -417,6 +424,59 @@ int pwa_eval_pdf(pwa_plan* h, const double* consts, int precision, long long beg
   if (rc) return rc;
   CU(cudaStreamSynchronize(s));
   return PWA_OK;
+}
+
+int pwa_fields_from_p4(pwa_plan* h, const double* p4, long long n, long long ld_in, double* out,
+                       long long ld_out, void* stream) {
+  if (!h) return PWA_ERR_ARG;
+  if (n < 0 || (n > 0 && (!p4 || !out || ld_in < n || ld_out < n)))
+    return set_err(h, PWA_ERR_ARG, "invalid fields_from_p4 arguments");
+  if (n == 0) return PWA_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  void* args[] = {(void*)&p4, &n, &ld_in, &out, &ld_out};
+  long long nb = (n + h->tpb - 1) / h->tpb;
+  if (nb > 16LL * h->sms) nb = 16LL * h->sms;
+  return launch(h, h->k.fields_from_p4, dim3((int)nb), dim3(h->tpb), args, s);
+}
+
+int pwa_toy_select(pwa_plan* h, const double* consts, unsigned long long seed, long long first,
+                   long long n, double fmax, int flat, double* out, void* stream) {
+  if (!h) return PWA_ERR_ARG;
+  if (!h->has_genbod)
+    return set_err(h, PWA_ERR_STATE, "model has no phase-space generator (masses missing)");
+  if (n < 0 || first < 0 || (n > 0 && !out) || (!flat && !consts))
+    return set_err(h, PWA_ERR_ARG, "invalid toy_select arguments");
+  if (n == 0) return PWA_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  std::vector<double> cbuf(h->nconst, 0.0);
+  if (consts) cbuf.assign(consts, consts + h->nconst);
+  void* args[] = {cbuf.data(), &seed, &first, &n, &fmax, &flat, &out};
+  const size_t smem = sizeof(double) * (size_t)(h->n_mass + h->n_angle) * h->tpb;
+  if (smem > 48 * 1024)
+    CU(cudaFuncSetAttribute((const void*)h->k.toy_select,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  long long nb = (n + h->tpb - 1) / h->tpb;
+  if (nb > 16LL * h->sms) nb = 16LL * h->sms;
+  cudaError_t e = cudaLaunchKernel((const void*)h->k.toy_select, dim3((int)nb), dim3(h->tpb), args,
+                                   smem, s);
+  if (e != cudaSuccess)
+    return set_err(h, PWA_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+  return PWA_OK;
+}
+
+int pwa_toy_fields(pwa_plan* h, unsigned long long seed, const long long* idx, long long n,
+                   double* out, long long ld_out, double* p4, long long ld_p4, void* stream) {
+  if (!h) return PWA_ERR_ARG;
+  if (!h->has_genbod)
+    return set_err(h, PWA_ERR_STATE, "model has no phase-space generator (masses missing)");
+  if (n < 0 || (n > 0 && (!idx || !out || ld_out < n || (p4 && ld_p4 < n))))
+    return set_err(h, PWA_ERR_ARG, "invalid toy_fields arguments");
+  if (n == 0) return PWA_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  void* args[] = {&seed, (void*)&idx, &n, &out, &ld_out, &p4, &ld_p4};
+  long long nb = (n + h->tpb - 1) / h->tpb;
+  if (nb > 16LL * h->sms) nb = 16LL * h->sms;
+  return launch(h, h->k.toy_fields, dim3((int)nb), dim3(h->tpb), args, s);
 }
 
 int pwa_build_gram(pwa_plan* h, const double* consts, void* stream, double* out) {

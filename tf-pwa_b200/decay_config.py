@@ -264,6 +264,8 @@ def init_params(group, vm, constrains=None):
     names = {"mass": {}, "width": {}, "total": [], "g_ls": {}}
     for p in group.resonances:
         head = var_name(str(p))
+        if p.model == "one":
+            continue  # fixed lineshape: no parameters (ParticleOne.init_params)
         if p.mass is not None or True:
             vm.add_real_var(f"{head}_mass", value=p.mass if p.mass is not None else 0.0,
                             trainable=False)

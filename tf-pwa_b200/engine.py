@@ -60,6 +60,10 @@ def load_library(path=LIB_PATH):
     lib.pwa_pool_fill.argtypes = [vp, ll, dp, vp, vp, vp, ll, ll, vp]
     lib.pwa_pieces_multi.argtypes = [vp, i, llp, llp, dp, dp, ctypes.c_double, vp, dp]
     lib.pwa_eval_noalloc.argtypes = [vp, dp, vp, vp, vp, ll, ll, ll, vp, vp]
+    ull = ctypes.c_ulonglong
+    lib.pwa_fields_from_p4.argtypes = [vp, vp, ll, ll, vp, ll, vp]
+    lib.pwa_toy_select.argtypes = [vp, dp, ull, ll, ll, ctypes.c_double, i, vp, vp]
+    lib.pwa_toy_fields.argtypes = [vp, ull, vp, ll, vp, ll, vp, ll, vp]
     lib.pwa_plan_destroy.argtypes = [vp]
     lib.pwa_compile_only.argtypes = [cp, sz, i, cp, cp, sz]
     lib.pwa_upload_events.argtypes = [vp, vp, vp, vp, ll, ll, i, vp]
@@ -83,7 +87,8 @@ EXPORTED = ("pwa_plan_create", "pwa_plan_destroy", "pwa_compile_only", "pwa_uplo
             "pwa_eval_cached_enqueue", "pwa_set_param_layout", "pwa_pieces_cached",
             "pwa_nll_grad_cached", "pwa_set_cached_variant", "pwa_pool_reserve",
             "pwa_pool_alloc", "pwa_pool_free", "pwa_pool_fill", "pwa_pieces_multi",
-            "pwa_eval_noalloc", "pwa_plan_info", "pwa_last_error")
+            "pwa_eval_noalloc", "pwa_fields_from_p4", "pwa_toy_select", "pwa_toy_fields",
+            "pwa_plan_info", "pwa_last_error")
 
 
 class PWAError(RuntimeError):
@@ -127,11 +132,11 @@ def combine_pieces(vec, P):
 class Engine:
     """A compiled model bound to a device: events, constants, evaluation."""
 
-    def __init__(self, group, plan, vm, tpb=128, compile=True):
+    def __init__(self, group, plan, vm, tpb=128, compile=True, order=None):
         self.group = group
         self.plan = plan
         self.vm = vm
-        self.code = ModelCode(group, plan)
+        self.code = ModelCode(group, plan, order)
         self.src = self.code.source()
         self.tpb = tpb
         self.h = None
@@ -536,6 +541,47 @@ class Engine:
                                                        ctypes.byref(nll), _dptr(g)),
                     "pwa_nll_grad_cached")
         return nll.value, g
+
+    # ------------------------------------------------------------ dataset step
+    def fields_from_p4(self, p4):
+        """Event fields (n_fields, N) on the device from final-state momenta
+        ``p4``: CUDA tensor (N, n_final, 4), finals in the plan's order."""
+        import torch
+
+        n = p4.shape[0]
+        soa = p4.to(torch.float64).permute(1, 2, 0).reshape(-1, n).contiguous()
+        out = torch.empty((self.plan.n_fields, n), dtype=torch.float64, device=p4.device)
+        self._check(load_library().pwa_fields_from_p4(self.h, soa.data_ptr(), n, n,
+                                                      out.data_ptr(), n, 0),
+                    "pwa_fields_from_p4")
+        return out
+
+    def toy_select(self, C, seed, first, n, fmax, flat, out):
+        """Accept flags / |A|^2 of candidates first..first+n into the CUDA
+        tensor ``out`` (see pwa_toy_select)."""
+        Cp = None if C is None else _dptr(np.ascontiguousarray(C, np.float64))
+        self._check(load_library().pwa_toy_select(self.h, Cp, int(seed), int(first), int(n),
+                                                  float(fmax), int(flat), out.data_ptr(),
+                                                  0), "pwa_toy_select")
+
+    def toy_fields(self, seed, idx, with_p4=False):
+        """Fields (n_fields, len(idx)) and optionally momenta (len, n_final, 4)
+        of candidates ``idx`` (int64 CUDA tensor)."""
+        import torch
+
+        n = idx.shape[0]
+        idx = idx.to(torch.int64).contiguous()
+        out = torch.empty((self.plan.n_fields, n), dtype=torch.float64, device=idx.device)
+        p4 = None
+        if with_p4:
+            p4 = torch.empty((4 * self.code.kin.nfin, n), dtype=torch.float64, device=idx.device)
+        self._check(load_library().pwa_toy_fields(self.h, int(seed), idx.data_ptr(), n,
+                                                  out.data_ptr(), n,
+                                                  None if p4 is None else p4.data_ptr(), n,
+                                                  0), "pwa_toy_fields")
+        if with_p4:
+            return out, p4.reshape(self.code.kin.nfin, 4, n).permute(2, 0, 1)
+        return out
 
     def set_cached_variant(self, variant):
         self._check(load_library().pwa_set_cached_variant(self.h, int(variant)),

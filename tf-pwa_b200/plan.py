@@ -49,8 +49,11 @@ class ChainTopology:
 class Plan:
     """Field layout + per-chain references into it."""
 
-    def __init__(self, group):
+    def __init__(self, group, order=None):
         self.group = group
+        # order of the final particles in momentum input (the config's
+        # data.dat_order; default: the decay group's finals)
+        self.order = [str(o) for o in (order if order is not None else group.outs)]
         self.topos = []          # list of ChainTopology (first chain of each)
         self.chain_topo = []     # per chain: index into self.topos
         for c in group:
