@@ -398,7 +398,7 @@ def main():
     k_kernel = args.steps
     t_kernel = timed(lambda: eng.eval_cached_enqueue(ck), k_kernel)
     variants = {}
-    for var in (0, 1, 2):
+    for var in (0, 1, 2, 3):
         eng.set_cached_variant(var)
         variants[var] = {"kernel_us": 1e6 * timed(lambda: eng.eval_cached_enqueue(ck), k_kernel)
                          / k_kernel,

@@ -136,8 +136,10 @@ int pwa_cache_data(pwa_plan* h, const double* consts, void* stream);
  * copies, 1 = direct loads with four blocks per SM and per-thread FP64
  * column sums, 2 = direct loads with the column sums of each warp's 32
  * events reduce-scattered in FP32 before FP64 accumulation (register use
- * independent of the column count), -1 = automatic (default: 1 for up to
- * 12 columns, else 2). */
+ * independent of the column count), 3 = shared-memory ring (two stages)
+ * whose consumers read their columns from shared memory and reduce-scatter
+ * the column sums, -1 = automatic (default: 1 for up to 12 columns, else
+ * 2). */
 int pwa_set_cached_variant(pwa_plan* h, int variant);
 
 /* Data-term kernels on the cache with column couplings ck[2*ncol]

@@ -195,6 +195,11 @@ class FCN:
     def grad(self, x=None):
         return self.get_nll_grad(x)[1]
 
+    def torch_nll(self, x):
+        """NLL(x) as a torch scalar whose backward is the engine's adjoint
+        gradient (``NLLFunction``)."""
+        return NLLFunction.apply(x, self)
+
     def nll_grad_hessian(self, x=None, step=1e-4):
         """Hessian by differencing the adjoint gradient: 4-point central
         stencil per parameter (error O(h^4)), symmetrised."""
@@ -213,6 +218,35 @@ class FCN:
             H[i] = (gs[0] - 8 * gs[1] + 8 * gs[2] - gs[3]) / (12 * h)
         self._set(x0)
         return nll, g0, 0.5 * (H + H.T)
+
+
+class NLLFunction:
+    """The NLL as a differentiable torch operation: forward runs the engine
+    (NLL and adjoint gradient in one evaluation), backward returns the
+    stored gradient times the incoming one.  ``NLLFunction.apply(x, fcn)``
+    with x a float64 tensor of the trainable parameters (vm order)."""
+
+    _fn = None
+
+    @classmethod
+    def apply(cls, x, fcn):
+        if cls._fn is None:
+            import torch
+
+            class _F(torch.autograd.Function):
+                @staticmethod
+                def forward(ctx, xx, f):
+                    nll, g = f.get_nll_grad(xx.detach().cpu().numpy())
+                    ctx.save_for_backward(torch.as_tensor(g, dtype=xx.dtype, device=xx.device))
+                    return xx.new_tensor(float(nll))
+
+                @staticmethod
+                def backward(ctx, gout):
+                    (g,) = ctx.saved_tensors
+                    return gout * g, None
+
+            cls._fn = _F
+        return cls._fn.apply(x, fcn)
 
 
 class FitResult:
@@ -401,3 +435,25 @@ class ConfigLoader:
         self.inv_he = inv
         err = np.sqrt(np.abs(np.diag(inv)))
         return dict(zip(self.vm.trainable_vars, err))
+
+    def cal_fitfractions(self, params={}, mcdata=None, res=None, exclude_res=[], batch=25000,
+                         method="old", fcn=None):
+        """Fit fractions and errors (``config_loader.py:893-916`` ->
+        ``applications.fit_fractions``): (frac, err_frac), keyed by resonance
+        name and by (name_i, name_j) pairs for interference terms.  The MC
+        sample is that of ``fcn`` (default: the last fitted FCN, else the
+        config's phsp); errors use ``self.inv_he`` from get_params_error."""
+        from .fitfractions import fit_fractions
+
+        if hasattr(params, "params"):
+            params = params.params
+        if params:
+            self.set_params(params)
+        if fcn is None:
+            fcn = getattr(self, "_fcn", None) or self.get_fcn(
+                None if mcdata is None else [self._merge(self.get_data("data")), mcdata, None])
+        if res is None:
+            res = sorted(set(str(p) for p in self.decay_group.resonances) - set(exclude_res))
+        frac, err, _ = fit_fractions(fcn.eng, self.vm, res, getattr(self, "inv_he", None),
+                                     use_gram=fcn.use_gram)
+        return frac, err

@@ -291,6 +291,71 @@ struct CCoup {
 #endif
 #define PWA_CACHE_NA (1 + 2 * PWA_NCOL)
 #define PWA_WAIT_LIMIT (1u << 22)
+// Blocks per group of the two-level partial reduction, and the most groups
+// a launch may have (the ticket buffer holds 2 + PWA_MAX_GROUPS counters).
+#define PWA_GROUP 16
+#define PWA_MAX_GROUPS 4096
+
+// Sum of the block partials (rows of `na` doubles, one per block) by the
+// last block to finish: thread j owns accumulators j, j + PWA_TPB, ...,
+// reads the rows in order (a warp reads consecutive accumulators of a row:
+// coalesced) with four interleaved partial sums, so many loads are in
+// flight.  The order depends only on the row count: reproducible.
+__device__ __forceinline__ void last_block_sum(const double* __restrict__ partials, int nrows,
+                                               int na, double* __restrict__ out) {
+  for (int j = threadIdx.x; j < na; j += PWA_TPB) {
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    int b = 0;
+#pragma unroll 4
+    for (; b + 4 <= nrows; b += 4) {
+      s0 += __ldcg(partials + (long long)b * na + j);
+      s1 += __ldcg(partials + (long long)(b + 1) * na + j);
+      s2 += __ldcg(partials + (long long)(b + 2) * na + j);
+      s3 += __ldcg(partials + (long long)(b + 3) * na + j);
+    }
+    for (; b < nrows; ++b) s0 += __ldcg(partials + (long long)b * na + j);
+    out[j] = (s0 + s1) + (s2 + s3);
+  }
+}
+
+// Ordered two-level reduction of the block partials (row b = block b's
+// `na` sums, written and fenced by every block before the call).  The last
+// block of each group of PWA_GROUP consecutive blocks (ticket[2 + g])
+// sums the group's rows in block order into group row g (stored after the
+// block rows); the last group (ticket[0]) sums the group rows in order into
+// out.  Returns true in that one block.  Counters are reset for the next
+// launch; the order depends only on the grid size, so results are
+// bitwise reproducible.  *s_flag is a __shared__ int of the caller.
+__device__ __forceinline__ bool grouped_sum(double* __restrict__ partials,
+                                            unsigned int* __restrict__ ticket, int na,
+                                            double* __restrict__ out, int* s_flag) {
+  const int nb = (int)gridDim.x, g = (int)blockIdx.x / PWA_GROUP;
+  const int ng = (nb + PWA_GROUP - 1) / PWA_GROUP;
+  const int gs = min(PWA_GROUP, nb - g * PWA_GROUP);
+  double* grows = partials + (long long)nb * na;
+  if (threadIdx.x == 0) *s_flag = (atomicAdd(ticket + 2 + g, 1u) == (unsigned)gs - 1);
+  __syncthreads();
+  if (!*s_flag) return false;
+  __threadfence();
+  for (int j = threadIdx.x; j < na; j += PWA_TPB) {
+    double s[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int r = 0; r < PWA_GROUP; ++r)
+      if (r < gs) s[r & 3] += __ldcg(partials + (long long)(g * PWA_GROUP + r) * na + j);
+    grows[(long long)g * na + j] = (s[0] + s[1]) + (s[2] + s[3]);
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ticket[2 + g] = 0u;
+    *s_flag = (atomicAdd(ticket, 1u) == (unsigned)ng - 1);
+  }
+  __syncthreads();
+  if (!*s_flag) return false;
+  __threadfence();
+  last_block_sum(grows, ng, na, out);
+  return true;
+}
 
 // Persistent streaming kernel over the column cache.  Thread 0 keeps
 // PWA_STAGES tiles in flight with cp.async.bulk into a shared-memory ring
@@ -415,17 +480,7 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB)
   if (tid == 0 && s_err) atomicOr((unsigned int*)(ticket + 1), 1u);
   __threadfence();
   __syncthreads();
-  if (tid == 0) s_last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
-  __syncthreads();
-  if (!s_last) return;
-  __threadfence();
-  // last block: fixed-order sums over blocks, one warp per accumulator
-  for (int j = warp; j < NA; j += PWA_TPB / 32) {
-    double s = 0.0;
-    for (int bb = lane; bb < (int)gridDim.x; bb += 32) s += __ldcg(partials + (long long)bb * NA + j);
-    s = warp_sum(s);
-    if (lane == 0) out[j] = s;
-  }
+  if (!grouped_sum(partials, ticket, NA, out, &s_last)) return;
   __syncthreads();
   if (tid == 0) {
     const unsigned e = atomicOr((unsigned int*)(ticket + 1), 0u);
@@ -519,16 +574,7 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, 4)
   }
   __threadfence();
   __syncthreads();
-  if (tid == 0) s_last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
-  __syncthreads();
-  if (!s_last) return;
-  __threadfence();
-  for (int j = warp; j < NA; j += PWA_TPB / 32) {
-    double s2 = 0.0;
-    for (int bb = lane; bb < (int)gridDim.x; bb += 32) s2 += __ldcg(partials + (long long)bb * NA + j);
-    s2 = warp_sum(s2);
-    if (lane == 0) out[j] = s2;
-  }
+  if (!grouped_sum(partials, ticket, NA, out, &s_last)) return;
   __syncthreads();
   if (tid == 0) {
     out[NA] = (double)atomicOr((unsigned int*)(ticket + 1), 0u);
@@ -552,29 +598,44 @@ struct CoupParam {  // couplings from the kernel's parameter block
   const CCoup& c;
   __device__ __forceinline__ double operator()(int i) const { return c.v[i]; }
 };
+struct CoupShared {  // couplings staged in shared memory (read per event, not hoisted)
+  const double* c;
+  __device__ __forceinline__ double operator()(int i) const { return c[i]; }
+};
 struct CoupGlobal {  // couplings from global memory (one row per request)
   const double* __restrict__ c;
   __device__ __forceinline__ double operator()(int i) const { return __ldg(c + i); }
 };
 
-// One event of a column tile: returns w * clip_log(f) and fills g (entries
-// 2k, 2k + 1 = re, im of fac * conj(A) F_k, zero beyond 2 * PWA_NCOL).
+// One event of a column tile: returns w * clip_log(f) and adds to g (entries
+// 2k, 2k + 1 = re, im of fac * conj(A) F_k; the caller zeroes g).  The
+// amplitude sums run in two interleaved FP64 partial sums per output to
+// halve the dependent-FMA chain.
 template <class Coup>
 __device__ __forceinline__ double cached_event(const float2 (&v)[PWA_NF], double w,
                                                const Coup& cp, float (&g)[PWA_GPAD]) {
-  double ar[PWA_NOUT], ai[PWA_NOUT];
+  double ar[PWA_NOUT], ai[PWA_NOUT], br2[PWA_NOUT], bi2[PWA_NOUT];
 #pragma unroll
-  for (int o = 0; o < PWA_NOUT; ++o) ar[o] = ai[o] = 0.0;
+  for (int o = 0; o < PWA_NOUT; ++o) ar[o] = ai[o] = br2[o] = bi2[o] = 0.0;
 #pragma unroll
   for (int j = 0; j < PWA_NF; ++j) {
     const int k = pwa_fk[j], o = pwa_fo[j];
     const double cr = cp(2 * k), ci = cp(2 * k + 1);
-    ar[o] = fma(cr, (double)v[j].x, fma(-ci, (double)v[j].y, ar[o]));
-    ai[o] = fma(cr, (double)v[j].y, fma(ci, (double)v[j].x, ai[o]));
+    if (j & 1) {
+      br2[o] = fma(cr, (double)v[j].x, fma(-ci, (double)v[j].y, br2[o]));
+      bi2[o] = fma(cr, (double)v[j].y, fma(ci, (double)v[j].x, bi2[o]));
+    } else {
+      ar[o] = fma(cr, (double)v[j].x, fma(-ci, (double)v[j].y, ar[o]));
+      ai[o] = fma(cr, (double)v[j].y, fma(ci, (double)v[j].x, ai[o]));
+    }
   }
   double f = 0.0;
 #pragma unroll
-  for (int o = 0; o < PWA_NOUT; ++o) f = fma(ar[o], ar[o], fma(ai[o], ai[o], f));
+  for (int o = 0; o < PWA_NOUT; ++o) {
+    ar[o] += br2[o];
+    ai[o] += bi2[o];
+    f = fma(ar[o], ar[o], fma(ai[o], ai[o], f));
+  }
   double dl;
   const double cl = clip_log(f, &dl);
   const double fac = w * dl;
@@ -585,8 +646,6 @@ __device__ __forceinline__ double cached_event(const float2 (&v)[PWA_NF], double
     bi[o] = (float)(-fac * ai[o]);
   }
 #pragma unroll
-  for (int j = 0; j < PWA_GPAD; ++j) g[j] = 0.f;
-#pragma unroll
   for (int j = 0; j < PWA_NF; ++j) {
     const int k = pwa_fk[j], o = pwa_fo[j];
     g[2 * k] = fmaf(br[o], v[j].x, fmaf(-bi[o], v[j].y, g[2 * k]));
@@ -595,11 +654,71 @@ __device__ __forceinline__ double cached_event(const float2 (&v)[PWA_NF], double
   return w * cl;
 }
 
-// four blocks per SM (128 registers) while the column sums fit one
-// reduce-scatter row (up to 16 complex columns), three above
+// four blocks per SM (128 registers)
 #ifndef PWA_WRED_MINB
-#define PWA_WRED_MINB (PWA_GPAD > 32 ? 3 : 4)
+#define PWA_WRED_MINB 4
 #endif
+
+// One event of a tile (its columns v[j] loaded once): returns
+// w * clip_log(f).  The sensitivities of the warp's 32 events are formed 16
+// complex columns at a time and reduce-scattered: gs[m] receives on each
+// lane the warp sum of entry 32 m + lane (entries 2k, 2k + 1 = re, im of
+// fac * conj(A) F_k).  Every lane of the warp must call it (shuffles).
+template <class Coup>
+__device__ __forceinline__ double cached_event_rs(const float2 (&v)[PWA_NF], double w,
+                                                  const Coup& cp, int lane,
+                                                  float (&gs)[PWA_GPAD / 32]) {
+  double ar[PWA_NOUT], ai[PWA_NOUT], br2[PWA_NOUT], bi2[PWA_NOUT];
+#pragma unroll
+  for (int o = 0; o < PWA_NOUT; ++o) ar[o] = ai[o] = br2[o] = bi2[o] = 0.0;
+#pragma unroll
+  for (int j = 0; j < PWA_NF; ++j) {
+    const int k = pwa_fk[j], o = pwa_fo[j];
+    const double cr = cp(2 * k), ci = cp(2 * k + 1);
+    if (j & 1) {
+      br2[o] = fma(cr, (double)v[j].x, fma(-ci, (double)v[j].y, br2[o]));
+      bi2[o] = fma(cr, (double)v[j].y, fma(ci, (double)v[j].x, bi2[o]));
+    } else {
+      ar[o] = fma(cr, (double)v[j].x, fma(-ci, (double)v[j].y, ar[o]));
+      ai[o] = fma(cr, (double)v[j].y, fma(ci, (double)v[j].x, ai[o]));
+    }
+  }
+  double f = 0.0;
+#pragma unroll
+  for (int o = 0; o < PWA_NOUT; ++o) {
+    ar[o] += br2[o];
+    ai[o] += bi2[o];
+    f = fma(ar[o], ar[o], fma(ai[o], ai[o], f));
+  }
+  double dl;
+  const double cl = clip_log(f, &dl);
+  const double fac = w * dl;
+  float br[PWA_NOUT], bi[PWA_NOUT];
+#pragma unroll
+  for (int o = 0; o < PWA_NOUT; ++o) {
+    br[o] = (float)(fac * ar[o]);
+    bi[o] = (float)(-fac * ai[o]);
+  }
+#pragma unroll
+  for (int m = 0; m < PWA_GPAD / 32; ++m) {
+    float g[32];
+#pragma unroll
+    for (int q = 0; q < 32; ++q) g[q] = 0.f;
+#pragma unroll
+    for (int j = 0; j < PWA_NF; ++j) {
+      const int k = pwa_fk[j], o = pwa_fo[j];
+      if (k >= 16 * m && k < 16 * m + 16) {
+        const int q = 2 * (k - 16 * m);
+        g[q] = fmaf(br[o], v[j].x, fmaf(-bi[o], v[j].y, g[q]));
+        g[q + 1] = fmaf(br[o], v[j].y, fmaf(bi[o], v[j].x, g[q + 1]));
+      }
+    }
+    warp_reduce_scatter<32>(g, lane);
+    gs[m] = g[0];
+  }
+  return w * cl;
+}
+
 extern "C" __global__ void __launch_bounds__(PWA_TPB, PWA_WRED_MINB)
     pwa_eval_cached_wred(const CCoup c, const float2* __restrict__ Fc,
                          const double* __restrict__ Wc, long long ntiles,
@@ -610,31 +729,34 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, PWA_WRED_MINB)
   __shared__ double red[PWA_TPB / 32][NA];
   __shared__ int s_last;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const CoupParam cp{c};
+  __shared__ double s_c[2 * PWA_NCOL];
+  for (int j = tid; j < 2 * PWA_NCOL; j += PWA_TPB) s_c[j] = c.v[j];
+  __syncthreads();
+  const CoupShared cp{s_c};
   double acc0 = 0.0;
   double accg[MG];
 #pragma unroll
   for (int j = 0; j < MG; ++j) accg[j] = 0.0;
+#pragma unroll 1
   for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const float2* F = Fc + t * PWA_NF * PWA_TPB + tid;
     float2 v[PWA_NF];
 #pragma unroll
     for (int j = 0; j < PWA_NF; ++j) v[j] = __ldcs(F + j * PWA_TPB);
     const double w = __ldcs(Wc + t * PWA_TPB + tid);
-    float g[PWA_GPAD];
-    acc0 += cached_event(v, w, cp, g);
-    warp_reduce_scatter<PWA_GPAD>(g, lane);
+    float gs[MG];
+    acc0 += cached_event_rs(v, w, cp, lane, gs);
 #pragma unroll
-    for (int j = 0; j < MG; ++j) accg[j] += (double)g[j];
+    for (int m = 0; m < MG; ++m) accg[m] += (double)gs[m];
   }
   {
     const double v0 = warp_sum(acc0);
     if (lane == 0) red[warp][0] = v0;
   }
 #pragma unroll
-  for (int j = 0; j < MG; ++j) {
-    const int idx = MG * lane + j;
-    if (idx < NG) red[warp][1 + idx] = accg[j];
+  for (int m = 0; m < MG; ++m) {
+    const int idx = 32 * m + lane;  // entry `lane` of column group m
+    if (idx < NG) red[warp][1 + idx] = accg[m];
   }
   __syncthreads();
   for (int j = tid; j < NA; j += PWA_TPB) {
@@ -645,19 +767,166 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, PWA_WRED_MINB)
   }
   __threadfence();
   __syncthreads();
-  if (tid == 0) s_last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
-  __syncthreads();
-  if (!s_last) return;
-  __threadfence();
-  for (int j = warp; j < NA; j += PWA_TPB / 32) {
-    double s2 = 0.0;
-    for (int bb = lane; bb < (int)gridDim.x; bb += 32) s2 += __ldcg(partials + (long long)bb * NA + j);
-    s2 = warp_sum(s2);
-    if (lane == 0) out[j] = s2;
-  }
+  if (!grouped_sum(partials, ticket, NA, out, &s_last)) return;
   __syncthreads();
   if (tid == 0) {
     out[NA] = (double)atomicOr((unsigned int*)(ticket + 1), 0u);
+    out[NA + 1] = seq;
+    ticket[0] = 0u;
+    ticket[1] = 0u;
+    __threadfence_system();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Shared-memory ring with register-light consumers.  Thread 0 keeps
+// PWA_RSTAGES tiles of the column cache in flight with cp.async.bulk (as in
+// pwa_eval_cached); every thread evaluates its event of the current tile
+// reading its columns from shared memory (FP64 amplitude), then forms the
+// column sensitivities 16 complex columns at a time and reduce-scatters each
+// group of 32 FP32 values across the warp, so a lane carries PWA_GPAD / 32
+// FP64 accumulators.  The bytes in flight are the ring's, not registers, so
+// the kernel keeps HBM busy at low occupancy.  Same outputs and protocol as
+// pwa_eval_cached.
+#ifndef PWA_RSTAGES
+#define PWA_RSTAGES 2
+#endif
+extern "C" __global__ void __launch_bounds__(PWA_TPB)
+    pwa_eval_cached_ring2(const CCoup c, const float2* __restrict__ Fc,
+                          const double* __restrict__ Wc, long long ntiles,
+                          double* __restrict__ partials, unsigned int* __restrict__ ticket,
+                          double* __restrict__ out, double seq) {
+  constexpr int NA = PWA_CACHE_NA;
+  constexpr int NG = 2 * PWA_NCOL, MG = PWA_GPAD / 32;
+  constexpr unsigned TILE_F = PWA_NF * PWA_TPB * sizeof(float2);
+  constexpr unsigned TILE_W = PWA_TPB * sizeof(double);
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  float2* sF = (float2*)smem_raw;                                    // [RSTAGES][NF][TPB]
+  double* sW = (double*)(smem_raw + PWA_RSTAGES * TILE_F);           // [RSTAGES][TPB]
+  __shared__ __align__(8) unsigned long long full[PWA_RSTAGES];
+  __shared__ double red[PWA_TPB / 32][NA];
+  __shared__ int s_last, s_err;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) {
+    s_err = 0;
+    for (int st = 0; st < PWA_RSTAGES; ++st) mbar_init(&full[st], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  const long long G = gridDim.x, b0 = blockIdx.x;
+  if (tid == 0) {
+    for (int st = 0; st < PWA_RSTAGES; ++st) {
+      const long long t = b0 + st * G;
+      if (t < ntiles) {
+        mbar_expect_tx(&full[st], TILE_F + TILE_W);
+        bulk_g2s(sF + (long long)st * PWA_NF * PWA_TPB, Fc + t * PWA_NF * PWA_TPB, TILE_F, &full[st]);
+        bulk_g2s(sW + st * PWA_TPB, Wc + t * PWA_TPB, TILE_W, &full[st]);
+      }
+    }
+  }
+  const CoupParam cp{c};
+  double acc0 = 0.0;
+  double accg[MG];
+#pragma unroll
+  for (int j = 0; j < MG; ++j) accg[j] = 0.0;
+  int it = 0;
+  for (long long t = b0; t < ntiles; t += G, ++it) {
+    const int st = it % PWA_RSTAGES;
+    const unsigned par = (unsigned)((it / PWA_RSTAGES) & 1);
+    if (!mbar_wait(&full[st], par, PWA_WAIT_LIMIT)) {
+      s_err = 1;  // benign race: any thread may set it
+    }
+    __syncthreads();
+    if (s_err) break;
+    const float2* F = sF + (long long)st * PWA_NF * PWA_TPB + tid;
+    const double w = sW[st * PWA_TPB + tid];
+    double ar[PWA_NOUT], ai[PWA_NOUT];
+#pragma unroll
+    for (int o = 0; o < PWA_NOUT; ++o) ar[o] = ai[o] = 0.0;
+#pragma unroll
+    for (int j = 0; j < PWA_NF; ++j) {
+      const int k = pwa_fk[j], o = pwa_fo[j];
+      const float2 v = F[j * PWA_TPB];
+      const double cr = cp(2 * k), ci = cp(2 * k + 1);
+      ar[o] = fma(cr, (double)v.x, fma(-ci, (double)v.y, ar[o]));
+      ai[o] = fma(cr, (double)v.y, fma(ci, (double)v.x, ai[o]));
+    }
+    double f = 0.0;
+#pragma unroll
+    for (int o = 0; o < PWA_NOUT; ++o) f = fma(ar[o], ar[o], fma(ai[o], ai[o], f));
+    double dl;
+    const double cl = clip_log(f, &dl);
+    acc0 = fma(w, cl, acc0);
+    const double fac = w * dl;
+    float br[PWA_NOUT], bi[PWA_NOUT];
+#pragma unroll
+    for (int o = 0; o < PWA_NOUT; ++o) {
+      br[o] = (float)(fac * ar[o]);
+      bi[o] = (float)(-fac * ai[o]);
+    }
+#pragma unroll
+    for (int m = 0; m < MG; ++m) {
+      float g[32];
+#pragma unroll
+      for (int q = 0; q < 32; ++q) g[q] = 0.f;
+#pragma unroll
+      for (int j = 0; j < PWA_NF; ++j) {
+        const int k = pwa_fk[j], o = pwa_fo[j];
+        if (k >= 16 * m && k < 16 * m + 16) {
+          const float2 v = F[j * PWA_TPB];
+          const int q = 2 * (k - 16 * m);
+          g[q] = fmaf(br[o], v.x, fmaf(-bi[o], v.y, g[q]));
+          g[q + 1] = fmaf(br[o], v.y, fmaf(bi[o], v.x, g[q + 1]));
+        }
+      }
+      warp_reduce_scatter<32>(g, lane);
+      accg[m] += (double)g[0];
+    }
+    __syncthreads();  // stage st fully consumed
+    if (tid == 0) {
+      const long long tn = t + (long long)PWA_RSTAGES * G;
+      if (tn < ntiles) {
+        fence_proxy_async_smem();
+        mbar_expect_tx(&full[st], TILE_F + TILE_W);
+        bulk_g2s(sF + (long long)st * PWA_NF * PWA_TPB, Fc + tn * PWA_NF * PWA_TPB, TILE_F,
+                 &full[st]);
+        bulk_g2s(sW + st * PWA_TPB, Wc + tn * PWA_TPB, TILE_W, &full[st]);
+      }
+    }
+  }
+  if (s_err) {
+    // drain: wait (bounded) for every copy this block issued before exiting
+    const int issued = it + PWA_RSTAGES;
+    if (tid == 0)
+      for (int k2 = it; k2 < issued; ++k2) {
+        const long long t2 = b0 + (long long)k2 * G;
+        if (t2 < ntiles) mbar_wait(&full[k2 % PWA_RSTAGES], (unsigned)((k2 / PWA_RSTAGES) & 1), PWA_WAIT_LIMIT);
+      }
+  }
+  {
+    const double v0 = warp_sum(acc0);
+    if (lane == 0) red[warp][0] = v0;
+  }
+#pragma unroll
+  for (int m = 0; m < MG; ++m) {
+    const int idx = 32 * m + lane;  // entry `lane` of column group m
+    if (idx < NG) red[warp][1 + idx] = accg[m];
+  }
+  __syncthreads();
+  for (int j = tid; j < NA; j += PWA_TPB) {
+    double s2 = 0.0;
+#pragma unroll
+    for (int w2 = 0; w2 < PWA_TPB / 32; ++w2) s2 += red[w2][j];
+    partials[(long long)blockIdx.x * NA + j] = s2;
+  }
+  if (tid == 0 && s_err) atomicOr((unsigned int*)(ticket + 1), 1u);
+  __threadfence();
+  __syncthreads();
+  if (!grouped_sum(partials, ticket, NA, out, &s_last)) return;
+  __syncthreads();
+  if (tid == 0) {
+    const unsigned e = atomicOr((unsigned int*)(ticket + 1), 0u);
+    out[NA] = (double)e;
     out[NA + 1] = seq;
     ticket[0] = 0u;
     ticket[1] = 0u;
@@ -680,7 +949,7 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, PWA_WRED_MINB)
                    const float2* __restrict__ Fc, const double* __restrict__ Wc,
                    double* __restrict__ tile_part) {
   constexpr int NA = PWA_CACHE_NA;
-  constexpr int NG = 2 * PWA_NCOL, MG = PWA_GPAD / 32;
+  constexpr int NG = 2 * PWA_NCOL;
   __shared__ double red[PWA_TPB / 32][NA];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (long long wi = blockIdx.x; wi < n_work; wi += gridDim.x) {
@@ -692,14 +961,13 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, PWA_WRED_MINB)
 #pragma unroll
     for (int j = 0; j < PWA_NF; ++j) v[j] = __ldcs(F + j * PWA_TPB);
     const double w = __ldcs(Wc + t * PWA_TPB + tid);
-    float g[PWA_GPAD];
-    const double s0 = warp_sum(cached_event(v, w, cp, g));
-    warp_reduce_scatter<PWA_GPAD>(g, lane);
+    float gs[PWA_GPAD / 32];
+    const double s0 = warp_sum(cached_event_rs(v, w, cp, lane, gs));
     if (lane == 0) red[warp][0] = s0;
 #pragma unroll
-    for (int j = 0; j < MG; ++j) {
-      const int idx = MG * lane + j;
-      if (idx < NG) red[warp][1 + idx] = (double)g[j];
+    for (int m = 0; m < PWA_GPAD / 32; ++m) {
+      const int idx = 32 * m + lane;
+      if (idx < NG) red[warp][1 + idx] = (double)gs[m];
     }
     __syncthreads();
     for (int j = tid; j < NA; j += PWA_TPB) {

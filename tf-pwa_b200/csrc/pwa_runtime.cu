@@ -29,7 +29,8 @@ struct Kernels {
   cudaKernel_t eval_f64 = nullptr, eval_f32 = nullptr, reduce = nullptr, pdf_f64 = nullptr,
                pdf_f32 = nullptr, columns_f64 = nullptr, gram_f64 = nullptr, sum_rows = nullptr,
                to_f32 = nullptr, cache_f32 = nullptr, eval_cached = nullptr,
-               eval_cached_direct = nullptr, eval_cached_wred = nullptr, eval_multi = nullptr, reduce_multi = nullptr,
+               eval_cached_direct = nullptr, eval_cached_wred = nullptr, eval_cached_ring2 = nullptr,
+               eval_multi = nullptr, reduce_multi = nullptr,
                fields_from_p4 = nullptr, toy_select = nullptr, toy_fields = nullptr;
 };
 
@@ -56,13 +57,15 @@ struct pwa_plan {
   float2* fcache = nullptr;
   double* wcache = nullptr;
   long long ntiles = 0, ntiles_cap = 0, fcache_n = 0;
-  int cached_blocks = 0, cached_blocks_direct = 0, cached_blocks_wred = 0;
+  int cached_blocks = 0, cached_blocks_direct = 0, cached_blocks_wred = 0, cached_blocks_ring2 = 0;
+  size_t cached_smem_ring2 = 0;
   // 0: shared-memory ring (bulk copies), 1: direct loads with per-thread FP64
   // column sums, 2: direct loads with warp reduce-scatter of the column sums;
+  // 3: shared-memory ring (2 stages) with warp reduce-scatter column sums;
   // -1: automatic (1 for up to 12 columns, else 2)
   int cached_variant = -1;
   size_t cached_smem = 0;
-  unsigned int* ticket = nullptr;  // [0] finished-block count, [1] error flag
+  unsigned int* ticket = nullptr;  // [0] finished groups, [1] error flag, [2 + g] group counts
   double* h_map = nullptr;         // mapped pinned result of the cached kernel
   double* d_map = nullptr;         // its device address
   double seq = 0.0;
@@ -105,6 +108,9 @@ int set_err(pwa_plan* h, int code, const std::string& msg) {
     if (e_ != cudaSuccess)                                                             \
       return set_err(h, PWA_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
   } while (0)
+
+// ticket words of the cached kernels: 2 + the most reduction groups (4096)
+constexpr int kTicketWords = 2 + 4096;
 
 int ensure_partials(pwa_plan* h, long long n) {
   if (n <= h->partials_cap) return PWA_OK;
@@ -262,6 +268,7 @@ int pwa_plan_create(const char* src, size_t src_len, int n_mass, int n_angle, in
             {"pwa_eval_cached", &h->k.eval_cached},
             {"pwa_eval_cached_direct", &h->k.eval_cached_direct},
             {"pwa_eval_cached_wred", &h->k.eval_cached_wred},
+            {"pwa_eval_cached_ring2", &h->k.eval_cached_ring2},
             {"pwa_fields_from_p4", &h->k.fields_from_p4},
             {"pwa_toy_select", &h->k.toy_select},
             {"pwa_toy_fields", &h->k.toy_fields},
@@ -274,8 +281,9 @@ int pwa_plan_create(const char* src, size_t src_len, int n_mass, int n_angle, in
     h->local_bytes[p] = (long long)a.localSizeBytes;
   }
   CU(cudaMalloc(&h->d_out, sizeof(double) * 2 * h->nacc));
-  CU(cudaMalloc(&h->ticket, 2 * sizeof(unsigned int)));
-  CU(cudaMemset(h->ticket, 0, 2 * sizeof(unsigned int)));
+  // [0] finished groups, [1] error flag, [2 + g] finished blocks of group g
+  CU(cudaMalloc(&h->ticket, kTicketWords * sizeof(unsigned int)));
+  CU(cudaMemset(h->ticket, 0, kTicketWords * sizeof(unsigned int)));
   CU(cudaHostAlloc(&h->h_map, sizeof(double) * (2 * ncol + 4), cudaHostAllocMapped));
   CU(cudaHostGetDevicePointer((void**)&h->d_map, h->h_map, 0));
   CU(cudaMallocHost(&h->h_out, sizeof(double) * 2 * (h->nacc > ncol * ncol ? h->nacc : ncol * ncol)));
@@ -598,9 +606,23 @@ int pwa_cache_data(pwa_plan* h, const double* consts, void* stream) {
   if (per_sm3 < 1) per_sm3 = 1;
   long long want3 = (long long)per_sm3 * h->sms;
   h->cached_blocks_wred = (int)(want3 < ntiles ? want3 : ntiles);
+  // ring with register-light consumers: 2 stages (PWA_RSTAGES) per block
+  h->cached_smem_ring2 = (size_t)2 * tile * (h->nf * sizeof(float2) + sizeof(double));
+  CU(cudaFuncSetAttribute((const void*)h->k.eval_cached_ring2,
+                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->cached_smem_ring2));
+  int per_sm4 = 0;
+  CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm4, (const void*)h->k.eval_cached_ring2,
+                                                   h->tpb, h->cached_smem_ring2));
+  if (per_sm4 < 1) return set_err(h, PWA_ERR_ARG, "column tile does not fit in shared memory");
+  long long want4 = (long long)per_sm4 * h->sms;
+  h->cached_blocks_ring2 = (int)(want4 < ntiles ? want4 : ntiles);
   int mb = h->cached_blocks > h->cached_blocks_direct ? h->cached_blocks : h->cached_blocks_direct;
   if (h->cached_blocks_wred > mb) mb = h->cached_blocks_wred;
-  rc = ensure_partials(h, (long long)mb * (1 + 2 * h->ncol));
+  if (h->cached_blocks_ring2 > mb) mb = h->cached_blocks_ring2;
+  if ((mb + 15) / 16 > kTicketWords - 2)
+    return set_err(h, PWA_ERR_ARG, "too many blocks for the grouped reduction");
+  // block rows + group rows of the two-level reduction (groups of 16 blocks)
+  rc = ensure_partials(h, (long long)(mb + (mb + 15) / 16) * (1 + 2 * h->ncol));
   if (rc) return rc;
   CU(cudaStreamSynchronize(s));
   h->fcache_n = n;
@@ -624,6 +646,9 @@ int pwa_eval_cached_enqueue(pwa_plan* h, const double* ck, void* stream) {
                                         dim3(h->cached_blocks_direct), dim3(h->tpb), args, 0, s)
       : variant == 2 ? cudaLaunchKernel((const void*)h->k.eval_cached_wred,
                                         dim3(h->cached_blocks_wred), dim3(h->tpb), args, 0, s)
+      : variant == 3 ? cudaLaunchKernel((const void*)h->k.eval_cached_ring2,
+                                        dim3(h->cached_blocks_ring2), dim3(h->tpb), args,
+                                        h->cached_smem_ring2, s)
                      : cudaLaunchKernel((const void*)h->k.eval_cached, dim3(h->cached_blocks),
                                         dim3(h->tpb), args, h->cached_smem, s);
   if (e != cudaSuccess)
@@ -637,7 +662,7 @@ int cached_result(pwa_plan* h, const double** sums) {
   const int na = 1 + 2 * h->ncol;
   const volatile double* m = h->h_map;
   if (m[na + 1] != h->seq) {
-    cudaMemset(h->ticket, 0, 2 * sizeof(unsigned int));
+    cudaMemset(h->ticket, 0, kTicketWords * sizeof(unsigned int));
     return set_err(h, PWA_ERR_CUDA, "cached evaluation did not complete (stale result)");
   }
   if (m[na] != 0.0) return set_err(h, PWA_ERR_CUDA, "cached evaluation: a barrier wait timed out");
@@ -647,7 +672,7 @@ int cached_result(pwa_plan* h, const double** sums) {
 
 int pwa_set_cached_variant(pwa_plan* h, int variant) {
   if (!h) return PWA_ERR_ARG;
-  if (variant < -1 || variant > 2) return set_err(h, PWA_ERR_ARG, "variant must be -1, 0, 1 or 2");
+  if (variant < -1 || variant > 3) return set_err(h, PWA_ERR_ARG, "variant must be -1 .. 3");
   h->cached_variant = variant;
   return PWA_OK;
 }
