@@ -19,6 +19,8 @@
  *                      (cal_angle_from_momentum at data load)
  *   pwa_toy_select /   flat phase space and toy        tf_pwa/phasespace.py:31-254,
  *   pwa_toy_fields     accept-reject on sum |A|^2      tf_pwa/applications.py:394-487
+ *   pwa_hessian_cached Hessian (differenced adjoint)   tf_pwa/model/model.py:513-561
+ *   pwa_read_dat       text momentum files             tf_pwa/data.py:300-365
  *   pwa_compile_only / pwa_last_error / pwa_plan_info / pwa_plan_destroy
  *                      build check and bookkeeping (no reference counterpart)
  *
@@ -119,6 +121,22 @@ int pwa_toy_select(pwa_plan* h, const double* consts, unsigned long long seed, l
 int pwa_toy_fields(pwa_plan* h, unsigned long long seed, const long long* idx, long long n,
                    double* out, long long ld_out, double* p4, long long ld_p4, void* stream);
 
+/* Hessian of the cached-form NLL with respect to the trainable parameters
+ * (tf_pwa/model/model.py:513-561, BaseModel.nll_grad_hessian; errors via
+ * tf_pwa/applications.py:280-309): central 4-point differences of the
+ * adjoint gradient, h_i = step * max(|x_i|, 1e-2), symmetrised; also the
+ * NLL and gradient at vars.  out_hess: n_train x n_train, row-major.
+ * Needs pwa_cache_data, pwa_build_gram and pwa_set_param_layout first. */
+int pwa_hessian_cached(pwa_plan* h, const double* vars, double sum_w, double step, void* stream,
+                       double* out_nll, double* out_grad, double* out_hess);
+
+/* Momentum file ingest (tf_pwa/data.py:300-365, load_dat_file): all
+ * whitespace- or comma-separated numbers of a text file ('#' starts a
+ * comment), parsed on all host cores, in file order, into out (host,
+ * capacity cap); *n_values = their count.  With out = NULL only the count is
+ * returned.  No plan handle: failures are reported by pwa_last_error(NULL). */
+int pwa_read_dat(const char* path, double* out, long long cap, long long* n_values);
+
 /* Gram matrix of the MC set, M_kl = sum_i w_i sum_o conj(F_ik,o) F_il,o,
  * in FP64; out[2*ncol*ncol] host, (re, im) row-major. */
 int pwa_build_gram(pwa_plan* h, const double* consts, void* stream, double* out);
@@ -138,8 +156,8 @@ int pwa_cache_data(pwa_plan* h, const double* consts, void* stream);
  * events reduce-scattered in FP32 before FP64 accumulation (register use
  * independent of the column count), 3 = shared-memory ring (two stages)
  * whose consumers read their columns from shared memory and reduce-scatter
- * the column sums, -1 = automatic (default: 1 for up to 12 columns, else
- * 2). */
+ * the column sums, -1 = automatic (default: 2, the fastest measured on
+ * the shipped models). */
 int pwa_set_cached_variant(pwa_plan* h, int variant);
 
 /* Data-term kernels on the cache with column couplings ck[2*ncol]

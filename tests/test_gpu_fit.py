@@ -95,3 +95,33 @@ def test_autograd_function_matches_finite_differences():
     np.testing.assert_allclose(x.grad.numpy(), g["grad"], rtol=1e-7,
                                atol=1e-7 * np.abs(g["grad"]).max())
     fcn.eng.close()
+
+
+def test_native_hessian_equals_python_stencil():
+    """pwa_hessian_cached (the stencil loop in the native library) equals the
+    same 4-point stencil of FCN gradients driven from Python, and agrees with
+    the plain-FP64 Hessian of the reference-parity path to 1e-4 of its
+    largest element (cached form: step 1e-2, see FCN.nll_grad_hessian)."""
+    cl, fm, g, meta = _fcn("lc2pkpi", "mixed")
+    assert fm.use_gram
+    nll_c, g_c, H_c = fm.nll_grad_hessian()
+    x0 = np.array(cl.vm.get_all_val())
+    P = len(x0)
+    H = np.zeros((P, P))
+    for i in range(P):
+        h = 1e-2 * max(abs(x0[i]), 1e-2)
+        gs = []
+        for s in (-2, -1, 1, 2):
+            xs = x0.copy()
+            xs[i] += s * h
+            gs.append(fm.get_nll_grad(xs)[1])
+        H[i] = (gs[0] - 8 * gs[1] + 8 * gs[2] - gs[3]) / (12 * h)
+    fm._set(x0)
+    H = 0.5 * (H + H.T)
+    np.testing.assert_allclose(H_c, H, rtol=1e-12, atol=1e-12 * np.abs(H).max())
+    assert np.array_equal(H_c, H_c.T)
+    _, fp, _, _ = _fcn("lc2pkpi", "plain")
+    _, _, H_p = fp.nll_grad_hessian()
+    np.testing.assert_allclose(H_c, H_p, rtol=0, atol=1e-4 * np.abs(H_p).max())
+    fm.eng.close()
+    fp.eng.close()

@@ -4,6 +4,7 @@ sm_100a (NVRTC, no device needed)."""
 import os
 import re
 
+import numpy as np
 import pytest
 
 from common import ROOT, load_model
@@ -30,3 +31,24 @@ def test_generated_model_compiles_for_sm100a(cfg):
     eng = Engine(dc.decay_group, plan, vm, compile=False)
     log = eng.compile_check("sm_100a")
     assert "pwa_eval_f64" in log and "pwa_eval_f32" in log
+
+
+def test_read_dat_matches_numpy(tmp_path):
+    """pwa_read_dat (multithreaded text ingest) returns numpy.loadtxt's
+    numbers in file order, comments skipped; bad tokens are errors."""
+    from tf_pwa_b200.api import load_dat_file
+    from tf_pwa_b200.engine import PWAError, read_dat
+
+    rng = np.random.default_rng(3)
+    a = rng.normal(size=(300000, 4)) * np.array([1.0, 1e-3, 1e3, 1e-12])
+    f = tmp_path / "p4.dat"
+    with open(f, "w") as fh:
+        fh.write("# E px py pz\n")
+        np.savetxt(fh, a, fmt="%.17g")
+    x = read_dat(str(f))
+    np.testing.assert_array_equal(x, a.reshape(-1))
+    np.testing.assert_array_equal(load_dat_file(str(f), 3)[:, 0, :], a[:100000 * 3:3])
+    bad = tmp_path / "bad.dat"
+    bad.write_text("1.0 2.0 x3\n")
+    with pytest.raises(PWAError):
+        read_dat(str(bad))

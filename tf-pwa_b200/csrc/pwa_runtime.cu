@@ -15,8 +15,11 @@
 #include <cstdio>
 #include <mutex>
 #include <cstring>
+#include <algorithm>
+#include <charconv>
 #include <map>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/pwa_b200.h"
@@ -62,7 +65,7 @@ struct pwa_plan {
   // 0: shared-memory ring (bulk copies), 1: direct loads with per-thread FP64
   // column sums, 2: direct loads with warp reduce-scatter of the column sums;
   // 3: shared-memory ring (2 stages) with warp reduce-scatter column sums;
-  // -1: automatic (1 for up to 12 columns, else 2)
+  // -1: automatic (2)
   int cached_variant = -1;
   size_t cached_smem = 0;
   unsigned int* ticket = nullptr;  // [0] finished groups, [1] error flag, [2 + g] group counts
@@ -97,8 +100,14 @@ struct pwa_plan {
 
 namespace {
 
+// message of the last failed call without a plan handle (per host thread)
+thread_local std::string g_err;
+
 int set_err(pwa_plan* h, int code, const std::string& msg) {
-  if (h) h->err = msg;
+  if (h)
+    h->err = msg;
+  else
+    g_err = msg;
   return code;
 }
 
@@ -640,7 +649,7 @@ int pwa_eval_cached_enqueue(pwa_plan* h, const double* ck, void* stream) {
   double seq = h->seq;
   void* args[] = {cbuf.data(), &h->fcache, &h->wcache, &nt, &h->partials, &h->ticket, &h->d_map,
                   &seq};
-  const int variant = h->cached_variant >= 0 ? h->cached_variant : (h->ncol <= 12 ? 1 : 2);
+  const int variant = h->cached_variant >= 0 ? h->cached_variant : 2;
   cudaError_t e =
       variant == 1   ? cudaLaunchKernel((const void*)h->k.eval_cached_direct,
                                         dim3(h->cached_blocks_direct), dim3(h->tpb), args, 0, s)
@@ -1020,8 +1029,140 @@ int pwa_plan_info(pwa_plan* h, long long* info) {
 }
 
 const char* pwa_last_error(pwa_plan* h) {
-  if (!h) return "null plan handle";
+  if (!h) return g_err.empty() ? "null plan handle" : g_err.c_str();
   return h->err.c_str();
+}
+
+int pwa_hessian_cached(pwa_plan* h, const double* vars, double sw, double step, void* stream,
+                       double* out_nll, double* out_grad, double* out_hess) {
+  if (!h) return PWA_ERR_ARG;
+  const int P = h->n_train;
+  if (!vars || !out_nll || (P && (!out_grad || !out_hess)) || !(step > 0.0))
+    return set_err(h, PWA_ERR_ARG, "invalid hessian arguments");
+  std::vector<double> x(vars, vars + h->n_vars);
+  int rc = pwa_nll_grad_cached(h, x.data(), sw, stream, out_nll, out_grad);
+  if (rc) return rc;
+  std::vector<double> g(4 * (size_t)P);
+  double nll_tmp;
+  for (int i = 0; i < P; ++i) {
+    const int vi = h->train_idx[i];
+    const double x0 = x[vi];
+    const double hs = step * std::max(std::fabs(x0), 1e-2);
+    const double shift[4] = {-2.0, -1.0, 1.0, 2.0};
+    for (int q = 0; q < 4; ++q) {
+      x[vi] = x0 + shift[q] * hs;
+      rc = pwa_nll_grad_cached(h, x.data(), sw, stream, &nll_tmp, g.data() + (size_t)q * P);
+      if (rc) return rc;
+    }
+    x[vi] = x0;
+    for (int j = 0; j < P; ++j)
+      out_hess[(size_t)i * P + j] =
+          (g[j] - 8.0 * g[P + j] + 8.0 * g[2 * P + j] - g[3 * P + j]) / (12.0 * hs);
+  }
+  for (int i = 0; i < P; ++i)
+    for (int j = i + 1; j < P; ++j) {
+      const double a = 0.5 * (out_hess[(size_t)i * P + j] + out_hess[(size_t)j * P + i]);
+      out_hess[(size_t)i * P + j] = out_hess[(size_t)j * P + i] = a;
+    }
+  return PWA_OK;
+}
+
+// ------------------------------------------------------------------ ingest
+// Text momentum files ("E px py pz" rows, '#' comments) parsed on all host
+// cores: the file is split at line ends, each thread parses its part with
+// strtod, the parts are concatenated in file order.
+namespace {
+bool read_file(const char* path, std::string* buf) {
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return false;
+  std::fseek(f, 0, SEEK_END);
+  const long n = std::ftell(f);
+  std::fseek(f, 0, SEEK_SET);
+  buf->resize(n > 0 ? (size_t)n : 0);
+  const size_t got = n > 0 ? std::fread(&(*buf)[0], 1, (size_t)n, f) : 0;
+  std::fclose(f);
+  return got == buf->size();
+}
+
+// parse [beg, end) of buf; append values to out; false on a bad token
+bool parse_range(const std::string& buf, size_t beg, size_t end, std::vector<double>* out) {
+  const char* p = buf.data() + beg;
+  const char* e = buf.data() + end;
+  while (p < e) {
+    const char c = *p;
+    if (c == '#') {
+      while (p < e && *p != '\n') ++p;
+      continue;
+    }
+    if (c == ' ' || c == '\t' || c == '\n' || c == '\r' || c == ',') {
+      ++p;
+      continue;
+    }
+    const char* q = p;
+    while (q < e && *q != ' ' && *q != '\t' && *q != '\n' && *q != '\r' && *q != ',' && *q != '#') ++q;
+    double v;
+    const char* s0 = (*p == '+') ? p + 1 : p;  // from_chars takes no leading '+'
+    const auto r = std::from_chars(s0, q, v);
+    if (r.ec != std::errc() || r.ptr != q) return false;
+    out->push_back(v);
+    p = q;
+  }
+  return true;
+}
+}  // namespace
+
+int pwa_read_dat(const char* path, double* out, long long cap, long long* n_values) {
+  if (!path || !n_values) return set_err(nullptr, PWA_ERR_ARG, "null argument");
+  // a size query parses the file and keeps the numbers for the next call on
+  // the same path from this host thread, which then only copies them
+  thread_local std::string kept_path;
+  thread_local std::vector<std::vector<double>> kept;
+  std::vector<std::vector<double>> parts;
+  if (out && kept_path == path) {
+    parts.swap(kept);
+    kept_path.clear();
+  } else {
+    std::string buf;
+    if (!read_file(path, &buf))
+      return set_err(nullptr, PWA_ERR_ARG, std::string("cannot read ") + path);
+    unsigned nt = std::thread::hardware_concurrency();
+    if (nt < 1) nt = 1;
+    if (nt > 64) nt = 64;
+    if (buf.size() < (size_t)(1 << 20)) nt = 1;
+    std::vector<size_t> cut(nt + 1, buf.size());
+    cut[0] = 0;
+    for (unsigned t = 1; t < nt; ++t) {
+      size_t c = buf.size() * t / nt;
+      while (c < buf.size() && buf[c] != '\n') ++c;
+      cut[t] = c < cut[t - 1] ? cut[t - 1] : c;
+    }
+    parts.assign(nt, {});
+    std::vector<int> ok(nt, 1);
+    std::vector<std::thread> th;
+    for (unsigned t = 0; t < nt; ++t)
+      th.emplace_back([&, t] {
+        parts[t].reserve((cut[t + 1] - cut[t]) / 8 + 16);
+        ok[t] = parse_range(buf, cut[t], cut[t + 1], &parts[t]);
+      });
+    for (auto& x : th) x.join();
+    for (unsigned t = 0; t < nt; ++t)
+      if (!ok[t]) return set_err(nullptr, PWA_ERR_ARG, std::string("bad number in ") + path);
+  }
+  long long n = 0;
+  for (const auto& v : parts) n += (long long)v.size();
+  *n_values = n;
+  if (!out) {
+    kept.swap(parts);
+    kept_path = path;
+    return PWA_OK;
+  }
+  if (n > cap) return set_err(nullptr, PWA_ERR_ARG, "output buffer too small");
+  long long o = 0;
+  for (const auto& v : parts) {
+    std::memcpy(out + o, v.data(), v.size() * sizeof(double));
+    o += (long long)v.size();
+  }
+  return PWA_OK;
 }
 
 }  // extern "C"

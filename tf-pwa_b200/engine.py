@@ -64,6 +64,8 @@ def load_library(path=LIB_PATH):
     lib.pwa_fields_from_p4.argtypes = [vp, vp, ll, ll, vp, ll, vp]
     lib.pwa_toy_select.argtypes = [vp, dp, ull, ll, ll, ctypes.c_double, i, vp, vp]
     lib.pwa_toy_fields.argtypes = [vp, ull, vp, ll, vp, ll, vp, ll, vp]
+    lib.pwa_hessian_cached.argtypes = [vp, dp, ctypes.c_double, ctypes.c_double, vp, dp, dp, dp]
+    lib.pwa_read_dat.argtypes = [cp, vp, ll, ctypes.POINTER(ll)]
     lib.pwa_plan_destroy.argtypes = [vp]
     lib.pwa_compile_only.argtypes = [cp, sz, i, cp, cp, sz]
     lib.pwa_upload_events.argtypes = [vp, vp, vp, vp, ll, ll, i, vp]
@@ -88,6 +90,7 @@ EXPORTED = ("pwa_plan_create", "pwa_plan_destroy", "pwa_compile_only", "pwa_uplo
             "pwa_nll_grad_cached", "pwa_set_cached_variant", "pwa_pool_reserve",
             "pwa_pool_alloc", "pwa_pool_free", "pwa_pool_fill", "pwa_pieces_multi",
             "pwa_eval_noalloc", "pwa_fields_from_p4", "pwa_toy_select", "pwa_toy_fields",
+            "pwa_hessian_cached", "pwa_read_dat",
             "pwa_plan_info", "pwa_last_error")
 
 
@@ -542,6 +545,19 @@ class Engine:
                     "pwa_nll_grad_cached")
         return nll.value, g
 
+    def hessian_cached(self, var_values, step=1e-4, stream=None):
+        """(nll, grad, Hessian) of the cached form, the Hessian by 4-point
+        differences of the adjoint gradient (C++ loop, pwa_hessian_cached)."""
+        v = np.ascontiguousarray(var_values, np.float64)
+        P = self._n_train
+        nll = ctypes.c_double()
+        g = np.zeros(P)
+        H = np.zeros((P, P))
+        self._check(load_library().pwa_hessian_cached(self.h, _dptr(v), self._sw, float(step),
+                                                      stream or 0, ctypes.byref(nll), _dptr(g),
+                                                      _dptr(H)), "pwa_hessian_cached")
+        return nll.value, g, H
+
     # ------------------------------------------------------------ dataset step
     def fields_from_p4(self, p4):
         """Event fields (n_fields, N) on the device from final-state momenta
@@ -631,3 +647,17 @@ class Engine:
         C = self.consts(vals)
         self._gram = self.build_gram(C)
         return self._gram
+
+
+def read_dat(path):
+    """All numbers of a text momentum file, parsed by the native library on
+    all host cores (pwa_read_dat); a flat FP64 array in file order."""
+    lib = load_library()
+    n = ctypes.c_longlong()
+    fn = os.fsencode(path)
+    if lib.pwa_read_dat(fn, None, 0, ctypes.byref(n)) != 0:
+        raise PWAError(lib.pwa_last_error(None).decode(errors="replace"))
+    out = np.empty(n.value, np.float64)
+    if lib.pwa_read_dat(fn, out.ctypes.data, n.value, ctypes.byref(n)) != 0:
+        raise PWAError(lib.pwa_last_error(None).decode(errors="replace"))
+    return out
