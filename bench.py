@@ -408,9 +408,14 @@ def main():
     eng.set_cached_variant(-1)
     Cp = eng_p.consts(vals)
     t_kernel_p = timed(lambda: eng_p.eval_enqueue(Cp, PLAIN_F64, mc=True), k_kernel)
+    # the FP32-amplitude recompute form (what a fit with floating masses and
+    # widths, where no column cache applies, can use instead of plain FP64)
+    t_f32 = timed(lambda: eng_p.nll_grad(vals, names, MIXED_F32), args.steps)
+    t_kernel_f32 = timed(lambda: eng_p.eval_enqueue(Cp, MIXED_F32, mc=True), k_kernel)
     ck_clocks = clocks.stop(local)
     nll_m, g_m = eng.nll_grad_cached(var_vec)
     nll_p, g_p = eng_p.nll_grad(vals, names, PLAIN_F64)
+    nll_f, g_f = eng_p.nll_grad(vals, names, MIXED_F32)
 
     n_data = n_sig + n_bg
     code = eng.code
@@ -435,15 +440,19 @@ def main():
         "plain_f64": {"value": world * args.steps / t_plain, "unit": "evals/s",
                       "ms_per_step": 1e3 * t_plain / args.steps,
                       "speedup_mixed_over_plain": t_plain / t_mixed},
+        "fp32_recompute": {"value": world * args.steps / t_f32, "unit": "evals/s",
+                           "ms_per_step": 1e3 * t_f32 / args.steps,
+                           "kernel_us": 1e6 * t_kernel_f32 / k_kernel,
+                           "dnll": nll_f - nll_p,
+                           "grad_max_rel": float(np.max(np.abs(g_f - g_p)) / np.max(np.abs(g_p)))},
         "e2e": {"value": world * args.steps / t_e2e, "unit": "evals/s",
                 "h2d_bytes_per_step": 16 * code.ncol,
                 "d2h_bytes_per_step": 8 * (1 + 2 * code.ncol),
                 "call": "FCN.nll_grad(x) with x a host numpy vector"},
         "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
                      "frac": ach / hbm, "traffic": None, "peak_kind": peak_kind,
-                     "kernel": ("pwa_eval_cached_direct" if code.ncol <= 12 else
-                                "pwa_eval_cached_wred") + " (data term, mixed form; ends with "
-                               "its own fixed-order reduction)",
+                     "kernel": "pwa_eval_cached_wred (data term, mixed form; ends with its "
+                               "own fixed-order two-level reduction)",
                      "algorithmic_bytes_per_launch": bytes_mixed,
                      "launch_us": 1e6 * t_kernel / k_kernel,
                      "plain_f64_kernel": {"achieved": ach_p, "frac": ach_p / hbm,

@@ -266,6 +266,42 @@ class Engine:
         for si, p in enumerate(self.code.shape_res):
             self.shape_index[(p, "m")] = 2 * si
             self.shape_index[(p, "g")] = 2 * si + 1
+        # column k = product of coupling_names[fac_idx[k, :]] (padded with -1)
+        nf = max(len(f) for f in self.col_factors)
+        self._fac_idx = np.full((len(self.col_factors), nf), -1, np.int64)
+        for k, f in enumerate(self.col_factors):
+            self._fac_idx[k, :len(f)] = [self.coupling_names.index(n) for n in f]
+        # per coupling: the columns it enters and how often
+        self._coup_cols = {}
+        for n in self.coupling_names:
+            ks = [k for k, f in enumerate(self.col_factors) if n in f]
+            cnt = [self.col_factors[k].count(n) for k in ks]
+            self._coup_cols[n] = (np.array(ks, np.int64), np.array(cnt))
+        self._shape_cache = (None, None)
+        self._jac_cache = {}
+        self._cn_index = {n: i for i, n in enumerate(self.coupling_names)}
+        self._cn_r = [n + "r" for n in self.coupling_names]
+        self._cn_i = [n + "i" for n in self.coupling_names]
+        self._cn_polar = np.array([self.vm.complex_vars.get(n, True) for n in self.coupling_names])
+        # incidence of couplings in columns; True where every coupling enters
+        # each of its columns once (then dc_k/dz = c_k / z)
+        self._inc = np.zeros((len(self.coupling_names), len(self.col_factors)))
+        for k, f in enumerate(self.col_factors):
+            for n in f:
+                self._inc[self._cn_index[n], k] += 1
+        self._inc_linear = bool(np.all(self._inc <= 1))
+        cidx = self.code.consts.index
+        self._slot_vg = []          # (coupling index, re slot, im slot) of vertex g's and totals
+        for d in self.code.vertices:
+            for i in range(len(d.get_ls_list())):
+                n = f"{d.params_head}_g_ls_{i}"
+                if n in self._cn_index:
+                    self._slot_vg.append((self._cn_index[n], cidx[f"{d}.g{i}.re"], cidx[f"{d}.g{i}.im"]))
+        for ci, ch in enumerate(self.group):
+            n = ch.params_head + "_total_0"
+            self._slot_vg.append((self._cn_index[n], cidx[f"t{ci}.re"], cidx[f"t{ci}.im"]))
+        a = np.array(self._slot_vg, np.int64).reshape(-1, 3)
+        self._vg_src, self._vg_re, self._vg_im = a[:, 0], a[:, 1], a[:, 2]
 
     def _nominal(self, p, vals, chain):
         if p in chain.inner:
@@ -309,14 +345,45 @@ class Engine:
             return m0 * m0 * g0 * pz0 / q0 ** (2 * L + 1), 1.0
         return m0 * m0 * g0 * pz0, 0.0
 
+    def _shape_key(self, vals):
+        return tuple(vals.get(k) for k in self._shape_names)
+
     def consts(self, vals):
-        """Constant block of one evaluation from the parameter dict."""
+        """Constant block of one evaluation from the parameter dict.  The
+        part that depends only on masses and widths (lineshape and barrier
+        constants) is cached per mass/width setting."""
+        c = self.code
+        if not hasattr(self, "_shape_names"):
+            self._shape_names = sorted(k for k in vals if k.endswith(("_mass", "_width")))
+        key = self._shape_key(vals)
+        if self._shape_cache[0] == key:
+            C = self._shape_cache[1].copy()
+            r = np.fromiter((vals[n] for n in self._cn_r), float, len(self._cn_r))
+            ph = np.fromiter((vals[n] for n in self._cn_i), float, len(self._cn_i))
+            z = np.where(self._cn_polar, r * np.exp(1j * ph), r + 1j * ph)
+            self._cvec, self._cr, self._cph = z, r, ph
+            self._cv = dict(zip(self.coupling_names, z))
+            self._ck = np.prod(np.append(z, 1.0 + 0j)[self._fac_idx], axis=1)
+            C[0:2 * c.ncol:2] = self._ck.real
+            C[1:2 * c.ncol:2] = self._ck.imag
+            C[self._vg_re] = z[self._vg_src].real
+            C[self._vg_im] = z[self._vg_src].imag
+            return C
+        C = self._consts_full(vals)
+        self._shape_cache = (key, C.copy())
+        return C
+
+    def _consts_full(self, vals):
         c = self.code
         C = np.zeros(len(c.consts))
         idx = c.consts.index
         cv = {n: self.complex_val(vals, n) for n in self.coupling_names}
-        self._ck = np.array([np.prod([cv[n] for n in f]) for f in self.col_factors])
+        cvec = np.array([cv[n] for n in self.coupling_names] + [1.0 + 0j])
+        self._ck = np.prod(cvec[self._fac_idx], axis=1)
         self._cv = cv
+        self._cvec = cvec[:-1]
+        self._cr = np.array([vals[n] for n in self._cn_r])
+        self._cph = np.array([vals[n] for n in self._cn_i])
         C[0:2 * c.ncol:2] = self._ck.real
         C[1:2 * c.ncol:2] = self._ck.imag
         for d in c.vertices:
@@ -362,6 +429,23 @@ class Engine:
         return C
 
     # ------------------------------------------------------------ jacobian
+    def _jac_layout(self, names):
+        """Index arrays of the coupling parameters among ``names`` (None if
+        a coupling enters a column more than once)."""
+        key = tuple(names)
+        lay = getattr(self, "_jac_lay", {}).get(key, 0)
+        if lay != 0:
+            return lay
+        if not self._inc_linear:
+            lay = None
+        else:
+            rows = [pi for pi, n in enumerate(names) if n[:-1] in self._cn_index]
+            ci = np.array([self._cn_index[names[pi][:-1]] for pi in rows], np.int64)
+            is_r = np.array([names[pi].endswith("r") for pi in rows])
+            lay = (ci, is_r, self._cn_polar[ci], np.array(rows, np.int64))
+        self._jac_lay = {key: lay}
+        return lay
+
     def jacobian(self, vals, names):
         """J[p, k] (complex) and shape selectors D[p, s] for parameters
         ``names`` at ``vals`` (call after consts())."""
@@ -370,7 +454,19 @@ class Engine:
         J = np.zeros((P, c.ncol), np.complex128)
         D = np.zeros((P, max(c.nshape, 1)))
         cv = self._cv
-        for pi, n in enumerate(names):
+        key = (tuple(names), self._shape_key(vals) if hasattr(self, "_shape_names") else None)
+        cached = self._jac_cache.get(key)
+        lay = self._jac_layout(names)
+        if lay is not None and np.all(self._cr[lay[0]] != 0):
+            # every coupling enters its columns linearly: dc_k/dtheta = c_k * f
+            ci, is_r, polar, rows = lay
+            z, r = self._cvec[ci], self._cr[ci]
+            f = np.where(polar, np.where(is_r, 1.0 / r, 1j), np.where(is_r, 1.0 / z, 1j / z))
+            J[rows] = self._inc[ci] * self._ck[None, :] * f[:, None]
+            names_left = [(pi, n) for pi, n in enumerate(names) if n[:-1] not in cv]
+        else:
+            names_left = list(enumerate(names))
+        for pi, n in names_left:
             base = n[:-1]
             if base in cv:
                 r, ph = vals[base + "r"], vals[base + "i"]
@@ -379,12 +475,21 @@ class Engine:
                     dz = np.exp(1j * ph) if n.endswith("r") else 1j * cv[base]
                 else:
                     dz = 1.0 if n.endswith("r") else 1j
-                for k, f in enumerate(self.col_factors):
-                    cnt = f.count(base)
-                    if cnt == 0:
-                        continue
-                    others = np.prod([cv[x] for x in f if x != base]) if len(f) > cnt else 1.0
-                    J[pi, k] += cnt * others * cv[base] ** (cnt - 1) * dz
+                ks, cnt = self._coup_cols[base]
+                z = cv[base]
+                if np.all(cnt == 1) and z != 0:
+                    # c_k is linear in this coupling: dc_k = c_k / z * dz
+                    J[pi, ks] = self._ck[ks] / z * dz
+                    continue
+                for k in ks:
+                    f = self.col_factors[k]
+                    m = f.count(base)
+                    others = np.prod([cv[x] for x in f if x != base]) if len(f) > m else 1.0
+                    J[pi, k] += m * others * z ** (m - 1) * dz
+                continue
+            if cached is not None:
+                J[pi] = cached[0][pi] * self._ck
+                D[pi] = cached[1][pi]
                 continue
             # masses / widths
             hit = None
@@ -419,6 +524,14 @@ class Engine:
                         if d.barrier_factor_norm:
                             kap += np.imag(vc[l][1]) / hh / np.real(v0[l][1])
                     J[pi, k] += self._ck[k] * kap
+        if cached is None and key[1] is not None:
+            # mass/width rows: J = kappa_k * c_k with kappa fixed per shape setting
+            kap = np.zeros((P, c.ncol), np.complex128)
+            for pi, n in enumerate(names):
+                if n[:-1] not in cv:
+                    kap[pi] = np.divide(J[pi], self._ck, out=np.zeros(c.ncol, np.complex128),
+                                        where=self._ck != 0)
+            self._jac_cache = {key: (kap, D.copy())}
         return J, D
 
     # ------------------------------------------------------------ evaluate
