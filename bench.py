@@ -36,6 +36,11 @@ WORKLOADS = {
                 "Lambda_c+ -> p K- pi+ (Lambda(1520), K*(892), Delta(1232); 3 chains, 8 LS "
                 "columns, 4 helicity combinations), 1e6 accept-reject signal + 1e5 flat "
                 "background (w=-0.1) data rows, 1e6 flat MC"),
+    "d2kpipi_float": ("d2kpipi_float.yml", 1_000_000, 0, 1_000_000,
+                      "NLL+grad evals/s @1M data+1M MC, masses and widths floating",
+                      "D0 -> K pi pi (K*(892) 1-, f0(980) 0+; 2 chains), both resonance masses "
+                      "and widths floating (no column cache), 1e6 accept-reject data, 1e6 flat "
+                      "MC"),
     "b2dstkpi": ("b2dstkpi.yml", 1_000_000, 0, 4_000_000,
                  "NLL+grad evals/s @1M data+4M MC",
                  "B -> D*(2007) (-> D pi_s) K pi, 12 resonances (J = 0..3) in the D*K, D*pi "
@@ -255,6 +260,90 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------- floating masses/widths
+def run_floating(args, rank, world, timed_factory):
+    """Workload with floating lineshape parameters: no column cache applies,
+    so the chosen form is the FP32-amplitude recompute kernel (FP64 masses,
+    lineshape constants and sums) against the plain FP64 kernels; the
+    Hessian comes from differenced adjoint gradients."""
+    import torch
+
+    from tf_pwa_b200.api import FCN
+    from tf_pwa_b200.engine import MIXED_F32, PLAIN_F64
+    from tf_pwa_b200.workload import make_dataset
+
+    t0 = time.perf_counter()
+    cl, data, bg, mc = make_dataset(CONFIG, args.n_sig, args.n_mc, seed=1 + rank)
+    t_data = time.perf_counter() - t0
+    fcn = FCN(cl, data, mc, precision="mixed")
+    assert not fcn.use_gram
+    fcn_p = FCN(cl, data, mc, precision="plain")
+    x0 = np.array(cl.vm.get_all_val())
+    vals, names = cl.vm.get_all_dic(), list(cl.vm.trainable_vars)
+    timed = timed_factory()
+    for _ in range(args.warmup):
+        fcn.nll_grad(x0)
+        fcn_p.nll_grad(x0)
+    clocks = Clocks(os.path.join(ROOT, "gpurun_out", f"clocks_rank{rank}.csv")
+                    if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else f"/tmp/clocks{rank}.csv")
+    clocks.start()
+    t_f32 = timed(lambda: fcn.nll_grad(x0), args.steps)
+    t_p = timed(lambda: fcn_p.nll_grad(x0), args.steps)
+    C = fcn.eng.consts(vals)
+    t_k = timed(lambda: fcn.eng.eval_enqueue(C, MIXED_F32, mc=True), args.steps)
+    t_kp = timed(lambda: fcn_p.eng.eval_enqueue(C, PLAIN_F64, mc=True), args.steps)
+    th = time.perf_counter()
+    _, _, H = fcn.nll_grad_hessian(x0)
+    t_hess = time.perf_counter() - th
+    cov = np.linalg.inv(H)
+    ck_clocks = clocks.stop(int(os.environ.get("LOCAL_RANK", "0")))
+    nll_f, g_f = fcn.nll_grad(x0)
+    nll_p, g_p = fcn_p.nll_grad(x0)
+    code = fcn.eng.code
+    n_all = args.n_sig + args.n_mc
+    bytes_f32 = n_all * (8 * len(code.mass_fields) + 4 * len(code.angle_fields) + 8)
+    bytes_f64 = n_all * (8 * len(code.mass_fields) + 8 * len(code.angle_fields) + 8)
+    hbm, peak_kind = _peaks()
+    ach = bytes_f32 / (t_k / args.steps) / 1e9
+    line = {
+        "metric": METRIC, "value": world * args.steps / t_f32, "unit": "evals/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * t_f32 / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "precision": "FP32 amplitudes recomputed from the "
+                   "angles every evaluation (FP64 masses, lineshape constants, log and sums); "
+                   "no column cache since masses and widths float",
+                   "events_per_rank": {"data": args.n_sig, "mc": args.n_mc},
+                   "l2": "256 MB buffer written before every timed step (L2 126 MB)",
+                   "parallelism": "single GPU"},
+        "plain_f64": {"value": world * args.steps / t_p, "unit": "evals/s",
+                      "ms_per_step": 1e3 * t_p / args.steps,
+                      "speedup_f32_over_plain": t_p / t_f32},
+        "e2e": {"value": world * args.steps / t_f32, "unit": "evals/s",
+                "h2d_bytes_per_step": 8 * len(x0), "d2h_bytes_per_step": 8 * (1 + len(x0)),
+                "call": "FCN.nll_grad(x) with x a host numpy vector"},
+        "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
+                     "frac": ach / hbm, "traffic": None, "peak_kind": peak_kind,
+                     "kernel": "pwa_eval_f32 + pwa_reduce (data + MC, FP32 amplitudes)",
+                     "algorithmic_bytes_per_launch": bytes_f32,
+                     "launch_us": 1e6 * t_k / args.steps,
+                     "plain_f64_kernel": {"launch_us": 1e6 * t_kp / args.steps,
+                                          "algorithmic_bytes_per_launch": bytes_f64}},
+        "gpu_launches": 2 * args.steps,
+        "hessian": {"seconds": t_hess, "n_params": len(x0), "evaluations": 4 * len(x0) + 1,
+                    "errors": dict(zip(names, np.sqrt(np.abs(np.diag(cov))).tolist()))},
+        "check": {"nll_f32": nll_f, "nll_plain": nll_p, "dnll": nll_f - nll_p,
+                  "grad_max_rel": float(np.max(np.abs(g_f - g_p)) / np.max(np.abs(g_p)))},
+        "setup_s": {"dataset": t_data},
+    }
+    if ck_clocks:
+        line["clocks"] = ck_clocks
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    fcn.eng.close()
+    fcn_p.eng.close()
+
+
 # ------------------------------------------------------------- serving arm
 def run_serving(args):
     """Toy-fit service: 512 fits of the d2kpipi model, event counts
@@ -325,31 +414,6 @@ def main():
     from tf_pwa_b200.api import FCN
     from tf_pwa_b200.workload import make_dataset
 
-    t_setup = time.perf_counter()
-
-    def log(msg):
-        print(f"[bench {time.perf_counter() - t_setup:8.1f}s] {msg}", file=sys.stderr, flush=True)
-
-    n_sig, n_bg, n_mc = args.n_sig, args.n_bg, args.n_mc
-    cl, data, bg, mc = make_dataset(CONFIG, n_sig, n_mc, n_bg=n_bg, bg_weight=BG_WEIGHT,
-                                    seed=1 + rank, device="cuda")
-    t_data = time.perf_counter() - t_setup
-    log(f"dataset: {n_sig} signal + {n_bg} background + {n_mc} MC events")
-    reduce_fn = None
-    if dist is not None:
-        def reduce_fn(vec):
-            t = torch.as_tensor(vec, device="cuda")
-            dist.all_reduce(t)
-            return t.cpu().numpy()
-    fcn = FCN(cl, data, mc, bg=bg, precision="mixed")         # Gram MC term
-    log("mixed-form FCN ready (column cache + Gram)")
-    fcn_plain = FCN(cl, data, mc, bg=bg, precision="plain")
-    log("plain FCN ready")
-    for f in (fcn, fcn_plain):
-        f.eng.dist_reduce = reduce_fn
-        f.eng.mc_share = 1.0 / world  # equal MC shards
-    x0 = np.array(cl.vm.get_all_val())
-    names = list(cl.vm.trainable_vars)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
 
     def barrier():
@@ -374,6 +438,34 @@ def main():
             dist.all_reduce(tt, op=dist.ReduceOp.MAX)
             t = float(tt.item())
         return t
+
+    t_setup = time.perf_counter()
+
+    def log(msg):
+        print(f"[bench {time.perf_counter() - t_setup:8.1f}s] {msg}", file=sys.stderr, flush=True)
+
+    if args.workload == "d2kpipi_float":
+        return run_floating(args, rank, world, lambda: timed)
+    n_sig, n_bg, n_mc = args.n_sig, args.n_bg, args.n_mc
+    cl, data, bg, mc = make_dataset(CONFIG, n_sig, n_mc, n_bg=n_bg, bg_weight=BG_WEIGHT,
+                                    seed=1 + rank, device="cuda")
+    t_data = time.perf_counter() - t_setup
+    log(f"dataset: {n_sig} signal + {n_bg} background + {n_mc} MC events")
+    reduce_fn = None
+    if dist is not None:
+        def reduce_fn(vec):
+            t = torch.as_tensor(vec, device="cuda")
+            dist.all_reduce(t)
+            return t.cpu().numpy()
+    fcn = FCN(cl, data, mc, bg=bg, precision="mixed")         # Gram MC term
+    log("mixed-form FCN ready (column cache + Gram)")
+    fcn_plain = FCN(cl, data, mc, bg=bg, precision="plain")
+    log("plain FCN ready")
+    for f in (fcn, fcn_plain):
+        f.eng.dist_reduce = reduce_fn
+        f.eng.mc_share = 1.0 / world  # equal MC shards
+    x0 = np.array(cl.vm.get_all_val())
+    names = list(cl.vm.trainable_vars)
 
     vals = cl.vm.get_all_dic()
     eng, eng_p = fcn.eng, fcn_plain.eng

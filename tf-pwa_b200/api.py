@@ -204,15 +204,16 @@ class FCN:
         """Hessian by differencing the adjoint gradient: 4-point central
         stencil per parameter, h_i = step * max(|x_i|, 1e-2) (error O(h^4)),
         symmetrised.  Default step: 1e-4 in the plain form; 1e-2 in the
-        cached form, whose per-warp FP32 column sums put ~1e-7 relative
-        rounding noise on the gradient (noise / h must stay small), and whose
-        whole stencil loop runs in the native library."""
+        mixed forms, whose FP32 per-event (or per-warp) values put 1e-7 to
+        1e-6 relative rounding noise on the gradient (noise / h must stay
+        small).  In the cached form the whole stencil loop runs in the native
+        library."""
         self._set(x)
+        if step is None:
+            step = 1e-4 if self.precision == PLAIN_F64 else 1e-2
         if self.use_gram:
             v = self.vm.variables
-            return self.eng.hessian_cached([v[k] for k in self._var_names],
-                                           1e-2 if step is None else step)
-        step = 1e-4 if step is None else step
+            return self.eng.hessian_cached([v[k] for k in self._var_names], step)
         x0 = np.array(self.vm.get_all_val())
         nll, g0 = self.get_nll_grad(x0)
         P = len(x0)
