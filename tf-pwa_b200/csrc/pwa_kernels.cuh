@@ -318,6 +318,24 @@ __device__ __forceinline__ void last_block_sum(const double* __restrict__ partia
   }
 }
 
+// Result publication by the block that wrote out[0 .. na): after the
+// block barrier, thread 0 writes the error flag, issues one system-scope
+// fence (cumulative: it orders the block's out[] writes, observed through
+// the barrier, before what follows) and writes the call number `seq` last,
+// so a host that sees out[na + 1] == seq (mapped memory) may read
+// everything before it.  Resets the counters for the next launch.
+__device__ __forceinline__ void publish_result(unsigned int* __restrict__ ticket, int na,
+                                               double* __restrict__ out, double seq) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    out[na] = (double)atomicOr((unsigned int*)(ticket + 1), 0u);
+    ticket[0] = 0u;
+    ticket[1] = 0u;
+    __threadfence_system();
+    out[na + 1] = seq;
+  }
+}
+
 // Ordered two-level reduction of the block partials (row b = block b's
 // `na` sums, written and fenced by every block before the call).  The last
 // block of each group of PWA_GROUP consecutive blocks (ticket[2 + g])
@@ -481,15 +499,7 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB)
   __threadfence();
   __syncthreads();
   if (!grouped_sum(partials, ticket, NA, out, &s_last)) return;
-  __syncthreads();
-  if (tid == 0) {
-    const unsigned e = atomicOr((unsigned int*)(ticket + 1), 0u);
-    out[NA] = (double)e;
-    out[NA + 1] = seq;
-    ticket[0] = 0u;
-    ticket[1] = 0u;
-    __threadfence_system();
-  }
+  publish_result(ticket, NA, out, seq);
 }
 
 // Direct-load variant of pwa_eval_cached: no shared-memory staging; each
@@ -575,14 +585,7 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, 4)
   __threadfence();
   __syncthreads();
   if (!grouped_sum(partials, ticket, NA, out, &s_last)) return;
-  __syncthreads();
-  if (tid == 0) {
-    out[NA] = (double)atomicOr((unsigned int*)(ticket + 1), 0u);
-    out[NA + 1] = seq;
-    ticket[0] = 0u;
-    ticket[1] = 0u;
-    __threadfence_system();
-  }
+  publish_result(ticket, NA, out, seq);
 }
 
 // ---------------------------------------------------------------------------
@@ -768,14 +771,7 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, PWA_WRED_MINB)
   __threadfence();
   __syncthreads();
   if (!grouped_sum(partials, ticket, NA, out, &s_last)) return;
-  __syncthreads();
-  if (tid == 0) {
-    out[NA] = (double)atomicOr((unsigned int*)(ticket + 1), 0u);
-    out[NA + 1] = seq;
-    ticket[0] = 0u;
-    ticket[1] = 0u;
-    __threadfence_system();
-  }
+  publish_result(ticket, NA, out, seq);
 }
 
 // ---------------------------------------------------------------------------
@@ -923,15 +919,7 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB)
   __threadfence();
   __syncthreads();
   if (!grouped_sum(partials, ticket, NA, out, &s_last)) return;
-  __syncthreads();
-  if (tid == 0) {
-    const unsigned e = atomicOr((unsigned int*)(ticket + 1), 0u);
-    out[NA] = (double)e;
-    out[NA + 1] = seq;
-    ticket[0] = 0u;
-    ticket[1] = 0u;
-    __threadfence_system();
-  }
+  publish_result(ticket, NA, out, seq);
 }
 
 // ---------------------------------------------------------------------------

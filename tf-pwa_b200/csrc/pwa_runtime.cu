@@ -16,6 +16,8 @@
 #include <mutex>
 #include <cstring>
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <charconv>
 #include <map>
 #include <string>
@@ -665,6 +667,28 @@ int pwa_eval_cached_enqueue(pwa_plan* h, const double* ck, void* stream) {
   return PWA_OK;
 }
 
+// Wait for the last cached launch: the kernel publishes its call number
+// last (after system fences) into mapped host memory, so polling it returns
+// as soon as the sums are visible, without a stream synchronisation.  After
+// one second without it (a failed launch or a very long kernel) fall back to
+// synchronising the stream, which also surfaces launch errors.
+void wait_cached(pwa_plan* h, cudaStream_t s) {
+  const int na = 1 + 2 * h->ncol;
+  const volatile double* m = h->h_map;
+  const auto t0 = std::chrono::steady_clock::now();
+  for (unsigned it = 1;; ++it) {
+    if (m[na + 1] == h->seq) {
+      std::atomic_thread_fence(std::memory_order_acquire);
+      return;
+    }
+    if ((it & 4095u) == 0 &&
+        std::chrono::steady_clock::now() - t0 > std::chrono::seconds(1)) {
+      cudaStreamSynchronize(s);
+      return;
+    }
+  }
+}
+
 // Result of the last cached launch (after the stream has been synchronised):
 // checks the error flag and the call number.
 int cached_result(pwa_plan* h, const double** sums) {
@@ -819,7 +843,7 @@ int pwa_pieces_cached(pwa_plan* h, const double* vars, double sw, double mc_shar
   cudaStream_t s = (cudaStream_t)stream;
   int rc = pwa_eval_cached_enqueue(h, ck.data(), stream);
   if (rc) return rc;
-  CU(cudaStreamSynchronize(s));
+  wait_cached(h, s);
   const double* sd = nullptr;
   rc = cached_result(h, &sd);
   if (rc) return rc;
