@@ -13,6 +13,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <mutex>
 #include <cstring>
 #include <algorithm>
@@ -163,15 +164,68 @@ std::string full_source(const char* src, size_t src_len, int tpb) {
 std::mutex g_cubin_mu;
 std::map<std::string, std::vector<char>> g_cubins;
 
+// Optional on-disk cache across processes: with PWA_CUBIN_CACHE=<dir> set,
+// cubins are stored as <dir>/pwa_<hash>.cubin, keyed by two 64-bit FNV-1a
+// hashes of (NVRTC version, arch, full source) and its length.
+std::string disk_cache_path(const std::string& key) {
+  const char* dir = std::getenv("PWA_CUBIN_CACHE");
+  if (!dir || !*dir) return std::string();
+  int major = 0, minor = 0;
+  nvrtcVersion(&major, &minor);
+  const std::string k = std::to_string(major) + "." + std::to_string(minor) + "\n" + key;
+  unsigned long long h1 = 1469598103934665603ull, h2 = 1099511628211ull * 7ull;
+  for (const char c : k) {
+    h1 = (h1 ^ (unsigned char)c) * 1099511628211ull;
+    h2 = (h2 ^ (unsigned char)c) * 1469598103934665603ull + 0x9E3779B97F4A7C15ull;
+  }
+  char name[96];
+  std::snprintf(name, sizeof(name), "/pwa_%016llx%016llx_%zx.cubin", h1, h2, k.size());
+  return std::string(dir) + name;
+}
+
+bool disk_cache_read(const std::string& path, std::vector<char>* cubin) {
+  if (path.empty()) return false;
+  FILE* f = std::fopen(path.c_str(), "rb");
+  if (!f) return false;
+  std::fseek(f, 0, SEEK_END);
+  const long n = std::ftell(f);
+  std::fseek(f, 0, SEEK_SET);
+  bool ok = n > 0;
+  if (ok) {
+    cubin->resize((size_t)n);
+    ok = std::fread(cubin->data(), 1, (size_t)n, f) == (size_t)n;
+  }
+  std::fclose(f);
+  return ok;
+}
+
+void disk_cache_write(const std::string& path, const std::vector<char>& cubin) {
+  if (path.empty()) return;
+  const std::string tmp = path + ".tmp" + std::to_string((long long)std::rand());
+  FILE* f = std::fopen(tmp.c_str(), "wb");
+  if (!f) return;
+  const bool ok = std::fwrite(cubin.data(), 1, cubin.size(), f) == cubin.size();
+  std::fclose(f);
+  if (ok) std::rename(tmp.c_str(), path.c_str());  // atomic replace
+  else std::remove(tmp.c_str());
+}
+
 int compile_cubin(const char* src, size_t src_len, int tpb, const std::string& arch, bool verbose,
                   std::vector<char>* cubin, std::string* log) {
   const std::string full = full_source(src, src_len, tpb);
   const std::string key = arch + '\n' + full;
+  std::string disk;
   if (!verbose) {
     std::lock_guard<std::mutex> g(g_cubin_mu);
     auto it = g_cubins.find(key);
     if (it != g_cubins.end()) {
       *cubin = it->second;
+      log->clear();
+      return PWA_OK;
+    }
+    disk = disk_cache_path(key);
+    if (disk_cache_read(disk, cubin)) {
+      g_cubins.emplace(key, *cubin);
       log->clear();
       return PWA_OK;
     }
@@ -206,6 +260,7 @@ int compile_cubin(const char* src, size_t src_len, int tpb, const std::string& a
   if (!verbose) {
     std::lock_guard<std::mutex> g(g_cubin_mu);
     g_cubins.emplace(key, *cubin);
+    disk_cache_write(disk, *cubin);
   }
   return PWA_OK;
 }
