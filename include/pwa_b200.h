@@ -21,6 +21,7 @@
  *   pwa_toy_fields     accept-reject on sum |A|^2      tf_pwa/applications.py:394-487
  *   pwa_hessian_cached Hessian (differenced adjoint)   tf_pwa/model/model.py:513-561
  *   pwa_read_dat       text momentum files             tf_pwa/data.py:300-365
+ *   pwa_server_*       many fits, each a BFGS driver   tf_pwa/fit.py:189-419 (one per fit)
  *   pwa_compile_only / pwa_last_error / pwa_plan_info / pwa_plan_destroy
  *                      build check and bookkeeping (no reference counterpart)
  *
@@ -39,6 +40,7 @@ extern "C" {
 #endif
 
 typedef struct pwa_plan pwa_plan;
+typedef struct pwa_server pwa_server;
 
 enum {
   PWA_OK = 0,
@@ -234,6 +236,34 @@ int pwa_eval_noalloc(pwa_plan* h, const double* consts, const double* xm, const 
 int pwa_plan_info(pwa_plan* h, long long* info);
 
 const char* pwa_last_error(pwa_plan* h);
+
+/* Native fit server: many concurrent fits of one model (toy, pull and
+ * significance studies, tf_pwa/fit.py:189-419 per fit) sharing the plan's
+ * MC Gram matrix.  Each fit is a BFGS state machine (inverse-Hessian
+ * update, backtracking Armijo line search; converged at max|g| < gtol,
+ * stopped when a step lowers the NLL by less than 1e-12 relative, after 20
+ * backtracks or at maxiter iterations); one scheduler thread admits fits into the plan's tile pool
+ * (pwa_pool_reserve first) and evaluates the pending point of every active
+ * fit in one multi-request launch per round.  base_vars: all variables
+ * (fixed values); consts: the constant block for the column caches.  While
+ * a server runs, no other thread may use its plan. */
+int pwa_server_create(pwa_plan* h, const double* base_vars, const double* consts, int max_active,
+                      double gtol, int maxiter, pwa_server** out);
+/* Queue a fit: x0 = its trainable start values; xm, xa, w = its events'
+ * mass/angle columns and weights on the device (stride ld), which must stay
+ * valid until its result is final. */
+int pwa_server_submit(pwa_server* s, const double* x0, const double* xm, const double* xa,
+                      const double* w, long long n, long long ld, long long* fit_id);
+/* Result of a fit (wait != 0: block until it is final).  status: 0 running,
+ * 1 converged, 2 stopped (iteration limit or line search), 3 failed;
+ * latency_s = finish - submission. */
+int pwa_server_result(pwa_server* s, long long fit_id, int wait, int* status, double* x,
+                      double* nll, int* n_eval, int* n_iter, double* latency_s);
+/* out[5]: rounds (launches), requests, seconds inside the launches, active
+ * fits, queued fits. */
+int pwa_server_stats(pwa_server* s, double* out);
+/* Stop the scheduler (unfinished fits end as failed) and free the server. */
+int pwa_server_destroy(pwa_server* s);
 
 #ifdef __cplusplus
 }

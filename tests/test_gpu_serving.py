@@ -105,3 +105,62 @@ def test_admission_under_budget(setup):
     assert all("error" not in j.result for j in jobs)
     # later fits waited for pool space
     assert jobs[3].admitted >= min(jobs[0].finished, jobs[1].finished)
+
+
+def test_native_server_alone_equals_in_mix(setup):
+    """Native server (BFGS state machines in the library): a fit's path and
+    result are bitwise the same alone and mixed with other fits; all fits
+    converge (max|g| < 1e-3, the reference fit's tolerance); the minimum
+    equals the one scipy's BFGS finds on the same events through the
+    reference-facing FCN (|dNLL| < 1e-8 relative)."""
+    from tf_pwa_b200.api import FCN, EventData
+    from tf_pwa_b200.serving import NativeFitServer
+
+    cl, data, mc = setup
+    sizes = [20000, 3000, 9000, 15000]
+    alone = _jobs(cl, data, sizes)[0]
+    srv = NativeFitServer(cl, mc, 1e9)
+    srv.submit(alone)
+    assert srv.result(alone, wait=True)
+    srv.close()
+    mixed = _jobs(cl, data, sizes)
+    srv = NativeFitServer(cl, mc, 1e9)
+    for j in mixed:
+        srv.submit(j)
+    for j in mixed:
+        assert srv.result(j, wait=True)
+    st = srv.stats()
+    srv.close()
+    assert st["requests"] > st["rounds"]  # requests shared launches
+    a, m = alone, mixed[0]
+    assert a.result["success"] and m.result["success"]
+    assert a.n_eval == m.n_eval
+    assert np.array_equal(a.result["x"], m.result["x"]) and a.result["nll"] == m.result["nll"]
+    for j in mixed:
+        assert j.result["success"], j.result
+    # same minimum as scipy BFGS on the FCN of the same events
+    j = mixed[0]
+    fcn = FCN(cl, EventData(j.fields, np.ones(j.n)), mc, precision="mixed")
+    from scipy.optimize import minimize
+
+    r = minimize(lambda x: fcn.nll_grad(x), j.x0, jac=True, method="BFGS",
+                 options={"gtol": 1e-3, "maxiter": 300})
+    assert abs(r.fun - j.result["nll"]) <= 1e-8 * abs(r.fun)
+    fcn.eng.close()
+
+
+def test_native_server_admission_small_pool(setup):
+    """With a pool for about two fits, four fits all finish (queued fits are
+    admitted as others release their tiles)."""
+    from tf_pwa_b200.serving import NativeFitServer
+
+    cl, data, mc = setup
+    jobs = _jobs(cl, data, [12000, 12000, 12000, 12000], seed=5)
+    c_nf = 2 * 8 + 8
+    srv = NativeFitServer(cl, mc, 2.2 * 12032 * c_nf)
+    for j in jobs:
+        srv.submit(j)
+    for j in jobs:
+        assert srv.result(j, wait=True)
+        assert j.result["success"]
+    srv.close()

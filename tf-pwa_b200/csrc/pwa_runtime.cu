@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <condition_variable>
 #include <charconv>
 #include <map>
 #include <string>
@@ -1330,3 +1331,359 @@ extern "C" int pwa_eval_noalloc(pwa_plan* h, const double* consts, const double*
   void* args2[] = {&scratch, &nacc, &blocks_data, &nblocks, &out};
   return launch(h, h->k.reduce, dim3(1), dim3(1024), args2, s);
 }
+
+// ---------------------------------------------------------------------------
+// Native fit server.
+//
+// Many fits of one model (toy, pull and significance studies) share the MC
+// sample and its Gram matrix; each fit has its own data events.  Every fit's
+// optimiser is a BFGS state machine (inverse-Hessian update, backtracking
+// line search with the Armijo condition and quadratic interpolation, stop
+// when max|g| < gtol, as tf_pwa/fit.py:189-419 drives scipy's BFGS).  One
+// scheduler thread admits fits into the tile pool as space frees up, and in
+// every round evaluates the pending point of EVERY active fit in one
+// multi-request launch (pwa_pieces_multi), then advances each state machine
+// by one step.  No per-fit threads, no interpreter in the loop.  A fit also
+// stops (status 2) when an accepted step lowers the NLL by less than 1e-12
+// relative (the rounding level), after 20 backtracks, or at maxiter.  A fit's
+// evaluations depend only on its own events and parameters (per-fit ordered
+// sums), so its path and result are bitwise the same alone or in any mix.
+namespace {
+
+struct SrvFit {
+  long long id = 0, n = 0, ld = 0;
+  const double *xm = nullptr, *xa = nullptr, *w = nullptr;
+  long long first_tile = -1, n_tiles = 0;
+  int P = 0;
+  std::vector<double> x, g, H, d, xt, gt;
+  double f = 0.0, ft = 0.0, gd = 0.0, alpha = 1.0;
+  int phase = 0;  // 0: evaluate the start point; 1: line-search trial
+  int n_eval = 0, n_iter = 0, n_ls = 0;
+  bool done = false, converged = false, failed = false;
+  double t_arrive = 0.0, t_admit = 0.0, t_done = 0.0;
+};
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+double inf_norm(const std::vector<double>& v) {
+  double m = 0.0;
+  for (double a : v) m = std::max(m, std::fabs(a));
+  return m;
+}
+
+}  // namespace
+
+struct pwa_server {
+  pwa_plan* h = nullptr;
+  std::vector<double> base_vars, consts;
+  int max_active = 256, maxiter = 300;
+  double gtol = 1e-5;
+  std::mutex mu;
+  std::condition_variable cv;
+  std::vector<SrvFit*> pending, active;
+  std::map<long long, SrvFit*> fits;
+  long long next_id = 0;
+  bool stop = false;
+  std::thread th;
+  std::string err;
+  long long batches = 0, requests = 0;
+  double busy = 0.0;
+};
+
+namespace {
+
+// direction and first trial point of an iteration
+void srv_new_direction(SrvFit* F, bool first) {
+  const int P = F->P;
+  F->d.assign(P, 0.0);
+  for (int i = 0; i < P; ++i)
+    for (int j = 0; j < P; ++j) F->d[i] -= F->H[(size_t)i * P + j] * F->g[j];
+  F->gd = 0.0;
+  for (int i = 0; i < P; ++i) F->gd += F->g[i] * F->d[i];
+  if (!(F->gd < 0.0)) {  // not a descent direction: restart from steepest descent
+    std::fill(F->H.begin(), F->H.end(), 0.0);
+    for (int i = 0; i < P; ++i) F->H[(size_t)i * P + i] = 1.0;
+    F->gd = 0.0;
+    for (int i = 0; i < P; ++i) {
+      F->d[i] = -F->g[i];
+      F->gd -= F->g[i] * F->g[i];
+    }
+  }
+  F->alpha = first ? std::min(1.0, 1.0 / std::max(inf_norm(F->g), 1e-300)) : 1.0;
+  F->n_ls = 0;
+  F->xt.resize(P);
+  for (int i = 0; i < P; ++i) F->xt[i] = F->x[i] + F->alpha * F->d[i];
+  F->phase = 1;
+}
+
+// one BFGS step from the evaluation (nll, grad) of the fit's pending point
+void srv_advance(SrvFit* F, double nll, const double* grad, double gtol, int maxiter) {
+  const int P = F->P;
+  F->n_eval++;
+  if (F->phase == 0) {
+    F->f = nll;
+    F->g.assign(grad, grad + P);
+    F->H.assign((size_t)P * P, 0.0);
+    for (int i = 0; i < P; ++i) F->H[(size_t)i * P + i] = 1.0;
+    if (!std::isfinite(nll)) {
+      F->done = F->failed = true;
+      return;
+    }
+    if (inf_norm(F->g) < gtol) {
+      F->done = F->converged = true;
+      return;
+    }
+    srv_new_direction(F, true);
+    return;
+  }
+  const double c1 = 1e-4;
+  if (std::isfinite(nll) && nll <= F->f + c1 * F->alpha * F->gd) {
+    std::vector<double> s(P), y(P), Hy(P, 0.0);
+    double sy = 0.0, yy = 0.0, ss = 0.0;
+    for (int i = 0; i < P; ++i) {
+      s[i] = F->xt[i] - F->x[i];
+      y[i] = grad[i] - F->g[i];
+      sy += s[i] * y[i];
+      yy += y[i] * y[i];
+      ss += s[i] * s[i];
+    }
+    if (F->n_iter == 0 && sy > 0.0 && yy > 0.0) {  // scale the initial inverse Hessian
+      const double sc = sy / yy;
+      for (int i = 0; i < P; ++i) F->H[(size_t)i * P + i] = sc;
+    }
+    if (sy > 1e-12 * std::sqrt(ss * yy)) {
+      const double rho = 1.0 / sy;
+      double yHy = 0.0;
+      for (int i = 0; i < P; ++i) {
+        for (int j = 0; j < P; ++j) Hy[i] += F->H[(size_t)i * P + j] * y[j];
+        yHy += y[i] * Hy[i];
+      }
+      const double c = rho * rho * yHy + rho;
+      for (int i = 0; i < P; ++i)
+        for (int j = 0; j < P; ++j)
+          F->H[(size_t)i * P + j] += -rho * (Hy[i] * s[j] + s[i] * Hy[j]) + c * s[i] * s[j];
+    }
+    const double decrease = F->f - nll;
+    const double f_old = F->f;
+    F->x = F->xt;
+    F->f = nll;
+    F->g.assign(grad, grad + P);
+    F->n_iter++;
+    if (inf_norm(F->g) < gtol) {
+      F->done = F->converged = true;
+      return;
+    }
+    // no progress left above the rounding level of the NLL, or iteration cap
+    if (decrease <= 1e-12 * std::max(1.0, std::fabs(f_old)) || F->n_iter >= maxiter) {
+      F->done = true;
+      return;
+    }
+    srv_new_direction(F, false);
+    return;
+  }
+  // reject: backtrack with a safeguarded quadratic interpolation
+  if (++F->n_ls > 20) {
+    F->done = true;  // line search failed: keep the best point
+    return;
+  }
+  const double a = F->alpha;
+  double an = -F->gd * a * a / (2.0 * (nll - F->f - F->gd * a));
+  if (!std::isfinite(an)) an = 0.5 * a;
+  an = std::min(std::max(an, 0.1 * a), 0.5 * a);
+  F->alpha = an;
+  for (int i = 0; i < P; ++i) F->xt[i] = F->x[i] + an * F->d[i];
+}
+
+void srv_loop(pwa_server* S) {
+  pwa_plan* h = S->h;
+  cudaSetDevice(h->device);
+  const int P = h->n_train, NV = h->n_vars;
+  std::vector<long long> ft, nt;
+  std::vector<double> vars, sw, out;
+  for (;;) {
+    std::vector<SrvFit*> batch;
+    {
+      std::unique_lock<std::mutex> lk(S->mu);
+      if (S->stop) {  // shutting down: unfinished fits end as failed
+        for (SrvFit* F : S->active) {
+          pwa_pool_free(h, F->first_tile);
+          F->done = F->failed = true;
+        }
+        for (SrvFit* F : S->pending) F->done = F->failed = true;
+        S->active.clear();
+        S->pending.clear();
+        S->cv.notify_all();
+        return;
+      }
+      // admission: pool space and the active-fit limit
+      while (!S->pending.empty() && (int)S->active.size() < S->max_active) {
+        SrvFit* F = S->pending.front();
+        long long a = -1, b = 0;
+        if (pwa_pool_alloc(h, F->n, &a, &b) != PWA_OK) break;
+        if (pwa_pool_fill(h, a, S->consts.data(), F->xm, F->xa, F->w, F->n, F->ld, nullptr) !=
+            PWA_OK) {
+          pwa_pool_free(h, a);
+          F->done = F->failed = true;
+          F->t_done = now_s();
+          S->pending.erase(S->pending.begin());
+          continue;
+        }
+        F->first_tile = a;
+        F->n_tiles = b;
+        F->t_admit = now_s();
+        S->active.push_back(F);
+        S->pending.erase(S->pending.begin());
+      }
+      if (S->active.empty()) {
+        S->cv.wait_for(lk, std::chrono::milliseconds(2));
+        continue;
+      }
+      batch = S->active;
+    }
+    const int n = (int)batch.size();
+    ft.resize(n);
+    nt.resize(n);
+    sw.resize(n);
+    vars.resize((size_t)n * NV);
+    out.resize((size_t)n * (3 + 2 * P));
+    for (int r = 0; r < n; ++r) {
+      SrvFit* F = batch[r];
+      ft[r] = F->first_tile;
+      nt[r] = F->n_tiles;
+      sw[r] = (double)F->n;
+      double* v = vars.data() + (size_t)r * NV;
+      std::copy(S->base_vars.begin(), S->base_vars.end(), v);
+      const std::vector<double>& xe = F->phase == 0 ? F->x : F->xt;
+      for (int t = 0; t < P; ++t) v[h->train_idx[t]] = xe[t];
+    }
+    const double t0 = now_s();
+    const int rc = pwa_pieces_multi(h, n, ft.data(), nt.data(), vars.data(), sw.data(), 1.0,
+                                    nullptr, out.data());
+    const double t1 = now_s();
+    std::vector<double> grad(P);
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->batches++;
+    S->requests += n;
+    S->busy += t1 - t0;
+    for (int r = 0; r < n; ++r) {
+      SrvFit* F = batch[r];
+      if (rc != PWA_OK) {
+        F->done = F->failed = true;
+        S->err = h->err;
+      } else {
+        const double* v = out.data() + (size_t)r * (3 + 2 * P);
+        const double nll = -v[0] + v[2] * std::log(v[1]);
+        for (int t = 0; t < P; ++t) grad[t] = -v[3 + t] + v[2] * v[3 + P + t] / v[1];
+        srv_advance(F, nll, grad.data(), S->gtol, S->maxiter);
+      }
+      if (F->done) {
+        F->t_done = t1;
+        pwa_pool_free(h, F->first_tile);
+        S->active.erase(std::find(S->active.begin(), S->active.end(), F));
+      }
+    }
+    S->cv.notify_all();
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int pwa_server_create(pwa_plan* h, const double* base_vars, const double* consts, int max_active,
+                      double gtol, int maxiter, pwa_server** out) {
+  if (!out) return PWA_ERR_ARG;
+  *out = nullptr;
+  if (!h) return PWA_ERR_ARG;
+  if (!base_vars || !consts || max_active <= 0 || !(gtol > 0.0) || maxiter <= 0)
+    return set_err(h, PWA_ERR_ARG, "invalid server arguments");
+  if (!h->pool_f) return set_err(h, PWA_ERR_STATE, "no pool reserved");
+  if (h->n_coup == 0) return set_err(h, PWA_ERR_STATE, "parameter layout not set");
+  if (!h->gram_valid) return set_err(h, PWA_ERR_STATE, "MC Gram matrix not built");
+  auto* S = new pwa_server();
+  S->h = h;
+  S->base_vars.assign(base_vars, base_vars + h->n_vars);
+  S->consts.assign(consts, consts + h->nconst);
+  S->max_active = max_active;
+  S->gtol = gtol;
+  S->maxiter = maxiter;
+  S->th = std::thread(srv_loop, S);
+  *out = S;
+  return PWA_OK;
+}
+
+int pwa_server_submit(pwa_server* S, const double* x0, const double* xm, const double* xa,
+                      const double* w, long long n, long long ld, long long* fit_id) {
+  if (!S || !x0 || !w || !fit_id || n <= 0 || ld < n) return PWA_ERR_ARG;
+  auto* F = new SrvFit();
+  F->P = S->h->n_train;
+  F->x.assign(x0, x0 + F->P);
+  F->xm = xm;
+  F->xa = xa;
+  F->w = w;
+  F->n = n;
+  F->ld = ld;
+  F->t_arrive = now_s();
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (S->stop) {
+      delete F;
+      return PWA_ERR_STATE;
+    }
+    F->id = S->next_id++;
+    S->fits[F->id] = F;
+    S->pending.push_back(F);
+  }
+  S->cv.notify_all();
+  *fit_id = F->id;
+  return PWA_OK;
+}
+
+int pwa_server_result(pwa_server* S, long long fit_id, int wait, int* status, double* x,
+                      double* nll, int* n_eval, int* n_iter, double* latency_s) {
+  if (!S || !status) return PWA_ERR_ARG;
+  std::unique_lock<std::mutex> lk(S->mu);
+  auto it = S->fits.find(fit_id);
+  if (it == S->fits.end()) return PWA_ERR_ARG;
+  SrvFit* F = it->second;
+  while (wait && !F->done) S->cv.wait_for(lk, std::chrono::milliseconds(50));
+  if (!F->done) {
+    *status = 0;
+    return PWA_OK;
+  }
+  *status = F->failed ? 3 : (F->converged ? 1 : 2);
+  if (x) std::copy(F->x.begin(), F->x.end(), x);
+  if (nll) *nll = F->f;
+  if (n_eval) *n_eval = F->n_eval;
+  if (n_iter) *n_iter = F->n_iter;
+  if (latency_s) *latency_s = F->t_done - F->t_arrive;
+  return PWA_OK;
+}
+
+int pwa_server_stats(pwa_server* S, double* out) {
+  if (!S || !out) return PWA_ERR_ARG;
+  std::lock_guard<std::mutex> lk(S->mu);
+  out[0] = (double)S->batches;
+  out[1] = (double)S->requests;
+  out[2] = S->busy;
+  out[3] = (double)S->active.size();
+  out[4] = (double)S->pending.size();
+  return PWA_OK;
+}
+
+int pwa_server_destroy(pwa_server* S) {
+  if (!S) return PWA_OK;
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->stop = true;
+  }
+  S->cv.notify_all();
+  if (S->th.joinable()) S->th.join();
+  for (auto& kv : S->fits) delete kv.second;
+  delete S;
+  return PWA_OK;
+}
+
+}  // extern "C"

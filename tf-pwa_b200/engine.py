@@ -66,6 +66,12 @@ def load_library(path=LIB_PATH):
     lib.pwa_toy_fields.argtypes = [vp, ull, vp, ll, vp, ll, vp, ll, vp]
     lib.pwa_hessian_cached.argtypes = [vp, dp, ctypes.c_double, ctypes.c_double, vp, dp, dp, dp]
     lib.pwa_read_dat.argtypes = [cp, vp, ll, ctypes.POINTER(ll)]
+    lib.pwa_server_create.argtypes = [vp, dp, dp, i, ctypes.c_double, i, ctypes.POINTER(vp)]
+    lib.pwa_server_submit.argtypes = [vp, dp, vp, vp, vp, ll, ll, ctypes.POINTER(ll)]
+    ip_ = ctypes.POINTER(ctypes.c_int)
+    lib.pwa_server_result.argtypes = [vp, ll, i, ip_, dp, dp, ip_, ip_, dp]
+    lib.pwa_server_stats.argtypes = [vp, dp]
+    lib.pwa_server_destroy.argtypes = [vp]
     lib.pwa_plan_destroy.argtypes = [vp]
     lib.pwa_compile_only.argtypes = [cp, sz, i, cp, cp, sz]
     lib.pwa_upload_events.argtypes = [vp, vp, vp, vp, ll, ll, i, vp]
@@ -90,7 +96,8 @@ EXPORTED = ("pwa_plan_create", "pwa_plan_destroy", "pwa_compile_only", "pwa_uplo
             "pwa_nll_grad_cached", "pwa_set_cached_variant", "pwa_pool_reserve",
             "pwa_pool_alloc", "pwa_pool_free", "pwa_pool_fill", "pwa_pieces_multi",
             "pwa_eval_noalloc", "pwa_fields_from_p4", "pwa_toy_select", "pwa_toy_fields",
-            "pwa_hessian_cached", "pwa_read_dat",
+            "pwa_hessian_cached", "pwa_read_dat", "pwa_server_create", "pwa_server_submit",
+            "pwa_server_result", "pwa_server_stats", "pwa_server_destroy",
             "pwa_plan_info", "pwa_last_error")
 
 

@@ -11,6 +11,11 @@ join the next one; fits are admitted as pool space (the HBM budget) and
 active slots free up.  A fit's result depends only on its own data and
 parameters: the per-tile sums and the per-fit reduction order are fixed, so
 its NLL and gradient are bitwise the same alone or in any mix.
+
+``NativeFitServer`` runs the same service with each fit's BFGS driver as a
+state machine inside the native library (one scheduler thread, no
+per-fit Python threads): every round evaluates the pending point of every
+active fit in one launch and advances each optimiser by one step.
 """
 import queue
 import threading
@@ -25,7 +30,10 @@ from .engine import Engine, combine_pieces
 class FitJob:
     """One fit: its data (device columns), start values, and results."""
 
-    def __init__(self, fid, fields, x0, arrival=None, gtol=1e-5, maxiter=300):
+    sid = None
+    latency = None
+
+    def __init__(self, fid, fields, x0, arrival=None, gtol=1e-3, maxiter=300):
         self.fid = fid
         self.fields = fields          # (n_fields, N) FP64 tensor on the device
         self.n = fields.shape[1]
@@ -201,9 +209,108 @@ class FitServer:
         return combine_pieces(out[0], len(self.train))
 
 
+class NativeFitServer:
+    """The same service with every fit's BFGS driver inside the native
+    library (``pwa_server_*``): one scheduler thread evaluates the pending
+    point of every active fit in one launch per round and advances each
+    fit's BFGS state machine; Python only submits fits and reads results."""
+
+    def __init__(self, config, mc, budget_bytes, max_active=256, tpb=128, gtol=1e-3,
+                 maxiter=300):
+        import ctypes
+
+        from .engine import _dptr, load_library
+
+        self.cl = config
+        self.vm = config.vm
+        self.eng = Engine(config.decay_group, config.plan, self.vm, tpb=tpb)
+        c = self.eng.code
+        x = mc.fields
+        self._mc = (x[c.mass_fields].contiguous(), x[c.angle_fields].contiguous(),
+                    torch.full((mc.n,), 1.0 / mc.n, dtype=torch.float64, device=x.device))
+        xm, xa, wm = self._mc
+        self.eng.upload_device(xm.data_ptr(), xa.data_ptr(), wm.data_ptr(), 0, mc.n, 0.0)
+        torch.cuda.synchronize()
+        vals = self.vm.get_all_dic()
+        self.eng.set_gram(vals)
+        consts = np.ascontiguousarray(self.eng.consts(vals))
+        self.var_names = list(self.vm.variables.keys())
+        self.train = list(self.vm.trainable_vars)
+        base = np.ascontiguousarray([vals[k] for k in self.var_names], np.float64)
+        self.eng.set_param_layout(self.var_names, self.train)
+        self.tile_bytes = tpb * (8 * c.nf + 8)
+        self.pool_tiles = max(1, int(budget_bytes // self.tile_bytes))
+        self.eng.pool_reserve(self.pool_tiles)
+        self._lib = load_library()
+        self.h = ctypes.c_void_p()
+        rc = self._lib.pwa_server_create(self.eng.h, _dptr(base), _dptr(consts), int(max_active),
+                                         float(gtol), int(maxiter), ctypes.byref(self.h))
+        if rc != 0:
+            raise RuntimeError("pwa_server_create: " + self._lib.pwa_last_error(self.eng.h).decode())
+        self._keep = {}
+        self._dptr = _dptr
+
+    def submit(self, job):
+        import ctypes
+
+        c = self.eng.code
+        x = job.fields
+        xm = x[c.mass_fields].contiguous()
+        xa = x[c.angle_fields].contiguous()
+        w = torch.ones(job.n, dtype=torch.float64, device=x.device)
+        x0 = np.ascontiguousarray(job.x0, np.float64)
+        fid = ctypes.c_longlong()
+        torch.cuda.synchronize()  # the columns exist before the scheduler reads them
+        rc = self._lib.pwa_server_submit(self.h, self._dptr(x0), xm.data_ptr(), xa.data_ptr(),
+                                         w.data_ptr(), job.n, job.n, ctypes.byref(fid))
+        if rc != 0:
+            raise RuntimeError(f"pwa_server_submit failed ({rc})")
+        job.sid = fid.value
+        self._keep[job.sid] = (xm, xa, w)
+        return job
+
+    def result(self, job, wait=True):
+        """Fills job.result / n_eval / latency once the fit is final; returns
+        True then (False while it runs, with wait=False)."""
+        import ctypes
+
+        P = len(self.train)
+        st, ne, ni = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        nll, lat = ctypes.c_double(), ctypes.c_double()
+        xo = np.zeros(P)
+        rc = self._lib.pwa_server_result(self.h, job.sid, int(wait), ctypes.byref(st), self._dptr(xo),
+                                         ctypes.byref(nll), ctypes.byref(ne), ctypes.byref(ni),
+                                         ctypes.byref(lat))
+        if rc != 0:
+            raise RuntimeError(f"pwa_server_result failed ({rc})")
+        if st.value == 0:
+            return False
+        job.n_eval = ne.value
+        job.latency = lat.value
+        job.result = {"x": xo, "nll": nll.value, "success": st.value == 1, "nit": ni.value}
+        if st.value == 3:
+            job.result["error"] = "failed"
+        self._keep.pop(job.sid, None)
+        return True
+
+    def stats(self):
+        import ctypes
+
+        out = (ctypes.c_double * 5)()
+        self._lib.pwa_server_stats(self.h, out)
+        return {"rounds": int(out[0]), "requests": int(out[1]), "launch_s": out[2],
+                "active": int(out[3]), "queued": int(out[4])}
+
+    def close(self):
+        if self.h:
+            self._lib.pwa_server_destroy(self.h)
+            self.h = None
+        self.eng.close()
+
+
 def serving_benchmark(n_fits=512, n_mc=1_000_000, n_min=1_000, n_max=1_000_000,
                       budget_gb=150.0, max_active=256, rate=None, seed=11, device="cuda",
-                      config="d2kpipi.yml", maxiter=300):
+                      config="d2kpipi.yml", maxiter=300, native=True):
     """Run the toy-fit service workload; returns a dict of measurements.
 
     Fits: event counts log-uniform in [n_min, n_max] (windows into one shared
@@ -224,7 +331,11 @@ def serving_benchmark(n_fits=512, n_mc=1_000_000, n_min=1_000, n_max=1_000_000,
 
     nf = ModelCode(cl.decay_group, cl.plan).nf
     need = float(((sizes + 127) // 128).sum() * 128 * (8 * nf + 8)) * 1.05
-    server = FitServer(cl, mc, min(budget_gb * 1e9, need), max_active=max_active)
+    budget = min(budget_gb * 1e9, need)
+    if native:
+        server = NativeFitServer(cl, mc, budget, max_active=max_active, maxiter=maxiter)
+    else:
+        server = FitServer(cl, mc, budget, max_active=max_active)
     starts = rng.integers(0, data.n - sizes + 1)
     if rate is None:
         rate = n_fits / 5.0
@@ -239,22 +350,36 @@ def serving_benchmark(n_fits=512, n_mc=1_000_000, n_min=1_000, n_max=1_000_000,
         x0 = truth + rng.normal(0.0, 0.1, truth.shape)
         fields = data.fields[:, starts[i]:starts[i] + sizes[i]]
         jobs.append(server.submit(FitJob(i, fields, x0, maxiter=maxiter)))
-    for j in jobs:
-        j.done.wait()
+    if native:
+        for j in jobs:
+            server.result(j, wait=True)
+        lat = np.array([j.latency for j in jobs])
+        st = server.stats()
+        rounds, reqs = st["rounds"], st["requests"]
+        batch_info = {"batches": rounds, "mean_requests_per_batch": reqs / max(rounds, 1),
+                      "launch_seconds": st["launch_s"]}
+    else:
+        for j in jobs:
+            j.done.wait()
+        lat = np.array([j.finished - j.arrival for j in jobs])
+        batches = np.array(server.batches) if server.batches else np.zeros((1, 3))
+        batch_info = {"batches": len(server.batches),
+                      "mean_requests_per_batch": float(batches[:, 0].mean()),
+                      "max_requests_per_batch": int(batches[:, 0].max()),
+                      "mean_batch_ms": 1e3 * float(batches[:, 2].mean())}
     t_total = time.perf_counter() - t_start
-    lat = np.array([j.finished - j.arrival for j in jobs])
     evals = int(sum(j.n_eval for j in jobs))
     errors = [j.result.get("error") for j in jobs if "error" in j.result]
-    batches = np.array(server.batches) if server.batches else np.zeros((1, 3))
-    server.close()
-    return {
+    converged = sum(1 for j in jobs if j.result.get("success"))
+    out = {
+        "driver": "native BFGS state machines" if native else "scipy BFGS, one thread per fit",
         "n_fits": n_fits, "evals": evals, "seconds": t_total, "evals_per_s": evals / t_total,
         "latency_p50_s": float(np.percentile(lat, 50)),
         "latency_p99_s": float(np.percentile(lat, 99)),
-        "mean_evals_per_fit": evals / n_fits, "errors": len(errors),
-        "batches": len(server.batches), "mean_requests_per_batch": float(batches[:, 0].mean()),
-        "max_requests_per_batch": int(batches[:, 0].max()),
-        "mean_batch_ms": 1e3 * float(batches[:, 2].mean()),
+        "mean_evals_per_fit": evals / n_fits, "errors": len(errors), "converged": converged,
         "events_total": int(sizes.sum()), "pool_tiles": server.pool_tiles,
         "pool_gb": server.pool_tiles * server.tile_bytes / 1e9, "budget_gb": budget_gb,
     }
+    out.update(batch_info)
+    server.close()
+    return out
