@@ -241,7 +241,7 @@ const char* pwa_last_error(pwa_plan* h);
  * significance studies, tf_pwa/fit.py:189-419 per fit) sharing the plan's
  * MC Gram matrix.  Each fit is a BFGS state machine (inverse-Hessian
  * update, backtracking Armijo line search; converged at max|g| < gtol,
- * stopped when a step lowers the NLL by less than 1e-12 relative, after 20
+ * stopped when a step lowers the NLL by less than 1e-14 relative, after 20
  * backtracks or at maxiter iterations); one scheduler thread admits fits into the plan's tile pool
  * (pwa_pool_reserve first) and evaluates the pending point of every active
  * fit in one multi-request launch per round.  base_vars: all variables

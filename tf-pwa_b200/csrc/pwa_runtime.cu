@@ -1344,7 +1344,7 @@ extern "C" int pwa_eval_noalloc(pwa_plan* h, const double* consts, const double*
 // every round evaluates the pending point of EVERY active fit in one
 // multi-request launch (pwa_pieces_multi), then advances each state machine
 // by one step.  No per-fit threads, no interpreter in the loop.  A fit also
-// stops (status 2) when an accepted step lowers the NLL by less than 1e-12
+// stops (status 2) when an accepted step lowers the NLL by less than 1e-14
 // relative (the rounding level), after 20 backtracks, or at maxiter.  A fit's
 // evaluations depend only on its own events and parameters (per-fit ordered
 // sums), so its path and result are bitwise the same alone or in any mix.
@@ -1476,7 +1476,7 @@ void srv_advance(SrvFit* F, double nll, const double* grad, double gtol, int max
       return;
     }
     // no progress left above the rounding level of the NLL, or iteration cap
-    if (decrease <= 1e-12 * std::max(1.0, std::fabs(f_old)) || F->n_iter >= maxiter) {
+    if (decrease <= 1e-14 * std::max(1.0, std::fabs(f_old)) || F->n_iter >= maxiter) {
       F->done = true;
       return;
     }
