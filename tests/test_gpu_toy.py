@@ -12,7 +12,7 @@
 import numpy as np
 import pytest
 
-from common import golden_data, load_golden, load_model
+from common import load_golden, load_model
 
 pytestmark = pytest.mark.gpu
 

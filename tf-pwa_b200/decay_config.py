@@ -24,7 +24,6 @@ import numpy as np
 import yaml
 
 from .particles import Decay, DecayChain, DecayGroup, Particle, var_name
-from .variables import VarsManager
 
 _PARTICLE_KEYS = {
     "Par": "P",

@@ -30,7 +30,6 @@ bounds) and the amplitude accept draw.
 """
 import math
 
-from .plan import ChainTopology  # noqa: F401  (topologies come from the plan)
 
 
 def _f(v):

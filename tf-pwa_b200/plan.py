@@ -19,7 +19,6 @@ standard topology; a chain reads the angles of its own decay's ``outs[0]``
 (``tf_pwa/amp/core.py:1414-1429``).  Helicity ``gamma`` is identically zero
 for two-body helicity angles and is not stored.
 """
-from .particles import DecayChain
 
 
 def node_name(finals):
