@@ -57,6 +57,7 @@ def test_small_and_ragged_sets(nd, nm):
 def test_error_codes_before_launch():
     from tf_pwa_b200.engine import Engine, load_library
 
+    ARG, STATE, OOM = 1, 4, 5  # PWA_ERR_* of include/pwa_b200.h
     lib = load_library()
     g, meta = load_golden("d2kpipi")
     dc, vm, plan = load_model(meta["config"])
@@ -68,27 +69,27 @@ def test_error_codes_before_launch():
     out = np.zeros(2 * eng.code.nacc)
     op = out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
     # nothing uploaded yet
-    assert lib.pwa_eval(h, cp, 0, 1, None, op) == 3  # PWA_ERR_STATE
-    assert lib.pwa_eval_cached_enqueue(h, cp, None) == 3
-    assert lib.pwa_set_cached_variant(h, 7) == 1  # PWA_ERR_ARG
+    assert lib.pwa_eval(h, cp, 0, 1, None, op) == STATE
+    assert lib.pwa_eval_cached_enqueue(h, cp, None) == STATE
+    assert lib.pwa_set_cached_variant(h, 7) == ARG
     # uploads with bad sizes
-    assert lib.pwa_upload_events(h, None, None, None, 0, 0, 0, None) == 1
+    assert lib.pwa_upload_events(h, None, None, None, 0, 0, 0, None) == ARG
     x, w = golden_data(g, meta)
     eng.upload(x, w, g["fields_mc"], np.ones(g["fields_mc"].shape[1]))
-    assert lib.pwa_eval(h, cp, 5, 1, None, op) == 1  # unknown precision
+    assert lib.pwa_eval(h, cp, 5, 1, None, op) == ARG  # unknown precision
     # pool before reservation, fill of an unallocated run
     a, b = ctypes.c_longlong(), ctypes.c_longlong()
-    assert lib.pwa_pool_alloc(h, 10, ctypes.byref(a), ctypes.byref(b)) == 3
+    assert lib.pwa_pool_alloc(h, 10, ctypes.byref(a), ctypes.byref(b)) == STATE
     eng.pool_reserve(4)
-    assert lib.pwa_pool_alloc(h, 10 ** 6, ctypes.byref(a), ctypes.byref(b)) == 5  # PWA_ERR_OOM
-    assert lib.pwa_pool_fill(h, 2, cp, None, None, None, 10, 10, None) == 1
+    assert lib.pwa_pool_alloc(h, 10 ** 6, ctypes.byref(a), ctypes.byref(b)) == OOM
+    assert lib.pwa_pool_fill(h, 2, cp, None, None, None, 10, 10, None) == ARG
     # dataset-step calls: empty and inconsistent sizes
     assert lib.pwa_toy_select(h, cp, 1, 0, 0, 0.0, 0, None, None) == 0
-    assert lib.pwa_fields_from_p4(h, None, 5, 4, None, 5, None) == 1
+    assert lib.pwa_fields_from_p4(h, None, 5, 4, None, 5, None) == ARG
     # server needs a parameter layout and a Gram matrix
     srv = ctypes.c_void_p()
     base = np.zeros(len(vm.variables))
     assert lib.pwa_server_create(h, base.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), cp,
-                                 4, 1e-3, 10, ctypes.byref(srv)) == 3
+                                 4, 1e-3, 10, ctypes.byref(srv)) == STATE
     assert lib.pwa_last_error(h)
     eng.close()
