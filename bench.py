@@ -278,6 +278,17 @@ def run_floating(args, rank, world, timed_factory):
     fcn = FCN(cl, data, mc, precision="mixed")
     assert not fcn.use_gram
     fcn_p = FCN(cl, data, mc, precision="plain")
+    if world > 1:
+        import torch.distributed as dist
+
+        def reduce_fn(vec):
+            t = torch.as_tensor(vec, device="cuda")
+            dist.all_reduce(t)
+            return t.cpu().numpy()
+
+        for f in (fcn, fcn_p):
+            f.eng.dist_reduce = reduce_fn
+            f.eng.mc_share = 1.0 / world  # equal MC shards
     x0 = np.array(cl.vm.get_all_val())
     vals, names = cl.vm.get_all_dic(), list(cl.vm.trainable_vars)
     timed = timed_factory()
@@ -315,7 +326,7 @@ def run_floating(args, rank, world, timed_factory):
                    "no column cache since masses and widths float",
                    "events_per_rank": {"data": args.n_sig, "mc": args.n_mc},
                    "l2": "256 MB buffer written before every timed step (L2 126 MB)",
-                   "parallelism": "single GPU"},
+                   "parallelism": f"dp{world}" if world > 1 else "single GPU"},
         "plain_f64": {"value": world * args.steps / t_p, "unit": "evals/s",
                       "ms_per_step": 1e3 * t_p / args.steps,
                       "speedup_f32_over_plain": t_p / t_f32},
