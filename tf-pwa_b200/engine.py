@@ -264,6 +264,12 @@ class Engine:
             for n in names:
                 if n not in self.coupling_names:
                     self.coupling_names.append(n)
+        # membership tests on particles/decays compare keys; precompute them
+        self._inner_keys = {id(c): {p.key() for p in c.inner} for c in g}
+        self._vertex_chain = {}
+        for c in g:
+            for d in c:
+                self._vertex_chain.setdefault(d.key(), c)
         self.res_info = {}
         for p in g.resonances:
             chains = [c for c in g if p in c.inner]
@@ -309,9 +315,28 @@ class Engine:
             self._slot_vg.append((self._cn_index[n], cidx[f"t{ci}.re"], cidx[f"t{ci}.im"]))
         a = np.array(self._slot_vg, np.int64).reshape(-1, 3)
         self._vg_src, self._vg_re, self._vg_im = a[:, 0], a[:, 1], a[:, 2]
+        # constant-block slots of the lineshape and barrier constants
+        self._res_slots = []
+        for p, kind in self.code.res:
+            if kind == "one":
+                continue
+            self._res_slots.append((p, kind, cidx[f"{p}.m0sq"],
+                                    cidx.get(f"{p}.K"), cidx.get(f"{p}.useq"), cidx.get(f"{p}.y")))
+        self._vtx_slots = []
+        for d in self.code.vertices:
+            sl = {}
+            for l in sorted(set(d.get_l_list())):
+                sl[l] = (cidx.get(f"{d}.Pz0_{l}") if d.has_barrier_factor and d.has_bprime else None,
+                         cidx.get(f"{d}.norm_{l}") if d.has_barrier_factor and d.barrier_factor_norm
+                         else None)
+            self._vtx_slots.append((d, self._vertex_chain[d.key()], sl))
+        self._shape_slots = [(p, cidx[f"{p}.kappa_m"], cidx[f"{p}.inv_g0"])
+                             for p in self.code.shape_res]
+        self._mass_names = {f"{p.params_head}_mass": p for p in self.group.resonances}
+        self._width_names = {f"{p.params_head}_width": p for p in self.group.resonances}
 
     def _nominal(self, p, vals, chain):
-        if p in chain.inner:
+        if p.key() in self._inner_keys[id(chain)]:
             return vals.get(f"{p.params_head}_mass", p.mass)
         return p.mass
 
@@ -393,46 +418,35 @@ class Engine:
         self._cph = np.array([vals[n] for n in self._cn_i])
         C[0:2 * c.ncol:2] = self._ck.real
         C[1:2 * c.ncol:2] = self._ck.imag
-        for d in c.vertices:
-            for i in range(len(d.get_ls_list())):
-                z = cv.get(f"{d.params_head}_g_ls_{i}")
-                if z is None:
-                    z = self.complex_val(vals, f"{d.params_head}_g_ls_{i}")
-                C[idx[f"{d}.g{i}.re"]] = z.real
-                C[idx[f"{d}.g{i}.im"]] = z.imag
-        for ci, ch in enumerate(self.group):
-            z = cv[ch.params_head + "_total_0"]
-            C[idx[f"t{ci}.re"]] = z.real
-            C[idx[f"t{ci}.im"]] = z.imag
-        for p, kind in c.res:
-            if kind == "one":
-                continue
+        C[self._vg_re] = self._cvec[self._vg_src].real
+        C[self._vg_im] = self._cvec[self._vg_src].imag
+        for p, kind, s_m0sq, s_k, s_useq, s_y in self._res_slots:
             dp, chain = self.res_info[p]
             m0 = self._nominal(p, vals, chain)
-            C[idx[f"{p}.m0sq"]] = m0 * m0
+            C[s_m0sq] = m0 * m0
             if kind == "BWR":
                 K, useq = self._lineshape_K(p, vals)
-                C[idx[f"{p}.K"]] = K
-                C[idx[f"{p}.useq"]] = useq
+                C[s_k] = K
+                C[s_useq] = useq
             else:
-                C[idx[f"{p}.y"]] = m0 * vals.get(f"{p.params_head}_width", p.width)
-        for d in c.vertices:
-            chain = [ch for ch in self.group if d in ch.decays][0]
+                C[s_y] = m0 * vals.get(f"{p.params_head}_width", p.width)
+        for d, chain, sl in self._vtx_slots:
             vc = self._vertex_consts(d, chain, vals)
             for l, (pz0, norm) in vc.items():
-                if d.has_barrier_factor and d.has_bprime:
-                    C[idx[f"{d}.Pz0_{l}"]] = pz0
-                if d.has_barrier_factor and d.barrier_factor_norm:
-                    C[idx[f"{d}.norm_{l}"]] = norm
-        for p in c.shape_res:
+                s_pz, s_norm = sl[l]
+                if s_pz is not None:
+                    C[s_pz] = pz0
+                if s_norm is not None:
+                    C[s_norm] = norm
+        for p, s_kap, s_ig in self._shape_slots:
             dp, chain = self.res_info[p]
             m0 = self._nominal(p, vals, chain)
             g0 = vals.get(f"{p.params_head}_width", p.width)
             h = 1e-20
             Kc, _ = self._lineshape_K(p, vals, m0=m0 + 1j * h)
             K0, _ = self._lineshape_K(p, vals, m0=m0)
-            C[idx[f"{p}.kappa_m"]] = np.imag(Kc) / h / np.real(K0) if np.real(K0) != 0 else 0.0
-            C[idx[f"{p}.inv_g0"]] = 1.0 / g0 if g0 else 0.0
+            C[s_kap] = np.imag(Kc) / h / np.real(K0) if np.real(K0) != 0 else 0.0
+            C[s_ig] = 1.0 / g0 if g0 else 0.0
         return C
 
     # ------------------------------------------------------------ jacobian
@@ -499,37 +513,42 @@ class Engine:
                 D[pi] = cached[1][pi]
                 continue
             # masses / widths
-            hit = None
-            for p in self.group.resonances:
-                if n == f"{p.params_head}_mass":
-                    hit = (p, "m")
-                elif n == f"{p.params_head}_width":
-                    hit = (p, "g")
-            if hit is None:
+            if n in self._mass_names:
+                p, kind = self._mass_names[n], "m"
+            elif n in self._width_names:
+                p, kind = self._width_names[n], "g"
+            else:
                 raise KeyError(f"unknown parameter {n}")
-            p, kind = hit
             if (p, kind) in self.shape_index:
                 D[pi, self.shape_index[(p, kind)]] = 1.0
             if kind == "m":
-                # barrier factors through q0^2 of every vertex touching p
+                # barrier factors through q0^2 of every vertex touching p:
+                # complex-step derivative of each vertex's constants, once
+                hh = 1e-20
+                dlog = {}  # (chain index, vertex index) -> {l: d ln bf_l / dm}
                 for k, (ci, lsi) in enumerate(c.columns):
                     chain = self.group[ci]
-                    if p not in chain.inner:
+                    if p.key() not in self._inner_keys[id(chain)]:
                         continue
                     kap = 0.0
                     for vi, d in enumerate(chain):
                         if p not in (d.core,) + d.outs or not d.has_barrier_factor:
                             continue
-                        l = d.get_ls_list()[lsi[vi]][0]
-                        hh = 1e-20
-                        m0 = self._nominal(p, vals, chain)
-                        vc = self._vertex_consts(d, chain, vals, {p: m0 + 1j * hh})
-                        v0 = self._vertex_consts(d, chain, vals)
-                        # bf_l ~ sqrt(Pz0_l) * norm_l
-                        if d.has_bprime:
-                            kap += 0.5 * np.imag(vc[l][0]) / hh / np.real(v0[l][0])
-                        if d.barrier_factor_norm:
-                            kap += np.imag(vc[l][1]) / hh / np.real(v0[l][1])
+                        if (ci, vi) not in dlog:
+                            m0 = self._nominal(p, vals, chain)
+                            vc = self._vertex_consts(d, chain, vals, {p: m0 + 1j * hh})
+                            v0 = self._vertex_consts(d, chain, vals)
+                            e = {}
+                            for l in v0:
+                                t = 0.0
+                                # bf_l ~ sqrt(Pz0_l) * norm_l
+                                if d.has_bprime:
+                                    t += 0.5 * np.imag(vc[l][0]) / hh / np.real(v0[l][0])
+                                if d.barrier_factor_norm:
+                                    t += np.imag(vc[l][1]) / hh / np.real(v0[l][1])
+                                e[l] = t
+                            dlog[(ci, vi)] = e
+                        kap += dlog[(ci, vi)][d.get_ls_list()[lsi[vi]][0]]
                     J[pi, k] += self._ck[k] * kap
         if cached is None and key[1] is not None:
             # mass/width rows: J = kappa_k * c_k with kappa fixed per shape setting
