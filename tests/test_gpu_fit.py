@@ -125,3 +125,32 @@ def test_native_hessian_equals_python_stencil():
     np.testing.assert_allclose(H_c, H_p, rtol=0, atol=1e-4 * np.abs(H_p).max())
     fm.eng.close()
     fp.eng.close()
+
+
+def test_bounded_fit_stays_inside_bounds(tmp_path):
+    """A fit with a floating mass bounded to a window that excludes the
+    generated value ends on the window's edge (the transform keeps it
+    inside), with the gradient chain rule through dy/dx."""
+    import os
+
+    import yaml
+
+    from tf_pwa_b200.api import FCN, ConfigLoader
+    from tf_pwa_b200.workload import make_dataset
+
+    cl0, data, _, mc = make_dataset("d2kpipi_float.yml", 20000, 40000, seed=9)
+    dic = yaml.safe_load(open(os.path.join(CONFIGS, "d2kpipi_float.yml")))
+    m_true = float(cl0.vm.get("R1_mass"))
+    dic["particle"]["R1"].update({"mass_min": m_true + 0.01, "mass_max": m_true + 0.05})
+    f = tmp_path / "c.yml"
+    f.write_text(yaml.safe_dump(dic))
+    cl = ConfigLoader(str(f))
+    cl.vm.set_all(cl0.vm.get_all_dic())
+    cl.vm.set_all({"R1_mass": m_true + 0.03})
+    fcn = FCN(cl, data, mc, precision="plain")
+    r = cl.fit(fcn=fcn, gtol=1e-4, maxiter=400)
+    m_fit = float(cl.vm.get("R1_mass"))
+    assert m_true + 0.01 - 1e-12 <= m_fit <= m_true + 0.05 + 1e-12
+    assert abs(m_fit - (m_true + 0.01)) < 2e-3  # pushed to the lower edge
+    assert np.isfinite(r.min_nll)
+    fcn.eng.close()

@@ -27,7 +27,7 @@ from .decay_config import DecayConfig, float_particles, init_params, load_yaml
 from .engine import MIXED_F32, PLAIN_F64, Engine, read_dat
 from .kinematics import event_fields, p4_dict
 from .plan import Plan
-from .variables import VarsManager
+from .variables import Bound, VarsManager
 
 PRECISIONS = {"plain": PLAIN_F64, "f64": PLAIN_F64, "mixed": MIXED_F32, "chosen": MIXED_F32}
 
@@ -296,8 +296,8 @@ class ConfigLoader:
         self.vm = vm if vm is not None else VarsManager(
             rng=np.random.default_rng(seed))
         self._names = init_params(self.decay_group, self.vm, self.config.get("constrains"))
-        float_particles(self.decay_group, self.vm, self._names,
-                        self.decay_config.particle_property)
+        self.bound_dic = float_particles(self.decay_group, self.vm, self._names,
+                                         self.decay_config.particle_property)
         self.plan = Plan(self.decay_group, self.config.get("data", {}).get("dat_order"))
         self.precision = precision
         self._amp = None
@@ -416,12 +416,33 @@ class ConfigLoader:
 
         if fcn is None:
             fcn = self.get_fcn(None if data is None else [data, phsp, bg], batch, precision)
-        x0 = np.array(self.vm.get_all_val())
-        maxiter = maxiter or max(100 * len(x0), 2000)
+        y0 = np.array(self.vm.get_all_val())
+        maxiter = maxiter or max(100 * len(y0), 2000)
+        # bounded variables are fitted through their transform
+        # (tf_pwa/fit.py:270-280, vm.trans_fcn_grad)
+        names = list(self.vm.trainable_vars)
+        bounds = {i: Bound(*self.bound_dic[n]) for i, n in enumerate(names)
+                  if n in getattr(self, "bound_dic", {})}
+
+        def to_y(x):
+            y = np.array(x, dtype=float)
+            for i, b in bounds.items():
+                y[i] = b.x2y(x[i])
+            return y
+
+        def fg(x):
+            nll, g = fcn.nll_grad(to_y(x))
+            g = np.array(g, dtype=float)
+            for i, b in bounds.items():
+                g[i] *= b.dydx(x[i])
+            return nll, g
+
+        x0 = y0.copy()
+        for i, b in bounds.items():
+            x0[i] = b.y2x(y0[i])
         t0 = time.time()
-        res = minimize(lambda x: fcn.nll_grad(x), x0, jac=True, method=method,
-                       options={"maxiter": maxiter, "gtol": gtol})
-        self.vm.set_all(list(res.x))
+        res = minimize(fg, x0, jac=True, method=method, options={"maxiter": maxiter, "gtol": gtol})
+        self.vm.set_all(list(to_y(res.x)))
         self.vm.std_polar_all()
         fr = FitResult(self.get_params(), fcn, res.fun, ndf=len(x0), success=bool(res.success),
                        message=str(res.message), hess_inv=getattr(res, "hess_inv", None),

@@ -304,6 +304,11 @@ def init_params(group, vm, constrains=None):
 
 
 def float_particles(group, vm, names, particle_property):
+    """Free the masses/widths marked ``float: m``/``g``; returns the fit
+    bounds {variable: (lower, upper)} from ``mass_min``/``mass_max`` and
+    ``width_min``/``width_max`` (None where not given), as
+    ``tf_pwa/config_loader/config_loader.py:460-496`` collects them."""
+    bounds = {}
     for c in group:
         for p in c.inner:
             cfg = particle_property.get(p.name, {})
@@ -312,7 +317,10 @@ def float_particles(group, vm, names, particle_property):
                 n = names["mass"][p]
                 if n not in vm.trainable_vars:
                     vm.set_fix(n, unfix=True)
+                bounds[n] = (cfg.get("mass_min"), cfg.get("mass_max"))
             if "g" in fl and p in names["width"]:
                 n = names["width"][p]
                 if n not in vm.trainable_vars:
                     vm.set_fix(n, unfix=True)
+                bounds[n] = (cfg.get("width_min"), cfg.get("width_max"))
+    return {k: v for k, v in bounds.items() if v != (None, None)}

@@ -124,3 +124,55 @@ class VarsManager:
                 r, p = -r, p + np.pi
             p = (p + np.pi) % (2 * np.pi) - np.pi
             self.variables[name + "r"], self.variables[name + "i"] = r, p
+
+
+class Bound:
+    """Boundary transform of one fit variable (``tf_pwa/variable.py:1029-1130``,
+    default functions): the optimiser works on an unbounded x, the model on
+    y = f(x) inside (lower, upper):
+
+    * both bounds: y = (b - a)(sin x + 1)/2 + a
+    * lower only:  y = a - 1 + sqrt(x^2 + 1)
+    * upper only:  y = b + 1 - sqrt(x^2 + 1)
+
+    Closed forms of f, dy/dx and the inverse (y clipped into the range first,
+    the non-negative root of the one-sided forms)."""
+
+    def __init__(self, lower=None, upper=None):
+        if lower is not None and upper is not None and lower > upper:
+            raise ValueError("lower bound is larger than upper bound")
+        self.lower, self.upper = lower, upper
+
+    def x2y(self, x):
+        a, b = self.lower, self.upper
+        if a is not None and b is not None:
+            return (b - a) * (np.sin(x) + 1) / 2 + a
+        if a is not None:
+            return a - 1 + np.sqrt(x * x + 1)
+        if b is not None:
+            return b + 1 - np.sqrt(x * x + 1)
+        return x
+
+    def dydx(self, x):
+        a, b = self.lower, self.upper
+        if a is not None and b is not None:
+            return (b - a) * np.cos(x) / 2
+        if a is not None:
+            return x / np.sqrt(x * x + 1)
+        if b is not None:
+            return -x / np.sqrt(x * x + 1)
+        return 1.0
+
+    def y2x(self, y):
+        a, b = self.lower, self.upper
+        if a is not None:
+            y = max(y, a)
+        if b is not None:
+            y = min(y, b)
+        if a is not None and b is not None:
+            return float(np.arcsin(np.clip(2 * (y - a) / (b - a) - 1, -1.0, 1.0)))
+        if a is not None:
+            return float(np.sqrt(max((y - a + 1) ** 2 - 1, 0.0)))
+        if b is not None:
+            return float(np.sqrt(max((b + 1 - y) ** 2 - 1, 0.0)))
+        return float(y)
