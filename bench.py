@@ -353,6 +353,11 @@ def run_floating(args, rank, world, timed_factory):
         print(json.dumps(line), flush=True)
     fcn.eng.close()
     fcn_p.eng.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 # ------------------------------------------------------------- serving arm
