@@ -48,6 +48,13 @@ WORKLOADS = {
                  "accept-reject data, 4e6 flat MC"),
 }
 CONFIG, N_SIG, N_BG, N_MC, METRIC, WORKLOAD = WORKLOADS["lc2pkpi"]
+# DRAM bytes (read + write) per data event of one launch of the cached
+# data-term kernel, from the ncu captures summarised in
+# profiles/pwa_eval_cached_wred_lc2pkpi.md (290.4 + 6.8 MB, 1.1e6 rows) and
+# profiles/pwa_eval_cached_wred_b2dstkpi.md (248.0 + 3.6 MB, 1e6 rows);
+# traffic grows with the rows, so a launch's traffic = this x its rows
+NCU_TRAFFIC_PER_ROW = {"lc2pkpi": (290.436096e6 + 6.841088e6) / 1.1e6,
+                       "b2dstkpi": (248.044032e6 + 3.609856e6) / 1e6}
 
 
 def _select(name):
@@ -566,7 +573,12 @@ def main():
                 "d2h_bytes_per_step": 8 * (1 + 2 * code.ncol),
                 "call": "FCN.nll_grad(x) with x a host numpy vector"},
         "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
-                     "frac": ach / hbm, "traffic": None, "peak_kind": peak_kind,
+                     "frac": ach / hbm,
+                     "traffic": (NCU_TRAFFIC_PER_ROW[args.workload] * n_data
+                                 if args.workload in NCU_TRAFFIC_PER_ROW else None),
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
+                                       "launch (profiles/), scaled by the rows",
+                     "peak_kind": peak_kind,
                      "kernel": "pwa_eval_cached_wred (data term, mixed form; ends with its "
                                "own fixed-order two-level reduction)",
                      "algorithmic_bytes_per_launch": bytes_mixed,
