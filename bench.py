@@ -49,10 +49,9 @@ WORKLOADS = {
 }
 CONFIG, N_SIG, N_BG, N_MC, METRIC, WORKLOAD = WORKLOADS["lc2pkpi"]
 # DRAM bytes (read + write) per data event of one launch of the cached
-# data-term kernel, from the ncu captures summarised in
-# profiles/pwa_eval_cached_wred_lc2pkpi.md (290.4 + 6.8 MB, 1.1e6 rows) and
-# profiles/pwa_eval_cached_wred_b2dstkpi.md (248.0 + 3.6 MB, 1e6 rows);
-# traffic grows with the rows, so a launch's traffic = this x its rows
+# data-term kernel, from ncu captures of that kernel at the bench sizes
+# (Lambda_c: 290.4 + 6.8 MB for 1.1e6 rows; four-body: 248.0 + 3.6 MB for
+# 1e6 rows); traffic grows with the rows, so a launch's traffic = this x rows
 NCU_TRAFFIC_PER_ROW = {"lc2pkpi": (290.436096e6 + 6.841088e6) / 1.1e6,
                        "b2dstkpi": (248.044032e6 + 3.609856e6) / 1e6}
 
@@ -577,7 +576,7 @@ def main():
                      "traffic": (NCU_TRAFFIC_PER_ROW[args.workload] * n_data
                                  if args.workload in NCU_TRAFFIC_PER_ROW else None),
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
-                                       "launch (profiles/), scaled by the rows",
+                                       "launch at the bench size, scaled by the rows",
                      "peak_kind": peak_kind,
                      "kernel": "pwa_eval_cached_wred (data term, mixed form; ends with its "
                                "own fixed-order two-level reduction)",
