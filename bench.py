@@ -78,6 +78,15 @@ def _peaks():
 
 
 # ----------------------------------------------------------------- clocks
+def _clocks_path(rank):
+    """Where the nvidia-smi samples of the timed region go (PWA_CLOCKS_DIR,
+    default the system temp directory)."""
+    import tempfile
+
+    d = os.environ.get("PWA_CLOCKS_DIR") or tempfile.gettempdir()
+    return os.path.join(d, f"clocks_rank{rank}.csv")
+
+
 class Clocks:
     def __init__(self, path):
         self.path = path
@@ -301,8 +310,7 @@ def run_floating(args, rank, world, timed_factory):
     for _ in range(args.warmup):
         fcn.nll_grad(x0)
         fcn_p.nll_grad(x0)
-    clocks = Clocks(os.path.join(ROOT, "gpurun_out", f"clocks_rank{rank}.csv")
-                    if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else f"/tmp/clocks{rank}.csv")
+    clocks = Clocks(_clocks_path(rank))
     clocks.start()
     t_f32 = timed(lambda: fcn.nll_grad(x0), args.steps)
     t_p = timed(lambda: fcn_p.nll_grad(x0), args.steps)
@@ -505,8 +513,7 @@ def main():
         fcn.nll_grad(x0)
         fcn_plain.nll_grad(x0)
 
-    clocks = Clocks(os.path.join(ROOT, "gpurun_out", f"clocks_rank{rank}.csv")
-                    if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else f"/tmp/clocks{rank}.csv")
+    clocks = Clocks(_clocks_path(rank))
     clocks.start()
     # headline: one NLL+gradient evaluation per step through the C ABI
     # (couplings -> cached-column kernel + Gram MC term -> chain rule)
