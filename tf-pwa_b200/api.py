@@ -13,12 +13,14 @@ path use, with the same names, arguments and parameter conventions:
 * ``FitResult``: ``tf_pwa/fit.py:497-536``.
 
 Data: the reference's ``E px py pz`` text files or ``.npy`` arrays, grouped
-per event in ``dat_order`` (``tf_pwa/data.py:300-365``); background files
-enter with weight ``-bg_weight`` (``config_loader/data.py:149-155,421-429``).
+per event in ``dat_order`` (``tf_pwa/data.py:300-365``); an index matching
+``negtive_idx`` (default ``bg*``) enters with weight ``-<idx>_weight``
+(``config_loader/data.py:149-169,215-232``).
 Every evaluation runs on the CUDA engine; there is no CPU path.
 """
 import json
 import os
+import re
 import time
 
 import numpy as np
@@ -346,20 +348,27 @@ class ConfigLoader:
             return None
         if isinstance(files, str):
             files = [files]
-        ret = []
+        # weight = sign * (scalar ``<idx>_weight`` or the concatenated weight
+        # files cut to the events read), sign -1 for indices matching
+        # ``negtive_idx`` (default "bg*")
+        wkey = dcfg.get(idx + "_weight")
+        wfile = None
+        if wkey is not None and not isinstance(wkey, (int, float)):
+            wfile = np.concatenate([np.loadtxt(self._path(x)).reshape(-1)
+                                    for x in (wkey if isinstance(wkey, list) else [wkey])])
+        sign = -1.0 if any(re.match(pat, idx) for pat in dcfg.get("negtive_idx", ["bg*"])) else 1.0
+        ret, off = [], 0
         for f in files:
             p4 = self.load_p4([f])
             n = p4.shape[0]
-            w = np.ones(n)
-            wkey = dcfg.get(idx + "_weight")
-            if isinstance(wkey, (int, float)):
-                w = w * float(wkey)
-            elif wkey is not None:
-                w = np.concatenate([np.loadtxt(self._path(x)).reshape(-1)
-                                    for x in (wkey if isinstance(wkey, list) else [wkey])])[:n]
-            if idx == "bg":
-                w = -abs(float(dcfg.get("bg_weight", 1.0))) * w if wkey is None or isinstance(wkey, (int, float)) else -w
-            ret.append(self.data_from_p4(p4, w))
+            if wfile is not None:
+                w = wfile[off:off + n]
+                if w.shape[0] != n:
+                    raise ValueError(f"{idx}_weight holds {wfile.shape[0]} values for more events")
+            else:
+                w = np.full(n, 1.0 if wkey is None else float(wkey))
+            off += n
+            ret.append(self.data_from_p4(p4, sign * w))
         self._data[idx] = ret
         return ret
 
