@@ -217,19 +217,31 @@ class FCN:
             v = self.vm.variables
             return self.eng.hessian_cached([v[k] for k in self._var_names], step)
         x0 = np.array(self.vm.get_all_val())
-        nll, g0 = self.get_nll_grad(x0)
-        P = len(x0)
-        H = np.zeros((P, P))
-        for i in range(P):
-            h = step * max(abs(x0[i]), 1e-2)
-            gs = []
-            for s in (-2, -1, 1, 2):
-                xs = x0.copy()
-                xs[i] += s * h
-                gs.append(self.get_nll_grad(xs)[1])
-            H[i] = (gs[0] - 8 * gs[1] + 8 * gs[2] - gs[3]) / (12 * h)
+        nll, g0, H = hessian_from_gradient(self.get_nll_grad, x0, step)
         self._set(x0)
-        return nll, g0, 0.5 * (H + H.T)
+        return nll, g0, H
+
+
+def hessian_from_gradient(nll_grad, x0, step):
+    """(f, g, H) at ``x0`` from a function returning (f, gradient): row i of
+    H is the 4-point central difference (g(x-2h) - 8g(x-h) + 8g(x+h) -
+    g(x+2h)) / 12h along parameter i, h = step * max(|x0_i|, 1e-2), exact
+    for gradients polynomial up to degree 4; the result is symmetrised.
+    Stands in for the reference's nested-tape ``sum_hessian``
+    (``tf_pwa/model/model.py:97-140``)."""
+    x0 = np.asarray(x0, dtype=np.float64)
+    f0, g0 = nll_grad(x0)
+    P = len(x0)
+    H = np.zeros((P, P))
+    for i in range(P):
+        h = step * max(abs(x0[i]), 1e-2)
+        gs = []
+        for s in (-2, -1, 1, 2):
+            xs = x0.copy()
+            xs[i] += s * h
+            gs.append(np.asarray(nll_grad(xs)[1], dtype=np.float64))
+        H[i] = (gs[0] - 8 * gs[1] + 8 * gs[2] - gs[3]) / (12 * h)
+    return f0, np.asarray(g0, dtype=np.float64), 0.5 * (H + H.T)
 
 
 class NLLFunction:
