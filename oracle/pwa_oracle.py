@@ -19,6 +19,7 @@ per-event inputs (invariant masses and helicity / alignment angles):
 * helicity coupling H = sum_ls g_ls bf_ls CG_ls: ``tf_pwa/amp/core.py:931-947,1025-1043``
 * decay amplitude H * D*: ``tf_pwa/amp/core.py:1149-1164``
 * lineshapes BWR / BW with running width Gamma(m): ``tf_pwa/breit_wigner.py:56-91,231-245``,
+  BWR2 with Gamma2(m) from q^2: ``tf_pwa/breit_wigner.py:193-210,248-265``,
   particle model ``tf_pwa/amp/core.py:349-418``
 * chain contraction with totals and alignment D's: ``tf_pwa/amp/core.py:1392-1445,1563-1604``
 * sum over chains and |A|^2: ``tf_pwa/amp/core.py:1696-1728,1919-1931``
@@ -185,6 +186,25 @@ def bwr(m, m0, g0, q, q0, L, d):
     return x / s + 1j * y / s
 
 
+def gamma2(m, g0, q2, q02, L, m0, d):
+    """Running width from q^2 and q0^2 (``tf_pwa/breit_wigner.py:248-265``):
+    (q^2/q0^2)^L sqrt(q^2/q0^2) on the principal complex branch, so the
+    width is imaginary where q^2/q0^2 < 0 (nominal mass below threshold)."""
+    r = q2 / q02
+    qq0 = (r ** L).astype(complex) * np.sqrt(r.astype(complex))
+    bp = bprime_poly(L, q02 * d * d) / bprime_poly(L, q2 * d * d)
+    return qq0 * (g0 * bp * m0 / m)
+
+
+def bwr2(m, m0, g0, q2, q02, L, d):
+    """BWR2 (``tf_pwa/breit_wigner.py:193-210``): with D = m0^2 - m^2 -
+    i m0 Gamma2(m), the value (Re D + i Im D) / |D|^2."""
+    g = gamma2(m, g0, q2, q02, L, m0, d)
+    dd = (m0 * m0 - m * m) - 1j * (m0 * g)
+    r2 = dd.real ** 2 + dd.imag ** 2
+    return dd.real / r2 + 1j * dd.imag / r2
+
+
 def bw(m, m0, g0):
     x = m0 * m0 - m * m
     y = m0 * g0
@@ -301,13 +321,14 @@ class OracleModel:
             d = chain.decay_of(p)
             b, c = d.outs
             m1d, m2d = self.data_mass(x, cf, b, chain), self.data_mass(x, cf, c, chain)
-            q = rel_p(m, m1d, m2d)
             m1n = self.mass_of(vals, b) if b in chain.inner else b.mass
             m2n = self.mass_of(vals, c) if c in chain.inner else c.mass
-            q0 = rel_p(m0, m1n, m2n)
             L = p.bw_l if p.bw_l is not None else min(d.get_l_list())
-            ret = bwr(m, m0, g0, q, q0, L, p.d)
-        if p.width_norm:
+            if kind == "BWR2":  # tf_pwa/amp/base.py:61-73
+                ret = bwr2(m, m0, g0, rel_p2(m, m1d, m2d), rel_p2(m0, m1n, m2n), L, p.d)
+            else:
+                ret = bwr(m, m0, g0, rel_p(m, m1d, m2d), rel_p(m0, m1n, m2n), L, p.d)
+        if p.width_norm_applies():  # core.py:415-417 (Particle class only)
             ret = g0 * ret
         return ret
 

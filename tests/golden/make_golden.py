@@ -41,6 +41,7 @@ CASES = {
     "lc2pkpi": ("lc2pkpi.yml", 400, 40, 1500, 13, False, {"bg_weight": 0.1}),
     "toy_vvp": ("toy_vvp.yml", 300, 30, 1200, 14, False, {"bg_weight": 0.1}),
     "b2dstkpi": ("b2dstkpi.yml", 300, 0, 1200, 15, False, {}),
+    "d2kpipi_shapes": ("d2kpipi_shapes.yml", 400, 0, 1500, 16, True, {}),
 }
 
 

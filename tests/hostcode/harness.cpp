@@ -71,18 +71,31 @@ extern "C" int hx_sums(const double* Cv, const double* XM, const double* XA, con
   return PWA_NACC;
 }
 
-// A[i * PWA_NOUT + o] as (re, im) pairs
+template <typename R>
+static void amp_t(const Consts& C, const R* XA, const double* XM, long long n, long long ld,
+                  double* out) {
+  for (long long i = 0; i < n; ++i) {
+    cpx<R> A[PWA_NOUT];
+    model_amp<R, false, false>(C, XA, XM, ld, i, A, nullptr);
+    for (int o = 0; o < PWA_NOUT; ++o) {
+      out[2 * (i * PWA_NOUT + o)] = double(A[o].re);
+      out[2 * (i * PWA_NOUT + o) + 1] = double(A[o].im);
+    }
+  }
+}
+
+// A[i * PWA_NOUT + o] as (re, im) pairs; f32 != 0: the FP32 form (angles
+// rounded to FP32, amplitude arithmetic in FP32)
 extern "C" int hx_amp(const double* Cv, const double* XM, const double* XA, long long n,
-                      long long ld, double* out) {
+                      long long ld, int f32, double* out) {
   Consts C;
   for (int j = 0; j < PWA_NCONST; ++j) C.v[j] = Cv[j];
-  for (long long i = 0; i < n; ++i) {
-    cpx<double> A[PWA_NOUT];
-    model_amp<double, false, false>(C, XA, XM, ld, i, A, nullptr);
-    for (int o = 0; o < PWA_NOUT; ++o) {
-      out[2 * (i * PWA_NOUT + o)] = A[o].re;
-      out[2 * (i * PWA_NOUT + o) + 1] = A[o].im;
-    }
+  if (f32) {
+    std::vector<float> xa((size_t)PWA_NANGLE_ROWS * ld);
+    for (size_t j = 0; j < xa.size(); ++j) xa[j] = (float)XA[j];
+    amp_t<float>(C, xa.data(), XM, n, ld, out);
+  } else {
+    amp_t<double>(C, XA, XM, n, ld, out);
   }
   return PWA_NOUT;
 }

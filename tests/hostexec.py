@@ -54,7 +54,7 @@ class HostModel:
         lib = ctypes.CDLL(so)
         ll, i, dp = ctypes.c_longlong, ctypes.c_int, ctypes.POINTER(ctypes.c_double)
         lib.hx_sums.argtypes = [dp, dp, dp, dp, ll, ll, ll, i, i, dp]
-        lib.hx_amp.argtypes = [dp, dp, dp, ll, ll, dp]
+        lib.hx_amp.argtypes = [dp, dp, dp, ll, ll, i, dp]
         lib.hx_columns.argtypes = [dp, dp, dp, ll, ll, dp]
         lib.hx_kin.argtypes = [dp, ll, dp]
         self.has_toy = hasattr(lib, "hx_toy")
@@ -83,16 +83,16 @@ class HostModel:
                          _dp(out))
         return out[:nacc], out[nacc:]
 
-    def amp(self, C, x):
+    def amp(self, C, x, f32=False):
         C = np.ascontiguousarray(C, np.float64)
         xm, xa = self._split(x)
         n = xm.shape[1]
         out = np.zeros(2 * n * self.code.nout)
-        self.lib.hx_amp(_dp(C), _dp(xm), _dp(xa), n, n, _dp(out))
+        self.lib.hx_amp(_dp(C), _dp(xm), _dp(xa), n, n, int(f32), _dp(out))
         return (out[0::2] + 1j * out[1::2]).reshape(n, self.code.nout)
 
-    def pdf(self, C, x):
-        return np.sum(np.abs(self.amp(C, x)) ** 2, axis=1)
+    def pdf(self, C, x, f32=False):
+        return np.sum(np.abs(self.amp(C, x, f32)) ** 2, axis=1)
 
     def columns(self, C, x):
         C = np.ascontiguousarray(C, np.float64)

@@ -27,7 +27,7 @@ def _fcn(name, precision="plain"):
     return cl, fcn, g, meta
 
 
-@pytest.mark.parametrize("name", ["d2kpipi", "d2kpipi_float"])
+@pytest.mark.parametrize("name", ["d2kpipi", "d2kpipi_float", "d2kpipi_shapes"])
 def test_hessian_matches_reference(name):
     cl, fcn, g, meta = _fcn(name)
     nll, grad, H = fcn.nll_grad_hessian()

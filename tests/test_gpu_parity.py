@@ -13,7 +13,7 @@ from common import golden_data, load_golden, load_model
 
 pytestmark = pytest.mark.gpu
 
-CASES = ["d2kpipi", "d2kpipi_float", "lc2pkpi", "b2dstkpi"]
+CASES = ["d2kpipi", "d2kpipi_float", "lc2pkpi", "b2dstkpi", "d2kpipi_shapes"]
 
 
 def _engine(name):

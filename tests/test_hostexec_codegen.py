@@ -5,7 +5,8 @@ event by event on the golden events, against the reference's numbers.
 This checks the code generator's arithmetic without a GPU, at the
 tolerances the GPU parity tests use:
 
-* sum |A|^2 per event from ``model_amp`` vs the reference's |A|^2 (1e-10);
+* sum |A|^2 per event from ``model_amp`` vs the reference's |A|^2 (1e-10;
+  2e-4 in the FP32 form);
 * the plain kernel's per-event loop (forward, clip_log / MC weight,
   adjoint with and without the half-angle stash) summed on the host and fed
   to the engine's host-side chain rule: NLL within 1e-9 relative and
@@ -25,7 +26,7 @@ import pytest
 from common import golden_data, load_golden, load_model
 from hostexec import HostModel
 
-CASES = ["d2kpipi", "d2kpipi_float", "lc2pkpi", "toy_vvp", "b2dstkpi"]
+CASES = ["d2kpipi", "d2kpipi_float", "lc2pkpi", "toy_vvp", "b2dstkpi", "d2kpipi_shapes"]
 
 _CACHE = {}
 
@@ -55,6 +56,8 @@ def test_pdf_matches_reference(name, build_dir):
     C = eng.consts(meta["variables"])
     for kind in ("data", "mc"):
         np.testing.assert_allclose(hm.pdf(C, g["fields_" + kind]), g["f_" + kind], rtol=1e-10)
+        np.testing.assert_allclose(hm.pdf(C, g["fields_" + kind], f32=True), g["f_" + kind],
+                                   rtol=2e-4)
 
 
 @pytest.mark.parametrize("stash", [False, True])
@@ -125,3 +128,32 @@ def test_generator_matches_oracle(name, build_dir):
     np.testing.assert_allclose(t["fields"], x_ref, rtol=0, atol=1e-11)
     f_ref = OracleModel(dc.decay_group, plan).pdf(x_ref, meta["variables"])
     np.testing.assert_allclose(t["f"], f_ref, rtol=1e-10)
+
+
+@pytest.mark.parametrize("name", ["d2kpipi", "d2kpipi_float", "d2kpipi_shapes"])
+def test_hessian_from_kernel_loop(name, build_dir):
+    """Differenced adjoint gradients of the host-run kernel loop against the
+    reference's nested-tape Hessian (same tolerance as the GPU test)."""
+    from tf_pwa_b200.api import hessian_from_gradient
+    from tf_pwa_b200.engine import PLAIN_F64
+
+    eng, hm, g, meta, _, _ = _setup(name, build_dir)
+    x, w = golden_data(g, meta)
+    xm = g["fields_mc"]
+    xall = np.concatenate([x, xm], 1)
+    wall = np.concatenate([w, np.ones(xm.shape[1]) / xm.shape[1]])
+    eng._sw = float(w.sum())
+    eng.eval_sums = lambda C, precision=PLAIN_F64, mc=True, stream=None: hm.sums(
+        C, xall, wall, x.shape[1])
+    names = meta["trainable"]
+    base = dict(meta["variables"])
+
+    def nll_grad(p):
+        v = dict(base)
+        v.update(zip(names, p))
+        return eng.nll_grad(v, names, PLAIN_F64)
+
+    nll, grad, H = hessian_from_gradient(nll_grad, [base[k] for k in names], 1e-4)
+    assert abs(nll - g["hess_nll"]) <= 1e-9 * abs(g["hess_nll"])
+    Href = g["hess"]
+    np.testing.assert_allclose(H, Href, rtol=2e-5, atol=2e-5 * np.abs(Href).max())

@@ -7,7 +7,7 @@ import pytest
 from common import golden_data, load_golden, load_model
 from oracle.pwa_oracle import OracleModel, OracleNLL
 
-CASES = ["d2kpipi", "d2kpipi_float", "lc2pkpi", "toy_vvp", "b2dstkpi"]
+CASES = ["d2kpipi", "d2kpipi_float", "lc2pkpi", "toy_vvp", "b2dstkpi", "d2kpipi_shapes"]
 
 
 @pytest.mark.parametrize("name", CASES)

@@ -118,19 +118,23 @@ class ModelCode:
         self.res = []
         for p in group.resonances:
             kind = p.lineshape_kind()
-            if p.width_norm:
-                raise NotImplementedError("width_norm lineshapes")
             self.res.append((p, kind))
             if kind == "BWR":
                 self.consts.add(f"{p}.m0sq")
                 self.consts.add(f"{p}.K")
                 self.consts.add(f"{p}.useq")
+            elif kind == "BWR2":
+                self.consts.add(f"{p}.m0sq")
+                self.consts.add(f"{p}.K")
+                self.consts.add(f"{p}.iq02")
             elif kind == "BW":
                 self.consts.add(f"{p}.m0sq")
                 self.consts.add(f"{p}.y")
+            if p.width_norm_applies():
+                self.consts.add(f"{p}.wn")
         self.shape_res = []
         for p, kind in self.res:
-            if kind in ("BWR", "BW"):
+            if kind in ("BWR", "BW", "BWR2"):
                 self.shape_res.append(p)
                 self.consts.add(f"{p}.kappa_m")
                 self.consts.add(f"{p}.inv_g0")
@@ -364,23 +368,50 @@ class ModelCode:
             m = f"xm{cf['mass'][p]}"
             bw_names.append(f"bw_{tag}")
             e(f"  const R xr_{tag} = R(C.v[{self.consts.index[f'{p}.m0sq']}] - {m} * {m});")
-            if kind == "BWR":
+            if kind == "BWR2":
+                # m0 Gamma2(m) = K (r^L sqrt|r|) / (m B(q^2)), r = q^2 / q0^2,
+                # real for r >= 0 and imaginary for r < 0 (principal sqrt);
+                # value (Re D + i Im D) / |D|^2 of D = m0^2 - m^2 - i m0 Gamma2
                 dp = c.decay_of(p)
                 b, cc = dp.outs
                 L_ = p.bw_l if p.bw_l is not None else min(dp.get_l_list())
-                e(f"  const R q_{tag} = R(rel_p<double>({m}, {dmass(b)}, {dmass(cc)}));")
+                e(f"  const R qq_{tag} = R(rel_p2<double>({m}, {dmass(b)}, {dmass(cc)}));")
                 co = bprime_coeff(L_)
-                z = f"(q_{tag} * q_{tag} * {_lit(p.d * p.d)})"
+                z = f"(qq_{tag} * {_lit(p.d * p.d)})"
                 poly = _lit(co[0])
                 for cc_ in co[1:]:
                     poly = f"fma({poly}, {z}, {_lit(cc_)})"
-                qp = "*".join([f"q_{tag}"] * (2 * L_ + 1))
-                e(f"  const R qp_{tag} = {cst(f'{p}.useq')} != R(0) ? ({qp}) : R(1);")
-                e(f"  const R y_{tag} = {cst(f'{p}.K')} * qp_{tag} / (R({m}) * ({poly}));")
+                e(f"  const R rr_{tag} = qq_{tag} * {cst(f'{p}.iq02')};")
+                ph = f"psqrt(rr_{tag} < R(0) ? -rr_{tag} : rr_{tag})"
+                for _ in range(L_):
+                    ph = f"{ph} * rr_{tag}"
+                e(f"  const R ya_{tag} = {cst(f'{p}.K')} * ({ph}) / (R({m}) * ({poly}));")
+                e(f"  const R y_{tag} = rr_{tag} < R(0) ? R(0) : ya_{tag};")
+                e(f"  const R yi_{tag} = rr_{tag} < R(0) ? ya_{tag} : R(0);")
+                e(f"  const R dre_{tag} = xr_{tag} + yi_{tag};")
+                e(f"  const R s_{tag} = dre_{tag} * dre_{tag} + y_{tag} * y_{tag};")
+                e(f"  const cpx<R> bw_{tag} = cmk<R>(dre_{tag} / s_{tag}, -y_{tag} / s_{tag});")
             else:
-                e(f"  const R y_{tag} = {cst(f'{p}.y')};")
-            e(f"  const R s_{tag} = xr_{tag} * xr_{tag} + y_{tag} * y_{tag};")
-            e(f"  const cpx<R> bw_{tag} = cmk<R>(xr_{tag} / s_{tag}, y_{tag} / s_{tag});")
+                if kind == "BWR":
+                    dp = c.decay_of(p)
+                    b, cc = dp.outs
+                    L_ = p.bw_l if p.bw_l is not None else min(dp.get_l_list())
+                    e(f"  const R q_{tag} = R(rel_p<double>({m}, {dmass(b)}, {dmass(cc)}));")
+                    co = bprime_coeff(L_)
+                    z = f"(q_{tag} * q_{tag} * {_lit(p.d * p.d)})"
+                    poly = _lit(co[0])
+                    for cc_ in co[1:]:
+                        poly = f"fma({poly}, {z}, {_lit(cc_)})"
+                    qp = "*".join([f"q_{tag}"] * (2 * L_ + 1))
+                    e(f"  const R qp_{tag} = {cst(f'{p}.useq')} != R(0) ? ({qp}) : R(1);")
+                    e(f"  const R y_{tag} = {cst(f'{p}.K')} * qp_{tag} / (R({m}) * ({poly}));")
+                else:
+                    e(f"  const R y_{tag} = {cst(f'{p}.y')};")
+                e(f"  const R s_{tag} = xr_{tag} * xr_{tag} + y_{tag} * y_{tag};")
+                e(f"  const cpx<R> bw_{tag} = cmk<R>(xr_{tag} / s_{tag}, y_{tag} / s_{tag});")
+            if p.width_norm_applies():
+                # the chain product takes Gamma0 R (the derivatives use R)
+                bw_names[-1] = f"cscale(bw_{tag}, {cst(f'{p}.wn')})"
         if bw_names:
             e(f"  cpx<R> BW_c{ci} = {bw_names[0]};")
             for nm in bw_names[1:]:
@@ -515,10 +546,21 @@ class ModelCode:
                 e("  }")
             for si, p in enumerate(self.shape_res):
                 if p in c.inner and self._first_chain(p) == ci:
+                    # log-derivatives of the lineshape R with respect to m0
+                    # and Gamma0 (kappa_m = dlog(m0 Gamma) / dm0 at fixed m)
                     tag = f"c{ci}r{c.inner.index(p)}"
+                    kap, ig = self._cst(f"{p}.kappa_m"), self._cst(f"{p}.inv_g0")
                     e(f"  {{ const R m0 = psqrt({self._cst(f'{p}.m0sq')});")
-                    e(f"    dm{si} = cmul(bw_{tag}, cmk<R>(R(-2) * m0, y_{tag} * {self._cst(f'{p}.kappa_m')}));")
-                    e(f"    dg{si} = cmul(bw_{tag}, cmk<R>(R(0), y_{tag} * {self._cst(f'{p}.inv_g0')})); }}")
+                    if p.lineshape_kind() == "BWR2":
+                        # R = 1 / conj(D): dlog R = -R conj(dD)
+                        e(f"    dm{si} = cmul(bw_{tag}, cmk<R>(-(R(2) * m0 + yi_{tag} * {kap}), -y_{tag} * {kap}));")
+                        e(f"    dg{si} = cmul(bw_{tag}, cmk<R>(-yi_{tag} * {ig}, -y_{tag} * {ig}));")
+                    else:
+                        e(f"    dm{si} = cmul(bw_{tag}, cmk<R>(R(-2) * m0, y_{tag} * {kap}));")
+                        e(f"    dg{si} = cmul(bw_{tag}, cmk<R>(R(0), y_{tag} * {ig}));")
+                    if p.width_norm_applies():
+                        e(f"    dg{si}.re += {ig};")
+                    e("  }")
             e("  }")
         for si, p in enumerate(self.shape_res):
             e(f"  accs[{2 * si}] += 2.0 * double(cmul(SR{si}, dm{si}).re);")

@@ -321,7 +321,8 @@ class Engine:
             if kind == "one":
                 continue
             self._res_slots.append((p, kind, cidx[f"{p}.m0sq"],
-                                    cidx.get(f"{p}.K"), cidx.get(f"{p}.useq"), cidx.get(f"{p}.y")))
+                                    cidx.get(f"{p}.K"), cidx.get(f"{p}.useq"), cidx.get(f"{p}.y"),
+                                    cidx.get(f"{p}.iq02"), cidx.get(f"{p}.wn")))
         self._vtx_slots = []
         for d in self.code.vertices:
             sl = {}
@@ -377,6 +378,17 @@ class Engine:
             return m0 * m0 * g0 * pz0 / q0 ** (2 * L + 1), 1.0
         return m0 * m0 * g0 * pz0, 0.0
 
+    def _lineshape_K2(self, p, vals, m0=None):
+        """(m0^2 Gamma0 B_L(q0^2 d^2), q0^2) of a BWR2 lineshape, q0^2 from
+        the nominal masses without clamping (``tf_pwa/amp/core.py:826-843``)."""
+        dp, chain = self.res_info[p]
+        m0 = self._nominal(p, vals, chain) if m0 is None else m0
+        g0 = vals.get(f"{p.params_head}_width", p.width)
+        b, c = dp.outs
+        L = p.bw_l if p.bw_l is not None else min(dp.get_l_list())
+        q02 = rel_p2(m0, self._nominal(b, vals, chain), self._nominal(c, vals, chain))
+        return m0 * m0 * g0 * poly(L, q02 * p.d * p.d), q02
+
     def _shape_key(self, vals):
         return tuple(vals.get(k) for k in self._shape_names)
 
@@ -420,16 +432,23 @@ class Engine:
         C[1:2 * c.ncol:2] = self._ck.imag
         C[self._vg_re] = self._cvec[self._vg_src].real
         C[self._vg_im] = self._cvec[self._vg_src].imag
-        for p, kind, s_m0sq, s_k, s_useq, s_y in self._res_slots:
+        for p, kind, s_m0sq, s_k, s_useq, s_y, s_iq, s_wn in self._res_slots:
             dp, chain = self.res_info[p]
             m0 = self._nominal(p, vals, chain)
+            g0 = vals.get(f"{p.params_head}_width", p.width)
             C[s_m0sq] = m0 * m0
             if kind == "BWR":
                 K, useq = self._lineshape_K(p, vals)
                 C[s_k] = K
                 C[s_useq] = useq
+            elif kind == "BWR2":
+                K, q02 = self._lineshape_K2(p, vals)
+                C[s_k] = K
+                C[s_iq] = 1.0 / q02
             else:
-                C[s_y] = m0 * vals.get(f"{p.params_head}_width", p.width)
+                C[s_y] = m0 * g0
+            if s_wn is not None:
+                C[s_wn] = g0
         for d, chain, sl in self._vtx_slots:
             vc = self._vertex_consts(d, chain, vals)
             for l, (pz0, norm) in vc.items():
@@ -443,9 +462,17 @@ class Engine:
             m0 = self._nominal(p, vals, chain)
             g0 = vals.get(f"{p.params_head}_width", p.width)
             h = 1e-20
-            Kc, _ = self._lineshape_K(p, vals, m0=m0 + 1j * h)
-            K0, _ = self._lineshape_K(p, vals, m0=m0)
-            C[s_kap] = np.imag(Kc) / h / np.real(K0) if np.real(K0) != 0 else 0.0
+            if p.lineshape_kind() == "BWR2":
+                # m0 Gamma2 = K r^(L+1/2) / (m B): dlog/dm0 = dlog K - (L + 1/2) dlog q0^2
+                Kc, qc = self._lineshape_K2(p, vals, m0=m0 + 1j * h)
+                K0, q0 = self._lineshape_K2(p, vals, m0=m0)
+                L = p.bw_l if p.bw_l is not None else min(dp.get_l_list())
+                C[s_kap] = (np.imag(Kc) / h / np.real(K0) if np.real(K0) != 0 else 0.0) \
+                    - (L + 0.5) * np.imag(qc) / h / np.real(q0)
+            else:
+                Kc, _ = self._lineshape_K(p, vals, m0=m0 + 1j * h)
+                K0, _ = self._lineshape_K(p, vals, m0=m0)
+                C[s_kap] = np.imag(Kc) / h / np.real(K0) if np.real(K0) != 0 else 0.0
             C[s_ig] = 1.0 / g0 if g0 else 0.0
         return C
 

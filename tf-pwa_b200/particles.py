@@ -252,14 +252,25 @@ class Particle:
         return str(self)
 
     def lineshape_kind(self):
-        """'one' (no width), 'BW' (fixed width) or 'BWR' (running width)."""
+        """'one' (no width), 'BW' (fixed width), 'BWR' (running width from
+        |q|, |q0|: ``tf_pwa/amp/core.py:399-418``) or 'BWR2' (running width
+        from q^2, q0^2, complex below threshold: ``tf_pwa/amp/base.py:37-73``)."""
         if self.width is None or self.model == "one":
             return "one"
         if self.model in ("BW",) or not self.running_width:
             return "BW"
         if self.model in ("default", "BWR", None):
             return "BWR"
+        if self.model == "BWR2":
+            return "BWR2"
         raise NotImplementedError(f"lineshape model {self.model!r} of {self}")
+
+    def width_norm_applies(self):
+        """R -> Gamma0 R: the ``width_norm`` option of the default particle
+        class (``tf_pwa/amp/core.py:415-417``); the BW and BWR2 classes
+        ignore it."""
+        return bool(self.width_norm) and self.width is not None and \
+            self.model in ("default", "BWR", None)
 
 
 class Decay:
