@@ -22,7 +22,8 @@ per-event inputs (invariant masses and helicity / alignment angles):
   BWR2 with Gamma2(m) from q^2: ``tf_pwa/breit_wigner.py:193-210,248-265``,
   particle model ``tf_pwa/amp/core.py:349-418``
 * chain contraction with totals and alignment D's: ``tf_pwa/amp/core.py:1392-1445,1563-1604``
-* sum over chains and |A|^2: ``tf_pwa/amp/core.py:1696-1728,1919-1931``
+* sum over chains and |A|^2: ``tf_pwa/amp/core.py:1696-1728,1919-1931``;
+  identical-particle swaps ``tf_pwa/amp/core.py:1826-1882``
 * clip_log and the weighted NLL with alpha scaling and normalised MC
   weights: ``tf_pwa/model/model.py:283-292,407-449,603-641,1126-1229``
 
@@ -332,9 +333,9 @@ class OracleModel:
             ret = g0 * ret
         return ret
 
-    def chain_amp(self, x, ci, vals, coup):
+    def chain_amp(self, x, ci, vals, coup, cf=None):
         chain = self.group[ci]
-        cf = self.plan.chains[ci]
+        cf = self.plan.chains[ci] if cf is None else cf
         tot, gl = coup[ci]
         L = self.letters
         ops, idx = [], []
@@ -358,9 +359,17 @@ class OracleModel:
         return np.einsum(",".join(idx) + "->" + final, *ops)
 
     def amp(self, x, vals, polar=None):
+        """Sum over chains (``core.py:1696-1728``); with identical particles
+        plus, per swap, the sign times the amplitude of the swapped fields
+        with its final-helicity axes reordered (``core.py:1871-1882``)."""
         polar = polar or {}
         coup = self.couplings(vals, polar)
-        return sum(self.chain_amp(x, ci, vals, coup) for ci in range(len(self.group)))
+        a = sum(self.chain_amp(x, ci, vals, coup) for ci in range(len(self.group)))
+        for sw in self.plan.swaps:
+            b = sum(self.chain_amp(x, ci, vals, coup, sw["chains"][ci])
+                    for ci in range(len(self.group)))
+            a = a + sw["factor"] * np.transpose(b, [0, 1] + [2 + t for t in sw["trans"]])
+        return a
 
     def pdf(self, x, vals, polar=None):
         a = self.amp(x, vals, polar)

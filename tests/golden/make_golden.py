@@ -42,6 +42,8 @@ CASES = {
     "toy_vvp": ("toy_vvp.yml", 300, 30, 1200, 14, False, {"bg_weight": 0.1}),
     "b2dstkpi": ("b2dstkpi.yml", 300, 0, 1200, 15, False, {}),
     "d2kpipi_shapes": ("d2kpipi_shapes.yml", 400, 0, 1500, 16, True, {}),
+    "dp2kpipi_ident": ("dp2kpipi_ident.yml", 400, 0, 1500, 17, True, {}),
+    "ident_fermions": ("ident_fermions.yml", 300, 0, 1200, 18, False, {}),
 }
 
 
@@ -62,7 +64,7 @@ def main(ref_root):
     load_pkg()
     from tf_pwa_b200.decay_config import DecayConfig, float_particles, init_params, load_yaml
     from tf_pwa_b200.phasespace import generate_phsp
-    from tf_pwa_b200.plan import Plan
+    from tf_pwa_b200.plan import Plan, split_swap
     from tf_pwa_b200.variables import VarsManager
     from tf_pwa.config_loader import ConfigLoader
 
@@ -74,7 +76,7 @@ def main(ref_root):
         dic = load_yaml(os.path.join(cfg_dir, cfg_file))
         dc = DecayConfig(dic)
         group = dc.decay_group
-        plan = Plan(group)
+        plan = Plan(group, dic["data"].get("dat_order"))
         order = dic["data"].get("dat_order")
         top = group.top
         masses = [dc.particle_property[o]["mass"] for o in order]
@@ -118,19 +120,24 @@ def main(ref_root):
         for kind, lst in datas.items():
             d = lst[0]
             cols = np.zeros((plan.n_fields, len(d["weight"])))
-            topo_keys = list(d["decay"].keys())
-            for fi, fname in enumerate(plan.fields):
+            # identical-particle swaps: the reference's id_swap data sets, in
+            # its permutation order
+            swap_sets = [d] + list(d.get("id_swap", {}).values())
+            for fi, full_name in enumerate(plan.fields):
+                sk, fname = split_swap(full_name)
+                ds = swap_sets[sk]
+                topo_keys = list(ds["decay"].keys())
                 parts = fname.split("/")
                 if parts[0] == "m":
-                    node = [k for k in d["particle"] if str(k) == parts[1]][0]
-                    cols[fi] = np.asarray(d["particle"][node]["m"])
+                    node = [k for k in ds["particle"] if str(k) == parts[1]][0]
+                    cols[fi] = np.asarray(ds["particle"][node]["m"])
                     continue
                 tidx = int(parts[0])
                 my_topo = plan.topos[tidx]
                 tstr = "[" + ", ".join(my_topo.decay_name(dd) for dd in my_topo.chain) + "]"
                 tkey = [k for k in topo_keys if str(k) == tstr]
                 assert tkey, (tstr, [str(k) for k in topo_keys])
-                dd = d["decay"][tkey[0]]
+                dd = ds["decay"][tkey[0]]
                 dkey = [k for k in dd if str(k) == parts[1]][0]
                 pkey = [k for k in dd[dkey] if str(k) == parts[2]][0]
                 if parts[3] == "aligned":

@@ -26,7 +26,8 @@ import pytest
 from common import golden_data, load_golden, load_model
 from hostexec import HostModel
 
-CASES = ["d2kpipi", "d2kpipi_float", "lc2pkpi", "toy_vvp", "b2dstkpi", "d2kpipi_shapes"]
+CASES = ["d2kpipi", "d2kpipi_float", "lc2pkpi", "toy_vvp", "b2dstkpi", "d2kpipi_shapes",
+         "dp2kpipi_ident", "ident_fermions"]
 
 _CACHE = {}
 
@@ -97,7 +98,8 @@ def test_columns_rebuild_amplitude(name, build_dir):
     np.testing.assert_allclose(A2, A, rtol=1e-12, atol=1e-12 * np.abs(A).max())
 
 
-@pytest.mark.parametrize("name", ["d2kpipi", "lc2pkpi", "toy_vvp", "b2dstkpi"])
+@pytest.mark.parametrize("name", ["d2kpipi", "lc2pkpi", "toy_vvp", "b2dstkpi", "dp2kpipi_ident",
+                                  "ident_fermions"])
 def test_kinematics_match_reference(name, build_dir):
     eng, hm, g, meta, _, _ = _setup(name, build_dir)
     for kind in ("data", "mc"):
@@ -105,7 +107,7 @@ def test_kinematics_match_reference(name, build_dir):
                                    atol=1e-11)
 
 
-@pytest.mark.parametrize("name", ["lc2pkpi", "b2dstkpi"])
+@pytest.mark.parametrize("name", ["lc2pkpi", "b2dstkpi", "ident_fermions"])
 def test_generator_matches_oracle(name, build_dir):
     from oracle.pwa_oracle import OracleModel
     from oracle.toy_oracle import genbod_levels, uniforms
@@ -130,7 +132,7 @@ def test_generator_matches_oracle(name, build_dir):
     np.testing.assert_allclose(t["f"], f_ref, rtol=1e-10)
 
 
-@pytest.mark.parametrize("name", ["d2kpipi", "d2kpipi_float", "d2kpipi_shapes"])
+@pytest.mark.parametrize("name", ["d2kpipi", "d2kpipi_float", "d2kpipi_shapes", "dp2kpipi_ident"])
 def test_hessian_from_kernel_loop(name, build_dir):
     """Differenced adjoint gradients of the host-run kernel loop against the
     reference's nested-tape Hessian (same tolerance as the GPU test)."""

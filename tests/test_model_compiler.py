@@ -5,7 +5,8 @@ import pytest
 
 from common import load_golden, load_model
 
-CASES = ["d2kpipi", "d2kpipi_float", "lc2pkpi", "toy_vvp", "b2dstkpi"]
+CASES = ["d2kpipi", "d2kpipi_float", "lc2pkpi", "toy_vvp", "b2dstkpi", "d2kpipi_shapes",
+         "dp2kpipi_ident", "ident_fermions"]
 
 
 @pytest.mark.parametrize("name", CASES)

@@ -27,6 +27,7 @@ mathematics is the reference's chain contraction
 import itertools
 
 from .kincode import KinCode
+from .plan import split_swap
 from .particles import bprime_coeff, small_d_weight, two
 
 _HEADER = """
@@ -87,8 +88,14 @@ class ModelCode:
         self.out_hel = list(itertools.product(*[p.spins for p in self.outs]))
         self.out_index = {o: j for j, o in enumerate(self.out_hel)}
         self.nout = len(self.out_hel)
-        self.mass_fields = [i for i, f in enumerate(plan.fields) if f.startswith("m/")]
-        self.angle_fields = [i for i, f in enumerate(plan.fields) if not f.startswith("m/")]
+        self.mass_fields = [i for i, f in enumerate(plan.fields)
+                            if split_swap(f)[1].startswith("m/")]
+        self.angle_fields = [i for i, f in enumerate(plan.fields)
+                             if not split_swap(f)[1].startswith("m/")]
+        # evaluation passes: the unswapped fields, then one per identical-
+        # particle swap (its fields, sign and helicity-axis order)
+        self.npass = 1 + len(plan.swaps)
+        self._pass = 0
         self.mass_slot = {f: k for k, f in enumerate(self.mass_fields)}
         self.angle_slot = {f: k for k, f in enumerate(self.angle_fields)}
         # constants: column couplings c_k, vertex couplings, chain totals
@@ -181,33 +188,39 @@ class ModelCode:
             self.chain_assign.append(rows)
         # structurally non-zero (column, output) pairs after alignment
         self._fset = set()
-        for ci in range(len(self.group)):
-            aligned = self._aligned_finals(ci)
-            for facs, pre, coefs in self.chain_assign[ci]:
-                outs = [pre]
-                for oi in aligned:
-                    new = []
-                    for o in outs:
-                        for l2 in self.outs[oi].spins:
-                            t = list(o)
-                            t[oi] = l2
-                            new.append(tuple(t))
-                    outs = new
-                for k in coefs:
-                    for o in outs:
-                        self._fset.add((k, self.out_index[o]))
+        for ps in range(self.npass):
+            self._pass = ps
+            for ci in range(len(self.group)):
+                aligned = self._aligned_finals(ci)
+                for facs, pre, coefs in self.chain_assign[ci]:
+                    outs = [pre]
+                    for oi in aligned:
+                        new = []
+                        for o in outs:
+                            for l2 in self.outs[oi].spins:
+                                t = list(o)
+                                t[oi] = l2
+                                new.append(tuple(t))
+                        outs = new
+                    for k in coefs:
+                        for o in outs:
+                            self._fset.add((k, self._out(o)))
+        self._pass = 0
         self.nf = len(self._fset)
-        # stash slots: one (sin, cos) pair per half angle of every chain
+        # stash slots: one (sin, cos) pair per half angle of every chain and pass
         self._slot = {}
-        for ci, c in enumerate(self.group):
-            cf = self.plan.chains[ci]
-            for vi, d in enumerate(c):
-                self._slot[(ci, f"c{ci}v{vi}b")] = len(self._slot)
-                self._slot[(ci, f"c{ci}v{vi}a")] = len(self._slot)
-            for o in cf["aligned"]:
-                oi = self.group.outs.index(o)
-                for a in "bag":
-                    self._slot[(ci, f"c{ci}al{oi}{a}")] = len(self._slot)
+        for ps in range(self.npass):
+            self._pass = ps
+            for ci, c in enumerate(self.group):
+                cf = self._cf(ci)
+                for vi, d in enumerate(c):
+                    self._slot[(ps, ci, f"c{ci}v{vi}b")] = len(self._slot)
+                    self._slot[(ps, ci, f"c{ci}v{vi}a")] = len(self._slot)
+                for o in cf["aligned"]:
+                    oi = self.group.outs.index(o)
+                    for a in "bag":
+                        self._slot[(ps, ci, f"c{ci}al{oi}{a}")] = len(self._slot)
+        self._pass = 0
         self.nstash = 2 * len(self._slot)
         self._mode = "plain"
 
@@ -218,8 +231,26 @@ class ModelCode:
     def _cpx(self, base):
         return f"cmk<R>({self._cst(base + '.re')}, {self._cst(base + '.im')})"
 
+    def _cf(self, ci):
+        """Field references of chain ci in the current pass."""
+        if self._pass == 0:
+            return self.plan.chains[ci]
+        return self.plan.swaps[self._pass - 1]["chains"][ci]
+
+    def _out(self, o):
+        """Output index of the chain helicity tuple o = (top, finals...) in
+        the current pass: a swap's amplitude enters with its final-helicity
+        axes reordered (out-axis j = its axis trans[j])."""
+        if self._pass == 0:
+            return self.out_index[o]
+        tr = self.plan.swaps[self._pass - 1]["trans"]
+        return self.out_index[(o[0],) + tuple(o[1 + t] for t in tr)]
+
+    def _factor(self):
+        return 1.0 if self._pass == 0 else self.plan.swaps[self._pass - 1]["factor"]
+
     def _aligned_finals(self, ci):
-        cf = self.plan.chains[ci]
+        cf = self._cf(ci)
         return [self.group.outs.index(o) + 1 for o in self.group.outs if o in cf["aligned"]]
 
     @staticmethod
@@ -259,7 +290,7 @@ class ModelCode:
         """sin/cos of half an angle: computed (and stashed in the forward
         pass) or read back from the stash (adjoint pass)."""
         nm = f"{key}"
-        slot = self._slot[(ci, key)]
+        slot = self._slot[(self._pass, ci, key)]
         if self._mode == "load":
             e(f"  const R s_{nm} = st[{2 * slot} * PWA_TPB], c_{nm} = st[{2 * slot + 1} * PWA_TPB];")
         else:
@@ -273,7 +304,7 @@ class ModelCode:
         """Masses, q^2, barrier factors, D elements, alignment D and
         lineshapes of chain ci (names prefixed by the chain)."""
         c = self.group[ci]
-        cf = self.plan.chains[ci]
+        cf = self._cf(ci)
         cst = self._cst
 
         def dmass(p):
@@ -449,8 +480,14 @@ class ModelCode:
     def _emit_forward(self, e):
         for oj in range(self.nout):
             e(f"  cpx<R> A{oj} = cmk<R>(R(0), R(0));")
+        for ps in range(self.npass):
+            self._pass = ps
+            self._emit_forward_pass(e)
+        self._pass = 0
+
+    def _emit_forward_pass(self, e):
         for ci, c in enumerate(self.group):
-            e(f"  {{ // chain {ci}: {c}")
+            e(f"  {{ // chain {ci}: {c}" + (f" (swap {self._pass})" if self._pass else ""))
             self._emit_chain_common(e, ci)
             hnames = {}
             for vi, d in enumerate(c):
@@ -488,19 +525,42 @@ class ModelCode:
                         prod = f"cmul({prod}, {v})"
                     e(f"  cfmac({nm}, {prod}, {vs[-1]});")
             cur = self._emit_align_forward(e, ci, pre, "Aa")
-            e(f"  const cpx<R> E_c{ci} = cmul({self._cpx(f't{ci}')}, BW_c{ci});")
+            if self._factor() == 1.0:
+                e(f"  const cpx<R> E_c{ci} = cmul({self._cpx(f't{ci}')}, BW_c{ci});")
+            else:
+                e(f"  const cpx<R> E_c{ci} = cscale(cmul({self._cpx(f't{ci}')}, BW_c{ci}), "
+                  f"{_lit(self._factor())});")
             for o, nm in cur.items():
-                e(f"  cfmac(A{self.out_index[o]}, E_c{ci}, {nm});")
+                e(f"  cfmac(A{self._out(o)}, E_c{ci}, {nm});")
             e("  }")
 
     # ------------------------------------------------------------ adjoint
     def _emit_adjoint(self, e):
         for si, p in enumerate(self.shape_res):
             e(f"  cpx<R> SR{si} = cmk<R>(R(0), R(0)), dm{si} = SR{si}, dg{si} = SR{si};")
+        for ps in range(self.npass):
+            self._pass = ps
+            if ps:
+                for si in range(len(self.shape_res)):
+                    e(f"  SR{si} = cmk<R>(R(0), R(0));")
+            self._emit_adjoint_pass(e)
+            # lineshape sensitivities of this pass (its own masses)
+            for si, p in enumerate(self.shape_res):
+                e(f"  accs[{2 * si}] += 2.0 * double(cmul(SR{si}, dm{si}).re);")
+                e(f"  accs[{2 * si + 1}] += 2.0 * double(cmul(SR{si}, dg{si}).re);")
+        self._pass = 0
+
+    def _emit_adjoint_pass(self, e):
+        fac = self._factor()
         for ci, c in enumerate(self.group):
-            e(f"  {{ // chain {ci}: {c}")
+            e(f"  {{ // chain {ci}: {c}" + (f" (swap {self._pass})" if self._pass else ""))
             self._emit_chain_common(e, ci)
-            cur = {o: f"Ab[{j}]" for o, j in self.out_index.items()}
+            # seed of each chain helicity tuple: the adjoint of the output it
+            # enters (times the swap sign)
+            if fac == 1.0:
+                cur = {o: f"Ab[{self._out(o)}]" for o in self.out_index}
+            else:
+                cur = {o: f"cscale(Ab[{self._out(o)}], {_lit(fac)})" for o in self.out_index}
             for oi in reversed(self._aligned_finals(ci)):
                 o = self.outs[oi]
                 j2 = two(o.J)
@@ -562,16 +622,20 @@ class ModelCode:
                         e(f"    dg{si}.re += {ig};")
                     e("  }")
             e("  }")
-        for si, p in enumerate(self.shape_res):
-            e(f"  accs[{2 * si}] += 2.0 * double(cmul(SR{si}, dm{si}).re);")
-            e(f"  accs[{2 * si + 1}] += 2.0 * double(cmul(SR{si}, dg{si}).re);")
 
     # ------------------------------------------------------------ columns
     def _emit_columns(self, e):
         for j in range(self.ncol * self.nout):
             e(f"  F[{j}] = cmk<R>(R(0), R(0));")
+        for ps in range(self.npass):
+            self._pass = ps
+            self._emit_columns_pass(e)
+        self._pass = 0
+
+    def _emit_columns_pass(self, e):
+        fac = self._factor()
         for ci, c in enumerate(self.group):
-            e(f"  {{ // chain {ci}: {c}")
+            e(f"  {{ // chain {ci}: {c}" + (f" (swap {self._pass})" if self._pass else ""))
             self._emit_chain_common(e, ci)
             for k in self.chain_columns[ci]:
                 e("  {")
@@ -592,7 +656,11 @@ class ModelCode:
                 cur = self._emit_align_forward(e, ci, pre, "Fa")
                 e(f"  const cpx<R> S = cscale(BW_c{ci}, {self._scale_k(ci, k)});")
                 for o, nm in cur.items():
-                    e(f"  F[{k * self.nout + self.out_index[o]}] = cmul(S, {nm});")
+                    j = k * self.nout + self._out(o)
+                    if self._pass == 0:
+                        e(f"  F[{j}] = cmul(S, {nm});")
+                    else:
+                        e(f"  F[{j}] = cadd(F[{j}], cscale(cmul(S, {nm}), {_lit(fac)}));")
                 e("  }")
             e("  }")
 

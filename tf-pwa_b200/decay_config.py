@@ -254,7 +254,15 @@ class DecayConfig:
             raise RuntimeError("no decay chain available, check the config")
         if self.data_config.get("cp_trans", True):
             pass  # charge-conjugation flips are disabled (decay_config.py:423-427)
-        return DecayGroup(chains)
+        group = DecayGroup(chains)
+        # data.identical_particles: lists of final particles whose momenta are
+        # symmetrised (tf_pwa/config_loader/decay_config.py:100-104)
+        ident = self.data_config.get("identical_particles")
+        if ident:
+            if self.data_config.get("cp_particles"):
+                raise NotImplementedError("cp_particles (CP-swap symmetrisation)")
+            group.identical_particles = [[str(x) for x in g] for g in ident]
+        return group
 
 
 def init_params(group, vm, constrains=None):

@@ -30,6 +30,7 @@ bounds) and the amplitude accept draw.
 """
 import math
 
+from .plan import split_swap
 
 
 def _f(v):
@@ -75,92 +76,103 @@ class KinCode:
             cnt[0] += 1
             return f"{prefix}{cnt[0]}"
 
-        frames = []
-        for t, topo in enumerate(plan.topos):
-            chain = topo.chain
-            mom = {}
-            for o in chain.outs:
-                mom[o] = f"P[{fin[str(o)]}]"
+        def build_frames(pexpr):
+            """Frames of every topology from the finals' momenta pexpr."""
+            frames = []
+            for t, topo in enumerate(plan.topos):
+                chain = topo.chain
+                mom = {}
+                for o in chain.outs:
+                    mom[o] = pexpr[str(o)]
 
-            def lsum(parts):
-                expr = parts[0]
-                for p in parts[1:]:
-                    expr = f"lv_add({expr}, {p})"
-                return expr
+                def lsum(parts):
+                    expr = parts[0]
+                    for p in parts[1:]:
+                        expr = f"lv_add({expr}, {p})"
+                    return expr
 
-            for p in chain.inner:
-                v = tmp(f"t{t}_n")
-                e(f"  const LV {v} = {lsum([mom[f] for f in chain.final_set(p)])};")
-                mom[p] = v
-            v = tmp(f"t{t}_top")
-            e(f"  const LV {v} = {lsum([mom[f] for f in chain.outs])};")
-            mom[chain.top] = v
-            top = chain.top
-            # successive rest-frame momenta (same visiting order as the host code)
-            part, core_map = {}, {}
-            decays = list(chain)
-            remaining = set(chain.inner) | set(chain.outs)
-            while decays:
-                later = []
-                for d in decays:
-                    if d.core == top:
-                        pr, src = mom[top], mom
-                    elif d.core in core_map:
-                        par = part[core_map[d.core]]
-                        pr, src = par[d.core], par
-                    else:
-                        later.append(d)
-                        continue
-                    rp = {}
-                    for j in d.outs:
-                        core_map[j] = d
-                        v = tmp(f"t{t}_r")
-                        e(f"  const LV {v} = kin_rest_vector({pr}, {src[j]});")
-                        rp[j] = v
-                        remaining.discard(j)
-                    for j in sorted(remaining, key=str):
-                        if j in src:
+                for p in chain.inner:
+                    v = tmp(f"t{t}_n")
+                    e(f"  const LV {v} = {lsum([mom[f] for f in chain.final_set(p)])};")
+                    mom[p] = v
+                v = tmp(f"t{t}_top")
+                e(f"  const LV {v} = {lsum([mom[f] for f in chain.outs])};")
+                mom[chain.top] = v
+                top = chain.top
+                # successive rest-frame momenta (same visiting order as the host code)
+                part, core_map = {}, {}
+                decays = list(chain)
+                remaining = set(chain.inner) | set(chain.outs)
+                while decays:
+                    later = []
+                    for d in decays:
+                        if d.core == top:
+                            pr, src = mom[top], mom
+                        elif d.core in core_map:
+                            par = part[core_map[d.core]]
+                            pr, src = par[d.core], par
+                        else:
+                            later.append(d)
+                            continue
+                        rp = {}
+                        for j in d.outs:
+                            core_map[j] = d
                             v = tmp(f"t{t}_r")
                             e(f"  const LV {v} = kin_rest_vector({pr}, {src[j]});")
                             rp[j] = v
-                    part[d] = rp
-                decays = later
-            # helicity angles, frames, SU(2) bookkeeping
-            set_x = {top: "V3{1.0, 0.0, 0.0}"}
-            set_z = {top: "V3{0.0, 0.0, 1.0}"}
-            angles, rmat, bmat = {}, {}, {}
-            decays = list(chain)
-            while decays:
-                later = []
-                for d in decays:
-                    if d.core not in set_x:
-                        later.append(d)
-                        continue
-                    bias = -math.pi
-                    for j in d.outs:
-                        z2 = tmp(f"t{t}_z")
-                        a, b, x2 = tmp(f"t{t}_a"), tmp(f"t{t}_b"), tmp(f"t{t}_x")
-                        e(f"  const V3 {z2} = lv_vec({part[d][j]});")
-                        e(f"  double {a}, {b}; V3 {x2};")
-                        e(f"  kin_angle_zx_z_getx({set_z[d.core]}, {set_x[d.core]}, {z2}, "
-                          f"&{a}, &{b}, &{x2});")
-                        e(f"  {a} = kin_fold({a}, {_f(bias)});")
-                        bias -= math.pi
-                        set_x[j], set_z[j] = x2, z2
-                        angles[(d, j)] = (a, b)
-                        if self.needs_su2:
-                            bm, rm = tmp(f"t{t}_B"), tmp(f"t{t}_R")
-                            e(f"  const SU2 {bm} = su2_boost_z_from_p({part[d][j]});")
-                            if d.core in rmat:
-                                e(f"  const SU2 {rm} = su2_mul(su2_rot_yz({b}, {a}), "
-                                  f"su2_mul({bmat[d.core]}, {rmat[d.core]}));")
-                            else:
-                                e(f"  const SU2 {rm} = su2_rot_yz({b}, {a});")
-                            bmat[j], rmat[j] = bm, rm
-                decays = later
-            frames.append((topo, angles, rmat, bmat, mom))
+                            remaining.discard(j)
+                        for j in sorted(remaining, key=str):
+                            if j in src:
+                                v = tmp(f"t{t}_r")
+                                e(f"  const LV {v} = kin_rest_vector({pr}, {src[j]});")
+                                rp[j] = v
+                        part[d] = rp
+                    decays = later
+                # helicity angles, frames, SU(2) bookkeeping
+                set_x = {top: "V3{1.0, 0.0, 0.0}"}
+                set_z = {top: "V3{0.0, 0.0, 1.0}"}
+                angles, rmat, bmat = {}, {}, {}
+                decays = list(chain)
+                while decays:
+                    later = []
+                    for d in decays:
+                        if d.core not in set_x:
+                            later.append(d)
+                            continue
+                        bias = -math.pi
+                        for j in d.outs:
+                            z2 = tmp(f"t{t}_z")
+                            a, b, x2 = tmp(f"t{t}_a"), tmp(f"t{t}_b"), tmp(f"t{t}_x")
+                            e(f"  const V3 {z2} = lv_vec({part[d][j]});")
+                            e(f"  double {a}, {b}; V3 {x2};")
+                            e(f"  kin_angle_zx_z_getx({set_z[d.core]}, {set_x[d.core]}, {z2}, "
+                              f"&{a}, &{b}, &{x2});")
+                            e(f"  {a} = kin_fold({a}, {_f(bias)});")
+                            bias -= math.pi
+                            set_x[j], set_z[j] = x2, z2
+                            angles[(d, j)] = (a, b)
+                            if self.needs_su2:
+                                bm, rm = tmp(f"t{t}_B"), tmp(f"t{t}_R")
+                                e(f"  const SU2 {bm} = su2_boost_z_from_p({part[d][j]});")
+                                if d.core in rmat:
+                                    e(f"  const SU2 {rm} = su2_mul(su2_rot_yz({b}, {a}), "
+                                      f"su2_mul({bmat[d.core]}, {rmat[d.core]}));")
+                                else:
+                                    e(f"  const SU2 {rm} = su2_rot_yz({b}, {a});")
+                                bmat[j], rmat[j] = bm, rm
+                    decays = later
+                frames.append((topo, angles, rmat, bmat, mom))
+            return frames
+
+        # unswapped momenta, then one relabelling per identical-particle swap
+        # (final pi takes the momentum of src[pi])
+        all_frames = [build_frames({o: f"P[{fin[o]}]" for o in fin})]
+        for sw in plan.swaps:
+            all_frames.append(build_frames({o: f"P[{fin[sw['src'].get(o, o)]}]" for o in fin}))
         # the plan's fields
-        for fi, fname in enumerate(plan.fields):
+        for fi, full_name in enumerate(plan.fields):
+            sk, fname = split_swap(full_name)
+            frames = all_frames[sk]
             parts = fname.split("/")
             if parts[0] == "m":
                 for topo, angles, rmat, bmat, mom in frames:

@@ -22,6 +22,8 @@ import math
 import numpy as np
 import torch
 
+from .plan import split_swap
+
 _EPS = 1e-14
 
 
@@ -198,18 +200,29 @@ def event_fields(plan, p4, device=None):
     n = next(iter(p4.values())).shape[0]
     dev = next(iter(p4.values())).device
     out = torch.zeros((plan.n_fields, n), dtype=torch.float64, device=dev)
-    frames = []
-    for tidx, topo in enumerate(plan.topos):
-        chain = topo.chain
-        mom = {}
-        for o in chain.outs:
-            mom[o] = p4[str(o)]
-        for p in chain.inner:
-            mom[p] = sum(mom[f] for f in chain.final_set(p))
-        mom[chain.top] = sum(mom[f] for f in chain.outs)
-        angles, rmat, bmat = _chain_frames(topo, mom)
-        frames.append((topo, angles, rmat, bmat, mom))
-    for fi, fname in enumerate(plan.fields):
+
+    def topo_frames(mom4):
+        frames = []
+        for tidx, topo in enumerate(plan.topos):
+            chain = topo.chain
+            mom = {}
+            for o in chain.outs:
+                mom[o] = mom4[str(o)]
+            for p in chain.inner:
+                mom[p] = sum(mom[f] for f in chain.final_set(p))
+            mom[chain.top] = sum(mom[f] for f in chain.outs)
+            angles, rmat, bmat = _chain_frames(topo, mom)
+            frames.append((topo, angles, rmat, bmat, mom))
+        return frames
+
+    # unswapped momenta, then one relabelling per identical-particle swap
+    # (final pi takes the momentum of src[pi])
+    all_frames = [topo_frames(p4)]
+    for sw in plan.swaps:
+        all_frames.append(topo_frames({k: p4[sw["src"].get(k, k)] for k in p4}))
+    for fi, full_name in enumerate(plan.fields):
+        sk, fname = split_swap(full_name)
+        frames = all_frames[sk]
         parts = fname.split("/")
         if parts[0] == "m":
             for topo, angles, rmat, bmat, mom in frames:

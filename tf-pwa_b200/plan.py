@@ -9,6 +9,12 @@ one per-event quantity produced once per dataset by the kinematics step:
 * ``<t>/<decay>/<final>/aligned/{alpha,beta,gamma}``: Wigner alignment
   angles of a final particle with spin in a non-reference chain.
 
+With identical final particles (``data.identical_particles``), every
+non-identity permutation of them adds a "swap": the same fields computed
+from the relabelled momenta, named ``s<k>|<field>``
+(``tf_pwa/cal_angle.py:684-756``), with the sign and helicity-axis order
+its amplitude is added with (``tf_pwa/amp/core.py:1826-1882``).
+
 Node and decay names follow the reference's standard topology
 (``tf_pwa/particle.py:698-717``): an inner node is named by its sorted final
 particles, ``(B, C)``; topologies are enumerated as in
@@ -19,6 +25,9 @@ standard topology; a chain reads the angles of its own decay's ``outs[0]``
 (``tf_pwa/amp/core.py:1414-1429``).  Helicity ``gamma`` is identically zero
 for two-body helicity angles and is not stored.
 """
+
+
+import itertools
 
 
 def node_name(finals):
@@ -66,10 +75,19 @@ class Plan:
                 self.topos.append(t)
         self.fields = []
         self._index = {}
+        self._prefix = ""
         self.align_ref = self._alignment_reference()
         self.chains = [self._chain_fields(i, c) for i, c in enumerate(group)]
+        self.swaps = []
+        for k, (src, factor, trans) in enumerate(
+                swap_specs(group, getattr(group, "identical_particles", None))):
+            self._prefix = f"s{k + 1}|"
+            chains = [self._chain_fields(i, c) for i, c in enumerate(group)]
+            self.swaps.append({"src": src, "factor": factor, "trans": trans, "chains": chains})
+        self._prefix = ""
 
     def field(self, name):
+        name = self._prefix + name
         if name not in self._index:
             self._index[name] = len(self.fields)
             self.fields.append(name)
@@ -123,3 +141,56 @@ class Plan:
     @property
     def n_fields(self):
         return len(self.fields)
+
+
+def split_swap(fname):
+    """(swap number, base field name): 0 for the unswapped fields."""
+    if fname.startswith("s") and "|" in fname:
+        head, rest = fname.split("|", 1)
+        return int(head[1:]), rest
+    return 0, fname
+
+
+def swap_specs(group, identical):
+    """Per non-identity permutation of the identical particles, in the
+    reference's order (``itertools.product`` of each group's permutations,
+    ``tf_pwa/cal_angle.py:684-716``):
+
+    * ``src``: final name -> name of the final whose momentum it takes;
+    * ``factor``: -1 per exchanged pair of half-integer-spin particles
+      (``tf_pwa/amp/core.py:1826-1840``);
+    * ``trans``: the helicity-axis order of the swapped amplitude,
+      out-axis j = swapped-amplitude axis trans[j]
+      (``tf_pwa/amp/core.py:1842-1867``)."""
+    if not identical:
+        return []
+    groups = [[str(x) for x in g] for g in identical]
+    outs = [str(o) for o in group.outs]
+    spin = {str(o): o.J for o in group.outs}
+    ident = tuple(tuple(g) for g in groups)
+    out = []
+    for comb in itertools.product(*[list(itertools.permutations(g)) for g in groups]):
+        if comb == ident:
+            continue
+        src = {}
+        for c, g in zip(comb, groups):
+            for ci, pi in zip(c, g):
+                src[pi] = ci
+        factor = 1.0
+        used = []
+        for g, c in zip(groups, comb):
+            if round(2 * spin[g[0]]) % 2 == 0:
+                continue
+            for m, n in zip(g, c):
+                if (m, n) in used or (n, m) in used:
+                    continue
+                used.append((m, n))
+                if m != n:
+                    factor = -factor
+        pairs = [(k, l) for g, c in zip(groups, comb) for k, l in zip(g, c)]
+        tmap = {l: k for k, l in pairs}
+        tmap.update(dict(pairs))
+        new_order = [tmap.get(o, o) for o in outs]
+        index_map = {k: i for i, k in enumerate(new_order)}
+        out.append((src, factor, [index_map[o] for o in outs]))
+    return out
