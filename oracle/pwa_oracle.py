@@ -23,7 +23,7 @@ per-event inputs (invariant masses and helicity / alignment angles):
   particle model ``tf_pwa/amp/core.py:349-418``
 * chain contraction with totals and alignment D's: ``tf_pwa/amp/core.py:1392-1445,1563-1604``
 * sum over chains and |A|^2: ``tf_pwa/amp/core.py:1696-1728,1919-1931``;
-  identical-particle swaps ``tf_pwa/amp/core.py:1826-1882``
+  identical-particle and CP-conjugate swaps ``tf_pwa/amp/core.py:1826-1913``
 * clip_log and the weighted NLL with alpha scaling and normalised MC
   weights: ``tf_pwa/model/model.py:283-292,407-449,603-641,1126-1229``
 
@@ -368,7 +368,10 @@ class OracleModel:
         for sw in self.plan.swaps:
             b = sum(self.chain_amp(x, ci, vals, coup, sw["chains"][ci])
                     for ci in range(len(self.group)))
-            a = a + sw["factor"] * np.transpose(b, [0, 1] + [2 + t for t in sw["trans"]])
+            b = np.transpose(b, [0, 1] + [2 + t for t in sw["trans"]])
+            if sw["flip"]:  # CP-conjugate: every helicity reversed (core.py:1899-1911)
+                b = b[(slice(None),) + (slice(None, None, -1),) * (b.ndim - 1)]
+            a = a + sw["factor"] * b
         return a
 
     def pdf(self, x, vals, polar=None):

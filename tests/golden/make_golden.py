@@ -44,6 +44,7 @@ CASES = {
     "d2kpipi_shapes": ("d2kpipi_shapes.yml", 400, 0, 1500, 16, True, {}),
     "dp2kpipi_ident": ("dp2kpipi_ident.yml", 400, 0, 1500, 17, True, {}),
     "ident_fermions": ("ident_fermions.yml", 300, 0, 1200, 18, False, {}),
+    "epem_cp": ("epem_cp.yml", 300, 0, 1200, 19, False, {}),
 }
 
 
@@ -121,8 +122,10 @@ def main(ref_root):
             d = lst[0]
             cols = np.zeros((plan.n_fields, len(d["weight"])))
             # identical-particle swaps: the reference's id_swap data sets, in
-            # its permutation order
+            # its permutation order, then the CP-conjugate ones
             swap_sets = [d] + list(d.get("id_swap", {}).values())
+            if "cp_swap" in d:  # the CP-conjugate data and its own swaps
+                swap_sets += [d["cp_swap"]] + list(d["cp_swap"].get("id_swap", {}).values())
             for fi, full_name in enumerate(plan.fields):
                 sk, fname = split_swap(full_name)
                 ds = swap_sets[sk]

@@ -105,6 +105,9 @@ class Tensor(torch.Tensor):
         return self.shape
 
     def __getitem__(self, idx):
+        # TF reads a list of slices / Ellipsis as a tuple of slice specs
+        if isinstance(idx, list) and any(isinstance(s, slice) or s is Ellipsis for s in idx):
+            idx = tuple(idx)
         idx_t = idx if isinstance(idx, tuple) else (idx,)
         flips = []
         new_idx = []

@@ -14,7 +14,7 @@ from common import golden_data, load_golden, load_model
 pytestmark = pytest.mark.gpu
 
 CASES = ["d2kpipi", "d2kpipi_float", "lc2pkpi", "b2dstkpi", "d2kpipi_shapes", "dp2kpipi_ident",
-         "ident_fermions"]
+         "ident_fermions", "epem_cp"]
 
 
 def _engine(name):
@@ -94,7 +94,8 @@ def test_reproducible_bitwise():
     eng.close()
 
 
-@pytest.mark.parametrize("name", ["d2kpipi", "lc2pkpi", "b2dstkpi", "dp2kpipi_ident", "ident_fermions"])
+@pytest.mark.parametrize("name", ["d2kpipi", "lc2pkpi", "b2dstkpi", "dp2kpipi_ident", "ident_fermions",
+                                  "epem_cp"])
 def test_cached_columns_fcn(name):
     """Mixed form with fixed masses/widths: FP32 column cache + FP64 Gram,
     NLL/gradient from the C-side chain rule, against the reference."""

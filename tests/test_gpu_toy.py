@@ -28,7 +28,8 @@ def _engine(cfg, variables=None):
     return Engine(dc.decay_group, plan, vm), dc, vm, plan
 
 
-@pytest.mark.parametrize("name", ["d2kpipi", "lc2pkpi", "b2dstkpi", "dp2kpipi_ident", "ident_fermions"])
+@pytest.mark.parametrize("name", ["d2kpipi", "lc2pkpi", "b2dstkpi", "dp2kpipi_ident", "ident_fermions",
+                                  "epem_cp"])
 def test_fields_from_p4_match_reference(name):
     import torch
 

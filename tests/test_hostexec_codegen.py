@@ -27,7 +27,7 @@ from common import golden_data, load_golden, load_model
 from hostexec import HostModel
 
 CASES = ["d2kpipi", "d2kpipi_float", "lc2pkpi", "toy_vvp", "b2dstkpi", "d2kpipi_shapes",
-         "dp2kpipi_ident", "ident_fermions"]
+         "dp2kpipi_ident", "ident_fermions", "epem_cp"]
 
 _CACHE = {}
 
@@ -99,7 +99,7 @@ def test_columns_rebuild_amplitude(name, build_dir):
 
 
 @pytest.mark.parametrize("name", ["d2kpipi", "lc2pkpi", "toy_vvp", "b2dstkpi", "dp2kpipi_ident",
-                                  "ident_fermions"])
+                                  "ident_fermions", "epem_cp"])
 def test_kinematics_match_reference(name, build_dir):
     eng, hm, g, meta, _, _ = _setup(name, build_dir)
     for kind in ("data", "mc"):
@@ -107,7 +107,7 @@ def test_kinematics_match_reference(name, build_dir):
                                    atol=1e-11)
 
 
-@pytest.mark.parametrize("name", ["lc2pkpi", "b2dstkpi", "ident_fermions"])
+@pytest.mark.parametrize("name", ["lc2pkpi", "b2dstkpi", "ident_fermions", "epem_cp"])
 def test_generator_matches_oracle(name, build_dir):
     from oracle.pwa_oracle import OracleModel
     from oracle.toy_oracle import genbod_levels, uniforms

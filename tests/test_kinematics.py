@@ -8,7 +8,7 @@ from common import load_golden, load_model
 
 
 @pytest.mark.parametrize("name", ["d2kpipi", "lc2pkpi", "toy_vvp", "b2dstkpi", "dp2kpipi_ident",
-                                  "ident_fermions"])
+                                  "ident_fermions", "epem_cp"])
 @pytest.mark.parametrize("kind", ["data", "mc"])
 def test_fields_match_reference_cal_angle(name, kind):
     from tf_pwa_b200.kinematics import event_fields, p4_dict

@@ -240,11 +240,15 @@ class ModelCode:
     def _out(self, o):
         """Output index of the chain helicity tuple o = (top, finals...) in
         the current pass: a swap's amplitude enters with its final-helicity
-        axes reordered (out-axis j = its axis trans[j])."""
+        axes reordered (out-axis j = its axis trans[j]) and, for the
+        CP-conjugate passes, every helicity reversed."""
         if self._pass == 0:
             return self.out_index[o]
-        tr = self.plan.swaps[self._pass - 1]["trans"]
-        return self.out_index[(o[0],) + tuple(o[1 + t] for t in tr)]
+        sw = self.plan.swaps[self._pass - 1]
+        o2 = (o[0],) + tuple(o[1 + t] for t in sw["trans"])
+        if sw["flip"]:
+            o2 = tuple(-h for h in o2)
+        return self.out_index[o2]
 
     def _factor(self):
         return 1.0 if self._pass == 0 else self.plan.swaps[self._pass - 1]["factor"]

@@ -256,12 +256,14 @@ class DecayConfig:
             pass  # charge-conjugation flips are disabled (decay_config.py:423-427)
         group = DecayGroup(chains)
         # data.identical_particles: lists of final particles whose momenta are
-        # symmetrised (tf_pwa/config_loader/decay_config.py:100-104)
+        # symmetrised; data.cp_particles: charge-conjugate final pairs of a
+        # self-conjugate system (tf_pwa/config_loader/decay_config.py:100-107)
         ident = self.data_config.get("identical_particles")
         if ident:
-            if self.data_config.get("cp_particles"):
-                raise NotImplementedError("cp_particles (CP-swap symmetrisation)")
             group.identical_particles = [[str(x) for x in g] for g in ident]
+        cp = self.data_config.get("cp_particles")
+        if cp:
+            group.cp_particles = [[str(x) for x in pr] for pr in cp]
         return group
 
 

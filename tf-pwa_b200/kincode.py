@@ -164,11 +164,15 @@ class KinCode:
                 frames.append((topo, angles, rmat, bmat, mom))
             return frames
 
-        # unswapped momenta, then one relabelling per identical-particle swap
-        # (final pi takes the momentum of src[pi])
+        # unswapped momenta, then one relabelling per swap (final pi takes the
+        # momentum of src[pi], three-momentum reversed in the CP-conjugate ones)
         all_frames = [build_frames({o: f"P[{fin[o]}]" for o in fin})]
         for sw in plan.swaps:
-            all_frames.append(build_frames({o: f"P[{fin[sw['src'].get(o, o)]}]" for o in fin}))
+            pe = {}
+            for o in fin:
+                q = f"P[{fin[sw['src'].get(o, o)]}]"
+                pe[o] = f"LV{{{q}.t, -{q}.x, -{q}.y, -{q}.z}}" if sw["neg"] else q
+            all_frames.append(build_frames(pe))
         # the plan's fields
         for fi, full_name in enumerate(plan.fields):
             sk, fname = split_swap(full_name)

@@ -215,11 +215,17 @@ def event_fields(plan, p4, device=None):
             frames.append((topo, angles, rmat, bmat, mom))
         return frames
 
-    # unswapped momenta, then one relabelling per identical-particle swap
-    # (final pi takes the momentum of src[pi])
+    # unswapped momenta, then one relabelling per swap (final pi takes the
+    # momentum of src[pi], three-momentum reversed in the CP-conjugate ones)
+    def neg(v):
+        return torch.cat([v[:, :1], -v[:, 1:]], 1)
+
     all_frames = [topo_frames(p4)]
     for sw in plan.swaps:
-        all_frames.append(topo_frames({k: p4[sw["src"].get(k, k)] for k in p4}))
+        moved = {k: p4[sw["src"].get(k, k)] for k in p4}
+        if sw["neg"]:
+            moved = {k: neg(v) for k, v in moved.items()}
+        all_frames.append(topo_frames(moved))
     for fi, full_name in enumerate(plan.fields):
         sk, fname = split_swap(full_name)
         frames = all_frames[sk]

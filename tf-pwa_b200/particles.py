@@ -412,6 +412,7 @@ class DecayGroup:
     def __init__(self, chains):
         self.chains = list(chains)
         self.identical_particles = None
+        self.cp_particles = None
         self.top = self.chains[0].top
         self.outs = sorted(self.chains[0].outs)
         for c in self.chains:

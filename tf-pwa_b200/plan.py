@@ -13,7 +13,12 @@ With identical final particles (``data.identical_particles``), every
 non-identity permutation of them adds a "swap": the same fields computed
 from the relabelled momenta, named ``s<k>|<field>``
 (``tf_pwa/cal_angle.py:684-756``), with the sign and helicity-axis order
-its amplitude is added with (``tf_pwa/amp/core.py:1826-1882``).
+its amplitude is added with (``tf_pwa/amp/core.py:1826-1882``).  With
+``data.cp_particles`` the CP-conjugate configuration (charge-conjugate
+finals exchanged, three-momenta reversed) and its own identical-particle
+swaps are further swaps, added with every helicity reversed and the product
+of the self-conjugate finals' C parities
+(``tf_pwa/cal_angle.py:708-717,799-822``, ``tf_pwa/amp/core.py:1884-1913``).
 
 Node and decay names follow the reference's standard topology
 (``tf_pwa/particle.py:698-717``): an inner node is named by its sorted final
@@ -79,11 +84,11 @@ class Plan:
         self.align_ref = self._alignment_reference()
         self.chains = [self._chain_fields(i, c) for i, c in enumerate(group)]
         self.swaps = []
-        for k, (src, factor, trans) in enumerate(
-                swap_specs(group, getattr(group, "identical_particles", None))):
+        for k, sw in enumerate(pass_specs(group, getattr(group, "identical_particles", None),
+                                          getattr(group, "cp_particles", None))):
             self._prefix = f"s{k + 1}|"
-            chains = [self._chain_fields(i, c) for i, c in enumerate(group)]
-            self.swaps.append({"src": src, "factor": factor, "trans": trans, "chains": chains})
+            sw["chains"] = [self._chain_fields(i, c) for i, c in enumerate(group)]
+            self.swaps.append(sw)
         self._prefix = ""
 
     def field(self, name):
@@ -151,6 +156,76 @@ def split_swap(fname):
     return 0, fname
 
 
+def _transpose_order(outs, pairs):
+    """Helicity-axis order of an exchange of the final pairs ``pairs``:
+    out-axis j takes axis order[j] (``tf_pwa/amp/core.py:1853-1867``)."""
+    tmap = {l: k for k, l in pairs}
+    tmap.update(dict(pairs))
+    new_order = [tmap.get(o, o) for o in outs]
+    index_map = {k: i for i, k in enumerate(new_order)}
+    return [index_map[o] for o in outs]
+
+
+def cp_charge_group(finals, identical, cp):
+    """Pairs of charge-conjugate final groups, self-conjugate finals paired
+    with themselves (``tf_pwa/particle.py:992-1022``)."""
+    used = set()
+    ret = []
+    for a, b in cp:
+        ga = next((g for g in identical if a in g), None)
+        gb = next((g for g in identical if b in g), None)
+        if ga is None and gb is None:
+            used.update((a, b))
+            ret.append([[a], [b]])
+        elif ga is None or gb is None or len(ga) != len(gb):
+            raise ValueError("cp_particles pair identical groups of different sizes")
+        else:
+            used.update(ga)
+            used.update(gb)
+            ret.append([list(ga), list(gb)])
+    for f in finals:
+        if f not in used:
+            ret.append([[f], [f]])
+    return ret
+
+
+def pass_specs(group, identical, cp):
+    """The identical-particle swaps of the unswapped momenta, then (with
+    CP-conjugate pairs) the CP-conjugate configuration and its swaps.  Each
+    is a dict with ``src`` (final -> final whose momentum it takes), ``neg``
+    (three-momenta reversed), ``factor``, ``trans`` (out-axis j = the
+    pass's helicity axis trans[j]) and ``flip`` (every helicity reversed)."""
+    ident = [[str(x) for x in g] for g in (identical or [])]
+    outs = [str(o) for o in group.outs]
+    passes = [dict(src=src, neg=False, factor=f, trans=t, flip=False)
+              for src, f, t in swap_specs(group, ident)]
+    if not cp:
+        return passes
+    cp = [[str(x) for x in pr] for pr in cp]
+    cg = cp_charge_group(outs, ident, cp)
+    byname = {str(o): o for o in group.outs}
+    cp_src, frac, change = {}, 1.0, []
+    for a, b in cg:
+        for i, j in zip(a, b):
+            cp_src[j] = i
+            if i != j:
+                cp_src[i] = j
+                change.append((i, j))
+            else:
+                c = byname[i].C
+                if c is None:
+                    raise ValueError(f"self-conjugate final {i} needs its C parity")
+                frac *= float(c)
+    t_cp = _transpose_order(outs, change)
+    passes.append(dict(src={o: cp_src.get(o, o) for o in outs}, neg=True, factor=frac,
+                       trans=t_cp, flip=True))
+    for src, f, t in swap_specs(group, ident):
+        # swap of the CP-conjugate momenta, then the CP transposition
+        passes.append(dict(src={o: cp_src.get(src.get(o, o), src.get(o, o)) for o in outs},
+                           neg=True, factor=f * frac, trans=[t[k] for k in t_cp], flip=True))
+    return passes
+
+
 def swap_specs(group, identical):
     """Per non-identity permutation of the identical particles, in the
     reference's order (``itertools.product`` of each group's permutations,
@@ -188,9 +263,5 @@ def swap_specs(group, identical):
                 if m != n:
                     factor = -factor
         pairs = [(k, l) for g, c in zip(groups, comb) for k, l in zip(g, c)]
-        tmap = {l: k for k, l in pairs}
-        tmap.update(dict(pairs))
-        new_order = [tmap.get(o, o) for o in outs]
-        index_map = {k: i for i, k in enumerate(new_order)}
-        out.append((src, factor, [index_map[o] for o in outs]))
+        out.append((src, factor, _transpose_order(outs, pairs)))
     return out
