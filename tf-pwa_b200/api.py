@@ -316,6 +316,9 @@ class ConfigLoader:
         self.precision = precision
         self._amp = None
         self._data = {}
+        self._toy_seed = 0 if seed is None else int(seed)
+        self._toy_calls = 0
+        self.max_amplitude = None
 
     # -- model --------------------------------------------------------------
     def get_decay(self, full=True):
@@ -487,6 +490,71 @@ class ConfigLoader:
         self.inv_he = inv
         err = np.sqrt(np.abs(np.diag(inv)))
         return dict(zip(self.vm.trainable_vars, err))
+
+    # -- toys and phase space (``tf_pwa/config_loader/sample.py``) ------------
+    def _toy_engine(self):
+        from .engine import Engine
+
+        return Engine(self.decay_group, self.plan, self.vm)
+
+    def _next_seed(self, seed):
+        """64-bit key of one generator call: the given seed, else the
+        loader's seed and a per-call counter (successive calls differ)."""
+        from .workload import _seed
+
+        if seed is not None:
+            return _seed(seed, 0)
+        self._toy_calls += 1
+        return _seed(self._toy_seed, 2 + self._toy_calls)
+
+    def generate_phsp(self, N=1000, include_charge=False, cal_max=False, seed=None):
+        """N flat phase-space events (``sample.py:254-260``) as device
+        EventData with unit weights: GENBOD candidates accepted on their
+        phase-space weight and their fields computed, in the engine's toy
+        kernels."""
+        from .workload import generate
+
+        if include_charge:
+            raise NotImplementedError("charge-conjugated events")
+        eng = self._toy_engine()
+        try:
+            x, _ = generate(eng, int(N), self._next_seed(seed))
+        finally:
+            eng.close()
+        return EventData(x, np.ones(int(N)))
+
+    def generate_phsp_p(self, N=1000, cal_max=False, seed=None):
+        """Momenta (N, n_final, 4) of N flat phase-space events in
+        ``dat_order`` (``sample.py:224-229``), on the device."""
+        from .workload import generate
+
+        eng = self._toy_engine()
+        try:
+            _, _, p4 = generate(eng, int(N), self._next_seed(seed), with_p4=True)
+        finally:
+            eng.close()
+        return p4
+
+    def generate_toy(self, N=1000, force=True, gen=None, gen_p=None, importance_f=None,
+                     max_N=100000, include_charge=False, cal_phsp_max=False, seed=None):
+        """N events of the current model by accept-reject on sum |A|^2
+        (``sample.py:75-141``, ``applications.py:394-487``) as device
+        EventData with unit weights.  The maximum found is kept in
+        ``self.max_amplitude`` and reused by later calls, as the reference
+        does; a candidate above it raises it and restarts the sample."""
+        from .workload import generate
+
+        if gen is not None or gen_p is not None or importance_f is not None or include_charge:
+            raise NotImplementedError("custom generators, importance functions or charges")
+        eng = self._toy_engine()
+        try:
+            C = eng.consts(self.vm.get_all_dic())
+            x, fmax = generate(eng, int(N), self._next_seed(seed), consts=C,
+                               fmax=self.max_amplitude)
+        finally:
+            eng.close()
+        self.max_amplitude = fmax
+        return EventData(x, np.ones(int(N)))
 
     def cal_fitfractions(self, params={}, mcdata=None, res=None, exclude_res=[], batch=25000,
                          method="old", fcn=None):

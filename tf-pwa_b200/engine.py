@@ -155,6 +155,8 @@ class Engine:
         self._gram = None
         self.mc_share = 1.0      # this device's fraction of the total MC weight
         self.dist_reduce = None  # vector sum over devices (multi-GPU)
+        self.device = "cuda"     # where the engine's tensors live
+        self.toy_chunk = 1 << 24  # generator candidates per toy-kernel launch
         self._prepare_structure()
         if compile:
             self._create()

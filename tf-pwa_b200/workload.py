@@ -41,15 +41,22 @@ def _seed(seed, stream):
     return (int(seed) * 0x9E3779B97F4A7C15 + 0x632BE59BD9B4E019 * (stream + 1)) & (2**64 - 1)
 
 
-def generate(eng, n, seed, consts=None, fmax=None, chunk=1 << 24):
+def generate(eng, n, seed, consts=None, fmax=None, chunk=None, with_p4=False):
     """n events on the device, generated in one pass per candidate chunk by
     the engine's toy kernels: flat phase space (``consts`` None) or signal
     by accept-reject on sum |A|^2 (the procedure of
     ``tf_pwa/applications.py:394-487``: a first chunk at the phase-space
     step alone gives fmax = 1.2 max sum |A|^2; a later candidate above fmax
-    raises fmax and restarts).  Returns (fields (n_fields, n), fmax)."""
+    raises fmax and restarts).  Returns (fields (n_fields, n), fmax), plus
+    the momenta (n, n_final, 4) with ``with_p4``."""
+    dev = eng.device
+    chunk = chunk or eng.toy_chunk
+    if n <= 0:
+        x = torch.zeros((eng.plan.n_fields, 0), dtype=torch.float64, device=dev)
+        p4 = torch.zeros((0, eng.code.kin.nfin, 4), dtype=torch.float64, device=dev)
+        return (x, fmax, p4) if with_p4 else (x, fmax)
     flat = consts is None
-    f = torch.empty(chunk, dtype=torch.float64, device="cuda")
+    f = torch.empty(chunk, dtype=torch.float64, device=dev)
     if not flat and fmax is None:
         eng.toy_select(consts, seed, 0, chunk, 0.0, 0, f)
         fmax = 1.2 * float(f.max())
@@ -70,6 +77,9 @@ def generate(eng, n, seed, consts=None, fmax=None, chunk=1 << 24):
         if not restart:
             break
     idx = torch.cat(sel)[:n]
+    if with_p4:
+        x, p4 = eng.toy_fields(seed, idx, with_p4=True)
+        return x, fmax, p4
     return eng.toy_fields(seed, idx), fmax
 
 
