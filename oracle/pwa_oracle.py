@@ -16,7 +16,8 @@ per-event inputs (invariant masses and helicity / alignment angles):
 * relative momenta q (clamped) and q^2 (unclamped): ``tf_pwa/amp/core.py:311-334``
 * Blatt-Weisskopf polynomial / B'_l(q^2): ``tf_pwa/breit_wigner.py:268-355``
 * barrier factor q^l B'_l of each LS: ``tf_pwa/amp/core.py:1072-1097``
-* helicity coupling H = sum_ls g_ls bf_ls CG_ls: ``tf_pwa/amp/core.py:931-947,1025-1043``
+* helicity coupling H = sum_ls g_ls bf_ls CG_ls, reversed for charge < 0
+  events: ``tf_pwa/amp/core.py:931-947,1025-1043``
 * decay amplitude H * D*: ``tf_pwa/amp/core.py:1149-1164``
 * lineshapes BWR / BW with running width Gamma(m): ``tf_pwa/breit_wigner.py:56-91,231-245``,
   BWR2 with Gamma2(m) from q^2: ``tf_pwa/breit_wigner.py:193-210,248-265``,
@@ -306,6 +307,10 @@ class OracleModel:
             mdep = np.broadcast_to(gls[None, :], (x.shape[1], len(ls)))
         cg = cg_matrix(a.J, b.J, c.J, ls, b.spins, c.spins)
         H = np.einsum("nl,lbc->nbc", mdep, cg)
+        ci = getattr(self.plan, "charge_index", None)
+        if ci is not None and d.allow_cc:
+            # charge < 0: H[..., ::-1, ::-1] (core.py:938-945)
+            H = np.where((x[ci] > 0)[:, None, None], H, H[:, ::-1, ::-1])
         return H[:, None, :, :] * Dc
 
     def lineshape(self, x, cf, chain, p, vals):

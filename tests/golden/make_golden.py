@@ -45,6 +45,8 @@ CASES = {
     "dp2kpipi_ident": ("dp2kpipi_ident.yml", 400, 0, 1500, 17, True, {}),
     "ident_fermions": ("ident_fermions.yml", 300, 0, 1200, 18, False, {}),
     "epem_cp": ("epem_cp.yml", 300, 0, 1200, 19, False, {}),
+    "lc2pkpi_cc": ("lc2pkpi_cc.yml", 400, 0, 1500, 20, False, {}),
+    "b2dstkpi_cc": ("b2dstkpi_cc.yml", 400, 0, 1500, 21, False, {}),
 }
 
 
@@ -98,6 +100,14 @@ def main(ref_root):
         if nb:
             dic2["data"]["bg"] = [os.path.join(tmp, "bg.dat")]
         dic2["data"].update(extra)
+        charges = {}
+        if plan.use_charge:
+            # per-event charge_conjugation files (random +1 / -1)
+            for kind, arr in p4.items():
+                charges[kind] = rng.choice([-1.0, 1.0], size=arr.shape[0])
+                fc = os.path.join(tmp, kind + "_charge.dat")
+                np.savetxt(fc, charges[kind], fmt="%.1f")
+                dic2["data"][kind + "_charge"] = [fc]
         cfg_path = os.path.join(tmp, "config.yml")
         with open(cfg_path, "w") as f:
             yaml.safe_dump(dic2, f)
@@ -127,6 +137,9 @@ def main(ref_root):
             if "cp_swap" in d:  # the CP-conjugate data and its own swaps
                 swap_sets += [d["cp_swap"]] + list(d["cp_swap"].get("id_swap", {}).values())
             for fi, full_name in enumerate(plan.fields):
+                if fi == plan.charge_index:
+                    cols[fi] = np.asarray(d["charge_conjugation"])
+                    continue
                 sk, fname = split_swap(full_name)
                 ds = swap_sets[sk]
                 topo_keys = list(ds["decay"].keys())
@@ -166,6 +179,8 @@ def main(ref_root):
         )
         if nb:
             out.update(fields_bg=fields["bg"], f_bg=f_vals["bg"], p4_bg=p4["bg"])
+        if charges:
+            out.update(charge_data=charges["data"], charge_mc=charges["phsp"])
         if do_hess:
             n2, g2, h2 = fcn.nll_grad_hessian()
             out.update(hess=np.asarray(h2, np.float64), hess_grad=np.asarray(g2, np.float64),

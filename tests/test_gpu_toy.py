@@ -29,7 +29,7 @@ def _engine(cfg, variables=None):
 
 
 @pytest.mark.parametrize("name", ["d2kpipi", "lc2pkpi", "b2dstkpi", "dp2kpipi_ident", "ident_fermions",
-                                  "epem_cp"])
+                                  "epem_cp", "lc2pkpi_cc", "b2dstkpi_cc"])
 def test_fields_from_p4_match_reference(name):
     import torch
 
@@ -37,7 +37,9 @@ def test_fields_from_p4_match_reference(name):
     eng, dc, vm, plan = _engine(meta["config"])
     for kind in ("data", "mc"):
         p4 = torch.as_tensor(g["p4_" + kind], device="cuda")
-        x = eng.fields_from_p4(p4).cpu().numpy()
+        ch = g.get("charge_" + kind)
+        x = eng.fields_from_p4(p4, charge=None if ch is None else
+                               torch.as_tensor(ch, device="cuda")).cpu().numpy()
         np.testing.assert_allclose(x, g["fields_" + kind], rtol=0, atol=TOL_FIELD)
     eng.close()
 

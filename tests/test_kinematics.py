@@ -8,14 +8,17 @@ from common import load_golden, load_model
 
 
 @pytest.mark.parametrize("name", ["d2kpipi", "lc2pkpi", "toy_vvp", "b2dstkpi", "dp2kpipi_ident",
-                                  "ident_fermions", "epem_cp"])
+                                  "ident_fermions", "epem_cp", "lc2pkpi_cc", "b2dstkpi_cc"])
 @pytest.mark.parametrize("kind", ["data", "mc"])
 def test_fields_match_reference_cal_angle(name, kind):
+    """(with per-event charges: parity transform of charge -1 momenta under
+    cp_trans, or the charge field without it)"""
     from tf_pwa_b200.kinematics import event_fields, p4_dict
 
     g, meta = load_golden(name)
     dc, vm, plan = load_model(meta["config"])
-    x = event_fields(plan, p4_dict(g["p4_" + kind], dc.data_config["dat_order"])).numpy()
+    x = event_fields(plan, p4_dict(g["p4_" + kind], dc.data_config["dat_order"]),
+                     charge=g.get("charge_" + kind)).numpy()
     np.testing.assert_allclose(x, g["fields_" + kind], rtol=0, atol=1e-11)
 
 

@@ -341,17 +341,21 @@ class ConfigLoader:
         files = [self._path(f) for f in (files if isinstance(files, list) else [files])]
         return load_dat_file(files, len(self.get_dat_order()))
 
-    def data_from_p4(self, p4, weight=None, device=None):
+    def data_from_p4(self, p4, weight=None, device=None, charge=None):
         """EventData from (N, n_final, 4) momenta in dat_order.  With
         ``device="cuda"`` the engine's kinematics kernel computes the fields
-        on the GPU (one thread per event); otherwise the host code does."""
+        on the GPU (one thread per event); otherwise the host code does.
+        ``charge``: per-event charge_conjugation (+1 / -1) for models whose
+        data carry charges."""
         if device is not None and str(device).startswith("cuda"):
             import torch
 
             eng = self.get_amplitude()._engine()
-            x = eng.fields_from_p4(torch.as_tensor(p4, dtype=torch.float64, device=device))
+            x = eng.fields_from_p4(torch.as_tensor(p4, dtype=torch.float64, device=device),
+                                   charge=charge)
             return EventData(x, weight)
-        x = event_fields(self.plan, p4_dict(p4, self.get_dat_order()), device=device)
+        x = event_fields(self.plan, p4_dict(p4, self.get_dat_order()), device=device,
+                         charge=charge)
         return EventData(x, weight)
 
     def get_data(self, idx):
@@ -372,6 +376,12 @@ class ConfigLoader:
             wfile = np.concatenate([np.loadtxt(self._path(x)).reshape(-1)
                                     for x in (wkey if isinstance(wkey, list) else [wkey])])
         sign = -1.0 if any(re.match(pat, idx) for pat in dcfg.get("negtive_idx", ["bg*"])) else 1.0
+        # per-event charges (``<idx>_charge``: a number or files, default +1)
+        ckey = dcfg.get(idx + "_charge")
+        cfile = None
+        if ckey is not None and not isinstance(ckey, (int, float)):
+            cfile = np.concatenate([np.loadtxt(self._path(x)).reshape(-1)
+                                    for x in (ckey if isinstance(ckey, list) else [ckey])])
         ret, off = [], 0
         for f in files:
             p4 = self.load_p4([f])
@@ -382,8 +392,14 @@ class ConfigLoader:
                     raise ValueError(f"{idx}_weight holds {wfile.shape[0]} values for more events")
             else:
                 w = np.full(n, 1.0 if wkey is None else float(wkey))
+            ch = None
+            if self.plan.use_charge:
+                ch = cfile[off:off + n] if cfile is not None else \
+                    np.full(n, 1.0 if ckey is None else float(ckey))
+                if ch.shape[0] != n:
+                    raise ValueError(f"{idx}_charge holds {cfile.shape[0]} values for more events")
             off += n
-            ret.append(self.data_from_p4(p4, sign * w))
+            ret.append(self.data_from_p4(p4, sign * w, charge=ch))
         self._data[idx] = ret
         return ret
 

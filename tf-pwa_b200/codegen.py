@@ -88,10 +88,14 @@ class ModelCode:
         self.out_hel = list(itertools.product(*[p.spins for p in self.outs]))
         self.out_index = {o: j for j, o in enumerate(self.out_hel)}
         self.nout = len(self.out_hel)
-        self.mass_fields = [i for i, f in enumerate(plan.fields)
-                            if split_swap(f)[1].startswith("m/")]
-        self.angle_fields = [i for i, f in enumerate(plan.fields)
-                             if not split_swap(f)[1].startswith("m/")]
+        # FP64 rows: invariant masses and the event charge; the rest are angles
+        fp64 = [split_swap(f)[1].startswith("m/") or i == plan.charge_index
+                for i, f in enumerate(plan.fields)]
+        self.mass_fields = [i for i, f in enumerate(fp64) if f]
+        self.angle_fields = [i for i, f in enumerate(fp64) if not f]
+        # charge < 0 events reverse the helicity couplings of the vertices
+        # that allow it (tf_pwa/amp/core.py:938-945)
+        self.flips = plan.charge_index is not None
         # evaluation passes: the unswapped fields, then one per identical-
         # particle swap (its fields, sign and helicity-axis order)
         self.npass = 1 + len(plan.swaps)
@@ -158,6 +162,7 @@ class ModelCode:
         for ci, c in enumerate(self.group):
             parts = [c.top] + c.inner + list(c.outs)
             cgs = [d.cg() for d in c]
+            cgs_cc = [self._cg_cc(d) for d in c]
             rows = []
             for hel in itertools.product(*[p.spins for p in parts]):
                 hmap = dict(zip(parts, hel))
@@ -178,11 +183,13 @@ class ModelCode:
                 coefs = {}
                 for k in self.chain_columns[ci]:
                     lsi = self.columns[k][1]
-                    cf = 1.0
+                    cf, cfc = 1.0, 1.0
                     for (vi, _, _, ib, ic) in facs:
                         cf *= cgs[vi][lsi[vi], ib, ic]
-                    if cf != 0.0:
-                        coefs[k] = cf
+                        cfc *= cgs_cc[vi][lsi[vi], ib, ic]
+                    if cf != 0.0 or cfc != 0.0:
+                        # a number, or (charge > 0, charge < 0) values
+                        coefs[k] = cf if cf == cfc else (cf, cfc)
                 if coefs:
                     rows.append((tuple(facs), pre_out, coefs))
             self.chain_assign.append(rows)
@@ -230,6 +237,22 @@ class ModelCode:
 
     def _cpx(self, base):
         return f"cmk<R>({self._cst(base + '.re')}, {self._cst(base + '.im')})"
+
+    def _cg_cc(self, d):
+        """CG table of vertex d for charge < 0 events: both daughter
+        helicity axes reversed where the vertex allows it."""
+        cg = d.cg()
+        if self.flips and getattr(d, "allow_cc", False):
+            return cg[:, ::-1, ::-1]
+        return cg
+
+    @staticmethod
+    def _coef(v):
+        """Literal of a coupling coefficient; a (charge > 0, charge < 0)
+        pair becomes a per-event select on ``cc``."""
+        if isinstance(v, tuple):
+            return f"(cc ? {_lit(v[1])} : {_lit(v[0])})"
+        return _lit(v)
 
     def _cf(self, ci):
         """Field references of chain ci in the current pass."""
@@ -289,6 +312,8 @@ class ModelCode:
         for f in self.angle_fields:
             a = f"XA + (long long){self.angle_slot[f]} * ld + i"
             e(f"  const R xa{f} = LDG ? __ldg({a}) : *({a});")
+        if self.flips:
+            e(f"  const bool cc = xm{self.plan.charge_index} < 0.0;")
 
     def _trig(self, e, ci, key, angle):
         """sin/cos of half an angle: computed (and stashed in the forward
@@ -497,10 +522,14 @@ class ModelCode:
             for vi, d in enumerate(c):
                 b, cc = d.outs
                 cg = d.cg()
+                cgc = self._cg_cc(d)
                 ls = d.get_ls_list()
                 for ib in range(len(b.spins)):
                     for ic in range(len(cc.spins)):
-                        terms = [(i, cg[i, ib, ic]) for i in range(len(ls)) if cg[i, ib, ic] != 0]
+                        terms = [(i, cg[i, ib, ic] if cg[i, ib, ic] == cgc[i, ib, ic]
+                                  else (cg[i, ib, ic], cgc[i, ib, ic]))
+                                 for i in range(len(ls))
+                                 if cg[i, ib, ic] != 0 or cgc[i, ib, ic] != 0]
                         if not terms:
                             continue
                         nm = f"H_c{ci}v{vi}_{ib}_{ic}"
@@ -509,7 +538,7 @@ class ModelCode:
                         for i, cgv in terms:
                             l = ls[i][0]
                             bfv = f"bf_c{ci}v{vi}_{l} * " if d.has_barrier_factor else ""
-                            e(f"  cfma({nm}, {bfv}{_lit(cgv)}, {self._cpx(f'{d}.g{i}')});")
+                            e(f"  cfma({nm}, {bfv}{self._coef(cgv)}, {self._cpx(f'{d}.g{i}')});")
             pre = {}
             for facs, po, coefs in self.chain_assign[ci]:
                 if any((vi, ib, ic) not in hnames for (vi, _, _, ib, ic) in facs):
@@ -599,7 +628,7 @@ class ModelCode:
                     prod = f"cmul({prod}, {dn})"
                 e(f"  {{ const cpx<R> rr = cmul({prod}, {cur[po]});")
                 for k, cfv in coefs.items():
-                    e(f"    cfma(Gk{k}, {_lit(cfv)}, rr);")
+                    e(f"    cfma(Gk{k}, {self._coef(cfv)}, rr);")
                 e("  }")
             for k in cols:
                 e(f"  {{ const cpx<R> g = cmul(cscale(BW_c{ci}, {self._scale_k(ci, k)}), Gk{k});")
@@ -656,7 +685,7 @@ class ModelCode:
                         nm = self._pre_name(ci, po, "Fp")
                         pre[po] = nm
                         e(f"  cpx<R> {nm} = cmk<R>(R(0), R(0));")
-                    e(f"  cfma({nm}, {_lit(coefs[k])}, {prod});")
+                    e(f"  cfma({nm}, {self._coef(coefs[k])}, {prod});")
                 cur = self._emit_align_forward(e, ci, pre, "Fa")
                 e(f"  const cpx<R> S = cscale(BW_c{ci}, {self._scale_k(ci, k)});")
                 for o, nm in cur.items():

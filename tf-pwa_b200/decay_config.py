@@ -253,7 +253,11 @@ class DecayConfig:
         if not chains:
             raise RuntimeError("no decay chain available, check the config")
         if self.data_config.get("cp_trans", True):
-            pass  # charge-conjugation flips are disabled (decay_config.py:423-427)
+            # charge < 0 events are parity-transformed instead of flipping the
+            # helicity couplings (tf_pwa/config_loader/decay_config.py:93-94,423-427)
+            for c in chains:
+                for d in c:
+                    d.allow_cc = False
         group = DecayGroup(chains)
         # data.identical_particles: lists of final particles whose momenta are
         # symmetrised; data.cp_particles: charge-conjugate final pairs of a
@@ -264,6 +268,12 @@ class DecayConfig:
         cp = self.data_config.get("cp_particles")
         if cp:
             group.cp_particles = [[str(x) for x in pr] for pr in cp]
+        # per-event charges (``<idx>_charge`` files, or use_charge: true):
+        # tf_pwa/config_loader/data.py:73-76,92,163-167
+        dk = self.data_config
+        group.charge = bool(dk.get("use_charge")) or any(
+            str(k).endswith("_charge") for k in dk)
+        group.cp_trans = bool(dk.get("cp_trans", True))
         return group
 
 

@@ -727,17 +727,30 @@ class Engine:
         return nll.value, g, H
 
     # ------------------------------------------------------------ dataset step
-    def fields_from_p4(self, p4):
+    def fields_from_p4(self, p4, charge=None):
         """Event fields (n_fields, N) on the device from final-state momenta
-        ``p4``: CUDA tensor (N, n_final, 4), finals in the plan's order."""
+        ``p4``: CUDA tensor (N, n_final, 4), finals in the plan's order.
+        For data with charges, ``charge`` (default all +1) fills the charge
+        field, or with cp_trans parity-transforms the charge < 0 events first
+        (``tf_pwa/cal_angle.py:569-573``)."""
         import torch
 
         n = p4.shape[0]
-        soa = p4.to(torch.float64).permute(1, 2, 0).reshape(-1, n).contiguous()
+        p4 = p4.to(torch.float64)
+        ci = self.plan.charge_index
+        ch = None
+        if self.plan.use_charge and charge is not None:
+            ch = torch.as_tensor(charge, dtype=torch.float64, device=p4.device)
+            if self.plan.cp_trans:
+                sgn = torch.where(ch > 0, 1.0, -1.0).to(torch.float64)[:, None, None]
+                p4 = torch.cat([p4[:, :, :1], p4[:, :, 1:] * sgn], 2)
+        soa = p4.permute(1, 2, 0).reshape(-1, n).contiguous()
         out = torch.empty((self.plan.n_fields, n), dtype=torch.float64, device=p4.device)
         self._check(load_library().pwa_fields_from_p4(self.h, soa.data_ptr(), n, n,
                                                       out.data_ptr(), n, 0),
                     "pwa_fields_from_p4")
+        if ch is not None and ci is not None:
+            out[ci] = ch
         return out
 
     def toy_select(self, C, seed, first, n, fmax, flat, out):

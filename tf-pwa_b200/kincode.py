@@ -175,6 +175,11 @@ class KinCode:
             all_frames.append(build_frames(pe))
         # the plan's fields
         for fi, full_name in enumerate(plan.fields):
+            if fi == plan.charge_index:
+                # the event's charge is data, not kinematics: +1 here (the
+                # generator's events), overwritten by the caller's charges
+                e(f"  F[{fi}] = 1.0;")
+                continue
             sk, fname = split_swap(full_name)
             frames = all_frames[sk]
             parts = fname.split("/")

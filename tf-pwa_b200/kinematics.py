@@ -191,15 +191,25 @@ def _chain_frames(chain_topo, mom):
     return angles, rmat, bmat
 
 
-def event_fields(plan, p4, device=None):
+def event_fields(plan, p4, device=None, charge=None):
     """(n_fields, N) FP64 event columns in plan order from final-state
     momenta ``p4`` = {final particle name: (N, 4) array or tensor} in the
     parent rest frame.  Returns a tensor on ``device`` (default: the input's
-    device, CPU for numpy input)."""
+    device, CPU for numpy input).  For data with charges, ``charge``
+    (default all +1) fills the charge field, or with cp_trans parity-
+    transforms the charge < 0 events first."""
     p4 = {k: torch.as_tensor(v, dtype=torch.float64, device=device) for k, v in p4.items()}
     n = next(iter(p4.values())).shape[0]
     dev = next(iter(p4.values())).device
     out = torch.zeros((plan.n_fields, n), dtype=torch.float64, device=dev)
+    if plan.use_charge:
+        ch = torch.ones(n, dtype=torch.float64, device=dev) if charge is None else \
+            torch.as_tensor(charge, dtype=torch.float64, device=dev)
+        if plan.charge_index is not None:
+            out[plan.charge_index] = ch
+        if plan.cp_trans:
+            sgn = torch.where(ch > 0, 1.0, -1.0).to(torch.float64)[:, None]
+            p4 = {k: torch.cat([v[:, :1], v[:, 1:] * sgn], 1) for k, v in p4.items()}
 
     def topo_frames(mom4):
         frames = []
@@ -227,6 +237,8 @@ def event_fields(plan, p4, device=None):
             moved = {k: neg(v) for k, v in moved.items()}
         all_frames.append(topo_frames(moved))
     for fi, full_name in enumerate(plan.fields):
+        if fi == plan.charge_index:
+            continue
         sk, fname = split_swap(full_name)
         frames = all_frames[sk]
         parts = fname.split("/")

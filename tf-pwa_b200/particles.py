@@ -293,6 +293,9 @@ class Decay:
         ls_sel = kw.pop("ls_list", None)
         self.ls_sel = None if ls_sel is None else tuple(tuple(i) for i in ls_sel)
         self.params_polar = kw.pop("params_polar", None)
+        # per-event charge conjugation flips this vertex's helicity coupling
+        # (tf_pwa/amp/core.py:697-716,938-945)
+        self.allow_cc = kw.pop("allow_cc", True)
         kw.pop("model", None)
         kw.pop("curve_style", None)
         for k in ("below_threshold", "barrier_factor_mass", "force_min_l", "aligned",
@@ -413,6 +416,8 @@ class DecayGroup:
         self.chains = list(chains)
         self.identical_particles = None
         self.cp_particles = None
+        self.charge = False       # per-event charge_conjugation field in use
+        self.cp_trans = True      # parity-transform charge < 0 momenta
         self.top = self.chains[0].top
         self.outs = sorted(self.chains[0].outs)
         for c in self.chains:

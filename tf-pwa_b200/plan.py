@@ -7,7 +7,12 @@ one per-event quantity produced once per dataset by the kinematics step:
 * ``<t>/<decay>/<particle>/{alpha,beta,gamma}``: helicity angles of a
   particle in its mother's frame, for topology ``t``;
 * ``<t>/<decay>/<final>/aligned/{alpha,beta,gamma}``: Wigner alignment
-  angles of a final particle with spin in a non-reference chain.
+  angles of a final particle with spin in a non-reference chain;
+* ``charge``: the event's charge_conjugation (+1 / -1), when the data carry
+  charges and ``cp_trans`` is off: charge -1 events flip the helicity
+  couplings of the vertices that allow it (``tf_pwa/amp/core.py:938-945``).
+  With ``cp_trans`` (the default) charge -1 events are parity-transformed
+  before the angles are computed instead (``tf_pwa/cal_angle.py:569-573``).
 
 With identical final particles (``data.identical_particles``), every
 non-identity permutation of them adds a "swap": the same fields computed
@@ -83,6 +88,14 @@ class Plan:
         self._prefix = ""
         self.align_ref = self._alignment_reference()
         self.chains = [self._chain_fields(i, c) for i, c in enumerate(group)]
+        # per-event charge_conjugation (+1 / -1) when the data carry charges:
+        # with cp_trans, charge < 0 momenta are parity-transformed before the
+        # angles; otherwise the charge is a field that flips the helicity
+        # couplings of the vertices that allow it
+        self.use_charge = bool(getattr(group, "charge", False))
+        self.cp_trans = getattr(group, "cp_trans", True)
+        flips = any(getattr(d, "allow_cc", False) for c in group for d in c)
+        self.charge_index = self.field("charge") if self.use_charge and flips else None
         self.swaps = []
         for k, sw in enumerate(pass_specs(group, getattr(group, "identical_particles", None),
                                           getattr(group, "cp_particles", None))):
