@@ -379,9 +379,32 @@ class OracleModel:
             a = a + sw["factor"] * b
         return a
 
+    def density(self, vals):
+        """Spin density matrix of a vector-polarised parent
+        (``tf_pwa/amp/core.py:1965-2000``), None when unpolarised."""
+        top = self.group.top
+        if getattr(top, "polarization", "none") == "none":
+            return None
+        h = str(top)
+        if top.J == 0.5:
+            px, py, pz = (vals[f"{h}_polarization_p{c}"] for c in "xyz")
+            return 0.5 * np.array([[1 + pz, px - 1j * py], [px + 1j * py, 1 - pz]])
+        p = [vals[f"{h}_polarization_p_{i}"] for i in range(8)]
+        r3 = np.sqrt(3.0)
+        return np.array([
+            [1 + p[2] + p[7] / r3, p[0] - 1j * p[1], p[3] - 1j * p[4]],
+            [p[0] + 1j * p[1], 1 - p[2] + p[7] / r3, p[5] - 1j * p[6]],
+            [p[3] + 1j * p[4], p[5] + 1j * p[6], 1 - 2 * p[7] / r3]])
+
     def pdf(self, x, vals, polar=None):
+        """sum |A|^2, or sum_l A_al rho_ab A_bl^* for a polarised parent
+        (``tf_pwa/amp/core.py:1919-1951``)."""
         a = self.amp(x, vals, polar)
-        return np.sum(np.abs(a.reshape(a.shape[0], -1)) ** 2, axis=1)
+        rho = self.density(vals)
+        if rho is None:
+            return np.sum(np.abs(a.reshape(a.shape[0], -1)) ** 2, axis=1)
+        a = a.reshape(a.shape[0], a.shape[1], -1)
+        return np.real(np.einsum("nal,ab,nbl->n", a, rho, np.conj(a)))
 
 
 # ----------------------------------------------------------- NLL
@@ -441,6 +464,17 @@ class OracleNLL:
         wm = self.wm / self.wm.sum()
         sw = self.wd.sum()
         I = np.sum(wm * fm0)
+        # df = 2 Re sum S dA with S = conj(A), or sum_b rho_ab conj(A_b) when
+        # the parent is polarised
+        rho = self.m.density(v0)
+
+        def seed(A):
+            if rho is None:
+                return np.conj(A)
+            a = A.reshape(A.shape[0], rho.shape[0], -1)
+            return np.einsum("ab,nbl->nal", rho, np.conj(a)).reshape(A.shape)
+
+        Sd, Sm = seed(Ad), seed(Am)
         dclip = np.where(fd0 > _EPS_CLIP, 1.0 / np.where(fd0 > _EPS_CLIP, fd0, 1.0),
                          1.0 / _EPS_CLIP - (fd0 - _EPS_CLIP) / _EPS_CLIP ** 2)
         for k, n in enumerate(self.names):
@@ -463,8 +497,8 @@ class OracleNLL:
                 v2[base + "r"], v2[base + "i"] = (0.0, 0.0)
                 Bd = (self.m.amp(self.xd, v1, self.polar) - self.m.amp(self.xd, v2, self.polar)).reshape(Ad.shape)
                 Bm = (self.m.amp(self.xm, v1, self.polar) - self.m.amp(self.xm, v2, self.polar)).reshape(Am.shape)
-                dfd = 2 * np.real(np.sum(np.conj(Ad) * Bd * dc, axis=1))
-                dfm = 2 * np.real(np.sum(np.conj(Am) * Bm * dc, axis=1))
+                dfd = 2 * np.real(np.sum(Sd * Bd * dc, axis=1))
+                dfm = 2 * np.real(np.sum(Sm * Bm * dc, axis=1))
                 g[k] = -np.sum(self.wd * dclip * dfd) + sw * np.sum(wm * dfm) / I
             else:
                 # 4-point central differences at h and h/2, Richardson-combined

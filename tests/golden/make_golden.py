@@ -47,6 +47,7 @@ CASES = {
     "epem_cp": ("epem_cp.yml", 300, 0, 1200, 19, False, {}),
     "lc2pkpi_cc": ("lc2pkpi_cc.yml", 400, 0, 1500, 20, False, {}),
     "b2dstkpi_cc": ("b2dstkpi_cc.yml", 400, 0, 1500, 21, False, {}),
+    "lc2pkpi_pol": ("lc2pkpi_pol.yml", 400, 0, 1500, 22, False, {}),
 }
 
 
@@ -122,6 +123,8 @@ def main(ref_root):
                 params[k] = float(rng.uniform(0.5, 2.0))
             elif k.endswith("i") and ("_g_ls_" in k or "_total_" in k):
                 params[k] = float(rng.uniform(-np.pi, np.pi))
+            elif "_polarization_" in k:
+                params[k] = float(rng.uniform(-0.4, 0.4))
             else:
                 params[k] = float(vm.get(k)) * float(rng.uniform(0.97, 1.03))
         vm.set_all(params)

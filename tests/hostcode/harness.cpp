@@ -20,8 +20,7 @@ static void sums_t(const Consts& C, const R* XA, const double* XM, const double*
   for (long long i = beg; i < end; ++i) {
     cpx<R> A[PWA_NOUT];
     model_amp<R, STASH, false>(C, XA, XM, ld, i, A, st);
-    double f = 0.0;
-    for (int o = 0; o < PWA_NOUT; ++o) f += double(cabs2(A[o]));
+    const double f = model_f<R>(C, A);
     const double w = W[i];
     double fac;
     if (is_data) {
@@ -34,8 +33,7 @@ static void sums_t(const Consts& C, const R* XA, const double* XM, const double*
       fac = w;
     }
     cpx<R> Ab[PWA_NOUT];
-    for (int o = 0; o < PWA_NOUT; ++o)
-      Ab[o] = cmk<R>(R(fac * double(A[o].re)), R(-fac * double(A[o].im)));
+    model_seed<R>(C, A, fac, Ab, acc + 1 + 2 * PWA_NCOL + PWA_NSHAPE);
     if (STASH)
       model_adj_stash<R, false>(C, XA, XM, ld, i, Ab, acc + 1, acc + 1 + 2 * PWA_NCOL, st);
     else
@@ -156,9 +154,7 @@ extern "C" int hx_toy(const double* Cv, unsigned long long seed, long long first
     }
     cpx<double> A[PWA_NOUT];
     model_amp<double, false, false>(C, sXA, sXM, 1, 0, A, nullptr);
-    double f = 0.0;
-    for (int o = 0; o < PWA_NOUT; ++o) f += cabs2(A[o]);
-    f_out[i] = f;
+    f_out[i] = model_f<double>(C, A);
     for (int fi = 0; fi < PWA_NFIN; ++fi) {
       P4[(4LL * fi) * n + i] = P[fi].t;
       P4[(4LL * fi + 1) * n + i] = P[fi].x;

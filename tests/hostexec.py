@@ -92,7 +92,17 @@ class HostModel:
         return (out[0::2] + 1j * out[1::2]).reshape(n, self.code.nout)
 
     def pdf(self, C, x, f32=False):
-        return np.sum(np.abs(self.amp(C, x, f32)) ** 2, axis=1)
+        """sum |A|^2, or with a polarised parent sum_l A_al rho_ab A_bl^*
+        with rho taken from the constant block."""
+        a = self.amp(C, x, f32)
+        c = self.code
+        if not c.pol_names:
+            return np.sum(np.abs(a) ** 2, axis=1)
+        na = c.na
+        rho = np.array([[C[c.consts.index[f"rho{i}_{j}.re"]] + 1j * C[c.consts.index[f"rho{i}_{j}.im"]]
+                         for j in range(na)] for i in range(na)])
+        a = a.reshape(a.shape[0], na, -1)
+        return np.real(np.einsum("nal,ab,nbl->n", a, rho, np.conj(a)))
 
     def columns(self, C, x):
         C = np.ascontiguousarray(C, np.float64)

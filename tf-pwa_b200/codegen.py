@@ -26,6 +26,7 @@ mathematics is the reference's chain contraction
 """
 import itertools
 
+from .decay_config import polarization_names
 from .kincode import KinCode
 from .plan import split_swap
 from .particles import bprime_coeff, small_d_weight, two
@@ -150,8 +151,18 @@ class ModelCode:
                 self.consts.add(f"{p}.kappa_m")
                 self.consts.add(f"{p}.inv_g0")
         self.nshape = 2 * len(self.shape_res)
+        # polarised parent: density matrix rho (constants) and the sums of
+        # the parent-helicity products T_ab for its gradient
+        self.pol_names = polarization_names(group)
+        self.na = len(group.top.spins)
+        self.nrho = 2 * self.na * self.na if self.pol_names else 0
+        if self.pol_names:
+            for a in range(self.na):
+                for b in range(self.na):
+                    self.consts.add(f"rho{a}_{b}.re")
+                    self.consts.add(f"rho{a}_{b}.im")
         self.ncol = len(self.columns)
-        self.nacc = 1 + 2 * self.ncol + self.nshape
+        self.nacc = 1 + 2 * self.ncol + self.nshape + self.nrho
         self._analyse()
 
     # ------------------------------------------------------------ analysis
@@ -697,6 +708,63 @@ class ModelCode:
                 e("  }")
             e("  }")
 
+    # ------------------------------------------------------------ |A|^2
+    def _pdf_source(self):
+        """``model_f``: sum |A|^2 (``tf_pwa/amp/core.py:1919-1931``) or, for a
+        polarised parent, sum_l sum_ab Re A_al rho_ab A_bl^* (core.py:
+        1933-1951); ``model_seed``: the adjoint seed dF/dA times fac and, when
+        polarised, the sums T_ab += fac sum_l A_al A_bl^* (accr)."""
+        L = ["template <typename R>",
+             "__device__ __forceinline__ double model_f(const Consts& C, const cpx<R>* A) {",
+             "  double f = 0.0;"]
+        if not self.pol_names:
+            L += [f"  f += double(cabs2(A[{o}]));" for o in range(self.nout)]
+        else:
+            na, nl = self.na, self.nout // self.na
+            for a in range(na):
+                for b in range(na):
+                    re, im = self.consts.index[f"rho{a}_{b}.re"], self.consts.index[f"rho{a}_{b}.im"]
+                    for li in range(nl):
+                        x, y = a * nl + li, b * nl + li
+                        # Re(u rho), u = A_x conj(A_y)
+                        L.append(f"  f += C.v[{re}] * (double(A[{x}].re) * double(A[{y}].re) + "
+                                 f"double(A[{x}].im) * double(A[{y}].im)) - C.v[{im}] * "
+                                 f"(double(A[{x}].im) * double(A[{y}].re) - "
+                                 f"double(A[{x}].re) * double(A[{y}].im));")
+        L += ["  return f;", "}", "",
+              "template <typename R>",
+              "__device__ __forceinline__ void model_seed(const Consts& C, const cpx<R>* A, "
+              "double fac, cpx<R>* Ab, double* accr) {"]
+        if not self.pol_names:
+            L += [f"  Ab[{o}] = cmk<R>(R(fac * double(A[{o}].re)), R(-fac * double(A[{o}].im)));"
+                  for o in range(self.nout)]
+        else:
+            na, nl = self.na, self.nout // self.na
+            for a in range(na):
+                for li in range(nl):
+                    x = a * nl + li
+                    L.append(f"  {{ double sr = 0.0, si = 0.0;  // sum_b rho_ab conj(A_b)")
+                    for b in range(na):
+                        y = b * nl + li
+                        re, im = self.consts.index[f"rho{a}_{b}.re"], self.consts.index[f"rho{a}_{b}.im"]
+                        L.append(f"    sr += C.v[{re}] * double(A[{y}].re) + C.v[{im}] * double(A[{y}].im);")
+                        L.append(f"    si += C.v[{im}] * double(A[{y}].re) - C.v[{re}] * double(A[{y}].im);")
+                    L.append(f"    Ab[{x}] = cmk<R>(R(fac * sr), R(fac * si)); }}")
+            for a in range(na):
+                for b in range(na):
+                    j = 2 * (a * na + b)
+                    terms_r, terms_i = [], []
+                    for li in range(nl):
+                        x, y = a * nl + li, b * nl + li
+                        terms_r.append(f"double(A[{x}].re) * double(A[{y}].re) + "
+                                       f"double(A[{x}].im) * double(A[{y}].im)")
+                        terms_i.append(f"double(A[{x}].im) * double(A[{y}].re) - "
+                                       f"double(A[{x}].re) * double(A[{y}].im)")
+                    L.append(f"  accr[{j}] += fac * ({' + '.join(terms_r)});")
+                    L.append(f"  accr[{j + 1}] += fac * ({' + '.join(terms_i)});")
+        L += ["}", ""]
+        return "\n".join(L)
+
     # ------------------------------------------------------------ emission
     def source(self):
         L = [_HEADER.format(ncol=self.ncol, nout=self.nout, nshape=self.nshape, nacc=self.nacc,
@@ -742,6 +810,7 @@ class ModelCode:
                  "    cpx<R>* __restrict__ F) {")
         L += body
         L.append("}\n")
+        L.append(self._pdf_source())
         fl = sorted(self._fset)
         L.append(f"#define PWA_NF {self.nf}")
         L.append("__device__ constexpr int pwa_fk[PWA_NF] = {" + ", ".join(str(k) for k, _ in fl) + "};")

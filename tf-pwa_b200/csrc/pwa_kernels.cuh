@@ -52,9 +52,7 @@ __device__ __forceinline__ void eval_body(const Consts& C, const R* __restrict__
 #else
     model_amp<R, false>(C, XA, XM, ld, i, A, nullptr);
 #endif
-    double f = 0.0;
-#pragma unroll
-    for (int o = 0; o < PWA_NOUT; ++o) f += double(cabs2(A[o]));
+    const double f = model_f<R>(C, A);
     const double w = __ldg(W + i);
     double fac;
     if (is_data) {
@@ -67,8 +65,7 @@ __device__ __forceinline__ void eval_body(const Consts& C, const R* __restrict__
       fac = w;
     }
     cpx<R> Ab[PWA_NOUT];
-#pragma unroll
-    for (int o = 0; o < PWA_NOUT; ++o) Ab[o] = cmk<R>(R(fac * double(A[o].re)), R(-fac * double(A[o].im)));
+    model_seed<R>(C, A, fac, Ab, acc + 1 + 2 * PWA_NCOL + PWA_NSHAPE);
 #if PWA_USE_STASH
     model_adj_stash<R>(C, XA, XM, ld, i, Ab, acc + 1, acc + 1 + 2 * PWA_NCOL, st);
 #else
@@ -132,10 +129,7 @@ __device__ __forceinline__ void pdf_body(const Consts& C, const R* __restrict__ 
        i += (long long)gridDim.x * blockDim.x) {
     cpx<R> A[PWA_NOUT];
     model_amp<R, false>(C, XA, XM, ld, i, A, nullptr);
-    double f = 0.0;
-#pragma unroll
-    for (int o = 0; o < PWA_NOUT; ++o) f += double(cabs2(A[o]));
-    out[i - beg] = f;
+    out[i - beg] = model_f<R>(C, A);
   }
 }
 
@@ -1045,9 +1039,7 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB)
           (pwa_field_mass[j] ? sXM : sXA)[pwa_field_slot[j] * PWA_TPB + tid] = F[j];
         cpx<double> A[PWA_NOUT];
         model_amp<double, false, false>(C, sXA, sXM, PWA_TPB, tid, A, nullptr);
-        double f = 0.0;
-#pragma unroll
-        for (int o = 0; o < PWA_NOUT; ++o) f += cabs2(A[o]);
+        const double f = model_f<double>(C, A);
         res = (fmax <= 0.0 || U[PWA_NDRAW - 1] * fmax < f) ? f : -1.0;
       }
     }

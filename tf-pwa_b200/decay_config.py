@@ -277,6 +277,23 @@ class DecayConfig:
         return group
 
 
+def polarization_names(group):
+    """Real parameters of the parent's polarisation: px, py, pz for spin
+    1/2, eight components for spin 1 (``tf_pwa/amp/core.py:1660-1671``)."""
+    top = group.top
+    pol = getattr(top, "polarization", "none")
+    if pol == "none":
+        return []
+    if pol != "vector":
+        raise NotImplementedError(f"polarization {pol!r}")
+    head = var_name(str(top))
+    if top.J == 0.5:
+        return [f"{head}_polarization_p{a}" for a in ("x", "y", "z")]
+    if top.J == 1:
+        return [f"{head}_polarization_p_{i}" for i in range(8)]
+    raise NotImplementedError("vector polarisation of a parent with spin other than 1/2 or 1")
+
+
 def init_params(group, vm, constrains=None):
     """Create the fit parameters of the group in the reference order."""
     constrains = constrains or {}
@@ -310,6 +327,10 @@ def init_params(group, vm, constrains=None):
             vm.set_fix(lst[0] + "r", 1.0)
             vm.set_fix(lst[0] + "i", 0.0)
             names["g_ls"][d] = lst
+    # polarisation vector of the parent (core.py:1660-1671)
+    names["polarization"] = polarization_names(group)
+    for n in names["polarization"]:
+        vm.add_real_var(n)
     # decay constraints: fix one chain total (config_loader.py:358-366)
     dic = (constrains.get("decay") or {})
     fix_idx = dic.get("fix_chain_idx", 0)

@@ -129,6 +129,34 @@ def poly(l, z):
     return r
 
 
+def density_matrix(J, p):
+    """(rho, [d rho / d p_k]) of a vector-polarised parent
+    (``tf_pwa/amp/core.py:1965-2000``): spin 1/2, rho = (1 + p . sigma) / 2;
+    spin 1, rho = 1 + sum_k p_k G_k with the eight Hermitian generators G_k
+    of the reference (in the parent's helicity order)."""
+    p = np.asarray(p, np.float64)
+    if J == 0.5:
+        px, py, pz = p
+        rho = 0.5 * np.array([[1 + pz, px - 1j * py], [px + 1j * py, 1 - pz]])
+        d = [0.5 * np.array([[0, 1], [1, 0]], complex),
+             0.5 * np.array([[0, -1j], [1j, 0]]),
+             0.5 * np.array([[1, 0], [0, -1]], complex)]
+        return rho, d
+    if J == 1:
+        s3 = 1.0 / np.sqrt(3.0)
+        G = np.zeros((8, 3, 3), complex)
+        G[0][0, 1], G[0][1, 0] = 1, 1
+        G[1][0, 1], G[1][1, 0] = -1j, 1j
+        G[2][0, 0], G[2][1, 1] = 1, -1
+        G[3][0, 2], G[3][2, 0] = 1, 1
+        G[4][0, 2], G[4][2, 0] = -1j, 1j
+        G[5][1, 2], G[5][2, 1] = 1, 1
+        G[6][1, 2], G[6][2, 1] = -1j, 1j
+        G[7] = np.diag([s3, s3, -2 * s3])
+        return np.eye(3) + np.tensordot(p, G, 1), list(G)
+    raise NotImplementedError("vector polarisation of a parent with spin other than 1/2 or 1")
+
+
 def combine_pieces(vec, P):
     """NLL and gradient from the summed piece vector of
     :meth:`Engine.local_pieces` (model.py:433-449):
@@ -168,7 +196,8 @@ class Engine:
         h = ctypes.c_void_p()
         src = self.src.encode()
         rc = lib.pwa_plan_create(src, len(src), len(c.mass_fields), len(c.angle_fields), c.ncol,
-                                 c.nout, c.nshape, len(c.consts), c.nf, self.tpb, ctypes.byref(h))
+                                 c.nout, c.nshape + c.nrho, len(c.consts), c.nf, self.tpb,
+                                 ctypes.byref(h))
         if rc != 0:
             msg = lib.pwa_last_error(h).decode(errors="replace")
             lib.pwa_plan_destroy(h)
@@ -335,6 +364,13 @@ class Engine:
             self._vtx_slots.append((d, self._vertex_chain[d.key()], sl))
         self._shape_slots = [(p, cidx[f"{p}.kappa_m"], cidx[f"{p}.inv_g0"])
                              for p in self.code.shape_res]
+        self._pol_names = list(self.code.pol_names)
+        self._pol_index = {n: i for i, n in enumerate(self._pol_names)}
+        if self._pol_names:
+            na = self.code.na
+            self._rho_re = np.array([cidx[f"rho{a}_{b}.re"] for a in range(na) for b in range(na)])
+            self._rho_im = np.array([cidx[f"rho{a}_{b}.im"] for a in range(na) for b in range(na)])
+            _, self._drho = density_matrix(self.group.top.J, np.zeros(len(self._pol_names)))
         self._mass_names = {f"{p.params_head}_mass": p for p in self.group.resonances}
         self._width_names = {f"{p.params_head}_width": p for p in self.group.resonances}
 
@@ -414,10 +450,20 @@ class Engine:
             C[1:2 * c.ncol:2] = self._ck.imag
             C[self._vg_re] = z[self._vg_src].real
             C[self._vg_im] = z[self._vg_src].imag
+            self._fill_rho(C, vals)
             return C
         C = self._consts_full(vals)
         self._shape_cache = (key, C.copy())
+        self._fill_rho(C, vals)
         return C
+
+    def _fill_rho(self, C, vals):
+        """Parent spin density matrix (polarised models) into its slots."""
+        if not self._pol_names:
+            return
+        rho, _ = density_matrix(self.group.top.J, [vals[n] for n in self._pol_names])
+        C[self._rho_re] = rho.real.reshape(-1)
+        C[self._rho_im] = rho.imag.reshape(-1)
 
     def _consts_full(self, vals):
         c = self.code
@@ -502,7 +548,7 @@ class Engine:
         c = self.code
         P = len(names)
         J = np.zeros((P, c.ncol), np.complex128)
-        D = np.zeros((P, max(c.nshape, 1)))
+        D = np.zeros((P, max(c.nshape + c.nrho, 1)))
         cv = self._cv
         key = (tuple(names), self._shape_key(vals) if hasattr(self, "_shape_names") else None)
         cached = self._jac_cache.get(key)
@@ -517,6 +563,13 @@ class Engine:
         else:
             names_left = list(enumerate(names))
         for pi, n in names_left:
+            if n in self._pol_index:
+                # polarisation: d f / d p = Re sum_ab T_ab d rho_ab / d p, T_ab
+                # the (a, b) parent-helicity product sums after the shape sums
+                dr = self._drho[self._pol_index[n]]
+                D[pi, c.nshape:c.nshape + c.nrho:2] = dr.real.reshape(-1)
+                D[pi, c.nshape + 1:c.nshape + c.nrho:2] = -dr.imag.reshape(-1)
+                continue
             base = n[:-1]
             if base in cv:
                 r, ph = vals[base + "r"], vals[base + "i"]
@@ -605,6 +658,8 @@ class Engine:
                                                     stream or 0), "pwa_eval_enqueue")
 
     def build_gram(self, C, stream=None):
+        if self.code.nrho:
+            raise PWAError("the column cache / Gram form does not apply to a polarised parent")
         K = self.code.ncol
         out = np.zeros(2 * K * K)
         C = np.ascontiguousarray(C, np.float64)
@@ -647,7 +702,7 @@ class Engine:
         Gm = sm[1:1 + 2 * K:2] + 1j * sm[2:2 + 2 * K:2]
         gd = 2 * np.real(J @ Gd)
         gm = 2 * np.real(J @ Gm)
-        if self.code.nshape:
+        if self.code.nshape + self.code.nrho:
             gd = gd + D @ sd[1 + 2 * K:]
             gm = gm + D @ sm[1 + 2 * K:]
         f = self.mc_share
@@ -687,6 +742,8 @@ class Engine:
             "pwa_set_param_layout")
 
     def cache_data(self, vals):
+        if self.code.nrho:
+            raise PWAError("the column cache / Gram form does not apply to a polarised parent")
         """Evaluate and keep the data events' partial-wave columns."""
         C = np.ascontiguousarray(self.consts(vals))
         self._check(load_library().pwa_cache_data(self.h, _dptr(C), 0), "pwa_cache_data")

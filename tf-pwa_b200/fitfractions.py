@@ -46,7 +46,7 @@ def restricted_integral(eng, vals, names, chains, use_gram):
     _, sm = eng.eval_sums(C, PLAIN_F64, mc=True)
     Gm = sm[1:1 + 2 * K:2] + 1j * sm[2:2 + 2 * K:2]
     g = 2 * np.real(J @ Gm)
-    if code.nshape:
+    if code.nshape + code.nrho:
         g = g + D @ sm[1 + 2 * K:]
     return float(sm[0]), g
 

@@ -227,6 +227,9 @@ class Particle:
         self.width_norm = kw.pop("width_norm", False)
         self.float = kw.pop("float", "")
         self.params = kw.pop("params", None)
+        # "vector": the parent's spin density matrix is fitted
+        # (tf_pwa/amp/core.py:1647-1671,1965-2000)
+        self.polarization = kw.pop("polarization", "none") or "none"
         self.d = 3.0
         self.extra = kw
         self.decay = []      # decays of this particle (config order)
