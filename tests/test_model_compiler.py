@@ -46,3 +46,24 @@ def test_bprime_coefficients():
 
     assert bprime_coeff(2) == [1.0, 3.0, 9.0]
     assert bprime_coeff(5) == [1.0, 15.0, 315.0, 6300.0, 99225.0, 893025.0]
+
+
+def test_unsupported_options_raise():
+    """Options the engine does not compile fail loudly instead of being
+    ignored: CP-violating chain totals, unknown lineshape models."""
+    import os
+
+    from common import CONFIGS
+    from tf_pwa_b200.codegen import ModelCode
+    from tf_pwa_b200.decay_config import DecayConfig, load_yaml
+    from tf_pwa_b200.plan import Plan
+
+    dic = load_yaml(os.path.join(CONFIGS, "d2kpipi.yml"))
+    dic["decay_chain"] = {"$all": {"is_cp": True}}
+    with pytest.raises(NotImplementedError):
+        DecayConfig(dic)
+    dic = load_yaml(os.path.join(CONFIGS, "d2kpipi.yml"))
+    dic["particle"]["R1"]["model"] = "Flatte"
+    dc = DecayConfig(dic)
+    with pytest.raises(NotImplementedError):
+        ModelCode(dc.decay_group, Plan(dc.decay_group))

@@ -258,6 +258,12 @@ class DecayConfig:
             for c in chains:
                 for d in c:
                     d.allow_cc = False
+        # decay_chain options (tf_pwa/config_loader/decay_config.py, the
+        # "decay_chain" section): none is compiled; CP-violating chain totals
+        # (is_cp) change the parameters, so refuse rather than ignore them
+        for key, opts in (self.config.get("decay_chain") or {}).items():
+            if any(v for v in (opts or {}).values()):
+                raise NotImplementedError(f"decay_chain options {opts} for {key}")
         group = DecayGroup(chains)
         # data.identical_particles: lists of final particles whose momenta are
         # symmetrised; data.cp_particles: charge-conjugate final pairs of a
