@@ -50,7 +50,8 @@ def test_bprime_coefficients():
 
 def test_unsupported_options_raise():
     """Options the engine does not compile fail loudly instead of being
-    ignored: CP-violating chain totals, unknown lineshape models."""
+    ignored: CP-violating chain totals, non-default kinematics options,
+    unknown lineshape models."""
     import os
 
     from common import CONFIGS
@@ -60,6 +61,10 @@ def test_unsupported_options_raise():
 
     dic = load_yaml(os.path.join(CONFIGS, "d2kpipi.yml"))
     dic["decay_chain"] = {"$all": {"is_cp": True}}
+    with pytest.raises(NotImplementedError):
+        DecayConfig(dic)
+    dic = load_yaml(os.path.join(CONFIGS, "d2kpipi.yml"))
+    dic["data"]["align_ref"] = "center_mass"
     with pytest.raises(NotImplementedError):
         DecayConfig(dic)
     dic = load_yaml(os.path.join(CONFIGS, "d2kpipi.yml"))

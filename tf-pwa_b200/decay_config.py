@@ -264,6 +264,13 @@ class DecayConfig:
         for key, opts in (self.config.get("decay_chain") or {}).items():
             if any(v for v in (opts or {}).values()):
                 raise NotImplementedError(f"decay_chain options {opts} for {key}")
+        # kinematics options of the reference's preprocessor
+        # (tf_pwa/config_loader/data.py:92-113): only the defaults are built
+        dk = self.data_config
+        for key, default in (("center_mass", False), ("r_boost", True), ("align_ref", None),
+                             ("only_left_angle", False), ("preprocessor", "default")):
+            if dk.get(key, default) != default:
+                raise NotImplementedError(f"data option {key}: {dk.get(key)!r}")
         group = DecayGroup(chains)
         # data.identical_particles: lists of final particles whose momenta are
         # symmetrised; data.cp_particles: charge-conjugate final pairs of a
