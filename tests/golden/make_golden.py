@@ -49,6 +49,7 @@ CASES = {
     "b2dstkpi_cc": ("b2dstkpi_cc.yml", 400, 0, 1500, 21, False, {}),
     "lc2pkpi_pol": ("lc2pkpi_pol.yml", 400, 0, 1500, 22, False, {}),
     "epem_pol": ("epem_pol.yml", 300, 0, 1200, 23, False, {}),
+    "ident3_fermions": ("ident3_fermions.yml", 300, 0, 1200, 24, False, {}),
 }
 
 

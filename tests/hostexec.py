@@ -7,6 +7,8 @@ of ``tests/hostcode/harness.cpp`` around it.  The tests run it on the golden
 events: the code generator's arithmetic (forward amplitude, adjoint,
 columns, kinematics, generator) is checked against the reference's numbers
 on CPU, one event at a time in FP64 (or FP32 where the kernel uses FP32).
+Compiled without optimisation: the straight-line model code builds in
+seconds that way, and x86-64 double arithmetic is the same at any level.
 """
 import ctypes
 import hashlib
@@ -45,7 +47,7 @@ class HostModel:
         if not os.path.exists(so):
             with open(src, "w") as f:
                 f.write(text)
-            r = subprocess.run(["g++", "-std=c++17", "-O1", "-fPIC", "-shared",
+            r = subprocess.run(["g++", "-std=c++17", "-O0", "-fPIC", "-shared",
                                 "-Wno-unknown-pragmas", "-Wno-pragma-once-outside-header",
                                 src, "-o", so + ".tmp"], capture_output=True, text=True)
             if r.returncode != 0:

@@ -8,7 +8,8 @@ from common import load_golden, load_model
 
 
 @pytest.mark.parametrize("name", ["d2kpipi", "lc2pkpi", "toy_vvp", "b2dstkpi", "dp2kpipi_ident",
-                                  "ident_fermions", "epem_cp", "lc2pkpi_cc", "b2dstkpi_cc"])
+                                  "ident_fermions", "epem_cp", "lc2pkpi_cc", "b2dstkpi_cc",
+                                  "ident3_fermions"])
 @pytest.mark.parametrize("kind", ["data", "mc"])
 def test_fields_match_reference_cal_angle(name, kind):
     """(with per-event charges: parity transform of charge -1 momenta under

@@ -7,7 +7,7 @@ from common import load_golden, load_model
 
 CASES = ["d2kpipi", "d2kpipi_float", "lc2pkpi", "toy_vvp", "b2dstkpi", "d2kpipi_shapes",
          "dp2kpipi_ident", "ident_fermions", "epem_cp", "lc2pkpi_cc", "b2dstkpi_cc",
-         "lc2pkpi_pol", "epem_pol"]
+         "lc2pkpi_pol", "epem_pol", "ident3_fermions"]
 
 
 @pytest.mark.parametrize("name", CASES)
