@@ -52,3 +52,29 @@ def test_read_dat_matches_numpy(tmp_path):
     bad.write_text("1.0 2.0 x3\n")
     with pytest.raises(PWAError):
         read_dat(str(bad))
+
+
+def test_argument_errors_without_a_device():
+    """Bad arguments come back as PWA_ERR_ARG with a message, before any
+    device call (so also on a machine without a GPU); calls on a null
+    handle are refused."""
+    import ctypes
+
+    from tf_pwa_b200.engine import load_library
+
+    lib = load_library()
+    h = ctypes.c_void_p()
+    src = b"// empty"
+    # ncol = 0 is invalid
+    rc = lib.pwa_plan_create(src, len(src), 1, 1, 0, 1, 0, 1, 1, 128, ctypes.byref(h))
+    assert rc == 1
+    assert len(lib.pwa_last_error(h)) > 0
+    lib.pwa_plan_destroy(h)
+    # threads per block must be a multiple of 32
+    h = ctypes.c_void_p()
+    rc = lib.pwa_plan_create(src, len(src), 1, 1, 1, 1, 0, 1, 1, 100, ctypes.byref(h))
+    assert rc == 1
+    lib.pwa_plan_destroy(h)
+    out = (ctypes.c_double * 4)()
+    assert lib.pwa_hessian_cached(None, out, 1.0, 1e-3, None, out, out, out) == 1
+    assert lib.pwa_last_error(None)
