@@ -50,7 +50,29 @@ CASES = {
     "lc2pkpi_pol": ("lc2pkpi_pol.yml", 400, 0, 1500, 22, False, {}),
     "epem_pol": ("epem_pol.yml", 300, 0, 1200, 23, False, {}),
     "ident3_fermions": ("ident3_fermions.yml", 300, 0, 1200, 24, False, {}),
+    "lc2pkpi_pol_lab": ("lc2pkpi_pol.yml", 400, 0, 1500, 25, False, {}),
 }
+# cases whose events are boosted out of the parent rest frame: parent
+# momentum (GeV) in a random direction per event (lab-frame input)
+BOOSTED = {"lc2pkpi_pol_lab": 2.0}
+
+
+def boost_events(arr, M, pmag, rng):
+    """(n, n_final, 4) rest-frame momenta boosted so that the parent has
+    momentum ``pmag`` along a random direction per event."""
+    n = arr.shape[0]
+    u = rng.normal(size=(n, 3))
+    u /= np.linalg.norm(u, axis=1, keepdims=True)
+    beta = u * (pmag / np.hypot(M, pmag))
+    b2 = np.sum(beta ** 2, 1)
+    g = 1.0 / np.sqrt(1.0 - b2)
+    out = np.empty_like(arr)
+    for f in range(arr.shape[1]):
+        E, p = arr[:, f, 0], arr[:, f, 1:]
+        bp = np.sum(beta * p, 1)
+        out[:, f, 0] = g * (E + bp)
+        out[:, f, 1:] = p + ((g - 1.0) * bp / b2 + g * E)[:, None] * beta
+    return out
 
 
 def load_pkg():
@@ -94,6 +116,8 @@ def main(ref_root):
                 continue
             ps = generate_phsp(M, masses, n, seed=1000 * seed + kk)
             arr = np.stack(ps, 1)  # (n, n_final, 4)
+            if name in BOOSTED:
+                arr = boost_events(arr, M, BOOSTED[name], rng)
             p4[kind] = arr
             np.savetxt(os.path.join(tmp, kind + ".dat"), arr.reshape(-1, 4), fmt="%.17g")
         dic2 = dict(dic)

@@ -29,7 +29,7 @@ def _engine(cfg, variables=None):
 
 
 @pytest.mark.parametrize("name", ["d2kpipi", "lc2pkpi", "b2dstkpi", "dp2kpipi_ident", "ident_fermions",
-                                  "epem_cp", "lc2pkpi_cc", "b2dstkpi_cc"])
+                                  "epem_cp", "lc2pkpi_cc", "b2dstkpi_cc", "lc2pkpi_pol_lab"])
 def test_fields_from_p4_match_reference(name):
     import torch
 

@@ -28,7 +28,7 @@ from hostexec import HostModel
 
 CASES = ["d2kpipi", "d2kpipi_float", "lc2pkpi", "toy_vvp", "b2dstkpi", "d2kpipi_shapes",
          "dp2kpipi_ident", "ident_fermions", "epem_cp", "lc2pkpi_cc", "b2dstkpi_cc",
-         "lc2pkpi_pol", "epem_pol", "ident3_fermions"]
+         "lc2pkpi_pol", "epem_pol", "ident3_fermions", "lc2pkpi_pol_lab"]
 
 _CACHE = {}
 
@@ -100,7 +100,7 @@ def test_columns_rebuild_amplitude(name, build_dir):
 
 
 @pytest.mark.parametrize("name", ["d2kpipi", "lc2pkpi", "toy_vvp", "b2dstkpi", "dp2kpipi_ident",
-                                  "ident_fermions", "epem_cp"])
+                                  "ident_fermions", "epem_cp", "lc2pkpi_pol_lab"])
 def test_kinematics_match_reference(name, build_dir):
     eng, hm, g, meta, _, _ = _setup(name, build_dir)
     for kind in ("data", "mc"):

@@ -9,11 +9,12 @@ from common import load_golden, load_model
 
 @pytest.mark.parametrize("name", ["d2kpipi", "lc2pkpi", "toy_vvp", "b2dstkpi", "dp2kpipi_ident",
                                   "ident_fermions", "epem_cp", "lc2pkpi_cc", "b2dstkpi_cc",
-                                  "ident3_fermions"])
+                                  "ident3_fermions", "lc2pkpi_pol_lab"])
 @pytest.mark.parametrize("kind", ["data", "mc"])
 def test_fields_match_reference_cal_angle(name, kind):
     """(with per-event charges: parity transform of charge -1 momenta under
-    cp_trans, or the charge field without it)"""
+    cp_trans, or the charge field without it; lc2pkpi_pol_lab: momenta out
+    of the parent rest frame, its flight direction as z)"""
     from tf_pwa_b200.kinematics import event_fields, p4_dict
 
     g, meta = load_golden(name)

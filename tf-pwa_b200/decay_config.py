@@ -287,6 +287,7 @@ class DecayConfig:
         group.charge = bool(dk.get("use_charge")) or any(
             str(k).endswith("_charge") for k in dk)
         group.cp_trans = bool(dk.get("cp_trans", True))
+        group.random_z = bool(dk.get("random_z", True))
         return group
 
 

@@ -131,6 +131,13 @@ class KinCode:
                 # helicity angles, frames, SU(2) bookkeeping
                 set_x = {top: "V3{1.0, 0.0, 0.0}"}
                 set_z = {top: "V3{0.0, 0.0, 1.0}"}
+                if plan.random_z:
+                    # a moving parent's flight direction is the z axis
+                    # (tf_pwa/cal_angle.py:431-438)
+                    bz = tmp(f"t{t}_bz")
+                    e(f"  V3 {bz} = lv_vec({mom[top]});")
+                    e(f"  if (sqrt(v3_dot({bz}, {bz})) < 1e-5) {bz} = V3{{0.0, 0.0, 1.0}};")
+                    set_z[top] = bz
                 angles, rmat, bmat = {}, {}, {}
                 decays = list(chain)
                 while decays:

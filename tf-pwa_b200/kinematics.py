@@ -120,9 +120,11 @@ def su2_euler(x):
 
 
 # ------------------------------------------------------------- chains
-def _chain_frames(chain_topo, mom):
+def _chain_frames(chain_topo, mom, random_z=False):
     """Helicity angles of every out of every decay, and per final particle
-    the SU(2) rotation and boost accumulated along the chain."""
+    the SU(2) rotation and boost accumulated along the chain.  With
+    ``random_z`` a moving parent's flight direction is the z axis of its
+    decay (``tf_pwa/cal_angle.py:431-438``)."""
     chain = chain_topo.chain
     top = chain.top
     # successive rest-frame momenta (cal_chain_boost)
@@ -162,6 +164,10 @@ def _chain_frames(chain_topo, mom):
     dev = mom[top].device
     set_x = {top: torch.tensor([1.0, 0.0, 0.0], dtype=torch.float64, device=dev).expand(n, 3)}
     set_z = {top: torch.tensor([0.0, 0.0, 1.0], dtype=torch.float64, device=dev).expand(n, 3)}
+    if random_z:
+        p3 = mom[top][:, 1:]
+        moving = (torch.linalg.norm(p3, dim=1) >= 1e-5)[:, None]
+        set_z[top] = torch.where(moving, p3, set_z[top])
     angles = {}
     rmat, bmat = {}, {}
     decays = list(chain)
@@ -221,7 +227,7 @@ def event_fields(plan, p4, device=None, charge=None):
             for p in chain.inner:
                 mom[p] = sum(mom[f] for f in chain.final_set(p))
             mom[chain.top] = sum(mom[f] for f in chain.outs)
-            angles, rmat, bmat = _chain_frames(topo, mom)
+            angles, rmat, bmat = _chain_frames(topo, mom, plan.random_z)
             frames.append((topo, angles, rmat, bmat, mom))
         return frames
 

@@ -421,6 +421,7 @@ class DecayGroup:
         self.cp_particles = None
         self.charge = False       # per-event charge_conjugation field in use
         self.cp_trans = True      # parity-transform charge < 0 momenta
+        self.random_z = True      # moving parent: flight direction as z
         self.top = self.chains[0].top
         self.outs = sorted(self.chains[0].outs)
         for c in self.chains:

@@ -94,6 +94,8 @@ class Plan:
         # couplings of the vertices that allow it
         self.use_charge = bool(getattr(group, "charge", False))
         self.cp_trans = getattr(group, "cp_trans", True)
+        # a moving parent's flight direction is the z axis of its decay
+        self.random_z = getattr(group, "random_z", True)
         flips = any(getattr(d, "allow_cc", False) for c in group for d in c)
         self.charge_index = self.field("charge") if self.use_charge and flips else None
         self.swaps = []
