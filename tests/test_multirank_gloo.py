@@ -9,7 +9,6 @@ gradient of all events (the reference's golden values)."""
 import os
 
 import numpy as np
-import pytest
 
 
 def _pieces(rank, world, q):

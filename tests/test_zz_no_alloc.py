@@ -13,8 +13,6 @@ tolerance 1e-12: identical FP64 arithmetic, only the block split differs).
 It lives in its own file, collected last, so a failure here does not hide
 the other tests.
 """
-import ctypes
-
 import numpy as np
 import pytest
 
