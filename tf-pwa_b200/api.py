@@ -172,10 +172,16 @@ class FCN:
         return self.vm.get_all_dic(trainable_only)
 
     def _set(self, x):
-        if x is not None and len(np.atleast_1d(x)) > 0 and not isinstance(x, dict):
+        if x is None:
+            return
+        if isinstance(x, dict):
+            if x:
+                self.vm.set_all(x)
+        elif isinstance(x, np.ndarray):
+            if x.size:
+                self.vm.set_all(x)
+        elif len(x):
             self.vm.set_all(list(x))
-        elif isinstance(x, dict) and x:
-            self.vm.set_all(x)
 
     def get_nll_grad(self, x=None):
         self._set(x)

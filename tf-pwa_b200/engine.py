@@ -51,7 +51,7 @@ def load_library(path=LIB_PATH):
     lib.pwa_eval_cached_enqueue.argtypes = [vp, dp, vp]
     lib.pwa_set_param_layout.argtypes = [vp, i, i, ip, ip, ip, i, ip, i, ip]
     lib.pwa_pieces_cached.argtypes = [vp, dp, ctypes.c_double, ctypes.c_double, vp, dp]
-    lib.pwa_nll_grad_cached.argtypes = [vp, dp, ctypes.c_double, vp, dp, dp]
+    lib.pwa_nll_grad_cached.argtypes = [vp, vp, ctypes.c_double, vp, vp, vp]
     lib.pwa_set_cached_variant.argtypes = [vp, i]
     llp = ctypes.POINTER(ll)
     lib.pwa_pool_reserve.argtypes = [vp, ll]
@@ -736,6 +736,12 @@ class Engine:
         self._layout = [self._ivec(x) for x in (r, im, pol, cf.reshape(-1), tr)]
         self._var_names = list(var_names)
         self._n_train = len(tr)
+        # per-call buffers of the cached evaluation, addresses taken once
+        self._vbuf = np.zeros(len(var_names))
+        self._gbuf = np.zeros(len(tr))
+        self._nbuf = np.zeros(1)
+        self._vbuf_p, self._gbuf_p, self._nbuf_p = (
+            self._vbuf.ctypes.data, self._gbuf.ctypes.data, self._nbuf.ctypes.data)
         (a, pa), (b, pb), (c, pc), (d, pd), (e, pe) = self._layout
         self._check(load_library().pwa_set_param_layout(
             self.h, len(var_names), len(r), pa, pb, pc, nfac, pd, len(tr), pe),
@@ -762,13 +768,11 @@ class Engine:
         if self.dist_reduce is not None:
             vec = self.dist_reduce(self.pieces_cached(var_values, stream=stream))
             return combine_pieces(vec, self._n_train)
-        v = np.ascontiguousarray(var_values, np.float64)
-        nll = ctypes.c_double()
-        g = np.zeros(self._n_train)
-        self._check(load_library().pwa_nll_grad_cached(self.h, _dptr(v), self._sw, stream or 0,
-                                                       ctypes.byref(nll), _dptr(g)),
+        self._vbuf[:] = var_values
+        self._check(load_library().pwa_nll_grad_cached(self.h, self._vbuf_p, self._sw,
+                                                       stream or 0, self._nbuf_p, self._gbuf_p),
                     "pwa_nll_grad_cached")
-        return nll.value, g
+        return float(self._nbuf[0]), self._gbuf.copy()
 
     def hessian_cached(self, var_values, step=1e-4, stream=None):
         """(nll, grad, Hessian) of the cached form, the Hessian by 4-point

@@ -82,12 +82,12 @@ class VarsManager:
             for k, v in vals.items():
                 self.set(k, v)
         else:
-            vals = list(vals)
+            # python floats (an array's tolist() is already float)
+            vals = vals.tolist() if isinstance(vals, np.ndarray) else [float(v) for v in vals]
             if len(vals) != len(self.trainable_vars):
                 raise ValueError(
                     f"expected {len(self.trainable_vars)} values, got {len(vals)}")
-            for k, v in zip(self.trainable_vars, vals):
-                self.variables[k] = float(v)
+            self.variables.update(zip(self.trainable_vars, vals))
 
     def get_all_val(self):
         return [self.variables[k] for k in self.trainable_vars]
