@@ -176,7 +176,8 @@ def bprime(l, q, q0, d):
 
 
 def gamma_running(m, g0, q, q0, L, m0, d):
-    qq0 = np.where(q0 > 1e-15, (q / q0) ** (2 * L + 1), 1.0)
+    ok = q0 > 1e-15
+    qq0 = np.where(ok, (q / np.where(ok, q0, 1.0)) ** (2 * L + 1), 1.0)
     return g0 * qq0 * (m0 / m) * bprime(L, q, q0, d) ** 2
 
 
