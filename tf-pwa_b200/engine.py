@@ -17,6 +17,7 @@ J_k = dc_k/dtheta + c_k * kappa_k(theta), c_k the product of the column's
 complex couplings (chain total and one g_ls per vertex) and kappa_k the
 derivative of the column's log barrier factors through q0 (nominal masses).
 """
+import cmath
 import ctypes
 import os
 
@@ -373,59 +374,200 @@ class Engine:
             _, self._drho = density_matrix(self.group.top.J, np.zeros(len(self._pol_names)))
         self._mass_names = {f"{p.params_head}_mass": p for p in self.group.resonances}
         self._width_names = {f"{p.params_head}_width": p for p in self.group.resonances}
+        self._build_vertex_tables()
 
-    def _nominal(self, p, vals, chain):
-        if p.key() in self._inner_keys[id(chain)]:
-            return vals.get(f"{p.params_head}_mass", p.mass)
-        return p.mass
+    # ------------------------------------------- vectorised barrier constants
+    def _build_vertex_tables(self):
+        """Rows for the barrier and lineshape constants, built once: nominal
+        masses gathered in one list (resonance masses from the parameters,
+        the others fixed), one row per vertex with its (l, slot) entries, one
+        row per lineshape, and for the Jacobian the (column, vertex entry)
+        pairs through which each resonance mass acts.  Evaluated with scalar
+        arithmetic (a few dozen rows: cheaper than array calls)."""
+        parts = {}
+        plist = []
 
-    def complex_val(self, vals, name):
-        r, i = vals[name + "r"], vals[name + "i"]
-        if self.vm.complex_vars.get(name, True):
-            return r * np.cos(i) + 1j * r * np.sin(i)
-        return r + 1j * i
+        def pidx(q):
+            k = q.key()
+            if k not in parts:
+                parts[k] = len(plist)
+                plist.append(q)
+            return parts[k]
 
-    def _vertex_consts(self, d, chain, vals, m_override=None):
-        """{l: (Pz0_l, norm_l)} of vertex d, masses optionally overridden."""
-        a, (b, c) = d.core, d.outs
-        mv = lambda p: (m_override[p] if m_override and p in m_override else self._nominal(p, vals, chain))  # noqa: E731
-        q02 = rel_p2(mv(a), mv(b), mv(c))
-        if d.no_q0:
-            q02 = 1.0 + 0 * q02
-        out = {}
-        for l in sorted(set(d.get_l_list())):
-            pz0 = poly(l, q02 * d.d * d.d) if d.has_bprime else 1.0
-            norm = 1.0 / np.abs(q02) ** (l / 2) if d.barrier_factor_norm else 1.0
-            if isinstance(q02, complex) or np.iscomplexobj(q02):
-                norm = 1.0 / np.sqrt(q02 * q02) ** (l / 2) if d.barrier_factor_norm else 1.0
-            out[l] = (pz0, norm)
+        for q in self.group.resonances:
+            dq, _ = self.res_info[q]
+            for x in (q,) + tuple(dq.outs):
+                pidx(x)
+        res_keys = {q.key() for q in self.group.resonances}
+        self._vt_rows = []
+        vindex = {}
+        for d, chain, sl in self._vtx_slots:
+            a, (b, cc) = d.core, d.outs
+            entries = []
+            for l in sorted(sl):
+                s_pz, s_norm = sl[l]
+                entries.append((l, tuple(bprime_coeff(l)), bool(d.has_bprime),
+                                bool(d.barrier_factor_norm),
+                                -1 if s_pz is None else s_pz, -1 if s_norm is None else s_norm))
+            vindex[d.key()] = len(self._vt_rows)
+            self._vt_rows.append((pidx(a), pidx(b), pidx(cc), bool(d.no_q0), float(d.d),
+                                  bool(d.has_barrier_factor), entries))
+        self._m_base = [q.mass if q.mass is not None else 0.0 for q in plist]
+        self._m_res = [(i, f"{q.params_head}_mass", q.mass) for i, q in enumerate(plist)
+                       if q.key() in res_keys]
+        # Jacobian rows of a resonance mass: the vertices it enters (with a
+        # barrier factor) and per column the (vertex, l) entries summed
+        self._jac_pairs = {}
+        for q in self.group.resonances:
+            contrib, verts = [], []
+            for k, (ci, lsi) in enumerate(self.code.columns):
+                chain = self.group[ci]
+                if q.key() not in self._inner_keys[id(chain)]:
+                    continue
+                for vi, d in enumerate(chain):
+                    if q not in (d.core,) + d.outs or not d.has_barrier_factor:
+                        continue
+                    v = vindex[d.key()]
+                    if v not in verts:
+                        verts.append(v)
+                    contrib.append((k, v, d.get_ls_list()[lsi[vi]][0]))
+            if contrib:
+                self._jac_pairs[q.key()] = (parts[q.key()], verts, contrib)
+        # lineshape rows
+        shape_pos = {q.key(): j for j, (q, _, _) in enumerate(self._shape_slots)}
+        self._ls_rows = []
+        for p, kind, s_m0sq, s_k, s_useq, s_y, s_iq, s_wn in self._res_slots:
+            dp, chain = self.res_info[p]
+            b, cc = dp.outs
+            L = p.bw_l if p.bw_l is not None else min(dp.get_l_list())
+            j = shape_pos.get(p.key())
+            sh = (-1, -1) if j is None else self._shape_slots[j][1:]
+            self._ls_rows.append((kind, parts[p.key()], parts[b.key()], parts[cc.key()], L,
+                                  float(p.d), f"{p.params_head}_width", p.width,
+                                  tuple(bprime_coeff(L)), s_m0sq, s_k, s_useq, s_y, s_iq, s_wn,
+                                  sh[0], sh[1]))
+
+    def _mass_list(self, vals):
+        M = list(self._m_base)
+        for i, n, dflt in self._m_res:
+            M[i] = vals.get(n, dflt)
+        return M
+
+    @staticmethod
+    def _vertex_entry_values(q02, d, entries):
+        """[(Pz0_l, norm_l)] of one vertex: ``poly(l, q02 d d)`` and
+        ``1 / |q02|^(l/2)`` (``1 / sqrt(q02 q02)^(l/2)`` when complex)."""
+        out = []
+        z = q02 * d * d
+        cplx = isinstance(q02, complex)
+        for l, coef, bp, bn, _, _ in entries:
+            if bp:
+                r = 0.0
+                for c_ in coef:
+                    r = r * z + c_
+            else:
+                r = 1.0
+            if bn:
+                nrm = 1.0 / (cmath.sqrt(q02 * q02) if cplx else abs(q02)) ** (l / 2)
+            else:
+                nrm = 1.0
+            out.append((r, nrm))
         return out
 
-    def _lineshape_K(self, p, vals, m0=None):
-        kind = p.lineshape_kind()
-        dp, chain = self.res_info[p]
-        m0 = self._nominal(p, vals, chain) if m0 is None else m0
-        g0 = vals.get(f"{p.params_head}_width", p.width)
-        if kind == "BW":
-            return m0 * g0, 1.0
-        b, c = dp.outs
-        L = p.bw_l if p.bw_l is not None else min(dp.get_l_list())
-        q0 = rel_p(m0, self._nominal(b, vals, chain), self._nominal(c, vals, chain))
-        pz0 = poly(L, (q0 * p.d) ** 2)
-        if np.real(q0) > 1e-15:
-            return m0 * m0 * g0 * pz0 / q0 ** (2 * L + 1), 1.0
-        return m0 * m0 * g0 * pz0, 0.0
+    @staticmethod
+    def _vertex_q02(M, row):
+        ia, ib, ic, noq0 = row[0], row[1], row[2], row[3]
+        if noq0:
+            return 1.0
+        return rel_p2(M[ia], M[ib], M[ic])
 
-    def _lineshape_K2(self, p, vals, m0=None):
-        """(m0^2 Gamma0 B_L(q0^2 d^2), q0^2) of a BWR2 lineshape, q0^2 from
-        the nominal masses without clamping (``tf_pwa/amp/core.py:826-843``)."""
-        dp, chain = self.res_info[p]
-        m0 = self._nominal(p, vals, chain) if m0 is None else m0
-        g0 = vals.get(f"{p.params_head}_width", p.width)
-        b, c = dp.outs
-        L = p.bw_l if p.bw_l is not None else min(dp.get_l_list())
-        q02 = rel_p2(m0, self._nominal(b, vals, chain), self._nominal(c, vals, chain))
-        return m0 * m0 * g0 * poly(L, q02 * p.d * p.d), q02
+    @staticmethod
+    def _lineshape_row_values(kind, m0, g0, mb, mc, L, d, coef):
+        """(K, useq, q0^2) of one lineshape at parent mass ``m0`` (real or
+        complex): BWR K = m0^2 Gamma0 B_L(q0 d) / q0^(2L+1) (q0 clamped at
+        threshold; without the q0 power and useq = 0 below it), BWR2
+        K = m0^2 Gamma0 B_L(q0^2 d^2) with q0^2 unclamped, BW K = m0 Gamma0."""
+        if kind == "BW":
+            return m0 * g0, 1.0, None
+        if kind == "BWR2":
+            q02 = rel_p2(m0, mb, mc)
+            z = q02 * d * d
+            r = 0.0
+            for c_ in coef:
+                r = r * z + c_
+            return m0 * m0 * g0 * r, 1.0, q02
+        q0 = rel_p(m0, mb, mc)
+        z = (q0 * d) ** 2
+        r = 0.0
+        for c_ in coef:
+            r = r * z + c_
+        if q0.real > 1e-15:
+            return m0 * m0 * g0 * r / q0 ** (2 * L + 1), 1.0, None
+        return m0 * m0 * g0 * r, 0.0, None
+
+    def _shape_consts(self, C, vals):
+        """Lineshape and barrier constants of the constant block at ``vals``."""
+        M = self._mass_list(vals)
+        for row in self._vt_rows:
+            entries = row[6]
+            vals_e = self._vertex_entry_values(self._vertex_q02(M, row), row[4], entries)
+            for (_, _, _, _, s_pz, s_norm), (pz, nrm) in zip(entries, vals_e):
+                if s_pz >= 0:
+                    C[s_pz] = pz
+                if s_norm >= 0:
+                    C[s_norm] = nrm
+        h = 1e-20
+        for (kind, im, ib, ic, L, d, gname, gdef, coef, s_m0sq, s_k, s_useq, s_y, s_iq, s_wn,
+             s_kap, s_ig) in self._ls_rows:
+            m0, mb, mc = M[im], M[ib], M[ic]
+            g0 = vals.get(gname, gdef)
+            C[s_m0sq] = m0 * m0
+            K, useq, q02 = self._lineshape_row_values(kind, m0, g0, mb, mc, L, d, coef)
+            if kind == "BWR":
+                C[s_k] = K
+                C[s_useq] = useq
+            elif kind == "BWR2":
+                C[s_k] = K
+                C[s_iq] = 1.0 / q02
+            else:
+                C[s_y] = K
+            if s_wn is not None:
+                C[s_wn] = g0
+            if s_kap >= 0:
+                # kappa = dlog(m0 Gamma) / dm0 by a complex step; for BWR2
+                # m0 Gamma2 = K r^(L+1/2) / (m B): dlog K - (L + 1/2) dlog q0^2
+                Kc, _, qc = self._lineshape_row_values(kind, complex(m0, h), g0, mb, mc, L, d,
+                                                       coef)
+                kap = Kc.imag / h / K.real if K.real != 0 else 0.0
+                if kind == "BWR2":
+                    kap -= (L + 0.5) * qc.imag / h / q02.real
+                C[s_kap] = kap
+                C[s_ig] = 1.0 / g0 if g0 else 0.0
+
+    def _mass_dlog(self, vals, key):
+        """{column: d ln(prod of its barrier factors) / d m} of a resonance
+        mass, by a complex step through the vertices it enters."""
+        qi, verts, contrib = self._jac_pairs[key]
+        M = self._mass_list(vals)
+        Mc = list(M)
+        Mc[qi] = complex(M[qi], 1e-20)
+        dlog = {}
+        for v in verts:
+            row = self._vt_rows[v]
+            e0 = self._vertex_entry_values(self._vertex_q02(M, row), row[4], row[6])
+            ec = self._vertex_entry_values(self._vertex_q02(Mc, row), row[4], row[6])
+            for (l, _, bp, bn, _, _), (pz0, n0), (pzc, nc) in zip(row[6], e0, ec):
+                t = 0.0
+                # bf_l ~ sqrt(Pz0_l) * norm_l
+                if bp:
+                    t += 0.5 * complex(pzc).imag / 1e-20 / complex(pz0).real
+                if bn:
+                    t += complex(nc).imag / 1e-20 / complex(n0).real
+                dlog[(v, l)] = t
+        kap = {}
+        for k, v, l in contrib:
+            kap[k] = kap.get(k, 0.0) + dlog[(v, l)]
+        return kap
 
     def _shape_key(self, vals):
         return tuple(vals.get(k) for k in self._shape_names)
@@ -434,28 +576,33 @@ class Engine:
         """Constant block of one evaluation from the parameter dict.  The
         part that depends only on masses and widths (lineshape and barrier
         constants) is cached per mass/width setting."""
-        c = self.code
         if not hasattr(self, "_shape_names"):
             self._shape_names = sorted(k for k in vals if k.endswith(("_mass", "_width")))
         key = self._shape_key(vals)
         if self._shape_cache[0] == key:
             C = self._shape_cache[1].copy()
-            r = np.fromiter((vals[n] for n in self._cn_r), float, len(self._cn_r))
-            ph = np.fromiter((vals[n] for n in self._cn_i), float, len(self._cn_i))
-            z = np.where(self._cn_polar, r * np.exp(1j * ph), r + 1j * ph)
-            self._cvec, self._cr, self._cph = z, r, ph
-            self._cv = dict(zip(self.coupling_names, z))
-            self._ck = np.prod(np.append(z, 1.0 + 0j)[self._fac_idx], axis=1)
-            C[0:2 * c.ncol:2] = self._ck.real
-            C[1:2 * c.ncol:2] = self._ck.imag
-            C[self._vg_re] = z[self._vg_src].real
-            C[self._vg_im] = z[self._vg_src].imag
-            self._fill_rho(C, vals)
-            return C
-        C = self._consts_full(vals)
-        self._shape_cache = (key, C.copy())
+        else:
+            C = np.zeros(len(self.code.consts))
+            self._shape_consts(C, vals)
+            self._shape_cache = (key, C.copy())
+        self._coupling_consts(C, vals)
         self._fill_rho(C, vals)
         return C
+
+    def _coupling_consts(self, C, vals):
+        """Column couplings c_k (products of the complex couplings), vertex
+        couplings and chain totals into the constant block."""
+        c = self.code
+        r = np.fromiter((vals[n] for n in self._cn_r), float, len(self._cn_r))
+        ph = np.fromiter((vals[n] for n in self._cn_i), float, len(self._cn_i))
+        z = np.where(self._cn_polar, r * np.exp(1j * ph), r + 1j * ph)
+        self._cvec, self._cr, self._cph = z, r, ph
+        self._cv = dict(zip(self.coupling_names, z))
+        self._ck = np.prod(np.append(z, 1.0 + 0j)[self._fac_idx], axis=1)
+        C[0:2 * c.ncol:2] = self._ck.real
+        C[1:2 * c.ncol:2] = self._ck.imag
+        C[self._vg_re] = z[self._vg_src].real
+        C[self._vg_im] = z[self._vg_src].imag
 
     def _fill_rho(self, C, vals):
         """Parent spin density matrix (polarised models) into its slots."""
@@ -464,65 +611,6 @@ class Engine:
         rho, _ = density_matrix(self.group.top.J, [vals[n] for n in self._pol_names])
         C[self._rho_re] = rho.real.reshape(-1)
         C[self._rho_im] = rho.imag.reshape(-1)
-
-    def _consts_full(self, vals):
-        c = self.code
-        C = np.zeros(len(c.consts))
-        idx = c.consts.index
-        cv = {n: self.complex_val(vals, n) for n in self.coupling_names}
-        cvec = np.array([cv[n] for n in self.coupling_names] + [1.0 + 0j])
-        self._ck = np.prod(cvec[self._fac_idx], axis=1)
-        self._cv = cv
-        self._cvec = cvec[:-1]
-        self._cr = np.array([vals[n] for n in self._cn_r])
-        self._cph = np.array([vals[n] for n in self._cn_i])
-        C[0:2 * c.ncol:2] = self._ck.real
-        C[1:2 * c.ncol:2] = self._ck.imag
-        C[self._vg_re] = self._cvec[self._vg_src].real
-        C[self._vg_im] = self._cvec[self._vg_src].imag
-        for p, kind, s_m0sq, s_k, s_useq, s_y, s_iq, s_wn in self._res_slots:
-            dp, chain = self.res_info[p]
-            m0 = self._nominal(p, vals, chain)
-            g0 = vals.get(f"{p.params_head}_width", p.width)
-            C[s_m0sq] = m0 * m0
-            if kind == "BWR":
-                K, useq = self._lineshape_K(p, vals)
-                C[s_k] = K
-                C[s_useq] = useq
-            elif kind == "BWR2":
-                K, q02 = self._lineshape_K2(p, vals)
-                C[s_k] = K
-                C[s_iq] = 1.0 / q02
-            else:
-                C[s_y] = m0 * g0
-            if s_wn is not None:
-                C[s_wn] = g0
-        for d, chain, sl in self._vtx_slots:
-            vc = self._vertex_consts(d, chain, vals)
-            for l, (pz0, norm) in vc.items():
-                s_pz, s_norm = sl[l]
-                if s_pz is not None:
-                    C[s_pz] = pz0
-                if s_norm is not None:
-                    C[s_norm] = norm
-        for p, s_kap, s_ig in self._shape_slots:
-            dp, chain = self.res_info[p]
-            m0 = self._nominal(p, vals, chain)
-            g0 = vals.get(f"{p.params_head}_width", p.width)
-            h = 1e-20
-            if p.lineshape_kind() == "BWR2":
-                # m0 Gamma2 = K r^(L+1/2) / (m B): dlog/dm0 = dlog K - (L + 1/2) dlog q0^2
-                Kc, qc = self._lineshape_K2(p, vals, m0=m0 + 1j * h)
-                K0, q0 = self._lineshape_K2(p, vals, m0=m0)
-                L = p.bw_l if p.bw_l is not None else min(dp.get_l_list())
-                C[s_kap] = (np.imag(Kc) / h / np.real(K0) if np.real(K0) != 0 else 0.0) \
-                    - (L + 0.5) * np.imag(qc) / h / np.real(q0)
-            else:
-                Kc, _ = self._lineshape_K(p, vals, m0=m0 + 1j * h)
-                K0, _ = self._lineshape_K(p, vals, m0=m0)
-                C[s_kap] = np.imag(Kc) / h / np.real(K0) if np.real(K0) != 0 else 0.0
-            C[s_ig] = 1.0 / g0 if g0 else 0.0
-        return C
 
     # ------------------------------------------------------------ jacobian
     def _jac_layout(self, names):
@@ -603,34 +691,9 @@ class Engine:
                 raise KeyError(f"unknown parameter {n}")
             if (p, kind) in self.shape_index:
                 D[pi, self.shape_index[(p, kind)]] = 1.0
-            if kind == "m":
-                # barrier factors through q0^2 of every vertex touching p:
-                # complex-step derivative of each vertex's constants, once
-                hh = 1e-20
-                dlog = {}  # (chain index, vertex index) -> {l: d ln bf_l / dm}
-                for k, (ci, lsi) in enumerate(c.columns):
-                    chain = self.group[ci]
-                    if p.key() not in self._inner_keys[id(chain)]:
-                        continue
-                    kap = 0.0
-                    for vi, d in enumerate(chain):
-                        if p not in (d.core,) + d.outs or not d.has_barrier_factor:
-                            continue
-                        if (ci, vi) not in dlog:
-                            m0 = self._nominal(p, vals, chain)
-                            vc = self._vertex_consts(d, chain, vals, {p: m0 + 1j * hh})
-                            v0 = self._vertex_consts(d, chain, vals)
-                            e = {}
-                            for l in v0:
-                                t = 0.0
-                                # bf_l ~ sqrt(Pz0_l) * norm_l
-                                if d.has_bprime:
-                                    t += 0.5 * np.imag(vc[l][0]) / hh / np.real(v0[l][0])
-                                if d.barrier_factor_norm:
-                                    t += np.imag(vc[l][1]) / hh / np.real(v0[l][1])
-                                e[l] = t
-                            dlog[(ci, vi)] = e
-                        kap += dlog[(ci, vi)][d.get_ls_list()[lsi[vi]][0]]
+            if kind == "m" and p.key() in self._jac_pairs:
+                # barrier factors through q0^2 of every vertex touching p
+                for k, kap in self._mass_dlog(vals, p.key()).items():
                     J[pi, k] += self._ck[k] * kap
         if cached is None and key[1] is not None:
             # mass/width rows: J = kappa_k * c_k with kappa fixed per shape setting
