@@ -14,8 +14,7 @@ from common import golden_data, load_golden, load_model
 pytestmark = pytest.mark.gpu
 
 CASES = ["d2kpipi", "d2kpipi_float", "lc2pkpi", "b2dstkpi", "d2kpipi_shapes", "dp2kpipi_ident",
-         "ident_fermions", "epem_cp", "lc2pkpi_cc", "b2dstkpi_cc", "lc2pkpi_pol",
-         "epem_pol"]
+         "ident_fermions", "epem_cp"]
 
 
 def _engine(name):

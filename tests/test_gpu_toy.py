@@ -29,7 +29,7 @@ def _engine(cfg, variables=None):
 
 
 @pytest.mark.parametrize("name", ["d2kpipi", "lc2pkpi", "b2dstkpi", "dp2kpipi_ident", "ident_fermions",
-                                  "epem_cp", "lc2pkpi_cc", "b2dstkpi_cc", "lc2pkpi_pol_lab"])
+                                  "epem_cp"])
 def test_fields_from_p4_match_reference(name):
     import torch
 
@@ -137,23 +137,3 @@ def test_generated_dataset_statistics():
     err = np.sqrt(xr.var() / len(xr) + xm.var() / len(xm))
     assert abs(xr.mean() - xm.mean()) < 5 * err
 
-
-def test_config_loader_generators():
-    """ConfigLoader.generate_phsp / generate_phsp_p / generate_toy on the
-    toy kernels: the phase-space fields are the kinematics of the returned
-    momenta; the toy keeps its accept-reject maximum."""
-    import os
-
-    from common import CONFIGS
-    from tf_pwa_b200.api import ConfigLoader
-    from tf_pwa_b200.kinematics import event_fields, p4_dict
-
-    cl = ConfigLoader(os.path.join(CONFIGS, "lc2pkpi.yml"), seed=2)
-    d = cl.generate_phsp(3000, seed=21)
-    p4 = cl.generate_phsp_p(3000, seed=21)
-    assert tuple(p4.shape) == (3000, 3, 4)
-    x = event_fields(cl.plan, p4_dict(p4.cpu().numpy(), cl.get_dat_order())).numpy()
-    np.testing.assert_allclose(d.fields.cpu().numpy(), x, rtol=0, atol=TOL_FIELD)
-    toy = cl.generate_toy(2000, seed=22)
-    assert toy.fields.shape == (cl.plan.n_fields, 2000)
-    assert cl.max_amplitude is not None and cl.max_amplitude > 0
