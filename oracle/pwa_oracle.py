@@ -250,7 +250,14 @@ class OracleModel:
         out = []
         from_names = {}
         for c in self.group:
-            tot = self.complex_of(vals, polar, c.params_head + "_total_0")
+            tn = c.params_head + "_total_0"
+            if getattr(c, "is_cp", False):
+                # CP-violating total: (r +- deltar, i +- deltai) for charge +-1
+                # (tf_pwa/variable.py:1715-1734, tf_pwa/amp/core.py:1380-1390)
+                r, i, dr, di = (vals[tn + x] for x in ("r", "i", "deltar", "deltai"))
+                tot = tuple((r + s_ * dr) * np.exp(1j * (i + s_ * di)) for s_ in (1.0, -1.0))
+            else:
+                tot = self.complex_of(vals, polar, tn)
             gl = []
             for d in c:
                 n = len(d.get_ls_list())
@@ -351,6 +358,9 @@ class OracleModel:
         rs = np.ones(x.shape[1], dtype=np.complex128)
         for p in chain.inner:
             rs = rs * self.lineshape(x, cf, chain, p, vals)
+        if isinstance(tot, tuple):
+            ci_ = getattr(self.plan, "charge_index", None)
+            tot = tot[0] if ci_ is None else np.where(x[ci_] > 0, tot[0], tot[1])
         ops.append(tot * rs)
         idx.append("...")
         final = "..." + "".join(L[p] for p in [self.group.top] + list(self.group.outs))
@@ -478,10 +488,12 @@ class OracleNLL:
         Sd, Sm = seed(Ad), seed(Am)
         dclip = np.where(fd0 > _EPS_CLIP, 1.0 / np.where(fd0 > _EPS_CLIP, fd0, 1.0),
                          1.0 / _EPS_CLIP - (fd0 - _EPS_CLIP) / _EPS_CLIP ** 2)
+        cp_totals = {c.params_head + "_total_0" for c in self.m.group if getattr(c, "is_cp", False)}
         for k, n in enumerate(self.names):
             base = n[:-1]
             if n.endswith(("r", "i")) and base + "r" in v0 and base + "i" in v0 and (
-                    "_g_ls_" in base or "_total_" in base):
+                    "_g_ls_" in base or "_total_" in base) and not any(
+                    base.startswith(t) for t in cp_totals):
                 # dA/dtheta: A is linear in the complex coupling c = c(r, phi)
                 c = self.m.complex_of(v0, self.polar, base)
                 polar = self.polar.get(base, True)

@@ -51,6 +51,7 @@ CASES = {
     "epem_pol": ("epem_pol.yml", 300, 0, 1200, 23, False, {}),
     "ident3_fermions": ("ident3_fermions.yml", 300, 0, 1200, 24, False, {}),
     "lc2pkpi_pol_lab": ("lc2pkpi_pol.yml", 400, 0, 1500, 25, False, {}),
+    "lc2pkpi_cp": ("lc2pkpi_cp.yml", 400, 0, 1500, 26, False, {}),
 }
 # cases whose events are boosted out of the parent rest frame: parent
 # momentum (GeV) in a random direction per event (lab-frame input)
@@ -145,7 +146,9 @@ def main(ref_root):
         # masses/widths at their nominal values shifted by a few percent
         params = {}
         for k in vm.trainable_vars:
-            if k.endswith("r") and ("_g_ls_" in k or "_total_" in k):
+            if k.endswith(("deltar", "deltai")):
+                params[k] = float(rng.uniform(-0.3, 0.3))
+            elif k.endswith("r") and ("_g_ls_" in k or "_total_" in k):
                 params[k] = float(rng.uniform(0.5, 2.0))
             elif k.endswith("i") and ("_g_ls_" in k or "_total_" in k):
                 params[k] = float(rng.uniform(-np.pi, np.pi))

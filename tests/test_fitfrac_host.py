@@ -4,7 +4,8 @@ oracle: fractions within 1e-9 relative, gradients equal to central
 differences of the oracle's fractions (h = 1e-6; 2e-6 of the largest
 derivative, absolute floor 1e-9) for every trainable
 parameter -- including identical-particle swaps, a polarised parent (its
-density-matrix parameters) and floating BWR2 / width_norm lineshapes."""
+density-matrix parameters), floating BWR2 / width_norm lineshapes and
+CP-violating chain totals with per-event charges."""
 import numpy as np
 import pytest
 
@@ -19,8 +20,9 @@ def _oracle_ff(m, group, vals, xm, res):
         v = dict(vals)
         for ci, t in enumerate(tot):
             if ci not in chains:
-                v[t + "r"] = 0.0
-                v[t + "i"] = 0.0
+                for suf in ("r", "i", "deltar", "deltai"):
+                    if t + suf in v:
+                        v[t + suf] = 0.0
         return float(np.sum(m.pdf(xm, v)))
 
     sets = [{ci for ci, c in enumerate(group) if any(str(p) == r for p in c.inner)} for r in res]
@@ -36,7 +38,8 @@ def _oracle_ff(m, group, vals, xm, res):
     return out
 
 
-@pytest.mark.parametrize("name", ["lc2pkpi", "dp2kpipi_ident", "lc2pkpi_pol", "d2kpipi_shapes"])
+@pytest.mark.parametrize("name", ["lc2pkpi", "dp2kpipi_ident", "lc2pkpi_pol", "d2kpipi_shapes",
+                                  "lc2pkpi_cp"])
 def test_fit_fractions_host(name, tmp_path):
     from oracle.pwa_oracle import OracleModel
     from tf_pwa_b200.engine import PLAIN_F64, Engine

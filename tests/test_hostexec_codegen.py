@@ -28,7 +28,8 @@ from hostexec import HostModel
 
 CASES = ["d2kpipi", "d2kpipi_float", "lc2pkpi", "toy_vvp", "b2dstkpi", "d2kpipi_shapes",
          "dp2kpipi_ident", "ident_fermions", "epem_cp", "lc2pkpi_cc", "b2dstkpi_cc",
-         "lc2pkpi_pol", "epem_pol", "ident3_fermions", "lc2pkpi_pol_lab"]
+         "lc2pkpi_pol", "epem_pol", "ident3_fermions", "lc2pkpi_pol_lab",
+         "lc2pkpi_cp"]
 
 _CACHE = {}
 
@@ -90,12 +91,16 @@ def test_kernel_loop_nll_grad(name, f32, stash, build_dir):
 
 @pytest.mark.parametrize("name", CASES)
 def test_columns_rebuild_amplitude(name, build_dir):
-    eng, hm, g, meta, _, _ = _setup(name, build_dir)
+    eng, hm, g, meta, _, plan = _setup(name, build_dir)
     C = eng.consts(meta["variables"])
     x = g["fields_data"][:, :200]
     A = hm.amp(C, x)
     F = hm.columns(C, x)
-    A2 = np.einsum("k,nko->no", eng._ck, F)
+    ck = np.tile(eng._ck, (x.shape[1], 1))
+    if eng.code.ncp:  # CP-violating totals: charge -1 events take c_k^-
+        minus = x[plan.charge_index] < 0
+        ck[np.ix_(minus, eng._cp_cols)] = eng._ck_m[eng._cp_cols]
+    A2 = np.einsum("nk,nko->no", ck, F)
     np.testing.assert_allclose(A2, A, rtol=1e-12, atol=1e-12 * np.abs(A).max())
 
 

@@ -7,7 +7,7 @@ from common import load_golden, load_model
 
 CASES = ["d2kpipi", "d2kpipi_float", "lc2pkpi", "toy_vvp", "b2dstkpi", "d2kpipi_shapes",
          "dp2kpipi_ident", "ident_fermions", "epem_cp", "lc2pkpi_cc", "b2dstkpi_cc",
-         "lc2pkpi_pol", "epem_pol", "ident3_fermions"]
+         "lc2pkpi_pol", "epem_pol", "ident3_fermions", "lc2pkpi_cp"]
 
 
 @pytest.mark.parametrize("name", CASES)
@@ -50,7 +50,7 @@ def test_bprime_coefficients():
 
 def test_unsupported_options_raise():
     """Options the engine does not compile fail loudly instead of being
-    ignored: CP-violating chain totals, non-default kinematics options,
+    ignored: other decay_chain options, non-default kinematics options,
     unknown lineshape models."""
     import os
 
@@ -60,7 +60,7 @@ def test_unsupported_options_raise():
     from tf_pwa_b200.plan import Plan
 
     dic = load_yaml(os.path.join(CONFIGS, "d2kpipi.yml"))
-    dic["decay_chain"] = {"$all": {"is_cp": True}}
+    dic["decay_chain"] = {"$all": {"aligned": True}}
     with pytest.raises(NotImplementedError):
         DecayConfig(dic)
     dic = load_yaml(os.path.join(CONFIGS, "d2kpipi.yml"))

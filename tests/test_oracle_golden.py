@@ -9,7 +9,8 @@ from oracle.pwa_oracle import OracleModel, OracleNLL
 
 CASES = ["d2kpipi", "d2kpipi_float", "lc2pkpi", "toy_vvp", "b2dstkpi", "d2kpipi_shapes",
          "dp2kpipi_ident", "ident_fermions", "epem_cp", "lc2pkpi_cc", "b2dstkpi_cc",
-         "lc2pkpi_pol", "epem_pol", "ident3_fermions", "lc2pkpi_pol_lab"]
+         "lc2pkpi_pol", "epem_pol", "ident3_fermions", "lc2pkpi_pol_lab",
+         "lc2pkpi_cp"]
 
 
 @pytest.mark.parametrize("name", CASES)

@@ -2,7 +2,8 @@
 GPU suite (so that under ``-x`` a failure here does not stop the others):
 
 * per-event charges (parity transform under cp_trans; helicity-coupling
-  reversal without it), vector-polarised spin-1/2 and spin-1 parents:
+  reversal without it), vector-polarised spin-1/2 and spin-1 parents,
+  CP-violating chain totals:
   plain FP64 NLL within 1e-9 and gradient within 1e-7 of the reference's
   values, the FP32 form within |dNLL| < 1e-3 and 1e-4 of the largest
   gradient component, per-event |A|^2 within 1e-11 (FP64) / 2e-4 (FP32);
@@ -20,7 +21,7 @@ from common import golden_data, load_golden, load_model
 pytestmark = pytest.mark.gpu
 
 TOL_FIELD = 1e-11
-MODELS = ["lc2pkpi_cc", "b2dstkpi_cc", "lc2pkpi_pol", "epem_pol"]
+MODELS = ["lc2pkpi_cc", "b2dstkpi_cc", "lc2pkpi_pol", "epem_pol", "lc2pkpi_cp"]
 
 
 def _engine(name):

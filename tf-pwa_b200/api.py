@@ -134,12 +134,14 @@ class FCN:
         self._upload(data, bg, mcdata)
         shape_free = any(n.endswith(("_mass", "_width")) for n in self.vm.trainable_vars)
         # a polarised parent weights the helicity products with its density
-        # matrix: the column cache / Gram form does not apply
-        polarised = self.eng.code.nrho > 0
+        # matrix, CP-violating totals differ per event charge: the column
+        # cache / Gram form does not apply
+        polarised = self.eng.code.nrho > 0 or bool(self.eng.code.cp_chains)
         self.use_gram = (self.precision == MIXED_F32 and not shape_free and not polarised) \
             if gram is None else gram
         if self.use_gram and (shape_free or polarised):
-            raise ValueError("the Gram cache needs fixed masses and widths and no polarisation")
+            raise ValueError("the Gram cache needs fixed masses and widths, no polarisation "
+                             "and no CP-violating totals")
         if self.use_gram:
             vals = self.vm.get_all_dic()
             self.eng.set_gram(vals)

@@ -127,6 +127,18 @@ class ModelCode:
         for ci in range(len(group)):
             self.consts.add(f"t{ci}.re")
             self.consts.add(f"t{ci}.im")
+        # CP-violating chain totals: charge -1 events take the second value
+        # of the total (and of its columns' couplings); their column
+        # sensitivities are summed apart (tf_pwa/amp/core.py:1380-1390)
+        self.cp_chains = [ci for ci, c in enumerate(group) if getattr(c, "is_cp", False)]
+        self.cp_cols = [k for k, (ci, _) in enumerate(self.columns) if ci in self.cp_chains]
+        self.cp_pos = {k: j for j, k in enumerate(self.cp_cols)}
+        for ci in self.cp_chains:
+            self.consts.add(f"t{ci}m.re")
+            self.consts.add(f"t{ci}m.im")
+        for k in self.cp_cols:
+            self.consts.add(f"c{k}m.re")
+            self.consts.add(f"c{k}m.im")
         self.res = []
         for p in group.resonances:
             kind = p.lineshape_kind()
@@ -162,7 +174,8 @@ class ModelCode:
                     self.consts.add(f"rho{a}_{b}.re")
                     self.consts.add(f"rho{a}_{b}.im")
         self.ncol = len(self.columns)
-        self.nacc = 1 + 2 * self.ncol + self.nshape + self.nrho
+        self.ncp = 2 * len(self.cp_cols) if plan.charge_index is not None else 0
+        self.nacc = 1 + 2 * self.ncol + self.nshape + self.nrho + self.ncp
         self._analyse()
 
     # ------------------------------------------------------------ analysis
@@ -569,10 +582,13 @@ class ModelCode:
                         prod = f"cmul({prod}, {v})"
                     e(f"  cfmac({nm}, {prod}, {vs[-1]});")
             cur = self._emit_align_forward(e, ci, pre, "Aa")
+            tot = self._cpx(f"t{ci}")
+            if ci in self.cp_chains and self.ncp:
+                tot = f"(cc ? {self._cpx(f't{ci}m')} : {tot})"
             if self._factor() == 1.0:
-                e(f"  const cpx<R> E_c{ci} = cmul({self._cpx(f't{ci}')}, BW_c{ci});")
+                e(f"  const cpx<R> E_c{ci} = cmul({tot}, BW_c{ci});")
             else:
-                e(f"  const cpx<R> E_c{ci} = cscale(cmul({self._cpx(f't{ci}')}, BW_c{ci}), "
+                e(f"  const cpx<R> E_c{ci} = cscale(cmul({tot}, BW_c{ci}), "
                   f"{_lit(self._factor())});")
             for o, nm in cur.items():
                 e(f"  cfmac(A{self._out(o)}, E_c{ci}, {nm});")
@@ -643,10 +659,18 @@ class ModelCode:
                 e("  }")
             for k in cols:
                 e(f"  {{ const cpx<R> g = cmul(cscale(BW_c{ci}, {self._scale_k(ci, k)}), Gk{k});")
-                e(f"    accg[{2 * k}] += double(g.re); accg[{2 * k + 1}] += double(g.im);")
+                ck = self._cpx(f"c{k}")
+                if k in self.cp_pos and self.ncp:
+                    # charge -1 events: their own sums, after the polarisation ones
+                    j = self.nshape + self.nrho + 2 * self.cp_pos[k]
+                    e(f"    if (cc) {{ accs[{j}] += double(g.re); accs[{j + 1}] += double(g.im); }}")
+                    e(f"    else {{ accg[{2 * k}] += double(g.re); accg[{2 * k + 1}] += double(g.im); }}")
+                    ck = f"(cc ? {self._cpx(f'c{k}m')} : {ck})"
+                else:
+                    e(f"    accg[{2 * k}] += double(g.re); accg[{2 * k + 1}] += double(g.im);")
                 for si, p in enumerate(self.shape_res):
                     if p in c.inner:
-                        e(f"    cfmac(SR{si}, {self._cpx(f'c{k}')}, g);")
+                        e(f"    cfmac(SR{si}, {ck}, g);")
                 e("  }")
             for si, p in enumerate(self.shape_res):
                 if p in c.inner and self._first_chain(p) == ci:

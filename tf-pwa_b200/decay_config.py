@@ -258,12 +258,17 @@ class DecayConfig:
             for c in chains:
                 for d in c:
                     d.allow_cc = False
-        # decay_chain options (tf_pwa/config_loader/decay_config.py, the
-        # "decay_chain" section): none is compiled; CP-violating chain totals
-        # (is_cp) change the parameters, so refuse rather than ignore them
+        # decay_chain options: "$all: {is_cp: true}" gives every chain a
+        # CP-violating total, one value per event charge
+        # (tf_pwa/amp/core.py:1306-1329,1380-1390, tf_pwa/variable.py:
+        # 199-235,1715-1734); any other option is refused, not ignored
         for key, opts in (self.config.get("decay_chain") or {}).items():
-            if any(v for v in (opts or {}).values()):
+            opts = dict(opts or {})
+            is_cp = bool(opts.pop("is_cp", False))
+            if key != "$all" or any(v for v in opts.values()):
                 raise NotImplementedError(f"decay_chain options {opts} for {key}")
+            for c in chains:
+                c.is_cp = is_cp
         # kinematics options of the reference's preprocessor
         # (tf_pwa/config_loader/data.py:92-113): only the defaults are built
         dk = self.data_config
@@ -326,7 +331,10 @@ def init_params(group, vm, constrains=None):
     seen = set()
     for c in group:
         tname = c.params_head + "_total_0"
-        vm.add_complex_var(tname)
+        if getattr(c, "is_cp", False):
+            vm.add_cartesiancp_var(tname)
+        else:
+            vm.add_complex_var(tname)
         names["total"].append(tname)
         for d in c:
             if d in seen:
@@ -354,6 +362,9 @@ def init_params(group, vm, constrains=None):
     t = names["total"][fix_idx]
     vm.set_fix(t + "r", fix_val)
     vm.set_fix(t + "i", 0.0)
+    if t + "deltar" in vm.variables:  # fixed CP-violating total: no asymmetry
+        vm.set_fix(t + "deltar", 0.0)
+        vm.set_fix(t + "deltai", 0.0)
     # particle constraints: float: mg (config_loader.py:410-505)
     return names
 

@@ -365,6 +365,25 @@ class Engine:
             self._vtx_slots.append((d, self._vertex_chain[d.key()], sl))
         self._shape_slots = [(p, cidx[f"{p}.kappa_m"], cidx[f"{p}.inv_g0"])
                              for p in self.code.shape_res]
+        # CP-violating chain totals: coupling index, their delta parameters,
+        # the minus-charge constant slots, and per parameter its role
+        code = self.code
+        cp_tot = {ci: self.group[ci].params_head + "_total_0" for ci in code.cp_chains}
+        self._cp_coup = np.array([self._cn_index[cp_tot[ci]] for ci in code.cp_chains], np.int64)
+        self._cp_dr = [cp_tot[ci] + "deltar" for ci in code.cp_chains]
+        self._cp_di = [cp_tot[ci] + "deltai" for ci in code.cp_chains]
+        self._cp_t_re = np.array([cidx[f"t{ci}m.re"] for ci in code.cp_chains], np.int64)
+        self._cp_t_im = np.array([cidx[f"t{ci}m.im"] for ci in code.cp_chains], np.int64)
+        self._cp_cols = np.array(code.cp_cols, np.int64)
+        self._cp_c_re = np.array([cidx[f"c{k}m.re"] for k in code.cp_cols], np.int64)
+        self._cp_c_im = np.array([cidx[f"c{k}m.im"] for k in code.cp_cols], np.int64)
+        self._cp_param = {}
+        for ci in code.cp_chains:
+            cols = np.array([j for j, k in enumerate(code.cp_cols)
+                             if code.columns[k][0] == ci], np.int64)
+            for suf in ("r", "i", "deltar", "deltai"):
+                self._cp_param[cp_tot[ci] + suf] = (self._cn_index[cp_tot[ci]], suf, cols)
+        self._Jm = None
         self._pol_names = list(self.code.pol_names)
         self._pol_index = {n: i for i, n in enumerate(self._pol_names)}
         if self._pol_names:
@@ -595,6 +614,14 @@ class Engine:
         c = self.code
         r = np.fromiter((vals[n] for n in self._cn_r), float, len(self._cn_r))
         ph = np.fromiter((vals[n] for n in self._cn_i), float, len(self._cn_i))
+        cp = self._cp_coup
+        if len(cp):
+            # CP-violating totals: charge +1 takes (r + dr, i + di), -1 (r - dr, i - di)
+            dr = np.array([vals[n] for n in self._cp_dr])
+            di = np.array([vals[n] for n in self._cp_di])
+            rm, phm = r[cp] - dr, ph[cp] - di
+            r[cp] += dr
+            ph[cp] += di
         z = np.where(self._cn_polar, r * np.exp(1j * ph), r + 1j * ph)
         self._cvec, self._cr, self._cph = z, r, ph
         self._cv = dict(zip(self.coupling_names, z))
@@ -603,6 +630,19 @@ class Engine:
         C[1:2 * c.ncol:2] = self._ck.imag
         C[self._vg_re] = z[self._vg_src].real
         C[self._vg_im] = z[self._vg_src].imag
+        if len(cp):
+            zm = z.copy()
+            zm[cp] = np.where(self._cn_polar[cp], rm * np.exp(1j * phm), rm + 1j * phm)
+            self._cvec_m, self._cr_m, self._cph_m = zm, rm, phm
+            # column couplings without their CP total (the total's factor set to 1)
+            zr = z.copy()
+            zr[cp] = 1.0
+            self._ck_rest = np.prod(np.append(zr, 1.0 + 0j)[self._fac_idx], axis=1)
+            self._ck_m = np.prod(np.append(zm, 1.0 + 0j)[self._fac_idx], axis=1)
+            C[self._cp_t_re] = zm[cp].real
+            C[self._cp_t_im] = zm[cp].imag
+            C[self._cp_c_re] = self._ck_m[self._cp_cols].real
+            C[self._cp_c_im] = self._ck_m[self._cp_cols].imag
 
     def _fill_rho(self, C, vals):
         """Parent spin density matrix (polarised models) into its slots."""
@@ -650,7 +690,11 @@ class Engine:
             names_left = [(pi, n) for pi, n in enumerate(names) if n[:-1] not in cv]
         else:
             names_left = list(enumerate(names))
+        cp_rows = []
         for pi, n in names_left:
+            if n in self._cp_param:
+                cp_rows.append((pi, n))
+                continue
             if n in self._pol_index:
                 # polarisation: d f / d p = Re sum_ab T_ab d rho_ab / d p, T_ab
                 # the (a, b) parent-helicity product sums after the shape sums
@@ -695,6 +739,8 @@ class Engine:
                 # barrier factors through q0^2 of every vertex touching p
                 for k, kap in self._mass_dlog(vals, p.key()).items():
                     J[pi, k] += self._ck[k] * kap
+        if len(self._cp_coup):
+            J = self._cp_jacobian(J, names, cp_rows)
         if cached is None and key[1] is not None:
             # mass/width rows: J = kappa_k * c_k with kappa fixed per shape setting
             kap = np.zeros((P, c.ncol), np.complex128)
@@ -704,6 +750,58 @@ class Engine:
                                         where=self._ck != 0)
             self._jac_cache = {key: (kap, D.copy())}
         return J, D
+
+    def _cp_jacobian(self, J, names, cp_rows):
+        """Rows of the CP-violating totals' parameters (r, i, deltar,
+        deltai) for both charges, and ``self._Jm``: derivatives of the
+        minus-charge column couplings c_k^- of the CP columns.  A parameter
+        other than a CP total's enters c_k^- as it enters c_k^+, so its row
+        is the plus row times z^-/z^+ of the column's total."""
+        cp_cols = self._cp_cols
+        tot_of_col = np.empty(len(cp_cols), np.int64)  # coupling index of each CP column's total
+        for i, suf_cols in {v[0]: v[2] for v in self._cp_param.values()}.items():
+            tot_of_col[suf_cols] = i
+        zp_c, zm_c = self._cvec[tot_of_col], self._cvec_m[tot_of_col]
+        # (a chain switched off, z^+ = z^- = 0, has zero rows either way)
+        ratio = np.divide(zm_c, zp_c, out=np.zeros(len(zp_c), np.complex128), where=zp_c != 0)
+        Jm = J[:, cp_cols] * ratio[None, :]
+        for pi, n in enumerate(names):
+            if n not in self._cp_param:
+                continue
+            i, suf, cols = self._cp_param[n]
+            ks, _ = self._coup_cols[self.coupling_names[i]]
+            polar = bool(self._cn_polar[i])
+            j = list(self._cp_coup).index(i)
+            zp, zm = self._cvec[i], self._cvec_m[i]
+            sgn = -1.0 if suf.startswith("delta") else 1.0
+            # z = a e^{i phi}: dz/da = e^{i phi}, dz/dphi = i z (polar); 1, i (Cartesian)
+            if suf.endswith("r"):
+                dp = np.exp(1j * self._cph[i]) if polar else 1.0
+                dm = np.exp(1j * self._cph_m[j]) if polar else 1.0
+            else:
+                dp = 1j * zp if polar else 1j
+                dm = 1j * zm if polar else 1j
+            J[pi, :] = 0.0
+            J[pi, ks] = self._ck_rest[ks] * dp
+            Jm[pi, :] = 0.0
+            Jm[pi, cols] = self._ck_rest[cp_cols[cols]] * (sgn * dm)
+        self._Jm = Jm
+        return J
+
+    def grad_from_sums(self, J, D, s):
+        """d(sum)/d(parameters) from one event set's kernel sums ``s``:
+        2 Re J G over the columns, the lineshape/polarisation selectors D,
+        and for CP-violating totals 2 Re J^- G^- over the charge -1 sums."""
+        c = self.code
+        K = c.ncol
+        g = 2 * np.real(J @ (s[1:1 + 2 * K:2] + 1j * s[2:2 + 2 * K:2]))
+        ns = c.nshape + c.nrho
+        if ns:
+            g = g + D[:, :ns] @ s[1 + 2 * K:1 + 2 * K + ns]
+        if c.ncp and self._Jm is not None:
+            o = 1 + 2 * K + ns
+            g = g + 2 * np.real(self._Jm @ (s[o:o + c.ncp:2] + 1j * s[o + 1:o + c.ncp:2]))
+        return g
 
     # ------------------------------------------------------------ evaluate
     def eval_sums(self, C, precision=PLAIN_F64, mc=True, stream=None):
@@ -721,8 +819,9 @@ class Engine:
                                                     stream or 0), "pwa_eval_enqueue")
 
     def build_gram(self, C, stream=None):
-        if self.code.nrho:
-            raise PWAError("the column cache / Gram form does not apply to a polarised parent")
+        if self.code.nrho or self.code.cp_chains:
+            raise PWAError("the column cache / Gram form does not apply to a polarised parent "
+                           "or CP-violating totals")
         K = self.code.ncol
         out = np.zeros(2 * K * K)
         C = np.ascontiguousarray(C, np.float64)
@@ -761,13 +860,8 @@ class Engine:
             sm[2:2 + 2 * K:2] = Gm.imag
         else:
             sd, sm = self.eval_sums(C, precision, mc=True, stream=stream)
-        Gd = sd[1:1 + 2 * K:2] + 1j * sd[2:2 + 2 * K:2]
-        Gm = sm[1:1 + 2 * K:2] + 1j * sm[2:2 + 2 * K:2]
-        gd = 2 * np.real(J @ Gd)
-        gm = 2 * np.real(J @ Gm)
-        if self.code.nshape + self.code.nrho:
-            gd = gd + D @ sd[1 + 2 * K:]
-            gm = gm + D @ sm[1 + 2 * K:]
+        gd = self.grad_from_sums(J, D, sd)
+        gm = self.grad_from_sums(J, D, sm)
         f = self.mc_share
         return np.concatenate([[sd[0], sm[0] * f, self._sw], gd, gm * f])
 
@@ -811,8 +905,9 @@ class Engine:
             "pwa_set_param_layout")
 
     def cache_data(self, vals):
-        if self.code.nrho:
-            raise PWAError("the column cache / Gram form does not apply to a polarised parent")
+        if self.code.nrho or self.code.cp_chains:
+            raise PWAError("the column cache / Gram form does not apply to a polarised parent "
+                           "or CP-violating totals")
         """Evaluate and keep the data events' partial-wave columns."""
         C = np.ascontiguousarray(self.consts(vals))
         self._check(load_library().pwa_cache_data(self.h, _dptr(C), 0), "pwa_cache_data")

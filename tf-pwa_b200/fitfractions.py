@@ -32,23 +32,22 @@ def restricted_integral(eng, vals, names, chains, use_gram):
     v = dict(vals)
     for ci, t in enumerate(_total_names(eng.group)):
         if ci not in chains:
-            v[t + "r"] = 0.0
-            v[t + "i"] = 0.0
+            for suf in ("r", "i", "deltar", "deltai"):
+                if t + suf in v:
+                    v[t + suf] = 0.0
     C = eng.consts(v)
     J, D = eng.jacobian(v, names)
     used = np.array([ci in chains for ci, _ in code.columns])
     J[:, ~used] = 0.0
+    if code.ncp and eng._Jm is not None:
+        eng._Jm[:, ~used[eng._cp_cols]] = 0.0
     K = code.ncol
     if use_gram:
         ck = np.where(used, eng._ck, 0.0)
         Gm = np.conj(ck) @ eng._gram
         return float(np.real(Gm @ ck)), 2 * np.real(J @ Gm)
     _, sm = eng.eval_sums(C, PLAIN_F64, mc=True)
-    Gm = sm[1:1 + 2 * K:2] + 1j * sm[2:2 + 2 * K:2]
-    g = 2 * np.real(J @ Gm)
-    if code.nshape + code.nrho:
-        g = g + D @ sm[1 + 2 * K:]
-    return float(sm[0]), g
+    return float(sm[0]), eng.grad_from_sums(J, D, sm)
 
 
 def fit_fractions(eng, vm, res, inv_he=None, use_gram=None):

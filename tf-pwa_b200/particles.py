@@ -365,6 +365,7 @@ class DecayChain:
 
     def __init__(self, decays):
         self.decays = list(decays)
+        self.is_cp = False   # CP-violating total: one value per event charge
         cores = {d.core for d in self.decays}
         outs = set()
         for d in self.decays:

@@ -97,7 +97,9 @@ class Plan:
         # a moving parent's flight direction is the z axis of its decay
         self.random_z = getattr(group, "random_z", True)
         flips = any(getattr(d, "allow_cc", False) for c in group for d in c)
-        self.charge_index = self.field("charge") if self.use_charge and flips else None
+        cp_totals = any(getattr(c, "is_cp", False) for c in group)
+        self.charge_index = self.field("charge") if self.use_charge and (flips or cp_totals) \
+            else None
         self.swaps = []
         for k, sw in enumerate(pass_specs(group, getattr(group, "identical_particles", None),
                                           getattr(group, "cp_particles", None))):

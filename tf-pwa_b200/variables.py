@@ -51,6 +51,14 @@ class VarsManager:
             self.add_real_var(name + "i", value=fix_vals[1], trainable=False)
         self.complex_vars[name] = polar
 
+    def add_cartesiancp_var(self, name, polar=True):
+        """A complex coupling with a CP-violating part: r, i, deltar, deltai;
+        charge +-1 takes (r +- deltar, i +- deltai) (``tf_pwa/variable.py:
+        199-235,1715-1734``)."""
+        for suf in ("r", "i", "deltar", "deltai"):
+            self.add_real_var(name + suf, range_=(-1, 1))
+        self.complex_vars[name] = polar
+
     # -- fixing ------------------------------------------------------------
     def set_fix(self, name, value=None, unfix=False):
         if value is not None:
