@@ -1,6 +1,7 @@
 """The golden comparisons have teeth: a deliberate mistake planted in the
 oracle (on the CPU) -- a wrong swap sign, no helicity-coupling reversal for
-charge -1 events, an unpolarised density matrix, BWR in place of BWR2 -- moves
+charge -1 events, an unpolarised density matrix, BWR in place of BWR2, CP
+asymmetries of the chain totals dropped -- moves
 sum |A|^2 far outside the parity tolerance against the reference's values."""
 import copy
 
@@ -69,3 +70,9 @@ def test_lineshape_options(what, monkeypatch):
     else:
         monkeypatch.setattr(Particle, "width_norm_applies", lambda self: False)
     assert _max_rel(m, g, meta) > 1e-3
+
+
+def test_cp_violating_totals():
+    g, meta, dc, plan, m = _setup("lc2pkpi_cp")
+    v = {k: (0.0 if k.endswith(("deltar", "deltai")) else x) for k, x in meta["variables"].items()}
+    assert np.max(np.abs(m.pdf(g["fields_data"], v) / g["f_data"] - 1)) > 1e-3
