@@ -690,11 +690,9 @@ class Engine:
             names_left = [(pi, n) for pi, n in enumerate(names) if n[:-1] not in cv]
         else:
             names_left = list(enumerate(names))
-        cp_rows = []
         for pi, n in names_left:
             if n in self._cp_param:
-                cp_rows.append((pi, n))
-                continue
+                continue  # CP-total parameters: _cp_jacobian
             if n in self._pol_index:
                 # polarisation: d f / d p = Re sum_ab T_ab d rho_ab / d p, T_ab
                 # the (a, b) parent-helicity product sums after the shape sums
@@ -740,7 +738,7 @@ class Engine:
                 for k, kap in self._mass_dlog(vals, p.key()).items():
                     J[pi, k] += self._ck[k] * kap
         if len(self._cp_coup):
-            J = self._cp_jacobian(J, names, cp_rows)
+            J = self._cp_jacobian(J, names)
         if cached is None and key[1] is not None:
             # mass/width rows: J = kappa_k * c_k with kappa fixed per shape setting
             kap = np.zeros((P, c.ncol), np.complex128)
@@ -751,7 +749,7 @@ class Engine:
             self._jac_cache = {key: (kap, D.copy())}
         return J, D
 
-    def _cp_jacobian(self, J, names, cp_rows):
+    def _cp_jacobian(self, J, names):
         """Rows of the CP-violating totals' parameters (r, i, deltar,
         deltai) for both charges, and ``self._Jm``: derivatives of the
         minus-charge column couplings c_k^- of the CP columns.  A parameter
