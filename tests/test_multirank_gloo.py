@@ -4,11 +4,15 @@ Each rank holds half of the data and half of the MC events, computes its
 piece vector [S_data, S_mc * f, sum w, g_data, g_mc * f] (f = the rank's
 share of the MC weight), the ranks sum the vectors with one all-reduce, and
 ``combine_pieces`` turns the sum into the NLL and gradient.  The pieces here
-come from the FP64 oracle; the result must equal the single-process NLL and
-gradient of all events (the reference's golden values)."""
+come from the FP64 oracle (first test) or from the engine's own
+``local_pieces`` with its MC share and all-reduce hook, the sums taken from
+the generated kernel code run on the host (CP-violating and polarised
+models); the result must equal the single-process NLL and gradient of all
+events (the reference's golden values)."""
 import os
 
 import numpy as np
+import pytest
 
 
 def _pieces(rank, world, q):
@@ -88,3 +92,80 @@ def test_two_rank_gloo_combination():
     for rank, nll, grad, ref_nll, ref_grad in res:
         assert abs(nll - ref_nll) <= 1e-10 * abs(ref_nll)
         np.testing.assert_allclose(grad, ref_grad, rtol=1e-8, atol=1e-8 * np.abs(ref_grad).max())
+
+
+def _engine_pieces(rank, world, q, name, build_dir):
+    """Engine.local_pieces on this rank's half of the events (device sums
+    from the generated kernel code run on the host), summed over the ranks
+    by the engine's own dist_reduce hook."""
+    import sys
+
+    here = os.path.dirname(os.path.abspath(__file__))
+    sys.path.insert(0, here)
+    sys.path.insert(0, os.path.dirname(here))
+    import conftest  # noqa: F401
+    import torch
+    import torch.distributed as dist
+
+    from common import golden_data, load_golden, load_model
+    from hostexec import HostModel
+    from tf_pwa_b200.engine import PLAIN_F64, Engine
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    g, meta = load_golden(name)
+    dc, vm, plan = load_model(meta["config"])
+    eng = Engine(dc.decay_group, plan, vm, compile=False)
+    hm = HostModel(eng.code, build_dir)
+    xd, wd = golden_data(g, meta)
+    xm = g["fields_mc"]
+    wm_all = np.ones(xm.shape[1]) / xm.shape[1]
+    sd_idx = np.array_split(np.arange(xd.shape[1]), world)[rank]
+    sm_idx = np.array_split(np.arange(xm.shape[1]), world)[rank]
+    share = wm_all[sm_idx].sum()
+    x = np.concatenate([xd[:, sd_idx], xm[:, sm_idx]], 1)
+    w = np.concatenate([wd[sd_idx], wm_all[sm_idx] / share])
+    nd = len(sd_idx)
+    eng.eval_sums = lambda C, precision=PLAIN_F64, mc=True, stream=None: hm.sums(C, x, w, nd)
+    eng._sw = float(wd[sd_idx].sum())
+    eng.mc_share = share
+
+    def reduce(vec):
+        t = torch.as_tensor(vec)
+        dist.all_reduce(t)
+        return t.numpy()
+
+    eng.dist_reduce = reduce
+    nll, grad = eng.nll_grad(meta["variables"], meta["trainable"], PLAIN_F64)
+    dist.destroy_process_group()
+    q.put((rank, nll, grad, float(g["nll"]), np.asarray(g["grad"])))
+
+
+@pytest.mark.parametrize("name", ["lc2pkpi_cp", "lc2pkpi_pol"])
+def test_two_rank_engine_pieces(name, tmp_path):
+    """The engine's multi-rank path (local pieces, MC share, all-reduce,
+    combine) with the charge -1 and polarisation sums of the later model
+    options: equal to the reference's single-process NLL and gradient."""
+    import torch.multiprocessing as mp
+
+    from common import load_golden, load_model
+    from hostexec import HostModel
+    from tf_pwa_b200.engine import Engine
+
+    g, meta = load_golden(name)
+    dc, vm, plan = load_model(meta["config"])
+    HostModel(Engine(dc.decay_group, plan, vm, compile=False).code, str(tmp_path))  # build once
+    os.environ["MASTER_PORT"] = str(29600 + os.getpid() % 1000 + (name == "lc2pkpi_pol"))
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_engine_pieces, args=(r, 2, q, name, str(tmp_path)))
+             for r in range(2)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=300) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank, nll, grad, ref_nll, ref_grad in res:
+        assert abs(nll - ref_nll) <= 1e-9 * abs(ref_nll)
+        np.testing.assert_allclose(grad, ref_grad, rtol=1e-7, atol=1e-7 * np.abs(ref_grad).max())
