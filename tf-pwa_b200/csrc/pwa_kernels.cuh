@@ -1,5 +1,6 @@
 // Kernels around the generated ``model_amp`` / ``model_adj`` /
-// ``model_columns`` functions.
+// ``model_columns`` functions and ``model_f`` / ``model_seed`` (sum |A|^2,
+// density-matrix weighted for a polarised parent, and the adjoint seed).
 //
 // Compiled together with the model code by NVRTC (sm_100a).  Events live in
 // HBM as structure-of-arrays columns: XM[n_mass][ld] (FP64 invariant
