@@ -33,26 +33,40 @@ def test_config_files_to_reference_fields(tmp_path):
     assert np.all(np.asarray(bg.weight) == -meta["extra_data"]["bg_weight"])
 
 
-def test_weight_files_follow_the_event_files(tmp_path):
-    """Two data files and one weight file: each file's events take the next
-    slice of the weights; a ``negtive_idx`` pattern flips the sign."""
+def test_files_split_by_particle_and_weight_files(tmp_path):
+    """A list of files is one sample split by particle (file i holds the
+    next particles of dat_order, event by event; ``tf_pwa/data.py:300-365``);
+    a list of lists is one sample per inner list; the weight files'
+    values are cut to the events read; a ``negtive_idx`` pattern flips the
+    sign."""
     from tf_pwa_b200.api import ConfigLoader
 
     g, meta = load_golden("lc2pkpi")
     p4 = g["p4_data"]
-    half = p4.shape[0] // 2
-    files = []
-    for i, part in enumerate((p4[:half], p4[half:])):
-        f = tmp_path / f"data{i}.dat"
-        np.savetxt(f, part.reshape(-1, 4), fmt="%.17g")
-        files.append(str(f))
-    w = np.linspace(0.5, 1.5, p4.shape[0])
+    n = p4.shape[0]
+    fa, fb = tmp_path / "p_K.dat", tmp_path / "pi.dat"
+    np.savetxt(fa, p4[:, :2].reshape(-1, 4), fmt="%.17g")
+    np.savetxt(fb, p4[:, 2:].reshape(-1, 4), fmt="%.17g")
+    w = np.linspace(0.5, 1.5, n + 7)  # longer than the sample: cut to n
     wf = tmp_path / "w.dat"
     np.savetxt(wf, w, fmt="%.17g")
     dic = yaml.safe_load(open(os.path.join(CONFIGS, meta["config"])))
-    dic["data"] = {"data": files, "data_weight": str(wf), "negtive_idx": ["data"]}
+    dic["data"] = dict(dic["data"], data=[str(fa), str(fb)], data_weight=str(wf),
+                       negtive_idx=["data"])
     cfg = tmp_path / "config.yml"
     cfg.write_text(yaml.safe_dump(dic))
-    d0, d1 = ConfigLoader(str(cfg)).get_data("data")
-    np.testing.assert_array_equal(np.asarray(d0.weight), -w[:half])
-    np.testing.assert_array_equal(np.asarray(d1.weight), -w[half:])
+    (d,) = ConfigLoader(str(cfg)).get_data("data")
+    np.testing.assert_allclose(d.numpy_fields(), g["fields_data"], rtol=0, atol=1e-11)
+    np.testing.assert_array_equal(np.asarray(d.weight), -w[:n])
+    # two samples (list of lists), each a single file
+    half = n // 2
+    f1, f2 = tmp_path / "s1.dat", tmp_path / "s2.dat"
+    np.savetxt(f1, p4[:half].reshape(-1, 4), fmt="%.17g")
+    np.savetxt(f2, p4[half:].reshape(-1, 4), fmt="%.17g")
+    dic["data"] = dict(dic["data"], data=[[str(f1)], [str(f2)]])
+    dic["data"].pop("data_weight")
+    dic["data"].pop("negtive_idx")
+    cfg.write_text(yaml.safe_dump(dic))
+    d1, d2 = ConfigLoader(str(cfg)).get_data("data")
+    np.testing.assert_allclose(np.concatenate([d1.numpy_fields(), d2.numpy_fields()], 1),
+                               g["fields_data"], rtol=0, atol=1e-11)

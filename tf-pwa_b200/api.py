@@ -52,10 +52,14 @@ class EventData:
 
 
 def load_dat_file(fnames, n_particles):
-    """(N, n_particles, 4) momenta from ``.dat``/``.npy``/``.npz`` files."""
+    """(N, n_particles, 4) momenta from ``.dat``/``.npy``/``.npz`` files
+    (``tf_pwa/data.py:300-365``): the files of one list hold the same N
+    events split by particle -- file i has N x n_i rows, event by event, for
+    the next n_i particles of ``dat_order`` -- so a single file holds all
+    particles of each event in turn."""
     if isinstance(fnames, str):
         fnames = [fnames]
-    out = []
+    datas = []
     for fn in fnames:
         if fn.endswith(".npz"):
             a = np.load(fn)["arr_0"]
@@ -63,8 +67,16 @@ def load_dat_file(fnames, n_particles):
             a = np.load(fn)
         else:
             a = read_dat(fn)
-        out.append(np.reshape(a, (-1, n_particles, 4)))
-    return np.concatenate(out, 0)
+        datas.append(np.reshape(a, (-1, 4)))
+    n_total = sum(d.shape[0] for d in datas)
+    if n_total % n_particles != 0:
+        raise ValueError(f"number of data find {n_total}/{n_particles}")
+    n_data = n_total // n_particles
+    parts = [d.reshape(n_data, d.shape[0] // n_data, 4) for d in datas]
+    out = np.concatenate(parts, 1)
+    if out.shape[1] != n_particles:
+        raise ValueError(f"files hold {out.shape[1]} particles per event, expected {n_particles}")
+    return out
 
 
 class AmplitudeModel:
@@ -379,6 +391,9 @@ class ConfigLoader:
             return None
         if isinstance(files, str):
             files = [files]
+        # a list of files is one sample split by particle; a list of lists,
+        # one sample per inner list (tf_pwa/config_loader/data.py:415-421)
+        groups = files if files and isinstance(files[0], (list, tuple)) else [files]
         # weight = sign * (scalar ``<idx>_weight`` or the concatenated weight
         # files cut to the events read), sign -1 for indices matching
         # ``negtive_idx`` (default "bg*")
@@ -395,8 +410,8 @@ class ConfigLoader:
             cfile = np.concatenate([np.loadtxt(self._path(x)).reshape(-1)
                                     for x in (ckey if isinstance(ckey, list) else [ckey])])
         ret, off = [], 0
-        for f in files:
-            p4 = self.load_p4([f])
+        for grp in groups:
+            p4 = self.load_p4(list(grp))
             n = p4.shape[0]
             if wfile is not None:
                 w = wfile[off:off + n]
