@@ -95,3 +95,29 @@ def test_fit_errors_fractions(host_engine, tmp_path, precision):
     inter = [v for k, v in frac.items() if not isinstance(k, str)]
     assert abs(sum(singles) + sum(inter) - 1.0) < 1e-9
     assert all(np.isfinite(e) for e in err_frac.values())
+
+
+def test_fit_arguments_as_reference(host_engine, tmp_path, capsys):
+    """ConfigLoader.fit takes the reference's arguments: the initial NLL is
+    printed, callback sees every iteration, grad_scale changes the
+    minimiser's scale but not the minimum reported, jac=False differences
+    the NLL, inmc / reweight are refused."""
+    from tf_pwa_b200.api import ConfigLoader
+
+    cfg, g, meta = _config(tmp_path, "d2kpipi")
+    cl = ConfigLoader(cfg)
+    cl.set_params(meta["variables"])
+    fcn = cl.get_fcn()
+    x0 = list(cl.vm.get_all_val())
+    seen = []
+    fr = cl.fit(fcn=fcn, callback=lambda xk: seen.append(np.array(xk)))
+    assert "initial NLL" in capsys.readouterr().out
+    assert seen and fr.success
+    cl.vm.set_all(x0)
+    fr2 = cl.fit(fcn=fcn, grad_scale=10.0, print_init_nll=False)
+    assert abs(fr2.min_nll - fr.min_nll) < 1e-6
+    cl.vm.set_all(x0)
+    fr3 = cl.fit(fcn=fcn, jac=False, print_init_nll=False)
+    assert abs(fr3.min_nll - fr.min_nll) < 1e-4
+    with pytest.raises(NotImplementedError):
+        cl.fit(fcn=fcn, reweight=True)

@@ -476,13 +476,24 @@ class ConfigLoader:
             json.dump(self.get_params(), f, indent=2)
 
     # -- fit ----------------------------------------------------------------
-    def fit(self, data=None, phsp=None, bg=None, batch=65000, method="BFGS", maxiter=None,
-            gtol=1e-3, fcn=None, precision=None):
-        """BFGS on FCN.nll_grad (``tf_pwa/fit.py:189-419``)."""
+    def fit(self, data=None, phsp=None, bg=None, inmc=None, batch=65000, method="BFGS",
+            check_grad=False, improve=False, reweight=False, maxiter=None, jac=True,
+            print_init_nll=True, callback=None, grad_scale=1.0, gtol=1e-3, fcn=None,
+            precision=None):
+        """BFGS on FCN.nll_grad (``config_loader.py:745-801``,
+        ``tf_pwa/fit.py:189-419``): same arguments; the objective and its
+        gradient are multiplied by ``grad_scale`` for the minimiser (gtol
+        too), ``jac=False`` lets scipy difference the NLL, ``callback`` goes
+        to scipy.  ``inmc`` samples and ``reweight`` are not supported;
+        ``check_grad`` and ``improve`` are accepted and have no effect."""
         from scipy.optimize import minimize
 
+        if inmc is not None or reweight:
+            raise NotImplementedError("inmc samples / reweight")
         if fcn is None:
             fcn = self.get_fcn(None if data is None else [data, phsp, bg], batch, precision)
+        if print_init_nll:
+            print("initial NLL: ", fcn.nll_grad()[0])
         y0 = np.array(self.vm.get_all_val())
         maxiter = maxiter or max(100 * len(y0), 2000)
         # bounded variables are fitted through their transform
@@ -502,17 +513,26 @@ class ConfigLoader:
             g = np.array(g, dtype=float)
             for i, b in bounds.items():
                 g[i] *= b.dydx(x[i])
-            return nll, g
+            return grad_scale * nll, grad_scale * g
 
         x0 = y0.copy()
         for i, b in bounds.items():
             x0[i] = b.y2x(y0[i])
         t0 = time.time()
-        res = minimize(fg, x0, jac=True, method=method, options={"maxiter": maxiter, "gtol": gtol})
+        opts = {"maxiter": maxiter, "gtol": gtol * grad_scale}
+        if jac:
+            res = minimize(fg, x0, jac=True, method=method, options=opts, callback=callback)
+        else:
+            res = minimize(lambda x: fg(x)[0], x0, method=method, options=opts,
+                           callback=callback)
         self.vm.set_all(list(to_y(res.x)))
         self.vm.std_polar_all()
-        fr = FitResult(self.get_params(), fcn, res.fun, ndf=len(x0), success=bool(res.success),
-                       message=str(res.message), hess_inv=getattr(res, "hess_inv", None),
+        hess_inv = getattr(res, "hess_inv", None)
+        if hess_inv is not None and not isinstance(hess_inv, np.ndarray):
+            hess_inv = None  # (L-BFGS-B returns an operator)
+        fr = FitResult(self.get_params(), fcn, res.fun / grad_scale, ndf=len(x0),
+                       success=bool(res.success), message=str(res.message),
+                       hess_inv=None if hess_inv is None else hess_inv * grad_scale,
                        n_call=fcn.n_call)
         fr.time = time.time() - t0
         self._fcn = fcn
