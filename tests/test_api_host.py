@@ -121,3 +121,40 @@ def test_fit_arguments_as_reference(host_engine, tmp_path, capsys):
     assert abs(fr3.min_nll - fr.min_nll) < 1e-4
     with pytest.raises(NotImplementedError):
         cl.fit(fcn=fcn, reweight=True)
+
+
+def test_force_pos_def():
+    """Inverse of a positive-definite Hessian unchanged; a small negative
+    eigenvalue (rounding) lifted to positive; a strongly indefinite matrix
+    turned into a positive-definite error matrix."""
+    from tf_pwa_b200.api import force_pos_def
+
+    rng = np.random.default_rng(3)
+    q, _ = np.linalg.qr(rng.normal(size=(5, 5)))
+    h = q @ np.diag([5.0, 3.0, 2.0, 1.0, 0.5]) @ q.T
+    np.testing.assert_allclose(force_pos_def(h), np.linalg.inv(h), rtol=1e-10, atol=1e-12)
+    h2 = q @ np.diag([5.0, 3.0, 2.0, 1.0, -1e-7]) @ q.T
+    assert np.all(np.linalg.eigvalsh(force_pos_def(h2)) > 0)
+    h3 = q @ np.diag([5.0, 3.0, 2.0, 1.0, -2.0]) @ q.T
+    v3 = force_pos_def(h3)
+    assert np.all(np.diag(v3) > 0)
+    d = np.sqrt(np.diag(v3))
+    assert np.all(np.linalg.eigvalsh(v3 / np.outer(d, d)) > 0)
+
+
+def test_params_error_arguments(host_engine, tmp_path):
+    """get_params_error with the reference's arguments: errors stored on the
+    fit result, using_cached reuses the inverse Hessian."""
+    from tf_pwa_b200.api import ConfigLoader
+
+    cfg, g, meta = _config(tmp_path, "d2kpipi")
+    cl = ConfigLoader(cfg)
+    cl.set_params(meta["variables"])
+    fcn = cl.get_fcn()
+    fr = cl.fit(fcn=fcn, print_init_nll=False)
+    err = cl.get_params_error(fr, fcn=fcn)
+    assert fr.error == err
+    assert cl.get_params_error(using_cached=True) == err
+    err2 = cl.get_params_error(fcn=fcn, force_pos=False)
+    for k in err:
+        assert err2[k] == pytest.approx(err[k], rel=1e-6)

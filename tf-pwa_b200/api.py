@@ -79,6 +79,37 @@ def load_dat_file(fnames, n_particles):
     return out
 
 
+def force_pos_def(h):
+    """Inverse of the Hessian ``h``, made positive definite where rounding
+    or a poorly constrained direction left it indefinite
+    (``tf_pwa/applications.py:206-276``): a small negative eigenvalue
+    (above -1e-5 of the largest) is lifted by 1.1 times its size before
+    inverting; a strongly indefinite matrix gets the diagonal correction of
+    Minuit2's MnPosDef on its pseudo-inverse (error diagonal raised to be
+    positive, then scaled until the correlation matrix is positive
+    definite)."""
+    h = np.asarray(h, np.float64)
+    e, v = np.linalg.eig(h)
+    inv = np.linalg.pinv(h)
+    e_min, e_max = float(np.min(e.real)), float(np.max(np.abs(e)))
+    if e_min > 0:
+        return inv
+    if e_min > -1e-5 * e_max:
+        e2 = np.where(e.real < 0, e - 1.1 * e_min, e)
+        return np.linalg.inv(np.real(v @ np.diag(e2) @ np.linalg.inv(v)))
+    eps2 = max(1e-6, 2.0 * np.sqrt(np.finfo(np.float64).eps))
+    err = inv.copy()
+    d = np.diag(err)
+    if d.min() <= 0:
+        err = err + np.eye(len(d)) * (0.5 + eps2 - d.min())
+    d = np.diag(err)
+    w = np.linalg.eigvalsh(err / np.sqrt(np.outer(d, d)))
+    pmin, pmax = float(w.min()), max(float(np.abs(w).max()), 1.0)
+    if pmin > eps2 * pmax:
+        return err
+    return err + np.diag(d * (0.001 * pmax - pmin))
+
+
 class AmplitudeModel:
     """sum |A|^2 of the model per event (``AbsPDF.__call__``)."""
 
@@ -536,23 +567,34 @@ class ConfigLoader:
                        n_call=fcn.n_call)
         fr.time = time.time() - t0
         self._fcn = fcn
+        self.fit_params = fr
         return fr
 
-    def get_params_error(self, params=None, data=None, phsp=None, bg=None, batch=10000,
-                         fcn=None):
-        """Errors from the inverse Hessian in FP64 (``applications.py:280-309``)."""
+    def get_params_error(self, params=None, data=None, phsp=None, bg=None, inmc=None,
+                         batch=10000, using_cached=False, method=None, force_pos=True,
+                         correct_params=None, fcn=None):
+        """Errors from the inverse Hessian in FP64 (``config_loader.py:814-873``,
+        ``applications.py:249-309``): with ``using_cached`` the last inverse
+        Hessian is reused; otherwise the Hessian (differenced adjoint
+        gradients) is inverted -- made positive definite first with
+        ``force_pos`` (``force_pos_def``), else by pseudo-inverse.  The
+        errors are also stored on the last fit's result."""
+        if inmc is not None or correct_params:
+            raise NotImplementedError("inmc samples / corrected parameters")
         if params is not None:
             self.set_params(params.params if isinstance(params, FitResult) else params)
-        fcn = fcn or getattr(self, "_fcn", None) or self.get_fcn(
-            None if data is None else [data, phsp, bg])
-        _, _, H = fcn.nll_grad_hessian()
-        try:
-            inv = np.linalg.inv(H)
-        except np.linalg.LinAlgError:
-            inv = np.linalg.pinv(H)
-        self.inv_he = inv
-        err = np.sqrt(np.abs(np.diag(inv)))
-        return dict(zip(self.vm.trainable_vars, err))
+        if using_cached and getattr(self, "inv_he", None) is not None:
+            inv = self.inv_he
+        else:
+            fcn = fcn or getattr(self, "_fcn", None) or self.get_fcn(
+                None if data is None else [data, phsp, bg])
+            _, _, H = fcn.nll_grad_hessian()
+            inv = force_pos_def(H) if force_pos else np.linalg.pinv(H)
+            self.inv_he = inv
+        err = dict(zip(self.vm.trainable_vars, np.sqrt(np.abs(np.diag(inv)))))
+        if getattr(self, "fit_params", None) is not None:
+            self.fit_params.set_error(err)
+        return err
 
     # -- toys and phase space (``tf_pwa/config_loader/sample.py``) ------------
     def _toy_engine(self):
