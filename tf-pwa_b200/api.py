@@ -478,7 +478,10 @@ class ConfigLoader:
             f = np.concatenate([d.fields for d in lst], 1)
         return EventData(f, np.concatenate([d.weight for d in lst]))
 
-    def get_fcn(self, all_data=None, batch=65000, precision=None, gram=None):
+    def get_fcn(self, all_data=None, batch=65000, vm=None, name="", precision=None, gram=None):
+        """FCN of the config's (or the given) data, phsp, bg samples
+        (``config_loader.py:659-720``); ``vm`` and ``name`` are accepted as in
+        the reference (the loader's own parameters are used)."""
         if all_data is None:
             data, phsp, bg, _ = self.get_all_data()
         else:
@@ -522,7 +525,8 @@ class ConfigLoader:
         if inmc is not None or reweight:
             raise NotImplementedError("inmc samples / reweight")
         if fcn is None:
-            fcn = self.get_fcn(None if data is None else [data, phsp, bg], batch, precision)
+            fcn = self.get_fcn(None if data is None else [data, phsp, bg], batch,
+                               precision=precision)
         if print_init_nll:
             print("initial NLL: ", fcn.nll_grad()[0])
         y0 = np.array(self.vm.get_all_val())
