@@ -158,3 +158,25 @@ def test_params_error_arguments(host_engine, tmp_path):
     err2 = cl.get_params_error(fcn=fcn, force_pos=False)
     for k in err:
         assert err2[k] == pytest.approx(err[k], rel=1e-6)
+
+
+def test_params_files(tmp_path):
+    """save_params / set_params round trip (the fit result's "value" layout
+    too), with neglect_params left untouched."""
+    import json
+
+    from tf_pwa_b200.api import ConfigLoader
+
+    cl = ConfigLoader(os.path.join(CONFIGS, "d2kpipi.yml"))
+    vals = cl.get_params()
+    f = tmp_path / "p.json"
+    cl.save_params(str(f))
+    k0, k1 = list(cl.vm.trainable_vars)[:2]
+    cl.vm.set(k0, 0.123)
+    cl.vm.set(k1, 0.456)
+    cl.set_params(str(f), neglect_params=[k1])
+    assert cl.vm.get(k0) == vals[k0] and cl.vm.get(k1) == 0.456
+    g = tmp_path / "fit.json"
+    g.write_text(json.dumps({"value": {k0: 0.789}, "error": {}}))
+    cl.set_params(str(g))
+    assert cl.vm.get(k0) == 0.789

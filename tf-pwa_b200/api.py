@@ -502,7 +502,9 @@ class ConfigLoader:
             with open(params) as f:
                 params = json.load(f)
             params = params.get("value", params)
-        self.vm.set_all({k: v for k, v in params.items() if k in self.vm.variables})
+        skip = set(neglect_params or [])
+        self.vm.set_all({k: v for k, v in params.items()
+                         if k in self.vm.variables and k not in skip})
         return True
 
     def save_params(self, file_name):
