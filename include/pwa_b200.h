@@ -58,7 +58,10 @@ enum { PWA_PLAIN_F64 = 0, PWA_MIXED_F32 = 1 };
  * headers and compiles for sm_100a on the current device.
  * n_mass / n_angle: number of FP64 mass / angle columns of an event;
  * ncol, nout, nshape, nconst, nf: model sizes matching the source (nf =
- * structurally non-zero (column, helicity) pairs, PWA_NF of the source).
+ * structurally non-zero (column, helicity) pairs, PWA_NF of the source;
+ * nshape = every accumulator past the 2*ncol column sums: lineshape,
+ * polarisation and charge -1 column sums, so that 1 + 2*ncol + nshape equals
+ * the source's PWA_NACC, else PWA_ERR_ARG).
  * tpb: threads per block of the fused kernels (32..1024, multiple of 32). */
 int pwa_plan_create(const char* src, size_t src_len, int n_mass, int n_angle, int ncol, int nout,
                     int nshape, int nconst, int nf, int tpb, pwa_plan** out);

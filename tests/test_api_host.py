@@ -180,3 +180,24 @@ def test_params_files(tmp_path):
     g.write_text(json.dumps({"value": {k0: 0.789}, "error": {}}))
     cl.set_params(str(g))
     assert cl.vm.get(k0) == 0.789
+
+
+def test_fcn_derivative_methods(host_engine, tmp_path):
+    """FCN.get_nll / get_grad / grad_hessp agree with nll_grad and the
+    differenced Hessian (Hessian-vector product within 1e-6 of H p)."""
+    from tf_pwa_b200.api import ConfigLoader
+
+    cfg, g, meta = _config(tmp_path, "d2kpipi_float")
+    cl = ConfigLoader(cfg)
+    cl.set_params(meta["variables"])
+    fcn = cl.get_fcn()
+    x = np.array(cl.vm.get_all_val())
+    nll, grad = fcn.nll_grad(x)
+    assert fcn.get_nll(x) == nll
+    np.testing.assert_array_equal(fcn.get_grad(x), grad)
+    _, _, H = fcn.nll_grad_hessian(x)
+    p = np.random.default_rng(2).normal(size=len(x))
+    g0, hp = fcn.grad_hessp(x, p)
+    np.testing.assert_array_equal(g0, grad)
+    np.testing.assert_allclose(hp, H @ p, rtol=1e-6, atol=1e-6 * np.abs(H @ p).max())
+    np.testing.assert_array_equal(np.array(cl.vm.get_all_val()), x)

@@ -72,3 +72,22 @@ def test_unsupported_options_raise():
     dc = DecayConfig(dic)
     with pytest.raises(NotImplementedError):
         ModelCode(dc.decay_group, Plan(dc.decay_group))
+
+
+@pytest.mark.parametrize("cfg", ["lc2pkpi_cp.yml", "lc2pkpi_pol.yml", "d2kpipi_shapes.yml",
+                                 "lc2pkpi_cc.yml"])
+def test_plan_accumulator_count(cfg):
+    """The accumulator count the engine hands the native plan (1 + 2*ncol +
+    nshape argument) equals the generated source's PWA_NACC, charge -1 and
+    polarisation sums included."""
+    import re
+
+    from tf_pwa_b200.engine import Engine
+
+    dc, vm, plan = load_model(cfg)
+    eng = Engine(dc.decay_group, plan, vm, compile=False)
+    c = eng.code
+    nacc = int(re.search(r"#define PWA_NACC (\d+)", eng.src).group(1))
+    assert nacc == 1 + 2 * c.ncol + c.nshape + c.nrho + c.ncp
+    if cfg == "lc2pkpi_cp.yml":
+        assert c.ncp > 0

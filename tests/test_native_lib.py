@@ -75,6 +75,13 @@ def test_argument_errors_without_a_device():
     rc = lib.pwa_plan_create(src, len(src), 1, 1, 1, 1, 0, 1, 1, 100, ctypes.byref(h))
     assert rc == 1
     lib.pwa_plan_destroy(h)
+    # the accumulator count must equal the source's PWA_NACC (1 + 2*2 + 3 = 8)
+    src = b"#define PWA_NACC 9\n"
+    h = ctypes.c_void_p()
+    rc = lib.pwa_plan_create(src, len(src), 1, 1, 2, 2, 3, 1, 1, 128, ctypes.byref(h))
+    assert rc == 1
+    assert b"PWA_NACC" in lib.pwa_last_error(h)
+    lib.pwa_plan_destroy(h)
     out = (ctypes.c_double * 4)()
     assert lib.pwa_hessian_cached(None, out, 1.0, 1e-3, None, out, out, out) == 1
     assert lib.pwa_last_error(None)

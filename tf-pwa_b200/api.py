@@ -244,6 +244,31 @@ class FCN:
         self.cached_nll = nll
         return float(nll), g
 
+    def get_nll(self, x=None):
+        return self.get_nll_grad(x)[0]
+
+    def get_grad(self, x=None):
+        return self.get_nll_grad(x)[1]
+
+    def grad_hessp(self, x, p, batch=None, step=None):
+        """(gradient at x, Hessian times p) (``tf_pwa/model/model.py:
+        1268-1275``): the product by a 4-point central difference of the
+        adjoint gradient along p; the step along p moves no parameter by
+        more than ``step * max(|x_i|, 1e-2)``, the per-parameter step of
+        ``nll_grad_hessian``."""
+        x0 = np.array(x if x is not None else self.vm.get_all_val(), dtype=np.float64)
+        p = np.asarray(p, dtype=np.float64)
+        if step is None:
+            step = 1e-4 if self.precision == PLAIN_F64 else 1e-2
+        pn = float(np.max(np.abs(p) / np.maximum(np.abs(x0), 1e-2)))
+        _, g0 = self.get_nll_grad(x0)
+        if pn == 0.0:
+            return g0, np.zeros_like(g0)
+        eps = step / pn
+        gs = [np.asarray(self.get_nll_grad(x0 + s_ * eps * p)[1]) for s_ in (-2, -1, 1, 2)]
+        self._set(x0)
+        return g0, (gs[0] - 8 * gs[1] + 8 * gs[2] - gs[3]) / (12 * eps)
+
     def __call__(self, x=None):
         nll, _ = self.get_nll_grad(x)
         self.cached_nll = nll

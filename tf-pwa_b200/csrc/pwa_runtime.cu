@@ -309,6 +309,19 @@ int pwa_plan_create(const char* src, size_t src_len, int n_mass, int n_angle, in
   h->nshape = nshape;
   h->nconst = nconst;
   h->nacc = 1 + 2 * ncol + nshape;
+  {
+    // the per-block partial sums are laid out with this count: it must be the
+    // source's own accumulator count, or the kernels write past the buffer
+    const std::string text(src, src_len);
+    const size_t at = text.find("#define PWA_NACC ");
+    if (at == std::string::npos ||
+        std::strtol(text.c_str() + at + 17, nullptr, 10) != (long)h->nacc) {
+      *out = h;
+      return set_err(h, PWA_ERR_ARG,
+                     "accumulator count 1 + 2*ncol + nshape = " + std::to_string(h->nacc) +
+                         " does not match the source's PWA_NACC");
+    }
+  }
   h->nf = nf;
   h->tpb = tpb;
   *out = h;

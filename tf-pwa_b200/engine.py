@@ -197,7 +197,7 @@ class Engine:
         h = ctypes.c_void_p()
         src = self.src.encode()
         rc = lib.pwa_plan_create(src, len(src), len(c.mass_fields), len(c.angle_fields), c.ncol,
-                                 c.nout, c.nshape + c.nrho, len(c.consts), c.nf, self.tpb,
+                                 c.nout, c.nshape + c.nrho + c.ncp, len(c.consts), c.nf, self.tpb,
                                  ctypes.byref(h))
         if rc != 0:
             msg = lib.pwa_last_error(h).decode(errors="replace")
