@@ -201,3 +201,76 @@ def test_fcn_derivative_methods(host_engine, tmp_path):
     np.testing.assert_array_equal(g0, grad)
     np.testing.assert_allclose(hp, H @ p, rtol=1e-6, atol=1e-6 * np.abs(H @ p).max())
     np.testing.assert_array_equal(np.array(cl.vm.get_all_val()), x)
+
+
+def test_refresh_vars_ranges():
+    """VarsManager.refresh_vars draws free couplings in their ranges, keeps
+    fixed ones, sets init values, and draws bounded parameters inside the
+    bounds (``tf_pwa/variable.py:329-420``)."""
+    from tf_pwa_b200.variables import VarsManager
+
+    vm = VarsManager(rng=np.random.default_rng(5))
+    vm.add_complex_var("a")
+    vm.add_complex_var("b", polar=False)
+    vm.add_complex_var("c", trainable=False)
+    vm.add_real_var("m", value=1.0)
+    vm.add_real_var("g", value=0.1)
+    vm.add_real_var("h", value=0.2)
+    vm.add_real_var("k", value=0.3)
+    vm.set_fix("k")
+    bounds = {"g": (0.05, 0.2), "h": (0.1, None), "k": (0.0, 1.0)}
+    for _ in range(50):
+        vm.refresh_vars(init_val={"m": [1.0, 0.01]}, bound_dic=bounds)
+        v = vm.variables
+        assert 0 <= v["ar"] <= 2 and -np.pi <= v["ai"] <= np.pi
+        assert -1 <= v["br"] <= 1 and -1 <= v["bi"] <= 1
+        assert (v["cr"], v["ci"]) == (1.0, 0.0)
+        assert 0.9 < v["m"] < 1.1 and 0.05 <= v["g"] <= 0.2 and v["h"] >= 0.1
+        assert v["k"] == 0.3
+    vm.refresh_vars(init_val={"m": 2.5}, bound_dic={})
+    assert vm.variables["m"] == 2.5
+
+
+def test_loader_fit_helpers(host_engine, tmp_path):
+    """get_ndf, reinit_params, get_phsp_noeff, cal_signal_yields and
+    likelihood_profile of the loader (``tf_pwa/config_loader/
+    config_loader.py:180-188,722-725,803-812,918-993``)."""
+    import warnings
+
+    from tf_pwa_b200.api import ConfigLoader
+
+    cfg, g, meta = _config(tmp_path, "d2kpipi_float")
+    cl = ConfigLoader(cfg, seed=3)
+    cl.set_params(meta["variables"])
+    assert cl.get_ndf() == len(cl.vm.trainable_vars)
+    # floated masses/widths keep their configured values, couplings move
+    floated = dict(cl.init_value)
+    assert floated
+    before = cl.get_params()
+    cl.reinit_params()
+    after = cl.get_params()
+    for k, v in floated.items():
+        assert after[k] == v
+    assert any(after[k] != before[k] for k in cl.vm.trainable_vars if k not in floated)
+    cl.set_params(before)
+    with warnings.catch_warnings(record=True) as w:
+        warnings.simplefilter("always")
+        ph = cl.get_phsp_noeff()
+    assert ph.n == g["fields_mc"].shape[1] and w
+    cl.fit(print_init_nll=False)
+    cl.get_params_error()
+    frac, err = cl.cal_fitfractions()
+    (ys,) = cl.cal_signal_yields()
+    n = g["p4_data"].shape[0]
+    for k, f in frac.items():
+        assert ys[k][0] == pytest.approx(f * n, rel=1e-12)
+        assert ys[k][1] == pytest.approx(np.hypot(n * err[k], np.sqrt(n) * f), rel=1e-12)
+    # profile in one coupling magnitude: the fitted point is the lowest
+    p0 = cl.get_params()
+    var = next(k for k in cl.vm.trainable_vars if k.endswith("r") and k not in floated)
+    v0 = p0[var]
+    vals, nlls = cl.likelihood_profile(var, v0 - 0.1 * abs(v0), v0 + 0.1 * abs(v0), N=2)
+    assert len(vals) == len(nlls) >= 2 and np.all(np.diff(vals) > 0)
+    assert min(nlls) == pytest.approx(nlls[vals.index(v0)], abs=1e-4)
+    assert var in cl.vm.trainable_vars
+    assert cl.get_params()[var] == v0

@@ -22,6 +22,7 @@ import json
 import os
 import re
 import time
+import warnings
 
 import numpy as np
 
@@ -393,6 +394,10 @@ class ConfigLoader:
         self.bound_dic = float_particles(self.decay_group, self.vm, self._names,
                                          self.decay_config.particle_property)
         self.plan = Plan(self.decay_group, self.config.get("data", {}).get("dat_order"))
+        # configured values of the floated masses/widths: kept by reinit_params
+        self.init_value = {n: self.vm.variables[n] for kind in ("mass", "width")
+                           for n in self._names.get(kind, {}).values()
+                           if n in self.vm.trainable_vars}
         self.precision = precision
         self._amp = None
         self._data = {}
@@ -601,6 +606,52 @@ class ConfigLoader:
         self.fit_params = fr
         return fr
 
+    def get_ndf(self):
+        """Number of free parameters (``config_loader.py:722-725``)."""
+        return len(self.vm.trainable_vars)
+
+    def reinit_params(self):
+        """New random starting point (``config_loader.py:803-805``)."""
+        self.vm.refresh_vars(init_val=self.init_value, bound_dic=self.bound_dic)
+
+    def fitNtimes(self, N, *args, **kwargs):
+        """N fits from random starting points, each result's parameters
+        printed as JSON (``config_loader.py:807-812``); returns the results."""
+        out = []
+        for _ in range(N):
+            self.reinit_params()
+            fr = self.fit(*args, **kwargs)
+            print(json.dumps(fr.params, indent=2), flush=True)
+            out.append(fr)
+        return out
+
+    def likelihood_profile(self, var, var_min, var_max, N=100):
+        """Profile of the minimum NLL in ``var`` (``config_loader.py:
+        964-993``): ``var`` fixed at steps of (var_max - var_min)/N upward
+        from its current value to var_max, then downward to var_min, a fit
+        of the other parameters at each; returns (values, NLLs) in
+        ascending order and restores the parameters and the free flag."""
+        params = self.get_params()
+        delta = (var_max - var_min) / N
+        unfix = var in self.vm.trainable_vars
+        up_v, up_n, down_v, down_n = [], [], [], []
+        v = params[var]
+        while v <= var_max:
+            self.vm.set_fix(var, v)
+            up_v.append(v)
+            up_n.append(self.fit(print_init_nll=False).min_nll)
+            v += delta
+        self.set_params(params)
+        v = params[var] - delta
+        while v >= var_min:
+            self.vm.set_fix(var, v)
+            down_v.append(v)
+            down_n.append(self.fit(print_init_nll=False).min_nll)
+            v -= delta
+        self.set_params(params)
+        self.vm.set_fix(var, params[var], unfix=unfix)
+        return down_v[::-1] + up_v, down_n[::-1] + up_n
+
     def get_params_error(self, params=None, data=None, phsp=None, bg=None, inmc=None,
                          batch=10000, using_cached=False, method=None, force_pos=True,
                          correct_params=None, fcn=None):
@@ -713,3 +764,39 @@ class ConfigLoader:
         frac, err, _ = fit_fractions(fcn.eng, self.vm, res, getattr(self, "inv_he", None),
                                      use_gram=fcn.use_gram)
         return frac, err
+
+    def get_phsp_noeff(self):
+        """The ``phsp_noeff`` sample, else the first ``phsp`` one
+        (``config_loader.py:180-188``)."""
+        if "phsp_noeff" in self.config.get("data", {}):
+            d = self.get_data("phsp_noeff")
+            assert len(d) == 1
+            return d[0]
+        warnings.warn("No data file as 'phsp_noeff', using the first 'phsp' file instead.")
+        return self.get_data("phsp")[0]
+
+    def cal_signal_yields(self, params={}, mcdata=None, batch=25000):
+        """Signal yield of each fit-fraction term, with error
+        (``config_loader.py:918-962``): N = data events - bg_weight * bg
+        events, error sqrt(N_data + bg_weight^2 N_bg) (sqrt(N_data) without
+        background; 0 for ``extended`` fits; per-event bg weights summed); yield_i = frac_i N, error
+        sqrt((N err_frac_i)^2 + (err_N frac_i)^2).  One dict per data
+        sample."""
+        frac, err = self.cal_fitfractions(params, mcdata, batch=batch)
+        dcfg = self.config.get("data", {})
+        data, bg = self.get_data("data"), self.get_data("bg")
+        out = []
+        for k, d in enumerate(data):
+            n_data = d.n
+            if bg is None:
+                n, n_err = float(n_data), float(np.sqrt(n_data))
+            else:
+                # bg rows carry weight -bg_weight: N_data - w N_bg, N_data + w^2 N_bg
+                wb = np.asarray(bg[k].weight, dtype=np.float64)
+                n, n_err = n_data + float(wb.sum()), float(np.sqrt(n_data + float(wb @ wb)))
+            if dcfg.get("extended", False):
+                n_err = 0.0
+            out.append({key: (f * n, float(np.sqrt((n * err.get(key, 0.0)) ** 2
+                                                   + (n_err * f) ** 2)))
+                        for key, f in frac.items()})
+        return out

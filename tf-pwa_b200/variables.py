@@ -59,6 +59,51 @@ class VarsManager:
             self.add_real_var(name + suf, range_=(-1, 1))
         self.complex_vars[name] = polar
 
+    def refresh_vars(self, init_val=None, bound_dic=None):
+        """Draw new starting values for the free parameters
+        (``tf_pwa/variable.py:329-420``): free parts of complex couplings
+        uniformly (polar: r in (0, 2), phase in (-pi, pi); cartesian: both
+        in (-1, 1)); ``init_val`` entries set to their value, or drawn from
+        a normal (mu, sigma) (redrawn until inside the bounds, where given);
+        other bounded parameters uniformly between the bounds, or a
+        chi-square(1) step inside a one-sided bound."""
+        init_val = init_val or {}
+        bound_dic = self.bnd_dic if bound_dic is None else bound_dic
+        free = set(self.trainable_vars)
+        rng = self._rng
+        for name, polar in self.complex_vars.items():
+            for suf in ("r", "i"):
+                n = name + suf
+                if n not in free:
+                    continue
+                if not polar:
+                    self.variables[n] = float(rng.uniform(-1, 1))
+                elif suf == "r":
+                    self.variables[n] = float(rng.uniform(0, 2))
+                else:
+                    self.variables[n] = float(rng.uniform(-np.pi, np.pi))
+        for n in [k for k in init_val if k in free]:
+            v = init_val[n]
+            if hasattr(v, "__len__"):
+                mu, sigma = v[0], v[1]
+                lo, hi = bound_dic.get(n, (None, None))
+                for _ in range(10000):
+                    val = float(rng.normal(mu, sigma))
+                    if (lo is None or val > lo) and (hi is None or val < hi):
+                        break
+                self.variables[n] = val
+            elif v is not None:
+                self.variables[n] = float(v)
+        for n, (lo, hi) in bound_dic.items():
+            if n in init_val or n not in free:
+                continue
+            if lo is not None and hi is not None:
+                self.variables[n] = float(rng.uniform(lo, hi))
+            elif lo is not None:
+                self.variables[n] = float(lo + rng.chisquare(1))
+            elif hi is not None:
+                self.variables[n] = float(hi - rng.chisquare(1))
+
     # -- fixing ------------------------------------------------------------
     def set_fix(self, name, value=None, unfix=False):
         if value is not None:
