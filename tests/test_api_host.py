@@ -274,3 +274,39 @@ def test_loader_fit_helpers(host_engine, tmp_path):
     assert min(nlls) == pytest.approx(nlls[vals.index(v0)], abs=1e-4)
     assert var in cl.vm.trainable_vars
     assert cl.get_params()[var] == v0
+
+
+def test_attach_fix_params_error(host_engine, tmp_path):
+    """attach_fix_params_error: V_a = J V_b J^T with J = da/db of the
+    minimum; J checked against refits with the fixed parameter moved."""
+    from tf_pwa_b200.api import ConfigLoader
+
+    cfg, g, meta = _config(tmp_path, "d2kpipi_float")
+    cl = ConfigLoader(cfg)
+    cl.set_params(meta["variables"])
+    b = "R2_width"
+    # a well-conditioned free set on this small sample: R2's coupling and mass
+    for n in (b, "R1_mass", "R1_width"):
+        cl.vm.set_fix(n)
+    cl.fit(print_init_nll=False, gtol=1e-9)
+    cl.get_params_error()
+    inv0 = cl.inv_he.copy()
+    free = list(cl.vm.trainable_vars)
+    a0 = np.array(cl.vm.get_all_val())
+    b0 = cl.vm.variables[b]
+    err_b = 1e-3
+    V = cl.attach_fix_params_error({b: err_b})
+    assert list(cl.vm.trainable_vars) == free and cl.vm.is_fixed(b)
+    np.testing.assert_allclose(cl.inv_he, inv0 + V, rtol=0, atol=0)
+    assert np.all(np.linalg.eigvalsh(V) > -1e-12 * np.abs(V).max())
+    # the slope of the refitted minimum in b
+    shifts = []
+    for d in (-1e-4, 1e-4):
+        cl.vm.set_all(list(a0))
+        cl.vm.variables[b] = b0 + d
+        cl.fit(print_init_nll=False, gtol=1e-9)
+        shifts.append(np.array(cl.vm.get_all_val()))
+    slope = (shifts[1] - shifts[0]) / 2e-4
+    # V = (slope err_b)(slope err_b)^T up to the sign of the slope
+    np.testing.assert_allclose(np.sqrt(np.diag(V)), np.abs(slope) * err_b,
+                               rtol=2e-2, atol=1e-3 * np.abs(slope).max() * err_b)

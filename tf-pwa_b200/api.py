@@ -678,6 +678,37 @@ class ConfigLoader:
             self.fit_params.set_error(err)
         return err
 
+    def attach_fix_params_error(self, params, V_b=None):
+        """Propagate the errors of fixed parameters b into the free ones a
+        (``config_loader.py:1049-1100``): with a(b) the minimum, da/db =
+        H_aa^-1 H_ab from the FP64 Hessian over a and b (b freed for the
+        Hessian, fixed again after); V_a = (da/db) V_b (da/db)^T, V_b by
+        default diag(error_b^2) from ``params`` {name: error}.  V_a is added
+        to ``self.inv_he`` and returned."""
+        new = list(params)
+        for n in new:
+            self.vm.set_fix(n, unfix=True)
+        all_params = list(self.vm.trainable_vars)
+        try:
+            fcn = self.get_fcn(precision="plain")
+            try:
+                _, _, hess = fcn.nll_grad_hessian()
+            finally:
+                fcn.eng.close()
+        finally:
+            for n in new:
+                self.vm.set_fix(n)
+        old = [n for n in all_params if n not in new]
+        ia = np.array([all_params.index(n) for n in old])
+        ib = np.array([all_params.index(n) for n in new])
+        grad = np.linalg.inv(hess[np.ix_(ia, ia)]) @ hess[np.ix_(ia, ib)]
+        if V_b is None:
+            V_b = np.diag([float(params[n]) for n in new]) ** 2
+        V = grad @ np.asarray(V_b, dtype=np.float64) @ grad.T
+        inv = getattr(self, "inv_he", None)
+        self.inv_he = V if inv is None else inv + V
+        return V
+
     # -- toys and phase space (``tf_pwa/config_loader/sample.py``) ------------
     def _toy_engine(self):
         from .engine import Engine
