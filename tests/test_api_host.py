@@ -310,3 +310,26 @@ def test_attach_fix_params_error(host_engine, tmp_path):
     # V = (slope err_b)(slope err_b)^T up to the sign of the slope
     np.testing.assert_allclose(np.sqrt(np.diag(V)), np.abs(slope) * err_b,
                                rtol=2e-2, atol=1e-3 * np.abs(slope).max() * err_b)
+
+
+def test_eval_amplitude_inputs(tmp_path, monkeypatch):
+    """eval_amplitude accepts per-final arrays (decay order), a dict and a
+    dat_order array, and hands the amplitude the same event fields."""
+    from tf_pwa_b200.api import ConfigLoader
+
+    cfg, g, meta = _config(tmp_path, "lc2pkpi")
+    cl = ConfigLoader(cfg)
+    seen = []
+    monkeypatch.setattr(cl, "get_amplitude", lambda *a, **k: (lambda d: seen.append(d.fields)))
+    p4 = g["p4_data"][:50]
+    order = cl.get_dat_order()
+    outs = [str(o) for o in cl.decay_group.outs]
+    cl.eval_amplitude(p4)
+    cl.eval_amplitude({n: p4[:, i] for i, n in enumerate(order)})
+    cl.eval_amplitude(*[p4[:, order.index(n)] for n in outs])
+    ref = cl.data_from_p4(p4).fields
+    assert len(seen) == 3
+    for f in seen:
+        np.testing.assert_array_equal(f, ref)
+    with pytest.raises(NotImplementedError):
+        cl.eval_amplitude(p4, extra={"center_mass": True})

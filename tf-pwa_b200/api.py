@@ -443,6 +443,29 @@ class ConfigLoader:
                          charge=charge)
         return EventData(x, weight)
 
+    def eval_amplitude(self, *p, extra=None):
+        """sum |A|^2 per event from momenta (``config_loader.py:239-249``):
+        one (N, 4) array per final particle in the decay's final-state order,
+        or one argument -- a {particle name: (N, 4)} dict or an
+        (N, n_final, 4) array in dat_order.  ``extra`` may hold the events'
+        ``charge``."""
+        extra = dict(extra or {})
+        charge = extra.pop("charge", extra.pop("charge_conjugation", None))
+        if extra:
+            raise NotImplementedError(f"eval_amplitude options {sorted(extra)}")
+        order = self.get_dat_order()
+        outs = [str(o) for o in self.decay_group.outs]
+        if len(p) == len(outs) and len(outs) > 1 or (len(p) == 1 and len(outs) == 1
+                                                     and np.ndim(p[0]) == 2):
+            p = (dict(zip(outs, p)),)
+        if len(p) != 1:
+            raise ValueError("eval_amplitude: give every final momentum, a dict or one array")
+        p4 = p[0]
+        if isinstance(p4, dict):
+            p4 = np.stack([np.asarray(p4[n], dtype=np.float64) for n in order], 1)
+        return self.get_amplitude()(self.data_from_p4(np.asarray(p4, dtype=np.float64),
+                                                      charge=charge))
+
     def get_data(self, idx):
         if idx in self._data:
             return self._data[idx]
