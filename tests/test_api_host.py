@@ -333,3 +333,19 @@ def test_eval_amplitude_inputs(tmp_path, monkeypatch):
         np.testing.assert_array_equal(f, ref)
     with pytest.raises(NotImplementedError):
         cl.eval_amplitude(p4, extra={"center_mass": True})
+
+
+def test_get_chain(tmp_path):
+    """get_chain by index and by particle names (``tf_pwa/particle.py:
+    888-956``)."""
+    from tf_pwa_b200.api import ConfigLoader
+
+    cfg, g, meta = _config(tmp_path, "d2kpipi_float")
+    cl = ConfigLoader(cfg)
+    c0, c1 = cl.decay_group.chains[:2]
+    assert cl.get_chain(1) is c1
+    r = [p for p in c1.inner][0]
+    assert cl.get_chain(str(r)) is c1 and cl.get_chain([r]) is c1
+    assert cl.get_chain(str(c0.top)) is c0
+    with pytest.raises(ValueError):
+        cl.get_chain("no_such_particle")

@@ -629,6 +629,10 @@ class ConfigLoader:
         self.fit_params = fr
         return fr
 
+    def get_chain(self, idx):
+        """``config_loader.py:889-891``: a chain by index or particle names."""
+        return self.full_decay.get_decay_chain(idx)
+
     def get_ndf(self):
         """Number of free parameters (``config_loader.py:722-725``)."""
         return len(self.vm.trainable_vars)

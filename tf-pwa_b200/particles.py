@@ -416,6 +416,24 @@ class DecayChain:
 class DecayGroup:
     """All chains of the model with the same top and final particles."""
 
+    def get_decay_chain(self, id_):
+        """Chain by index, or the first chain holding every named particle
+        (a "R1/R2" string, a list, or a particle) (``tf_pwa/particle.py:
+        888-956``)."""
+        if isinstance(id_, int):
+            return self.chains[id_]
+        if isinstance(id_, str):
+            names = id_.split("/")
+        elif isinstance(id_, (list, tuple)):
+            names = [str(i) for i in id_]
+        else:
+            names = [str(id_)]
+        for c in self.chains:
+            have = {str(p) for p in [c.top] + list(c.inner) + list(c.outs)}
+            if all(n in have for n in names):
+                return c
+        raise ValueError(f"Not found such decay chain: {names}")
+
     def __init__(self, chains):
         self.chains = list(chains)
         self.identical_particles = None
