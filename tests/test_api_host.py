@@ -349,3 +349,18 @@ def test_get_chain(tmp_path):
     assert cl.get_chain(str(c0.top)) is c0
     with pytest.raises(ValueError):
         cl.get_chain("no_such_particle")
+
+
+def test_fcn_hessian_argument_order(host_engine, tmp_path):
+    """nll_grad_hessian(x, batch) as the reference: a positional batch
+    leaves the difference step at its default."""
+    from tf_pwa_b200.api import ConfigLoader
+
+    cfg, g, meta = _config(tmp_path, "d2kpipi_float")
+    cl = ConfigLoader(cfg)
+    cl.set_params(meta["variables"])
+    fcn = cl.get_fcn()
+    x = np.array(cl.vm.get_all_val())
+    _, _, H1 = fcn.nll_grad_hessian(x)
+    _, _, H2 = fcn.nll_grad_hessian(x, 65000)
+    np.testing.assert_array_equal(H1, H2)

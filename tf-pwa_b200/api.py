@@ -283,14 +283,15 @@ class FCN:
         gradient (``NLLFunction``)."""
         return NLLFunction.apply(x, self)
 
-    def nll_grad_hessian(self, x=None, step=None):
+    def nll_grad_hessian(self, x=None, batch=None, step=None):
         """Hessian by differencing the adjoint gradient: 4-point central
         stencil per parameter, h_i = step * max(|x_i|, 1e-2) (error O(h^4)),
         symmetrised.  Default step: 1e-4 in the plain form; 1e-2 in the
         mixed forms, whose FP32 per-event (or per-warp) values put 1e-7 to
         1e-6 relative rounding noise on the gradient (noise / h must stay
         small).  In the cached form the whole stencil loop runs in the native
-        library."""
+        library.  ``batch`` is accepted in the reference's position
+        (``tf_pwa/model/model.py:1258``); the engine does not batch."""
         self._set(x)
         if step is None:
             step = 1e-4 if self.precision == PLAIN_F64 else 1e-2
