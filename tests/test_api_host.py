@@ -364,3 +364,20 @@ def test_fcn_hessian_argument_order(host_engine, tmp_path):
     _, _, H1 = fcn.nll_grad_hessian(x)
     _, _, H2 = fcn.nll_grad_hessian(x, 65000)
     np.testing.assert_array_equal(H1, H2)
+
+
+def test_fcn_positional_order(host_engine, tmp_path):
+    """FCN(model, data, mcdata, bg, batch) as the reference: a positional
+    batch does not change the likelihood; inmc samples are refused."""
+    from tf_pwa_b200.api import FCN, ConfigLoader
+
+    cfg, g, meta = _config(tmp_path, "d2kpipi_float")
+    cl = ConfigLoader(cfg)
+    cl.set_params(meta["variables"])
+    data, phsp, _, _ = cl.get_all_data()
+    a = FCN(cl, data[0], phsp[0]).nll_grad()
+    b = FCN(cl, data[0], phsp[0], None, 1000).nll_grad()
+    assert a[0] == b[0]
+    np.testing.assert_array_equal(a[1], b[1])
+    with pytest.raises(NotImplementedError):
+        FCN(cl, data[0], phsp[0], None, 1000, phsp[0])

@@ -156,10 +156,15 @@ class FCN:
 
     ``precision``: "plain" (FP64 throughout) or "mixed" (FP32 amplitudes,
     FP64 sums; with ``gram=True`` and fixed masses/widths the MC integral
-    uses the cached Gram matrix)."""
+    uses the cached Gram matrix).  ``bg``, ``batch`` take the reference's
+    positions; ``w_bkg`` (weight of bg rows without their own weights),
+    ``precision`` and ``gram`` are passed by keyword."""
 
-    def __init__(self, config, data, mcdata, bg=None, w_bkg=1.0, precision="plain",
-                 gram=None, batch=65000):
+    def __init__(self, config, data, mcdata, bg=None, batch=65000, inmc=None, gauss_constr=None,
+                 w_bkg=1.0, precision="plain", gram=None):
+        # positional order of tf_pwa/model/model.py:1126-1135
+        if inmc is not None or gauss_constr:
+            raise NotImplementedError("inmc samples / Gaussian constraints")
         self.config = config
         self.vm = config.vm
         self.precision = PRECISIONS[precision]
