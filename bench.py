@@ -137,7 +137,10 @@ class Clocks:
 _W = {}
 
 
-def _oracle_init(cfg):
+def _oracle_init(cfg, shm_name, shape):
+    """Worker set-up: the model and a view of the shared event fields."""
+    from multiprocessing import shared_memory
+
     sys.path.insert(0, ROOT)
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import conftest  # noqa: F401  (package loader)
@@ -146,130 +149,158 @@ def _oracle_init(cfg):
 
     dc, vm, plan = load_model(cfg)
     _W["m"] = OracleModel(dc.decay_group, plan)
+    _W["shm"] = shared_memory.SharedMemory(name=shm_name)
+    _W["x"] = np.ndarray(shape, dtype=np.float64, buffer=_W["shm"].buf)
 
 
 def _oracle_chunk(args):
-    """Sums of one chunk: data log-term and MC integral with the derivative
-    of each w.r.t. every free complex coupling (what the reference's
-    GradientTape pass produces)."""
-    xd, wd, xm, wm, vals, names = args
-    from oracle.pwa_oracle import clip_log
+    """Sums of one event range [b, e) of one set, in batches of 65000 (the
+    reference FCN's batch): data (sum w clip_log f, sum w clip_log'(f) G_k)
+    or MC (sum w f, sum w G_k) from the partial-wave columns -- the NLL and
+    every coupling derivative from one pass, as the reference's
+    GradientTape pass over FCN.nll_grad."""
+    b, e, w, vals, data = args
+    from oracle.pwa_oracle import column_sums
 
-    m = _W["m"]
-    out = {}
-    for tag, x, w in (("d", xd, wd), ("m", xm, wm)):
-        A = m.amp(x, vals).reshape(x.shape[1], -1)
-        f = np.sum(np.abs(A) ** 2, 1)
-        grads = []
-        for n in names:
-            base = n[:-1]
-            v1, v2 = dict(vals), dict(vals)
-            v1[base + "r"], v1[base + "i"] = 1.0, 0.0
-            v2[base + "r"], v2[base + "i"] = 0.0, 0.0
-            B = (m.amp(x, v1) - m.amp(x, v2)).reshape(A.shape)
-            grads.append(np.sum(np.conj(A) * B, 1))
-        if tag == "d":
-            out["d"] = (np.sum(w * clip_log(f)), [np.sum(w / f * g) for g in grads])
-        else:
-            out["m"] = (np.sum(w * f), [np.sum(w * g) for g in grads])
-    return out
+    s, g = 0.0, 0.0
+    for q in range(b, e, 65000):
+        r = min(q + 65000, e)
+        s1, g1 = column_sums(_W["m"], _W["x"][:, q:r], w[q - b:r - b], vals, {}, data)
+        s, g = s + s1, g + g1
+    return s, g
 
 
 class CpuOracle:
-    """FP64 oracle NLL + gradient on a bounded sample, all host cores
-    (spawned worker processes, one chunk of events each)."""
+    """FP64 oracle NLL + gradient over the whole workload (1.1e6 data rows +
+    1e6 MC events for the Lambda_c workload) on all host cores: spawned
+    worker processes, one contiguous range of events each, fields in shared
+    memory, one pass per evaluation (partial-wave columns, then all
+    coupling derivatives).  Events: seeded flat phase space (the timing of
+    an evaluation does not depend on where the events lie)."""
 
-    def __init__(self, n_sample, seed=5):
+    def __init__(self, n_data, n_mc, n_bg=0, seed=5):
         import multiprocessing as mp
+        from multiprocessing import shared_memory
 
         _pkg()
         from tf_pwa_b200.api import ConfigLoader
         from tf_pwa_b200.kinematics import event_fields, p4_dict
+        from tf_pwa_b200.phasespace import generate_phsp
         from tf_pwa_b200.workload import config_path, seeded_params
 
-        from oracle.toy_oracle import select
-        from tf_pwa_b200.kincode import KinCode
-
         cl = ConfigLoader(config_path(CONFIG), seed=seed)
-        vals = seeded_params(cl.vm, seed)
+        self.vals = seeded_params(cl.vm, seed)
+        self.trainable = list(cl.vm.trainable_vars)
         order = cl.get_dat_order()
-        kin = KinCode(cl.plan, order)
+        pp = cl.decay_config.particle_property
+        masses = [pp[o]["mass"] for o in order]
+        M = pp[str(cl.decay_group.top)]["mass"]
+        n = n_data + n_mc
+        ps = generate_phsp(M, masses, n, seed=seed)
+        p4 = np.stack(ps, 1)
+        self.shm = shared_memory.SharedMemory(create=True, size=8 * cl.plan.n_fields * n)
+        x = np.ndarray((cl.plan.n_fields, n), dtype=np.float64, buffer=self.shm.buf)
+        for q in range(0, n, 500_000):
+            r = min(q + 500_000, n)
+            x[:, q:r] = event_fields(cl.plan, p4_dict(p4[q:r], order)).numpy()
+        w = np.ones(n_data)
+        if n_bg:
+            w[n_data - n_bg:] = -BG_WEIGHT
+        w = w * (w.sum() / (w * w).sum())
+        self.sw = float(w.sum())
+        wm = np.ones(n_mc) / n_mc
+        self.cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (
+            os.cpu_count() or 1)
+        self.args = []
+        for lo, hi, ww, is_d, off in ((0, n_data, w, True, 0), (n_data, n, wm, False, n_data)):
+            cuts = np.linspace(lo, hi, self.cores + 1).astype(np.int64)
+            for b, e in zip(cuts[:-1], cuts[1:]):
+                if e > b:
+                    self.args.append((int(b), int(e), ww[b - off:e - off], self.vals, is_d))
+        self.n_data, self.n_mc = n_data, n_mc
+        from oracle.pwa_oracle import OracleModel
 
-        def gen(s):
-            """n_sample flat phase-space events (the generator's CPU oracle)."""
-            ps = []
-            first = 0
-            while sum(len(p) for p in ps) < n_sample:
-                out, p = select(s, first, 4 * n_sample, kin.levels, kin.nfin)
-                ps.append(np.transpose(p[:, :, out >= 0], (2, 0, 1)))
-                first += 4 * n_sample
-            p4 = np.concatenate(ps)[:n_sample]
-            return event_fields(cl.plan, p4_dict(p4, order)).numpy()
-
-        xd, xm = gen(seed), gen(seed + 1)
-        names = sorted({n[:-1] + "r" for n in cl.vm.trainable_vars})
-        self.cores = os.cpu_count() or 1
-        chunks = [c for c in np.array_split(np.arange(n_sample), self.cores) if len(c)]
-        self.args = [(xd[:, c], np.ones(len(c)), xm[:, c], np.ones(len(c)) / n_sample, vals,
-                      names) for c in chunks]
-        self.n = n_sample
-        self.pool = mp.get_context("spawn").Pool(len(self.args), initializer=_oracle_init,
-                                                 initargs=(CONFIG,))
-        self.pool.map(_oracle_chunk, self.args)  # warm
+        self.names = OracleModel(cl.decay_group, cl.plan).columns(x[:, :1], self.vals, {})[1]
+        env = {k: os.environ.get(k) for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS",
+                                               "MKL_NUM_THREADS")}
+        for k in env:
+            os.environ[k] = "1"  # one thread per worker process
+        try:
+            self.pool = mp.get_context("spawn").Pool(
+                self.cores, initializer=_oracle_init,
+                initargs=(CONFIG, self.shm.name, (cl.plan.n_fields, n)))
+        finally:
+            for k, v in env.items():
+                if v is None:
+                    os.environ.pop(k, None)
+                else:
+                    os.environ[k] = v
+        self.step()  # warm: imports, CG tables
 
     def step(self):
+        """One NLL + gradient evaluation; returns its wall time (s)."""
+        from oracle.pwa_oracle import nll_grad_from_sums
+
         t0 = time.perf_counter()
-        self.pool.map(_oracle_chunk, self.args)
+        res = self.pool.map(_oracle_chunk, self.args, chunksize=1)
+        sd = sum(r[0] for r, a in zip(res, self.args) if a[4])
+        gd = sum(r[1] for r, a in zip(res, self.args) if a[4])
+        sm = sum(r[0] for r, a in zip(res, self.args) if not a[4])
+        gm = sum(r[1] for r, a in zip(res, self.args) if not a[4])
+        self.result = nll_grad_from_sums(self.names, self.vals, {}, self.trainable, sd, gd, sm,
+                                         gm, self.sw)
         return time.perf_counter() - t0
 
-    def scale(self):
-        """sample -> full workload (data + MC events)."""
-        return (N_SIG + N_BG + N_MC) / (2.0 * self.n)
-
-    def describe(self, t):
-        return (f"{self.n} data + {self.n} MC events of the same model per step, FP64 numpy "
-                f"oracle (forward + per-coupling derivative columns), {len(self.args)} spawned "
-                f"workers, {t:.3f} s per step, scaled x{self.scale():.1f} to the full workload")
+    def describe(self, t, steps):
+        return (f"whole workload every step ({self.n_data} data rows + {self.n_mc} MC events, "
+                f"seeded flat phase space), FP64 numpy oracle, one pass per evaluation "
+                f"(partial-wave columns, then NLL and all {len(self.trainable)} coupling "
+                f"derivatives), {self.cores} spawned single-thread workers, "
+                f"{t:.3f} s per evaluation over {steps} evaluations")
 
     def close(self):
         self.pool.close()
         self.pool.join()
+        self.shm.close()
+        self.shm.unlink()
 
 
-def cpu_baseline(n_sample, steps=3):
-    o = CpuOracle(n_sample)
+def cpu_baseline(n_sig, n_bg, n_mc, steps=3):
+    o = CpuOracle(n_sig + n_bg, n_mc, n_bg)
     try:
         t = float(np.mean([o.step() for _ in range(steps)]))
     finally:
         o.close()
-    return {"value": 1.0 / (t * o.scale()), "unit": "evals/s", "cores": len(o.args),
-            "kind": "port", "sample": o.describe(t)}
+    return {"value": 1.0 / t, "unit": "evals/s", "cores": o.cores, "kind": "port",
+            "sample": o.describe(t, steps)}
 
 
 # ------------------------------------------------------------ reference arm
 def run_reference(args, rank):
     """The reference's CPU path on the host cores.  TensorFlow is not
     installed, so the reference package cannot run; its FP64 restatement
-    (the oracle) stands in, on a bounded per-step sample."""
+    (the oracle) stands in, over the whole workload every step."""
     if rank != 0:
         return
-    o = CpuOracle(int(os.environ.get("PWA_REF_SAMPLE", "8000")))
+    o = CpuOracle(args.n_sig + args.n_bg, args.n_mc, args.n_bg)
     try:
-        for _ in range(max(args.warmup, 1)):
+        for _ in range(max(args.warmup - 1, 0)):  # one warm step ran at set-up
             o.step()
         ts = [o.step() for _ in range(args.steps)]
     finally:
         o.close()
-    t = float(np.mean(ts)) * o.scale()
+    t = float(np.mean(ts))
     v = 1.0 / t
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "evals/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * t, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "precision": "FP64 CPU (numpy oracle standing in "
+            "config": {"workload": WORKLOAD,
+                       "events_per_rank": {"data": args.n_sig + args.n_bg, "mc": args.n_mc},
+                       "precision": "FP64 CPU (numpy oracle standing in "
                        "for the reference's TensorFlow CPU path, which is not installed)"},
-            "cpu_baseline": {"value": v, "unit": "evals/s", "cores": len(o.args), "kind": "port",
-                             "sample": o.describe(float(np.mean(ts)))},
+            "cpu_baseline": {"value": v, "unit": "evals/s", "cores": o.cores, "kind": "port",
+                             "sample": o.describe(t, args.steps)},
             "e2e": {"value": v, "unit": "evals/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -411,7 +442,8 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours")
-    ap.add_argument("--cpu-sample", type=int, default=int(os.environ.get("PWA_CPU_SAMPLE", "2000")))
+    ap.add_argument("--cpu-steps", type=int, default=3,
+                    help="evaluations of the CPU oracle baseline (whole workload each)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--serving", action="store_true",
                     help="run the toy-fit serving workload instead (separate JSON line)")
@@ -603,7 +635,7 @@ def main():
         line["clocks"] = ck_clocks
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            line["cpu_baseline"] = cpu_baseline(args.cpu_sample)
+            line["cpu_baseline"] = cpu_baseline(n_sig, n_bg, n_mc, args.cpu_steps)
         except Exception as e:  # reported, never fatal
             line["cpu_baseline"] = {"error": repr(e)}
     if rank == 0:

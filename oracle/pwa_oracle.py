@@ -43,18 +43,23 @@ _EPS_CLIP = 1e-6
 # ----------------------------------------------------------- D functions
 @lru_cache(maxsize=None)
 def d_weight(j2):
-    """Wigner weights w[l, m1, m2] for spin j = j2/2 (dfun.py:118-143)."""
-    j = j2
-    ret = np.zeros((j + 1, j + 1, j + 1))
-    f = lambda x: math.factorial(x >> 1)  # noqa: E731
-    for m in range(-j, j + 1, 2):
-        for n in range(-j, j + 1, 2):
-            for k in range(max(0, n - m), min(j - m, j + n) + 1, 2):
-                l = (2 * k + (m - n)) // 2
-                sign = (-1) ** ((k + m - n) // 2)
-                v = sign * math.sqrt(1.0 * f(j + m) * f(j - m) * f(j + n) * f(j - n))
-                v /= f(j - m - k) * f(j + n - k) * f(k + m - n) * f(k)
-                ret[l][(m + j) // 2][(n + j) // 2] = v
+    """Wigner weights w[l, m1 + j, m2 + j] for spin j = j2/2: the coefficient
+    of sin^l(b/2) cos^(2j-l)(b/2) in d^j_{m1 m2}(b), the quantity of
+    ``tf_pwa/dfun.py:118-143``.  Written from Wigner's explicit sum
+    d = sum_s (-1)^(m1-m2+s) sqrt((j+m1)!(j-m1)!(j+m2)!(j-m2)!)
+        / ((j+m2-s)! s! (m1-m2+s)! (j-m1-s)!) cos^(2j+m2-m1-2s) sin^(m1-m2+2s),
+    with all quantities in units of 1/2 kept as integers (a = j+m1,
+    b = j+m2 are integers)."""
+    n = j2
+    fa = math.factorial
+    ret = np.zeros((n + 1, n + 1, n + 1))
+    for a in range(n + 1):          # j + m1
+        for b in range(n + 1):      # j + m2
+            dm = a - b              # m1 - m2
+            root = math.sqrt(fa(a) * fa(n - a) * fa(b) * fa(n - b))
+            for s_ in range(max(0, -dm), min(b, n - a) + 1):
+                den = fa(b - s_) * fa(s_) * fa(dm + s_) * fa(n - a - s_)
+                ret[dm + 2 * s_, a, b] += (-1) ** (dm + s_) * root / den
     return ret
 
 
@@ -282,8 +287,10 @@ class OracleModel:
             return x[cf["mass"][p]]
         return np.full(x.shape[1], p.mass)
 
-    def decay_amp(self, x, cf, chain, k, d, vals, gls):
-        """(N, n_a, n_b, n_c) complex amplitude of vertex d (core.py:1149-1164)."""
+    def decay_amp(self, x, cf, chain, k, d, vals, gls, per_ls=False):
+        """(N, n_a, n_b, n_c) complex amplitude of vertex d (core.py:1149-1164);
+        with ``per_ls`` the term of every LS coupling apart, (N, n_ls, n_a,
+        n_b, n_c), at unit coupling."""
         a, (b, c) = d.core, d.outs
         f = cf["decays"][k]
         alpha, beta = x[f["alpha"]], x[f["beta"]]
@@ -310,15 +317,21 @@ class OracleModel:
                 else:
                     t = q2 ** (l / 2) if d.has_ql else np.ones_like(q2)
                 bfs.append(t)
-            mdep = gls[None, :] * np.stack(bfs, -1)
+            bfv = np.stack(bfs, -1)
         else:
-            mdep = np.broadcast_to(gls[None, :], (x.shape[1], len(ls)))
+            bfv = np.ones((x.shape[1], len(ls)))
         cg = cg_matrix(a.J, b.J, c.J, ls, b.spins, c.spins)
-        H = np.einsum("nl,lbc->nbc", mdep, cg)
+        if per_ls:
+            H = np.einsum("nl,lbc->nlbc", bfv, cg)
+        else:
+            H = np.einsum("nl,lbc->nbc", gls[None, :] * bfv, cg)
         ci = getattr(self.plan, "charge_index", None)
         if ci is not None and d.allow_cc:
             # charge < 0: H[..., ::-1, ::-1] (core.py:938-945)
-            H = np.where((x[ci] > 0)[:, None, None], H, H[:, ::-1, ::-1])
+            pos = (x[ci] > 0).reshape((-1,) + (1,) * (H.ndim - 1))
+            H = np.where(pos, H, H[..., ::-1, ::-1])
+        if per_ls:
+            return H[:, :, None, :, :] * Dc[:, None]
         return H[:, None, :, :] * Dc
 
     def lineshape(self, x, cf, chain, p, vals):
@@ -346,24 +359,32 @@ class OracleModel:
             ret = g0 * ret
         return ret
 
-    def chain_amp(self, x, ci, vals, coup, cf=None):
+    def chain_amp(self, x, ci, vals, coup, cf=None, per_ls=False):
+        """Amplitude of chain ci (``tf_pwa/amp/core.py:1392-1445``); with
+        ``per_ls`` one term per combination of LS couplings (one per vertex)
+        at unit couplings and unit total, (N, n_ls_1, n_ls_2, ..., helicities)."""
         chain = self.group[ci]
         cf = self.plan.chains[ci] if cf is None else cf
         tot, gl = coup[ci]
         L = self.letters
         ops, idx = [], []
+        ls_letters = "ZYXWVUTS"
         for k, d in enumerate(chain):
-            ops.append(self.decay_amp(x, cf, chain, k, d, vals, gl[k]))
-            idx.append("..." + "".join(L[p] for p in (d.core,) + d.outs))
+            ops.append(self.decay_amp(x, cf, chain, k, d, vals, gl[k], per_ls))
+            idx.append("..." + (ls_letters[k] if per_ls else "")
+                       + "".join(L[p] for p in (d.core,) + d.outs))
         rs = np.ones(x.shape[1], dtype=np.complex128)
         for p in chain.inner:
             rs = rs * self.lineshape(x, cf, chain, p, vals)
-        if isinstance(tot, tuple):
+        if per_ls:
+            tot = 1.0
+        elif isinstance(tot, tuple):
             ci_ = getattr(self.plan, "charge_index", None)
             tot = tot[0] if ci_ is None else np.where(x[ci_] > 0, tot[0], tot[1])
         ops.append(tot * rs)
         idx.append("...")
-        final = "..." + "".join(L[p] for p in [self.group.top] + list(self.group.outs))
+        final = "..." + (ls_letters[:len(chain)] if per_ls else "") + "".join(
+            L[p] for p in [self.group.top] + list(self.group.outs))
         for k, d in enumerate(chain):
             for o in d.outs:
                 if o in cf["aligned"] and o.J != 0:
@@ -372,7 +393,7 @@ class OracleModel:
                     ops.append(dt)
                     idx.append("..." + L[o] + L[o].upper())
                     final = final.replace(L[o], L[o].upper())
-        return np.einsum(",".join(idx) + "->" + final, *ops)
+        return np.einsum(",".join(idx) + "->" + final, *ops, optimize=per_ls)
 
     def amp(self, x, vals, polar=None):
         """Sum over chains (``core.py:1696-1728``); with identical particles
@@ -389,6 +410,42 @@ class OracleModel:
                 b = b[(slice(None),) + (slice(None, None, -1),) * (b.ndim - 1)]
             a = a + sw["factor"] * b
         return a
+
+    def columns(self, x, vals, polar=None):
+        """Partial-wave columns of the amplitude: A = sum_k c_k F_k with
+        c_k = chain total x one LS coupling per vertex.  Returns F
+        (N, K, n_out) and, per column, (total name, [g_ls names]).  Column k
+        is the chain amplitude with that total and those couplings set to 1
+        and the vertex's other LS couplings to 0 (H is linear in the g_ls,
+        ``tf_pwa/amp/core.py:931-947``), identical-particle swaps summed in
+        with their signs as in :meth:`amp`.  With the columns, one pass
+        gives the NLL and every coupling derivative (what the reference's
+        GradientTape pass over ``FCN.nll_grad`` produces)."""
+        import itertools
+
+        polar = polar or {}
+        if self.density(vals) is not None or any(getattr(c, "is_cp", False)
+                                                 for c in self.group):
+            raise ValueError("columns: unpolarised models without CP-violating totals only")
+        coup = self.couplings(vals, polar)
+        cols, names = [], []
+        for ci, chain in enumerate(self.group):
+            nls = [len(d.get_ls_list()) for d in chain]
+            nv = len(chain)
+            a = self.chain_amp(x, ci, vals, coup, per_ls=True)
+            for sw in self.plan.swaps:
+                b = self.chain_amp(x, ci, vals, coup, sw["chains"][ci], per_ls=True)
+                # helicity axes follow the nv LS axes
+                b = np.transpose(b, list(range(2 + nv)) + [2 + nv + t for t in sw["trans"]])
+                if sw["flip"]:
+                    b = b[(slice(None),) * (1 + nv) + (slice(None, None, -1),) * (b.ndim - 1 - nv)]
+                a = a + sw["factor"] * b
+            a = a.reshape(a.shape[0], int(np.prod(nls)), -1)
+            for q, combo in enumerate(itertools.product(*[range(n) for n in nls])):
+                cols.append(a[:, q])
+                names.append((chain.params_head + "_total_0",
+                              [f"{d.params_head}_g_ls_{l}" for d, l in zip(chain, combo)]))
+        return np.stack(cols, 1), names
 
     def density(self, vals):
         """Spin density matrix of a vector-polarised parent
@@ -526,3 +583,60 @@ class OracleNLL:
                 h = rel_step * max(abs(p[k]), 1e-3)
                 g[k] = (16 * d4(h / 2) - d4(h)) / 15
         return g
+
+
+# ------------------------------------------------ one-pass NLL + gradient
+def column_sums(model, x, w, vals, polar, data):
+    """Sums over one event set from its partial-wave columns: data
+    (sum w clip_log f, sum_n w clip_log'(f_n) G_nk) or MC (sum w f,
+    sum_n w G_nk), G_nk = sum_o conj(A_no) F_nko.  Returns (S, G (K,))."""
+    F, names = model.columns(x, vals, polar)
+    c = coupling_products(names, vals, polar)
+    A = np.einsum("k,nko->no", c, F)
+    f = np.sum(np.abs(A) ** 2, 1)
+    G = np.einsum("no,nko->nk", np.conj(A), F)
+    if data:
+        dl = np.where(f > _EPS_CLIP, 1.0 / np.where(f > _EPS_CLIP, f, 1.0),
+                      1.0 / _EPS_CLIP - (f - _EPS_CLIP) / _EPS_CLIP ** 2)
+        return float(np.sum(w * clip_log(f))), (w * dl) @ G
+    return float(np.sum(w * f)), w @ G
+
+
+def coupling_products(names, vals, polar):
+    """c_k = total x product of the column's g_ls (complex)."""
+    out = []
+    for tot, gs in names:
+        c = OracleModel.complex_of(vals, polar, tot)
+        for g in gs:
+            c = c * OracleModel.complex_of(vals, polar, g)
+        out.append(c)
+    return np.array(out)
+
+
+def nll_grad_from_sums(names, vals, polar, trainable, sd, gd, sm, gm, sw):
+    """NLL = -S_d + sw ln S_m and its derivative with respect to the
+    trainable coupling parts (r/i, polar or Cartesian): df = 2 Re(dc_k G_k)."""
+    nll = -sd + sw * np.log(sm)
+    c = coupling_products(names, vals, polar)
+    grad = np.zeros(len(trainable))
+    for t, n in enumerate(trainable):
+        base, part = n[:-1], n[-1]
+        if part not in "ri" or base + "r" not in vals or base + "i" not in vals:
+            raise ValueError(f"{n}: not a coupling part")
+        g = OracleModel.complex_of(vals, polar, base)
+        if polar.get(base, True):
+            r, ph = vals[base + "r"], vals[base + "i"]
+            dg = np.exp(1j * ph) if part == "r" else 1j * g
+        else:
+            dg = 1.0 if part == "r" else 1j
+        dc = np.zeros(len(names), np.complex128)
+        for k, (tot, gs) in enumerate(names):
+            facs = [tot] + list(gs)
+            m = facs.count(base)
+            if m:
+                rest = 1.0 + 0j
+                for q in facs:
+                    rest = rest * OracleModel.complex_of(vals, polar, q)
+                dc[k] = m * rest / g * dg
+        grad[t] = -2.0 * np.real(dc @ gd) + sw * 2.0 * np.real(dc @ gm) / sm
+    return nll, grad

@@ -53,6 +53,24 @@ CASES = {
     "lc2pkpi_pol_lab": ("lc2pkpi_pol.yml", 400, 0, 1500, 25, False, {}),
     "lc2pkpi_cp": ("lc2pkpi_cp.yml", 400, 0, 1500, 26, False, {}),
 }
+# cases at the workloads' own sizes: the events are not stored (a test
+# regenerates them from the seeds with the same generator); the reference's
+# NLL and gradient are, with its fields and |A|^2 at SUBSET events per set
+CASES.update({
+    "d2kpipi_1e4": ("d2kpipi.yml", 10_000, 0, 100_000, 31, False, {}),
+    "lc2pkpi_full": ("lc2pkpi.yml", 100_000, 10_000, 1_000_000, 32, False, {"bg_weight": 0.1}),
+})
+LARGE = {"d2kpipi_1e4", "lc2pkpi_full"}
+SUBSET_F = 2048   # events per set whose fields are stored
+SUBSET_A = 8192   # events per set whose |A|^2 is stored
+
+
+def subset_index(n, k, seed):
+    """Sorted distinct event indices of one set (seeded)."""
+    k = min(k, n)
+    return np.sort(np.random.default_rng(seed).choice(n, size=k, replace=False))
+
+
 # cases whose events are boosted out of the parent rest frame: parent
 # momentum (GeV) in a random direction per event (lab-frame input)
 BOOSTED = {"lc2pkpi_pol_lab": 2.0}
@@ -98,7 +116,7 @@ def main(ref_root):
     from tf_pwa.config_loader import ConfigLoader
 
     cfg_dir = os.path.join(REPO, "tf-pwa_b200", "configs")
-    only = sys.argv[2:] or list(CASES)
+    only = sys.argv[2:] or [c for c in CASES if c not in LARGE]
     for name in only:
         cfg_file, nd, nb, nm, seed, do_hess, extra = CASES[name]
         rng = np.random.default_rng(seed)
@@ -121,6 +139,7 @@ def main(ref_root):
                 arr = boost_events(arr, M, BOOSTED[name], rng)
             p4[kind] = arr
             np.savetxt(os.path.join(tmp, kind + ".dat"), arr.reshape(-1, 4), fmt="%.17g")
+            print(name, kind, n, "events written", flush=True)
         dic2 = dict(dic)
         dic2["data"] = dict(dic.get("data", {}))
         dic2["data"].update({"data": [os.path.join(tmp, "data.dat")],
@@ -199,9 +218,49 @@ def main(ref_root):
                     for pkey, pv in dv.items():
                         if isinstance(pv, dict) and "ang" in pv:
                             assert np.all(np.asarray(pv["ang"]["gamma"]) == 0)
-        f_vals = {k: np.asarray(amp(datas[k][0])) for k in datas}
+        if name in LARGE:
+            # |A|^2 in batches (the reference's own batching of FCN)
+            f_vals = {}
+            for k in datas:
+                from tf_pwa.data import data_split
+
+                f_vals[k] = np.concatenate([np.asarray(amp(b))
+                                            for b in data_split(datas[k][0], 65000)])
+        else:
+            f_vals = {k: np.asarray(amp(datas[k][0])) for k in datas}
         fcn = ref.get_fcn()
         nll, grad = fcn.nll_grad()
+        if name in LARGE:
+            out = dict(nll=np.float64(nll), grad=np.asarray(grad, np.float64),
+                       sum_w=np.float64(np.sum(np.asarray(fcn.weight, np.float64))))
+            for k, tag in (("data", "data"), ("phsp", "mc"), ("bg", "bg")):
+                if k not in fields:
+                    continue
+                n_k = fields[k].shape[1]
+                i_f = subset_index(n_k, SUBSET_F, 7 * seed + len(tag))
+                i_a = subset_index(n_k, SUBSET_A, 11 * seed + len(tag))
+                out.update({f"idx_fields_{tag}": i_f, f"fields_{tag}": fields[k][:, i_f],
+                            f"idx_f_{tag}": i_a, f"f_{tag}": f_vals[k][i_a],
+                            f"n_{tag}": np.int64(n_k),
+                            f"sum_f_{tag}": np.float64(np.sum(f_vals[k]))})
+            np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+            meta = {
+                "config": cfg_file,
+                "extra_data": extra,
+                "trainable": list(vm.trainable_vars),
+                "variables": all_vals,
+                "fields": plan.fields,
+                "seed": seed,
+                "events": {"generator": "tf_pwa_b200.phasespace.generate_phsp",
+                           "seeds": {"data": 1000 * seed, "bg": 1000 * seed + 1,
+                                     "mc": 1000 * seed + 2},
+                           "sizes": {"data": nd, "bg": nb, "mc": nm}},
+            }
+            with open(os.path.join(HERE, name + ".json"), "w") as f:
+                json.dump(meta, f, indent=1)
+            shutil.rmtree(tmp)
+            print(name, "nll", float(nll), "n_trainable", len(vm.trainable_vars))
+            continue
         out = dict(
             fields_data=fields["data"], fields_mc=fields["phsp"],
             f_data=f_vals["data"], f_mc=f_vals["phsp"],

@@ -10,9 +10,10 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def _run(extra_env):
-    env = dict(os.environ, PWA_REF_SAMPLE="400", **extra_env)
+    env = dict(os.environ, **extra_env)
     return subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
-                           "--steps", "1", "--warmup", "1"],
+                           "--steps", "2", "--warmup", "1", "--n-sig", "3000", "--n-bg", "300",
+                           "--n-mc", "4000"],
                           cwd=ROOT, env=env, capture_output=True, text=True, timeout=600)
 
 
@@ -30,7 +31,8 @@ def test_reference_arm_line():
     assert d["value"] > 0 and abs(d["ms_per_step"] - 1e3 / d["value"]) < 1e-6 * d["ms_per_step"]
     cb = d["cpu_baseline"]
     assert cb["kind"] == "port" and cb["value"] == d["value"] and cb["cores"] >= 1
-    assert "400 data + 400 MC" in cb["sample"]
+    assert "3300 data rows + 4000 MC events" in cb["sample"]
+    assert d["config"]["events_per_rank"] == {"data": 3300, "mc": 4000}
     assert d["e2e"] == {"value": d["value"], "unit": "evals/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}
     assert "workload" in d["config"]

@@ -47,7 +47,7 @@ def test_small_and_ragged_sets(nd, nm):
     cfg.vm, cfg.decay_group, cfg.plan = vm, dc.decay_group, plan
     fcn = FCN(cfg, EventData(xd, wd), EventData(xm), precision="mixed")
     assert fcn.use_gram
-    for var in (0, 1, 2, 3):
+    for var in (0, 1, 2, 3, 4, 5):
         fcn.eng.set_cached_variant(var)
         nll_m, _ = fcn.nll_grad()
         assert abs(nll_m - ref) <= 1e-6 * max(abs(ref), 1.0), (var, nll_m, ref)

@@ -130,11 +130,13 @@ def test_cached_columns_fcn(name):
 
 @pytest.mark.parametrize("name", ["lc2pkpi", "b2dstkpi"])
 def test_cached_kernel_variants_agree(name):
-    """The four data-term kernels on the column cache (shared-memory ring,
+    """The six data-term kernels on the column cache (shared-memory ring,
     per-thread FP64 column sums, warp reduce-scatter of FP32 column sums,
-    ring with reduce-scatter consumers)
-    give the same NLL (FP64 amplitude and log in all three) and gradients
-    that differ only by FP32 rounding of per-event / per-warp sums."""
+    ring with reduce-scatter consumers, one block per SM with contiguous
+    warp runs, one block per SM with a producer warp and a deep bulk-copy
+    ring) give the same NLL (FP64 amplitude and log in all of them) and
+    gradients that differ only by FP32 rounding of per-event / per-warp
+    sums."""
     from tf_pwa_b200.api import FCN, EventData
     from common import load_model as lm
 
@@ -152,12 +154,15 @@ def test_cached_kernel_variants_agree(name):
               precision="mixed")
     vals = [vm.variables[k] for k in fcn._var_names]
     res = {}
-    for var in (0, 1, 2, 3):
+    for var in (0, 1, 2, 3, 4, 5):
         fcn.eng.set_cached_variant(var)
         res[var] = fcn.eng.nll_grad_cached(vals)
+        # a second call reuses the ticket counters the first one reset
+        n_again, g_again = fcn.eng.nll_grad_cached(vals)
+        assert n_again == res[var][0] and np.array_equal(g_again, res[var][1])
     fcn.eng.close()
     n1, g1 = res[1]
-    for var in (0, 2, 3):
+    for var in (0, 2, 3, 4, 5):
         n, gr = res[var]
         assert abs(n - n1) <= 1e-12 * abs(n1)
         np.testing.assert_allclose(gr, g1, rtol=1e-5, atol=1e-6 * np.abs(g1).max())

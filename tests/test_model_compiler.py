@@ -91,3 +91,38 @@ def test_plan_accumulator_count(cfg):
     assert nacc == 1 + 2 * c.ncol + c.nshape + c.nrho + c.ncp
     if cfg == "lc2pkpi_cp.yml":
         assert c.ncp > 0
+
+
+def test_small_d_weights_match_reference_table():
+    """The Wigner small-d coefficient tables (spinor-polynomial derivation)
+    equal the reference's own tables (tests/golden/small_d.json, recorded
+    from tf_pwa.dfun.small_d_weight) for 2j = 0 .. 10, and the matrices
+    they give are orthogonal with d(0) = 1 and d^{1/2}(b) the rotation by
+    b/2."""
+    import json
+    import os
+
+    from common import GOLDEN
+    from oracle.pwa_oracle import d_weight
+    from tf_pwa_b200.particles import small_d_weight
+
+    with open(os.path.join(GOLDEN, "small_d.json")) as f:
+        ref = json.load(f)
+    for j2s, table in ref.items():
+        j2 = int(j2s)
+        w = small_d_weight(j2)
+        t = np.array(table)
+        np.testing.assert_allclose(w, t, rtol=1e-14, atol=1e-14 * max(1.0, np.abs(t).max()))
+        # the oracle's table (Wigner's explicit sum) as well
+        np.testing.assert_allclose(d_weight(j2), t, rtol=1e-14,
+                                   atol=1e-14 * max(1.0, np.abs(t).max()))
+        for beta in (0.0, 0.37, 1.9, 3.0):
+            x, y = np.sin(beta / 2), np.cos(beta / 2)
+            powers = np.array([x ** l * y ** (j2 - l) for l in range(j2 + 1)])
+            d = np.einsum("l,lab->ab", powers, w)
+            np.testing.assert_allclose(d @ d.T, np.eye(j2 + 1), atol=1e-12)
+            if beta == 0.0:
+                np.testing.assert_allclose(d, np.eye(j2 + 1), atol=1e-15)
+            if j2 == 1:
+                # rows/columns m = -1/2, +1/2: d_{1/2,-1/2} = -sin(b/2)
+                np.testing.assert_allclose(d, [[y, x], [-x, y]], atol=1e-15)

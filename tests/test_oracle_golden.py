@@ -75,3 +75,29 @@ def test_known_answers():
     assert clip_log(np.array([1.0]))[0] == 0.0
     x = np.array([0.5e-6])
     assert np.isfinite(clip_log(x)).all()
+
+
+@pytest.mark.parametrize("name", ["d2kpipi", "lc2pkpi", "dp2kpipi_ident", "b2dstkpi"])
+def test_oracle_one_pass_gradient(name):
+    """The oracle's one-pass form (partial-wave columns, then every coupling
+    derivative from the same pass -- the CPU baseline's formulation) equals
+    the reference's NLL and GradientTape gradient."""
+    from common import golden_data, load_golden, load_model
+    from oracle.pwa_oracle import OracleModel, column_sums, nll_grad_from_sums
+
+    g, meta = load_golden(name)
+    dc, vm, plan = load_model(meta["config"])
+    vals = meta["variables"]
+    x, w = golden_data(g, meta)
+    xm = g["fields_mc"]
+    wm = np.ones(xm.shape[1]) / xm.shape[1]
+    m = OracleModel(dc.decay_group, plan)
+    names = m.columns(x[:, :2], vals, {})[1]
+    sd, gd = column_sums(m, x, w, vals, {}, True)
+    sm, gm = column_sums(m, xm, wm, vals, {}, False)
+    tr = [t for t in meta["trainable"] if "_g_ls_" in t or "_total_" in t]
+    nll, grad = nll_grad_from_sums(names, vals, {}, tr, sd, gd, sm, gm, w.sum())
+    idx = [meta["trainable"].index(t) for t in tr]
+    assert abs(nll - float(g["nll"])) <= 1e-12 * abs(float(g["nll"]))
+    np.testing.assert_allclose(grad, g["grad"][idx], rtol=0,
+                               atol=1e-10 * np.abs(g["grad"]).max())

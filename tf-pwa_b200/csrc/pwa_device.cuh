@@ -219,6 +219,10 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
       "l"(src), "r"(bytes), "r"(smem_addr(bar))
       : "memory");
 }
+// one arrival (count 1) on `bar`, release semantics at CTA scope
+__device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
 __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity,
                                           unsigned limit) {
   for (unsigned it = 0; it < limit; ++it) {

@@ -281,6 +281,16 @@ struct CCoup {
   double v[2 * PWA_NCOL];  // column couplings c_k, (re, im) pairs
 };
 
+// Couplings from the parameter block to shared memory with constant
+// indices only (an index that depends on the thread would make the
+// compiler copy the whole parameter block to local memory).
+__device__ __forceinline__ void stage_couplings(const CCoup& c, double* s_c) {
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int j = 0; j < 2 * PWA_NCOL; ++j) s_c[j] = c.v[j];
+  }
+}
+
 #ifndef PWA_STAGES
 #define PWA_STAGES 3
 #endif
@@ -591,6 +601,16 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, 4)
 // PWA_GPAD / 32 FP64 accumulators across tiles instead of 2 * PWA_NCOL:
 // the register footprint no longer grows with the number of columns.
 #define PWA_GPAD ((2 * PWA_NCOL + 31) / 32 * 32)
+// With 2 * PWA_NCOL <= 16 the sensitivities form one group of 16 values:
+// four halving steps leave lanes 2i and 2i + 1 with halves of entry i, one
+// more shuffle gives both the warp sum (16 shuffles instead of 31).
+// Otherwise PWA_GPAD / 32 groups of 32: lane l holds entry 32 m + l of group m.
+#define PWA_RS16 (2 * PWA_NCOL <= 16)
+#define PWA_MG (PWA_RS16 ? 1 : PWA_GPAD / 32)
+__device__ __forceinline__ int rs_entry(int m, int lane) {
+  return PWA_RS16 ? (lane >> 1) : 32 * m + lane;
+}
+__device__ __forceinline__ bool rs_owner(int lane) { return PWA_RS16 ? !(lane & 1) : true; }
 
 struct CoupParam {  // couplings from the kernel's parameter block
   const CCoup& c;
@@ -665,7 +685,7 @@ __device__ __forceinline__ double cached_event(const float2 (&v)[PWA_NF], double
 template <class Coup>
 __device__ __forceinline__ double cached_event_rs(const float2 (&v)[PWA_NF], double w,
                                                   const Coup& cp, int lane,
-                                                  float (&gs)[PWA_GPAD / 32]) {
+                                                  float (&gs)[PWA_MG]) {
   double ar[PWA_NOUT], ai[PWA_NOUT], br2[PWA_NOUT], bi2[PWA_NOUT];
 #pragma unroll
   for (int o = 0; o < PWA_NOUT; ++o) ar[o] = ai[o] = br2[o] = bi2[o] = 0.0;
@@ -697,6 +717,21 @@ __device__ __forceinline__ double cached_event_rs(const float2 (&v)[PWA_NF], dou
     br[o] = (float)(fac * ar[o]);
     bi[o] = (float)(-fac * ai[o]);
   }
+#if PWA_RS16
+  {
+    float g[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) g[q] = 0.f;
+#pragma unroll
+    for (int j = 0; j < PWA_NF; ++j) {
+      const int k = pwa_fk[j], o = pwa_fo[j];
+      g[2 * k] = fmaf(br[o], v[j].x, fmaf(-bi[o], v[j].y, g[2 * k]));
+      g[2 * k + 1] = fmaf(br[o], v[j].y, fmaf(bi[o], v[j].x, g[2 * k + 1]));
+    }
+    warp_rs_step<16, 16, 16>(g, lane);
+    gs[0] = g[0] + __shfl_xor_sync(0xffffffffu, g[0], 1);
+  }
+#else
 #pragma unroll
   for (int m = 0; m < PWA_GPAD / 32; ++m) {
     float g[32];
@@ -714,6 +749,7 @@ __device__ __forceinline__ double cached_event_rs(const float2 (&v)[PWA_NF], dou
     warp_reduce_scatter<32>(g, lane);
     gs[m] = g[0];
   }
+#endif
   return w * cl;
 }
 
@@ -723,12 +759,12 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, PWA_WRED_MINB)
                          double* __restrict__ partials, unsigned int* __restrict__ ticket,
                          double* __restrict__ out, double seq) {
   constexpr int NA = PWA_CACHE_NA;
-  constexpr int NG = 2 * PWA_NCOL, MG = PWA_GPAD / 32;
+  constexpr int NG = 2 * PWA_NCOL, MG = PWA_MG;
   __shared__ double red[PWA_TPB / 32][NA];
   __shared__ int s_last;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   __shared__ double s_c[2 * PWA_NCOL];
-  for (int j = tid; j < 2 * PWA_NCOL; j += PWA_TPB) s_c[j] = c.v[j];
+  stage_couplings(c, s_c);
   __syncthreads();
   const CoupShared cp{s_c};
   double acc0 = 0.0;
@@ -753,8 +789,8 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, PWA_WRED_MINB)
   }
 #pragma unroll
   for (int m = 0; m < MG; ++m) {
-    const int idx = 32 * m + lane;  // entry `lane` of column group m
-    if (idx < NG) red[warp][1 + idx] = accg[m];
+    const int idx = rs_entry(m, lane);
+    if (rs_owner(lane) && idx < NG) red[warp][1 + idx] = accg[m];
   }
   __syncthreads();
   for (int j = tid; j < NA; j += PWA_TPB) {
@@ -918,6 +954,238 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB)
 }
 
 // ---------------------------------------------------------------------------
+// Kernels with one block per SM.  Their block partials are few (one row per
+// SM), so a single ordered level replaces the two-level reduction: every
+// block writes its row and fences it, the last block to take ticket[0] sums
+// all rows.  Its threads form `slices` = blockDim / na groups; slice s sums
+// rows s, s + slices, ... in order (two interleaved chains), then thread j
+// adds the slices' values in order.  The order depends only on the grid:
+// bitwise reproducible.  scratch: __shared__, at least blockDim doubles.
+__device__ __forceinline__ bool flat_sum(const double* __restrict__ partials,
+                                         unsigned int* __restrict__ ticket, int na,
+                                         double* __restrict__ out, double* scratch,
+                                         int* s_flag) {
+  const int nrows = (int)gridDim.x, nt = (int)blockDim.x, t = (int)threadIdx.x;
+  if (t == 0) *s_flag = (atomicAdd(ticket, 1u) == (unsigned)nrows - 1);
+  __syncthreads();
+  if (!*s_flag) return false;
+  __threadfence();
+  const int slices = nt / na;
+  if (slices == 0) {
+    for (int j = t; j < na; j += nt) {
+      double a0 = 0.0, a1 = 0.0;
+      int r = 0;
+      for (; r + 1 < nrows; r += 2) {
+        a0 += __ldcg(partials + (long long)r * na + j);
+        a1 += __ldcg(partials + (long long)(r + 1) * na + j);
+      }
+      if (r < nrows) a0 += __ldcg(partials + (long long)r * na + j);
+      out[j] = a0 + a1;
+    }
+    return true;
+  }
+  if (t < slices * na) {
+    const int j = t % na, s = t / na;
+    double a0 = 0.0, a1 = 0.0;
+    int r = s;
+    for (; r + slices < nrows; r += 2 * slices) {
+      a0 += __ldcg(partials + (long long)r * na + j);
+      a1 += __ldcg(partials + (long long)(r + slices) * na + j);
+    }
+    if (r < nrows) a0 += __ldcg(partials + (long long)r * na + j);
+    scratch[s * na + j] = a0 + a1;
+  }
+  __syncthreads();
+  for (int j = t; j < na; j += nt) {
+    double a = 0.0;
+    for (int s = 0; s < slices; ++s) a += scratch[s * na + j];
+    out[j] = a;
+  }
+  return true;
+}
+
+// Warp sums of one block (acc0 on every lane, column group m's entry on
+// lane l = value 32 m + l) into red[warp][.], then the block's row of
+// partials in warp order.  All threads of the block call it.
+template <int NW>
+__device__ __forceinline__ void cached_block_row(double acc0, const double* accg,
+                                                 double (*red)[PWA_CACHE_NA], int warp, int lane,
+                                                 bool active, double* __restrict__ partials) {
+  constexpr int NA = PWA_CACHE_NA, NG = 2 * PWA_NCOL, MG = PWA_MG;
+  if (active) {
+    const double v0 = warp_sum(acc0);
+    if (lane == 0) red[warp][0] = v0;
+#pragma unroll
+    for (int m = 0; m < MG; ++m) {
+      const int idx = rs_entry(m, lane);
+      if (rs_owner(lane) && idx < NG) red[warp][1 + idx] = accg[m];
+    }
+  }
+  __syncthreads();
+  for (int j = (int)threadIdx.x; j < NA; j += (int)blockDim.x) {
+    double s = 0.0;
+#pragma unroll
+    for (int w2 = 0; w2 < NW; ++w2) s += red[w2][j];
+    partials[(long long)blockIdx.x * NA + j] = s;
+  }
+  __threadfence();
+  __syncthreads();
+}
+
+// Variant 4: one block of PWA_WIDE_WARPS warps per SM.  Each warp streams a
+// contiguous run of 32-event units (a quarter of a 128-event tile: 256
+// contiguous bytes per cached pair) with the register-held columns and the
+// warp reduce-scatter of pwa_eval_cached_wred; contiguous runs keep every
+// warp's addresses within a few pages and balance the work to one unit.
+#ifndef PWA_WIDE_WARPS
+#define PWA_WIDE_WARPS 16
+#endif
+extern "C" __global__ void __launch_bounds__(PWA_WIDE_WARPS * 32, 1)
+    pwa_eval_cached_wide(const CCoup c, const float2* __restrict__ Fc,
+                         const double* __restrict__ Wc, long long ntiles,
+                         double* __restrict__ partials, unsigned int* __restrict__ ticket,
+                         double* __restrict__ out, double seq) {
+  constexpr int NA = PWA_CACHE_NA, MG = PWA_MG;
+  constexpr int NW = PWA_WIDE_WARPS, UPT = PWA_TPB / 32;
+  __shared__ double red[NW][NA];
+  __shared__ double s_c[2 * PWA_NCOL];
+  __shared__ double scratch[NW * 32];
+  __shared__ int s_last;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  stage_couplings(c, s_c);
+  __syncthreads();
+  const CoupShared cp{s_c};
+  const long long U = ntiles * UPT, W = (long long)gridDim.x * NW;
+  const long long gw = (long long)blockIdx.x * NW + warp;
+  const long long u0 = gw * U / W, u1 = (gw + 1) * U / W;
+  double acc0 = 0.0;
+  double accg[MG];
+#pragma unroll
+  for (int m = 0; m < MG; ++m) accg[m] = 0.0;
+#pragma unroll 1
+  for (long long u = u0; u < u1; ++u) {
+    const long long t = u / UPT;
+    const int e = (int)(u - t * UPT) * 32 + lane;
+    const float2* F = Fc + t * PWA_NF * PWA_TPB + e;
+    float2 v[PWA_NF];
+#pragma unroll
+    for (int j = 0; j < PWA_NF; ++j) v[j] = __ldcs(F + j * PWA_TPB);
+    const double w = __ldcs(Wc + t * PWA_TPB + e);
+    float gs[MG];
+    acc0 += cached_event_rs(v, w, cp, lane, gs);
+#pragma unroll
+    for (int m = 0; m < MG; ++m) accg[m] += (double)gs[m];
+  }
+  cached_block_row<NW>(acc0, accg, red, warp, lane, true, partials);
+  if (!flat_sum(partials, ticket, NA, out, scratch, &s_last)) return;
+  publish_result(ticket, NA, out, seq);
+}
+
+// Variant 5: warp-specialised ring, one block per SM.  One producer lane
+// keeps up to `stages` (<= PWA_TMA_MAXST) whole 128-event tiles in flight
+// with cp.async.bulk (no multicast) into a shared-memory ring; a stage has
+// a full barrier (transaction bytes) and an empty barrier (one arrival per
+// consumer warp of the group that reads it).  PWA_TMA_GROUPS groups of
+// PWA_TPB / 32 consumer warps take the block's tiles in turn; a consumer
+// warp copies its 32 events' columns to registers, releases the stage at
+// once, then evaluates them as pwa_eval_cached_wred does.  The block's tiles
+// are one contiguous run.  Waits are bounded: a wait that gives up sets the
+// error flag, the producer waits (bounded) for every copy it issued, and
+// the host sees out[NA] != 0.
+#ifndef PWA_TMA_GROUPS
+#define PWA_TMA_GROUPS 2
+#endif
+#define PWA_TMA_MAXST 8
+#define PWA_TMA_THREADS ((PWA_TMA_GROUPS * (PWA_TPB / 32) + 1) * 32)
+extern "C" __global__ void __launch_bounds__(PWA_TMA_THREADS, 1)
+    pwa_eval_cached_tma(const CCoup c, const float2* __restrict__ Fc,
+                        const double* __restrict__ Wc, long long ntiles,
+                        double* __restrict__ partials, unsigned int* __restrict__ ticket,
+                        double* __restrict__ out, double seq, int stages) {
+  constexpr int NA = PWA_CACHE_NA, MG = PWA_MG;
+  constexpr int UPT = PWA_TPB / 32, NCW = PWA_TMA_GROUPS * UPT;
+  constexpr unsigned TILE_F = PWA_NF * PWA_TPB * sizeof(float2);
+  constexpr unsigned TILE_W = PWA_TPB * sizeof(double);
+  constexpr unsigned STAGE = TILE_F + TILE_W;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ __align__(8) unsigned long long full[PWA_TMA_MAXST], empty[PWA_TMA_MAXST];
+  __shared__ double red[NCW][NA];
+  __shared__ double s_c[2 * PWA_NCOL];
+  __shared__ double scratch[PWA_TMA_THREADS];
+  __shared__ int s_last;
+  __shared__ volatile int s_err;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) {
+    s_err = 0;
+    for (int st = 0; st < stages; ++st) {
+      mbar_init(&full[st], 1);
+      mbar_init(&empty[st], UPT);
+    }
+    mbar_fence_init();
+  }
+  stage_couplings(c, s_c);
+  __syncthreads();
+  const long long B = gridDim.x, b = blockIdx.x;
+  const long long t0 = b * ntiles / B, t1 = (b + 1) * ntiles / B;
+  const int n_it = (int)(t1 - t0);
+  double acc0 = 0.0;
+  double accg[MG];
+#pragma unroll
+  for (int m = 0; m < MG; ++m) accg[m] = 0.0;
+  int issued = 0;
+  if (warp == NCW) {
+    if (lane == 0) {
+      for (int it = 0; it < n_it; ++it) {
+        const int st = it % stages;
+        if (it >= stages &&
+            !mbar_wait(&empty[st], (unsigned)((it / stages - 1) & 1), PWA_WAIT_LIMIT)) {
+          s_err = 1;
+          break;
+        }
+        if (s_err) break;
+        fence_proxy_async_smem();
+        unsigned char* dst = smem_raw + (size_t)st * STAGE;
+        mbar_expect_tx(&full[st], STAGE);
+        bulk_g2s(dst, Fc + (t0 + it) * PWA_NF * PWA_TPB, TILE_F, &full[st]);
+        bulk_g2s(dst + TILE_F, Wc + (t0 + it) * PWA_TPB, TILE_W, &full[st]);
+        issued = it + 1;
+      }
+    }
+  } else {
+    const int g = warp / UPT, q = warp % UPT;
+    const CoupShared cp{s_c};
+    for (int it = g; it < n_it; it += PWA_TMA_GROUPS) {
+      const int st = it % stages;
+      if (!mbar_wait(&full[st], (unsigned)((it / stages) & 1), PWA_WAIT_LIMIT)) s_err = 1;
+      if (s_err) break;
+      const unsigned char* src = smem_raw + (size_t)st * STAGE;
+      const float2* F = (const float2*)src + q * 32 + lane;
+      float2 v[PWA_NF];
+#pragma unroll
+      for (int j = 0; j < PWA_NF; ++j) v[j] = F[j * PWA_TPB];
+      const double w = ((const double*)(src + TILE_F))[q * 32 + lane];
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[st]);
+      float gs[MG];
+      acc0 += cached_event_rs(v, w, cp, lane, gs);
+#pragma unroll
+      for (int m = 0; m < MG; ++m) accg[m] += (double)gs[m];
+    }
+  }
+  __syncthreads();
+  if (s_err && warp == NCW && lane == 0) {
+    // no copy may still be writing shared memory when the block exits: wait
+    // (bounded) for the last phase of every stage that received a copy
+    for (int it = issued - stages > 0 ? issued - stages : 0; it < issued; ++it)
+      mbar_wait(&full[it % stages], (unsigned)((it / stages) & 1), PWA_WAIT_LIMIT);
+    atomicOr((unsigned int*)(ticket + 1), 1u);
+  }
+  cached_block_row<NCW>(acc0, accg, red, warp, lane, warp < NCW, partials);
+  if (!flat_sum(partials, ticket, NA, out, scratch, &s_last)) return;
+  publish_result(ticket, NA, out, seq);
+}
+
+// ---------------------------------------------------------------------------
 // Many fits in one launch (serving).  Each fit's data-event column cache is a
 // run of tiles in a shared pool (same tile layout as above).  The launch gets
 // a work list of (request, pool tile) pairs covering the tiles of every fit
@@ -944,13 +1212,13 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, PWA_WRED_MINB)
 #pragma unroll
     for (int j = 0; j < PWA_NF; ++j) v[j] = __ldcs(F + j * PWA_TPB);
     const double w = __ldcs(Wc + t * PWA_TPB + tid);
-    float gs[PWA_GPAD / 32];
+    float gs[PWA_MG];
     const double s0 = warp_sum(cached_event_rs(v, w, cp, lane, gs));
     if (lane == 0) red[warp][0] = s0;
 #pragma unroll
-    for (int m = 0; m < PWA_GPAD / 32; ++m) {
-      const int idx = 32 * m + lane;
-      if (idx < NG) red[warp][1 + idx] = (double)gs[m];
+    for (int m = 0; m < PWA_MG; ++m) {
+      const int idx = rs_entry(m, lane);
+      if (rs_owner(lane) && idx < NG) red[warp][1 + idx] = (double)gs[m];
     }
     __syncthreads();
     for (int j = tid; j < NA; j += PWA_TPB) {

@@ -37,7 +37,7 @@ struct Kernels {
                pdf_f32 = nullptr, columns_f64 = nullptr, gram_f64 = nullptr, sum_rows = nullptr,
                to_f32 = nullptr, cache_f32 = nullptr, eval_cached = nullptr,
                eval_cached_direct = nullptr, eval_cached_wred = nullptr, eval_cached_ring2 = nullptr,
-               eval_multi = nullptr, reduce_multi = nullptr,
+               eval_cached_wide = nullptr, eval_cached_tma = nullptr, eval_multi = nullptr, reduce_multi = nullptr,
                fields_from_p4 = nullptr, toy_select = nullptr, toy_fields = nullptr;
 };
 
@@ -66,9 +66,15 @@ struct pwa_plan {
   long long ntiles = 0, ntiles_cap = 0, fcache_n = 0;
   int cached_blocks = 0, cached_blocks_direct = 0, cached_blocks_wred = 0, cached_blocks_ring2 = 0;
   size_t cached_smem_ring2 = 0;
+  // one block per SM: the wide kernel and the warp-specialised bulk-copy ring
+  int cached_blocks_wide = 0, cached_blocks_tma = 0, tma_stages = 0, tma_threads = 0,
+      wide_threads = 0;
+  size_t cached_smem_tma = 0;
   // 0: shared-memory ring (bulk copies), 1: direct loads with per-thread FP64
   // column sums, 2: direct loads with warp reduce-scatter of the column sums;
   // 3: shared-memory ring (2 stages) with warp reduce-scatter column sums;
+  // 4: one block per SM, contiguous warp runs, single-level reduction;
+  // 5: one block per SM, producer warp + deep bulk-copy ring;
   // -1: automatic (2)
   int cached_variant = -1;
   size_t cached_smem = 0;
@@ -349,6 +355,8 @@ int pwa_plan_create(const char* src, size_t src_len, int n_mass, int n_angle, in
             {"pwa_eval_cached_direct", &h->k.eval_cached_direct},
             {"pwa_eval_cached_wred", &h->k.eval_cached_wred},
             {"pwa_eval_cached_ring2", &h->k.eval_cached_ring2},
+            {"pwa_eval_cached_wide", &h->k.eval_cached_wide},
+            {"pwa_eval_cached_tma", &h->k.eval_cached_tma},
             {"pwa_fields_from_p4", &h->k.fields_from_p4},
             {"pwa_toy_select", &h->k.toy_select},
             {"pwa_toy_fields", &h->k.toy_fields},
@@ -696,6 +704,34 @@ int pwa_cache_data(pwa_plan* h, const double* consts, void* stream) {
   if (per_sm4 < 1) return set_err(h, PWA_ERR_ARG, "column tile does not fit in shared memory");
   long long want4 = (long long)per_sm4 * h->sms;
   h->cached_blocks_ring2 = (int)(want4 < ntiles ? want4 : ntiles);
+  // one block per SM (variants 4, 5): block size from the kernels' own
+  // launch bounds, ring depth from the shared memory left beside the
+  // static arrays
+  {
+    cudaFuncAttributes a;
+    CU(cudaFuncGetAttributes(&a, (const void*)h->k.eval_cached_wide));
+    h->wide_threads = a.maxThreadsPerBlock;
+    CU(cudaFuncGetAttributes(&a, (const void*)h->k.eval_cached_tma));
+    h->tma_threads = a.maxThreadsPerBlock;
+    int optin = 0;
+    CU(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
+    const size_t stage = (size_t)tile * (h->nf * sizeof(float2) + sizeof(double));
+    long long st = ((long long)optin - (long long)a.sharedSizeBytes - 1024) / (long long)stage;
+    if (st > 8) st = 8;  // PWA_TMA_MAXST
+    h->tma_stages = (int)st;
+    h->cached_smem_tma = (size_t)st * stage;
+    h->cached_blocks_wide = (int)(h->sms < ntiles ? h->sms : ntiles);
+    h->cached_blocks_tma = 0;
+    if (st >= 2) {
+      CU(cudaFuncSetAttribute((const void*)h->k.eval_cached_tma,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)h->cached_smem_tma));
+      int per = 0;
+      CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void*)h->k.eval_cached_tma,
+                                                       h->tma_threads, h->cached_smem_tma));
+      if (per >= 1) h->cached_blocks_tma = (int)(h->sms < ntiles ? h->sms : ntiles);
+    }
+  }
   int mb = h->cached_blocks > h->cached_blocks_direct ? h->cached_blocks : h->cached_blocks_direct;
   if (h->cached_blocks_wred > mb) mb = h->cached_blocks_wred;
   if (h->cached_blocks_ring2 > mb) mb = h->cached_blocks_ring2;
@@ -719,9 +755,17 @@ int pwa_eval_cached_enqueue(pwa_plan* h, const double* ck, void* stream) {
   h->seq += 1.0;
   double seq = h->seq;
   void* args[] = {cbuf.data(), &h->fcache, &h->wcache, &nt, &h->partials, &h->ticket, &h->d_map,
-                  &seq};
-  const int variant = h->cached_variant >= 0 ? h->cached_variant : 2;
+                  &seq, &h->tma_stages};
+  int variant = h->cached_variant >= 0 ? h->cached_variant : 2;
+  if (variant == 5 && h->cached_blocks_tma == 0) variant = 4;  // ring does not fit
   cudaError_t e =
+      variant == 4   ? cudaLaunchKernel((const void*)h->k.eval_cached_wide,
+                                        dim3(h->cached_blocks_wide), dim3(h->wide_threads), args,
+                                        0, s)
+      : variant == 5 ? cudaLaunchKernel((const void*)h->k.eval_cached_tma,
+                                        dim3(h->cached_blocks_tma), dim3(h->tma_threads), args,
+                                        h->cached_smem_tma, s)
+      :
       variant == 1   ? cudaLaunchKernel((const void*)h->k.eval_cached_direct,
                                         dim3(h->cached_blocks_direct), dim3(h->tpb), args, 0, s)
       : variant == 2 ? cudaLaunchKernel((const void*)h->k.eval_cached_wred,
@@ -774,7 +818,7 @@ int cached_result(pwa_plan* h, const double** sums) {
 
 int pwa_set_cached_variant(pwa_plan* h, int variant) {
   if (!h) return PWA_ERR_ARG;
-  if (variant < -1 || variant > 3) return set_err(h, PWA_ERR_ARG, "variant must be -1 .. 3");
+  if (variant < -1 || variant > 5) return set_err(h, PWA_ERR_ARG, "variant must be -1 .. 5");
   h->cached_variant = variant;
   return PWA_OK;
 }

@@ -151,24 +151,35 @@ def cg_matrix(ja, jb, jc, ls, hel_b, hel_c):
 
 @lru_cache(maxsize=None)
 def small_d_weight(j2):
-    """w[l, m1, m2] with d^{j}_{m1 m2}(b) = sum_l w sin^l(b/2) cos^{2j-l}(b/2).
+    """w[l, a, b] with d^j_{m' m}(beta) = sum_l w[l, a, b] x^l y^(2j - l),
+    x = sin(beta/2), y = cos(beta/2), a = m' + j, b = m + j, ``j2`` = 2j.
 
-    ``j2`` = 2j; indices m1, m2 run over (m+j).  Restates the weight table of
-    ``tf_pwa/dfun.py:118-143`` (Wigner's explicit formula)."""
-    j = j2
-    ret = np.zeros((j + 1, j + 1, j + 1))
-
-    def f(x):
-        return math.factorial(x >> 1)
-
-    for m in range(-j, j + 1, 2):
-        for n in range(-j, j + 1, 2):
-            for k in range(max(0, n - m), min(j - m, j + n) + 1, 2):
-                l = (2 * k + (m - n)) // 2
-                sign = (-1) ** ((k + m - n) // 2)
-                tmp = sign * math.sqrt(1.0 * f(j + m) * f(j - m) * f(j + n) * f(j - n))
-                tmp /= f(j - m - k) * f(j + n - k) * f(k + m - n) * f(k)
-                ret[l][(m + j) // 2][(n + j) // 2] = tmp
+    Derived from the spinor (two-variable polynomial) picture of SU(2):
+    |j m> is u^(j+m) v^(j-m) / sqrt((j+m)! (j-m)!), and the rotation about y
+    maps u -> y u + x v, v -> -x u + y v (the spin-1/2 matrix
+    [[y, -x], [x, y]]).  Expanding (y u + x v)^(j+m) (-x u + y v)^(j-m) with
+    binomials, the coefficient of u^(j+m') v^(j-m') times
+    sqrt((j+m')! (j-m')! / ((j+m)! (j-m)!)) is d^j_{m' m}.  Integer
+    binomial sums, one square root per (m', m).  The table is the same
+    quantity as ``tf_pwa/dfun.py:118-143`` (pinned to it in the tests)."""
+    n = j2  # 2j
+    ret = np.zeros((n + 1, n + 1, n + 1))
+    fact = math.factorial
+    for b in range(n + 1):  # m + j
+        up, dn = b, n - b  # powers of u and v in |j m>
+        for a in range(n + 1):  # m' + j
+            # coefficient of u^a v^(n-a): choose p u's from the first
+            # factor (weight y^p x^(up-p)) and q = a - p from the second
+            # (weight (-x)^q y^(dn-q)); the power of x is up - p + q
+            coef = {}
+            for p in range(max(0, a - dn), min(up, a) + 1):
+                q = a - p
+                c = math.comb(up, p) * math.comb(dn, q) * (-1) ** q
+                lx = up - p + q
+                coef[lx] = coef.get(lx, 0) + c
+            norm = math.sqrt(fact(a) * fact(n - a) / (fact(b) * fact(n - b)))
+            for lx, c in coef.items():
+                ret[lx, a, b] = c * norm
     return ret
 
 
