@@ -143,8 +143,16 @@ int pwa_hessian_cached(pwa_plan* h, const double* vars, double sum_w, double ste
 int pwa_read_dat(const char* path, double* out, long long cap, long long* n_values);
 
 /* Gram matrix of the MC set, M_kl = sum_i w_i sum_o conj(F_ik,o) F_il,o,
- * in FP64; out[2*ncol*ncol] host, (re, im) row-major. */
+ * to FP64 accuracy; out[2*ncol*ncol] host, (re, im) row-major. */
 int pwa_build_gram(pwa_plan* h, const double* consts, void* stream, double* out);
+
+/* How pwa_build_gram contracts the columns (tf_pwa/model/opt_int.py:128-296
+ * builds the same matrix with a TF einsum): 0 = FP64 on the CUDA cores,
+ * 1 = tensor cores (tcgen05 int8 MMAs on seven exact slices of every value,
+ * exact int32 accumulation, FP64 recombination; models with at most 32
+ * columns, others use 0), -1 = automatic (1 where it applies).  The error
+ * flag of the tensor-core kernel turns into PWA_ERR_CUDA. */
+int pwa_set_gram_method(pwa_plan* h, int method);
 
 /* ---- fixed masses/widths: cached partial-wave columns -------------------
  * The reference's cached-integral / cached-amplitude modes
@@ -161,8 +169,10 @@ int pwa_cache_data(pwa_plan* h, const double* consts, void* stream);
  * events reduce-scattered in FP32 before FP64 accumulation (register use
  * independent of the column count), 3 = shared-memory ring (two stages)
  * whose consumers read their columns from shared memory and reduce-scatter
- * the column sums, -1 = automatic (default: 2, the fastest measured on
- * the shipped models). */
+ * the column sums, 4 = one block of 16 warps per SM, each warp a
+ * contiguous run of events, single-level ordered reduction, 5 = one block
+ * per SM with a producer warp keeping a deep ring of bulk copies in flight
+ * for 8 consumer warps, -1 = automatic (default: 2). */
 int pwa_set_cached_variant(pwa_plan* h, int variant);
 
 /* Data-term kernels on the cache with column couplings ck[2*ncol]
@@ -219,8 +229,9 @@ int pwa_pieces_multi(pwa_plan* h, int n_req, const long long* first_tile, const 
 
 /* Allocation-free variant of pwa_eval's device work (plain FP64 kernels),
  * with no counterpart in the reference.  For callers that cannot call
- * cudaMalloc while they run (inside a stream capture, or under a framework
- * that owns all device memory).  The caller passes device inputs xm
+ * cudaMalloc while they run: a host framework that owns every device byte
+ * through its own arena and forbids plug-ins from allocating, or a loop
+ * that must not take the allocator's locks.  The caller passes device inputs xm
  * [n_mass][ld], xa [n_angle][ld], w [ld] (data rows first, then MC, same
  * meaning as pwa_upload_events) and a device output out[2*nacc] (data sums,
  * then MC sums, as pwa_eval).  Block partials live in a fixed device array
@@ -228,11 +239,27 @@ int pwa_pieces_multi(pwa_plan* h, int n_req, const long long* first_tile, const 
  * by every GPU that loads the library until exit); models with more than
  * 256 accumulators are rejected with PWA_ERR_ARG.  Allocates nothing and
  * does not wait.  The first call on a device looks up the array's device
- * address; make that first call before any stream capture.  Calls share the
- * array: calls that overlap on the GPU race. */
+ * address; make that first call before any stream capture.  The address is
+ * kept for the life of the process: a cudaDeviceReset in between is not
+ * supported.  The current device must be the plan's (else PWA_ERR_STATE).
+ * The array is built as sm_100a code: this call needs a compute capability
+ * 10.0 GPU.  Calls share the array: calls that overlap on the GPU race. */
 int pwa_eval_noalloc(pwa_plan* h, const double* consts, const double* xm, const double* xa,
                      const double* w, long long n_data, long long n_mc, long long ld,
                      double* out, void* stream);
+
+/* Check of the failure detection of the cached evaluation, with no
+ * counterpart in the reference (its fit loop reports a failed evaluation,
+ * tf_pwa/fit.py:13-15,257-260).  mode 0 launches a one-block kernel whose
+ * barrier wait gives up after `polls` polls (the bytes it waits for are
+ * never sent; the one copy it did issue is drained before it exits) and
+ * publishes the error flag as a stalled cached kernel would; mode 1
+ * launches nothing, so the host's poll of the mapped result gives up after
+ * host_limit_s seconds.  Returns what an evaluation would: PWA_ERR_CUDA
+ * with "a barrier wait timed out" (mode 0) or "stale result" (mode 1) in
+ * pwa_last_error.  The plan stays usable.  ticket memory (>= 1 KB) is the
+ * copy's source. */
+int pwa_wait_check(pwa_plan* h, int mode, unsigned polls, double host_limit_s, void* stream);
 
 /* info[0..7]: registers/thread of eval_f64, eval_f32, local bytes f64, f32,
  * blocks, blocks_data, nacc, threads per block. */

@@ -12,6 +12,7 @@
 #include <math.h>
 
 #define __device__
+#define __host__
 #define __forceinline__ inline
 #define __ldg(p) (*(p))
 

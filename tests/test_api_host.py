@@ -14,42 +14,6 @@ from common import CONFIGS, load_golden
 from hostexec import HostModel
 
 
-@pytest.fixture()
-def host_engine(monkeypatch, tmp_path):
-    """Engine whose plan creation, upload and evaluation run on the host."""
-    import tf_pwa_b200.engine as E
-
-    built = {}
-
-    def _create(self):
-        self.h = None
-        key = self.src
-        if key not in built:
-            built[key] = HostModel(self.code, str(tmp_path))
-        self._host = built[key]
-
-    def upload(self, x_data, w_data, x_mc=None, w_mc=None, stream=None):
-        xd = np.asarray(x_data, np.float64)
-        wd = np.asarray(w_data, np.float64)
-        xm = np.asarray(x_mc, np.float64)
-        wm = np.ones(xm.shape[1]) if w_mc is None else np.asarray(w_mc, np.float64)
-        self._hx = (np.concatenate([xd, xm], 1), np.concatenate([wd, wm / wm.sum()]),
-                    xd.shape[1])
-        self._n_data, self._n_mc = xd.shape[1], xm.shape[1]
-        self._sw = float(wd.sum())
-        self._gram = None
-
-    def eval_sums(self, C, precision=E.PLAIN_F64, mc=True, stream=None):
-        x, w, nd = self._hx
-        return self._host.sums(C, x, w, nd, f32=precision == E.MIXED_F32)
-
-    monkeypatch.setattr(E.Engine, "_create", _create)
-    monkeypatch.setattr(E.Engine, "upload", upload)
-    monkeypatch.setattr(E.Engine, "eval_sums", eval_sums)
-    monkeypatch.setattr(E.Engine, "close", lambda self: None)
-    return E
-
-
 def _config(tmp_path, name):
     """The golden events written as the reference's data files."""
     g, meta = load_golden(name)

@@ -1,8 +1,8 @@
 """The allocation-free entry point ``pwa_eval_noalloc``.
 
-Some callers cannot call cudaMalloc while they run -- for example code that
-records work inside a CUDA stream capture, or a host framework that hands
-out all device memory from its own arena.  ``pwa_eval_noalloc`` evaluates
+Some callers cannot call cudaMalloc while they run -- for example a host
+framework that hands out all device memory from its own arena, or a loop
+that must not take the allocator's locks.  ``pwa_eval_noalloc`` evaluates
 the fused FP64 kernels on events the caller already holds on the device and
 writes the sums into a caller-provided device buffer, keeping its block
 partials in a fixed device array inside the library instead of allocating.

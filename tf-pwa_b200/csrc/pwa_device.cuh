@@ -235,6 +235,72 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned pari
   return false;
 }
 
+// ------------------------------------------------ tensor memory / tcgen05
+// Fifth-generation tensor-core primitives (sm_100a): tensor-memory
+// allocation, MMA issue from shared-memory descriptors, completion through
+// an mbarrier, and loads of the accumulator back into registers.
+__device__ __forceinline__ void tmem_alloc(unsigned* dst_smem, unsigned ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                   smem_addr(dst_smem)),
+               "r"(ncols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(unsigned taddr, unsigned ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols)
+               : "memory");
+}
+// Shared-memory matrix descriptor, K-major, no swizzle: core matrices of 8
+// rows x 16 bytes stored contiguously; `sbo` = bytes between core matrices
+// adjacent in the M/N direction, `lbo` = bytes between the two 16-byte K
+// halves of one 32-byte K step; version field 1 (sm_100).
+__device__ __forceinline__ unsigned long long umma_desc(const void* p, unsigned lbo, unsigned sbo) {
+  const unsigned long long a = (smem_addr(p) >> 4) & 0x3FFFu;
+  return a | ((unsigned long long)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((unsigned long long)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+// Instruction descriptor of kind::i8: signed A and B, S32 accumulator, both
+// operands K-major, M (64 or 128) and N (multiple of 16 up to 256).
+__host__ __device__ constexpr unsigned umma_idesc_s8(int m, int n) {
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(n >> 3) << 17) |
+         ((unsigned)(m >> 4) << 24);
+}
+// D[tmem] (+)= A . B^T with int8 operands from shared memory (one thread).
+__device__ __forceinline__ void umma_s8(unsigned d_tmem, unsigned long long a_desc,
+                                        unsigned long long b_desc, unsigned idesc, bool accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n}" ::"r"(d_tmem),
+      "l"(a_desc), "l"(b_desc), "r"(idesc), "r"((unsigned)accumulate)
+      : "memory");
+}
+// arrive on `bar` once every MMA this thread issued so far has completed
+__device__ __forceinline__ void umma_commit(unsigned long long* bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+          smem_addr(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+// 16 consecutive 32-bit accumulator columns of this thread's lane
+__device__ __forceinline__ void tmem_ld16(unsigned taddr, int (&v)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+      "%14,%15}, [%16];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+        "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+        "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() {
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
 // ------------------------------------------------------------ kinematics
 // FP64 four-vector algebra for the dataset step (four-momenta -> masses,
 // helicity and alignment angles), restating tf_pwa/angle.py

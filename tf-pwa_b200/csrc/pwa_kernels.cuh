@@ -25,6 +25,11 @@
 #ifndef PWA_TPB
 #define PWA_TPB 128
 #endif
+// polls of an mbarrier before a wait gives up (the kernel then reports an
+// error instead of hanging)
+#ifndef PWA_WAIT_LIMIT
+#define PWA_WAIT_LIMIT (1u << 22)
+#endif
 
 template <typename R>
 __device__ __forceinline__ void eval_body(const Consts& C, const R* __restrict__ XA,
@@ -233,6 +238,255 @@ extern "C" __global__ void pwa_sum_rows(const double* __restrict__ in, int nrows
   }
 }
 
+// ---------------------------------------------------------------------------
+// Gram matrix on the tensor cores, exact-integer sliced products (the Ozaki
+// scheme: Ozaki, Ogita, Oishi, Rump, Numer. Algorithms 59 (2012); integer
+// tensor cores as in Ootomo, Ozaki, Yokota, IJHPCA 38 (2024)).
+//
+// Rows r = (event i, helicity o) of X[r][c] = Re F_ic,o (c < NCOL) or
+// Im F_i(c-NCOL),o and of Y = w_i X; G = X^T Y (KC x KC real, KC = 2 NCOL)
+// holds Re M = G_RR + G_II and Im M = G_RI - G_IR.  Column c of X is scaled
+// by 2^-eA_c (max |X_c| < 2^eA_c * 127/128) and split into PWA_OZ_S int8
+// slices a_s (weights 2^-7s, |a_1| <= 127, |a_s| <= 64 after): x =
+// 2^eA (sum_s a_s 2^-7s) + O(2^(eA-7S-1)), every step exact in FP64.  The
+// products a_s b_t with s + t = g <= S + 1 accumulate exactly in int32 in
+// the tensor memory (one accumulator per g, KC x CP columns, rows >= KC of
+// the M = 128 tile zero), flushed to FP64 registers every PWA_OZ_FLUSH
+// rows (int32 cannot overflow: rows x sum |a_s b_t| < 2^31), and
+// G_cd = 2^(eA_c + eB_d) sum_g D_g 2^-7g.  Truncation error ~2^-49 of the
+// column maxima per product: FP64-level.
+#define PWA_OZ_S 7
+#define PWA_OZ_KC (2 * PWA_NCOL)
+#define PWA_OZ_CP ((PWA_OZ_KC + 15) / 16 * 16)
+#define PWA_OZ_KB 64                       // rows per shared-memory stage
+#define PWA_OZ_FLUSH 16384                 // rows between accumulator flushes
+#define PWA_OZ_ABYTES (128 * PWA_OZ_KB)    // one A slice: M = 128 rows x KB
+#define PWA_OZ_BBYTES (PWA_OZ_CP * PWA_OZ_KB)
+#define PWA_OZ_STAGE (PWA_OZ_S * (PWA_OZ_ABYTES + PWA_OZ_BBYTES))
+#define PWA_OZ_TCOLS (PWA_OZ_S * PWA_OZ_CP <= 32 ? 32 : PWA_OZ_S * PWA_OZ_CP <= 64 ? 64 \
+                      : PWA_OZ_S * PWA_OZ_CP <= 128 ? 128 : PWA_OZ_S * PWA_OZ_CP <= 256 ? 256 : 512)
+#define PWA_OZ_OK (PWA_OZ_KC <= 64)
+
+// Column maxima of |X| and |w X| over n events of F (rows of NCOL*NOUT
+// complex): mx[c] and mx[KC + c] as FP64 bit patterns (non-negative
+// doubles order like their bits), combined with atomicMax.
+extern "C" __global__ void __launch_bounds__(PWA_TPB)
+    pwa_gram_colmax(const double* __restrict__ F, const double* __restrict__ W, long long n,
+                    unsigned long long* __restrict__ mx) {
+  constexpr int KC = PWA_OZ_KC, NO = PWA_NOUT;
+  for (int c = 0; c < KC; ++c) {
+    double ma = 0.0, mb = 0.0;
+    const int k = c % PWA_NCOL, im = c / PWA_NCOL;
+    for (long long i = (long long)blockIdx.x * PWA_TPB + threadIdx.x; i < n;
+         i += (long long)gridDim.x * PWA_TPB) {
+      const double w = fabs(W[i]);
+#pragma unroll
+      for (int o = 0; o < NO; ++o) {
+        const double x = fabs(F[i * (2LL * PWA_NCOL * NO) + 2 * (k * NO + o) + im]);
+        ma = fmax(ma, x);
+        mb = fmax(mb, w * x);
+      }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      ma = fmax(ma, __shfl_xor_sync(0xffffffffu, ma, off));
+      mb = fmax(mb, __shfl_xor_sync(0xffffffffu, mb, off));
+    }
+    if ((threadIdx.x & 31) == 0) {
+      atomicMax(mx + c, (unsigned long long)__double_as_longlong(ma));
+      atomicMax(mx + KC + c, (unsigned long long)__double_as_longlong(mb));
+    }
+  }
+}
+
+// exponent e with max < 2^e * 127/128 (0 for an all-zero column)
+__device__ __forceinline__ int oz_exponent(double mx) {
+  if (!(mx > 0.0)) return 0;
+  int e;
+  const double m = frexp(mx, &e);  // mx = m 2^e, m in [0.5, 1)
+  return m * 128.0 <= 127.0 ? e : e + 1;
+}
+
+// int8 slices of x 2^-e packed four rows at a time: word[s] byte j = slice
+// s of value j
+__device__ __forceinline__ void oz_slices4(const double (&x)[4], int e, unsigned (&word)[PWA_OZ_S]) {
+#pragma unroll
+  for (int s = 0; s < PWA_OZ_S; ++s) word[s] = 0u;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    double v = ldexp(x[j], 7 - e);  // first slice's scale: |v| < 127
+#pragma unroll
+    for (int s = 0; s < PWA_OZ_S; ++s) {
+      const double a = rint(v);
+      word[s] |= ((unsigned)(int)a & 0xFFu) << (8 * j);
+      v = (v - a) * 128.0;  // exact: the fraction of v, then 7 more bits
+    }
+  }
+}
+
+// One block per SM, PWA_TPB threads; dynamic shared memory: two stages of
+// PWA_OZ_STAGE bytes (1024-aligned).  Block b takes a contiguous run of the
+// rows; it writes partial[b][c][d] (KC x KC FP64) for an ordered sum.
+// e8[2 KC]: column maxima (pwa_gram_colmax) as FP64 bits.  err[0] is set
+// when a wait on the tensor cores gives up.
+extern "C" __global__ void __launch_bounds__(PWA_TPB, 1)
+    pwa_gram_tc(const double* __restrict__ F, const double* __restrict__ W, long long n,
+                const unsigned long long* __restrict__ e8, double* __restrict__ partial,
+                unsigned int* __restrict__ err) {
+#if PWA_OZ_OK
+  constexpr int KC = PWA_OZ_KC, CP = PWA_OZ_CP, S = PWA_OZ_S, KB = PWA_OZ_KB;
+  constexpr int NO = PWA_NOUT, NQ = KB / 4;  // four-row groups per stage
+  constexpr unsigned IDESC = umma_idesc_s8(128, CP);
+  extern __shared__ __align__(1024) unsigned char oz_smem[];
+  __shared__ __align__(8) unsigned long long done[2];
+  __shared__ unsigned s_tmem;
+  __shared__ int s_e[2 * KC];
+  __shared__ int s_err;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  unsigned char* base = (unsigned char*)(((size_t)oz_smem + 1023) & ~(size_t)1023);
+  // zero both stages (A rows >= KC stay zero), exponents, barriers, TMEM
+  for (int j = tid; j < 2 * PWA_OZ_STAGE / 4; j += PWA_TPB) ((unsigned*)base)[j] = 0u;
+  for (int c = tid; c < 2 * KC; c += PWA_TPB) s_e[c] = oz_exponent(__longlong_as_double((long long)e8[c]));
+  if (tid == 0) {
+    s_err = 0;
+    mbar_init(&done[0], 1);
+    mbar_init(&done[1], 1);
+    mbar_fence_init();
+  }
+  __syncwarp();
+  if (warp == 0) tmem_alloc(&s_tmem, PWA_OZ_TCOLS);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const unsigned tmem = s_tmem;
+  const long long R = n * NO;
+  const long long r0 = (long long)blockIdx.x * R / gridDim.x;
+  const long long r1 = (long long)(blockIdx.x + 1) * R / gridDim.x;
+  double acc[CP];
+#pragma unroll
+  for (int d = 0; d < CP; ++d) acc[d] = 0.0;
+  int uses[2] = {0, 0};
+  bool fresh = true;  // next MMA of each accumulator starts it from zero
+  int stage = 0;
+  long long since_flush = 0;
+  for (long long rb = r0; rb < r1 || since_flush > 0; rb += KB) {
+    const bool have = rb < r1;
+    const bool flush = !have || since_flush + KB > PWA_OZ_FLUSH;
+    if (flush && since_flush > 0) {
+      // wait for every MMA issued so far, then move the accumulators to FP64
+      for (int st = 0; st < 2; ++st)
+        if (uses[st] && !mbar_wait(&done[st], (unsigned)((uses[st] - 1) & 1), PWA_WAIT_LIMIT))
+          s_err = 1;
+      tc_fence_after();
+      __syncwarp();  // tcgen05.ld is warp-collective: reconverge first
+      if (warp < 2) {  // TMEM lanes 0..63 = rows c of the accumulators
+#pragma unroll
+        for (int g = 0; g < S; ++g) {
+          const double sc = ldexp(1.0, -7 * (g + 2));
+#pragma unroll
+          for (int q = 0; q < CP / 16; ++q) {
+            int v[16];
+            tmem_ld16(tmem + ((unsigned)(warp * 32) << 16) + (unsigned)(g * CP + 16 * q), v);
+            tmem_wait_ld();
+#pragma unroll
+            for (int j = 0; j < 16; ++j) acc[16 * q + j] = fma((double)v[j], sc, acc[16 * q + j]);
+          }
+        }
+      }
+      tc_fence_before();
+      __syncthreads();
+      tc_fence_after();
+      fresh = true;
+      since_flush = 0;
+      if (!have) break;
+    }
+    if (s_err) break;
+    // refill `stage`: its previous MMAs must be complete
+    if (uses[stage] && !mbar_wait(&done[stage], (unsigned)((uses[stage] - 1) & 1), PWA_WAIT_LIMIT))
+      s_err = 1;
+    unsigned char* A = base + (size_t)stage * PWA_OZ_STAGE;
+    unsigned char* B = A + (size_t)S * PWA_OZ_ABYTES;
+    for (int item = tid; item < 2 * KC * NQ; item += PWA_TPB) {
+      const bool isb = item >= KC * NQ;
+      const int it = isb ? item - KC * NQ : item;
+      const int c = it / NQ, kq = it % NQ;
+      const int k = c % PWA_NCOL, im = c / PWA_NCOL;
+      double x[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const long long r = rb + 4 * kq + j;
+        x[j] = 0.0;
+        if (r < r1) {
+          const long long i = r / NO;
+          const int o = (int)(r - i * NO);
+          x[j] = F[i * (2LL * PWA_NCOL * NO) + 2 * (k * NO + o) + im];
+          if (isb) x[j] *= W[i];
+        }
+      }
+      unsigned word[S];
+      oz_slices4(x, s_e[(isb ? KC : 0) + c], word);
+      // K-major core-matrix layout: byte (row m, k) = (k/16)*(M/8*128) +
+      // (m/8)*128 + (m%8)*16 + k%16 with M = 128 (A) or CP (B)
+      const int kk = 4 * kq;
+      const int mrows = isb ? CP : 128;
+      const int off = (kk / 16) * (mrows / 8 * 128) + (c / 8) * 128 + (c % 8) * 16 + (kk % 16);
+      unsigned char* dst = isb ? B : A;
+      const int sbytes = isb ? PWA_OZ_BBYTES : PWA_OZ_ABYTES;
+#pragma unroll
+      for (int s = 0; s < S; ++s) *(unsigned*)(dst + s * sbytes + off) = word[s];
+    }
+    fence_proxy_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    if (tid == 0) {
+      tc_fence_after();
+#pragma unroll 1
+      for (int q = 0; q < KB / 32; ++q) {
+#pragma unroll 1
+        for (int g = 2; g <= S + 1; ++g) {
+          bool first = fresh && q == 0;
+          for (int s = g - S > 1 ? g - S : 1; s <= S && s < g; ++s) {
+            const int t = g - s;
+            const unsigned long long ad =
+                umma_desc(A + (size_t)(s - 1) * PWA_OZ_ABYTES + 2 * q * (128 / 8 * 128),
+                          128 / 8 * 128, 128);
+            const unsigned long long bd =
+                umma_desc(B + (size_t)(t - 1) * PWA_OZ_BBYTES + 2 * q * (CP / 8 * 128), CP / 8 * 128,
+                          128);
+            umma_s8(tmem + (unsigned)((g - 2) * CP), ad, bd, IDESC, !first);
+            first = false;
+          }
+        }
+      }
+      umma_commit(&done[stage]);
+    }
+    __syncwarp();
+    // no barrier here: the other threads go on to fill the other stage
+    // while thread 0 issues; a stage is refilled only after its commit
+    uses[stage]++;
+    fresh = false;
+    since_flush += KB;
+    stage ^= 1;
+  }
+  if (s_err && tid == 0) atomicOr(err, 1u);
+  // wait (bounded) for any MMA still running before the tensor memory goes
+  for (int st = 0; st < 2; ++st)
+    if (uses[st]) mbar_wait(&done[st], (unsigned)((uses[st] - 1) & 1), PWA_WAIT_LIMIT);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  __syncwarp();
+  if (warp == 0) tmem_dealloc(tmem, PWA_OZ_TCOLS);
+  const int c = tid;
+  if (c < KC) {
+    const int ea = s_e[c];
+#pragma unroll
+    for (int d = 0; d < CP; ++d)
+      if (d < KC) partial[(long long)blockIdx.x * KC * KC + c * KC + d] = ldexp(acc[d], ea + s_e[KC + d]);
+  }
+#endif
+}
+
 // FP64 -> FP32 copy of the angle columns for the mixed-precision kernels.
 extern "C" __global__ void pwa_to_f32(const double* __restrict__ in, float* __restrict__ out,
                                       long long n) {
@@ -295,7 +549,6 @@ __device__ __forceinline__ void stage_couplings(const CCoup& c, double* s_c) {
 #define PWA_STAGES 3
 #endif
 #define PWA_CACHE_NA (1 + 2 * PWA_NCOL)
-#define PWA_WAIT_LIMIT (1u << 22)
 // Blocks per group of the two-level partial reduction, and the most groups
 // a launch may have (the ticket buffer holds 2 + PWA_MAX_GROUPS counters).
 #define PWA_GROUP 16
@@ -951,6 +1204,38 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB)
   __syncthreads();
   if (!grouped_sum(partials, ticket, NA, out, &s_last)) return;
   publish_result(ticket, NA, out, seq);
+}
+
+// ---------------------------------------------------------------------------
+// Check of the bounded waits and of the error protocol of the cached
+// kernels (one block, PWA_TPB threads).  Thread 0 arms barrier `never`
+// for one tile of bytes that no copy will bring, and barrier `real` for
+// one bulk copy of `src` that it does issue; it waits on `never` for
+// `polls` polls (the wait gives up), then waits (bounded) on `real`, so no
+// copy is in flight when the block exits, and publishes zero sums with
+// the error flag set -- what a stalled ring kernel reports.
+extern "C" __global__ void __launch_bounds__(PWA_TPB)
+    pwa_wait_check(const double* __restrict__ src, unsigned polls,
+                   unsigned int* __restrict__ ticket, double* __restrict__ out, double seq,
+                   int na) {
+  __shared__ __align__(128) double buf[PWA_TPB];
+  __shared__ __align__(8) unsigned long long never, real;
+  if (threadIdx.x == 0) {
+    mbar_init(&never, 1);
+    mbar_init(&real, 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    mbar_expect_tx(&never, (unsigned)sizeof(buf));
+    mbar_expect_tx(&real, (unsigned)sizeof(buf));
+    bulk_g2s(buf, src, (unsigned)sizeof(buf), &real);
+    const bool ok = mbar_wait(&never, 0u, polls);
+    mbar_wait(&real, 0u, PWA_WAIT_LIMIT);
+    if (!ok) atomicOr((unsigned int*)(ticket + 1), 1u);
+  }
+  for (int j = threadIdx.x; j < na; j += PWA_TPB) out[j] = 0.0;
+  publish_result(ticket, na, out, seq);
 }
 
 // ---------------------------------------------------------------------------

@@ -37,7 +37,8 @@ struct Kernels {
                pdf_f32 = nullptr, columns_f64 = nullptr, gram_f64 = nullptr, sum_rows = nullptr,
                to_f32 = nullptr, cache_f32 = nullptr, eval_cached = nullptr,
                eval_cached_direct = nullptr, eval_cached_wred = nullptr, eval_cached_ring2 = nullptr,
-               eval_cached_wide = nullptr, eval_cached_tma = nullptr, eval_multi = nullptr, reduce_multi = nullptr,
+               eval_cached_wide = nullptr, eval_cached_tma = nullptr, eval_multi = nullptr,
+               gram_colmax = nullptr, gram_tc = nullptr, wait_check = nullptr, reduce_multi = nullptr,
                fields_from_p4 = nullptr, toy_select = nullptr, toy_fields = nullptr;
 };
 
@@ -84,6 +85,7 @@ struct pwa_plan {
   double seq = 0.0;
   std::vector<double> gram;  // MC Gram matrix, (re, im) row-major ncol x ncol
   bool gram_valid = false;
+  int gram_method = -1;  // 0 FP64 CUDA cores, 1 tensor cores, -1 automatic
   // pool of column-cache tiles shared by many fits (serving)
   float2* pool_f = nullptr;
   double* pool_w = nullptr;
@@ -357,6 +359,9 @@ int pwa_plan_create(const char* src, size_t src_len, int n_mass, int n_angle, in
             {"pwa_eval_cached_ring2", &h->k.eval_cached_ring2},
             {"pwa_eval_cached_wide", &h->k.eval_cached_wide},
             {"pwa_eval_cached_tma", &h->k.eval_cached_tma},
+            {"pwa_gram_colmax", &h->k.gram_colmax},
+            {"pwa_gram_tc", &h->k.gram_tc},
+            {"pwa_wait_check", &h->k.wait_check},
             {"pwa_fields_from_p4", &h->k.fields_from_p4},
             {"pwa_toy_select", &h->k.toy_select},
             {"pwa_toy_fields", &h->k.toy_fields},
@@ -575,11 +580,65 @@ int pwa_toy_fields(pwa_plan* h, unsigned long long seed, const long long* idx, l
   return launch(h, h->k.toy_fields, dim3((int)nb), dim3(h->tpb), args, s);
 }
 
+namespace {
+// Tensor-core Gram of one chunk of `cnt` columns rows F (device) with
+// weights wptr: adds the chunk's complex K x K sums to acc (host).
+int gram_tc_chunk(pwa_plan* h, double* F, double* wptr, long long cnt, double* gpart,
+                  double* gsum, unsigned long long* mx, unsigned int* err, cudaStream_t s,
+                  std::vector<double>* acc) {
+  const int K = h->ncol, KC = 2 * K, CP = (KC + 15) / 16 * 16;
+  CU(cudaMemsetAsync(mx, 0, sizeof(unsigned long long) * 2 * KC, s));
+  long long nb = (cnt + h->tpb - 1) / h->tpb;
+  if (nb > 4LL * h->sms) nb = 4LL * h->sms;
+  void* a1[] = {&F, &wptr, &cnt, &mx};
+  int rc = launch(h, h->k.gram_colmax, dim3((int)nb), dim3(h->tpb), a1, s);
+  if (rc) return rc;
+  // two stages of seven A slices (128 x 64 bytes) and seven B slices
+  // (CP x 64 bytes), plus 1 KB for the 1024-byte alignment of the base
+  const size_t smem = 2 * (size_t)7 * (128 * 64 + CP * 64) + 1024;
+  CU(cudaFuncSetAttribute((const void*)h->k.gram_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)smem));
+  const int gb = h->sms;
+  void* a2[] = {&F, &wptr, &cnt, &mx, &gpart, &err};
+  cudaError_t e = cudaLaunchKernel((const void*)h->k.gram_tc, dim3(gb), dim3(h->tpb), a2, smem, s);
+  if (e != cudaSuccess)
+    return set_err(h, PWA_ERR_CUDA, std::string("gram kernel launch: ") + cudaGetErrorString(e));
+  int nrows = gb, ncols = KC * KC;
+  void* a3[] = {&gpart, &nrows, &ncols, &gsum};
+  rc = launch(h, h->k.sum_rows, dim3(16), dim3(256), a3, s);
+  if (rc) return rc;
+  std::vector<double> G((size_t)KC * KC);
+  unsigned int herr = 0;
+  CU(cudaMemcpyAsync(G.data(), gsum, sizeof(double) * G.size(), cudaMemcpyDeviceToHost, s));
+  CU(cudaMemcpyAsync(&herr, err, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  if (herr) return set_err(h, PWA_ERR_CUDA, "tensor-core Gram: a wait on the tensor cores timed out");
+  // G = X^T (w X) over the real columns (re 0..K-1, im K..2K-1):
+  // Re M_kl = G_RR + G_II, Im M_kl = G_RI - G_IR
+  for (int k = 0; k < K; ++k)
+    for (int l = 0; l < K; ++l) {
+      const double rr = G[(size_t)k * KC + l], ii = G[(size_t)(K + k) * KC + K + l];
+      const double ri = G[(size_t)k * KC + K + l], ir = G[(size_t)(K + k) * KC + l];
+      (*acc)[2 * ((size_t)k * K + l)] += rr + ii;
+      (*acc)[2 * ((size_t)k * K + l) + 1] += ri - ir;
+    }
+  return PWA_OK;
+}
+}  // namespace
+
+int pwa_set_gram_method(pwa_plan* h, int method) {
+  if (!h) return PWA_ERR_ARG;
+  if (method < -1 || method > 1) return set_err(h, PWA_ERR_ARG, "gram method must be -1, 0 or 1");
+  h->gram_method = method;
+  return PWA_OK;
+}
+
 int pwa_build_gram(pwa_plan* h, const double* consts, void* stream, double* out) {
   if (!h) return PWA_ERR_ARG;
   if (!h->w || h->n_mc <= 0) return set_err(h, PWA_ERR_STATE, "no MC events uploaded");
   if (!consts) return set_err(h, PWA_ERR_ARG, "invalid gram arguments");
   cudaStream_t s = (cudaStream_t)stream;
+  const bool tc = h->gram_method != 0 && 2 * h->ncol <= 64;
   std::vector<double> cbuf(consts, consts + h->nconst);
   const long long row = 2LL * h->ncol * h->nout;
   // chunked: columns of at most `chunk` events at a time
@@ -594,14 +653,19 @@ int pwa_build_gram(pwa_plan* h, const double* consts, void* stream, double* out)
   double* gpart = nullptr;
   double* gsum = nullptr;
   double* gtot = nullptr;
-  if (cudaMalloc(&gpart, sizeof(double) * nkk * gb) != cudaSuccess ||
-      cudaMalloc(&gsum, sizeof(double) * nkk) != cudaSuccess ||
-      cudaMalloc(&gtot, sizeof(double) * nkk) != cudaSuccess) {
+  // the tensor-core path writes one KC x KC real block per SM (KC = 2 ncol)
+  if (cudaMalloc(&gpart, sizeof(double) * 2 * nkk * gb) != cudaSuccess ||
+      cudaMalloc(&gsum, sizeof(double) * 2 * nkk) != cudaSuccess ||
+      cudaMalloc(&gtot, sizeof(double) * 4 * h->ncol + 64) != cudaSuccess) {
     cudaFree(F);
     if (gpart) cudaFree(gpart);
     if (gsum) cudaFree(gsum);
     return set_err(h, PWA_ERR_OOM, "cudaMalloc gram partials failed");
   }
+  // gtot: column maxima (2 KC 64-bit words) then the error flag
+  unsigned long long* mx = (unsigned long long*)gtot;
+  unsigned int* gerr = (unsigned int*)(gtot + 4 * h->ncol);
+  if (tc) cudaMemsetAsync(gerr, 0, sizeof(unsigned int), s);
   int rc = PWA_OK;
   std::vector<double> acc(nkk, 0.0), part(nkk);
   long long ld = h->ld;
@@ -614,6 +678,11 @@ int pwa_build_gram(pwa_plan* h, const double* consts, void* stream, double* out)
     rc = launch(h, h->k.columns_f64, dim3((int)nb), dim3(h->tpb), a1, s);
     if (rc) break;
     double* wptr = h->w + b0;
+    if (tc) {
+      rc = gram_tc_chunk(h, F, wptr, cnt, gpart, gsum, mx, gerr, s, &acc);
+      if (rc) break;
+      continue;
+    }
     void* a2[] = {&F, &wptr, &cnt, &gpart};
     rc = launch(h, h->k.gram_f64, dim3(gb), dim3(h->tpb), a2, s);
     if (rc) break;
@@ -783,9 +852,9 @@ int pwa_eval_cached_enqueue(pwa_plan* h, const double* ck, void* stream) {
 // Wait for the last cached launch: the kernel publishes its call number
 // last (after system fences) into mapped host memory, so polling it returns
 // as soon as the sums are visible, without a stream synchronisation.  After
-// one second without it (a failed launch or a very long kernel) fall back to
-// synchronising the stream, which also surfaces launch errors.
-void wait_cached(pwa_plan* h, cudaStream_t s) {
+// `limit_s` seconds without it (a failed launch or a very long kernel) fall
+// back to synchronising the stream, which also surfaces launch errors.
+void wait_cached(pwa_plan* h, cudaStream_t s, double limit_s = 1.0) {
   const int na = 1 + 2 * h->ncol;
   const volatile double* m = h->h_map;
   const auto t0 = std::chrono::steady_clock::now();
@@ -795,7 +864,7 @@ void wait_cached(pwa_plan* h, cudaStream_t s) {
       return;
     }
     if ((it & 4095u) == 0 &&
-        std::chrono::steady_clock::now() - t0 > std::chrono::seconds(1)) {
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > limit_s) {
       cudaStreamSynchronize(s);
       return;
     }
@@ -814,6 +883,27 @@ int cached_result(pwa_plan* h, const double** sums) {
   if (m[na] != 0.0) return set_err(h, PWA_ERR_CUDA, "cached evaluation: a barrier wait timed out");
   *sums = h->h_map;
   return PWA_OK;
+}
+
+int pwa_wait_check(pwa_plan* h, int mode, unsigned polls, double host_limit_s, void* stream) {
+  if (!h) return PWA_ERR_ARG;
+  if (!h->lib) return set_err(h, PWA_ERR_STATE, "plan not compiled");
+  if ((mode != 0 && mode != 1) || !(host_limit_s > 0.0) || polls < 1)
+    return set_err(h, PWA_ERR_ARG, "invalid wait-check arguments");
+  cudaStream_t s = (cudaStream_t)stream;
+  h->seq += 1.0;
+  if (mode == 0) {
+    // any 1 KB of device memory serves as the source of the one real copy
+    const double* src = (const double*)h->ticket;
+    int na = 1 + 2 * h->ncol;
+    double seq = h->seq;
+    void* args[] = {(void*)&src, &polls, &h->ticket, &h->d_map, &seq, &na};
+    const int rc = launch(h, h->k.wait_check, dim3(1), dim3(h->tpb), args, s);
+    if (rc) return rc;
+  }
+  wait_cached(h, s, host_limit_s);
+  const double* sd = nullptr;
+  return cached_result(h, &sd);
 }
 
 int pwa_set_cached_variant(pwa_plan* h, int variant) {
@@ -1307,9 +1397,10 @@ int pwa_read_dat(const char* path, double* out, long long cap, long long* n_valu
 // ---------------------------------------------------------------------------
 // Allocation-free evaluation.
 //
-// Callers that may not allocate device memory while they run -- code inside
-// a CUDA stream capture, or a host framework that owns every device byte
-// through its own arena and forbids cudaMalloc from plug-ins -- still need
+// Callers that may not allocate device memory while they run -- a host
+// framework that owns every device byte through its own arena and forbids
+// cudaMalloc from plug-ins, or a loop that must not take the allocator's
+// locks -- still need
 // the fused evaluation's block partials somewhere.  pwa_eval_noalloc keeps
 // them in this fixed, file-scope device array instead of the plan's
 // cudaMalloc'd scratch.  The array is part of this library's device image:
@@ -1328,7 +1419,9 @@ double* g_noalloc_ptr[kMaxDevices] = {nullptr};
 
 // Device address of the scratch array for `dev` (the current device).  The
 // name g_pwa_noalloc_scratch is only a host-side stand-in in host code; its
-// device address comes from cudaGetSymbolAddress, once per device.
+// device address comes from cudaGetSymbolAddress, once per device, and is
+// kept for the process (a cudaDeviceReset in between would leave it stale;
+// that is documented as unsupported).
 int noalloc_scratch(pwa_plan* h, int dev, double** out) {
   if (dev < 0 || dev >= kMaxDevices) return set_err(h, PWA_ERR_ARG, "device ordinal out of range");
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
@@ -1359,6 +1452,11 @@ extern "C" int pwa_eval_noalloc(pwa_plan* h, const double* consts, const double*
                    "supports at most " + std::to_string(PWA_NOALLOC_MAX_NACC));
   int dev = 0;
   CU(cudaGetDevice(&dev));
+  // the grid is sized from the plan's device (SM count, occupancy)
+  if (dev != h->device)
+    return set_err(h, PWA_ERR_STATE,
+                   "current device " + std::to_string(dev) + " is not the plan's device " +
+                       std::to_string(h->device));
   double* scratch = nullptr;
   int rc = noalloc_scratch(h, dev, &scratch);
   if (rc) return rc;

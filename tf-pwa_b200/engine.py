@@ -54,6 +54,8 @@ def load_library(path=LIB_PATH):
     lib.pwa_pieces_cached.argtypes = [vp, dp, ctypes.c_double, ctypes.c_double, vp, dp]
     lib.pwa_nll_grad_cached.argtypes = [vp, vp, ctypes.c_double, vp, vp, vp]
     lib.pwa_set_cached_variant.argtypes = [vp, i]
+    lib.pwa_set_gram_method.argtypes = [vp, i]
+    lib.pwa_wait_check.argtypes = [vp, i, ctypes.c_uint, ctypes.c_double, vp]
     llp = ctypes.POINTER(ll)
     lib.pwa_pool_reserve.argtypes = [vp, ll]
     lib.pwa_pool_alloc.argtypes = [vp, ll, llp, llp]
@@ -996,6 +998,12 @@ class Engine:
         if with_p4:
             return out, p4.reshape(self.code.kin.nfin, 4, n).permute(2, 0, 1)
         return out
+
+    def set_gram_method(self, method):
+        """0: FP64 Gram on the CUDA cores; 1: tensor cores (int8 slices,
+        exact integer accumulation); -1: automatic."""
+        self._check(load_library().pwa_set_gram_method(self.h, int(method)),
+                    "pwa_set_gram_method")
 
     def set_cached_variant(self, variant):
         self._check(load_library().pwa_set_cached_variant(self.h, int(variant)),
