@@ -175,6 +175,21 @@ int pwa_cache_data(pwa_plan* h, const double* consts, void* stream);
  * for 8 consumer warps, -1 = automatic (default: 2). */
 int pwa_set_cached_variant(pwa_plan* h, int variant);
 
+/* Autotuner of the cached data-term kernel (no counterpart in the
+ * reference, which has no kernels): times every configuration -- variant
+ * 2 at each block count per SM the occupancy allows, variants 1 and 4,
+ * variant 5 at every ring depth from 3 stages to the shared-memory limit,
+ * variants 0 and 3 -- with CUDA events over `reps` back-to-back launches
+ * on the plan's column cache and couplings ck, keeps the fastest.
+ * out[i] = mean microseconds per launch of configuration i (at most 32),
+ * *n_cand their count.  pwa_cached_config reads the configuration in use
+ * (variant, ring depth, blocks per SM of variant 2); pwa_set_cached_config
+ * sets one (0 = keep the default for that field). */
+int pwa_autotune_cached(pwa_plan* h, const double* ck, int reps, void* stream, int* n_cand,
+                        double* out);
+int pwa_cached_config(pwa_plan* h, int* out);
+int pwa_set_cached_config(pwa_plan* h, int variant, int stages, int bps);
+
 /* Data-term kernels on the cache with column couplings ck[2*ncol]
  * (re, im); sums (1 + 2*ncol doubles) stay on the device. */
 int pwa_eval_cached_enqueue(pwa_plan* h, const double* ck, void* stream);
@@ -260,6 +275,13 @@ int pwa_eval_noalloc(pwa_plan* h, const double* consts, const double* xm, const 
  * pwa_last_error.  The plan stays usable.  ticket memory (>= 1 KB) is the
  * copy's source. */
 int pwa_wait_check(pwa_plan* h, int mode, unsigned polls, double host_limit_s, void* stream);
+
+/* Peak FMA throughput of the CUDA cores (*out, flop/s), the roofline of the
+ * compute-bound amplitude kernels (no counterpart in the reference):
+ * precision PWA_PLAIN_F64 or PWA_MIXED_F32 (FP32 FMAs); 8 blocks of 256
+ * threads per SM, each thread eight independent chains of `iters` (a
+ * multiple of 4) FMAs, timed with CUDA events after one warm-up launch. */
+int pwa_fma_peak(pwa_plan* h, int precision, long long iters, void* stream, double* out);
 
 /* info[0..7]: registers/thread of eval_f64, eval_f32, local bytes f64, f32,
  * blocks, blocks_data, nacc, threads per block. */

@@ -191,12 +191,18 @@ class FCN:
         if self.use_gram and (shape_free or polarised):
             raise ValueError("the Gram cache needs fixed masses and widths, no polarisation "
                              "and no CP-violating totals")
+        self.tune = None
         if self.use_gram:
             vals = self.vm.get_all_dic()
             self.eng.set_gram(vals)
             self.eng.cache_data(vals)
             self._var_names = list(self.vm.variables.keys())
             self.eng.set_param_layout(self._var_names, self.vm.trainable_vars)
+            # pick the fastest configuration of the cached data-term kernel
+            # for this model and event count (PWA_AUTOTUNE=0: keep the default)
+            if os.environ.get("PWA_AUTOTUNE", "1") != "0":
+                self.eng.consts(vals)
+                self.tune = self.eng.autotune_cached()
 
     def _upload(self, data, bg, mcdata):
         import torch

@@ -487,6 +487,37 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, 1)
 #endif
 }
 
+// Peak FMA throughput of the CUDA cores, the roofline of the compute-bound
+// amplitude kernels: every thread runs eight independent chains of `iters`
+// fused multiply-adds (FP64 or FP32) and stores their sum, so nothing is
+// eliminated.  Work: 2 * 8 * iters flops per thread.
+template <typename R>
+__device__ __forceinline__ void fma_chains(long long iters, R* __restrict__ out) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  R a[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) a[j] = R(1) + R(t % 7) * R(0.001) + R(j) * R(0.01);
+  const R b = R(0.9999999), c = R(1e-7);
+#pragma unroll 1
+  for (long long i = 0; i < iters; i += 4) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) a[j] = fma(a[j], b, c);
+    }
+  }
+  R s = R(0);
+#pragma unroll
+  for (int j = 0; j < 8; ++j) s += a[j];
+  out[t] = s;
+}
+extern "C" __global__ void pwa_fma_peak_f64(long long iters, double* __restrict__ out) {
+  fma_chains<double>(iters, out);
+}
+extern "C" __global__ void pwa_fma_peak_f32(long long iters, float* __restrict__ out) {
+  fma_chains<float>(iters, out);
+}
+
 // FP64 -> FP32 copy of the angle columns for the mixed-precision kernels.
 extern "C" __global__ void pwa_to_f32(const double* __restrict__ in, float* __restrict__ out,
                                       long long n) {

@@ -38,7 +38,8 @@ struct Kernels {
                to_f32 = nullptr, cache_f32 = nullptr, eval_cached = nullptr,
                eval_cached_direct = nullptr, eval_cached_wred = nullptr, eval_cached_ring2 = nullptr,
                eval_cached_wide = nullptr, eval_cached_tma = nullptr, eval_multi = nullptr,
-               gram_colmax = nullptr, gram_tc = nullptr, wait_check = nullptr, reduce_multi = nullptr,
+               gram_colmax = nullptr, gram_tc = nullptr, wait_check = nullptr,
+               fma_f64 = nullptr, fma_f32 = nullptr, reduce_multi = nullptr,
                fields_from_p4 = nullptr, toy_select = nullptr, toy_fields = nullptr;
 };
 
@@ -71,6 +72,9 @@ struct pwa_plan {
   int cached_blocks_wide = 0, cached_blocks_tma = 0, tma_stages = 0, tma_threads = 0,
       wide_threads = 0;
   size_t cached_smem_tma = 0;
+  int tma_stages_max = 0, wred_per_sm = 0, wred_bps = 0;  // wred_bps 0: occupancy limit
+  size_t tma_stage_bytes = 0;
+  std::vector<int> tuned;  // (variant, stages, bps) chosen by pwa_autotune_cached
   // 0: shared-memory ring (bulk copies), 1: direct loads with per-thread FP64
   // column sums, 2: direct loads with warp reduce-scatter of the column sums;
   // 3: shared-memory ring (2 stages) with warp reduce-scatter column sums;
@@ -362,6 +366,8 @@ int pwa_plan_create(const char* src, size_t src_len, int n_mass, int n_angle, in
             {"pwa_gram_colmax", &h->k.gram_colmax},
             {"pwa_gram_tc", &h->k.gram_tc},
             {"pwa_wait_check", &h->k.wait_check},
+            {"pwa_fma_peak_f64", &h->k.fma_f64},
+            {"pwa_fma_peak_f32", &h->k.fma_f32},
             {"pwa_fields_from_p4", &h->k.fields_from_p4},
             {"pwa_toy_select", &h->k.toy_select},
             {"pwa_toy_fields", &h->k.toy_fields},
@@ -710,6 +716,8 @@ int pwa_build_gram(pwa_plan* h, const double* consts, void* stream, double* out)
 }
 
 
+static void apply_cached_config(pwa_plan* h, int variant, int stages, int bps);
+
 int pwa_cache_data(pwa_plan* h, const double* consts, void* stream) {
   if (!h) return PWA_ERR_ARG;
   if (!h->w || h->n_data <= 0) return set_err(h, PWA_ERR_STATE, "no data events uploaded");
@@ -761,7 +769,9 @@ int pwa_cache_data(pwa_plan* h, const double* consts, void* stream) {
   CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm3, (const void*)h->k.eval_cached_wred,
                                                    h->tpb, 0));
   if (per_sm3 < 1) per_sm3 = 1;
-  long long want3 = (long long)per_sm3 * h->sms;
+  h->wred_per_sm = per_sm3;
+  const int bps3 = h->wred_bps > 0 && h->wred_bps < per_sm3 ? h->wred_bps : per_sm3;
+  long long want3 = (long long)bps3 * h->sms;
   h->cached_blocks_wred = (int)(want3 < ntiles ? want3 : ntiles);
   // ring with register-light consumers: 2 stages (PWA_RSTAGES) per block
   h->cached_smem_ring2 = (size_t)2 * tile * (h->nf * sizeof(float2) + sizeof(double));
@@ -788,6 +798,8 @@ int pwa_cache_data(pwa_plan* h, const double* consts, void* stream) {
     long long st = ((long long)optin - (long long)a.sharedSizeBytes - 1024) / (long long)stage;
     if (st > 8) st = 8;  // PWA_TMA_MAXST
     h->tma_stages = (int)st;
+    h->tma_stages_max = (int)st;
+    h->tma_stage_bytes = stage;
     h->cached_smem_tma = (size_t)st * stage;
     h->cached_blocks_wide = (int)(h->sms < ntiles ? h->sms : ntiles);
     h->cached_blocks_tma = 0;
@@ -811,6 +823,7 @@ int pwa_cache_data(pwa_plan* h, const double* consts, void* stream) {
   if (rc) return rc;
   CU(cudaStreamSynchronize(s));
   h->fcache_n = n;
+  if (h->tuned.size() == 3) apply_cached_config(h, h->tuned[0], h->tuned[1], h->tuned[2]);
   return PWA_OK;
 }
 
@@ -904,6 +917,128 @@ int pwa_wait_check(pwa_plan* h, int mode, unsigned polls, double host_limit_s, v
   wait_cached(h, s, host_limit_s);
   const double* sd = nullptr;
   return cached_result(h, &sd);
+}
+
+int pwa_fma_peak(pwa_plan* h, int precision, long long iters, void* stream, double* out) {
+  if (!h || !out) return PWA_ERR_ARG;
+  if (!h->lib) return set_err(h, PWA_ERR_STATE, "plan not compiled");
+  if ((precision != PWA_PLAIN_F64 && precision != PWA_MIXED_F32) || iters < 4 || iters % 4)
+    return set_err(h, PWA_ERR_ARG, "invalid fma-peak arguments");
+  cudaStream_t s = (cudaStream_t)stream;
+  const int threads = 256, blocks = 8 * h->sms;
+  void* buf = nullptr;
+  if (cudaMalloc(&buf, sizeof(double) * threads * blocks) != cudaSuccess)
+    return set_err(h, PWA_ERR_OOM, "cudaMalloc of the fma-peak output failed");
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int rc = PWA_OK;
+  const cudaKernel_t k = precision == PWA_PLAIN_F64 ? h->k.fma_f64 : h->k.fma_f32;
+  void* args[] = {&iters, &buf};
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    rc = set_err(h, PWA_ERR_CUDA, "cudaEventCreate failed");
+  } else {
+    float ms = 0.f;
+    rc = launch(h, k, dim3(blocks), dim3(threads), args, s);  // warm-up
+    if (!rc) cudaEventRecord(e0, s);
+    if (!rc) rc = launch(h, k, dim3(blocks), dim3(threads), args, s);
+    if (!rc) cudaEventRecord(e1, s);
+    if (!rc && (cudaEventSynchronize(e1) != cudaSuccess ||
+                cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess || ms <= 0.f))
+      rc = set_err(h, PWA_ERR_CUDA, "fma-peak timing failed");
+    if (!rc) *out = 2.0 * 8.0 * (double)iters * threads * blocks / (1e-3 * ms);
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFree(buf);
+  return rc;
+}
+
+// Geometry of one cached-kernel configuration (variant, TMA ring depth,
+// blocks per SM of variant 2) applied to the plan.
+static void apply_cached_config(pwa_plan* h, int variant, int stages, int bps) {
+  h->cached_variant = variant;
+  if (variant == 5 && stages >= 2 && stages <= h->tma_stages_max) {
+    h->tma_stages = stages;
+    h->cached_smem_tma = (size_t)stages * h->tma_stage_bytes;
+  }
+  if (variant == 2) {
+    h->wred_bps = bps;
+    const int b = bps > 0 && bps < h->wred_per_sm ? bps : h->wred_per_sm;
+    const long long want = (long long)b * h->sms;
+    h->cached_blocks_wred = (int)(want < h->ntiles ? want : h->ntiles);
+  }
+}
+
+int pwa_autotune_cached(pwa_plan* h, const double* ck, int reps, void* stream, int* n_cand,
+                        double* out) {
+  if (!h) return PWA_ERR_ARG;
+  if (h->fcache_n <= 0) return set_err(h, PWA_ERR_STATE, "no column cache (call pwa_cache_data)");
+  if (!ck || !n_cand || !out || reps < 1) return set_err(h, PWA_ERR_ARG, "invalid autotune arguments");
+  cudaStream_t s = (cudaStream_t)stream;
+  struct Cand {
+    int variant, stages, bps;
+  };
+  std::vector<Cand> cands;
+  for (int b = h->wred_per_sm; b >= 2; --b) cands.push_back({2, 0, b});
+  cands.push_back({1, 0, 0});
+  cands.push_back({4, 0, 0});
+  if (h->cached_blocks_tma > 0)
+    for (int st = 3; st <= h->tma_stages_max; ++st) cands.push_back({5, st, 0});
+  cands.push_back({0, 0, 0});
+  cands.push_back({3, 0, 0});
+  if ((int)cands.size() > 32) cands.resize(32);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    if (e0) cudaEventDestroy(e0);
+    return set_err(h, PWA_ERR_CUDA, "cudaEventCreate failed");
+  }
+  int best = -1, rc = PWA_OK;
+  double best_us = 0.0;
+  for (size_t c = 0; c < cands.size() && rc == PWA_OK; ++c) {
+    apply_cached_config(h, cands[c].variant, cands[c].stages, cands[c].bps);
+    for (int w = 0; w < 2 && rc == PWA_OK; ++w) rc = pwa_eval_cached_enqueue(h, ck, stream);
+    if (rc) break;
+    cudaEventRecord(e0, s);
+    for (int r = 0; r < reps && rc == PWA_OK; ++r) rc = pwa_eval_cached_enqueue(h, ck, stream);
+    cudaEventRecord(e1, s);
+    if (rc) break;
+    float ms = 0.f;
+    if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+      rc = set_err(h, PWA_ERR_CUDA, "autotune timing failed");
+      break;
+    }
+    wait_cached(h, s);
+    const double* sd = nullptr;
+    rc = cached_result(h, &sd);
+    if (rc) break;
+    const double us = 1e3 * ms / reps;
+    out[c] = us;
+    if (best < 0 || us < best_us) best = (int)c, best_us = us;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *n_cand = (int)cands.size();
+  if (best >= 0) apply_cached_config(h, cands[best].variant, cands[best].stages, cands[best].bps);
+  if (rc) return rc;
+  h->tuned = {cands[best].variant, cands[best].stages, cands[best].bps};
+  return PWA_OK;
+}
+
+int pwa_cached_config(pwa_plan* h, int* out) {
+  if (!h || !out) return PWA_ERR_ARG;
+  out[0] = h->cached_variant >= 0 ? h->cached_variant : 2;
+  out[1] = h->tma_stages;
+  out[2] = h->wred_bps > 0 ? h->wred_bps : h->wred_per_sm;
+  return PWA_OK;
+}
+
+int pwa_set_cached_config(pwa_plan* h, int variant, int stages, int bps) {
+  if (!h) return PWA_ERR_ARG;
+  if (variant < -1 || variant > 5 || stages < 0 || bps < 0)
+    return set_err(h, PWA_ERR_ARG, "invalid cached-kernel configuration");
+  if (variant == 5 && stages && (stages < 2 || stages > h->tma_stages_max))
+    return set_err(h, PWA_ERR_ARG, "ring depth outside 2 .. the shared-memory limit");
+  apply_cached_config(h, variant, stages, bps);
+  return PWA_OK;
 }
 
 int pwa_set_cached_variant(pwa_plan* h, int variant) {

@@ -56,6 +56,10 @@ def load_library(path=LIB_PATH):
     lib.pwa_set_cached_variant.argtypes = [vp, i]
     lib.pwa_set_gram_method.argtypes = [vp, i]
     lib.pwa_wait_check.argtypes = [vp, i, ctypes.c_uint, ctypes.c_double, vp]
+    lib.pwa_fma_peak.argtypes = [vp, i, ll, vp, dp]
+    lib.pwa_autotune_cached.argtypes = [vp, dp, i, vp, ip, dp]
+    lib.pwa_cached_config.argtypes = [vp, ip]
+    lib.pwa_set_cached_config.argtypes = [vp, i, i, i]
     llp = ctypes.POINTER(ll)
     lib.pwa_pool_reserve.argtypes = [vp, ll]
     lib.pwa_pool_alloc.argtypes = [vp, ll, llp, llp]
@@ -999,6 +1003,53 @@ class Engine:
             return out, p4.reshape(self.code.kin.nfin, 4, n).permute(2, 0, 1)
         return out
 
+    def fma_peak(self, precision=PLAIN_F64, iters=1 << 16):
+        """Measured peak FMA throughput (flop/s) of the CUDA cores in FP64
+        (PLAIN_F64) or FP32 (MIXED_F32)."""
+        out = ctypes.c_double()
+        self._check(load_library().pwa_fma_peak(self.h, precision, int(iters), 0,
+                                                ctypes.byref(out)), "pwa_fma_peak")
+        return out.value
+
+    def autotune_cached(self, reps=8):
+        """Time every configuration of the cached data-term kernel on this
+        plan's column cache and keep the fastest (pwa_autotune_cached).
+        Returns the per-configuration microseconds and the choice
+        (variant, ring depth, blocks per SM).  The choice is remembered per
+        model source and tile count for the process, and across processes
+        in PWA_CUBIN_CACHE when that directory is set."""
+        key = self._tune_key()
+        hit = _TUNED.get(key) or _tune_disk_read(key)
+        if hit is not None:
+            self.set_cached_config(*hit)
+            _TUNED[key] = hit
+            return None, tuple(hit)
+        ck = np.ascontiguousarray(np.stack([self._ck.real, self._ck.imag], 1).reshape(-1))
+        n = ctypes.c_int()
+        out = np.zeros(32)
+        self._check(load_library().pwa_autotune_cached(self.h, _dptr(ck), int(reps), 0,
+                                                       ctypes.byref(n), _dptr(out)),
+                    "pwa_autotune_cached")
+        cfg = self.cached_config()
+        _TUNED[key] = cfg
+        _tune_disk_write(key, cfg)
+        return out[:n.value].copy(), cfg
+
+    def _tune_key(self):
+        import hashlib
+
+        ntiles = (self._n_data + self.tpb - 1) // self.tpb
+        return hashlib.sha1(self.src.encode()).hexdigest()[:20] + f"_{ntiles}"
+
+    def cached_config(self):
+        out = (ctypes.c_int * 3)()
+        self._check(load_library().pwa_cached_config(self.h, out), "pwa_cached_config")
+        return tuple(out)
+
+    def set_cached_config(self, variant, stages=0, bps=0):
+        self._check(load_library().pwa_set_cached_config(self.h, int(variant), int(stages),
+                                                         int(bps)), "pwa_set_cached_config")
+
     def set_gram_method(self, method):
         """0: FP64 Gram on the CUDA cores; 1: tensor cores (int8 slices,
         exact integer accumulation); -1: automatic."""
@@ -1053,6 +1104,37 @@ class Engine:
         C = self.consts(vals)
         self._gram = self.build_gram(C)
         return self._gram
+
+
+# cached-kernel configurations chosen by Engine.autotune_cached, per model
+# source and tile count
+_TUNED = {}
+
+
+def _tune_path(key):
+    d = os.environ.get("PWA_CUBIN_CACHE")
+    return os.path.join(d, f"pwa_tune_{key}.txt") if d else None
+
+
+def _tune_disk_read(key):
+    p = _tune_path(key)
+    try:
+        with open(p) as f:
+            v = tuple(int(x) for x in f.read().split())
+        return v if len(v) == 3 else None
+    except (OSError, TypeError, ValueError):
+        return None
+
+
+def _tune_disk_write(key, cfg):
+    p = _tune_path(key)
+    if p:
+        try:
+            with open(p + ".tmp", "w") as f:
+                f.write(" ".join(str(int(x)) for x in cfg))
+            os.replace(p + ".tmp", p)
+        except OSError:
+            pass
 
 
 def read_dat(path):
