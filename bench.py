@@ -306,8 +306,223 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+# ----------------------------------------------------------- GPU timing
+class Timer:
+    """k timed steps, L2 flushed (a 256 MB buffer written, L2 is 126 MB)
+    before each; device time from CUDA events on the launching (current)
+    stream, max over ranks."""
+
+    def __init__(self, dist):
+        import torch
+
+        self.torch, self.dist = torch, dist
+        self.flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def barrier(self):
+        self.torch.cuda.synchronize()
+        if self.dist is not None:
+            self.dist.barrier()
+
+    def __call__(self, step_fn, k):
+        torch = self.torch
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(k)]
+        self.barrier()
+        for i in range(k):
+            self.flush.zero_()
+            ev[i][0].record()
+            step_fn()
+            ev[i][1].record()
+        self.barrier()
+        t = sum(a.elapsed_time(b) for a, b in ev) / 1e3
+        if self.dist is not None:
+            tt = torch.tensor([t], device="cuda", dtype=torch.float64)
+            self.dist.all_reduce(tt, op=self.dist.ReduceOp.MAX)
+            t = float(tt.item())
+        return t
+
+
+def _reduce_fn(dist):
+    if dist is None:
+        return None
+    import torch
+
+    def reduce_fn(vec):
+        t = torch.as_tensor(vec, device="cuda")
+        dist.all_reduce(t)
+        return t.cpu().numpy()
+
+    return reduce_fn
+
+
+# Forward flops per event of sum |A|^2 (fma = 2 flops; divisions, square
+# roots and transcendental calls counted apart), counted from the oracle's
+# expression graph by oracle/flop_count.py (pinned by
+# tests/test_flop_count.py): the compute work unit of the amplitude kernels.
+FWD_FLOPS = {"d2kpipi_float": (318, 77), "lc2pkpi": (1614, 228), "b2dstkpi": (6760, 1081)}
+# FP64 operations per event of one launch of the plain kernel (forward and
+# adjoint, data and MC alike), 2 * DFMA + DADD + DMUL executed, from an ncu
+# capture of pwa_eval_f64 (None: not captured; the forward count is used)
+NCU_F64_FLOPS_PER_EVENT = {}
+
+CACHED_KERNEL = {0: "pwa_eval_cached (bulk-copy ring, per-thread FP64 column sums)",
+                 1: "pwa_eval_cached_direct (direct loads, per-thread FP64 column sums)",
+                 2: "pwa_eval_cached_wred (direct loads, warp reduce-scatter column sums)",
+                 3: "pwa_eval_cached_ring2 (two-stage ring, reduce-scatter consumers)",
+                 4: "pwa_eval_cached_wide (one block of 16 warps per SM, contiguous runs)",
+                 5: "pwa_eval_cached_tma (one block per SM, producer warp, deep bulk-copy ring)"}
+
+
+def measure_cached(name, args, rank, world, dist, timed, log, n_sig, n_bg, n_mc,
+                   variants=True):
+    """Fixed masses and widths: the mixed form (FP32 column cache, FP64
+    amplitudes / log / sums, FP64 Gram MC term) against the plain FP64
+    kernels and the FP32-recompute form, on one workload.  Returns the JSON
+    line (without the CPU baseline) and the engines' peak info."""
+    import torch
+
+    from tf_pwa_b200.api import FCN
+    from tf_pwa_b200.engine import MIXED_F32, PLAIN_F64
+    from tf_pwa_b200.workload import make_dataset
+
+    config, _, _, _, metric, workload = WORKLOADS[name]
+    t0 = time.perf_counter()
+    cl, data, bg, mc = make_dataset(config, n_sig, n_mc, n_bg=n_bg, bg_weight=BG_WEIGHT,
+                                    seed=1 + rank, device="cuda")
+    t_data = time.perf_counter() - t0
+    log(f"{name}: dataset {n_sig} signal + {n_bg} background + {n_mc} MC events")
+    t0 = time.perf_counter()
+    fcn = FCN(cl, data, mc, bg=bg, precision="mixed")  # column cache + Gram, autotuned
+    t_mixed_setup = time.perf_counter() - t0
+    log(f"{name}: mixed-form FCN ready (tuned {fcn.eng.cached_config()})")
+    fcn_plain = FCN(cl, data, mc, bg=bg, precision="plain")
+    for f in (fcn, fcn_plain):
+        f.eng.dist_reduce = _reduce_fn(dist)
+        f.eng.mc_share = 1.0 / world  # equal MC shards
+    x0 = np.array(cl.vm.get_all_val())
+    names = list(cl.vm.trainable_vars)
+    vals = cl.vm.get_all_dic()
+    eng, eng_p = fcn.eng, fcn_plain.eng
+    var_vec = np.array([vals[k] for k in fcn._var_names])
+    for _ in range(args.warmup):
+        fcn.nll_grad(x0)
+        fcn_plain.nll_grad(x0)
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    clocks = Clocks(_clocks_path(rank))
+    clocks.start()
+    # headline: one NLL+gradient evaluation per step through the C ABI
+    # (couplings -> cached-column kernel + Gram MC term -> chain rule)
+    t_mixed = timed(lambda: eng.nll_grad_cached(var_vec), args.steps)
+    t_plain = timed(lambda: eng_p.nll_grad(vals, names, PLAIN_F64), args.steps)
+    # e2e through the public API with host parameters
+    t_e2e = timed(lambda: fcn.nll_grad(x0), args.steps)
+    # roofline: the data-term kernel (with its own ordered reduction) alone
+    eng.consts(vals)
+    ck = np.stack([eng._ck.real, eng._ck.imag], 1).reshape(-1)
+    k_kernel = args.steps
+    t_kernel = timed(lambda: eng.eval_cached_enqueue(ck), k_kernel)
+    Cp = eng_p.consts(vals)
+    t_kernel_p = timed(lambda: eng_p.eval_enqueue(Cp, PLAIN_F64, mc=True), k_kernel)
+    # the FP32-amplitude recompute form (what a fit with floating masses and
+    # widths, where no column cache applies, uses instead of plain FP64)
+    t_f32 = timed(lambda: eng_p.nll_grad(vals, names, MIXED_F32), args.steps)
+    t_kernel_f32 = timed(lambda: eng_p.eval_enqueue(Cp, MIXED_F32, mc=True), k_kernel)
+    ck_clocks = clocks.stop(local)
+    tuned = eng.cached_config()
+    var_table = {}
+    if variants:
+        for var in (0, 1, 2, 3, 4, 5):
+            eng.set_cached_config(var)
+            var_table[var] = {
+                "kernel_us": 1e6 * timed(lambda: eng.eval_cached_enqueue(ck), k_kernel) / k_kernel,
+                "step_us": 1e6 * timed(lambda: eng.nll_grad_cached(var_vec), args.steps)
+                / args.steps,
+                "nll": eng.nll_grad_cached(var_vec)[0]}
+        eng.set_cached_config(*tuned)
+    nll_m, g_m = eng.nll_grad_cached(var_vec)
+    nll_p, g_p = eng_p.nll_grad(vals, names, PLAIN_F64)
+    nll_f, g_f = eng_p.nll_grad(vals, names, MIXED_F32)
+    peaks = {"f64_tflops": eng.fma_peak(PLAIN_F64) / 1e12,
+             "f32_tflops": eng.fma_peak(MIXED_F32) / 1e12}
+
+    n_data = n_sig + n_bg
+    code = eng.code
+    n_mass, n_ang = len(code.mass_fields), len(code.angle_fields)
+    bytes_mixed = n_data * (8 * code.nf + 8)
+    hbm, peak_kind = _peaks()
+    ach = bytes_mixed / (t_kernel / k_kernel) / 1e9
+    n_ev = n_data + n_mc
+    fl_ev = NCU_F64_FLOPS_PER_EVENT.get(name)
+    fl_kind = "ncu: 2 DFMA + DADD + DMUL executed per event (forward and adjoint)"
+    if fl_ev is None:
+        fl_ev, fl_kind = FWD_FLOPS[name][0], "forward sum |A|^2 only (oracle count): a lower bound"
+    ach_p = fl_ev * n_ev / (t_kernel_p / k_kernel) / 1e12
+    value = world * args.steps / t_mixed
+    line = {
+        "metric": metric, "value": value, "unit": "evals/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_mixed / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": workload, "precision": "mixed: per-event partial-wave columns "
+                   "cached as FP32 (computed in FP64), FP64 amplitude sum, log and reductions; "
+                   "MC integral from the FP64-accurate Gram matrix (masses/widths fixed)",
+                   "events_per_rank": {"data": n_data, "mc": n_mc},
+                   "l2": "256 MB buffer written before every timed step (L2 126 MB); inputs "
+                         "larger than L2 as well",
+                   "parallelism": f"dp{world}" if world > 1 else "single GPU"},
+        "plain_f64": {"value": world * args.steps / t_plain, "unit": "evals/s",
+                      "ms_per_step": 1e3 * t_plain / args.steps,
+                      "speedup_mixed_over_plain": t_plain / t_mixed},
+        "fp32_recompute": {"value": world * args.steps / t_f32, "unit": "evals/s",
+                           "ms_per_step": 1e3 * t_f32 / args.steps,
+                           "kernel_us": 1e6 * t_kernel_f32 / k_kernel,
+                           "dnll": nll_f - nll_p,
+                           "grad_max_rel": float(np.max(np.abs(g_f - g_p)) / np.max(np.abs(g_p)))},
+        "e2e": {"value": world * args.steps / t_e2e, "unit": "evals/s",
+                "h2d_bytes_per_step": 8 * len(x0),
+                "d2h_bytes_per_step": 8 * (1 + len(x0)),
+                "call": "FCN.nll_grad(x) with x a host numpy vector"},
+        "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
+                     "frac": ach / hbm,
+                     "traffic": (NCU_TRAFFIC_PER_ROW[name] * n_data
+                                 if name in NCU_TRAFFIC_PER_ROW else None),
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
+                                       "launch at the bench size, scaled by the rows",
+                     "peak_kind": peak_kind,
+                     "kernel": CACHED_KERNEL[tuned[0]] + "; ends with its own fixed-order "
+                               "reduction",
+                     "algorithmic_bytes_per_launch": bytes_mixed,
+                     "launch_us": 1e6 * t_kernel / k_kernel,
+                     "plain_f64_kernel": {
+                         "bound": "fp64", "achieved": ach_p, "peak": peaks["f64_tflops"],
+                         "unit": "TFLOP/s", "frac": ach_p / peaks["f64_tflops"],
+                         "peak_kind": "measured here (pwa_fma_peak, FP64 FMA chains)",
+                         "flops_per_event": fl_ev, "flops_source": fl_kind,
+                         "launch_us": 1e6 * t_kernel_p / k_kernel,
+                         "events_per_launch": n_ev}},
+        "fma_peaks": peaks,
+        "gpu_launches": args.steps,
+        "autotune": {"choice": {"variant": tuned[0], "ring_stages": tuned[1],
+                                "blocks_per_sm": tuned[2]},
+                     "table_us": None if fcn.tune is None or fcn.tune[0] is None
+                     else [round(float(x), 2) for x in fcn.tune[0]]},
+        "cached_variants": var_table,
+        "check": {"nll_mixed": nll_m, "nll_plain": nll_p, "dnll": nll_m - nll_p,
+                  "grad_max_rel": float(np.max(np.abs(g_m - g_p)) / np.max(np.abs(g_p)))},
+        "setup_s": {"dataset": t_data, "mixed_fcn": t_mixed_setup},
+        "engine": eng.info(),
+    }
+    if ck_clocks:
+        line["clocks"] = ck_clocks
+    fcn.eng.close()
+    fcn_plain.eng.close()
+    del fcn, fcn_plain, data, bg, mc
+    torch.cuda.empty_cache()
+    return line
+
+
 # ------------------------------------------------- floating masses/widths
-def run_floating(args, rank, world, timed_factory):
+def measure_floating(name, args, rank, world, dist, timed, log, n_sig, n_mc):
     """Workload with floating lineshape parameters: no column cache applies,
     so the chosen form is the FP32-amplitude recompute kernel (FP64 masses,
     lineshape constants and sums) against the plain FP64 kernels; the
@@ -318,26 +533,19 @@ def run_floating(args, rank, world, timed_factory):
     from tf_pwa_b200.engine import MIXED_F32, PLAIN_F64
     from tf_pwa_b200.workload import make_dataset
 
+    config, _, _, _, metric, workload = WORKLOADS[name]
     t0 = time.perf_counter()
-    cl, data, bg, mc = make_dataset(CONFIG, args.n_sig, args.n_mc, seed=1 + rank)
+    cl, data, bg, mc = make_dataset(config, n_sig, n_mc, seed=1 + rank)
     t_data = time.perf_counter() - t0
+    log(f"{name}: dataset {n_sig} data + {n_mc} MC events")
     fcn = FCN(cl, data, mc, precision="mixed")
     assert not fcn.use_gram
     fcn_p = FCN(cl, data, mc, precision="plain")
-    if world > 1:
-        import torch.distributed as dist
-
-        def reduce_fn(vec):
-            t = torch.as_tensor(vec, device="cuda")
-            dist.all_reduce(t)
-            return t.cpu().numpy()
-
-        for f in (fcn, fcn_p):
-            f.eng.dist_reduce = reduce_fn
-            f.eng.mc_share = 1.0 / world  # equal MC shards
+    for f in (fcn, fcn_p):
+        f.eng.dist_reduce = _reduce_fn(dist)
+        f.eng.mc_share = 1.0 / world  # equal MC shards
     x0 = np.array(cl.vm.get_all_val())
     vals, names = cl.vm.get_all_dic(), list(cl.vm.trainable_vars)
-    timed = timed_factory()
     for _ in range(args.warmup):
         fcn.nll_grad(x0)
         fcn_p.nll_grad(x0)
@@ -356,20 +564,20 @@ def run_floating(args, rank, world, timed_factory):
     nll_f, g_f = fcn.nll_grad(x0)
     nll_p, g_p = fcn_p.nll_grad(x0)
     code = fcn.eng.code
-    n_all = args.n_sig + args.n_mc
+    n_all = n_sig + n_mc
     bytes_f32 = n_all * (8 * len(code.mass_fields) + 4 * len(code.angle_fields) + 8)
     bytes_f64 = n_all * (8 * len(code.mass_fields) + 8 * len(code.angle_fields) + 8)
     hbm, peak_kind = _peaks()
     ach = bytes_f32 / (t_k / args.steps) / 1e9
     line = {
-        "metric": METRIC, "value": world * args.steps / t_f32, "unit": "evals/s",
+        "metric": metric, "value": world * args.steps / t_f32, "unit": "evals/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * t_f32 / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "precision": "FP32 amplitudes recomputed from the "
+        "config": {"workload": workload, "precision": "FP32 amplitudes recomputed from the "
                    "angles every evaluation (FP64 masses, lineshape constants, log and sums); "
                    "no column cache since masses and widths float",
-                   "events_per_rank": {"data": args.n_sig, "mc": args.n_mc},
+                   "events_per_rank": {"data": n_sig, "mc": n_mc},
                    "l2": "256 MB buffer written before every timed step (L2 126 MB)",
                    "parallelism": f"dp{world}" if world > 1 else "single GPU"},
         "plain_f64": {"value": world * args.steps / t_p, "unit": "evals/s",
@@ -394,18 +602,27 @@ def run_floating(args, rank, world, timed_factory):
     }
     if ck_clocks:
         line["clocks"] = ck_clocks
-    if rank == 0:
-        print(json.dumps(line), flush=True)
     fcn.eng.close()
     fcn_p.eng.close()
-    if world > 1:
-        import torch.distributed as dist
+    del fcn, fcn_p, data, mc
+    torch.cuda.empty_cache()
+    return line
 
-        dist.barrier()
-        dist.destroy_process_group()
+
+def _compact(line):
+    """A workload's line trimmed for the `workloads` key of the headline line."""
+    keep = ("metric", "value", "unit", "ms_per_step", "config", "plain_f64", "fp32_recompute",
+            "e2e", "roofline", "autotune", "hessian", "check", "clocks", "setup_s")
+    return {k: line[k] for k in keep if k in line}
 
 
 # ------------------------------------------------------------- serving arm
+SERVING_METRIC = "toy-fit service: per-fit latency p50/p99 and aggregate NLL+grad evals/s"
+SERVING_WORKLOAD = ("d2kpipi model (2 chains), fits with log-uniform 1e3..1e6 data events, "
+                    "shared 1e6 MC, Poisson arrivals, BFGS per fit, admission under a 150 GB "
+                    "HBM budget, mixed form (column cache + Gram)")
+
+
 def run_serving(args):
     """Toy-fit service: 512 fits of the d2kpipi model, event counts
     log-uniform in [1e3, 1e6], shared 1e6-event MC, Poisson arrivals, each
@@ -424,15 +641,24 @@ def run_serving(args):
     r = serving_benchmark(n_fits=args.n_fits, rate=rate, native=True)
     r_py = serving_benchmark(n_fits=args.n_fits, rate=rate, native=False)
     r_slow = serving_benchmark(n_fits=args.n_fits, rate=args.n_fits / 1.0, native=True)
-    line = {"metric": "toy-fit service: per-fit latency p50/p99 and aggregate NLL+grad evals/s",
+    line = {"metric": SERVING_METRIC,
             "value": r["evals_per_s"], "unit": "evals/s", "n_gpus": 1,
             "higher_is_better": True, "data": "synthetic", "dtype": "f64",
-            "config": {"workload": "d2kpipi model (2 chains), fits with log-uniform 1e3..1e6 "
-                       "data events, shared 1e6 MC, Poisson arrivals, BFGS per fit, "
-                       "admission under a 150 GB HBM budget, mixed form (column cache + Gram)"},
+            "config": {"workload": SERVING_WORKLOAD},
             "serving": r, "serving_python_drivers": r_py,
             "serving_arrivals_over_1s": r_slow}
     print(json.dumps(line), flush=True)
+
+
+def serving_summary(n_fits):
+    """The native service, saturated (all fits at once) and under Poisson
+    arrivals over about one second."""
+    from tf_pwa_b200.serving import serving_benchmark
+
+    r = serving_benchmark(n_fits=n_fits, rate=1e9, native=True)
+    r_slow = serving_benchmark(n_fits=n_fits, rate=n_fits / 1.0, native=True)
+    return {"metric": SERVING_METRIC, "unit": "evals/s", "workload": SERVING_WORKLOAD,
+            "saturated": r, "arrivals_over_1s": r_slow}
 
 
 # ----------------------------------------------------------------- our arm
@@ -445,6 +671,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=3,
                     help="evaluations of the CPU oracle baseline (whole workload each)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--headline-only", action="store_true",
+                    help="skip the four-body, floating-shape and serving keys")
     ap.add_argument("--serving", action="store_true",
                     help="run the toy-fit serving workload instead (separate JSON line)")
     ap.add_argument("--n-fits", type=int, default=512)
@@ -480,168 +708,41 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
     _pkg()
-    from tf_pwa_b200.engine import MIXED_F32, PLAIN_F64
-    from tf_pwa_b200.api import FCN
-    from tf_pwa_b200.workload import make_dataset
-
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
-
-    def barrier():
-        torch.cuda.synchronize()
-        if dist is not None:
-            dist.barrier()
-
-    def timed(step_fn, k):
-        """k steps, L2 flushed before each; device time from CUDA events."""
-        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-              for _ in range(k)]
-        barrier()
-        for i in range(k):
-            flush.zero_()
-            ev[i][0].record()
-            step_fn()
-            ev[i][1].record()
-        barrier()
-        t = sum(a.elapsed_time(b) for a, b in ev) / 1e3
-        if dist is not None:
-            tt = torch.tensor([t], device="cuda", dtype=torch.float64)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            t = float(tt.item())
-        return t
-
+    timed = Timer(dist)
     t_setup = time.perf_counter()
 
     def log(msg):
         print(f"[bench {time.perf_counter() - t_setup:8.1f}s] {msg}", file=sys.stderr, flush=True)
 
     if args.workload == "d2kpipi_float":
-        return run_floating(args, rank, world, lambda: timed)
-    n_sig, n_bg, n_mc = args.n_sig, args.n_bg, args.n_mc
-    cl, data, bg, mc = make_dataset(CONFIG, n_sig, n_mc, n_bg=n_bg, bg_weight=BG_WEIGHT,
-                                    seed=1 + rank, device="cuda")
-    t_data = time.perf_counter() - t_setup
-    log(f"dataset: {n_sig} signal + {n_bg} background + {n_mc} MC events")
-    reduce_fn = None
-    if dist is not None:
-        def reduce_fn(vec):
-            t = torch.as_tensor(vec, device="cuda")
-            dist.all_reduce(t)
-            return t.cpu().numpy()
-    fcn = FCN(cl, data, mc, bg=bg, precision="mixed")         # Gram MC term
-    log("mixed-form FCN ready (column cache + Gram)")
-    fcn_plain = FCN(cl, data, mc, bg=bg, precision="plain")
-    log("plain FCN ready")
-    for f in (fcn, fcn_plain):
-        f.eng.dist_reduce = reduce_fn
-        f.eng.mc_share = 1.0 / world  # equal MC shards
-    x0 = np.array(cl.vm.get_all_val())
-    names = list(cl.vm.trainable_vars)
-
-    vals = cl.vm.get_all_dic()
-    eng, eng_p = fcn.eng, fcn_plain.eng
-    var_vec = np.array([vals[k] for k in fcn._var_names])
-    # warm-up
-    for _ in range(args.warmup):
-        fcn.nll_grad(x0)
-        fcn_plain.nll_grad(x0)
-
-    clocks = Clocks(_clocks_path(rank))
-    clocks.start()
-    # headline: one NLL+gradient evaluation per step through the C ABI
-    # (couplings -> cached-column kernel + Gram MC term -> chain rule)
-    t_mixed = timed(lambda: eng.nll_grad_cached(var_vec), args.steps)
-    t_plain = timed(lambda: eng_p.nll_grad(vals, names, PLAIN_F64), args.steps)
-    # e2e through the public API with host parameters
-    t_e2e = timed(lambda: fcn.nll_grad(x0), args.steps)
-    # roofline: the data-term kernel + fixed-order reduction alone
-    eng.consts(vals)
-    ck = np.stack([eng._ck.real, eng._ck.imag], 1).reshape(-1)
-    k_kernel = args.steps
-    t_kernel = timed(lambda: eng.eval_cached_enqueue(ck), k_kernel)
-    variants = {}
-    for var in (0, 1, 2, 3):
-        eng.set_cached_variant(var)
-        variants[var] = {"kernel_us": 1e6 * timed(lambda: eng.eval_cached_enqueue(ck), k_kernel)
-                         / k_kernel,
-                         "step_us": 1e6 * timed(lambda: eng.nll_grad_cached(var_vec), args.steps)
-                         / args.steps,
-                         "nll": eng.nll_grad_cached(var_vec)[0]}
-    eng.set_cached_variant(-1)
-    Cp = eng_p.consts(vals)
-    t_kernel_p = timed(lambda: eng_p.eval_enqueue(Cp, PLAIN_F64, mc=True), k_kernel)
-    # the FP32-amplitude recompute form (what a fit with floating masses and
-    # widths, where no column cache applies, can use instead of plain FP64)
-    t_f32 = timed(lambda: eng_p.nll_grad(vals, names, MIXED_F32), args.steps)
-    t_kernel_f32 = timed(lambda: eng_p.eval_enqueue(Cp, MIXED_F32, mc=True), k_kernel)
-    ck_clocks = clocks.stop(local)
-    nll_m, g_m = eng.nll_grad_cached(var_vec)
-    nll_p, g_p = eng_p.nll_grad(vals, names, PLAIN_F64)
-    nll_f, g_f = eng_p.nll_grad(vals, names, MIXED_F32)
-
-    n_data = n_sig + n_bg
-    code = eng.code
-    n_mass, n_ang = len(code.mass_fields), len(code.angle_fields)
-    bytes_mixed = n_data * (8 * code.nf + 8)
-    bytes_plain = (n_data + n_mc) * (8 * n_mass + 8 * n_ang + 8)
-    hbm, peak_kind = _peaks()
-    ach = bytes_mixed / (t_kernel / k_kernel) / 1e9
-    ach_p = bytes_plain / (t_kernel_p / k_kernel) / 1e9
-    value = world * args.steps / t_mixed
-    line = {
-        "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_mixed / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic",
-        "config": {"workload": WORKLOAD, "precision": "mixed: per-event partial-wave columns "
-                   "cached as FP32 (computed in FP64), FP64 amplitude sum, log and reductions; "
-                   "MC integral from the FP64 Gram matrix (masses/widths fixed)",
-                   "events_per_rank": {"data": n_data, "mc": n_mc},
-                   "l2": "256 MB buffer written before every timed step (L2 126 MB)",
-                   "parallelism": f"dp{world}" if world > 1 else "single GPU"},
-        "plain_f64": {"value": world * args.steps / t_plain, "unit": "evals/s",
-                      "ms_per_step": 1e3 * t_plain / args.steps,
-                      "speedup_mixed_over_plain": t_plain / t_mixed},
-        "fp32_recompute": {"value": world * args.steps / t_f32, "unit": "evals/s",
-                           "ms_per_step": 1e3 * t_f32 / args.steps,
-                           "kernel_us": 1e6 * t_kernel_f32 / k_kernel,
-                           "dnll": nll_f - nll_p,
-                           "grad_max_rel": float(np.max(np.abs(g_f - g_p)) / np.max(np.abs(g_p)))},
-        "e2e": {"value": world * args.steps / t_e2e, "unit": "evals/s",
-                "h2d_bytes_per_step": 16 * code.ncol,
-                "d2h_bytes_per_step": 8 * (1 + 2 * code.ncol),
-                "call": "FCN.nll_grad(x) with x a host numpy vector"},
-        "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
-                     "frac": ach / hbm,
-                     "traffic": (NCU_TRAFFIC_PER_ROW[args.workload] * n_data
-                                 if args.workload in NCU_TRAFFIC_PER_ROW else None),
-                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
-                                       "launch at the bench size, scaled by the rows",
-                     "peak_kind": peak_kind,
-                     "kernel": "pwa_eval_cached_wred (data term, mixed form; ends with its "
-                               "own fixed-order two-level reduction)",
-                     "algorithmic_bytes_per_launch": bytes_mixed,
-                     "launch_us": 1e6 * t_kernel / k_kernel,
-                     "plain_f64_kernel": {"achieved": ach_p, "frac": ach_p / hbm,
-                                          "launch_us": 1e6 * t_kernel_p / k_kernel,
-                                          "algorithmic_bytes_per_launch": bytes_plain}},
-        "gpu_launches": args.steps,
-        "cached_variants": variants,
-        "check": {"nll_mixed": nll_m, "nll_plain": nll_p, "dnll": nll_m - nll_p,
-                  "grad_max_rel": float(np.max(np.abs(g_m - g_p)) / np.max(np.abs(g_p)))},
-        "setup_s": {"dataset": t_data},
-        "engine": eng.info(),
-    }
-    if ck_clocks:
-        line["clocks"] = ck_clocks
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line = measure_floating(args.workload, args, rank, world, dist, timed, log, args.n_sig,
+                                args.n_mc)
+    else:
+        line = measure_cached(args.workload, args, rank, world, dist, timed, log, args.n_sig,
+                              args.n_bg, args.n_mc)
+    if world == 1 and args.workload == "lc2pkpi" and not args.headline_only:
+        # the other workloads the metric names, each at its own size and with
+        # its own roofline, and the serving loop (one GPU)
+        extra = {}
         try:
-            line["cpu_baseline"] = cpu_baseline(n_sig, n_bg, n_mc, args.cpu_steps)
+            _, s4, b4, m4, _, _ = WORKLOADS["b2dstkpi"]
+            extra["b2dstkpi"] = _compact(measure_cached("b2dstkpi", args, rank, world, dist,
+                                                        timed, log, s4, b4, m4, variants=False))
+            _, sf, _, mf, _, _ = WORKLOADS["d2kpipi_float"]
+            extra["d2kpipi_float"] = _compact(measure_floating("d2kpipi_float", args, rank,
+                                                               world, dist, timed, log, sf, mf))
+            log("serving")
+            line["serving"] = serving_summary(args.n_fits)
+        except Exception as e:  # reported, never fatal to the headline
+            extra["error"] = repr(e)
+        line["workloads"] = extra
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == "lc2pkpi":
+        try:
+            line["cpu_baseline"] = cpu_baseline(args.n_sig, args.n_bg, args.n_mc, args.cpu_steps)
         except Exception as e:  # reported, never fatal
             line["cpu_baseline"] = {"error": repr(e)}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    fcn.eng.close()
-    fcn_plain.eng.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

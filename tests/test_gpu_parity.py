@@ -14,7 +14,7 @@ from common import golden_data, load_golden, load_model
 pytestmark = pytest.mark.gpu
 
 CASES = ["d2kpipi", "d2kpipi_float", "lc2pkpi", "b2dstkpi", "d2kpipi_shapes", "dp2kpipi_ident",
-         "ident_fermions", "epem_cp"]
+         "ident_fermions", "epem_cp", "toy_vvp", "ident3_fermions"]
 
 
 def _engine(name):
