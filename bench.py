@@ -307,16 +307,22 @@ def run_reference(args, rank):
 
 
 # ----------------------------------------------------------- GPU timing
+L2_BYTES = 126e6
+
+
 class Timer:
-    """k timed steps, L2 flushed (a 256 MB buffer written, L2 is 126 MB)
-    before each; device time from CUDA events on the launching (current)
-    stream, max over ranks."""
+    """k timed steps, device time from CUDA events on the launching
+    (current) stream, max over ranks.  With ``flush`` set, a 256 MB buffer
+    is written before every step (L2 is 126 MB); workloads whose inputs per
+    launch exceed twice the L2 run without it (their inputs do not fit in
+    L2, so no step finds the previous step's data there)."""
 
     def __init__(self, dist):
         import torch
 
         self.torch, self.dist = torch, dist
         self.flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+        self.do_flush = True
 
     def barrier(self):
         self.torch.cuda.synchronize()
@@ -329,7 +335,8 @@ class Timer:
               for _ in range(k)]
         self.barrier()
         for i in range(k):
-            self.flush.zero_()
+            if self.do_flush:
+                self.flush.zero_()
             ev[i][0].record()
             step_fn()
             ev[i][1].record()
@@ -404,6 +411,15 @@ def measure_cached(name, args, rank, world, dist, timed, log, n_sig, n_bg, n_mc,
     vals = cl.vm.get_all_dic()
     eng, eng_p = fcn.eng, fcn_plain.eng
     var_vec = np.array([vals[k] for k in fcn._var_names])
+    code = eng.code
+    n_data = n_sig + n_bg
+    bytes_mixed = n_data * (8 * code.nf + 8)
+    bytes_f32 = (n_data + n_mc) * (8 * len(code.mass_fields) + 4 * len(code.angle_fields) + 8)
+    timed.do_flush = min(bytes_mixed, bytes_f32) < 2 * L2_BYTES
+    l2_note = ("256 MB buffer written before every timed step (L2 126 MB)" if timed.do_flush
+               else f"inputs larger than L2: {bytes_mixed / 1e6:.0f} MB per launch of the "
+                    f"cached kernel, {bytes_f32 / 1e6:.0f} MB of the FP32 kernel (L2 126 MB); "
+                    "no flush")
     for _ in range(args.warmup):
         fcn.nll_grad(x0)
         fcn_plain.nll_grad(x0)
@@ -445,10 +461,6 @@ def measure_cached(name, args, rank, world, dist, timed, log, n_sig, n_bg, n_mc,
     peaks = {"f64_tflops": eng.fma_peak(PLAIN_F64) / 1e12,
              "f32_tflops": eng.fma_peak(MIXED_F32) / 1e12}
 
-    n_data = n_sig + n_bg
-    code = eng.code
-    n_mass, n_ang = len(code.mass_fields), len(code.angle_fields)
-    bytes_mixed = n_data * (8 * code.nf + 8)
     hbm, peak_kind = _peaks()
     ach = bytes_mixed / (t_kernel / k_kernel) / 1e9
     n_ev = n_data + n_mc
@@ -467,8 +479,7 @@ def measure_cached(name, args, rank, world, dist, timed, log, n_sig, n_bg, n_mc,
                    "cached as FP32 (computed in FP64), FP64 amplitude sum, log and reductions; "
                    "MC integral from the FP64-accurate Gram matrix (masses/widths fixed)",
                    "events_per_rank": {"data": n_data, "mc": n_mc},
-                   "l2": "256 MB buffer written before every timed step (L2 126 MB); inputs "
-                         "larger than L2 as well",
+                   "l2": l2_note,
                    "parallelism": f"dp{world}" if world > 1 else "single GPU"},
         "plain_f64": {"value": world * args.steps / t_plain, "unit": "evals/s",
                       "ms_per_step": 1e3 * t_plain / args.steps,
@@ -546,6 +557,7 @@ def measure_floating(name, args, rank, world, dist, timed, log, n_sig, n_mc):
         f.eng.mc_share = 1.0 / world  # equal MC shards
     x0 = np.array(cl.vm.get_all_val())
     vals, names = cl.vm.get_all_dic(), list(cl.vm.trainable_vars)
+    timed.do_flush = True  # its inputs fit in L2
     for _ in range(args.warmup):
         fcn.nll_grad(x0)
         fcn_p.nll_grad(x0)

@@ -65,6 +65,55 @@ SUBSET_F = 2048   # events per set whose fields are stored
 SUBSET_A = 8192   # events per set whose |A|^2 is stored
 
 
+# signal data of the large cases by accept-reject on the model's |A|^2, as
+# the workload definition asks: candidates from the flat generator (seeded),
+# kept where u * fmax < sum |A|^2 at the case's parameters; the kept indices
+# are stored, so a test regenerates the same candidates and keeps the same
+# events without evaluating the model
+ACCEPT_REJECT = {"d2kpipi_1e4": 100_000, "lc2pkpi_full": 6_000_000}
+
+
+def draw_params(names, rng, base):
+    """Seeded parameter values: |g| ~ U(0.5, 2), phase ~ U(-pi, pi); CP
+    deltas ~ U(-0.3, 0.3); polarisations ~ U(-0.4, 0.4); masses and widths
+    at their nominal values times U(0.97, 1.03)."""
+    params = {}
+    for k in names:
+        if k.endswith(("deltar", "deltai")):
+            params[k] = float(rng.uniform(-0.3, 0.3))
+        elif k.endswith("r") and ("_g_ls_" in k or "_total_" in k):
+            params[k] = float(rng.uniform(0.5, 2.0))
+        elif k.endswith("i") and ("_g_ls_" in k or "_total_" in k):
+            params[k] = float(rng.uniform(-np.pi, np.pi))
+        elif "_polarization_" in k:
+            params[k] = float(rng.uniform(-0.4, 0.4))
+        else:
+            params[k] = float(base[k]) * float(rng.uniform(0.97, 1.03))
+    return params
+
+
+def accept_reject(dc, plan, order, M, masses, n_cand, n_keep, seed, vals):
+    """Indices (into n_cand flat candidates of generate_phsp(seed)) of the
+    first n_keep events kept by u * fmax < sum |A|^2 (oracle, FP64, at the
+    parameter values ``vals``), fmax = 1.1 max over the candidates."""
+    sys.path.insert(0, REPO)
+    from oracle.pwa_oracle import OracleModel
+    from tf_pwa_b200.kinematics import event_fields, p4_dict
+    from tf_pwa_b200.phasespace import generate_phsp
+
+    arr = np.stack(generate_phsp(M, masses, n_cand, seed=seed), 1)
+    m = OracleModel(dc.decay_group, plan)
+    f = np.empty(n_cand)
+    for q in range(0, n_cand, 200_000):
+        r = min(q + 200_000, n_cand)
+        x = event_fields(plan, p4_dict(arr[q:r], order)).numpy()
+        f[q:r] = m.pdf(x, vals)
+    u = np.random.default_rng(seed + 99).uniform(size=n_cand)
+    idx = np.nonzero(u * 1.1 * f.max() < f)[0]
+    assert len(idx) >= n_keep, (len(idx), n_keep)
+    return idx[:n_keep].astype(np.int64), arr
+
+
 def subset_index(n, k, seed):
     """Sorted distinct event indices of one set (seeded)."""
     k = min(k, n)
@@ -130,11 +179,24 @@ def main(ref_root):
         M = dc.particle_property[str(top)]["mass"]
         tmp = tempfile.mkdtemp()
         p4 = {}
+        pre_params, kept = None, None
+        if name in ACCEPT_REJECT:
+            vm0 = VarsManager(rng=np.random.default_rng(0))
+            nm0 = init_params(group, vm0, dic.get("constrains"))
+            float_particles(group, vm0, nm0, dc.particle_property)
+            pre_params = draw_params(vm0.trainable_vars, rng, vm0.get_all_dic())
         for kk, (kind, n) in enumerate((("data", nd), ("bg", nb), ("phsp", nm))):
             if n == 0:
                 continue
-            ps = generate_phsp(M, masses, n, seed=1000 * seed + kk)
-            arr = np.stack(ps, 1)  # (n, n_final, 4)
+            if kind == "data" and name in ACCEPT_REJECT:
+                vals0 = vm0.get_all_dic()
+                vals0.update(pre_params)
+                kept, cand = accept_reject(dc, plan, order, M, masses, ACCEPT_REJECT[name], n,
+                                           1000 * seed + kk, vals0)
+                arr = cand[kept]
+            else:
+                ps = generate_phsp(M, masses, n, seed=1000 * seed + kk)
+                arr = np.stack(ps, 1)  # (n, n_final, 4)
             if name in BOOSTED:
                 arr = boost_events(arr, M, BOOSTED[name], rng)
             p4[kind] = arr
@@ -164,7 +226,10 @@ def main(ref_root):
         # seeded parameter values: |g| ~ U(0.5, 2), phase ~ U(-pi, pi);
         # masses/widths at their nominal values shifted by a few percent
         params = {}
-        for k in vm.trainable_vars:
+        if pre_params is not None:
+            assert list(pre_params) == list(vm.trainable_vars)
+            params = dict(pre_params)
+        for k in ([] if pre_params is not None else vm.trainable_vars):
             if k.endswith(("deltar", "deltai")):
                 params[k] = float(rng.uniform(-0.3, 0.3))
             elif k.endswith("r") and ("_g_ls_" in k or "_total_" in k):
@@ -233,6 +298,8 @@ def main(ref_root):
         if name in LARGE:
             out = dict(nll=np.float64(nll), grad=np.asarray(grad, np.float64),
                        sum_w=np.float64(np.sum(np.asarray(fcn.weight, np.float64))))
+            if kept is not None:
+                out["data_kept"] = kept
             for k, tag in (("data", "data"), ("phsp", "mc"), ("bg", "bg")):
                 if k not in fields:
                     continue
@@ -254,7 +321,8 @@ def main(ref_root):
                 "events": {"generator": "tf_pwa_b200.phasespace.generate_phsp",
                            "seeds": {"data": 1000 * seed, "bg": 1000 * seed + 1,
                                      "mc": 1000 * seed + 2},
-                           "sizes": {"data": nd, "bg": nb, "mc": nm}},
+                           "sizes": {"data": nd, "bg": nb, "mc": nm},
+                           "data_candidates": ACCEPT_REJECT.get(name)},
             }
             with open(os.path.join(HERE, name + ".json"), "w") as f:
                 json.dump(meta, f, indent=1)

@@ -1,7 +1,9 @@
 """Parity against the reference at the workloads' own sizes (through the C ABI).
 
 D -> K pi pi with 1e4 data / 1e5 MC events, and Lambda_c -> p K pi with 1e5
-signal + 1e4 background rows (weight -0.1) / 1e6 MC events.  The golden
+signal + 1e4 background rows (weight -0.1) / 1e6 MC events; the signal
+data are drawn from the model by accept-reject on |A|^2, as the workloads
+define them.  The golden
 files (``tests/golden/make_golden.py``, cases ``d2kpipi_1e4`` and
 ``lc2pkpi_full``) hold the reference's own NLL and GradientTape gradient
 over all events, its fields and |A|^2 at seeded subsets of the events, and
@@ -27,8 +29,10 @@ class _Cfg:
     pass
 
 
-def _events(meta, dc, plan):
-    """Momenta (n, n_final, 4) of every set, regenerated from the seeds."""
+def _events(meta, g, dc, plan):
+    """Momenta (n, n_final, 4) of every set, regenerated from the seeds; the
+    signal data are the stored accept-reject survivors among their flat
+    candidates."""
     from tf_pwa_b200.decay_config import load_yaml
     from tf_pwa_b200.phasespace import generate_phsp
 
@@ -43,7 +47,14 @@ def _events(meta, dc, plan):
     out = {}
     for tag in ("data", "bg", "mc"):
         n = ev["sizes"][tag]
-        if n:
+        if not n:
+            continue
+        if tag == "data" and ev.get("data_candidates"):
+            cand = np.stack(generate_phsp(M, masses, ev["data_candidates"],
+                                          seed=ev["seeds"][tag]), 1)
+            out[tag] = cand[g["data_kept"]]
+            assert out[tag].shape[0] == n
+        else:
             out[tag] = np.stack(generate_phsp(M, masses, n, seed=ev["seeds"][tag]), 1)
     return out
 
@@ -58,7 +69,7 @@ def case(request):
     g, meta = load_golden(request.param)
     dc, vm, plan = load_model(meta["config"])
     vm.set_all(meta["variables"])
-    p4 = _events(meta, dc, plan)
+    p4 = _events(meta, g, dc, plan)
     eng = Engine(dc.decay_group, plan, vm)
     fields = {t: eng.fields_from_p4(torch.as_tensor(a, device="cuda")) for t, a in p4.items()}
     cfg = _Cfg()
