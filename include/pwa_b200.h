@@ -314,6 +314,13 @@ int pwa_server_result(pwa_server* s, long long fit_id, int wait, int* status, do
 /* out[5]: rounds (launches), requests, seconds inside the launches, active
  * fits, queued fits. */
 int pwa_server_stats(pwa_server* s, double* out);
+/* The service's own tuning of its multi-request launch (no counterpart in
+ * the reference): its first rounds with at least 16 tiles per SM of work
+ * try each block count per SM the occupancy allows (up to four), three
+ * rounds each, timing seconds per work tile, and keep the fastest.
+ * out[9]: [0] the block count chosen (0 while tuning), then per candidate
+ * (block count, median seconds per tile). */
+int pwa_server_tuning(pwa_server* s, double* out);
 /* Stop the scheduler (unfinished fits end as failed) and free the server. */
 int pwa_server_destroy(pwa_server* s);
 

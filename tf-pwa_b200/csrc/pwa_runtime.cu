@@ -104,6 +104,7 @@ struct pwa_plan {
   double* d_tile_part = nullptr;
   double* d_multi_out = nullptr;
   long long multi_cap_work = 0, multi_cap_req = 0;
+  int multi_bps = 0;  // blocks per SM of pwa_eval_multi (0: occupancy limit)
   // parameter layout for the C-side chain rule
   int n_vars = 0, n_coup = 0, nfac = 0, n_train = 0;
   std::vector<int> coup_r, coup_i, coup_polar, col_fac, train_idx;
@@ -1339,6 +1340,7 @@ int pwa_pieces_multi(pwa_plan* h, int n_req, const long long* first_tile, const 
   int per_sm = 0;
   CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)h->k.eval_multi, h->tpb, 0));
   if (per_sm < 1) per_sm = 1;
+  if (h->multi_bps > 0 && h->multi_bps < per_sm) per_sm = h->multi_bps;
   long long nb = (long long)per_sm * h->sms;
   if (nb > n_work) nb = n_work;
   void* a1[] = {&h->d_ck, &h->d_work_req, &h->d_work_tile, &n_work, &h->pool_f, &h->pool_w,
@@ -1680,6 +1682,12 @@ struct pwa_server {
   std::string err;
   long long batches = 0, requests = 0;
   double busy = 0.0;
+  // online tuning of the multi-request launch: the first large rounds try
+  // each block count per SM in turn, timing seconds per work tile; the
+  // fastest (median of three rounds each) is kept for the rest
+  std::vector<int> tune_cand;
+  std::vector<std::vector<double>> tune_t;
+  int tune_next = 0, tuned_bps = 0;
 };
 
 namespace {
@@ -1848,10 +1856,31 @@ void srv_loop(pwa_server* S) {
       const std::vector<double>& xe = F->phase == 0 ? F->x : F->xt;
       for (int t = 0; t < P; ++t) v[h->train_idx[t]] = xe[t];
     }
+    long long n_work = 0;
+    for (int r = 0; r < n; ++r) n_work += nt[r];
+    // a round large enough to fill the GPU several times over is a tuning sample
+    const bool sample = !S->tuned_bps && !S->tune_cand.empty() && n_work >= 4LL * h->sms * 4;
+    if (sample) h->multi_bps = S->tune_cand[S->tune_next];
     const double t0 = now_s();
     const int rc = pwa_pieces_multi(h, n, ft.data(), nt.data(), vars.data(), sw.data(), 1.0,
                                     nullptr, out.data());
     const double t1 = now_s();
+    if (sample && rc == PWA_OK) {
+      S->tune_t[S->tune_next].push_back((t1 - t0) / (double)n_work);
+      S->tune_next = (S->tune_next + 1) % (int)S->tune_cand.size();
+      bool all = true;
+      for (const auto& v : S->tune_t) all = all && v.size() >= 3;
+      if (all) {
+        double best = 0.0;
+        for (size_t c = 0; c < S->tune_cand.size(); ++c) {
+          std::vector<double> v = S->tune_t[c];
+          std::sort(v.begin(), v.end());
+          const double med = v[v.size() / 2];
+          if (!S->tuned_bps || med < best) S->tuned_bps = S->tune_cand[c], best = med;
+        }
+        h->multi_bps = S->tuned_bps;
+      }
+    }
     std::vector<double> grad(P);
     std::lock_guard<std::mutex> lk(S->mu);
     S->batches++;
@@ -1899,6 +1928,13 @@ int pwa_server_create(pwa_plan* h, const double* base_vars, const double* consts
   S->max_active = max_active;
   S->gtol = gtol;
   S->maxiter = maxiter;
+  {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)h->k.eval_multi,
+                                                      h->tpb, 0) == cudaSuccess)
+      for (int b = per_sm; b >= 1 && (int)S->tune_cand.size() < 4; --b) S->tune_cand.push_back(b);
+    S->tune_t.assign(S->tune_cand.size(), {});
+  }
   S->th = std::thread(srv_loop, S);
   *out = S;
   return PWA_OK;
@@ -1960,6 +1996,23 @@ int pwa_server_stats(pwa_server* S, double* out) {
   out[2] = S->busy;
   out[3] = (double)S->active.size();
   out[4] = (double)S->pending.size();
+  return PWA_OK;
+}
+
+int pwa_server_tuning(pwa_server* S, double* out) {
+  if (!S || !out) return PWA_ERR_ARG;
+  std::lock_guard<std::mutex> lk(S->mu);
+  out[0] = (double)S->tuned_bps;
+  for (int c = 0; c < 4; ++c) {
+    out[1 + 2 * c] = c < (int)S->tune_cand.size() ? (double)S->tune_cand[c] : 0.0;
+    double m = 0.0;
+    if (c < (int)S->tune_t.size() && !S->tune_t[c].empty()) {
+      std::vector<double> v = S->tune_t[c];
+      std::sort(v.begin(), v.end());
+      m = v[v.size() / 2];
+    }
+    out[2 + 2 * c] = m;
+  }
   return PWA_OK;
 }
 

@@ -78,6 +78,7 @@ def load_library(path=LIB_PATH):
     ip_ = ctypes.POINTER(ctypes.c_int)
     lib.pwa_server_result.argtypes = [vp, ll, i, ip_, dp, dp, ip_, ip_, dp]
     lib.pwa_server_stats.argtypes = [vp, dp]
+    lib.pwa_server_tuning.argtypes = [vp, dp]
     lib.pwa_server_destroy.argtypes = [vp]
     lib.pwa_plan_destroy.argtypes = [vp]
     lib.pwa_compile_only.argtypes = [cp, sz, i, cp, cp, sz]

@@ -310,6 +310,17 @@ class NativeFitServer:
         return {"rounds": int(out[0]), "requests": int(out[1]), "launch_s": out[2],
                 "active": int(out[3]), "queued": int(out[4])}
 
+    def tuning(self):
+        """Block count per SM the service chose for its launches and the
+        median seconds per work tile of each candidate."""
+        import ctypes
+
+        out = (ctypes.c_double * 9)()
+        self._lib.pwa_server_tuning(self.h, out)
+        return {"blocks_per_sm": int(out[0]),
+                "candidates": {int(out[1 + 2 * c]): out[2 + 2 * c] for c in range(4)
+                               if out[1 + 2 * c] > 0}}
+
     def close(self):
         if self.h:
             self._lib.pwa_server_destroy(self.h)
@@ -376,7 +387,7 @@ def serving_benchmark(n_fits=512, n_mc=1_000_000, n_min=1_000, n_max=1_000_000,
         st = server.stats()
         rounds, reqs = st["rounds"], st["requests"]
         batch_info = {"batches": rounds, "mean_requests_per_batch": reqs / max(rounds, 1),
-                      "launch_seconds": st["launch_s"]}
+                      "launch_seconds": st["launch_s"], "tuning": server.tuning()}
     else:
         for j in jobs:
             j.done.wait()
