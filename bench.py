@@ -516,7 +516,9 @@ def measure_cached(name, args, rank, world, dist, timed, log, n_sig, n_bg, n_mc,
         "autotune": {"choice": {"variant": tuned[0], "ring_stages": tuned[1],
                                 "blocks_per_sm": tuned[2]},
                      "table_us": None if fcn.tune is None or fcn.tune[0] is None
-                     else [round(float(x), 2) for x in fcn.tune[0]]},
+                     else [round(float(x), 2) for x in fcn.tune[0]],
+                     "error": fcn.tune[2] if fcn.tune is not None and len(fcn.tune) > 2
+                     else None},
         "cached_variants": var_table,
         "check": {"nll_mixed": nll_m, "nll_plain": nll_p, "dnll": nll_m - nll_p,
                   "grad_max_rel": float(np.max(np.abs(g_m - g_p)) / np.max(np.abs(g_p)))},

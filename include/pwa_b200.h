@@ -214,6 +214,18 @@ int pwa_pieces_cached(pwa_plan* h, const double* vars, double sw, double mc_shar
 
 /* NLL and gradient (FCN.nll_grad, tf_pwa/model/model.py:1223-1229) on one
  * device from the cache: vars[n_vars] in, *out_nll and out_grad[n_train]. */
+/* Many parameter points in one pass over the column cache (the reference
+ * evaluates each point of a Hessian stencil, line search or likelihood scan
+ * separately, tf_pwa/model/model.py:513-561): vars holds n_pts rows of
+ * n_vars values; out n_pts rows of the piece vector of pwa_pieces_cached.
+ * Each warp holds its events' columns in registers and evaluates every
+ * point on them with FP32 amplitudes and FP32 log (FP64 sums), so
+ * gradients are good to ~1e-6 relative and the NLL to ~1e-4 absolute at
+ * 1e6 events; pwa_hessian_cached uses it for its 4 n_train stencil
+ * points.  Points beyond what one launch's shared memory holds (about 100
+ * for 8 columns, 25 for 30) go in further launches. */
+int pwa_pieces_points(pwa_plan* h, int n_pts, const double* vars, double sw, double mc_share,
+                      void* stream, double* out);
 int pwa_nll_grad_cached(pwa_plan* h, const double* vars, double sw, void* stream,
                         double* out_nll, double* out_grad);
 

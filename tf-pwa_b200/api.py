@@ -27,7 +27,7 @@ import warnings
 import numpy as np
 
 from .decay_config import DecayConfig, float_particles, init_params, load_yaml
-from .engine import MIXED_F32, PLAIN_F64, Engine, read_dat
+from .engine import MIXED_F32, PLAIN_F64, Engine, PWAError, read_dat
 from .kinematics import event_fields, p4_dict
 from .plan import Plan
 from .variables import Bound, VarsManager
@@ -202,7 +202,12 @@ class FCN:
             # for this model and event count (PWA_AUTOTUNE=0: keep the default)
             if os.environ.get("PWA_AUTOTUNE", "1") != "0":
                 self.eng.consts(vals)
-                self.tune = self.eng.autotune_cached()
+                try:
+                    self.tune = self.eng.autotune_cached()
+                except PWAError as e:  # keep the default configuration
+                    warnings.warn(f"cached-kernel autotuning failed, default kept: {e}")
+                    self.tune = (None, None, str(e))
+                    self.eng.set_cached_config(-1)
 
     def _upload(self, data, bg, mcdata):
         import torch

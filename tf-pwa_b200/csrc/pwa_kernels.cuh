@@ -1502,6 +1502,152 @@ extern "C" __global__ void __launch_bounds__(PWA_TMA_THREADS, 1)
 }
 
 // ---------------------------------------------------------------------------
+// Many parameter points in one pass over the column cache (Hessian stencils,
+// line-search trials, likelihood scans).  One block of PWA_PTS_WARPS warps
+// per SM; each warp takes a contiguous run of 32-event units, holds the
+// unit's columns in registers and evaluates every point m of the launch on
+// them: A_o = sum_k c_mk F_ko in FP32 (couplings staged as FP32 in shared
+// memory), f = sum_o |A_o|^2, w * log f (FP32 log, summed in FP64) and the
+// sensitivities fac * conj(A) F_k (fac = w clip_log'(f), FP32, reduce-
+// scattered across the warp, FP64 accumulation).  Per-warp FP64 rows of
+// (point, accumulator) live in shared memory; the block writes its row of
+// n_pts * NA sums and the last block sums the rows in a fixed order into
+// out[n_pts][NA].  FP32 amplitudes keep the gradient to ~1e-6 relative:
+// the differenced Hessian needs no more (the centre point of a stencil is
+// evaluated by the FP64-amplitude kernel).
+#ifndef PWA_PTS_WARPS
+#define PWA_PTS_WARPS 16
+#endif
+__device__ __forceinline__ float clip_logf(float x, float* dx) {
+  const float eps = 1e-6f;
+  if (x > eps) {
+    *dx = 1.0f / x;
+    return logf(x);
+  }
+  const float t = (x - eps) / eps;
+  *dx = 1.0f / eps - (x - eps) / (eps * eps);
+  return -13.815510557964274f + t - 0.5f * t * t;  // log(1e-6) + t - t^2/2
+}
+
+extern "C" __global__ void __launch_bounds__(PWA_PTS_WARPS * 32, 1)
+    pwa_eval_cached_points(const double* __restrict__ ck, int n_pts,
+                           const float2* __restrict__ Fc, const double* __restrict__ Wc,
+                           long long ntiles, double* __restrict__ partials,
+                           unsigned int* __restrict__ ticket, double* __restrict__ out) {
+  constexpr int NA = PWA_CACHE_NA, NG = 2 * PWA_NCOL;
+  constexpr int NW = PWA_PTS_WARPS, UPT = PWA_TPB / 32;
+  extern __shared__ __align__(16) double pts_smem[];
+  double* s_acc = pts_smem;                                   // [NW][n_pts][NA]
+  float* s_c = (float*)(pts_smem + (size_t)NW * n_pts * NA);  // [n_pts][2 NCOL]
+  __shared__ int s_last;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int j = tid; j < NW * n_pts * NA; j += NW * 32) s_acc[j] = 0.0;
+  for (int j = tid; j < n_pts * NG; j += NW * 32) s_c[j] = (float)ck[j];
+  __syncthreads();
+  const long long U = ntiles * UPT, W = (long long)gridDim.x * NW;
+  const long long gw = (long long)blockIdx.x * NW + warp;
+  const long long u0 = gw * U / W, u1 = (gw + 1) * U / W;
+  double* my = s_acc + (size_t)warp * n_pts * NA;
+#pragma unroll 1
+  for (long long u = u0; u < u1; ++u) {
+    const long long t = u / UPT;
+    const int e = (int)(u - t * UPT) * 32 + lane;
+    const float2* F = Fc + t * PWA_NF * PWA_TPB + e;
+    float2 v[PWA_NF];
+#pragma unroll
+    for (int j = 0; j < PWA_NF; ++j) v[j] = __ldcs(F + j * PWA_TPB);
+    const float w = (float)__ldcs(Wc + t * PWA_TPB + e);
+#pragma unroll 1
+    for (int m = 0; m < n_pts; ++m) {
+      const float* c = s_c + m * NG;
+      float ar[PWA_NOUT], ai[PWA_NOUT];
+#pragma unroll
+      for (int o = 0; o < PWA_NOUT; ++o) ar[o] = ai[o] = 0.f;
+#pragma unroll
+      for (int j = 0; j < PWA_NF; ++j) {
+        const int k = pwa_fk[j], o = pwa_fo[j];
+        const float cr = c[2 * k], ci = c[2 * k + 1];
+        ar[o] = fmaf(cr, v[j].x, fmaf(-ci, v[j].y, ar[o]));
+        ai[o] = fmaf(cr, v[j].y, fmaf(ci, v[j].x, ai[o]));
+      }
+      float f = 0.f;
+#pragma unroll
+      for (int o = 0; o < PWA_NOUT; ++o) f = fmaf(ar[o], ar[o], fmaf(ai[o], ai[o], f));
+      float dl;
+      const float cl = clip_logf(f, &dl);
+      const float fac = w * dl;
+      float br[PWA_NOUT], bi[PWA_NOUT];
+#pragma unroll
+      for (int o = 0; o < PWA_NOUT; ++o) {
+        br[o] = fac * ar[o];
+        bi[o] = -fac * ai[o];
+      }
+      const double s0 = warp_sum((double)(w * cl));
+      if (lane == 0) my[m * NA] += s0;
+#if PWA_RS16
+      float g[16];
+#pragma unroll
+      for (int q = 0; q < 16; ++q) g[q] = 0.f;
+#pragma unroll
+      for (int j = 0; j < PWA_NF; ++j) {
+        const int k = pwa_fk[j], o = pwa_fo[j];
+        g[2 * k] = fmaf(br[o], v[j].x, fmaf(-bi[o], v[j].y, g[2 * k]));
+        g[2 * k + 1] = fmaf(br[o], v[j].y, fmaf(bi[o], v[j].x, g[2 * k + 1]));
+      }
+      warp_rs_step<16, 16, 16>(g, lane);
+      const float gs = g[0] + __shfl_xor_sync(0xffffffffu, g[0], 1);
+      const int idx = lane >> 1;
+      if (!(lane & 1) && idx < NG) my[m * NA + 1 + idx] += (double)gs;
+#else
+#pragma unroll
+      for (int mg = 0; mg < PWA_GPAD / 32; ++mg) {
+        float g[32];
+#pragma unroll
+        for (int q = 0; q < 32; ++q) g[q] = 0.f;
+#pragma unroll
+        for (int j = 0; j < PWA_NF; ++j) {
+          const int k = pwa_fk[j], o = pwa_fo[j];
+          if (k >= 16 * mg && k < 16 * mg + 16) {
+            const int q = 2 * (k - 16 * mg);
+            g[q] = fmaf(br[o], v[j].x, fmaf(-bi[o], v[j].y, g[q]));
+            g[q + 1] = fmaf(br[o], v[j].y, fmaf(bi[o], v[j].x, g[q + 1]));
+          }
+        }
+        warp_reduce_scatter<32>(g, lane);
+        const int idx = 32 * mg + lane;
+        if (idx < NG) my[m * NA + 1 + idx] += (double)g[0];
+      }
+#endif
+    }
+  }
+  __syncthreads();
+  // block row: the warps' rows summed in warp order
+  const int tot = n_pts * NA;
+  for (int j = tid; j < tot; j += NW * 32) {
+    double a = 0.0;
+    for (int w2 = 0; w2 < NW; ++w2) a += s_acc[(size_t)w2 * tot + j];
+    partials[(long long)blockIdx.x * tot + j] = a;
+  }
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) s_last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  for (int j = tid; j < tot; j += NW * 32) {
+    double a0 = 0.0, a1 = 0.0;
+    int r = 0;
+    for (; r + 1 < (int)gridDim.x; r += 2) {
+      a0 += __ldcg(partials + (long long)r * tot + j);
+      a1 += __ldcg(partials + (long long)(r + 1) * tot + j);
+    }
+    if (r < (int)gridDim.x) a0 += __ldcg(partials + (long long)r * tot + j);
+    out[j] = a0 + a1;
+  }
+  if (tid == 0) ticket[0] = 0u;
+}
+
+// ---------------------------------------------------------------------------
 // Many fits in one launch (serving).  Each fit's data-event column cache is a
 // run of tiles in a shared pool (same tile layout as above).  The launch gets
 // a work list of (request, pool tile) pairs covering the tiles of every fit

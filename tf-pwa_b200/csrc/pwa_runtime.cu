@@ -39,7 +39,7 @@ struct Kernels {
                eval_cached_direct = nullptr, eval_cached_wred = nullptr, eval_cached_ring2 = nullptr,
                eval_cached_wide = nullptr, eval_cached_tma = nullptr, eval_multi = nullptr,
                gram_colmax = nullptr, gram_tc = nullptr, wait_check = nullptr,
-               fma_f64 = nullptr, fma_f32 = nullptr, reduce_multi = nullptr,
+               fma_f64 = nullptr, fma_f32 = nullptr, eval_points = nullptr, reduce_multi = nullptr,
                fields_from_p4 = nullptr, toy_select = nullptr, toy_fields = nullptr;
 };
 
@@ -105,6 +105,9 @@ struct pwa_plan {
   double* d_multi_out = nullptr;
   long long multi_cap_work = 0, multi_cap_req = 0;
   int multi_bps = 0;  // blocks per SM of pwa_eval_multi (0: occupancy limit)
+  // multi-point evaluation: device couplings and sums of up to pts_cap points
+  double* d_pts = nullptr;
+  int pts_cap = 0;
   // parameter layout for the C-side chain rule
   int n_vars = 0, n_coup = 0, nfac = 0, n_train = 0;
   std::vector<int> coup_r, coup_i, coup_polar, col_fac, train_idx;
@@ -368,6 +371,7 @@ int pwa_plan_create(const char* src, size_t src_len, int n_mass, int n_angle, in
             {"pwa_gram_tc", &h->k.gram_tc},
             {"pwa_wait_check", &h->k.wait_check},
             {"pwa_fma_peak_f64", &h->k.fma_f64},
+            {"pwa_eval_cached_points", &h->k.eval_points},
             {"pwa_fma_peak_f32", &h->k.fma_f32},
             {"pwa_fields_from_p4", &h->k.fields_from_p4},
             {"pwa_toy_select", &h->k.toy_select},
@@ -405,6 +409,7 @@ int pwa_plan_destroy(pwa_plan* h) {
   if (h->d_ck) cudaFree(h->d_ck);
   if (h->d_tile_part) cudaFree(h->d_tile_part);
   if (h->d_multi_out) cudaFree(h->d_multi_out);
+  if (h->d_pts) cudaFree(h->d_pts);
   if (h->h_map) cudaFreeHost(h->h_map);
   if (h->d_out) cudaFree(h->d_out);
   if (h->h_out) cudaFreeHost(h->h_out);
@@ -987,6 +992,12 @@ int pwa_autotune_cached(pwa_plan* h, const double* ck, int reps, void* stream, i
   cands.push_back({0, 0, 0});
   cands.push_back({3, 0, 0});
   if ((int)cands.size() > 32) cands.resize(32);
+  {
+    const cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess)
+      return set_err(h, PWA_ERR_CUDA, std::string("autotune: stream not clean before timing: ") +
+                                          cudaGetErrorString(e));
+  }
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
     if (e0) cudaEventDestroy(e0);
@@ -998,13 +1009,18 @@ int pwa_autotune_cached(pwa_plan* h, const double* ck, int reps, void* stream, i
     apply_cached_config(h, cands[c].variant, cands[c].stages, cands[c].bps);
     for (int w = 0; w < 2 && rc == PWA_OK; ++w) rc = pwa_eval_cached_enqueue(h, ck, stream);
     if (rc) break;
-    cudaEventRecord(e0, s);
-    for (int r = 0; r < reps && rc == PWA_OK; ++r) rc = pwa_eval_cached_enqueue(h, ck, stream);
-    cudaEventRecord(e1, s);
+    cudaError_t e = cudaEventRecord(e0, s);
+    for (int r = 0; r < reps && rc == PWA_OK && e == cudaSuccess; ++r)
+      rc = pwa_eval_cached_enqueue(h, ck, stream);
     if (rc) break;
+    if (e == cudaSuccess) e = cudaEventRecord(e1, s);
     float ms = 0.f;
-    if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
-      rc = set_err(h, PWA_ERR_CUDA, "autotune timing failed");
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    if (e != cudaSuccess) {
+      rc = set_err(h, PWA_ERR_CUDA, "autotune timing of configuration " + std::to_string(c) +
+                                        " (variant " + std::to_string(cands[c].variant) +
+                                        "): " + cudaGetErrorString(e));
       break;
     }
     wait_cached(h, s);
@@ -1366,6 +1382,83 @@ int pwa_pieces_multi(pwa_plan* h, int n_req, const long long* first_tile, const 
   return PWA_OK;
 }
 
+namespace {
+constexpr int kPtsWarps = 16;  // PWA_PTS_WARPS
+
+// Points one launch of pwa_eval_cached_points can take (shared memory:
+// per-warp FP64 rows of n_pts * NA sums plus FP32 couplings).
+int points_per_launch(pwa_plan* h) {
+  int optin = 0;
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
+  const int na = 1 + 2 * h->ncol;
+  const long long per = (long long)kPtsWarps * na * 8 + 2LL * h->ncol * 4;
+  long long m = ((long long)optin - 2048) / per;
+  if (m > 128) m = 128;
+  return (int)(m < 1 ? 1 : m);
+}
+
+// Data-term sums (n_pts rows of 1 + 2 ncol) of the column couplings ck
+// (n_pts rows of 2 ncol), at most points_per_launch(h) points.
+int eval_points_chunk(pwa_plan* h, const double* ck, int n_pts, cudaStream_t s, double* sums) {
+  const int K = h->ncol, NA = 1 + 2 * K;
+  if (n_pts > h->pts_cap) {
+    if (h->d_pts) cudaFree(h->d_pts);
+    h->d_pts = nullptr;
+    h->pts_cap = 0;
+    if (cudaMalloc(&h->d_pts, sizeof(double) * (size_t)n_pts * (2 * K + NA)) != cudaSuccess)
+      return set_err(h, PWA_ERR_OOM, "cudaMalloc of the multi-point buffers failed");
+    h->pts_cap = n_pts;
+  }
+  const int nb = (int)(h->sms < h->ntiles ? h->sms : h->ntiles);
+  int rc = ensure_partials(h, (long long)nb * n_pts * NA);
+  if (rc) return rc;
+  double* d_ck = h->d_pts;
+  double* d_out = h->d_pts + (size_t)n_pts * 2 * K;
+  CU(cudaMemcpyAsync(d_ck, ck, sizeof(double) * (size_t)n_pts * 2 * K, cudaMemcpyHostToDevice, s));
+  const size_t smem = (size_t)kPtsWarps * n_pts * NA * 8 + (size_t)n_pts * 2 * K * 4;
+  CU(cudaFuncSetAttribute((const void*)h->k.eval_points,
+                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  long long nt = h->ntiles;
+  void* args[] = {&d_ck, &n_pts, &h->fcache, &h->wcache, &nt, &h->partials, &h->ticket, &d_out};
+  cudaError_t e = cudaLaunchKernel((const void*)h->k.eval_points, dim3(nb), dim3(kPtsWarps * 32),
+                                   args, smem, s);
+  if (e != cudaSuccess)
+    return set_err(h, PWA_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+  CU(cudaMemcpyAsync(sums, d_out, sizeof(double) * (size_t)n_pts * NA, cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  return PWA_OK;
+}
+}  // namespace
+
+int pwa_pieces_points(pwa_plan* h, int n_pts, const double* vars, double sw, double mc_share,
+                      void* stream, double* out) {
+  if (!h) return PWA_ERR_ARG;
+  if (n_pts <= 0 || !vars || !out) return set_err(h, PWA_ERR_ARG, "invalid multi-point arguments");
+  if (h->fcache_n <= 0) return set_err(h, PWA_ERR_STATE, "no column cache (call pwa_cache_data)");
+  if (h->n_coup == 0) return set_err(h, PWA_ERR_STATE, "parameter layout not set");
+  if (!h->gram_valid) return set_err(h, PWA_ERR_STATE, "MC Gram matrix not built");
+  cudaStream_t s = (cudaStream_t)stream;
+  const int K = h->ncol, NA = 1 + 2 * K, P = h->n_train;
+  const int per = points_per_launch(h);
+  std::vector<std::vector<cplx>> zs(n_pts);
+  std::vector<double> ck((size_t)n_pts * 2 * K), sums((size_t)n_pts * NA);
+  for (int m = 0; m < n_pts; ++m)
+    column_couplings(h, vars + (size_t)m * h->n_vars, &zs[m], ck.data() + (size_t)m * 2 * K);
+  for (int m0 = 0; m0 < n_pts; m0 += per) {
+    const int cnt = n_pts - m0 < per ? n_pts - m0 : per;
+    const int rc = eval_points_chunk(h, ck.data() + (size_t)m0 * 2 * K, cnt, s,
+                                     sums.data() + (size_t)m0 * NA);
+    if (rc) return rc;
+  }
+  for (int m = 0; m < n_pts; ++m) {
+    const int rc = pieces_from_sums(h, vars + (size_t)m * h->n_vars, zs[m],
+                                    ck.data() + (size_t)m * 2 * K, sums.data() + (size_t)m * NA,
+                                    sw, mc_share, out + (size_t)m * (3 + 2 * P));
+    if (rc) return rc;
+  }
+  return PWA_OK;
+}
+
 int pwa_nll_grad_cached(pwa_plan* h, const double* vars, double sw, void* stream,
                         double* out_nll, double* out_grad) {
   if (!h) return PWA_ERR_ARG;
@@ -1406,22 +1499,30 @@ int pwa_hessian_cached(pwa_plan* h, const double* vars, double sw, double step, 
   std::vector<double> x(vars, vars + h->n_vars);
   int rc = pwa_nll_grad_cached(h, x.data(), sw, stream, out_nll, out_grad);
   if (rc) return rc;
-  std::vector<double> g(4 * (size_t)P);
-  double nll_tmp;
+  // the 4P stencil points in one multi-point pass over the column cache
+  const double shift[4] = {-2.0, -1.0, 1.0, 2.0};
+  std::vector<double> pts((size_t)4 * P * h->n_vars), hs(P);
   for (int i = 0; i < P; ++i) {
     const int vi = h->train_idx[i];
-    const double x0 = x[vi];
-    const double hs = step * std::max(std::fabs(x0), 1e-2);
-    const double shift[4] = {-2.0, -1.0, 1.0, 2.0};
+    hs[i] = step * std::max(std::fabs(x[vi]), 1e-2);
     for (int q = 0; q < 4; ++q) {
-      x[vi] = x0 + shift[q] * hs;
-      rc = pwa_nll_grad_cached(h, x.data(), sw, stream, &nll_tmp, g.data() + (size_t)q * P);
-      if (rc) return rc;
+      double* row = pts.data() + ((size_t)4 * i + q) * h->n_vars;
+      std::copy(x.begin(), x.end(), row);
+      row[vi] = x[vi] + shift[q] * hs[i];
     }
-    x[vi] = x0;
+  }
+  std::vector<double> pc((size_t)4 * P * (3 + 2 * P));
+  rc = pwa_pieces_points(h, 4 * P, pts.data(), sw, 1.0, stream, pc.data());
+  if (rc) return rc;
+  std::vector<double> g(4 * (size_t)P);
+  for (int i = 0; i < P; ++i) {
+    for (int q = 0; q < 4; ++q) {
+      const double* v = pc.data() + ((size_t)4 * i + q) * (3 + 2 * P);
+      for (int t = 0; t < P; ++t) g[(size_t)q * P + t] = -v[3 + t] + v[2] * v[3 + P + t] / v[1];
+    }
     for (int j = 0; j < P; ++j)
       out_hess[(size_t)i * P + j] =
-          (g[j] - 8.0 * g[P + j] + 8.0 * g[2 * P + j] - g[3 * P + j]) / (12.0 * hs);
+          (g[j] - 8.0 * g[P + j] + 8.0 * g[2 * P + j] - g[3 * P + j]) / (12.0 * hs[i]);
   }
   for (int i = 0; i < P; ++i)
     for (int j = i + 1; j < P; ++j) {

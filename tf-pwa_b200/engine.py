@@ -57,6 +57,7 @@ def load_library(path=LIB_PATH):
     lib.pwa_set_gram_method.argtypes = [vp, i]
     lib.pwa_wait_check.argtypes = [vp, i, ctypes.c_uint, ctypes.c_double, vp]
     lib.pwa_fma_peak.argtypes = [vp, i, ll, vp, dp]
+    lib.pwa_pieces_points.argtypes = [vp, i, dp, ctypes.c_double, ctypes.c_double, vp, dp]
     lib.pwa_autotune_cached.argtypes = [vp, dp, i, vp, ip, dp]
     lib.pwa_cached_config.argtypes = [vp, ip]
     lib.pwa_set_cached_config.argtypes = [vp, i, i, i]
@@ -936,6 +937,17 @@ class Engine:
                                                        stream or 0, self._nbuf_p, self._gbuf_p),
                     "pwa_nll_grad_cached")
         return float(self._nbuf[0]), self._gbuf.copy()
+
+    def pieces_points(self, var_rows, mc_share=None, stream=None):
+        """Piece vectors of many parameter points (rows of all variables) in
+        one pass over the column cache (FP32 amplitudes; pwa_pieces_points)."""
+        V = np.ascontiguousarray(var_rows, np.float64)
+        out = np.zeros((V.shape[0], 3 + 2 * self._n_train))
+        share = self.mc_share if mc_share is None else mc_share
+        self._check(load_library().pwa_pieces_points(self.h, V.shape[0], _dptr(V), self._sw,
+                                                     share, stream or 0, _dptr(out)),
+                    "pwa_pieces_points")
+        return out
 
     def hessian_cached(self, var_values, step=1e-4, stream=None):
         """(nll, grad, Hessian) of the cached form, the Hessian by 4-point
