@@ -178,7 +178,8 @@ int pwa_set_cached_variant(pwa_plan* h, int variant);
 /* Autotuner of the cached data-term kernel (no counterpart in the
  * reference, which has no kernels): times every configuration -- variant
  * 2 at each block count per SM the occupancy allows, variants 1 and 4,
- * variant 5 at every ring depth from 3 stages to the shared-memory limit,
+ * variant 5 at every even ring depth from 4 stages to the shared-memory
+ * limit (its two consumer groups need an even depth),
  * variants 0 and 3 -- with CUDA events over `reps` back-to-back launches
  * on the plan's column cache and couplings ck, keeps the fastest.
  * out[i] = mean microseconds per launch of configuration i (at most 32),

@@ -154,6 +154,10 @@ def test_cached_kernel_variants_agree(name):
               precision="mixed")
     vals = [vm.variables[k] for k in fcn._var_names]
     res = {}
+    from tf_pwa_b200.engine import PWAError
+
+    with pytest.raises(PWAError):  # the ring's two consumer groups need an even depth
+        fcn.eng.set_cached_config(5, 3)
     for var in (0, 1, 2, 3, 4, 5):
         fcn.eng.set_cached_variant(var)
         res[var] = fcn.eng.nll_grad_cached(vals)

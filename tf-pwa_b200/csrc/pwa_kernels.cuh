@@ -1407,7 +1407,11 @@ extern "C" __global__ void __launch_bounds__(PWA_WIDE_WARPS * 32, 1)
 // once, then evaluates them as pwa_eval_cached_wred does.  The block's tiles
 // are one contiguous run.  Waits are bounded: a wait that gives up sets the
 // error flag, the producer waits (bounded) for every copy it issued, and
-// the host sees out[NA] != 0.
+// the host sees out[NA] != 0.  The ring depth must be a multiple of
+// PWA_TMA_GROUPS: then every stage is read by one consumer group only, in
+// iteration order, so no group ever waits on a barrier phase two ahead of
+// the current one (a parity wait for that phase would return at once).
+// Any other depth is refused with the error flag before any barrier use.
 #ifndef PWA_TMA_GROUPS
 #define PWA_TMA_GROUPS 2
 #endif
@@ -1431,6 +1435,16 @@ extern "C" __global__ void __launch_bounds__(PWA_TMA_THREADS, 1)
   __shared__ int s_last;
   __shared__ volatile int s_err;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (stages < PWA_TMA_GROUPS || stages > PWA_TMA_MAXST || stages % PWA_TMA_GROUPS) {
+    // refused depth: report it like a stalled ring (zero sums, error flag)
+    if (tid == 0) atomicOr((unsigned int*)(ticket + 1), 1u);
+    for (int j = tid; j < NA; j += PWA_TMA_THREADS) partials[(long long)blockIdx.x * NA + j] = 0.0;
+    __threadfence();
+    __syncthreads();
+    if (!flat_sum(partials, ticket, NA, out, scratch, &s_last)) return;
+    publish_result(ticket, NA, out, seq);
+    return;
+  }
   if (tid == 0) {
     s_err = 0;
     for (int st = 0; st < stages; ++st) {

@@ -140,6 +140,9 @@ int set_err(pwa_plan* h, int code, const std::string& msg) {
 
 // ticket words of the cached kernels: 2 + the most reduction groups (4096)
 constexpr int kTicketWords = 2 + 4096;
+// consumer groups of pwa_eval_cached_tma (PWA_TMA_GROUPS): its ring depth
+// must be a multiple of this
+constexpr int kTmaGroups = 2;
 
 int ensure_partials(pwa_plan* h, long long n) {
   if (n <= h->partials_cap) return PWA_OK;
@@ -803,6 +806,7 @@ int pwa_cache_data(pwa_plan* h, const double* consts, void* stream) {
     const size_t stage = (size_t)tile * (h->nf * sizeof(float2) + sizeof(double));
     long long st = ((long long)optin - (long long)a.sharedSizeBytes - 1024) / (long long)stage;
     if (st > 8) st = 8;  // PWA_TMA_MAXST
+    st -= st % kTmaGroups;  // a multiple of the consumer groups (see the kernel)
     h->tma_stages = (int)st;
     h->tma_stages_max = (int)st;
     h->tma_stage_bytes = stage;
@@ -962,7 +966,7 @@ int pwa_fma_peak(pwa_plan* h, int precision, long long iters, void* stream, doub
 // blocks per SM of variant 2) applied to the plan.
 static void apply_cached_config(pwa_plan* h, int variant, int stages, int bps) {
   h->cached_variant = variant;
-  if (variant == 5 && stages >= 2 && stages <= h->tma_stages_max) {
+  if (variant == 5 && stages >= 2 && stages <= h->tma_stages_max && stages % kTmaGroups == 0) {
     h->tma_stages = stages;
     h->cached_smem_tma = (size_t)stages * h->tma_stage_bytes;
   }
@@ -988,7 +992,8 @@ int pwa_autotune_cached(pwa_plan* h, const double* ck, int reps, void* stream, i
   cands.push_back({1, 0, 0});
   cands.push_back({4, 0, 0});
   if (h->cached_blocks_tma > 0)
-    for (int st = 3; st <= h->tma_stages_max; ++st) cands.push_back({5, st, 0});
+    for (int st = 2 * kTmaGroups; st <= h->tma_stages_max; st += kTmaGroups)
+      cands.push_back({5, st, 0});
   cands.push_back({0, 0, 0});
   cands.push_back({3, 0, 0});
   if ((int)cands.size() > 32) cands.resize(32);
@@ -1052,8 +1057,10 @@ int pwa_set_cached_config(pwa_plan* h, int variant, int stages, int bps) {
   if (!h) return PWA_ERR_ARG;
   if (variant < -1 || variant > 5 || stages < 0 || bps < 0)
     return set_err(h, PWA_ERR_ARG, "invalid cached-kernel configuration");
-  if (variant == 5 && stages && (stages < 2 || stages > h->tma_stages_max))
-    return set_err(h, PWA_ERR_ARG, "ring depth outside 2 .. the shared-memory limit");
+  if (variant == 5 && stages &&
+      (stages < 2 || stages > h->tma_stages_max || stages % kTmaGroups))
+    return set_err(h, PWA_ERR_ARG,
+                   "ring depth must be an even number from 2 to the shared-memory limit");
   apply_cached_config(h, variant, stages, bps);
   return PWA_OK;
 }
