@@ -312,10 +312,10 @@ L2_BYTES = 126e6
 
 class Timer:
     """k timed steps, device time from CUDA events on the launching
-    (current) stream, max over ranks.  With ``flush`` set, a 256 MB buffer
-    is written before every step (L2 is 126 MB); workloads whose inputs per
-    launch exceed twice the L2 run without it (their inputs do not fit in
-    L2, so no step finds the previous step's data there)."""
+    (current) stream, max over ranks.  With ``do_flush`` set, a 256 MB
+    buffer is written before every step (L2 is 126 MB); workloads whose
+    every kernel streams more than the L2 holds per launch run without it
+    (inputs larger than L2: a step finds none of its inputs there)."""
 
     def __init__(self, dist):
         import torch
@@ -415,7 +415,7 @@ def measure_cached(name, args, rank, world, dist, timed, log, n_sig, n_bg, n_mc,
     n_data = n_sig + n_bg
     bytes_mixed = n_data * (8 * code.nf + 8)
     bytes_f32 = (n_data + n_mc) * (8 * len(code.mass_fields) + 4 * len(code.angle_fields) + 8)
-    timed.do_flush = min(bytes_mixed, bytes_f32) < 2 * L2_BYTES
+    timed.do_flush = min(bytes_mixed, bytes_f32) <= L2_BYTES
     l2_note = ("256 MB buffer written before every timed step (L2 126 MB)" if timed.do_flush
                else f"inputs larger than L2: {bytes_mixed / 1e6:.0f} MB per launch of the "
                     f"cached kernel, {bytes_f32 / 1e6:.0f} MB of the FP32 kernel (L2 126 MB); "

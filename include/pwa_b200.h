@@ -150,8 +150,9 @@ int pwa_build_gram(pwa_plan* h, const double* consts, void* stream, double* out)
  * builds the same matrix with a TF einsum): 0 = FP64 on the CUDA cores,
  * 1 = tensor cores (tcgen05 int8 MMAs on seven exact slices of every value,
  * exact int32 accumulation, FP64 recombination; models with at most 32
- * columns, others use 0), -1 = automatic (1 where it applies).  The error
- * flag of the tensor-core kernel turns into PWA_ERR_CUDA. */
+ * columns, others use 0), -1 = automatic (0: at the shipped models' column
+ * counts the slicing costs more than the FP64 products it replaces).  The
+ * error flag of the tensor-core kernel turns into PWA_ERR_CUDA. */
 int pwa_set_gram_method(pwa_plan* h, int method);
 
 /* ---- fixed masses/widths: cached partial-wave columns -------------------

@@ -48,6 +48,22 @@ def _lit(v):
     return f"R({r})"
 
 
+def _f32_exact(v):
+    """True when v is a float exactly representable in FP32."""
+    import struct
+
+    v = float(v)
+    return struct.unpack("f", struct.pack("f", v))[0] == v
+
+
+def _klit(v, x):
+    """Literal v times expression x: a plain product when v is exact in
+    FP32, else mulk (FP32 hi + lo parts of v in the FP32 kernels)."""
+    if _f32_exact(v):
+        return f"{_lit(v)} * {x}"
+    return f"mulk<R>({x}, {repr(float(v))})"
+
+
 def _key(t):
     return [float(x) for x in t]
 
@@ -259,6 +275,11 @@ class ModelCode:
     def _cst(self, name):
         return f"R(C.v[{self.consts.index[name]}])"
 
+    def _cv(self, name):
+        """The FP64 constant itself (for mulk / cfmak / cmulk, which keep
+        its FP32 rounding from biasing every event alike)."""
+        return f"C.v[{self.consts.index[name]}]"
+
     def _cpx(self, base):
         return f"cmk<R>({self._cst(base + '.re')}, {self._cst(base + '.im')})"
 
@@ -277,6 +298,19 @@ class ModelCode:
         if isinstance(v, tuple):
             return f"(cc ? {_lit(v[1])} : {_lit(v[0])})"
         return _lit(v)
+
+    @staticmethod
+    def _kcoef(v, bfv):
+        """Coefficient v (or a charge-select pair) times the barrier factor
+        expression ``bfv`` ("bf * " or empty), hi/lo-split in FP32."""
+        x = bfv[:-3] if bfv else "R(1)"
+        if isinstance(v, tuple):
+            if _f32_exact(v[0]) and _f32_exact(v[1]):
+                return f"{x} * (cc ? {_lit(v[1])} : {_lit(v[0])})"
+            return f"mulk<R>({x}, cc ? {repr(float(v[1]))} : {repr(float(v[0]))})"
+        if _f32_exact(v):
+            return f"{x} * {_lit(v)}"
+        return f"mulk<R>({x}, {repr(float(v))})"
 
     def _cf(self, ci):
         """Field references of chain ci in the current pass."""
@@ -387,13 +421,13 @@ class ModelCode:
                         poly = _lit(co[0])
                         for cc_ in co[1:]:
                             poly = f"fma({poly}, {z}, {_lit(cc_)})"
-                        e(f"  R bp_{tag}_{l} = {cst(f'{d}.Pz0_{l}')} / ({poly});")
+                        e(f"  R bp_{tag}_{l} = mulk<R>(R(1) / ({poly}), {self._cv(f'{d}.Pz0_{l}')});")
                         e(f"  bp_{tag}_{l} = bp_{tag}_{l} > R(0) ? bp_{tag}_{l} : R(1);")
                         bf = f"({ql}) * psqrt(bp_{tag}_{l})"
                     else:
                         bf = ql
                     if d.barrier_factor_norm:
-                        bf = f"({bf}) * {cst(f'{d}.norm_{l}')}"
+                        bf = f"mulk<R>({bf}, {self._cv(f'{d}.norm_{l}')})"
                     e(f"  const R bf_{tag}_{l} = {bf};")
             # D*^{Ja}_{la, lb-lc}(alpha, beta, 0); indices are 2m + 2J
             j2 = two(a.J)
@@ -415,7 +449,7 @@ class ModelCode:
             w = small_d_weight(j2)
             for i1, i2 in sorted(need):
                 k1, k2 = i1 // 2, i2 // 2
-                terms = [f"{_lit(w[l][k1][k2])} * sp_{tag}[{l}] * cp_{tag}[{j2 - l}]"
+                terms = [_klit(w[l][k1][k2], f"(sp_{tag}[{l}] * cp_{tag}[{j2 - l}])")
                          for l in range(j2 + 1) if w[l][k1][k2] != 0]
                 dexpr = " + ".join(terms) if terms else "R(0)"
                 nm = self._d_name(ci, vi, i1, i2)
@@ -439,7 +473,7 @@ class ModelCode:
             for l1 in o.spins:
                 for l2 in o.spins:
                     n1, n2 = two(l1) + j2, two(l2) + j2
-                    terms = [f"{_lit(w[l][n1 // 2][n2 // 2])} * sp_{tag}[{l}] * cp_{tag}[{j2 - l}]"
+                    terms = [_klit(w[l][n1 // 2][n2 // 2], f"(sp_{tag}[{l}] * cp_{tag}[{j2 - l}])")
                              for l in range(j2 + 1) if w[l][n1 // 2][n2 // 2] != 0]
                     dexpr = " + ".join(terms) if terms else "R(0)"
                     e(f"  const cpx<R> Dal_{tag}_{n1}_{n2} = cscale(cmul(ea_{tag}[{n1}], eg_{tag}[{n2}]), {dexpr});")
@@ -465,11 +499,11 @@ class ModelCode:
                 poly = _lit(co[0])
                 for cc_ in co[1:]:
                     poly = f"fma({poly}, {z}, {_lit(cc_)})"
-                e(f"  const R rr_{tag} = qq_{tag} * {cst(f'{p}.iq02')};")
+                e(f"  const R rr_{tag} = mulk<R>(qq_{tag}, {self._cv(f'{p}.iq02')});")
                 ph = f"psqrt(rr_{tag} < R(0) ? -rr_{tag} : rr_{tag})"
                 for _ in range(L_):
                     ph = f"{ph} * rr_{tag}"
-                e(f"  const R ya_{tag} = {cst(f'{p}.K')} * ({ph}) / (R({m}) * ({poly}));")
+                e(f"  const R ya_{tag} = mulk<R>(({ph}) / (R({m}) * ({poly})), {self._cv(f'{p}.K')});")
                 e(f"  const R y_{tag} = rr_{tag} < R(0) ? R(0) : ya_{tag};")
                 e(f"  const R yi_{tag} = rr_{tag} < R(0) ? ya_{tag} : R(0);")
                 e(f"  const R dre_{tag} = xr_{tag} + yi_{tag};")
@@ -488,14 +522,21 @@ class ModelCode:
                         poly = f"fma({poly}, {z}, {_lit(cc_)})"
                     qp = "*".join([f"q_{tag}"] * (2 * L_ + 1))
                     e(f"  const R qp_{tag} = {cst(f'{p}.useq')} != R(0) ? ({qp}) : R(1);")
-                    e(f"  const R y_{tag} = {cst(f'{p}.K')} * qp_{tag} / (R({m}) * ({poly}));")
+                    e(f"  const R y_{tag} = mulk<R>(qp_{tag} / (R({m}) * ({poly})), {self._cv(f'{p}.K')});")
+                    e(f"  const R s_{tag} = xr_{tag} * xr_{tag} + y_{tag} * y_{tag};")
+                    e(f"  const cpx<R> bw_{tag} = cmk<R>(xr_{tag} / s_{tag}, y_{tag} / s_{tag});")
                 else:
+                    # constant width: value from the FP64 m0^2 - m^2 and m0 Gamma0
                     e(f"  const R y_{tag} = {cst(f'{p}.y')};")
-                e(f"  const R s_{tag} = xr_{tag} * xr_{tag} + y_{tag} * y_{tag};")
-                e(f"  const cpx<R> bw_{tag} = cmk<R>(xr_{tag} / s_{tag}, y_{tag} / s_{tag});")
+                    e(f"  cpx<R> bw_{tag};")
+                    e(f"  {{ const double xd = {self._cv(f'{p}.m0sq')} - {m} * {m}, "
+                      f"yd = {self._cv(f'{p}.y')}, sd = xd * xd + yd * yd;")
+                    e(f"    bw_{tag} = cmk<R>(R(xd / sd), R(yd / sd)); }}")
             if p.width_norm_applies():
                 # the chain product takes Gamma0 R (the derivatives use R)
-                bw_names[-1] = f"cscale(bw_{tag}, {cst(f'{p}.wn')})"
+                wn = self._cv(f'{p}.wn')
+                bw_names[-1] = (f"cmk<R>(mulk<R>(bw_{tag}.re, {wn}), "
+                                f"mulk<R>(bw_{tag}.im, {wn}))")
         if bw_names:
             e(f"  cpx<R> BW_c{ci} = {bw_names[0]};")
             for nm in bw_names[1:]:
@@ -562,7 +603,9 @@ class ModelCode:
                         for i, cgv in terms:
                             l = ls[i][0]
                             bfv = f"bf_c{ci}v{vi}_{l} * " if d.has_barrier_factor else ""
-                            e(f"  cfma({nm}, {bfv}{self._coef(cgv)}, {self._cpx(f'{d}.g{i}')});")
+                            g = f"{d}.g{i}"
+                            e(f"  cfmak({nm}, {self._kcoef(cgv, bfv)}, {self._cv(g + '.re')}, "
+                              f"{self._cv(g + '.im')});")
             pre = {}
             for facs, po, coefs in self.chain_assign[ci]:
                 if any((vi, ib, ic) not in hnames for (vi, _, _, ib, ic) in facs):
@@ -582,13 +625,14 @@ class ModelCode:
                         prod = f"cmul({prod}, {v})"
                     e(f"  cfmac({nm}, {prod}, {vs[-1]});")
             cur = self._emit_align_forward(e, ci, pre, "Aa")
-            tot = self._cpx(f"t{ci}")
+            tre, tim = self._cv(f"t{ci}.re"), self._cv(f"t{ci}.im")
             if ci in self.cp_chains and self.ncp:
-                tot = f"(cc ? {self._cpx(f't{ci}m')} : {tot})"
+                tre = f"(cc ? {self._cv(f't{ci}m.re')} : {tre})"
+                tim = f"(cc ? {self._cv(f't{ci}m.im')} : {tim})"
             if self._factor() == 1.0:
-                e(f"  const cpx<R> E_c{ci} = cmul({tot}, BW_c{ci});")
+                e(f"  const cpx<R> E_c{ci} = cmulk<R>({tre}, {tim}, BW_c{ci});")
             else:
-                e(f"  const cpx<R> E_c{ci} = cscale(cmul({tot}, BW_c{ci}), "
+                e(f"  const cpx<R> E_c{ci} = cscale(cmulk<R>({tre}, {tim}, BW_c{ci}), "
                   f"{_lit(self._factor())});")
             for o, nm in cur.items():
                 e(f"  cfmac(A{self._out(o)}, E_c{ci}, {nm});")

@@ -65,6 +65,45 @@ __device__ __forceinline__ R cabs2(cpx<R> a) {
 }
 
 // ------------------------------------------------------ precision helpers
+// Products with FP64 constants (couplings, CG and Wigner-d coefficients,
+// barrier and lineshape normalisations).  In the FP32 kernels the constant
+// is split into FP32 hi + lo parts, so its rounding to FP32 -- the same for
+// every event, which would shift the NLL like a parameter change -- leaves
+// only per-event rounding of the product.  In FP64 they are plain products.
+template <typename R>
+__device__ __forceinline__ R mulk(R x, double c) {
+  if constexpr (sizeof(R) == 4) {
+    const float hi = (float)c;
+    return fmaf(x, hi, x * (float)(c - (double)hi));
+  } else {
+    return x * c;
+  }
+}
+// acc += s * (re + i im)
+template <typename R>
+__device__ __forceinline__ void cfmak(cpx<R>& acc, R s, double re, double im) {
+  if constexpr (sizeof(R) == 4) {
+    const float rh = (float)re, ih = (float)im;
+    acc.re = fmaf(s, rh, fmaf(s, (float)(re - (double)rh), acc.re));
+    acc.im = fmaf(s, ih, fmaf(s, (float)(im - (double)ih), acc.im));
+  } else {
+    acc.re = fma(s, re, acc.re);
+    acc.im = fma(s, im, acc.im);
+  }
+}
+// (re + i im) * z
+template <typename R>
+__device__ __forceinline__ cpx<R> cmulk(double re, double im, cpx<R> z) {
+  if constexpr (sizeof(R) == 4) {
+    const float rh = (float)re, ih = (float)im;
+    const float rl = (float)(re - (double)rh), il = (float)(im - (double)ih);
+    const cpx<float> a = cmul(cmk<float>(rh, ih), z), b = cmul(cmk<float>(rl, il), z);
+    return cmk<float>(a.re + b.re, a.im + b.im);
+  } else {
+    return cmul(cmk<double>(re, im), z);
+  }
+}
+
 __device__ __forceinline__ void psincos(double x, double* s, double* c) { sincos(x, s, c); }
 __device__ __forceinline__ void psincos(float x, float* s, float* c) { sincosf(x, s, c); }
 __device__ __forceinline__ double psqrt(double x) { return sqrt(x); }

@@ -307,35 +307,45 @@ __device__ __forceinline__ int oz_exponent(double mx) {
   return m * 128.0 <= 127.0 ? e : e + 1;
 }
 
-// int8 slices of x 2^-e packed four rows at a time: word[s] byte j = slice
-// s of value j
-__device__ __forceinline__ void oz_slices4(const double (&x)[4], int e, unsigned (&word)[PWA_OZ_S]) {
+// int8 slices of 16 consecutive rows of one column, x 2^-e: word[s][q]
+// byte j = slice s of value 4 q + j (16 bytes per slice: one core-matrix
+// row of a K-major operand)
+__device__ __forceinline__ void oz_slices16(const double (&x)[16], int e,
+                                            unsigned (&word)[PWA_OZ_S][4]) {
 #pragma unroll
-  for (int s = 0; s < PWA_OZ_S; ++s) word[s] = 0u;
+  for (int s = 0; s < PWA_OZ_S; ++s)
 #pragma unroll
-  for (int j = 0; j < 4; ++j) {
+    for (int q = 0; q < 4; ++q) word[s][q] = 0u;
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
     double v = ldexp(x[j], 7 - e);  // first slice's scale: |v| < 127
 #pragma unroll
     for (int s = 0; s < PWA_OZ_S; ++s) {
       const double a = rint(v);
-      word[s] |= ((unsigned)(int)a & 0xFFu) << (8 * j);
+      word[s][j >> 2] |= ((unsigned)(int)a & 0xFFu) << (8 * (j & 3));
       v = (v - a) * 128.0;  // exact: the fraction of v, then 7 more bits
     }
   }
 }
 
-// One block per SM, PWA_TPB threads; dynamic shared memory: two stages of
-// PWA_OZ_STAGE bytes (1024-aligned).  Block b takes a contiguous run of the
-// rows; it writes partial[b][c][d] (KC x KC FP64) for an ordered sum.
-// e8[2 KC]: column maxima (pwa_gram_colmax) as FP64 bits.  err[0] is set
-// when a wait on the tensor cores gives up.
-extern "C" __global__ void __launch_bounds__(PWA_TPB, 1)
+// One block of PWA_OZ_THREADS threads per SM; dynamic shared memory: two
+// stages of PWA_OZ_STAGE bytes (1024-aligned) and the FP64 accumulators.
+// Block b takes a contiguous run of the rows; it writes partial[b][c][d]
+// (KC x KC FP64) for an ordered sum.  e8[2 KC]: column maxima
+// (pwa_gram_colmax) as FP64 bits.  err[0] is set when a wait on the tensor
+// cores gives up.  The stage fill gives each thread 16 rows of one column
+// (FP64 loads, exact slicing, one 16-byte store per slice); thread 0 issues
+// the MMAs of a filled stage while the others fill the next one.
+#define PWA_OZ_THREADS 512
+#define PWA_OZ_ACCLD (PWA_OZ_CP + 1)  // padded row of the shared accumulators
+extern "C" __global__ void __launch_bounds__(PWA_OZ_THREADS, 1)
     pwa_gram_tc(const double* __restrict__ F, const double* __restrict__ W, long long n,
                 const unsigned long long* __restrict__ e8, double* __restrict__ partial,
                 unsigned int* __restrict__ err) {
 #if PWA_OZ_OK
   constexpr int KC = PWA_OZ_KC, CP = PWA_OZ_CP, S = PWA_OZ_S, KB = PWA_OZ_KB;
-  constexpr int NO = PWA_NOUT, NQ = KB / 4;  // four-row groups per stage
+  constexpr int NO = PWA_NOUT, NK16 = KB / 16;  // 16-row groups per stage
+  constexpr int NT = PWA_OZ_THREADS;
   constexpr unsigned IDESC = umma_idesc_s8(128, CP);
   extern __shared__ __align__(1024) unsigned char oz_smem[];
   __shared__ __align__(8) unsigned long long done[2];
@@ -344,9 +354,12 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, 1)
   __shared__ int s_err;
   const int tid = threadIdx.x, warp = tid >> 5;
   unsigned char* base = (unsigned char*)(((size_t)oz_smem + 1023) & ~(size_t)1023);
-  // zero both stages (A rows >= KC stay zero), exponents, barriers, TMEM
-  for (int j = tid; j < 2 * PWA_OZ_STAGE / 4; j += PWA_TPB) ((unsigned*)base)[j] = 0u;
-  for (int c = tid; c < 2 * KC; c += PWA_TPB) s_e[c] = oz_exponent(__longlong_as_double((long long)e8[c]));
+  double* s_acc = (double*)(base + 2 * PWA_OZ_STAGE);  // [KC][PWA_OZ_ACCLD]
+  // zero both stages (A rows >= KC stay zero), accumulators, exponents,
+  // barriers, TMEM
+  for (int j = tid; j < 2 * PWA_OZ_STAGE / 4; j += NT) ((unsigned*)base)[j] = 0u;
+  for (int j = tid; j < KC * PWA_OZ_ACCLD; j += NT) s_acc[j] = 0.0;
+  for (int c = tid; c < 2 * KC; c += NT) s_e[c] = oz_exponent(__longlong_as_double((long long)e8[c]));
   if (tid == 0) {
     s_err = 0;
     mbar_init(&done[0], 1);
@@ -362,9 +375,6 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, 1)
   const long long R = n * NO;
   const long long r0 = (long long)blockIdx.x * R / gridDim.x;
   const long long r1 = (long long)(blockIdx.x + 1) * R / gridDim.x;
-  double acc[CP];
-#pragma unroll
-  for (int d = 0; d < CP; ++d) acc[d] = 0.0;
   int uses[2] = {0, 0};
   bool fresh = true;  // next MMA of each accumulator starts it from zero
   int stage = 0;
@@ -373,14 +383,15 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, 1)
     const bool have = rb < r1;
     const bool flush = !have || since_flush + KB > PWA_OZ_FLUSH;
     if (flush && since_flush > 0) {
-      // wait for every MMA issued so far, then move the accumulators to FP64
+      // wait for every MMA issued so far, then add the accumulators to FP64
       for (int st = 0; st < 2; ++st)
         if (uses[st] && !mbar_wait(&done[st], (unsigned)((uses[st] - 1) & 1), PWA_WAIT_LIMIT))
           s_err = 1;
       tc_fence_after();
       __syncwarp();  // tcgen05.ld is warp-collective: reconverge first
       if (warp < 2) {  // TMEM lanes 0..63 = rows c of the accumulators
-#pragma unroll
+        const int c = tid;
+#pragma unroll 1
         for (int g = 0; g < S; ++g) {
           const double sc = ldexp(1.0, -7 * (g + 2));
 #pragma unroll
@@ -388,8 +399,13 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, 1)
             int v[16];
             tmem_ld16(tmem + ((unsigned)(warp * 32) << 16) + (unsigned)(g * CP + 16 * q), v);
             tmem_wait_ld();
+            if (c < KC) {
 #pragma unroll
-            for (int j = 0; j < 16; ++j) acc[16 * q + j] = fma((double)v[j], sc, acc[16 * q + j]);
+              for (int j = 0; j < 16; ++j) {
+                double* a = s_acc + c * PWA_OZ_ACCLD + 16 * q + j;
+                *a = fma((double)v[j], sc, *a);
+              }
+            }
           }
         }
       }
@@ -406,34 +422,34 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, 1)
       s_err = 1;
     unsigned char* A = base + (size_t)stage * PWA_OZ_STAGE;
     unsigned char* B = A + (size_t)S * PWA_OZ_ABYTES;
-    for (int item = tid; item < 2 * KC * NQ; item += PWA_TPB) {
-      const bool isb = item >= KC * NQ;
-      const int it = isb ? item - KC * NQ : item;
-      const int c = it / NQ, kq = it % NQ;
+    for (int item = tid; item < 2 * KC * NK16; item += NT) {
+      const bool isb = item >= KC * NK16;
+      const int it = isb ? item - KC * NK16 : item;
+      const int c = it % KC, k16 = it / KC;
       const int k = c % PWA_NCOL, im = c / PWA_NCOL;
-      double x[4];
+      double x[16];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const long long r = rb + 4 * kq + j;
+      for (int j = 0; j < 16; ++j) {
+        const long long r = rb + 16 * k16 + j;
         x[j] = 0.0;
         if (r < r1) {
           const long long i = r / NO;
           const int o = (int)(r - i * NO);
-          x[j] = F[i * (2LL * PWA_NCOL * NO) + 2 * (k * NO + o) + im];
-          if (isb) x[j] *= W[i];
+          x[j] = __ldg(F + i * (2LL * PWA_NCOL * NO) + 2 * (k * NO + o) + im);
+          if (isb) x[j] *= __ldg(W + i);
         }
       }
-      unsigned word[S];
-      oz_slices4(x, s_e[(isb ? KC : 0) + c], word);
+      unsigned word[S][4];
+      oz_slices16(x, s_e[(isb ? KC : 0) + c], word);
       // K-major core-matrix layout: byte (row m, k) = (k/16)*(M/8*128) +
       // (m/8)*128 + (m%8)*16 + k%16 with M = 128 (A) or CP (B)
-      const int kk = 4 * kq;
       const int mrows = isb ? CP : 128;
-      const int off = (kk / 16) * (mrows / 8 * 128) + (c / 8) * 128 + (c % 8) * 16 + (kk % 16);
+      const int off = k16 * (mrows / 8 * 128) + (c / 8) * 128 + (c % 8) * 16;
       unsigned char* dst = isb ? B : A;
       const int sbytes = isb ? PWA_OZ_BBYTES : PWA_OZ_ABYTES;
 #pragma unroll
-      for (int s = 0; s < S; ++s) *(unsigned*)(dst + s * sbytes + off) = word[s];
+      for (int s = 0; s < S; ++s)
+        *(uint4*)(dst + s * sbytes + off) = make_uint4(word[s][0], word[s][1], word[s][2], word[s][3]);
     }
     fence_proxy_async_smem();
     tc_fence_before();
@@ -477,12 +493,10 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, 1)
   tc_fence_after();
   __syncwarp();
   if (warp == 0) tmem_dealloc(tmem, PWA_OZ_TCOLS);
-  const int c = tid;
-  if (c < KC) {
-    const int ea = s_e[c];
-#pragma unroll
-    for (int d = 0; d < CP; ++d)
-      if (d < KC) partial[(long long)blockIdx.x * KC * KC + c * KC + d] = ldexp(acc[d], ea + s_e[KC + d]);
+  for (int j = tid; j < KC * KC; j += NT) {
+    const int c = j / KC, d = j % KC;
+    partial[(long long)blockIdx.x * KC * KC + j] =
+        ldexp(s_acc[c * PWA_OZ_ACCLD + d], s_e[c] + s_e[KC + d]);
   }
 #endif
 }

@@ -89,7 +89,7 @@ struct pwa_plan {
   double seq = 0.0;
   std::vector<double> gram;  // MC Gram matrix, (re, im) row-major ncol x ncol
   bool gram_valid = false;
-  int gram_method = -1;  // 0 FP64 CUDA cores, 1 tensor cores, -1 automatic
+  int gram_method = -1;  // 0 FP64 CUDA cores, 1 tensor cores, -1 automatic (0)
   // pool of column-cache tiles shared by many fits (serving)
   float2* pool_f = nullptr;
   double* pool_w = nullptr;
@@ -609,13 +609,14 @@ int gram_tc_chunk(pwa_plan* h, double* F, double* wptr, long long cnt, double* g
   int rc = launch(h, h->k.gram_colmax, dim3((int)nb), dim3(h->tpb), a1, s);
   if (rc) return rc;
   // two stages of seven A slices (128 x 64 bytes) and seven B slices
-  // (CP x 64 bytes), plus 1 KB for the 1024-byte alignment of the base
-  const size_t smem = 2 * (size_t)7 * (128 * 64 + CP * 64) + 1024;
+  // (CP x 64 bytes), 1 KB for the 1024-byte alignment of the base, and the
+  // FP64 accumulators (KC rows of CP + 1)
+  const size_t smem = 2 * (size_t)7 * (128 * 64 + CP * 64) + 1024 + sizeof(double) * KC * (CP + 1);
   CU(cudaFuncSetAttribute((const void*)h->k.gram_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)smem));
   const int gb = h->sms;
   void* a2[] = {&F, &wptr, &cnt, &mx, &gpart, &err};
-  cudaError_t e = cudaLaunchKernel((const void*)h->k.gram_tc, dim3(gb), dim3(h->tpb), a2, smem, s);
+  cudaError_t e = cudaLaunchKernel((const void*)h->k.gram_tc, dim3(gb), dim3(512), a2, smem, s);
   if (e != cudaSuccess)
     return set_err(h, PWA_ERR_CUDA, std::string("gram kernel launch: ") + cudaGetErrorString(e));
   int nrows = gb, ncols = KC * KC;
@@ -653,7 +654,7 @@ int pwa_build_gram(pwa_plan* h, const double* consts, void* stream, double* out)
   if (!h->w || h->n_mc <= 0) return set_err(h, PWA_ERR_STATE, "no MC events uploaded");
   if (!consts) return set_err(h, PWA_ERR_ARG, "invalid gram arguments");
   cudaStream_t s = (cudaStream_t)stream;
-  const bool tc = h->gram_method != 0 && 2 * h->ncol <= 64;
+  const bool tc = h->gram_method == 1 && 2 * h->ncol <= 64;
   std::vector<double> cbuf(consts, consts + h->nconst);
   const long long row = 2LL * h->ncol * h->nout;
   // chunked: columns of at most `chunk` events at a time
