@@ -181,8 +181,10 @@ int pwa_set_cached_variant(pwa_plan* h, int variant);
  * 2 at each block count per SM the occupancy allows, variants 1 and 4,
  * variant 5 at every even ring depth from 4 stages to the shared-memory
  * limit (its two consumer groups need an even depth),
- * variants 0 and 3 -- with CUDA events over `reps` back-to-back launches
- * on the plan's column cache and couplings ck, keeps the fastest.
+ * variants 0 and 3 -- with CUDA events around each of `reps` launches on
+ * the plan's column cache and couplings ck, every launch after a write of
+ * a 256 MB buffer (L2 flushed; the buffer is allocated for the call and
+ * freed), and keeps the fastest.
  * out[i] = mean microseconds per launch of configuration i (at most 32),
  * *n_cand their count.  pwa_cached_config reads the configuration in use
  * (variant, ring depth, blocks per SM of variant 2); pwa_set_cached_config
