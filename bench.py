@@ -442,6 +442,16 @@ def measure_cached(name, args, rank, world, dist, timed, log, n_sig, n_bg, n_mc,
     ck = np.stack([eng._ck.real, eng._ck.imag], 1).reshape(-1)
     k_kernel = args.steps
     t_kernel = timed(lambda: eng.eval_cached_enqueue(ck), k_kernel)
+    # the same number of bytes read by a library reduction (torch.sum of an
+    # FP32 tensor), same L2 protocol: what one plain pass over that many bytes
+    # costs on this GPU, fixed per-launch part included
+    floor_buf = torch.ones(bytes_mixed // 4, dtype=torch.float32, device="cuda")
+    t_floor = timed(lambda: floor_buf.sum(), k_kernel)
+    del floor_buf
+    # Hessian of all trainable parameters: the 4P stencil points of the
+    # differenced adjoint gradient in one multi-point pass over the cache
+    k_hess = 3
+    t_hess = timed(lambda: eng.hessian_cached(var_vec, 1e-2), k_hess)
     Cp = eng_p.consts(vals)
     t_kernel_p = timed(lambda: eng_p.eval_enqueue(Cp, PLAIN_F64, mc=True), k_kernel)
     # the FP32-amplitude recompute form (what a fit with floating masses and
@@ -509,6 +519,10 @@ def measure_cached(name, args, rank, world, dist, timed, log, n_sig, n_bg, n_mc,
                                "reduction",
                      "algorithmic_bytes_per_launch": bytes_mixed,
                      "launch_us": 1e6 * t_kernel / k_kernel,
+                     "read_floor": {
+                         "what": "torch.sum over the same number of bytes, same L2 protocol",
+                         "launch_us": 1e6 * t_floor / k_kernel,
+                         "kernel_over_floor": t_kernel / t_floor},
                      "plain_f64_kernel": {
                          "bound": "fp64", "achieved": ach_p, "peak": peaks["f64_tflops"],
                          "unit": "TFLOP/s", "frac": ach_p / peaks["f64_tflops"],
@@ -523,8 +537,14 @@ def measure_cached(name, args, rank, world, dist, timed, log, n_sig, n_bg, n_mc,
                      "table_us": None if fcn.tune is None or fcn.tune[0] is None
                      else [round(float(x), 2) for x in fcn.tune[0]],
                      "error": fcn.tune[2] if fcn.tune is not None and len(fcn.tune) > 2
-                     else None},
+                     else None,
+                     "pinned": os.environ.get("PWA_CACHED_CONFIG")},
         "cached_variants": var_table,
+        "hessian": {"ms": 1e3 * t_hess / k_hess, "n_params": len(names),
+                    "stencil_points": 4 * len(names),
+                    "in_single_steps": (t_hess / k_hess) / (t_mixed / args.steps),
+                    "call": "pwa_hessian_cached: one evaluation + the 4P stencil points "
+                            "in one multi-point pass over the column cache"},
         "check": {"nll_mixed": nll_m, "nll_plain": nll_p, "dnll": nll_m - nll_p,
                   "grad_max_rel": float(np.max(np.abs(g_m - g_p)) / np.max(np.abs(g_p)))},
         "setup_s": {"dataset": t_data, "mixed_fcn": t_mixed_setup},

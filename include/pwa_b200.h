@@ -22,7 +22,7 @@
  *   pwa_hessian_cached Hessian (differenced adjoint)   tf_pwa/model/model.py:513-561
  *   pwa_read_dat       text momentum files             tf_pwa/data.py:300-365
  *   pwa_server_*       many fits, each a BFGS driver   tf_pwa/fit.py:189-419 (one per fit)
- *   pwa_compile_only / pwa_last_error / pwa_plan_info / pwa_plan_destroy
+ *   pwa_compile_only / pwa_precompile / pwa_last_error / pwa_plan_info / pwa_plan_destroy
  *                      build check and bookkeeping (no reference counterpart)
  *
  * Conventions: plain pointers and sizes only; every call returns 0 on success
@@ -73,6 +73,14 @@ int pwa_plan_destroy(pwa_plan* h);
  * by the build step to check generated models on a machine without a GPU. */
 int pwa_compile_only(const char* src, size_t src_len, int tpb, const char* arch, char* log_buf,
                      size_t log_len);
+
+/* Compile the model module for `arch` without a device and store the cubin
+ * in the on-disk cache (PWA_CUBIN_CACHE=<dir>), where pwa_plan_create on a
+ * device of that architecture finds it instead of compiling: ahead-of-time
+ * builds of known models.  PWA_ERR_STATE when the variable is not set;
+ * NVRTC errors as PWA_ERR_COMPILE with the log in log_buf. */
+int pwa_precompile(const char* src, size_t src_len, int tpb, const char* arch, char* log_buf,
+                   size_t log_len);
 
 /* Events: xm[n_mass][n_data+n_mc], xa[n_angle][n_data+n_mc], w[n_data+n_mc]
  * (row-major; data rows first, then MC).  Data weights are the final

@@ -199,8 +199,14 @@ class FCN:
             self._var_names = list(self.vm.variables.keys())
             self.eng.set_param_layout(self._var_names, self.vm.trainable_vars)
             # pick the fastest configuration of the cached data-term kernel
-            # for this model and event count (PWA_AUTOTUNE=0: keep the default)
-            if os.environ.get("PWA_AUTOTUNE", "1") != "0":
+            # for this model and event count (PWA_AUTOTUNE=0: keep the default;
+            # PWA_CACHED_CONFIG="variant,ring_depth,blocks_per_sm": pin one)
+            pin = os.environ.get("PWA_CACHED_CONFIG")
+            if pin:
+                parts = [int(v) for v in pin.split(",")]
+                self.eng.set_cached_config(*(parts + [0, 0])[:3])
+                self.tune = (None, self.eng.cached_config(), None)
+            elif os.environ.get("PWA_AUTOTUNE", "1") != "0":
                 self.eng.consts(vals)
                 try:
                     self.tune = self.eng.autotune_cached()

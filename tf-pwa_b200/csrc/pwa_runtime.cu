@@ -54,7 +54,8 @@ struct pwa_plan {
   int regs[2] = {0, 0};
   long long local_bytes[2] = {0, 0};
   int device = 0, sms = 0;
-  int nblocks = 0, blocks_data = 0;
+  int nblocks = 0, blocks_data = 0;  // grid of pwa_eval_f64 (all / data blocks)
+  int nblocks32 = 0, blocks_data32 = 0;  // grid of pwa_eval_f32
   // events
   double* xm = nullptr;
   double* xa = nullptr;
@@ -309,6 +310,23 @@ int pwa_compile_only(const char* src, size_t src_len, int tpb, const char* arch,
   return rc;
 }
 
+int pwa_precompile(const char* src, size_t src_len, int tpb, const char* arch, char* log_buf,
+                   size_t log_len) {
+  if (!src || !arch || tpb < 32 || tpb > 1024 || tpb % 32) return PWA_ERR_ARG;
+  std::vector<char> cubin;
+  std::string log;
+  int rc = compile_cubin(src, src_len, tpb, arch, false, &cubin, &log);
+  if (rc == PWA_OK && disk_cache_path(arch + '\n' + full_source(src, src_len, tpb)).empty()) {
+    log = "PWA_CUBIN_CACHE is not set: nothing was stored";
+    rc = PWA_ERR_STATE;
+  }
+  if (log_buf && log_len) {
+    std::strncpy(log_buf, log.c_str(), log_len - 1);
+    log_buf[log_len - 1] = '\0';
+  }
+  return rc;
+}
+
 int pwa_plan_create(const char* src, size_t src_len, int n_mass, int n_angle, int ncol, int nout,
                     int nshape, int nconst, int nf, int tpb, pwa_plan** out) {
   if (!out) return PWA_ERR_ARG;
@@ -462,20 +480,29 @@ int pwa_upload_events(pwa_plan* h, const double* xm, const double* xa, const dou
     int rc = launch(h, h->k.to_f32, dim3(h->sms * 4), dim3(256), args, s);
     if (rc) return rc;
   }
-  // persistent grid: occupancy-limited blocks on every SM, split by set size
-  int per_sm = 0;
-  CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)h->k.eval_f64, h->tpb, 0));
-  if (per_sm < 1) per_sm = 1;
-  long long want = (long long)per_sm * h->sms;
-  long long need = (n + h->tpb - 1) / h->tpb;
-  long long nb = want < need ? want : need;
-  if (nb < 2) nb = 2;
-  long long bd = n_mc == 0 ? nb : (n_data == 0 ? 0 : (nb * n_data + n / 2) / n);
-  if (n_data > 0 && bd < 1) bd = 1;
-  if (n_mc > 0 && bd > nb - 1) bd = nb - 1;
-  h->nblocks = (int)nb;
-  h->blocks_data = (int)bd;
-  int rc = ensure_partials(h, (long long)h->nblocks * h->nacc);
+  // persistent grids: occupancy-limited blocks on every SM, split by set
+  // size (the FP64 and FP32 kernels are compiled for different occupancies)
+  auto grid = [&](cudaKernel_t k, int* nb_out, int* bd_out) -> cudaError_t {
+    int per_sm = 0;
+    const cudaError_t e =
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k, h->tpb, 0);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
+    const long long want = (long long)per_sm * h->sms;
+    const long long need = (n + h->tpb - 1) / h->tpb;
+    long long nb = want < need ? want : need;
+    if (nb < 2) nb = 2;
+    long long bd = n_mc == 0 ? nb : (n_data == 0 ? 0 : (nb * n_data + n / 2) / n);
+    if (n_data > 0 && bd < 1) bd = 1;
+    if (n_mc > 0 && bd > nb - 1) bd = nb - 1;
+    *nb_out = (int)nb;
+    *bd_out = (int)bd;
+    return cudaSuccess;
+  };
+  CU(grid(h->k.eval_f64, &h->nblocks, &h->blocks_data));
+  CU(grid(h->k.eval_f32, &h->nblocks32, &h->blocks_data32));
+  const int nb_max = h->nblocks > h->nblocks32 ? h->nblocks : h->nblocks32;
+  int rc = ensure_partials(h, (long long)nb_max * h->nacc);
   if (rc) return rc;
   CU(cudaStreamSynchronize(s));
   return PWA_OK;
@@ -489,10 +516,13 @@ int pwa_eval_enqueue(pwa_plan* h, const double* consts, int precision, int mc, v
   cudaStream_t s = (cudaStream_t)stream;
   std::vector<double> cbuf(consts, consts + h->nconst);
   long long n_all = mc ? h->n_data + h->n_mc : h->n_data;
-  int nblocks = mc ? h->nblocks : h->blocks_data;
-  if (!mc && h->n_mc == 0) nblocks = h->nblocks;
+  const bool f64 = precision == PWA_PLAIN_F64;
+  const int nb_all = f64 ? h->nblocks : h->nblocks32;
+  const int nb_data = f64 ? h->blocks_data : h->blocks_data32;
+  int nblocks = mc ? nb_all : nb_data;
+  if (!mc && h->n_mc == 0) nblocks = nb_all;
   if (nblocks < 1) nblocks = 1;
-  int bd = mc ? h->blocks_data : nblocks;
+  int bd = mc ? nb_data : nblocks;
   const void* xa = precision == PWA_PLAIN_F64 ? (const void*)h->xa : (const void*)h->xa32;
   long long nd = h->n_data, ld = h->ld;
   void* args[] = {cbuf.data(), (void*)&xa, &h->xm, &h->w, &nd, &n_all, &ld, &bd, &h->partials};

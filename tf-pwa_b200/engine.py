@@ -32,7 +32,24 @@ LIB_PATH = os.path.join(HERE, "libpwa_b200.so")
 PLAIN_F64 = 0
 MIXED_F32 = 1
 
+# Compiled model modules are kept on disk across processes: in the directory
+# PWA_CUBIN_CACHE names when it is set (set and empty: no disk cache), else in
+# the package's own _cubins directory, where the build step stores the
+# shipped models ahead of time (Engine.precompile).
+CUBIN_DIR = os.path.join(HERE, "_cubins")
+
 _lib = None
+
+
+def _default_cubin_cache():
+    if "PWA_CUBIN_CACHE" in os.environ:
+        return
+    try:
+        os.makedirs(CUBIN_DIR, exist_ok=True)
+    except OSError:
+        return
+    if os.access(CUBIN_DIR, os.W_OK | os.X_OK):
+        os.environ["PWA_CUBIN_CACHE"] = CUBIN_DIR
 
 
 def load_library(path=LIB_PATH):
@@ -40,6 +57,7 @@ def load_library(path=LIB_PATH):
     global _lib
     if _lib is not None:
         return _lib
+    _default_cubin_cache()
     if not os.path.exists(path):
         raise RuntimeError(
             f"{path} not found: build it first (python -c 'import __graft_entry__ as g; g.build()')")
@@ -83,6 +101,7 @@ def load_library(path=LIB_PATH):
     lib.pwa_server_destroy.argtypes = [vp]
     lib.pwa_plan_destroy.argtypes = [vp]
     lib.pwa_compile_only.argtypes = [cp, sz, i, cp, cp, sz]
+    lib.pwa_precompile.argtypes = [cp, sz, i, cp, cp, sz]
     lib.pwa_upload_events.argtypes = [vp, vp, vp, vp, ll, ll, i, vp]
     lib.pwa_eval.argtypes = [vp, dp, i, i, vp, dp]
     lib.pwa_eval_enqueue.argtypes = [vp, dp, i, i, vp]
@@ -99,7 +118,8 @@ def load_library(path=LIB_PATH):
     return lib
 
 
-EXPORTED = ("pwa_plan_create", "pwa_plan_destroy", "pwa_compile_only", "pwa_upload_events",
+EXPORTED = ("pwa_plan_create", "pwa_plan_destroy", "pwa_compile_only", "pwa_precompile",
+            "pwa_upload_events",
             "pwa_eval", "pwa_eval_enqueue", "pwa_eval_pdf", "pwa_build_gram", "pwa_cache_data",
             "pwa_eval_cached_enqueue", "pwa_set_param_layout", "pwa_pieces_cached",
             "pwa_nll_grad_cached", "pwa_set_cached_variant", "pwa_pool_reserve",
@@ -245,6 +265,17 @@ class Engine:
         if rc != 0:
             raise PWAError(f"compile failed: {log}")
         return log
+
+    def precompile(self, arch="sm_100a"):
+        """Compile this model's module without a device into the on-disk
+        cubin cache (pwa_precompile), so that a later process on a device
+        of ``arch`` loads it instead of compiling."""
+        load_library()
+        buf = ctypes.create_string_buffer(1 << 12)
+        src = self.src.encode()
+        rc = load_library().pwa_precompile(src, len(src), self.tpb, arch.encode(), buf, len(buf))
+        if rc != 0:
+            raise PWAError(f"precompile failed: {buf.value.decode(errors='replace')}")
 
     # ------------------------------------------------------------- events
     def split_fields(self, x):
