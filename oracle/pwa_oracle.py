@@ -640,3 +640,112 @@ def nll_grad_from_sums(names, vals, polar, trainable, sd, gd, sm, gm, sw):
                 dc[k] = m * rest / g * dg
         grad[t] = -2.0 * np.real(dc @ gd) + sw * 2.0 * np.real(dc @ gm) / sm
     return nll, grad
+
+
+# ------------------------------------------- exact Hessian of the couplings
+def clip_log_d12(x, eps=_EPS_CLIP):
+    """First and second derivatives of clip_log (model.py:283-292): 1/x and
+    -1/x^2 above eps, the quadratic continuation's 1/eps - (x-eps)/eps^2 and
+    -1/eps^2 below."""
+    big = x > eps
+    xs = np.where(big, x, 1.0)
+    d1 = np.where(big, 1.0 / xs, 1.0 / eps - (x - eps) / eps ** 2)
+    d2 = np.where(big, -1.0 / xs ** 2, -1.0 / eps ** 2)
+    return d1, d2
+
+
+def hessian_sums(model, x, w, vals, polar):
+    """Data sums for the exact second derivatives of -sum w clip_log(f) in
+    the couplings: with A_o = sum_k c_k F_ko, f = sum_o |A_o|^2 = c^H Q c
+    (Q_lk = sum_o conj(F_lo) F_ko) and G_k = sum_o conj(A_o) F_ko,
+      S0 = sum w t(f),  S1 = sum w t'(f) G,
+      H1 = sum w t'(f) Q   (K x K Hermitian),
+      H2 = sum w t''(f) g g^T,  g = (Re G, -Im G)   (2K x 2K),
+    which give d2/da db of the data term as
+      -2 Re[(c_b)^H H1 c_a] - 2 Re(c_ab . S1) - 4 (Re c_a, Im c_a) H2 (Re c_b, Im c_b)^T
+    for c_a = dc/da, c_ab = d2c/da db.  The reference obtains the same
+    matrix by nested GradientTape (tf_pwa/model/model.py:513-561)."""
+    F, names = model.columns(x, vals, polar)
+    c = coupling_products(names, vals, polar)
+    A = np.einsum("k,nko->no", c, F)
+    f = np.sum(np.abs(A) ** 2, 1)
+    G = np.einsum("no,nko->nk", np.conj(A), F)
+    d1, d2 = clip_log_d12(f)
+    S0 = float(np.sum(w * clip_log(f)))
+    S1 = (w * d1) @ G
+    H1 = np.einsum("n,nlo,nko->lk", w * d1, np.conj(F), F)
+    g = np.concatenate([G.real, -G.imag], 1)
+    H2 = np.einsum("n,np,nq->pq", w * d2, g, g)
+    return S0, S1, H1, H2, names
+
+
+def gram_matrix(model, x, w, vals, polar):
+    """M_lk = sum w sum_o conj(F_lo) F_ko (the MC integral I = c^H M c)."""
+    F, names = model.columns(x, vals, polar)
+    return np.einsum("n,nlo,nko->lk", w, np.conj(F), F), names
+
+
+def coupling_derivatives(names, vals, polar, trainable):
+    """dc/da (P, K) and d2c/da db (P, P, K) of the column couplings c_k =
+    product of the column's factors (chain total, one g_ls per vertex) with
+    respect to the trainable coupling parts (r/i, polar or Cartesian)."""
+    P, K = len(trainable), len(names)
+
+    def z_of(base):
+        return OracleModel.complex_of(vals, polar, base)
+
+    def dz(base, part):
+        if polar.get(base, True):
+            return np.exp(1j * vals[base + "i"]) if part == "r" else 1j * z_of(base)
+        return 1.0 + 0j if part == "r" else 1j
+
+    def d2z(base, p1, p2):
+        if not polar.get(base, True):
+            return 0j
+        e = np.exp(1j * vals[base + "i"])
+        if p1 == p2 == "r":
+            return 0j
+        if p1 == p2 == "i":
+            return -z_of(base)
+        return 1j * e
+
+    parts = [(n[:-1], n[-1]) for n in trainable]
+    dc = np.zeros((P, K), np.complex128)
+    d2c = np.zeros((P, P, K), np.complex128)
+    for k, (tot, gs) in enumerate(names):
+        facs = [tot] + list(gs)
+        zs = [z_of(q) for q in facs]
+        for a, (ba, pa) in enumerate(parts):
+            for i, q in enumerate(facs):
+                if q != ba:
+                    continue
+                rest = np.prod([zs[m] for m in range(len(facs)) if m != i])
+                dc[a, k] += dz(ba, pa) * rest
+                for b, (bb, pb) in enumerate(parts):
+                    if bb == ba:
+                        d2c[a, b, k] += d2z(ba, pa, pb) * rest
+                    for j, q2 in enumerate(facs):
+                        if j == i or q2 != bb:
+                            continue
+                        rest2 = np.prod([zs[m] for m in range(len(facs)) if m not in (i, j)])
+                        d2c[a, b, k] += dz(ba, pa) * dz(bb, pb) * rest2
+    return dc, d2c
+
+
+def nll_grad_hessian_from_sums(names, vals, polar, trainable, sums, M, sw):
+    """NLL, gradient and exact Hessian from the data sums of
+    :func:`hessian_sums` and the MC Gram matrix M (sum_w-normalised
+    weights): NLL = -S0 + sw ln I, I = c^H M c."""
+    S0, S1, H1, H2 = sums
+    c = coupling_products(names, vals, polar)
+    dc, d2c = coupling_derivatives(names, vals, polar, trainable)
+    I = float(np.real(np.conj(c) @ M @ c))
+    Mc = np.conj(c) @ M  # (c^H M)_k
+    dI = 2.0 * np.real(dc @ Mc)
+    grad = -2.0 * np.real(dc @ S1) + sw * dI / I
+    ch = np.concatenate([dc.real, dc.imag], 1)
+    Hd = (-2.0 * np.real(np.conj(dc) @ H1 @ dc.T).T
+          - 2.0 * np.real(d2c @ S1) - 4.0 * ch @ H2 @ ch.T)
+    d2I = 2.0 * np.real(np.conj(dc) @ M @ dc.T).T + 2.0 * np.real(d2c @ Mc)
+    H = Hd + sw * (d2I / I - np.outer(dI, dI) / I ** 2)
+    return -S0 + sw * np.log(I), grad, 0.5 * (H + H.T)

@@ -38,12 +38,12 @@ CASES = {
     # name: (config file, n_data, n_bg, n_mc, seed, hessian, extra data keys)
     "d2kpipi": ("d2kpipi.yml", 400, 0, 1500, 11, True, {}),
     "d2kpipi_float": ("d2kpipi_float.yml", 400, 0, 1500, 12, True, {}),
-    "lc2pkpi": ("lc2pkpi.yml", 400, 40, 1500, 13, False, {"bg_weight": 0.1}),
-    "toy_vvp": ("toy_vvp.yml", 300, 30, 1200, 14, False, {"bg_weight": 0.1}),
-    "b2dstkpi": ("b2dstkpi.yml", 300, 0, 1200, 15, False, {}),
+    "lc2pkpi": ("lc2pkpi.yml", 400, 40, 1500, 13, True, {"bg_weight": 0.1}),
+    "toy_vvp": ("toy_vvp.yml", 300, 30, 1200, 14, True, {"bg_weight": 0.1}),
+    "b2dstkpi": ("b2dstkpi.yml", 300, 0, 1200, 15, True, {}),
     "d2kpipi_shapes": ("d2kpipi_shapes.yml", 400, 0, 1500, 16, True, {}),
     "dp2kpipi_ident": ("dp2kpipi_ident.yml", 400, 0, 1500, 17, True, {}),
-    "ident_fermions": ("ident_fermions.yml", 300, 0, 1200, 18, False, {}),
+    "ident_fermions": ("ident_fermions.yml", 300, 0, 1200, 18, True, {}),
     "epem_cp": ("epem_cp.yml", 300, 0, 1200, 19, False, {}),
     "lc2pkpi_cc": ("lc2pkpi_cc.yml", 400, 0, 1500, 20, False, {}),
     "b2dstkpi_cc": ("b2dstkpi_cc.yml", 400, 0, 1500, 21, False, {}),

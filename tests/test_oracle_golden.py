@@ -101,3 +101,31 @@ def test_oracle_one_pass_gradient(name):
     assert abs(nll - float(g["nll"])) <= 1e-12 * abs(float(g["nll"]))
     np.testing.assert_allclose(grad, g["grad"][idx], rtol=0,
                                atol=1e-10 * np.abs(g["grad"]).max())
+
+
+@pytest.mark.parametrize("name", ["d2kpipi", "lc2pkpi", "dp2kpipi_ident", "ident_fermions",
+                                  "toy_vvp", "b2dstkpi"])
+def test_oracle_exact_coupling_hessian(name):
+    """The closed-form second derivatives in the couplings (two weighted
+    Gram-type sums over the data, the MC Gram matrix and the derivatives
+    of the column couplings) equal the reference's nested-GradientTape
+    Hessian (FCN.nll_grad_hessian) on the golden events."""
+    from common import golden_data, load_golden, load_model
+    from oracle.pwa_oracle import (OracleModel, gram_matrix, hessian_sums,
+                                   nll_grad_hessian_from_sums)
+
+    g, meta = load_golden(name)
+    dc, vm, plan = load_model(meta["config"])
+    vals = meta["variables"]
+    x, w = golden_data(g, meta)
+    xm = g["fields_mc"]
+    wm = np.ones(xm.shape[1]) / xm.shape[1]
+    m = OracleModel(dc.decay_group, plan)
+    S0, S1, H1, H2, names = hessian_sums(m, x, w, vals, {})
+    M, _ = gram_matrix(m, xm, wm, vals, {})
+    nll, grad, H = nll_grad_hessian_from_sums(names, vals, {}, meta["trainable"],
+                                              (S0, S1, H1, H2), M, w.sum())
+    assert abs(nll - float(g["hess_nll"])) <= 1e-12 * abs(float(g["hess_nll"]))
+    np.testing.assert_allclose(grad, g["hess_grad"], rtol=0,
+                               atol=1e-12 * np.abs(g["hess_grad"]).max())
+    np.testing.assert_allclose(H, g["hess"], rtol=0, atol=1e-12 * np.abs(g["hess"]).max())
