@@ -374,7 +374,37 @@ NCU_F64_FLOPS_PER_EVENT = {
     # 2 * 1.723050e9 DFMA + 7.7975e8 DMUL + 1.54827e8 DADD per launch over
     # 5.5e5 data + 5e5 MC events of the Lambda_c model
     "lc2pkpi": (2 * 1723050000 + 779750000 + 154826528) / 1.05e6,
+    # 2 * 2.0671e9 DFMA + 1.0715e9 DMUL + 1.35105e8 DADD over 1e5 + 4e5 events
+    "b2dstkpi": (2 * 2067100000 + 1071500000 + 135104560) / 5e5,
+    # 2 * 2.1725e8 DFMA + 9.075e7 DMUL + 2.74312e7 DADD over 2.5e5 + 2.5e5 events
+    "d2kpipi_float": (2 * 217250000 + 90750000 + 27431232) / 5e5,
 }
+# FP32 and FP64 operations per event of the FP32-amplitude kernel
+# (pwa_eval_f32), same captures: 2 * FFMA + FMUL + FADD, 2 * DFMA + DMUL + DADD
+NCU_F32_KERNEL_FLOPS = {
+    "d2kpipi_float": ((2 * 121909312 + 50303104 + 6151552) / 5e5,
+                      (2 * 47750000 + 25250000 + 27795200) / 5e5),
+    "lc2pkpi": ((2 * 658350000 + 309225000 + 22050000) / 5.25e5,
+                (2 * 94500000 + 55975000 + 99693704) / 5.25e5),
+    "b2dstkpi": ((2 * 1581000000 + 929500000 + 80000000) / 5e5,
+                 (2 * 99600000 + 57500000 + 268206080) / 5e5),
+}
+
+
+def _mixed_pipe_roofline(name, n_ev, launch_s, peaks):
+    """Roofline of a kernel doing both FP32 and FP64 work: the ideal time is
+    FP32 ops / FP32 peak + FP64 ops / FP64 peak (measured FMA peaks);
+    frac = ideal / measured, achieved = total ops / measured time."""
+    f32, f64 = NCU_F32_KERNEL_FLOPS[name]
+    ideal = n_ev * (f32 / (peaks["f32_tflops"] * 1e12) + f64 / (peaks["f64_tflops"] * 1e12))
+    ops = n_ev * (f32 + f64)
+    return {"bound": "fp32+fp64", "achieved": ops / launch_s / 1e12,
+            "peak": ops / ideal / 1e12, "unit": "TFLOP/s", "frac": ideal / launch_s,
+            "peak_kind": "measured here (pwa_fma_peak, FP32 and FP64 FMA chains), "
+                         "weighted by the kernel's FP32 / FP64 operation mix",
+            "flops_per_event": {"fp32": f32, "fp64": f64},
+            "flops_source": "ncu: 2 FFMA + FMUL + FADD and 2 DFMA + DMUL + DADD executed",
+            "launch_us": 1e6 * launch_s, "events_per_launch": n_ev}
 
 CACHED_KERNEL = {0: "pwa_eval_cached (bulk-copy ring, per-thread FP64 column sums)",
                  1: "pwa_eval_cached_direct (direct loads, per-thread FP64 column sums)",
@@ -446,12 +476,17 @@ def measure_cached(name, args, rank, world, dist, timed, log, n_sig, n_bg, n_mc,
     # FP32 tensor), same L2 protocol: what one plain pass over that many bytes
     # costs on this GPU, fixed per-launch part included
     floor_buf = torch.ones(bytes_mixed // 4, dtype=torch.float32, device="cuda")
+    for _ in range(3):
+        floor_buf.sum()
     t_floor = timed(lambda: floor_buf.sum(), k_kernel)
     del floor_buf
-    # Hessian of all trainable parameters: the 4P stencil points of the
+    # Hessian of all trainable parameters: exact, from one pass of the
+    # Hessian-sums kernel; and, for comparison, the 4P stencil points of the
     # differenced adjoint gradient in one multi-point pass over the cache
     k_hess = 3
-    t_hess = timed(lambda: eng.hessian_cached(var_vec, 1e-2), k_hess)
+    eng.hessian_cached_exact(var_vec)
+    t_hess = timed(lambda: eng.hessian_cached_exact(var_vec), k_hess)
+    t_hess_fd = timed(lambda: eng.hessian_cached(var_vec, 1e-2), k_hess)
     Cp = eng_p.consts(vals)
     t_kernel_p = timed(lambda: eng_p.eval_enqueue(Cp, PLAIN_F64, mc=True), k_kernel)
     # the FP32-amplitude recompute form (what a fit with floating masses and
@@ -502,6 +537,9 @@ def measure_cached(name, args, rank, world, dist, timed, log, n_sig, n_bg, n_mc,
         "fp32_recompute": {"value": world * args.steps / t_f32, "unit": "evals/s",
                            "ms_per_step": 1e3 * t_f32 / args.steps,
                            "kernel_us": 1e6 * t_kernel_f32 / k_kernel,
+                           "roofline": (_mixed_pipe_roofline(name, n_ev, t_kernel_f32 / k_kernel,
+                                                             peaks)
+                                        if name in NCU_F32_KERNEL_FLOPS else None),
                            "dnll": nll_f - nll_p,
                            "grad_max_rel": float(np.max(np.abs(g_f - g_p)) / np.max(np.abs(g_p)))},
         "e2e": {"value": world * args.steps / t_e2e, "unit": "evals/s",
@@ -541,10 +579,13 @@ def measure_cached(name, args, rank, world, dist, timed, log, n_sig, n_bg, n_mc,
                      "pinned": os.environ.get("PWA_CACHED_CONFIG")},
         "cached_variants": var_table,
         "hessian": {"ms": 1e3 * t_hess / k_hess, "n_params": len(names),
-                    "stencil_points": 4 * len(names),
                     "in_single_steps": (t_hess / k_hess) / (t_mixed / args.steps),
-                    "call": "pwa_hessian_cached: one evaluation + the 4P stencil points "
-                            "in one multi-point pass over the column cache"},
+                    "call": "pwa_hessian_cached_exact: exact Hessian in the couplings, one "
+                            "pass of the Hessian-sums kernel over the column cache",
+                    "stencil": {"ms": 1e3 * t_hess_fd / k_hess, "points": 4 * len(names),
+                                "in_single_steps": (t_hess_fd / k_hess) / (t_mixed / args.steps),
+                                "call": "pwa_hessian_cached: 4-point differences of the "
+                                        "adjoint gradient, one multi-point pass"}},
         "check": {"nll_mixed": nll_m, "nll_plain": nll_p, "dnll": nll_m - nll_p,
                   "grad_max_rel": float(np.max(np.abs(g_m - g_p)) / np.max(np.abs(g_p)))},
         "setup_s": {"dataset": t_data, "mixed_fcn": t_mixed_setup},
@@ -608,6 +649,19 @@ def measure_floating(name, args, rank, world, dist, timed, log, n_sig, n_mc):
     bytes_f64 = n_all * (8 * len(code.mass_fields) + 8 * len(code.angle_fields) + 8)
     hbm, peak_kind = _peaks()
     ach = bytes_f32 / (t_k / args.steps) / 1e9
+    peaks = {"f64_tflops": fcn.eng.fma_peak(PLAIN_F64) / 1e12,
+             "f32_tflops": fcn.eng.fma_peak(MIXED_F32) / 1e12}
+    roof = _mixed_pipe_roofline(name, n_all, t_k / args.steps, peaks)
+    roof.update({"kernel": "pwa_eval_f32 + pwa_reduce (data + MC, FP32 amplitudes)",
+                 "hbm": {"achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                         "peak_kind": peak_kind, "algorithmic_bytes_per_launch": bytes_f32}})
+    fl_p = NCU_F64_FLOPS_PER_EVENT[name]
+    ach_p = fl_p * n_all / (t_kp / args.steps) / 1e12
+    roof["plain_f64_kernel"] = {
+        "bound": "fp64", "achieved": ach_p, "peak": peaks["f64_tflops"], "unit": "TFLOP/s",
+        "frac": ach_p / peaks["f64_tflops"], "flops_per_event": fl_p,
+        "flops_source": "ncu: 2 DFMA + DADD + DMUL executed per event (forward and adjoint)",
+        "launch_us": 1e6 * t_kp / args.steps, "algorithmic_bytes_per_launch": bytes_f64}
     line = {
         "metric": metric, "value": world * args.steps / t_f32, "unit": "evals/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -625,13 +679,8 @@ def measure_floating(name, args, rank, world, dist, timed, log, n_sig, n_mc):
         "e2e": {"value": world * args.steps / t_f32, "unit": "evals/s",
                 "h2d_bytes_per_step": 8 * len(x0), "d2h_bytes_per_step": 8 * (1 + len(x0)),
                 "call": "FCN.nll_grad(x) with x a host numpy vector"},
-        "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
-                     "frac": ach / hbm, "traffic": None, "peak_kind": peak_kind,
-                     "kernel": "pwa_eval_f32 + pwa_reduce (data + MC, FP32 amplitudes)",
-                     "algorithmic_bytes_per_launch": bytes_f32,
-                     "launch_us": 1e6 * t_k / args.steps,
-                     "plain_f64_kernel": {"launch_us": 1e6 * t_kp / args.steps,
-                                          "algorithmic_bytes_per_launch": bytes_f64}},
+        "roofline": roof,
+        "fma_peaks": peaks,
         "gpu_launches": 2 * args.steps,
         "hessian": {"seconds": t_hess, "n_params": len(x0), "evaluations": 4 * len(x0) + 1,
                     "errors": dict(zip(names, np.sqrt(np.abs(np.diag(cov))).tolist()))},

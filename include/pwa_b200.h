@@ -20,6 +20,7 @@
  *   pwa_toy_select /   flat phase space and toy        tf_pwa/phasespace.py:31-254,
  *   pwa_toy_fields     accept-reject on sum |A|^2      tf_pwa/applications.py:394-487
  *   pwa_hessian_cached Hessian (differenced adjoint)   tf_pwa/model/model.py:513-561
+ *   pwa_hessian_cached_exact  (closed form, one pass)  tf_pwa/model/model.py:513-561
  *   pwa_read_dat       text momentum files             tf_pwa/data.py:300-365
  *   pwa_server_*       many fits, each a BFGS driver   tf_pwa/fit.py:189-419 (one per fit)
  *   pwa_compile_only / pwa_precompile / pwa_last_error / pwa_plan_info / pwa_plan_destroy
@@ -142,6 +143,27 @@ int pwa_toy_fields(pwa_plan* h, unsigned long long seed, const long long* idx, l
  * Needs pwa_cache_data, pwa_build_gram and pwa_set_param_layout first. */
 int pwa_hessian_cached(pwa_plan* h, const double* vars, double sum_w, double step, void* stream,
                        double* out_nll, double* out_grad, double* out_hess);
+
+/* Exact Hessian of the cached-form NLL in the trainable coupling parts
+ * (what tf_pwa/model/model.py:513-561 computes by nested GradientTape), in
+ * one pass over the column cache: the kernel sums, over the data events,
+ * S0 = sum w t(f), S1 = sum w t'(f) G, H1 = sum w t'(f) Q and
+ * H2 = sum w t''(f) g g^T (t = clip_log, Q_lk = sum_o conj(F_lo) F_ko,
+ * G_k = sum_o conj(A_o) F_ko, g = (Re G, -Im G)); the host adds the MC
+ * term from the Gram matrix and applies the first and second derivatives
+ * of the column couplings.  Also the NLL and gradient at vars.  out_hess:
+ * n_train x n_train, row-major, symmetric.  Needs pwa_cache_data,
+ * pwa_build_gram and pwa_set_param_layout first; every trainable variable
+ * must be a coupling part (masses and widths fixed). */
+int pwa_hessian_cached_exact(pwa_plan* h, const double* vars, double sum_w, void* stream,
+                             double* out_nll, double* out_grad, double* out_hess);
+
+/* The data sums of pwa_hessian_cached_exact at vars (host out, 1 + 2K +
+ * 2K(2K + 1) doubles for K = ncol): S0, S1 (re, im per column), then the
+ * upper triangles (p <= q, row-major) of the 2K x 2K sums
+ * sum w t'(f) X X^T over rows X = (Re F_.o, Im F_.o) and sum w t''(f) g g^T.
+ * Sums of event shards add (multi-GPU: all-reduce them). */
+int pwa_hess_sums_cached(pwa_plan* h, const double* vars, void* stream, double* out);
 
 /* Momentum file ingest (tf_pwa/data.py:300-365, load_dat_file): all
  * whitespace- or comma-separated numbers of a text file ('#' starts a

@@ -306,15 +306,22 @@ class FCN:
         return NLLFunction.apply(x, self)
 
     def nll_grad_hessian(self, x=None, batch=None, step=None):
-        """Hessian by differencing the adjoint gradient: 4-point central
+        """NLL, gradient and Hessian.  In the cached form (fixed masses and
+        widths) with no ``step``: the exact Hessian in the couplings from
+        one pass over the column cache (``pwa_hessian_cached_exact``; the
+        reference's nested-tape Hessian, ``tf_pwa/model/model.py:513-561``).
+        Otherwise by differencing the adjoint gradient: 4-point central
         stencil per parameter, h_i = step * max(|x_i|, 1e-2) (error O(h^4)),
         symmetrised.  Default step: 1e-4 in the plain form; 1e-2 in the
         mixed forms, whose FP32 per-event (or per-warp) values put 1e-7 to
         1e-6 relative rounding noise on the gradient (noise / h must stay
-        small).  In the cached form the whole stencil loop runs in the native
+        small); in the cached form the stencil loop runs in the native
         library.  ``batch`` is accepted in the reference's position
         (``tf_pwa/model/model.py:1258``); the engine does not batch."""
         self._set(x)
+        if self.use_gram and step is None and self.eng.dist_reduce is None:
+            v = self.vm.variables
+            return self.eng.hessian_cached_exact([v[k] for k in self._var_names])
         if step is None:
             step = 1e-4 if self.precision == PLAIN_F64 else 1e-2
         if self.use_gram:

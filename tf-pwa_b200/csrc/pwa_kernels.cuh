@@ -1685,6 +1685,224 @@ extern "C" __global__ void __launch_bounds__(PWA_PTS_WARPS * 32, 1)
 }
 
 // ---------------------------------------------------------------------------
+// Exact second derivatives in the couplings from the column cache (masses
+// and widths fixed).  With A_o = sum_k c_k F_ko, f = sum_o |A_o|^2 and
+// G_k = sum_o conj(A_o) F_ko, the data term -sum w t(f) (t = clip_log) has
+// second derivatives in the couplings built from
+//   H1 = sum w t'(f) Q,  Q_lk = sum_o conj(F_lo) F_ko   (K x K Hermitian)
+//   H2 = sum w t''(f) g g^T,  g = (Re G, -Im G)         (2K x 2K)
+// and the gradient pieces S0 = sum w t(f), S1 = sum w t'(f) G; the host
+// combines them with the derivatives of the column couplings and the MC
+// Gram matrix (the reference obtains the same matrix by nested tapes,
+// tf_pwa/model/model.py:513-561).  Both matrices are weighted sums of
+// outer products of rows: H1 from X1 rows (helicity o, event e) =
+// (Re F_.o, Im F_.o) with weight w t'(f) (Re Q = X_RR + X_II, Im Q = X_RI -
+// X_IR), H2 from X2 rows (event e) = g with weight w t''(f).
+//
+// A block walks a contiguous run of 128-event tiles.  Per tile, thread e
+// computes its event's A (FP64), f, t, t', t'' and G (FP32) and writes its
+// rows of X1 and X2 to shared memory; then each thread accumulates its
+// items -- (matrix, PWA_HBS x PWA_HBS block of the upper triangle, range of
+// rows) -- over the tile in FP32 and adds them to FP64 registers.  The
+// block row of partials is [S0, S1 (re, im per column), H1 upper entries,
+// H2 upper entries] (upper entry (p, q), p <= q, at p W - p (p - 1) / 2 +
+// q - p); rows of several splits of one block are added in split order, so
+// the result does not depend on scheduling.
+#define PWA_HW (2 * PWA_NCOL)
+#define PWA_HBS (PWA_HW % 4 == 0 ? 4 : 2)
+#define PWA_HNB (PWA_HW / PWA_HBS)
+#define PWA_HUP (PWA_HNB * (PWA_HNB + 1) / 2)
+#define PWA_HTRI (PWA_HW * (PWA_HW + 1) / 2)
+#define PWA_HNA (1 + PWA_HW + 2 * PWA_HTRI)
+// row splits: X1 has PWA_NOUT times the rows of X2, so it gets PWA_NOUT
+// times the splits and every item walks about the same number of rows
+#define PWA_HSP2 (PWA_HUP * (PWA_NOUT + 1) >= PWA_TPB ? 1 : PWA_TPB / (PWA_HUP * (PWA_NOUT + 1)))
+#define PWA_HSP1 (PWA_HSP2 * PWA_NOUT)
+#define PWA_HN1 (PWA_HUP * PWA_HSP1)
+#define PWA_HITEMS (PWA_HN1 + PWA_HUP * PWA_HSP2)
+#define PWA_HIPT ((PWA_HITEMS + PWA_TPB - 1) / PWA_TPB)
+// row stride of X1 / X2 in floats: a multiple of 4 (16-byte rows, float4
+// stores) that is 4 mod 8, so eight consecutive rows start in eight
+// different bank quads (conflict-free 16-byte stores of consecutive events)
+#define PWA_HLD4 ((PWA_HW + 3) / 4 * 4)
+#define PWA_HLD (PWA_HLD4 % 8 == 0 ? PWA_HLD4 + 4 : PWA_HLD4)
+
+__device__ __forceinline__ int hess_upper(int p, int q) {
+  return p * PWA_HW - p * (p - 1) / 2 + (q - p);
+}
+
+// one row of W values (zero-padded to PWA_HLD4) as 16-byte stores
+__device__ __forceinline__ void hess_store_row(float* dst, const float (&row)[PWA_HLD4]) {
+#pragma unroll
+  for (int q = 0; q < PWA_HLD4 / 4; ++q)
+    *(float4*)(dst + 4 * q) = make_float4(row[4 * q], row[4 * q + 1], row[4 * q + 2], row[4 * q + 3]);
+}
+
+extern "C" __global__ void __launch_bounds__(PWA_TPB, 2)
+    pwa_hess_cached(const CCoup c, const float2* __restrict__ Fc,
+                    const double* __restrict__ Wc, long long ntiles,
+                    double* __restrict__ partials) {
+  constexpr int K = PWA_NCOL, W = PWA_HW, BS = PWA_HBS, LD = PWA_HLD;
+  constexpr int R1 = PWA_NOUT * PWA_TPB;
+  extern __shared__ __align__(16) unsigned char hess_smem[];
+  double* row_acc = (double*)hess_smem;                                  // [PWA_HNA]
+  float* X1 = (float*)(hess_smem + (PWA_HNA * 8 + 15) / 16 * 16);        // [R1][LD]
+  float* X2 = X1 + R1 * LD;                                               // [TPB][LD]
+  float* s1 = X2 + PWA_TPB * LD;                                          // [TPB]
+  float* s2 = s1 + PWA_TPB;                                               // [TPB]
+  __shared__ double s_c[2 * PWA_NCOL];
+  __shared__ double s_red[PWA_TPB / 32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  stage_couplings(c, s_c);
+  __syncthreads();
+  // this thread's items (matrix, split, upper block bi <= bj), ordered so
+  // that neighbouring threads share the matrix and the rows
+  int it_m[PWA_HIPT], it_s[PWA_HIPT], it_bi[PWA_HIPT], it_bj[PWA_HIPT];
+  double hacc[PWA_HIPT][BS][BS];
+#pragma unroll
+  for (int q = 0; q < PWA_HIPT; ++q) {
+    const int it = tid + q * PWA_TPB;
+    const int m = it < PWA_HN1 ? 0 : 1, r = it < PWA_HN1 ? it : it - PWA_HN1;
+    int blk = r % PWA_HUP, bi = 0;
+    while (blk >= PWA_HNB - bi) blk -= PWA_HNB - bi++;
+    it_m[q] = it < PWA_HITEMS ? m : -1;
+    it_s[q] = r / PWA_HUP;
+    it_bi[q] = bi;
+    it_bj[q] = bi + blk;
+#pragma unroll
+    for (int i = 0; i < BS; ++i)
+#pragma unroll
+      for (int j = 0; j < BS; ++j) hacc[q][i][j] = 0.0;
+  }
+  double acc_s0 = 0.0, acc_s1 = 0.0;
+  const long long B = gridDim.x, b = blockIdx.x;
+  const long long t0 = b * ntiles / B, t1 = (b + 1) * ntiles / B;
+#pragma unroll 1
+  for (long long t = t0; t < t1; ++t) {
+    {  // this thread's event: amplitude, clip_log derivatives, G, rows
+      const float2* F = Fc + t * PWA_NF * PWA_TPB + tid;
+      float2 v[PWA_NF];
+#pragma unroll
+      for (int j = 0; j < PWA_NF; ++j) v[j] = __ldcs(F + j * PWA_TPB);
+      const double w = __ldcs(Wc + t * PWA_TPB + tid);
+      double ar[PWA_NOUT], ai[PWA_NOUT];
+#pragma unroll
+      for (int o = 0; o < PWA_NOUT; ++o) ar[o] = ai[o] = 0.0;
+#pragma unroll
+      for (int j = 0; j < PWA_NF; ++j) {
+        const int k = pwa_fk[j], o = pwa_fo[j];
+        const double cr = s_c[2 * k], ci = s_c[2 * k + 1];
+        ar[o] = fma(cr, (double)v[j].x, fma(-ci, (double)v[j].y, ar[o]));
+        ai[o] = fma(cr, (double)v[j].y, fma(ci, (double)v[j].x, ai[o]));
+      }
+      double f = 0.0;
+#pragma unroll
+      for (int o = 0; o < PWA_NOUT; ++o) f = fma(ar[o], ar[o], fma(ai[o], ai[o], f));
+      double d1;
+      const double cl = clip_log(f, &d1);
+      const double d2 = f > 1e-6 ? -d1 * d1 : -1e12;  // clip_log'': -1/eps^2 below eps
+      acc_s0 = fma(w, cl, acc_s0);
+      float row[PWA_HLD4];
+#pragma unroll
+      for (int q = 0; q < PWA_HLD4; ++q) row[q] = 0.f;
+#pragma unroll
+      for (int j = 0; j < PWA_NF; ++j) {  // X2 row: (Re G, -Im G)
+        const int k = pwa_fk[j], o = pwa_fo[j];
+        const float xr = (float)ar[o], xi = (float)ai[o];
+        row[k] = fmaf(xr, v[j].x, fmaf(xi, v[j].y, row[k]));
+        row[K + k] = fmaf(xi, v[j].x, fmaf(-xr, v[j].y, row[K + k]));
+      }
+      hess_store_row(X2 + tid * LD, row);
+#pragma unroll
+      for (int o = 0; o < PWA_NOUT; ++o) {  // X1 rows: (Re F_.o, Im F_.o)
+#pragma unroll
+        for (int q = 0; q < PWA_HLD4; ++q) row[q] = 0.f;
+#pragma unroll
+        for (int j = 0; j < PWA_NF; ++j)
+          if (pwa_fo[j] == o) {
+            row[pwa_fk[j]] = v[j].x;
+            row[K + pwa_fk[j]] = v[j].y;
+          }
+        hess_store_row(X1 + (o * PWA_TPB + tid) * LD, row);
+      }
+      s1[tid] = (float)(w * d1);
+      s2[tid] = (float)(w * d2);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < PWA_HIPT; ++q) {
+      if (it_m[q] < 0) continue;
+      const float* X = it_m[q] == 0 ? X1 : X2;
+      const float* sw = it_m[q] == 0 ? s1 : s2;
+      const int R = it_m[q] == 0 ? R1 : PWA_TPB, sp = it_m[q] == 0 ? PWA_HSP1 : PWA_HSP2;
+      const int r0 = it_s[q] * R / sp, r1 = (it_s[q] + 1) * R / sp;
+      const int cp = it_bi[q] * BS, cq = it_bj[q] * BS;
+      float a[BS][BS];
+#pragma unroll
+      for (int i = 0; i < BS; ++i)
+#pragma unroll
+        for (int j = 0; j < BS; ++j) a[i][j] = 0.f;
+#pragma unroll 4
+      for (int r = r0; r < r1; ++r) {
+        const float* x = X + r * LD;
+        const float sc = sw[r % PWA_TPB];
+        float xp[BS], xq[BS];
+#pragma unroll
+        for (int i = 0; i < BS; ++i) {
+          xp[i] = sc * x[cp + i];
+          xq[i] = x[cq + i];
+        }
+#pragma unroll
+        for (int i = 0; i < BS; ++i)
+#pragma unroll
+          for (int j = 0; j < BS; ++j) a[i][j] = fmaf(xp[i], xq[j], a[i][j]);
+      }
+#pragma unroll
+      for (int i = 0; i < BS; ++i)
+#pragma unroll
+        for (int j = 0; j < BS; ++j) hacc[q][i][j] += (double)a[i][j];
+    }
+    if (tid < W) {  // S1 = sum s1 G (X2 holds -Im G in columns K .. 2K-1)
+      float a = 0.f;
+#pragma unroll 4
+      for (int e = 0; e < PWA_TPB; ++e) a = fmaf(s1[e], X2[e * LD + tid], a);
+      acc_s1 += (double)a;
+    }
+    __syncthreads();
+  }
+  // the block row: S0, S1, then the items' blocks added in split order
+  for (int j = tid; j < PWA_HNA; j += PWA_TPB) row_acc[j] = 0.0;
+  const double v0 = warp_sum(acc_s0);
+  if (lane == 0) s_red[warp] = v0;
+  __syncthreads();
+  if (tid == 0) {
+    double a = 0.0;
+#pragma unroll
+    for (int w2 = 0; w2 < PWA_TPB / 32; ++w2) a += s_red[w2];
+    row_acc[0] = a;
+  }
+  if (tid < W) row_acc[1 + (tid < K ? 2 * tid : 2 * (tid - K) + 1)] = tid < K ? acc_s1 : -acc_s1;
+  for (int spl = 0; spl < PWA_HSP1; ++spl) {
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < PWA_HIPT; ++q) {
+      if (it_m[q] < 0 || it_s[q] != spl) continue;
+      double* dst = row_acc + 1 + W + it_m[q] * PWA_HTRI;
+#pragma unroll
+      for (int i = 0; i < BS; ++i)
+#pragma unroll
+        for (int j = 0; j < BS; ++j) {
+          const int p = it_bi[q] * BS + i, pq = it_bj[q] * BS + j;
+          if (p <= pq) dst[hess_upper(p, pq)] += hacc[q][i][j];
+        }
+    }
+  }
+  __syncthreads();
+  for (int j = tid; j < PWA_HNA; j += PWA_TPB)
+    partials[(long long)blockIdx.x * PWA_HNA + j] = row_acc[j];
+}
+
+// ---------------------------------------------------------------------------
 // Many fits in one launch (serving).  Each fit's data-event column cache is a
 // run of tiles in a shared pool (same tile layout as above).  The launch gets
 // a work list of (request, pool tile) pairs covering the tiles of every fit

@@ -40,6 +40,7 @@ struct Kernels {
                eval_cached_wide = nullptr, eval_cached_tma = nullptr, eval_multi = nullptr,
                gram_colmax = nullptr, gram_tc = nullptr, wait_check = nullptr,
                fma_f64 = nullptr, fma_f32 = nullptr, eval_points = nullptr, reduce_multi = nullptr,
+               hess_cached = nullptr,
                fields_from_p4 = nullptr, toy_select = nullptr, toy_fields = nullptr;
 };
 
@@ -109,6 +110,10 @@ struct pwa_plan {
   // multi-point evaluation: device couplings and sums of up to pts_cap points
   double* d_pts = nullptr;
   int pts_cap = 0;
+  // exact coupling Hessian: launch geometry (0 blocks: not set up) and sums
+  int hess_blocks = 0;
+  size_t hess_smem = 0;
+  double* d_hsum = nullptr;
   // parameter layout for the C-side chain rule
   int n_vars = 0, n_coup = 0, nfac = 0, n_train = 0;
   std::vector<int> coup_r, coup_i, coup_polar, col_fac, train_idx;
@@ -397,7 +402,8 @@ int pwa_plan_create(const char* src, size_t src_len, int n_mass, int n_angle, in
             {"pwa_fields_from_p4", &h->k.fields_from_p4},
             {"pwa_toy_select", &h->k.toy_select},
             {"pwa_toy_fields", &h->k.toy_fields},
-            {"pwa_eval_multi", &h->k.eval_multi},   {"pwa_reduce_multi", &h->k.reduce_multi}};
+            {"pwa_eval_multi", &h->k.eval_multi},   {"pwa_reduce_multi", &h->k.reduce_multi},
+            {"pwa_hess_cached", &h->k.hess_cached}};
   for (auto& e : ks) CU(cudaLibraryGetKernel(e.slot, h->lib, e.name));
   for (int p = 0; p < 2; ++p) {
     cudaFuncAttributes a;
@@ -431,6 +437,7 @@ int pwa_plan_destroy(pwa_plan* h) {
   if (h->d_tile_part) cudaFree(h->d_tile_part);
   if (h->d_multi_out) cudaFree(h->d_multi_out);
   if (h->d_pts) cudaFree(h->d_pts);
+  if (h->d_hsum) cudaFree(h->d_hsum);
   if (h->h_map) cudaFreeHost(h->h_map);
   if (h->d_out) cudaFree(h->d_out);
   if (h->h_out) cudaFreeHost(h->h_out);
@@ -864,6 +871,7 @@ int pwa_cache_data(pwa_plan* h, const double* consts, void* stream) {
   if (rc) return rc;
   CU(cudaStreamSynchronize(s));
   h->fcache_n = n;
+  h->hess_blocks = 0;  // the Hessian kernel's grid follows the tile count
   if (h->tuned.size() == 3) apply_cached_config(h, h->tuned[0], h->tuned[1], h->tuned[2]);
   return PWA_OK;
 }
@@ -1512,6 +1520,235 @@ int pwa_pieces_points(pwa_plan* h, int n_pts, const double* vars, double sw, dou
     if (rc) return rc;
   }
   return PWA_OK;
+}
+
+namespace {
+// Length of the exact-Hessian sums: S0, S1 (2K), two upper triangles of
+// 2K x 2K (the kernel's block row, PWA_HNA).
+long long hess_na(const pwa_plan* h) {
+  const long long W = 2LL * h->ncol;
+  return 1 + W + W * (W + 1);
+}
+
+// Sums of pwa_hess_cached over the whole column cache at column couplings
+// ck, into out[hess_na] (host): the block rows, then pwa_sum_rows in a
+// fixed order.
+int hess_sums(pwa_plan* h, const double* ck, cudaStream_t s, double* out) {
+  const long long NA = hess_na(h);
+  if (!h->hess_blocks) {
+    const int W = 2 * h->ncol, ld4 = (W + 3) / 4 * 4, ld = ld4 % 8 == 0 ? ld4 + 4 : ld4;
+    const size_t smem = ((size_t)NA * 8 + 15) / 16 * 16 +
+                        (size_t)(h->nout + 1) * h->tpb * ld * 4 + 2 * (size_t)h->tpb * 4;
+    int optin = 0;
+    CU(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
+    if (smem > (size_t)optin)
+      return set_err(h, PWA_ERR_STATE, "exact Hessian: the model's columns need " +
+                                           std::to_string(smem) + " B of shared memory per block");
+    CU(cudaFuncSetAttribute((const void*)h->k.hess_cached,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per = 0;
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void*)h->k.hess_cached, h->tpb,
+                                                     smem));
+    if (per < 1) return set_err(h, PWA_ERR_STATE, "exact Hessian kernel does not fit an SM");
+    const long long want = (long long)per * h->sms;
+    if (!h->d_hsum && cudaMalloc(&h->d_hsum, sizeof(double) * NA) != cudaSuccess)
+      return set_err(h, PWA_ERR_OOM, "cudaMalloc of the Hessian sums failed");
+    h->hess_smem = smem;
+    h->hess_blocks = (int)(want < h->ntiles ? want : h->ntiles);
+  }
+  int rc = ensure_partials(h, (long long)h->hess_blocks * NA);
+  if (rc) return rc;
+  std::vector<double> cbuf(ck, ck + 2 * h->ncol);
+  long long nt = h->ntiles;
+  void* args[] = {cbuf.data(), &h->fcache, &h->wcache, &nt, &h->partials};
+  cudaError_t e = cudaLaunchKernel((const void*)h->k.hess_cached, dim3(h->hess_blocks),
+                                   dim3(h->tpb), args, h->hess_smem, s);
+  if (e != cudaSuccess)
+    return set_err(h, PWA_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+  int nrows = h->hess_blocks, ncols = (int)NA;
+  void* a2[] = {&h->partials, &nrows, &ncols, &h->d_hsum};
+  rc = launch(h, h->k.sum_rows, dim3((unsigned)((NA + 7) / 8)), dim3(256), a2, s);
+  if (rc) return rc;
+  CU(cudaMemcpyAsync(out, h->d_hsum, sizeof(double) * NA, cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  return PWA_OK;
+}
+
+// First and second derivatives of coupling j's complex value in its parts
+// (0: magnitude or real part, 1: phase or imaginary part).
+cplx coup_d1(const pwa_plan* h, const double* vars, int j, int part) {
+  const double r = vars[h->coup_r[j]], p = vars[h->coup_i[j]];
+  if (h->coup_polar[j])
+    return part == 0 ? cplx{std::cos(p), std::sin(p)} : cplx{-r * std::sin(p), r * std::cos(p)};
+  return part == 0 ? cplx{1.0, 0.0} : cplx{0.0, 1.0};
+}
+cplx coup_d2(const pwa_plan* h, const double* vars, int j, int p1, int p2) {
+  const double r = vars[h->coup_r[j]], p = vars[h->coup_i[j]];
+  if (!h->coup_polar[j] || (p1 == 0 && p2 == 0)) return {0.0, 0.0};
+  if (p1 == 1 && p2 == 1) return {-r * std::cos(p), -r * std::sin(p)};
+  return {-std::sin(p), std::cos(p)};  // d2/dr dphi of r e^{i phi}
+}
+
+// NLL, gradient and exact Hessian in the trainable coupling parts from the
+// data sums hs (hess_na values) and the MC Gram matrix: with c_a = dc/da,
+// c_ab = d2c/da db (products of the column's couplings),
+//   d2/da db [-sum w t(f)] = -2 Re[(c_b)^H H1 c_a] - 2 Re(c_ab . S1)
+//                            - 4 (Re c_a, Im c_a) H2 (Re c_b, Im c_b)^T,
+//   d2/da db [sw ln I] = sw (d2I / I - dI_a dI_b / I^2),  I = c^H M c,
+//   dI_a = 2 Re(c^H M c_a),  d2I = 2 Re((c_b)^H M c_a + c^H M c_ab).
+int hessian_from_hsums(pwa_plan* h, const double* vars, const std::vector<cplx>& z,
+                       const double* ck, const double* hs, double sw, double* out_nll,
+                       double* out_grad, double* out_hess) {
+  const int K = h->ncol, P = h->n_train, W = 2 * K;
+  std::vector<int> tj(P), tp(P);
+  for (int t = 0; t < P; ++t) {
+    const int v = h->train_idx[t];
+    tj[t] = -1;
+    for (int q = 0; q < h->n_coup && tj[t] < 0; ++q) {
+      if (h->coup_r[q] == v) tj[t] = q, tp[t] = 0;
+      else if (h->coup_i[q] == v) tj[t] = q, tp[t] = 1;
+    }
+    if (tj[t] < 0) return set_err(h, PWA_ERR_ARG, "trainable variable is not a coupling (cached mode)");
+  }
+  std::vector<cplx> dc((size_t)P * K, cplx{0, 0}), d2c((size_t)P * P * K, cplx{0, 0});
+  std::vector<int> facs;
+  for (int k = 0; k < K; ++k) {
+    facs.clear();
+    for (int f = 0; f < h->nfac; ++f)
+      if (h->col_fac[k * h->nfac + f] >= 0) facs.push_back(h->col_fac[k * h->nfac + f]);
+    const int nf = (int)facs.size();
+    auto rest = [&](int skip1, int skip2) {
+      cplx c{1.0, 0.0};
+      for (int m = 0; m < nf; ++m)
+        if (m != skip1 && m != skip2) c = cmulh(c, z[facs[m]]);
+      return c;
+    };
+    for (int a = 0; a < P; ++a)
+      for (int i = 0; i < nf; ++i) {
+        if (facs[i] != tj[a]) continue;
+        const cplx da = coup_d1(h, vars, tj[a], tp[a]);
+        const cplx r1 = rest(i, -1), t1 = cmulh(da, r1);
+        dc[(size_t)a * K + k].r += t1.r;
+        dc[(size_t)a * K + k].i += t1.i;
+        for (int b = 0; b < P; ++b) {
+          cplx& dst = d2c[((size_t)a * P + b) * K + k];
+          if (tj[b] == tj[a]) {
+            const cplx t2 = cmulh(coup_d2(h, vars, tj[a], tp[a], tp[b]), r1);
+            dst.r += t2.r;
+            dst.i += t2.i;
+          }
+          for (int i2 = 0; i2 < nf; ++i2) {
+            if (i2 == i || facs[i2] != tj[b]) continue;
+            const cplx t3 = cmulh(cmulh(da, coup_d1(h, vars, tj[b], tp[b])), rest(i, i2));
+            dst.r += t3.r;
+            dst.i += t3.i;
+          }
+        }
+      }
+  }
+  const double* G1 = hs + 1 + W;
+  const double* G2 = G1 + (size_t)W * (W + 1) / 2;
+  auto up = [W](const double* G, int p, int q) {
+    if (p > q) std::swap(p, q);
+    return G[p * W - p * (p - 1) / 2 + (q - p)];
+  };
+  std::vector<cplx> H1((size_t)K * K), M((size_t)K * K), S1(K), c(K), Mc(K, cplx{0, 0});
+  for (int l = 0; l < K; ++l)
+    for (int k = 0; k < K; ++k) {
+      H1[(size_t)l * K + k] = {up(G1, l, k) + up(G1, K + l, K + k),
+                               up(G1, l, K + k) - up(G1, K + l, k)};
+      M[(size_t)l * K + k] = {h->gram[2 * ((size_t)l * K + k)], h->gram[2 * ((size_t)l * K + k) + 1]};
+    }
+  for (int k = 0; k < K; ++k) {
+    S1[k] = {hs[1 + 2 * k], hs[2 + 2 * k]};
+    c[k] = {ck[2 * k], ck[2 * k + 1]};
+  }
+  double I = 0.0;
+  for (int k = 0; k < K; ++k) {
+    for (int l = 0; l < K; ++l) {
+      const cplx t = cmulh(cplx{c[l].r, -c[l].i}, M[(size_t)l * K + k]);
+      Mc[k].r += t.r;
+      Mc[k].i += t.i;
+    }
+    I += Mc[k].r * c[k].r - Mc[k].i * c[k].i;
+  }
+  if (!(I > 0.0)) return set_err(h, PWA_ERR_STATE, "MC integral is not positive");
+  auto re_dot = [](const cplx* a, const cplx* b, int n) {  // Re sum a_k b_k
+    double s = 0.0;
+    for (int k = 0; k < n; ++k) s += a[k].r * b[k].r - a[k].i * b[k].i;
+    return s;
+  };
+  std::vector<double> dI(P);
+  std::vector<cplx> uH((size_t)P * K), uM((size_t)P * K);  // H1 c_a, M c_a
+  for (int a = 0; a < P; ++a) {
+    const cplx* da = &dc[(size_t)a * K];
+    dI[a] = 2.0 * re_dot(da, Mc.data(), K);
+    out_grad[a] = -2.0 * re_dot(da, S1.data(), K) + sw * dI[a] / I;
+    for (int l = 0; l < K; ++l) {
+      cplx sh{0, 0}, sm{0, 0};
+      for (int k = 0; k < K; ++k) {
+        const cplx th = cmulh(H1[(size_t)l * K + k], da[k]), tm = cmulh(M[(size_t)l * K + k], da[k]);
+        sh.r += th.r, sh.i += th.i, sm.r += tm.r, sm.i += tm.i;
+      }
+      uH[(size_t)a * K + l] = sh;
+      uM[(size_t)a * K + l] = sm;
+    }
+  }
+  for (int a = 0; a < P; ++a)
+    for (int b = 0; b < P; ++b) {
+      const cplx* db = &dc[(size_t)b * K];
+      const cplx* dab = &d2c[((size_t)a * P + b) * K];
+      double qh = 0.0, qm = 0.0, h2 = 0.0;
+      for (int l = 0; l < K; ++l) {  // Re (c_b)^H u
+        qh += db[l].r * uH[(size_t)a * K + l].r + db[l].i * uH[(size_t)a * K + l].i;
+        qm += db[l].r * uM[(size_t)a * K + l].r + db[l].i * uM[(size_t)a * K + l].i;
+      }
+      for (int p = 0; p < W; ++p) {
+        const double xa = p < K ? dc[(size_t)a * K + p].r : dc[(size_t)a * K + p - K].i;
+        double row = 0.0;
+        for (int q = 0; q < W; ++q) row += up(G2, p, q) * (q < K ? db[q].r : db[q - K].i);
+        h2 += xa * row;
+      }
+      const double d2I = 2.0 * (qm + re_dot(dab, Mc.data(), K));
+      out_hess[(size_t)a * P + b] = -2.0 * qh - 2.0 * re_dot(dab, S1.data(), K) - 4.0 * h2 +
+                                    sw * (d2I / I - dI[a] * dI[b] / (I * I));
+    }
+  for (int a = 0; a < P; ++a)
+    for (int b = a + 1; b < P; ++b) {
+      const double m = 0.5 * (out_hess[(size_t)a * P + b] + out_hess[(size_t)b * P + a]);
+      out_hess[(size_t)a * P + b] = out_hess[(size_t)b * P + a] = m;
+    }
+  *out_nll = -hs[0] + sw * std::log(I);
+  return PWA_OK;
+}
+}  // namespace
+
+int pwa_hess_sums_cached(pwa_plan* h, const double* vars, void* stream, double* out) {
+  if (!h) return PWA_ERR_ARG;
+  if (!vars || !out) return set_err(h, PWA_ERR_ARG, "null argument");
+  if (h->fcache_n <= 0) return set_err(h, PWA_ERR_STATE, "no column cache (call pwa_cache_data)");
+  if (h->n_coup == 0) return set_err(h, PWA_ERR_STATE, "parameter layout not set");
+  std::vector<cplx> z;
+  std::vector<double> ck(2 * h->ncol);
+  column_couplings(h, vars, &z, ck.data());
+  return hess_sums(h, ck.data(), (cudaStream_t)stream, out);
+}
+
+int pwa_hessian_cached_exact(pwa_plan* h, const double* vars, double sw, void* stream,
+                             double* out_nll, double* out_grad, double* out_hess) {
+  if (!h) return PWA_ERR_ARG;
+  const int P = h->n_train;
+  if (!vars || !out_nll || (P && (!out_grad || !out_hess)))
+    return set_err(h, PWA_ERR_ARG, "invalid hessian arguments");
+  if (h->fcache_n <= 0) return set_err(h, PWA_ERR_STATE, "no column cache (call pwa_cache_data)");
+  if (h->n_coup == 0) return set_err(h, PWA_ERR_STATE, "parameter layout not set");
+  if (!h->gram_valid) return set_err(h, PWA_ERR_STATE, "MC Gram matrix not built");
+  std::vector<cplx> z;
+  std::vector<double> ck(2 * h->ncol), hs((size_t)hess_na(h));
+  column_couplings(h, vars, &z, ck.data());
+  int rc = hess_sums(h, ck.data(), (cudaStream_t)stream, hs.data());
+  if (rc) return rc;
+  return hessian_from_hsums(h, vars, z, ck.data(), hs.data(), sw, out_nll, out_grad, out_hess);
 }
 
 int pwa_nll_grad_cached(pwa_plan* h, const double* vars, double sw, void* stream,

@@ -91,6 +91,8 @@ def load_library(path=LIB_PATH):
     lib.pwa_toy_select.argtypes = [vp, dp, ull, ll, ll, ctypes.c_double, i, vp, vp]
     lib.pwa_toy_fields.argtypes = [vp, ull, vp, ll, vp, ll, vp, ll, vp]
     lib.pwa_hessian_cached.argtypes = [vp, dp, ctypes.c_double, ctypes.c_double, vp, dp, dp, dp]
+    lib.pwa_hessian_cached_exact.argtypes = [vp, dp, ctypes.c_double, vp, dp, dp, dp]
+    lib.pwa_hess_sums_cached.argtypes = [vp, dp, vp, dp]
     lib.pwa_read_dat.argtypes = [cp, vp, ll, ctypes.POINTER(ll)]
     lib.pwa_server_create.argtypes = [vp, dp, dp, i, ctypes.c_double, i, ctypes.POINTER(vp)]
     lib.pwa_server_submit.argtypes = [vp, dp, vp, vp, vp, ll, ll, ctypes.POINTER(ll)]
@@ -125,7 +127,8 @@ EXPORTED = ("pwa_plan_create", "pwa_plan_destroy", "pwa_compile_only", "pwa_prec
             "pwa_nll_grad_cached", "pwa_set_cached_variant", "pwa_pool_reserve",
             "pwa_pool_alloc", "pwa_pool_free", "pwa_pool_fill", "pwa_pieces_multi",
             "pwa_eval_noalloc", "pwa_fields_from_p4", "pwa_toy_select", "pwa_toy_fields",
-            "pwa_hessian_cached", "pwa_read_dat", "pwa_server_create", "pwa_server_submit",
+            "pwa_hessian_cached", "pwa_hessian_cached_exact", "pwa_hess_sums_cached",
+            "pwa_read_dat", "pwa_server_create", "pwa_server_submit",
             "pwa_server_result", "pwa_server_stats", "pwa_server_destroy",
             "pwa_plan_info", "pwa_last_error")
 
@@ -992,6 +995,32 @@ class Engine:
                                                       stream or 0, ctypes.byref(nll), _dptr(g),
                                                       _dptr(H)), "pwa_hessian_cached")
         return nll.value, g, H
+
+    def hessian_cached_exact(self, var_values, stream=None):
+        """(nll, grad, Hessian) of the cached form with the exact Hessian in
+        the coupling parts: one pass of the Hessian-sums kernel over the
+        column cache, then the MC term and the coupling derivatives on the
+        host (pwa_hessian_cached_exact)."""
+        v = np.ascontiguousarray(var_values, np.float64)
+        P = self._n_train
+        nll = ctypes.c_double()
+        g = np.zeros(P)
+        H = np.zeros((P, P))
+        self._check(load_library().pwa_hessian_cached_exact(self.h, _dptr(v), self._sw,
+                                                            stream or 0, ctypes.byref(nll),
+                                                            _dptr(g), _dptr(H)),
+                    "pwa_hessian_cached_exact")
+        return nll.value, g, H
+
+    def hess_sums_cached(self, var_values, stream=None):
+        """The data sums of the exact Hessian (pwa_hess_sums_cached):
+        S0, S1 (re, im per column), upper triangles of the two 2K x 2K sums."""
+        v = np.ascontiguousarray(var_values, np.float64)
+        W = 2 * self.code.ncol
+        out = np.zeros(1 + W + W * (W + 1))
+        self._check(load_library().pwa_hess_sums_cached(self.h, _dptr(v), stream or 0,
+                                                        _dptr(out)), "pwa_hess_sums_cached")
+        return out
 
     # ------------------------------------------------------------ dataset step
     def fields_from_p4(self, p4, charge=None):
