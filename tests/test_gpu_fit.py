@@ -182,15 +182,15 @@ def test_multi_point_pass_matches_single_points(name):
     fm.eng.close()
 
 
-EXACT_CASES = ["d2kpipi", "lc2pkpi", "dp2kpipi_ident", "ident_fermions", "toy_vvp", "b2dstkpi"]
+EXACT_CASES = ["d2kpipi", "lc2pkpi", "dp2kpipi_ident", "ident_fermions", "b2dstkpi"]
 
 
 @pytest.mark.parametrize("name", EXACT_CASES)
 def test_exact_hessian_sums_match_oracle(name):
     """The Hessian-sums kernel (pwa_hess_sums_cached) against the oracle's
-    FP64 sums from the same columns: S0 to 1e-9, the gradient sum and both
-    2K x 2K sums to 1e-5 of their largest entry (FP32 columns and products,
-    FP64 across tiles)."""
+    FP64 sums from the FP64 columns: S0 to 1e-7 (the cached columns are FP32,
+    as in the mixed form's NLL), the gradient sum and both 2K x 2K sums to
+    1e-5 of their largest entry (FP32 products, FP64 across tiles)."""
     from oracle.pwa_oracle import OracleModel, hessian_sums
     from common import load_model
 
@@ -204,7 +204,7 @@ def test_exact_hessian_sums_match_oracle(name):
                                          meta["variables"], {})
     K = len(S1)
     W = 2 * K
-    assert abs(hs[0] - S0) <= 1e-9 * abs(S0)
+    assert abs(hs[0] - S0) <= 1e-7 * abs(S0)
     s1 = hs[1:1 + W].reshape(K, 2)
     ref1 = np.stack([S1.real, S1.imag], 1)
     np.testing.assert_allclose(s1, ref1, rtol=0, atol=1e-5 * np.abs(ref1).max())
@@ -225,12 +225,12 @@ def test_exact_hessian_sums_match_oracle(name):
 def test_exact_hessian_matches_reference(name):
     """FCN.nll_grad_hessian in the cached form (exact Hessian in the
     couplings, one pass) against the reference's nested-tape Hessian on the
-    golden events: NLL 1e-9, gradient and Hessian 1e-5 of their largest
-    entry (FP32 columns)."""
+    golden events: NLL 1e-7 relative, gradient and Hessian 1e-5 of their
+    largest entry (FP32 columns)."""
     cl, fm, g, meta = _fcn(name, "mixed")
     assert fm.use_gram
     nll, grad, H = fm.nll_grad_hessian()
-    assert abs(nll - g["hess_nll"]) <= 1e-9 * abs(g["hess_nll"])
+    assert abs(nll - g["hess_nll"]) <= 1e-7 * abs(g["hess_nll"])
     np.testing.assert_allclose(grad, g["hess_grad"], rtol=0,
                                atol=1e-5 * np.abs(g["hess_grad"]).max())
     np.testing.assert_allclose(H, g["hess"], rtol=0, atol=1e-5 * np.abs(g["hess"]).max())
@@ -258,3 +258,24 @@ def test_exact_hessian_large_matches_plain_stencil():
     np.testing.assert_allclose(H, H_p, rtol=0, atol=1e-4 * np.abs(H_p).max())
     fm.eng.close()
     fp.eng.close()
+
+
+def test_wide_model_hessian_falls_back_to_stencil():
+    """toy_vvp (spin-1 finals: 18 columns x 18 helicity outputs) has per-tile
+    rows larger than a block's shared memory: the exact-sums kernel refuses
+    with PWA_ERR_STATE, the cached form's evaluation runs the non-ring
+    variants, and FCN.nll_grad_hessian falls back to the 4-point stencil,
+    which matches the reference's Hessian to 1e-4 of its largest entry."""
+    from tf_pwa_b200.engine import PWAError
+
+    cl, fm, g, meta = _fcn("toy_vvp", "mixed")
+    assert fm.use_gram
+    v = fm.vm.variables
+    with pytest.raises(PWAError, match="shared memory"):
+        fm.eng.hess_sums_cached([v[k] for k in fm._var_names])
+    nll, grad, H = fm.nll_grad_hessian()
+    assert abs(nll - g["hess_nll"]) < 1e-3
+    np.testing.assert_allclose(grad, g["hess_grad"], rtol=0,
+                               atol=1e-4 * np.abs(g["hess_grad"]).max())
+    np.testing.assert_allclose(H, g["hess"], rtol=0, atol=1e-4 * np.abs(g["hess"]).max())
+    fm.eng.close()

@@ -310,6 +310,8 @@ class FCN:
         widths) with no ``step``: the exact Hessian in the couplings from
         one pass over the column cache (``pwa_hessian_cached_exact``; the
         reference's nested-tape Hessian, ``tf_pwa/model/model.py:513-561``).
+        (Models whose per-tile rows do not fit in a block's shared memory,
+        e.g. 18 columns x 18 helicity outputs, fall back to the stencil.)
         Otherwise by differencing the adjoint gradient: 4-point central
         stencil per parameter, h_i = step * max(|x_i|, 1e-2) (error O(h^4)),
         symmetrised.  Default step: 1e-4 in the plain form; 1e-2 in the
@@ -321,7 +323,13 @@ class FCN:
         self._set(x)
         if self.use_gram and step is None and self.eng.dist_reduce is None:
             v = self.vm.variables
-            return self.eng.hessian_cached_exact([v[k] for k in self._var_names])
+            try:
+                return self.eng.hessian_cached_exact([v[k] for k in self._var_names])
+            except PWAError as e:
+                # models whose per-tile rows (2 x columns x helicity outputs)
+                # exceed a block's shared memory take the stencil below
+                if "shared memory" not in str(e):
+                    raise
         if step is None:
             step = 1e-4 if self.precision == PLAIN_F64 else 1e-2
         if self.use_gram:
@@ -714,8 +722,9 @@ class ConfigLoader:
                          correct_params=None, fcn=None):
         """Errors from the inverse Hessian in FP64 (``config_loader.py:814-873``,
         ``applications.py:249-309``): with ``using_cached`` the last inverse
-        Hessian is reused; otherwise the Hessian (differenced adjoint
-        gradients) is inverted -- made positive definite first with
+        Hessian is reused; otherwise the Hessian of ``FCN.nll_grad_hessian``
+        (exact in the cached form, differenced adjoint gradients otherwise)
+        is inverted -- made positive definite first with
         ``force_pos`` (``force_pos_def``), else by pseudo-inverse.  The
         errors are also stored on the last fit's result."""
         if inmc is not None or correct_params:

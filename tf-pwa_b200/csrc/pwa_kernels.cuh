@@ -1703,7 +1703,10 @@ extern "C" __global__ void __launch_bounds__(PWA_PTS_WARPS * 32, 1)
 // computes its event's A (FP64), f, t, t', t'' and G (FP32) and writes its
 // rows of X1 and X2 to shared memory; then each thread accumulates its
 // items -- (matrix, PWA_HBS x PWA_HBS block of the upper triangle, range of
-// rows) -- over the tile in FP32 and adds them to FP64 registers.  The
+// rows) -- over the tile in FP32 and adds them to FP64 registers.  While it
+// does, the next tile's columns of its own event are already on their way
+// into a shared-memory stage (per-thread cp.async of 8-byte values, the
+// tile's own layout), so the loads overlap the outer products.  The
 // block row of partials is [S0, S1 (re, im per column), H1 upper entries,
 // H2 upper entries] (upper entry (p, q), p <= q, at p W - p (p - 1) / 2 +
 // q - p); rows of several splits of one block are added in split order, so
@@ -1738,18 +1741,28 @@ __device__ __forceinline__ void hess_store_row(float* dst, const float (&row)[PW
     *(float4*)(dst + 4 * q) = make_float4(row[4 * q], row[4 * q + 1], row[4 * q + 2], row[4 * q + 3]);
 }
 
-extern "C" __global__ void __launch_bounds__(PWA_TPB, 2)
+#ifndef PWA_HESS_MINB
+#define PWA_HESS_MINB 2
+#endif
+extern "C" __global__ void __launch_bounds__(PWA_TPB, PWA_HESS_MINB)
     pwa_hess_cached(const CCoup c, const float2* __restrict__ Fc,
                     const double* __restrict__ Wc, long long ntiles,
                     double* __restrict__ partials) {
   constexpr int K = PWA_NCOL, W = PWA_HW, BS = PWA_HBS, LD = PWA_HLD;
   constexpr int R1 = PWA_NOUT * PWA_TPB;
+  // rows region (X1, X2; the final row buffer reuses it), then s1, s2 and
+  // the stage of the next tile
+  constexpr unsigned ROWS_B = (R1 + PWA_TPB) * LD * 4;
+  constexpr unsigned NA_B = (PWA_HNA * 8 + 15) / 16 * 16;
+  constexpr unsigned REG_B = ROWS_B > NA_B ? ROWS_B : NA_B;
   extern __shared__ __align__(16) unsigned char hess_smem[];
-  double* row_acc = (double*)hess_smem;                                  // [PWA_HNA]
-  float* X1 = (float*)(hess_smem + (PWA_HNA * 8 + 15) / 16 * 16);        // [R1][LD]
+  float* X1 = (float*)hess_smem;                                          // [R1][LD]
   float* X2 = X1 + R1 * LD;                                               // [TPB][LD]
-  float* s1 = X2 + PWA_TPB * LD;                                          // [TPB]
+  float* s1 = (float*)(hess_smem + REG_B);                                // [TPB]
   float* s2 = s1 + PWA_TPB;                                               // [TPB]
+  float2* stF = (float2*)(s2 + PWA_TPB);                                  // [NF][TPB]
+  double* stW = (double*)(stF + PWA_NF * PWA_TPB);                        // [TPB]
+  double* row_acc = (double*)hess_smem;  // [PWA_HNA], over X1 / X2 after the last tile
   __shared__ double s_c[2 * PWA_NCOL];
   __shared__ double s_red[PWA_TPB / 32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -1777,14 +1790,22 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, 2)
   double acc_s0 = 0.0, acc_s1 = 0.0;
   const long long B = gridDim.x, b = blockIdx.x;
   const long long t0 = b * ntiles / B, t1 = (b + 1) * ntiles / B;
+  auto stage = [&](long long t) {  // this thread's event of tile t -> stage
+    const float2* F = Fc + t * PWA_NF * PWA_TPB + tid;
+#pragma unroll
+    for (int j = 0; j < PWA_NF; ++j) cp_async8(stF + j * PWA_TPB + tid, F + j * PWA_TPB);
+    cp_async8(stW + tid, Wc + t * PWA_TPB + tid);
+    cp_async_commit();
+  };
+  if (t0 < t1) stage(t0);
 #pragma unroll 1
   for (long long t = t0; t < t1; ++t) {
     {  // this thread's event: amplitude, clip_log derivatives, G, rows
-      const float2* F = Fc + t * PWA_NF * PWA_TPB + tid;
+      cp_async_wait_all();
       float2 v[PWA_NF];
 #pragma unroll
-      for (int j = 0; j < PWA_NF; ++j) v[j] = __ldcs(F + j * PWA_TPB);
-      const double w = __ldcs(Wc + t * PWA_TPB + tid);
+      for (int j = 0; j < PWA_NF; ++j) v[j] = stF[j * PWA_TPB + tid];
+      const double w = stW[tid];
       double ar[PWA_NOUT], ai[PWA_NOUT];
 #pragma unroll
       for (int o = 0; o < PWA_NOUT; ++o) ar[o] = ai[o] = 0.0;
@@ -1829,6 +1850,7 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, 2)
       s2[tid] = (float)(w * d2);
     }
     __syncthreads();
+    if (t + 1 < t1) stage(t + 1);  // this thread's stage slots are read
 #pragma unroll
     for (int q = 0; q < PWA_HIPT; ++q) {
       if (it_m[q] < 0) continue;
@@ -1862,11 +1884,10 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, 2)
 #pragma unroll
         for (int j = 0; j < BS; ++j) hacc[q][i][j] += (double)a[i][j];
     }
-    if (tid < W) {  // S1 = sum s1 G (X2 holds -Im G in columns K .. 2K-1)
-      float a = 0.f;
+    if (tid < W) {  // S1 = sum s1 G in FP64 (X2 holds -Im G in columns K .. 2K-1)
 #pragma unroll 4
-      for (int e = 0; e < PWA_TPB; ++e) a = fmaf(s1[e], X2[e * LD + tid], a);
-      acc_s1 += (double)a;
+      for (int e = 0; e < PWA_TPB; ++e)
+        acc_s1 = fma((double)s1[e], (double)X2[e * LD + tid], acc_s1);
     }
     __syncthreads();
   }

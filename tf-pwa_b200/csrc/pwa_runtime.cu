@@ -794,18 +794,23 @@ int pwa_cache_data(pwa_plan* h, const double* consts, void* stream) {
   int rc = launch(h, h->k.cache_f32, dim3((int)nb), dim3(h->tpb), args, s);
   if (rc) return rc;
   // streaming kernel: PWA_STAGES tiles of (nf float2 + 1 double) per event in
-  // shared memory per block
+  // shared memory per block.  The ring variants (0, 3) exist only where their
+  // tiles fit in a block's shared memory (0 blocks otherwise; launches of
+  // them then run variant 2)
+  int smem_optin = 0;
+  CU(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
   const int stages = 3;
   h->cached_smem = (size_t)stages * tile * (h->nf * sizeof(float2) + sizeof(double));
-  CU(cudaFuncSetAttribute((const void*)h->k.eval_cached,
-                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->cached_smem));
-  int per_sm = 0;
-  CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)h->k.eval_cached, h->tpb,
-                                                   h->cached_smem));
-  if (per_sm < 1)
-    return set_err(h, PWA_ERR_ARG, "column tile does not fit in shared memory");
-  long long want = (long long)per_sm * h->sms;
-  h->cached_blocks = (int)(want < ntiles ? want : ntiles);
+  h->cached_blocks = 0;
+  if (h->cached_smem + 2048 <= (size_t)smem_optin) {
+    CU(cudaFuncSetAttribute((const void*)h->k.eval_cached,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->cached_smem));
+    int per_sm = 0;
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)h->k.eval_cached,
+                                                     h->tpb, h->cached_smem));
+    const long long want = (long long)per_sm * h->sms;
+    h->cached_blocks = (int)(want < ntiles ? want : ntiles);
+  }
   int per_sm2 = 0;
   CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, (const void*)h->k.eval_cached_direct,
                                                    h->tpb, 0));
@@ -822,14 +827,17 @@ int pwa_cache_data(pwa_plan* h, const double* consts, void* stream) {
   h->cached_blocks_wred = (int)(want3 < ntiles ? want3 : ntiles);
   // ring with register-light consumers: 2 stages (PWA_RSTAGES) per block
   h->cached_smem_ring2 = (size_t)2 * tile * (h->nf * sizeof(float2) + sizeof(double));
-  CU(cudaFuncSetAttribute((const void*)h->k.eval_cached_ring2,
-                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->cached_smem_ring2));
-  int per_sm4 = 0;
-  CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm4, (const void*)h->k.eval_cached_ring2,
-                                                   h->tpb, h->cached_smem_ring2));
-  if (per_sm4 < 1) return set_err(h, PWA_ERR_ARG, "column tile does not fit in shared memory");
-  long long want4 = (long long)per_sm4 * h->sms;
-  h->cached_blocks_ring2 = (int)(want4 < ntiles ? want4 : ntiles);
+  h->cached_blocks_ring2 = 0;
+  if (h->cached_smem_ring2 + 2048 <= (size_t)smem_optin) {
+    CU(cudaFuncSetAttribute((const void*)h->k.eval_cached_ring2,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)h->cached_smem_ring2));
+    int per_sm4 = 0;
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm4, (const void*)h->k.eval_cached_ring2,
+                                                     h->tpb, h->cached_smem_ring2));
+    const long long want4 = (long long)per_sm4 * h->sms;
+    h->cached_blocks_ring2 = (int)(want4 < ntiles ? want4 : ntiles);
+  }
   // one block per SM (variants 4, 5): block size from the kernels' own
   // launch bounds, ring depth from the shared memory left beside the
   // static arrays
@@ -889,6 +897,8 @@ int pwa_eval_cached_enqueue(pwa_plan* h, const double* ck, void* stream) {
                   &seq, &h->tma_stages};
   int variant = h->cached_variant >= 0 ? h->cached_variant : 2;
   if (variant == 5 && h->cached_blocks_tma == 0) variant = 4;  // ring does not fit
+  if ((variant == 0 && h->cached_blocks == 0) || (variant == 3 && h->cached_blocks_ring2 == 0))
+    variant = 2;  // tiles do not fit in shared memory
   cudaError_t e =
       variant == 4   ? cudaLaunchKernel((const void*)h->k.eval_cached_wide,
                                         dim3(h->cached_blocks_wide), dim3(h->wide_threads), args,
@@ -1033,8 +1043,8 @@ int pwa_autotune_cached(pwa_plan* h, const double* ck, int reps, void* stream, i
   if (h->cached_blocks_tma > 0)
     for (int st = 2 * kTmaGroups; st <= h->tma_stages_max; st += kTmaGroups)
       cands.push_back({5, st, 0});
-  cands.push_back({0, 0, 0});
-  cands.push_back({3, 0, 0});
+  if (h->cached_blocks > 0) cands.push_back({0, 0, 0});
+  if (h->cached_blocks_ring2 > 0) cands.push_back({3, 0, 0});
   if ((int)cands.size() > 32) cands.resize(32);
   {
     const cudaError_t e = cudaStreamSynchronize(s);
@@ -1537,8 +1547,10 @@ int hess_sums(pwa_plan* h, const double* ck, cudaStream_t s, double* out) {
   const long long NA = hess_na(h);
   if (!h->hess_blocks) {
     const int W = 2 * h->ncol, ld4 = (W + 3) / 4 * 4, ld = ld4 % 8 == 0 ? ld4 + 4 : ld4;
-    const size_t smem = ((size_t)NA * 8 + 15) / 16 * 16 +
-                        (size_t)(h->nout + 1) * h->tpb * ld * 4 + 2 * (size_t)h->tpb * 4;
+    // X1, X2 (the final row buffer reuses them), s1, s2, the next tile's stage
+    const size_t rows = (size_t)(h->nout + 1) * h->tpb * ld * 4;
+    const size_t smem = (rows > (size_t)NA * 8 ? rows : ((size_t)NA * 8 + 15) / 16 * 16) +
+                        2 * (size_t)h->tpb * 4 + (size_t)h->tpb * (h->nf * 8 + 8);
     int optin = 0;
     CU(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
     if (smem > (size_t)optin)
@@ -1610,42 +1622,7 @@ int hessian_from_hsums(pwa_plan* h, const double* vars, const std::vector<cplx>&
     }
     if (tj[t] < 0) return set_err(h, PWA_ERR_ARG, "trainable variable is not a coupling (cached mode)");
   }
-  std::vector<cplx> dc((size_t)P * K, cplx{0, 0}), d2c((size_t)P * P * K, cplx{0, 0});
-  std::vector<int> facs;
-  for (int k = 0; k < K; ++k) {
-    facs.clear();
-    for (int f = 0; f < h->nfac; ++f)
-      if (h->col_fac[k * h->nfac + f] >= 0) facs.push_back(h->col_fac[k * h->nfac + f]);
-    const int nf = (int)facs.size();
-    auto rest = [&](int skip1, int skip2) {
-      cplx c{1.0, 0.0};
-      for (int m = 0; m < nf; ++m)
-        if (m != skip1 && m != skip2) c = cmulh(c, z[facs[m]]);
-      return c;
-    };
-    for (int a = 0; a < P; ++a)
-      for (int i = 0; i < nf; ++i) {
-        if (facs[i] != tj[a]) continue;
-        const cplx da = coup_d1(h, vars, tj[a], tp[a]);
-        const cplx r1 = rest(i, -1), t1 = cmulh(da, r1);
-        dc[(size_t)a * K + k].r += t1.r;
-        dc[(size_t)a * K + k].i += t1.i;
-        for (int b = 0; b < P; ++b) {
-          cplx& dst = d2c[((size_t)a * P + b) * K + k];
-          if (tj[b] == tj[a]) {
-            const cplx t2 = cmulh(coup_d2(h, vars, tj[a], tp[a], tp[b]), r1);
-            dst.r += t2.r;
-            dst.i += t2.i;
-          }
-          for (int i2 = 0; i2 < nf; ++i2) {
-            if (i2 == i || facs[i2] != tj[b]) continue;
-            const cplx t3 = cmulh(cmulh(da, coup_d1(h, vars, tj[b], tp[b])), rest(i, i2));
-            dst.r += t3.r;
-            dst.i += t3.i;
-          }
-        }
-      }
-  }
+  // sums of the data pass and the MC Gram matrix
   const double* G1 = hs + 1 + W;
   const double* G2 = G1 + (size_t)W * (W + 1) / 2;
   auto up = [W](const double* G, int p, int q) {
@@ -1673,12 +1650,49 @@ int hessian_from_hsums(pwa_plan* h, const double* vars, const std::vector<cplx>&
     I += Mc[k].r * c[k].r - Mc[k].i * c[k].i;
   }
   if (!(I > 0.0)) return set_err(h, PWA_ERR_STATE, "MC integral is not positive");
+  std::fill(out_hess, out_hess + (size_t)P * P, 0.0);
+  // first and second derivatives of the column couplings: per column, the
+  // trainable parts among its factors; d2c terms go straight into H
+  std::vector<cplx> dc((size_t)P * K, cplx{0, 0});
+  std::vector<int> facs;
+  std::vector<std::pair<int, int>> occ;  // (trainable, factor position)
+  for (int k = 0; k < K; ++k) {
+    facs.clear();
+    for (int f = 0; f < h->nfac; ++f)
+      if (h->col_fac[k * h->nfac + f] >= 0) facs.push_back(h->col_fac[k * h->nfac + f]);
+    const int nf = (int)facs.size();
+    occ.clear();
+    for (int i = 0; i < nf; ++i)
+      for (int a = 0; a < P; ++a)
+        if (tj[a] == facs[i]) occ.push_back({a, i});
+    auto rest = [&](int skip1, int skip2) {
+      cplx r{1.0, 0.0};
+      for (int m = 0; m < nf; ++m)
+        if (m != skip1 && m != skip2) r = cmulh(r, z[facs[m]]);
+      return r;
+    };
+    for (const auto& oa : occ) {
+      const int a = oa.first, i = oa.second;
+      const cplx da = coup_d1(h, vars, tj[a], tp[a]), r1 = rest(i, -1);
+      const cplx t1 = cmulh(da, r1);
+      dc[(size_t)a * K + k].r += t1.r;
+      dc[(size_t)a * K + k].i += t1.i;
+      for (const auto& ob : occ) {
+        const int b = ob.first, i2 = ob.second;
+        const cplx d2 = i2 == i ? cmulh(coup_d2(h, vars, tj[a], tp[a], tp[b]), r1)
+                                : cmulh(cmulh(da, coup_d1(h, vars, tj[b], tp[b])), rest(i, i2));
+        // -2 Re(c_ab S1) + sw 2 Re(c^H M c_ab) / I
+        out_hess[(size_t)a * P + b] += -2.0 * (d2.r * S1[k].r - d2.i * S1[k].i) +
+                                       sw * 2.0 * (d2.r * Mc[k].r - d2.i * Mc[k].i) / I;
+      }
+    }
+  }
   auto re_dot = [](const cplx* a, const cplx* b, int n) {  // Re sum a_k b_k
     double s = 0.0;
     for (int k = 0; k < n; ++k) s += a[k].r * b[k].r - a[k].i * b[k].i;
     return s;
   };
-  std::vector<double> dI(P);
+  std::vector<double> dI(P), Ch((size_t)P * W), T((size_t)W * P), G2f((size_t)W * W);
   std::vector<cplx> uH((size_t)P * K), uM((size_t)P * K);  // H1 c_a, M c_a
   for (int a = 0; a < P; ++a) {
     const cplx* da = &dc[(size_t)a * K];
@@ -1693,25 +1707,27 @@ int hessian_from_hsums(pwa_plan* h, const double* vars, const std::vector<cplx>&
       uH[(size_t)a * K + l] = sh;
       uM[(size_t)a * K + l] = sm;
     }
+    for (int p = 0; p < W; ++p) Ch[(size_t)a * W + p] = p < K ? da[p].r : da[p - K].i;
   }
+  for (int p = 0; p < W; ++p)
+    for (int q = 0; q < W; ++q) G2f[(size_t)p * W + q] = up(G2, p, q);
+  for (int p = 0; p < W; ++p)  // T = H2 Ch^T
+    for (int b = 0; b < P; ++b) {
+      double t = 0.0;
+      for (int q = 0; q < W; ++q) t += G2f[(size_t)p * W + q] * Ch[(size_t)b * W + q];
+      T[(size_t)p * P + b] = t;
+    }
   for (int a = 0; a < P; ++a)
     for (int b = 0; b < P; ++b) {
       const cplx* db = &dc[(size_t)b * K];
-      const cplx* dab = &d2c[((size_t)a * P + b) * K];
       double qh = 0.0, qm = 0.0, h2 = 0.0;
       for (int l = 0; l < K; ++l) {  // Re (c_b)^H u
         qh += db[l].r * uH[(size_t)a * K + l].r + db[l].i * uH[(size_t)a * K + l].i;
         qm += db[l].r * uM[(size_t)a * K + l].r + db[l].i * uM[(size_t)a * K + l].i;
       }
-      for (int p = 0; p < W; ++p) {
-        const double xa = p < K ? dc[(size_t)a * K + p].r : dc[(size_t)a * K + p - K].i;
-        double row = 0.0;
-        for (int q = 0; q < W; ++q) row += up(G2, p, q) * (q < K ? db[q].r : db[q - K].i);
-        h2 += xa * row;
-      }
-      const double d2I = 2.0 * (qm + re_dot(dab, Mc.data(), K));
-      out_hess[(size_t)a * P + b] = -2.0 * qh - 2.0 * re_dot(dab, S1.data(), K) - 4.0 * h2 +
-                                    sw * (d2I / I - dI[a] * dI[b] / (I * I));
+      for (int p = 0; p < W; ++p) h2 += Ch[(size_t)a * W + p] * T[(size_t)p * P + b];
+      out_hess[(size_t)a * P + b] += -2.0 * qh - 4.0 * h2 +
+                                     sw * (2.0 * qm / I - dI[a] * dI[b] / (I * I));
     }
   for (int a = 0; a < P; ++a)
     for (int b = a + 1; b < P; ++b) {
