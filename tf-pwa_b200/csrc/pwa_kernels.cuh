@@ -1742,7 +1742,12 @@ __device__ __forceinline__ void hess_store_row(float* dst, const float (&row)[PW
 }
 
 #ifndef PWA_HESS_MINB
-#define PWA_HESS_MINB 2
+#define PWA_HESS_MINB 3
+#endif
+// 1: the next tile is staged by cp.async while the outer products run (the
+// host reserves the stage when the model source defines this to 1)
+#ifndef PWA_HESS_STAGE
+#define PWA_HESS_STAGE 0
 #endif
 extern "C" __global__ void __launch_bounds__(PWA_TPB, PWA_HESS_MINB)
     pwa_hess_cached(const CCoup c, const float2* __restrict__ Fc,
@@ -1787,9 +1792,15 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, PWA_HESS_MINB)
 #pragma unroll
       for (int j = 0; j < BS; ++j) hacc[q][i][j] = 0.0;
   }
-  double acc_s0 = 0.0, acc_s1 = 0.0;
+  // S1 (FP64, four interleaved chains) on the last threads, which hold the
+  // fewest items: column c = PWA_TPB - 1 - tid + q PWA_TPB
+  constexpr int NS1 = (W + PWA_TPB - 1) / PWA_TPB;
+  double acc_s0 = 0.0, acc_s1[NS1];
+#pragma unroll
+  for (int q = 0; q < NS1; ++q) acc_s1[q] = 0.0;
   const long long B = gridDim.x, b = blockIdx.x;
   const long long t0 = b * ntiles / B, t1 = (b + 1) * ntiles / B;
+#if PWA_HESS_STAGE
   auto stage = [&](long long t) {  // this thread's event of tile t -> stage
     const float2* F = Fc + t * PWA_NF * PWA_TPB + tid;
 #pragma unroll
@@ -1798,14 +1809,22 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, PWA_HESS_MINB)
     cp_async_commit();
   };
   if (t0 < t1) stage(t0);
+#endif
 #pragma unroll 1
   for (long long t = t0; t < t1; ++t) {
     {  // this thread's event: amplitude, clip_log derivatives, G, rows
-      cp_async_wait_all();
       float2 v[PWA_NF];
+#if PWA_HESS_STAGE
+      cp_async_wait_all();
 #pragma unroll
       for (int j = 0; j < PWA_NF; ++j) v[j] = stF[j * PWA_TPB + tid];
       const double w = stW[tid];
+#else
+      const float2* F = Fc + t * PWA_NF * PWA_TPB + tid;
+#pragma unroll
+      for (int j = 0; j < PWA_NF; ++j) v[j] = __ldcs(F + j * PWA_TPB);
+      const double w = __ldcs(Wc + t * PWA_TPB + tid);
+#endif
       double ar[PWA_NOUT], ai[PWA_NOUT];
 #pragma unroll
       for (int o = 0; o < PWA_NOUT; ++o) ar[o] = ai[o] = 0.0;
@@ -1850,7 +1869,9 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, PWA_HESS_MINB)
       s2[tid] = (float)(w * d2);
     }
     __syncthreads();
+#if PWA_HESS_STAGE
     if (t + 1 < t1) stage(t + 1);  // this thread's stage slots are read
+#endif
 #pragma unroll
     for (int q = 0; q < PWA_HIPT; ++q) {
       if (it_m[q] < 0) continue;
@@ -1884,10 +1905,19 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, PWA_HESS_MINB)
 #pragma unroll
         for (int j = 0; j < BS; ++j) hacc[q][i][j] += (double)a[i][j];
     }
-    if (tid < W) {  // S1 = sum s1 G in FP64 (X2 holds -Im G in columns K .. 2K-1)
-#pragma unroll 4
-      for (int e = 0; e < PWA_TPB; ++e)
-        acc_s1 = fma((double)s1[e], (double)X2[e * LD + tid], acc_s1);
+#pragma unroll
+    for (int q = 0; q < NS1; ++q) {  // S1 = sum s1 G (X2: -Im G in columns K .. 2K-1)
+      const int col = PWA_TPB - 1 - tid + q * PWA_TPB;
+      if (col >= W) continue;
+      double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+#pragma unroll 2
+      for (int e = 0; e < PWA_TPB; e += 4) {
+        a0 = fma((double)s1[e], (double)X2[e * LD + col], a0);
+        a1 = fma((double)s1[e + 1], (double)X2[(e + 1) * LD + col], a1);
+        a2 = fma((double)s1[e + 2], (double)X2[(e + 2) * LD + col], a2);
+        a3 = fma((double)s1[e + 3], (double)X2[(e + 3) * LD + col], a3);
+      }
+      acc_s1[q] += (a0 + a1) + (a2 + a3);
     }
     __syncthreads();
   }
@@ -1902,7 +1932,11 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, PWA_HESS_MINB)
     for (int w2 = 0; w2 < PWA_TPB / 32; ++w2) a += s_red[w2];
     row_acc[0] = a;
   }
-  if (tid < W) row_acc[1 + (tid < K ? 2 * tid : 2 * (tid - K) + 1)] = tid < K ? acc_s1 : -acc_s1;
+#pragma unroll
+  for (int q = 0; q < NS1; ++q) {
+    const int col = PWA_TPB - 1 - tid + q * PWA_TPB;
+    if (col < W) row_acc[1 + (col < K ? 2 * col : 2 * (col - K) + 1)] = col < K ? acc_s1[q] : -acc_s1[q];
+  }
   for (int spl = 0; spl < PWA_HSP1; ++spl) {
     __syncthreads();
 #pragma unroll

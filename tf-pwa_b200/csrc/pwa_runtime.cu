@@ -113,6 +113,7 @@ struct pwa_plan {
   // exact coupling Hessian: launch geometry (0 blocks: not set up) and sums
   int hess_blocks = 0;
   size_t hess_smem = 0;
+  bool hess_stage = false;  // the module stages the next tile (PWA_HESS_STAGE 1)
   double* d_hsum = nullptr;
   // parameter layout for the C-side chain rule
   int n_vars = 0, n_coup = 0, nfac = 0, n_train = 0;
@@ -345,6 +346,8 @@ int pwa_plan_create(const char* src, size_t src_len, int n_mass, int n_angle, in
   h->n_mass = n_mass;
   h->has_genbod =
       std::string(src, src_len).find("#define PWA_HAS_GENBOD 1") != std::string::npos;
+  h->hess_stage =
+      std::string(src, src_len).find("#define PWA_HESS_STAGE 1") != std::string::npos;
   h->n_angle = n_angle;
   h->ncol = ncol;
   h->nout = nout;
@@ -1550,7 +1553,8 @@ int hess_sums(pwa_plan* h, const double* ck, cudaStream_t s, double* out) {
     // X1, X2 (the final row buffer reuses them), s1, s2, the next tile's stage
     const size_t rows = (size_t)(h->nout + 1) * h->tpb * ld * 4;
     const size_t smem = (rows > (size_t)NA * 8 ? rows : ((size_t)NA * 8 + 15) / 16 * 16) +
-                        2 * (size_t)h->tpb * 4 + (size_t)h->tpb * (h->nf * 8 + 8);
+                        2 * (size_t)h->tpb * 4 +
+                        (h->hess_stage ? (size_t)h->tpb * (h->nf * 8 + 8) : 0);
     int optin = 0;
     CU(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
     if (smem > (size_t)optin)
