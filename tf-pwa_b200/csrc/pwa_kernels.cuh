@@ -1792,12 +1792,12 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, PWA_HESS_MINB)
 #pragma unroll
       for (int j = 0; j < BS; ++j) hacc[q][i][j] = 0.0;
   }
-  // S1 (FP64, four interleaved chains) on the last threads, which hold the
-  // fewest items: column c = PWA_TPB - 1 - tid + q PWA_TPB
-  constexpr int NS1 = (W + PWA_TPB - 1) / PWA_TPB;
-  double acc_s0 = 0.0, acc_s1[NS1];
+  // S1 as in the evaluation kernels: each event's w t'(f) G (entries 2k,
+  // 2k + 1 = re, im of column k) reduce-scattered across the warp in FP32,
+  // the lane's entries accumulated in FP64
+  double acc_s0 = 0.0, acc_s1[PWA_MG];
 #pragma unroll
-  for (int q = 0; q < NS1; ++q) acc_s1[q] = 0.0;
+  for (int q = 0; q < PWA_MG; ++q) acc_s1[q] = 0.0;
   const long long B = gridDim.x, b = blockIdx.x;
   const long long t0 = b * ntiles / B, t1 = (b + 1) * ntiles / B;
 #if PWA_HESS_STAGE
@@ -1853,6 +1853,29 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, PWA_HESS_MINB)
         row[K + k] = fmaf(xi, v[j].x, fmaf(-xr, v[j].y, row[K + k]));
       }
       hess_store_row(X2 + tid * LD, row);
+      {
+        const float f1 = (float)(w * d1);
+#if PWA_RS16
+        float gq[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q)
+          gq[q] = q < W ? ((q & 1) ? -f1 * row[K + (q >> 1)] : f1 * row[q >> 1]) : 0.f;
+        warp_rs_step<16, 16, 16>(gq, lane);
+        acc_s1[0] += (double)(gq[0] + __shfl_xor_sync(0xffffffffu, gq[0], 1));
+#else
+#pragma unroll
+        for (int m = 0; m < PWA_GPAD / 32; ++m) {
+          float gq[32];
+#pragma unroll
+          for (int q = 0; q < 32; ++q) {
+            const int e = 32 * m + q;
+            gq[q] = e < W ? ((e & 1) ? -f1 * row[K + (e >> 1)] : f1 * row[e >> 1]) : 0.f;
+          }
+          warp_reduce_scatter<32>(gq, lane);
+          acc_s1[m] += (double)gq[0];
+        }
+#endif
+      }
 #pragma unroll
       for (int o = 0; o < PWA_NOUT; ++o) {  // X1 rows: (Re F_.o, Im F_.o)
 #pragma unroll
@@ -1905,20 +1928,6 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, PWA_HESS_MINB)
 #pragma unroll
         for (int j = 0; j < BS; ++j) hacc[q][i][j] += (double)a[i][j];
     }
-#pragma unroll
-    for (int q = 0; q < NS1; ++q) {  // S1 = sum s1 G (X2: -Im G in columns K .. 2K-1)
-      const int col = PWA_TPB - 1 - tid + q * PWA_TPB;
-      if (col >= W) continue;
-      double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-#pragma unroll 2
-      for (int e = 0; e < PWA_TPB; e += 4) {
-        a0 = fma((double)s1[e], (double)X2[e * LD + col], a0);
-        a1 = fma((double)s1[e + 1], (double)X2[(e + 1) * LD + col], a1);
-        a2 = fma((double)s1[e + 2], (double)X2[(e + 2) * LD + col], a2);
-        a3 = fma((double)s1[e + 3], (double)X2[(e + 3) * LD + col], a3);
-      }
-      acc_s1[q] += (a0 + a1) + (a2 + a3);
-    }
     __syncthreads();
   }
   // the block row: S0, S1, then the items' blocks added in split order
@@ -1932,10 +1941,15 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, PWA_HESS_MINB)
     for (int w2 = 0; w2 < PWA_TPB / 32; ++w2) a += s_red[w2];
     row_acc[0] = a;
   }
+  for (int w2 = 0; w2 < PWA_TPB / 32; ++w2) {  // the warps' S1 entries in warp order
+    __syncthreads();
+    if (warp == w2) {
 #pragma unroll
-  for (int q = 0; q < NS1; ++q) {
-    const int col = PWA_TPB - 1 - tid + q * PWA_TPB;
-    if (col < W) row_acc[1 + (col < K ? 2 * col : 2 * (col - K) + 1)] = col < K ? acc_s1[q] : -acc_s1[q];
+      for (int m = 0; m < PWA_MG; ++m) {
+        const int idx = rs_entry(m, lane);
+        if (rs_owner(lane) && idx < W) row_acc[1 + idx] += acc_s1[m];
+      }
+    }
   }
   for (int spl = 0; spl < PWA_HSP1; ++spl) {
     __syncthreads();
