@@ -1702,8 +1702,9 @@ extern "C" __global__ void __launch_bounds__(PWA_PTS_WARPS * 32, 1)
 // A block walks a contiguous run of 128-event tiles.  Per tile, thread e
 // computes its event's A (FP64), f, t, t', t'' and G (FP32) and writes its
 // rows of X1 and X2 to shared memory; then each thread accumulates its
-// items -- (matrix, PWA_HBS x PWA_HBS block of the upper triangle, range of
-// rows) -- over the tile in FP32 and adds them to FP64 registers.  While it
+// items -- (matrix, PWA_HBS x PWA_HBS block of the upper triangle, split s
+// of the rows: every sp-th row from s) -- over the tile in FP32 and adds
+// them to FP64 registers.  While it
 // does, the next tile's columns of its own event are already on their way
 // into a shared-memory stage (per-thread cp.async of 8-byte values, the
 // tile's own layout), so the loads overlap the outer products.  The
@@ -1900,8 +1901,9 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, PWA_HESS_MINB)
       if (it_m[q] < 0) continue;
       const float* X = it_m[q] == 0 ? X1 : X2;
       const float* sw = it_m[q] == 0 ? s1 : s2;
+      // split s takes rows s, s + sp, s + 2 sp, ...: the splits sharing a
+      // warp read neighbouring rows, which start in different bank quads
       const int R = it_m[q] == 0 ? R1 : PWA_TPB, sp = it_m[q] == 0 ? PWA_HSP1 : PWA_HSP2;
-      const int r0 = it_s[q] * R / sp, r1 = (it_s[q] + 1) * R / sp;
       const int cp = it_bi[q] * BS, cq = it_bj[q] * BS;
       float a[BS][BS];
 #pragma unroll
@@ -1909,7 +1911,7 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, PWA_HESS_MINB)
 #pragma unroll
         for (int j = 0; j < BS; ++j) a[i][j] = 0.f;
 #pragma unroll 4
-      for (int r = r0; r < r1; ++r) {
+      for (int r = it_s[q]; r < R; r += sp) {
         const float* x = X + r * LD;
         const float sc = sw[r % PWA_TPB];
         float xp[BS], xq[BS];

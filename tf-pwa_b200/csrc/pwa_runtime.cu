@@ -1721,8 +1721,8 @@ int hessian_from_hsums(pwa_plan* h, const double* vars, const std::vector<cplx>&
       for (int q = 0; q < W; ++q) t += G2f[(size_t)p * W + q] * Ch[(size_t)b * W + q];
       T[(size_t)p * P + b] = t;
     }
-  for (int a = 0; a < P; ++a)
-    for (int b = 0; b < P; ++b) {
+  for (int a = 0; a < P; ++a)  // the symmetric part, upper triangle mirrored
+    for (int b = a; b < P; ++b) {
       const cplx* db = &dc[(size_t)b * K];
       double qh = 0.0, qm = 0.0, h2 = 0.0;
       for (int l = 0; l < K; ++l) {  // Re (c_b)^H u
@@ -1730,8 +1730,9 @@ int hessian_from_hsums(pwa_plan* h, const double* vars, const std::vector<cplx>&
         qm += db[l].r * uM[(size_t)a * K + l].r + db[l].i * uM[(size_t)a * K + l].i;
       }
       for (int p = 0; p < W; ++p) h2 += Ch[(size_t)a * W + p] * T[(size_t)p * P + b];
-      out_hess[(size_t)a * P + b] += -2.0 * qh - 4.0 * h2 +
-                                     sw * (2.0 * qm / I - dI[a] * dI[b] / (I * I));
+      const double m = -2.0 * qh - 4.0 * h2 + sw * (2.0 * qm / I - dI[a] * dI[b] / (I * I));
+      out_hess[(size_t)a * P + b] += m;
+      if (b != a) out_hess[(size_t)b * P + a] += m;
     }
   for (int a = 0; a < P; ++a)
     for (int b = a + 1; b < P; ++b) {
