@@ -135,6 +135,23 @@ int pwa_toy_select(pwa_plan* h, const double* consts, unsigned long long seed, l
 int pwa_toy_fields(pwa_plan* h, unsigned long long seed, const long long* idx, long long n,
                    double* out, long long ld_out, double* p4, long long ld_p4, void* stream);
 
+/* ---- floating masses/widths: shape-free column cache -------------------
+ * For models whose columns factorise as (lineshapes of the chain) x
+ * (shape-free column) -- one pass, no polarised parent, no CP-violating
+ * totals -- pwa_shape_cache computes, at the shape setting in consts, every
+ * event's (data and MC) columns without their lineshapes (FP64, stored
+ * FP32).  pwa_eval_shapecache then evaluates at any setting: lineshapes from
+ * the resident masses, the column couplings times ratio[ncol] (each
+ * column's barrier normalisations now over at the cache's setting), and
+ * returns the sums of pwa_eval (out[2 * nacc]: data, MC), so the chain rule
+ * of the plain form applies.  The reference recomputes the whole amplitude
+ * per evaluation when shapes float (tf_pwa/model/model.py:407-449,
+ * tf_pwa/amp/core.py:1392-1445); PWA_ERR_STATE for models that do not
+ * factorise. */
+int pwa_shape_cache(pwa_plan* h, const double* consts, void* stream);
+int pwa_eval_shapecache(pwa_plan* h, const double* consts, const double* ratio, void* stream,
+                        double* out);
+
 /* Hessian of the cached-form NLL with respect to the trainable parameters
  * (tf_pwa/model/model.py:513-561, BaseModel.nll_grad_hessian; errors via
  * tf_pwa/applications.py:280-309): central 4-point differences of the

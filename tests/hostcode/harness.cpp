@@ -114,6 +114,43 @@ extern "C" int hx_columns(const double* Cv, const double* XM, const double* XA, 
   return PWA_NCOL;
 }
 
+// columns without their chains' lineshapes, layout of hx_columns
+extern "C" int hx_columns_ns(const double* Cv, const double* XM, const double* XA, long long n,
+                             long long ld, double* out) {
+  Consts C;
+  for (int j = 0; j < PWA_NCONST; ++j) C.v[j] = Cv[j];
+  for (long long i = 0; i < n; ++i) {
+    cpx<double> F[PWA_NCOL * PWA_NOUT];
+    model_columns_ns<double, false>(C, XA, XM, ld, i, F);
+    for (int j = 0; j < PWA_NCOL * PWA_NOUT; ++j) {
+      out[2 * (i * PWA_NCOL * PWA_NOUT + j)] = F[j].re;
+      out[2 * (i * PWA_NCOL * PWA_NOUT + j) + 1] = F[j].im;
+    }
+  }
+  return PWA_NCOL;
+}
+
+// per event: chain lineshape products BW[PWA_NCHAIN], then the log-derivative
+// factors DM, DG [PWA_NSRES] of each floating lineshape, as (re, im) pairs
+extern "C" int hx_shapes(const double* Cv, const double* XM, long long n, long long ld,
+                         double* out) {
+  Consts C;
+  for (int j = 0; j < PWA_NCONST; ++j) C.v[j] = Cv[j];
+  constexpr int NS = PWA_NSRES > 0 ? PWA_NSRES : 1, W = PWA_NCHAIN + 2 * NS;
+  for (long long i = 0; i < n; ++i) {
+    cpx<double> BW[PWA_NCHAIN], DM[NS], DG[NS];
+    for (int q = 0; q < NS; ++q) DM[q] = DG[q] = cmk<double>(0.0, 0.0);
+    model_shapes<double, false>(C, XM, ld, i, BW, DM, DG);
+    double* o = out + 2 * i * W;
+    for (int c = 0; c < PWA_NCHAIN; ++c) o[2 * c] = BW[c].re, o[2 * c + 1] = BW[c].im;
+    for (int q = 0; q < NS; ++q) {
+      o[2 * (PWA_NCHAIN + q)] = DM[q].re, o[2 * (PWA_NCHAIN + q) + 1] = DM[q].im;
+      o[2 * (PWA_NCHAIN + NS + q)] = DG[q].re, o[2 * (PWA_NCHAIN + NS + q) + 1] = DG[q].im;
+    }
+  }
+  return W;
+}
+
 // P4 rows (4 f + c), stride n -> fields rows j (plan order), stride n
 extern "C" int hx_kin(const double* P4, long long n, double* out) {
   for (long long i = 0; i < n; ++i) {

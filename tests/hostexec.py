@@ -58,6 +58,8 @@ class HostModel:
         lib.hx_sums.argtypes = [dp, dp, dp, dp, ll, ll, ll, i, i, dp]
         lib.hx_amp.argtypes = [dp, dp, dp, ll, ll, i, dp]
         lib.hx_columns.argtypes = [dp, dp, dp, ll, ll, dp]
+        lib.hx_columns_ns.argtypes = [dp, dp, dp, ll, ll, dp]
+        lib.hx_shapes.argtypes = [dp, dp, ll, ll, dp]
         lib.hx_kin.argtypes = [dp, ll, dp]
         self.has_toy = hasattr(lib, "hx_toy")
         if self.has_toy:
@@ -114,6 +116,28 @@ class HostModel:
         out = np.zeros(2 * n * K * O)
         self.lib.hx_columns(_dp(C), _dp(xm), _dp(xa), n, n, _dp(out))
         return (out[0::2] + 1j * out[1::2]).reshape(n, K, O)
+
+    def columns_ns(self, C, x):
+        """Columns without their chains' lineshapes (model_columns_ns)."""
+        C = np.ascontiguousarray(C, np.float64)
+        xm, xa = self._split(x)
+        n = xm.shape[1]
+        K, O = self.code.ncol, self.code.nout
+        out = np.zeros(2 * n * K * O)
+        self.lib.hx_columns_ns(_dp(C), _dp(xm), _dp(xa), n, n, _dp(out))
+        return (out[0::2] + 1j * out[1::2]).reshape(n, K, O)
+
+    def shapes(self, C, x):
+        """(BW (n, n_chain), DM (n, n_sres), DG (n, n_sres)) of model_shapes."""
+        C = np.ascontiguousarray(C, np.float64)
+        xm, _ = self._split(x)
+        n = xm.shape[1]
+        nch, ns = len(self.code.group), max(len(self.code.shape_res), 1)
+        W = nch + 2 * ns
+        out = np.zeros(2 * n * W)
+        self.lib.hx_shapes(_dp(C), _dp(xm), n, n, _dp(out))
+        z = (out[0::2] + 1j * out[1::2]).reshape(n, W)
+        return z[:, :nch], z[:, nch:nch + ns], z[:, nch + ns:]
 
     def kin(self, p4):
         """(N, n_final, 4) momenta in dat_order -> (n_fields, N) fields."""

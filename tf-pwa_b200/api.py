@@ -156,12 +156,14 @@ class FCN:
 
     ``precision``: "plain" (FP64 throughout) or "mixed" (FP32 amplitudes,
     FP64 sums; with ``gram=True`` and fixed masses/widths the MC integral
-    uses the cached Gram matrix).  ``bg``, ``batch`` take the reference's
+    uses the cached Gram matrix; with floating masses/widths and
+    ``shape_cache`` (default where the columns factorise) every evaluation
+    reads the cached shape-free columns and recomputes only the lineshapes).  ``bg``, ``batch`` take the reference's
     positions; ``w_bkg`` (weight of bg rows without their own weights),
     ``precision`` and ``gram`` are passed by keyword."""
 
     def __init__(self, config, data, mcdata, bg=None, batch=65000, inmc=None, gauss_constr=None,
-                 w_bkg=1.0, precision="plain", gram=None):
+                 w_bkg=1.0, precision="plain", gram=None, shape_cache=None):
         # positional order of tf_pwa/model/model.py:1126-1135
         if inmc is not None or gauss_constr:
             raise NotImplementedError("inmc samples / Gaussian constraints")
@@ -192,6 +194,20 @@ class FCN:
             raise ValueError("the Gram cache needs fixed masses and widths, no polarisation "
                              "and no CP-violating totals")
         self.tune = None
+        # floating masses/widths in the mixed form: the shape-free column
+        # cache where the columns factorise (else the FP32 recompute form)
+        self.use_shape_cache = (self.precision == MIXED_F32 and shape_free
+                                and self.eng.code.shape_cache_ok) \
+            if shape_cache is None else shape_cache
+        if self.use_shape_cache:
+            try:
+                self.eng.shape_cache(self.vm.get_all_dic())
+                self.eng.use_shape_cache = True
+            except PWAError as e:
+                if shape_cache:
+                    raise
+                warnings.warn(f"floating-shape column cache not used: {e}")
+                self.use_shape_cache = False
         if self.use_gram:
             vals = self.vm.get_all_dic()
             self.eng.set_gram(vals)

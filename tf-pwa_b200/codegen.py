@@ -373,6 +373,33 @@ class ModelCode:
         if self.flips:
             e(f"  const bool cc = xm{self.plan.charge_index} < 0.0;")
 
+    def _emit_mass_loads(self, e):
+        for f in self.mass_fields:
+            a = f"XM + (long long){self.mass_slot[f]} * ld + i"
+            e(f"  const double xm{f} = LDG ? __ldg({a}) : *({a});")
+
+    def column_barrier_consts(self, k):
+        """Constants whose product scales column k's barrier factors (each
+        vertex's q^l sqrt(Pz0_l / B(q^2)) times norm_l): ("sqrt", name) per
+        vertex with a B' factor, ("lin", name) per normalised one."""
+        ci, lsi = self.columns[k]
+        out = []
+        for vi, d in enumerate(self.group[ci]):
+            if d.has_barrier_factor:
+                l = d.get_ls_list()[lsi[vi]][0]
+                if d.has_bprime:
+                    out.append(("sqrt", f"{d}.Pz0_{l}"))
+                if d.barrier_factor_norm:
+                    out.append(("lin", f"{d}.norm_{l}"))
+        return out
+
+    @property
+    def shape_cache_ok(self):
+        """Whether the columns factorise as (lineshapes of the chain) x
+        (shape-free column): one pass (no identical-particle swaps), no
+        polarised parent, no CP-violating totals."""
+        return self.npass == 1 and not self.pol_names and not self.cp_chains
+
     def _trig(self, e, ci, key, angle):
         """sin/cos of half an angle: computed (and stashed in the forward
         pass) or read back from the stash (adjoint pass)."""
@@ -477,6 +504,20 @@ class ModelCode:
                              for l in range(j2 + 1) if w[l][n1 // 2][n2 // 2] != 0]
                     dexpr = " + ".join(terms) if terms else "R(0)"
                     e(f"  const cpx<R> Dal_{tag}_{n1}_{n2} = cscale(cmul(ea_{tag}[{n1}], eg_{tag}[{n2}]), {dexpr});")
+        self._emit_lineshapes(e, ci)
+
+    def _emit_lineshapes(self, e, ci):
+        """Lineshapes of chain ci's resonances from their invariant masses and
+        the constant block: bw_<tag> per resonance, BW_c<ci> their product."""
+        c = self.group[ci]
+        cf = self._cf(ci)
+        cst = self._cst
+
+        def dmass(p):
+            if p in c.inner:
+                return f"xm{cf['mass'][p]}"
+            return repr(float(p.mass))
+
         bw_names = []
         for p in c.inner:
             kind = p.lineshape_kind()
@@ -716,24 +757,30 @@ class ModelCode:
                     if p in c.inner:
                         e(f"    cfmac(SR{si}, {ck}, g);")
                 e("  }")
-            for si, p in enumerate(self.shape_res):
-                if p in c.inner and self._first_chain(p) == ci:
-                    # log-derivatives of the lineshape R with respect to m0
-                    # and Gamma0 (kappa_m = dlog(m0 Gamma) / dm0 at fixed m)
-                    tag = f"c{ci}r{c.inner.index(p)}"
-                    kap, ig = self._cst(f"{p}.kappa_m"), self._cst(f"{p}.inv_g0")
-                    e(f"  {{ const R m0 = psqrt({self._cst(f'{p}.m0sq')});")
-                    if p.lineshape_kind() == "BWR2":
-                        # R = 1 / conj(D): dlog R = -R conj(dD)
-                        e(f"    dm{si} = cmul(bw_{tag}, cmk<R>(-(R(2) * m0 + yi_{tag} * {kap}), -y_{tag} * {kap}));")
-                        e(f"    dg{si} = cmul(bw_{tag}, cmk<R>(-yi_{tag} * {ig}, -y_{tag} * {ig}));")
-                    else:
-                        e(f"    dm{si} = cmul(bw_{tag}, cmk<R>(R(-2) * m0, y_{tag} * {kap}));")
-                        e(f"    dg{si} = cmul(bw_{tag}, cmk<R>(R(0), y_{tag} * {ig}));")
-                    if p.width_norm_applies():
-                        e(f"    dg{si}.re += {ig};")
-                    e("  }")
+            self._emit_shape_derivs(e, ci, "dm{si}", "dg{si}")
             e("  }")
+
+    def _emit_shape_derivs(self, e, ci, dm_fmt, dg_fmt):
+        """Log-derivatives of each floating lineshape R whose first chain is
+        ci with respect to m0 and Gamma0 (kappa_m = dlog(m0 Gamma) / dm0 at
+        fixed m), into the names dm_fmt / dg_fmt (formatted with si)."""
+        c = self.group[ci]
+        for si, p in enumerate(self.shape_res):
+            if p in c.inner and self._first_chain(p) == ci:
+                tag = f"c{ci}r{c.inner.index(p)}"
+                dm, dg = dm_fmt.format(si=si), dg_fmt.format(si=si)
+                kap, ig = self._cst(f"{p}.kappa_m"), self._cst(f"{p}.inv_g0")
+                e(f"  {{ const R m0 = psqrt({self._cst(f'{p}.m0sq')});")
+                if p.lineshape_kind() == "BWR2":
+                    # R = 1 / conj(D): dlog R = -R conj(dD)
+                    e(f"    {dm} = cmul(bw_{tag}, cmk<R>(-(R(2) * m0 + yi_{tag} * {kap}), -y_{tag} * {kap}));")
+                    e(f"    {dg} = cmul(bw_{tag}, cmk<R>(-yi_{tag} * {ig}, -y_{tag} * {ig}));")
+                else:
+                    e(f"    {dm} = cmul(bw_{tag}, cmk<R>(R(-2) * m0, y_{tag} * {kap}));")
+                    e(f"    {dg} = cmul(bw_{tag}, cmk<R>(R(0), y_{tag} * {ig}));")
+                if p.width_norm_applies():
+                    e(f"    {dg}.re += {ig};")
+                e("  }")
 
     # ------------------------------------------------------------ columns
     def _emit_columns(self, e):
@@ -766,7 +813,12 @@ class ModelCode:
                         e(f"  cpx<R> {nm} = cmk<R>(R(0), R(0));")
                     e(f"  cfma({nm}, {self._coef(coefs[k])}, {prod});")
                 cur = self._emit_align_forward(e, ci, pre, "Fa")
-                e(f"  const cpx<R> S = cscale(BW_c{ci}, {self._scale_k(ci, k)});")
+                if getattr(self, "_noshape", False):
+                    # the column without its chain's lineshapes (they are
+                    # applied per evaluation from the masses)
+                    e(f"  const cpx<R> S = cmk<R>({self._scale_k(ci, k)}, R(0));")
+                else:
+                    e(f"  const cpx<R> S = cscale(BW_c{ci}, {self._scale_k(ci, k)});")
                 for o, nm in cur.items():
                     j = k * self.nout + self._out(o)
                     if self._pass == 0:
@@ -878,6 +930,39 @@ class ModelCode:
                  "    cpx<R>* __restrict__ F) {")
         L += body
         L.append("}\n")
+        # columns without lineshapes, and the lineshapes with their
+        # log-derivatives from the masses alone (floating-shape column cache)
+        body = []
+        self._mode = "plain"
+        self._noshape = True
+        self._emit_loads(body.append)
+        self._emit_columns(body.append)
+        self._noshape = False
+        L.append(f"template <typename R, bool LDG = true>\n__device__ __forceinline__ void model_columns_ns(\n{sig},\n"
+                 "    cpx<R>* __restrict__ F) {")
+        L += body
+        L.append("}\n")
+        body = []
+        self._emit_mass_loads(body.append)
+        for ci in range(len(self.group)):
+            body.append(f"  {{ // chain {ci}")
+            self._emit_lineshapes(body.append, ci)
+            body.append(f"  BW[{ci}] = BW_c{ci};")
+            self._emit_shape_derivs(body.append, ci, "DM[{si}]", "DG[{si}]")
+            body.append("  }")
+        L.append("template <typename R, bool LDG = true>\n__device__ __forceinline__ void model_shapes(\n"
+                 "    const Consts& C, const double* __restrict__ XM, long long ld, long long i,\n"
+                 "    cpx<R>* __restrict__ BW, cpx<R>* __restrict__ DM, cpx<R>* __restrict__ DG) {")
+        L += body
+        L.append("}\n")
+        nch, nsr = len(self.group), len(self.shape_res)
+        L.append(f"#define PWA_NCHAIN {nch}\n#define PWA_NSRES {nsr}\n"
+                 f"#define PWA_SHAPE_CACHE_OK {1 if self.shape_cache_ok else 0}")
+        L.append("__device__ constexpr int pwa_col_chain[PWA_NCOL] = {" +
+                 ", ".join(str(ci) for ci, _ in self.columns) + "};")
+        rows = [", ".join("1" if p in c.inner else "0" for c in self.group) for p in self.shape_res]
+        L.append("__device__ constexpr int pwa_sres_chain[PWA_NSRES > 0 ? PWA_NSRES : 1][PWA_NCHAIN] = {" +
+                 (", ".join("{" + r + "}" for r in rows) if rows else "{" + ", ".join(["0"] * nch) + "}") + "};")
         L.append(self._pdf_source())
         fl = sorted(self._fset)
         L.append(f"#define PWA_NF {self.nf}")

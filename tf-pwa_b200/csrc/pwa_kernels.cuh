@@ -585,6 +585,152 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Floating-shape column cache.  With one pass (no identical-particle swaps),
+// no polarised parent and no CP-violating totals (PWA_SHAPE_CACHE_OK), a
+// column factorises as
+//   F_k,o(event) = r_k BW_ch(k)(m; shapes) Fhat_k,o(event):
+// Fhat is the column without its chain's lineshapes (model_columns_ns, in
+// FP64 at the shape setting of the cache, stored FP32 in the tile layout of
+// the cached kernels, for data and MC events), BW the product of the
+// chain's lineshapes from the event's masses (model_shapes, FP64), and r_k
+// the ratio of the column's barrier normalisations (sqrt(Pz0_l) norm_l per
+// vertex) now and at the cache's setting (host).  An evaluation reads the
+// columns and the masses and produces the sums of pwa_eval_f64 -- S0, the
+// column sums and the lineshape sums (tf_pwa/model/model.py:407-449 with
+// the derivatives of the lineshapes, tf_pwa/breit_wigner.py:56-91) -- so
+// the host's chain rule is the plain form's.
+extern "C" __global__ void __launch_bounds__(PWA_TPB)
+    pwa_cache_ns_f32(const Consts C, const double* __restrict__ XA, const double* __restrict__ XM,
+                     long long n, long long ntiles, long long ld, float2* __restrict__ Fc) {
+  const long long total = ntiles * PWA_TPB;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long t = i / PWA_TPB, e = i % PWA_TPB;
+    if (i < n) {
+      cpx<double> F[PWA_NCOL * PWA_NOUT];
+      model_columns_ns<double>(C, XA, XM, ld, i, F);
+#pragma unroll
+      for (int j = 0; j < PWA_NF; ++j) {
+        const cpx<double> v = F[pwa_fk[j] * PWA_NOUT + pwa_fo[j]];
+        Fc[(t * PWA_NF + j) * PWA_TPB + e] = make_float2((float)v.re, (float)v.im);
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < PWA_NF; ++j) Fc[(t * PWA_NF + j) * PWA_TPB + e] = make_float2(0.f, 0.f);
+    }
+  }
+}
+
+struct CRatio {
+  double v[PWA_NCOL];  // r_k: barrier normalisations now / at the cache's setting
+};
+
+#ifndef PWA_SC_MINB
+#define PWA_SC_MINB 2
+#endif
+extern "C" __global__ void __launch_bounds__(PWA_TPB, PWA_SC_MINB)
+    pwa_eval_shapecache(const Consts C, const CRatio rk, const float2* __restrict__ Fc,
+                        const double* __restrict__ XM, const double* __restrict__ W,
+                        long long n_data, long long n_all, long long ld, int blocks_data,
+                        double* __restrict__ partials) {
+  constexpr int K = PWA_NCOL, NS = PWA_NSRES > 0 ? PWA_NSRES : 1;
+  const bool is_data = (int)blockIdx.x < blocks_data;
+  const long long beg = is_data ? 0 : n_data;
+  const long long end = is_data ? n_data : n_all;
+  const int nb = is_data ? blocks_data : (int)gridDim.x - blocks_data;
+  const int b = is_data ? (int)blockIdx.x : (int)blockIdx.x - blocks_data;
+  double acc[PWA_NACC];
+#pragma unroll
+  for (int j = 0; j < PWA_NACC; ++j) acc[j] = 0.0;
+  for (long long i = beg + (long long)b * PWA_TPB + threadIdx.x; i < end;
+       i += (long long)nb * PWA_TPB) {
+    const long long t = i / PWA_TPB, e = i % PWA_TPB;
+    float2 v[PWA_NF];
+#pragma unroll
+    for (int j = 0; j < PWA_NF; ++j) v[j] = __ldcs(Fc + (t * PWA_NF + j) * PWA_TPB + e);
+    cpx<double> BW[PWA_NCHAIN], DM[NS], DG[NS];
+    model_shapes<double>(C, XM, ld, i, BW, DM, DG);
+    // F = s_k Fhat with s_k = r_k BW_ch(k); A_o = sum_k c_k s_k Fhat_k,o
+    double ar[PWA_NOUT], ai[PWA_NOUT];
+#pragma unroll
+    for (int o = 0; o < PWA_NOUT; ++o) ar[o] = ai[o] = 0.0;
+#pragma unroll
+    for (int j = 0; j < PWA_NF; ++j) {
+      const int k = pwa_fk[j], o = pwa_fo[j];
+      const cpx<double> bw = BW[pwa_col_chain[k]];
+      const cpx<double> cs = cmul(cmk<double>(C.v[2 * k], C.v[2 * k + 1]),
+                                  cmk<double>(rk.v[k] * bw.re, rk.v[k] * bw.im));
+      const double x = (double)v[j].x, y = (double)v[j].y;
+      ar[o] = fma(cs.re, x, fma(-cs.im, y, ar[o]));
+      ai[o] = fma(cs.re, y, fma(cs.im, x, ai[o]));
+    }
+    double f = 0.0;
+#pragma unroll
+    for (int o = 0; o < PWA_NOUT; ++o) f = fma(ar[o], ar[o], fma(ai[o], ai[o], f));
+    const double w = __ldg(W + i);
+    double fac;
+    if (is_data) {
+      double dl;
+      const double cl = clip_log(f, &dl);
+      acc[0] = fma(w, cl, acc[0]);
+      fac = w * dl;
+    } else {
+      acc[0] = fma(w, f, acc[0]);
+      fac = w;
+    }
+    // g_k = fac s_k sum_o conj(A_o) Fhat_k,o (the pairs j run column by
+    // column);  SR_s = sum over the columns of the chains holding shape s of
+    // c_k g_k
+    cpx<double> SR[NS];
+#pragma unroll
+    for (int q = 0; q < NS; ++q) SR[q] = cmk<double>(0.0, 0.0);
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      cpx<double> hk = cmk<double>(0.0, 0.0);
+#pragma unroll
+      for (int j = 0; j < PWA_NF; ++j) {
+        if (pwa_fk[j] != k) continue;
+        const int o = pwa_fo[j];
+        const double x = (double)v[j].x, y = (double)v[j].y;
+        hk.re = fma(ar[o], x, fma(ai[o], y, hk.re));
+        hk.im = fma(ar[o], y, fma(-ai[o], x, hk.im));
+      }
+      const cpx<double> bw = BW[pwa_col_chain[k]];
+      const cpx<double> g =
+          cscale(cmul(cmk<double>(rk.v[k] * bw.re, rk.v[k] * bw.im), hk), fac);
+      acc[1 + 2 * k] += g.re;
+      acc[2 + 2 * k] += g.im;
+      const cpx<double> cg = cmul(cmk<double>(C.v[2 * k], C.v[2 * k + 1]), g);
+#pragma unroll
+      for (int q = 0; q < PWA_NSRES; ++q)
+        if (pwa_sres_chain[q][pwa_col_chain[k]]) {
+          SR[q].re += cg.re;
+          SR[q].im += cg.im;
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < PWA_NSRES; ++q) {
+      acc[1 + 2 * K + 2 * q] += 2.0 * cmul(SR[q], DM[q]).re;
+      acc[2 + 2 * K + 2 * q] += 2.0 * cmul(SR[q], DG[q]).re;
+    }
+  }
+  __shared__ double red[PWA_TPB / 32][PWA_NACC];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int j = 0; j < PWA_NACC; ++j) {
+    const double vv = warp_sum(acc[j]);
+    if (lane == 0) red[warp][j] = vv;
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < PWA_NACC; j += PWA_TPB) {
+    double sacc = 0.0;
+#pragma unroll
+    for (int w2 = 0; w2 < PWA_TPB / 32; ++w2) sacc += red[w2][j];
+    partials[(long long)blockIdx.x * PWA_NACC + j] = sacc;
+  }
+}
+
 struct CCoup {
   double v[2 * PWA_NCOL];  // column couplings c_k, (re, im) pairs
 };

@@ -40,7 +40,7 @@ struct Kernels {
                eval_cached_wide = nullptr, eval_cached_tma = nullptr, eval_multi = nullptr,
                gram_colmax = nullptr, gram_tc = nullptr, wait_check = nullptr,
                fma_f64 = nullptr, fma_f32 = nullptr, eval_points = nullptr, reduce_multi = nullptr,
-               hess_cached = nullptr,
+               hess_cached = nullptr, cache_ns_f32 = nullptr, eval_shapecache = nullptr,
                fields_from_p4 = nullptr, toy_select = nullptr, toy_fields = nullptr;
 };
 
@@ -114,6 +114,12 @@ struct pwa_plan {
   int hess_blocks = 0;
   size_t hess_smem = 0;
   bool hess_stage = false;  // the module stages the next tile (PWA_HESS_STAGE 1)
+  // floating-shape column cache: shape-free columns of every event (data and
+  // MC), tile layout; its grid (0: not set up)
+  float2* scache = nullptr;
+  long long scache_n = 0;
+  int sc_blocks = 0, sc_blocks_data = 0;
+  bool shape_cache_ok = false;  // the model's columns factorise (PWA_SHAPE_CACHE_OK 1)
   double* d_hsum = nullptr;
   // parameter layout for the C-side chain rule
   int n_vars = 0, n_coup = 0, nfac = 0, n_train = 0;
@@ -348,6 +354,8 @@ int pwa_plan_create(const char* src, size_t src_len, int n_mass, int n_angle, in
       std::string(src, src_len).find("#define PWA_HAS_GENBOD 1") != std::string::npos;
   h->hess_stage =
       std::string(src, src_len).find("#define PWA_HESS_STAGE 1") != std::string::npos;
+  h->shape_cache_ok =
+      std::string(src, src_len).find("#define PWA_SHAPE_CACHE_OK 1") != std::string::npos;
   h->n_angle = n_angle;
   h->ncol = ncol;
   h->nout = nout;
@@ -406,7 +414,9 @@ int pwa_plan_create(const char* src, size_t src_len, int n_mass, int n_angle, in
             {"pwa_toy_select", &h->k.toy_select},
             {"pwa_toy_fields", &h->k.toy_fields},
             {"pwa_eval_multi", &h->k.eval_multi},   {"pwa_reduce_multi", &h->k.reduce_multi},
-            {"pwa_hess_cached", &h->k.hess_cached}};
+            {"pwa_hess_cached", &h->k.hess_cached},
+            {"pwa_cache_ns_f32", &h->k.cache_ns_f32},
+            {"pwa_eval_shapecache", &h->k.eval_shapecache}};
   for (auto& e : ks) CU(cudaLibraryGetKernel(e.slot, h->lib, e.name));
   for (int p = 0; p < 2; ++p) {
     cudaFuncAttributes a;
@@ -441,6 +451,7 @@ int pwa_plan_destroy(pwa_plan* h) {
   if (h->d_multi_out) cudaFree(h->d_multi_out);
   if (h->d_pts) cudaFree(h->d_pts);
   if (h->d_hsum) cudaFree(h->d_hsum);
+  if (h->scache) cudaFree(h->scache);
   if (h->h_map) cudaFreeHost(h->h_map);
   if (h->d_out) cudaFree(h->d_out);
   if (h->h_out) cudaFreeHost(h->h_out);
@@ -475,6 +486,7 @@ int pwa_upload_events(pwa_plan* h, const double* xm, const double* xa, const dou
   h->n_data = n_data;
   h->n_mc = n_mc;
   h->fcache_n = 0;
+  h->scache_n = 0;  // the floating-shape column cache belongs to the old events
   h->gram_valid = false;
   const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
   if (h->n_mass)
@@ -558,6 +570,71 @@ int pwa_eval(pwa_plan* h, const double* consts, int precision, int mc, void* str
   std::memcpy(out, h->h_out, sizeof(double) * 2 * nacc);
   if (!mc)
     for (int j = 0; j < nacc; ++j) out[nacc + j] = 0.0;
+  return PWA_OK;
+}
+
+int pwa_shape_cache(pwa_plan* h, const double* consts, void* stream) {
+  if (!h) return PWA_ERR_ARG;
+  if (!h->w) return set_err(h, PWA_ERR_STATE, "no events uploaded");
+  if (!consts) return set_err(h, PWA_ERR_ARG, "null constants");
+  if (!h->shape_cache_ok)
+    return set_err(h, PWA_ERR_STATE,
+                   "the model's columns do not factorise (swaps, polarisation or CP totals)");
+  cudaStream_t s = (cudaStream_t)stream;
+  const long long n = h->n_data + h->n_mc, tile = h->tpb, ntiles = (n + tile - 1) / tile;
+  if (h->scache) cudaFree(h->scache);
+  h->scache = nullptr;
+  h->scache_n = 0;
+  if (cudaMalloc(&h->scache, sizeof(float2) * tile * h->nf * (size_t)ntiles) != cudaSuccess)
+    return set_err(h, PWA_ERR_OOM, "cudaMalloc of the floating-shape column cache failed");
+  std::vector<double> cbuf(consts, consts + h->nconst);
+  long long ld = h->ld;
+  void* args[] = {cbuf.data(), &h->xa, &h->xm, (void*)&n, (void*)&ntiles, &ld, &h->scache};
+  long long nb = (ntiles * tile + tile - 1) / tile;
+  if (nb > 16LL * h->sms) nb = 16LL * h->sms;
+  int rc = launch(h, h->k.cache_ns_f32, dim3((int)nb), dim3(h->tpb), args, s);
+  if (rc) return rc;
+  // persistent grid split between data and MC events as the plain kernels
+  int per_sm = 0;
+  CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)h->k.eval_shapecache,
+                                                   h->tpb, 0));
+  if (per_sm < 1) per_sm = 1;
+  const long long want = (long long)per_sm * h->sms;
+  long long gb = want < ntiles ? want : ntiles;
+  if (gb < 2) gb = 2;
+  long long bd = h->n_mc == 0 ? gb : (h->n_data == 0 ? 0 : (gb * h->n_data + n / 2) / n);
+  if (h->n_data > 0 && bd < 1) bd = 1;
+  if (h->n_mc > 0 && bd > gb - 1) bd = gb - 1;
+  rc = ensure_partials(h, gb * h->nacc);
+  if (rc) return rc;
+  h->sc_blocks = (int)gb;
+  h->sc_blocks_data = (int)bd;
+  CU(cudaStreamSynchronize(s));
+  h->scache_n = n;
+  return PWA_OK;
+}
+
+int pwa_eval_shapecache(pwa_plan* h, const double* consts, const double* ratio, void* stream,
+                        double* out) {
+  if (!h) return PWA_ERR_ARG;
+  if (!consts || !ratio || !out) return set_err(h, PWA_ERR_ARG, "null argument");
+  if (h->scache_n != h->n_data + h->n_mc || h->scache_n <= 0)
+    return set_err(h, PWA_ERR_STATE, "no floating-shape column cache (call pwa_shape_cache)");
+  cudaStream_t s = (cudaStream_t)stream;
+  std::vector<double> cbuf(consts, consts + h->nconst), rbuf(ratio, ratio + h->ncol);
+  long long nd = h->n_data, na = h->n_data + h->n_mc, ld = h->ld;
+  int bd = h->sc_blocks_data, nb = h->sc_blocks;
+  void* args[] = {cbuf.data(), rbuf.data(), &h->scache, &h->xm, &h->w, &nd, &na, &ld, &bd,
+                  &h->partials};
+  int rc = launch(h, h->k.eval_shapecache, dim3(nb), dim3(h->tpb), args, s);
+  if (rc) return rc;
+  int nacc = h->nacc;
+  void* args2[] = {&h->partials, &nacc, &bd, &nb, &h->d_out};
+  rc = launch(h, h->k.reduce, dim3(1), dim3(1024), args2, s);
+  if (rc) return rc;
+  CU(cudaMemcpyAsync(h->h_out, h->d_out, sizeof(double) * 2 * nacc, cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  std::memcpy(out, h->h_out, sizeof(double) * 2 * nacc);
   return PWA_OK;
 }
 

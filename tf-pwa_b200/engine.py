@@ -93,6 +93,8 @@ def load_library(path=LIB_PATH):
     lib.pwa_hessian_cached.argtypes = [vp, dp, ctypes.c_double, ctypes.c_double, vp, dp, dp, dp]
     lib.pwa_hessian_cached_exact.argtypes = [vp, dp, ctypes.c_double, vp, dp, dp, dp]
     lib.pwa_hess_sums_cached.argtypes = [vp, dp, vp, dp]
+    lib.pwa_shape_cache.argtypes = [vp, dp, vp]
+    lib.pwa_eval_shapecache.argtypes = [vp, dp, dp, vp, dp]
     lib.pwa_read_dat.argtypes = [cp, vp, ll, ctypes.POINTER(ll)]
     lib.pwa_server_create.argtypes = [vp, dp, dp, i, ctypes.c_double, i, ctypes.POINTER(vp)]
     lib.pwa_server_submit.argtypes = [vp, dp, vp, vp, vp, ll, ll, ctypes.POINTER(ll)]
@@ -128,6 +130,7 @@ EXPORTED = ("pwa_plan_create", "pwa_plan_destroy", "pwa_compile_only", "pwa_prec
             "pwa_pool_alloc", "pwa_pool_free", "pwa_pool_fill", "pwa_pieces_multi",
             "pwa_eval_noalloc", "pwa_fields_from_p4", "pwa_toy_select", "pwa_toy_fields",
             "pwa_hessian_cached", "pwa_hessian_cached_exact", "pwa_hess_sums_cached",
+            "pwa_shape_cache", "pwa_eval_shapecache",
             "pwa_read_dat", "pwa_server_create", "pwa_server_submit",
             "pwa_server_result", "pwa_server_stats", "pwa_server_destroy",
             "pwa_plan_info", "pwa_last_error")
@@ -214,6 +217,8 @@ class Engine:
         self._sw = None
         self._gram = None
         self.mc_share = 1.0      # this device's fraction of the total MC weight
+        self.use_shape_cache = False  # evaluations from the floating-shape column cache
+        self._sc_rho = None
         self.dist_reduce = None  # vector sum over devices (multi-GPU)
         self.device = "cuda"     # where the engine's tensors live
         self.toy_chunk = 1 << 24  # generator candidates per toy-kernel launch
@@ -852,6 +857,62 @@ class Engine:
                                             stream or 0, _dptr(out)), "pwa_eval")
         return out[:nacc], out[nacc:]
 
+    # ------------------------------------ floating shapes: shape-free columns
+    def _column_rho(self, C):
+        """Per column, the product of its barrier normalisations in the
+        constant block (sqrt(Pz0_l) per B' vertex, norm_l per normalised
+        one): the columns' only dependence on the shapes besides the
+        lineshapes themselves."""
+        if not hasattr(self, "_rho_terms"):
+            idx = self.code.consts.index
+            self._rho_terms = [[(kind == "sqrt", idx[name])
+                                for kind, name in self.code.column_barrier_consts(k)]
+                               for k in range(self.code.ncol)]
+        rho = np.ones(self.code.ncol)
+        for k, terms in enumerate(self._rho_terms):
+            for is_sqrt, j in terms:
+                v = C[j]
+                if is_sqrt:
+                    if not v > 0.0:
+                        raise PWAError("non-positive barrier normalisation: the columns do not "
+                                       "factorise at this shape setting")
+                    v = np.sqrt(v)
+                rho[k] *= v
+        return rho
+
+    def shape_cache(self, vals, stream=None):
+        """Build the floating-shape column cache (pwa_shape_cache): every
+        event's columns without their lineshapes, at the shapes in vals."""
+        if not self.code.shape_cache_ok:
+            raise PWAError("the floating-shape column cache needs one pass, no polarised "
+                           "parent and no CP-violating totals")
+        C = np.ascontiguousarray(self.consts(vals), np.float64)
+        rho = self._column_rho(C)
+        self._check(load_library().pwa_shape_cache(self.h, _dptr(C), stream or 0),
+                    "pwa_shape_cache")
+        self._sc_rho = rho
+
+    def _sc_ok(self, C):
+        """Whether the shape cache applies at this setting (every barrier
+        normalisation positive); otherwise the evaluation recomputes."""
+        try:
+            self._column_rho(C)
+            return True
+        except PWAError:
+            return False
+
+    def eval_sums_shapecache(self, C, stream=None):
+        """Sums of one evaluation from the floating-shape column cache (the
+        layout of eval_sums: data and MC rows of nacc)."""
+        nacc = self.code.nacc
+        C = np.ascontiguousarray(C, np.float64)
+        ratio = np.ascontiguousarray(self._column_rho(C) / self._sc_rho)
+        out = np.zeros(2 * nacc)
+        self._check(load_library().pwa_eval_shapecache(self.h, _dptr(C), _dptr(ratio),
+                                                       stream or 0, _dptr(out)),
+                    "pwa_eval_shapecache")
+        return out[:nacc], out[nacc:]
+
     def eval_enqueue(self, C, precision=PLAIN_F64, mc=True, stream=None):
         """Launch the evaluation kernels without waiting (for timing)."""
         C = np.ascontiguousarray(C, np.float64)
@@ -898,6 +959,8 @@ class Engine:
             sm[0] = float(np.real(Gm @ ck))
             sm[1:1 + 2 * K:2] = Gm.real
             sm[2:2 + 2 * K:2] = Gm.imag
+        elif self.use_shape_cache and precision != PLAIN_F64 and self._sc_ok(C):
+            sd, sm = self.eval_sums_shapecache(C, stream=stream)
         else:
             sd, sm = self.eval_sums(C, precision, mc=True, stream=stream)
         gd = self.grad_from_sums(J, D, sd)
