@@ -602,10 +602,12 @@ def measure_cached(name, args, rank, world, dist, timed, log, n_sig, n_bg, n_mc,
 
 # ------------------------------------------------- floating masses/widths
 def measure_floating(name, args, rank, world, dist, timed, log, n_sig, n_mc):
-    """Workload with floating lineshape parameters: no column cache applies,
-    so the chosen form is the FP32-amplitude recompute kernel (FP64 masses,
-    lineshape constants and sums) against the plain FP64 kernels; the
-    Hessian comes from differenced adjoint gradients."""
+    """Workload with floating lineshape parameters (no Gram matrix): the
+    chosen form is the floating-shape column cache (shape-free columns
+    cached in FP32, lineshapes recomputed from the resident masses every
+    evaluation, FP64 amplitude and sums), beside the FP32-amplitude
+    recompute form and the plain FP64 kernels; the Hessian comes from
+    differenced adjoint gradients."""
     import torch
 
     from tf_pwa_b200.api import FCN
@@ -617,10 +619,13 @@ def measure_floating(name, args, rank, world, dist, timed, log, n_sig, n_mc):
     cl, data, bg, mc = make_dataset(config, n_sig, n_mc, seed=1 + rank)
     t_data = time.perf_counter() - t0
     log(f"{name}: dataset {n_sig} data + {n_mc} MC events")
+    t0 = time.perf_counter()
     fcn = FCN(cl, data, mc, precision="mixed")
+    t_cache = time.perf_counter() - t0
     assert not fcn.use_gram
+    fcn_r = FCN(cl, data, mc, precision="mixed", shape_cache=False)
     fcn_p = FCN(cl, data, mc, precision="plain")
-    for f in (fcn, fcn_p):
+    for f in (fcn, fcn_r, fcn_p):
         f.eng.dist_reduce = _reduce_fn(dist)
         f.eng.mc_share = 1.0 / world  # equal MC shards
     x0 = np.array(cl.vm.get_all_val())
@@ -628,55 +633,75 @@ def measure_floating(name, args, rank, world, dist, timed, log, n_sig, n_mc):
     timed.do_flush = True  # its inputs fit in L2
     for _ in range(args.warmup):
         fcn.nll_grad(x0)
+        fcn_r.nll_grad(x0)
         fcn_p.nll_grad(x0)
     clocks = Clocks(_clocks_path(rank))
     clocks.start()
-    t_f32 = timed(lambda: fcn.nll_grad(x0), args.steps)
+    t_sc = timed(lambda: fcn.nll_grad(x0), args.steps)
+    t_f32 = timed(lambda: fcn_r.nll_grad(x0), args.steps)
     t_p = timed(lambda: fcn_p.nll_grad(x0), args.steps)
     C = fcn.eng.consts(vals)
-    t_k = timed(lambda: fcn.eng.eval_enqueue(C, MIXED_F32, mc=True), args.steps)
+    for _ in range(3):
+        fcn.eng.eval_shapecache_enqueue(C)
+    t_ks = timed(lambda: fcn.eng.eval_shapecache_enqueue(C), args.steps)
+    t_k = timed(lambda: fcn_r.eng.eval_enqueue(C, MIXED_F32, mc=True), args.steps)
     t_kp = timed(lambda: fcn_p.eng.eval_enqueue(C, PLAIN_F64, mc=True), args.steps)
     th = time.perf_counter()
     _, _, H = fcn.nll_grad_hessian(x0)
     t_hess = time.perf_counter() - th
     cov = np.linalg.inv(H)
     ck_clocks = clocks.stop(int(os.environ.get("LOCAL_RANK", "0")))
-    nll_f, g_f = fcn.nll_grad(x0)
+    nll_s, g_s = fcn.nll_grad(x0)
+    nll_f, g_f = fcn_r.nll_grad(x0)
     nll_p, g_p = fcn_p.nll_grad(x0)
     code = fcn.eng.code
     n_all = n_sig + n_mc
     bytes_f32 = n_all * (8 * len(code.mass_fields) + 4 * len(code.angle_fields) + 8)
     bytes_f64 = n_all * (8 * len(code.mass_fields) + 8 * len(code.angle_fields) + 8)
+    bytes_sc = n_all * (8 * code.nf + 8 * len(code.mass_fields) + 8)
     hbm, peak_kind = _peaks()
+    ach_s = bytes_sc / (t_ks / args.steps) / 1e9
     ach = bytes_f32 / (t_k / args.steps) / 1e9
     peaks = {"f64_tflops": fcn.eng.fma_peak(PLAIN_F64) / 1e12,
              "f32_tflops": fcn.eng.fma_peak(MIXED_F32) / 1e12}
-    roof = _mixed_pipe_roofline(name, n_all, t_k / args.steps, peaks)
-    roof.update({"kernel": "pwa_eval_f32 + pwa_reduce (data + MC, FP32 amplitudes)",
-                 "hbm": {"achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
-                         "peak_kind": peak_kind, "algorithmic_bytes_per_launch": bytes_f32}})
+    roof_r = _mixed_pipe_roofline(name, n_all, t_k / args.steps, peaks)
+    roof_r.update({"kernel": "pwa_eval_f32 + pwa_reduce (data + MC, FP32 amplitudes)",
+                   "hbm": {"achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                           "peak_kind": peak_kind, "algorithmic_bytes_per_launch": bytes_f32}})
     fl_p = NCU_F64_FLOPS_PER_EVENT[name]
     ach_p = fl_p * n_all / (t_kp / args.steps) / 1e12
-    roof["plain_f64_kernel"] = {
-        "bound": "fp64", "achieved": ach_p, "peak": peaks["f64_tflops"], "unit": "TFLOP/s",
-        "frac": ach_p / peaks["f64_tflops"], "flops_per_event": fl_p,
-        "flops_source": "ncu: 2 DFMA + DADD + DMUL executed per event (forward and adjoint)",
-        "launch_us": 1e6 * t_kp / args.steps, "algorithmic_bytes_per_launch": bytes_f64}
+    roof = {"bound": "hbm", "achieved": ach_s, "peak": hbm, "unit": "GB/s", "frac": ach_s / hbm,
+            "traffic": None, "peak_kind": peak_kind,
+            "kernel": "pwa_eval_shapecache + pwa_reduce (data + MC: FP32 shape-free columns, "
+                      "FP64 masses, lineshapes recomputed)",
+            "algorithmic_bytes_per_launch": bytes_sc, "launch_us": 1e6 * t_ks / args.steps,
+            "plain_f64_kernel": {
+                "bound": "fp64", "achieved": ach_p, "peak": peaks["f64_tflops"],
+                "unit": "TFLOP/s", "frac": ach_p / peaks["f64_tflops"], "flops_per_event": fl_p,
+                "flops_source": "ncu: 2 DFMA + DADD + DMUL executed per event (forward and "
+                                "adjoint)",
+                "launch_us": 1e6 * t_kp / args.steps, "algorithmic_bytes_per_launch": bytes_f64}}
     line = {
-        "metric": metric, "value": world * args.steps / t_f32, "unit": "evals/s",
+        "metric": metric, "value": world * args.steps / t_sc, "unit": "evals/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * t_f32 / args.steps, "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": 1e3 * t_sc / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": workload, "precision": "FP32 amplitudes recomputed from the "
-                   "angles every evaluation (FP64 masses, lineshape constants, log and sums); "
-                   "no column cache since masses and widths float",
+        "config": {"workload": workload, "precision": "floating-shape column cache: per-event "
+                   "partial-wave columns without their lineshapes cached as FP32 (computed in "
+                   "FP64), lineshapes and their derivatives recomputed in FP64 from the resident "
+                   "masses every evaluation, FP64 amplitude, log and sums",
                    "events_per_rank": {"data": n_sig, "mc": n_mc},
                    "l2": "256 MB buffer written before every timed step (L2 126 MB)",
                    "parallelism": f"dp{world}" if world > 1 else "single GPU"},
         "plain_f64": {"value": world * args.steps / t_p, "unit": "evals/s",
                       "ms_per_step": 1e3 * t_p / args.steps,
-                      "speedup_f32_over_plain": t_p / t_f32},
-        "e2e": {"value": world * args.steps / t_f32, "unit": "evals/s",
+                      "speedup_over_plain": t_p / t_sc},
+        "fp32_recompute": {"value": world * args.steps / t_f32, "unit": "evals/s",
+                           "ms_per_step": 1e3 * t_f32 / args.steps,
+                           "kernel_us": 1e6 * t_k / args.steps, "roofline": roof_r,
+                           "dnll": nll_f - nll_p,
+                           "grad_max_rel": float(np.max(np.abs(g_f - g_p)) / np.max(np.abs(g_p)))},
+        "e2e": {"value": world * args.steps / t_sc, "unit": "evals/s",
                 "h2d_bytes_per_step": 8 * len(x0), "d2h_bytes_per_step": 8 * (1 + len(x0)),
                 "call": "FCN.nll_grad(x) with x a host numpy vector"},
         "roofline": roof,
@@ -684,15 +709,15 @@ def measure_floating(name, args, rank, world, dist, timed, log, n_sig, n_mc):
         "gpu_launches": 2 * args.steps,
         "hessian": {"seconds": t_hess, "n_params": len(x0), "evaluations": 4 * len(x0) + 1,
                     "errors": dict(zip(names, np.sqrt(np.abs(np.diag(cov))).tolist()))},
-        "check": {"nll_f32": nll_f, "nll_plain": nll_p, "dnll": nll_f - nll_p,
-                  "grad_max_rel": float(np.max(np.abs(g_f - g_p)) / np.max(np.abs(g_p)))},
-        "setup_s": {"dataset": t_data},
+        "check": {"nll_shape_cache": nll_s, "nll_plain": nll_p, "dnll": nll_s - nll_p,
+                  "grad_max_rel": float(np.max(np.abs(g_s - g_p)) / np.max(np.abs(g_p)))},
+        "setup_s": {"dataset": t_data, "shape_cache_fcn": t_cache},
     }
     if ck_clocks:
         line["clocks"] = ck_clocks
-    fcn.eng.close()
-    fcn_p.eng.close()
-    del fcn, fcn_p, data, mc
+    for f in (fcn, fcn_r, fcn_p):
+        f.eng.close()
+    del fcn, fcn_r, fcn_p, data, mc
     torch.cuda.empty_cache()
     return line
 

@@ -151,6 +151,10 @@ int pwa_toy_fields(pwa_plan* h, unsigned long long seed, const long long* idx, l
 int pwa_shape_cache(pwa_plan* h, const double* consts, void* stream);
 int pwa_eval_shapecache(pwa_plan* h, const double* consts, const double* ratio, void* stream,
                         double* out);
+/* The same launches without the copy back (results in device memory, for
+ * timing or chaining on the stream). */
+int pwa_eval_shapecache_enqueue(pwa_plan* h, const double* consts, const double* ratio,
+                                void* stream);
 
 /* Hessian of the cached-form NLL with respect to the trainable parameters
  * (tf_pwa/model/model.py:513-561, BaseModel.nll_grad_hessian; errors via

@@ -614,10 +614,10 @@ int pwa_shape_cache(pwa_plan* h, const double* consts, void* stream) {
   return PWA_OK;
 }
 
-int pwa_eval_shapecache(pwa_plan* h, const double* consts, const double* ratio, void* stream,
-                        double* out) {
+int pwa_eval_shapecache_enqueue(pwa_plan* h, const double* consts, const double* ratio,
+                                void* stream) {
   if (!h) return PWA_ERR_ARG;
-  if (!consts || !ratio || !out) return set_err(h, PWA_ERR_ARG, "null argument");
+  if (!consts || !ratio) return set_err(h, PWA_ERR_ARG, "null argument");
   if (h->scache_n != h->n_data + h->n_mc || h->scache_n <= 0)
     return set_err(h, PWA_ERR_STATE, "no floating-shape column cache (call pwa_shape_cache)");
   cudaStream_t s = (cudaStream_t)stream;
@@ -630,8 +630,17 @@ int pwa_eval_shapecache(pwa_plan* h, const double* consts, const double* ratio, 
   if (rc) return rc;
   int nacc = h->nacc;
   void* args2[] = {&h->partials, &nacc, &bd, &nb, &h->d_out};
-  rc = launch(h, h->k.reduce, dim3(1), dim3(1024), args2, s);
+  return launch(h, h->k.reduce, dim3(1), dim3(1024), args2, s);
+}
+
+int pwa_eval_shapecache(pwa_plan* h, const double* consts, const double* ratio, void* stream,
+                        double* out) {
+  if (!h) return PWA_ERR_ARG;
+  if (!out) return set_err(h, PWA_ERR_ARG, "null output");
+  int rc = pwa_eval_shapecache_enqueue(h, consts, ratio, stream);
   if (rc) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int nacc = h->nacc;
   CU(cudaMemcpyAsync(h->h_out, h->d_out, sizeof(double) * 2 * nacc, cudaMemcpyDeviceToHost, s));
   CU(cudaStreamSynchronize(s));
   std::memcpy(out, h->h_out, sizeof(double) * 2 * nacc);

@@ -95,6 +95,7 @@ def load_library(path=LIB_PATH):
     lib.pwa_hess_sums_cached.argtypes = [vp, dp, vp, dp]
     lib.pwa_shape_cache.argtypes = [vp, dp, vp]
     lib.pwa_eval_shapecache.argtypes = [vp, dp, dp, vp, dp]
+    lib.pwa_eval_shapecache_enqueue.argtypes = [vp, dp, dp, vp]
     lib.pwa_read_dat.argtypes = [cp, vp, ll, ctypes.POINTER(ll)]
     lib.pwa_server_create.argtypes = [vp, dp, dp, i, ctypes.c_double, i, ctypes.POINTER(vp)]
     lib.pwa_server_submit.argtypes = [vp, dp, vp, vp, vp, ll, ll, ctypes.POINTER(ll)]
@@ -130,7 +131,7 @@ EXPORTED = ("pwa_plan_create", "pwa_plan_destroy", "pwa_compile_only", "pwa_prec
             "pwa_pool_alloc", "pwa_pool_free", "pwa_pool_fill", "pwa_pieces_multi",
             "pwa_eval_noalloc", "pwa_fields_from_p4", "pwa_toy_select", "pwa_toy_fields",
             "pwa_hessian_cached", "pwa_hessian_cached_exact", "pwa_hess_sums_cached",
-            "pwa_shape_cache", "pwa_eval_shapecache",
+            "pwa_shape_cache", "pwa_eval_shapecache", "pwa_eval_shapecache_enqueue",
             "pwa_read_dat", "pwa_server_create", "pwa_server_submit",
             "pwa_server_result", "pwa_server_stats", "pwa_server_destroy",
             "pwa_plan_info", "pwa_last_error")
@@ -865,19 +866,19 @@ class Engine:
         lineshapes themselves."""
         if not hasattr(self, "_rho_terms"):
             idx = self.code.consts.index
-            self._rho_terms = [[(kind == "sqrt", idx[name])
-                                for kind, name in self.code.column_barrier_consts(k)]
-                               for k in range(self.code.ncol)]
+            t = [(k, idx[name], kind == "sqrt") for k in range(self.code.ncol)
+                 for kind, name in self.code.column_barrier_consts(k)]
+            self._rho_terms = (np.array([x[0] for x in t], np.int64),
+                               np.array([x[1] for x in t], np.int64),
+                               np.array([x[2] for x in t], bool))
+        cols, slots, sq = self._rho_terms
+        v = np.asarray(C)[slots]
+        if np.any(sq & ~(v > 0.0)):
+            raise PWAError("non-positive barrier normalisation: the columns do not factorise "
+                           "at this shape setting")
+        v = np.where(sq, np.sqrt(np.where(sq, v, 1.0)), v)
         rho = np.ones(self.code.ncol)
-        for k, terms in enumerate(self._rho_terms):
-            for is_sqrt, j in terms:
-                v = C[j]
-                if is_sqrt:
-                    if not v > 0.0:
-                        raise PWAError("non-positive barrier normalisation: the columns do not "
-                                       "factorise at this shape setting")
-                    v = np.sqrt(v)
-                rho[k] *= v
+        np.multiply.at(rho, cols, v)
         return rho
 
     def shape_cache(self, vals, stream=None):
@@ -892,26 +893,36 @@ class Engine:
                     "pwa_shape_cache")
         self._sc_rho = rho
 
-    def _sc_ok(self, C):
-        """Whether the shape cache applies at this setting (every barrier
-        normalisation positive); otherwise the evaluation recomputes."""
+    def _sc_ratio(self, C):
+        """The columns' barrier-normalisation ratios to the cache's setting
+        (kept in self._ratio), or None where a normalisation is not positive
+        (the columns do not factorise there: the evaluation recomputes)."""
         try:
-            self._column_rho(C)
-            return True
+            self._ratio = np.ascontiguousarray(self._column_rho(C) / self._sc_rho)
         except PWAError:
-            return False
+            self._ratio = None
+        return self._ratio
 
-    def eval_sums_shapecache(self, C, stream=None):
+    def eval_sums_shapecache(self, C, stream=None, ratio=None):
         """Sums of one evaluation from the floating-shape column cache (the
         layout of eval_sums: data and MC rows of nacc)."""
         nacc = self.code.nacc
         C = np.ascontiguousarray(C, np.float64)
-        ratio = np.ascontiguousarray(self._column_rho(C) / self._sc_rho)
+        if ratio is None:
+            ratio = np.ascontiguousarray(self._column_rho(C) / self._sc_rho)
         out = np.zeros(2 * nacc)
         self._check(load_library().pwa_eval_shapecache(self.h, _dptr(C), _dptr(ratio),
                                                        stream or 0, _dptr(out)),
                     "pwa_eval_shapecache")
         return out[:nacc], out[nacc:]
+
+    def eval_shapecache_enqueue(self, C, stream=None):
+        """Launch one floating-shape-cache evaluation without waiting."""
+        C = np.ascontiguousarray(C, np.float64)
+        ratio = np.ascontiguousarray(self._column_rho(C) / self._sc_rho)
+        self._check(load_library().pwa_eval_shapecache_enqueue(self.h, _dptr(C), _dptr(ratio),
+                                                               stream or 0),
+                    "pwa_eval_shapecache_enqueue")
 
     def eval_enqueue(self, C, precision=PLAIN_F64, mc=True, stream=None):
         """Launch the evaluation kernels without waiting (for timing)."""
@@ -959,8 +970,8 @@ class Engine:
             sm[0] = float(np.real(Gm @ ck))
             sm[1:1 + 2 * K:2] = Gm.real
             sm[2:2 + 2 * K:2] = Gm.imag
-        elif self.use_shape_cache and precision != PLAIN_F64 and self._sc_ok(C):
-            sd, sm = self.eval_sums_shapecache(C, stream=stream)
+        elif self.use_shape_cache and precision != PLAIN_F64 and self._sc_ratio(C) is not None:
+            sd, sm = self.eval_sums_shapecache(C, stream=stream, ratio=self._ratio)
         else:
             sd, sm = self.eval_sums(C, precision, mc=True, stream=stream)
         gd = self.grad_from_sums(J, D, sd)
