@@ -873,13 +873,12 @@ class Engine:
                                np.array([x[2] for x in t], bool))
         cols, slots, sq = self._rho_terms
         v = np.asarray(C)[slots]
-        if np.any(sq & ~(v > 0.0)):
+        if not np.all(v > 0.0):  # B' normalisations and 1 / |q0^2|^(l/2) are positive
             raise PWAError("non-positive barrier normalisation: the columns do not factorise "
                            "at this shape setting")
-        v = np.where(sq, np.sqrt(np.where(sq, v, 1.0)), v)
-        rho = np.ones(self.code.ncol)
-        np.multiply.at(rho, cols, v)
-        return rho
+        # product per column as exp of the summed logs (sqrt terms at half weight)
+        return np.exp(np.bincount(cols, weights=np.where(sq, 0.5, 1.0) * np.log(v),
+                                  minlength=self.code.ncol))
 
     def shape_cache(self, vals, stream=None):
         """Build the floating-shape column cache (pwa_shape_cache): every
