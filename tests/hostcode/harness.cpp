@@ -44,11 +44,21 @@ static void sums_t(const Consts& C, const R* XA, const double* XM, const double*
 // out[0 .. PWA_NACC): data sums, out[PWA_NACC .. 2 PWA_NACC): MC sums.
 // XA holds FP64 angles; with f32 != 0 they are rounded to FP32 first (the
 // FP32-recompute form stores its angle fields as FP32).
+// the constant block as the library packs it: FP64 values, then each
+// one's FP32 rounding and the FP32 rounding of the rest
+static void fill_consts(Consts& C, const double* Cv) {
+  for (int j = 0; j < PWA_NCONST; ++j) {
+    C.v[j] = Cv[j];
+    C.h[j] = (float)Cv[j];
+    C.l[j] = (float)(Cv[j] - (double)C.h[j]);
+  }
+}
+
 extern "C" int hx_sums(const double* Cv, const double* XM, const double* XA, const double* W,
                        long long n_data, long long n_all, long long ld, int f32, int stash,
                        double* out) {
   Consts C;
-  for (int j = 0; j < PWA_NCONST; ++j) C.v[j] = Cv[j];
+  fill_consts(C, Cv);
   if (f32) {
     std::vector<float> xa((size_t)PWA_NANGLE_ROWS * ld);
     for (size_t j = 0; j < xa.size(); ++j) xa[j] = (float)XA[j];
@@ -87,7 +97,7 @@ static void amp_t(const Consts& C, const R* XA, const double* XM, long long n, l
 extern "C" int hx_amp(const double* Cv, const double* XM, const double* XA, long long n,
                       long long ld, int f32, double* out) {
   Consts C;
-  for (int j = 0; j < PWA_NCONST; ++j) C.v[j] = Cv[j];
+  fill_consts(C, Cv);
   if (f32) {
     std::vector<float> xa((size_t)PWA_NANGLE_ROWS * ld);
     for (size_t j = 0; j < xa.size(); ++j) xa[j] = (float)XA[j];
@@ -102,7 +112,7 @@ extern "C" int hx_amp(const double* Cv, const double* XM, const double* XA, long
 extern "C" int hx_columns(const double* Cv, const double* XM, const double* XA, long long n,
                           long long ld, double* out) {
   Consts C;
-  for (int j = 0; j < PWA_NCONST; ++j) C.v[j] = Cv[j];
+  fill_consts(C, Cv);
   for (long long i = 0; i < n; ++i) {
     cpx<double> F[PWA_NCOL * PWA_NOUT];
     model_columns<double, false>(C, XA, XM, ld, i, F);
@@ -118,7 +128,7 @@ extern "C" int hx_columns(const double* Cv, const double* XM, const double* XA, 
 extern "C" int hx_columns_ns(const double* Cv, const double* XM, const double* XA, long long n,
                              long long ld, double* out) {
   Consts C;
-  for (int j = 0; j < PWA_NCONST; ++j) C.v[j] = Cv[j];
+  fill_consts(C, Cv);
   for (long long i = 0; i < n; ++i) {
     cpx<double> F[PWA_NCOL * PWA_NOUT];
     model_columns_ns<double, false>(C, XA, XM, ld, i, F);
@@ -135,7 +145,7 @@ extern "C" int hx_columns_ns(const double* Cv, const double* XM, const double* X
 extern "C" int hx_shapes(const double* Cv, const double* XM, long long n, long long ld,
                          double* out) {
   Consts C;
-  for (int j = 0; j < PWA_NCONST; ++j) C.v[j] = Cv[j];
+  fill_consts(C, Cv);
   constexpr int NS = PWA_NSRES > 0 ? PWA_NSRES : 1, W = PWA_NCHAIN + 2 * NS;
   for (long long i = 0; i < n; ++i) {
     cpx<double> BW[PWA_NCHAIN], DM[NS], DG[NS];
@@ -173,7 +183,7 @@ extern "C" int hx_toy(const double* Cv, unsigned long long seed, long long first
                       double* wps, double* u_ps, double* u_amp, double* f_out, double* P4,
                       double* fields) {
   Consts C;
-  for (int j = 0; j < PWA_NCONST; ++j) C.v[j] = Cv[j];
+  fill_consts(C, Cv);
   for (long long i = 0; i < n; ++i) {
     double U[PWA_NDRAW];
     event_uniforms(seed, (unsigned long long)(first + i), U);

@@ -37,7 +37,44 @@ _HEADER = """
 #define PWA_NSHAPE {nshape}
 #define PWA_NACC {nacc}
 #define PWA_NCONST {nconst}
-struct Consts {{ double v[PWA_NCONST]; }};
+// the constant block of one evaluation; h, l: each constant's FP32 rounding
+// and the FP32 rounding of the rest, split once per evaluation on the host
+struct Consts {{ double v[PWA_NCONST]; float h[PWA_NCONST]; float l[PWA_NCONST]; }};
+// constant i as R (the FP32 kernels read its FP32 rounding: no per-event
+// conversion)
+template <typename R>
+__device__ __forceinline__ R cR(const Consts& C, int i) {{
+  if constexpr (sizeof(R) == 4) return C.h[i];
+  else return C.v[i];
+}}
+// products with constant i: FP32 hi + lo parts in the FP32 kernels (the
+// rounding of a constant, alike for every event, must not bias the sums), a
+// plain product in FP64 -- mulk / cfmak / cmulk with the split precomputed
+template <typename R>
+__device__ __forceinline__ R mulkc(R x, const Consts& C, int i) {{
+  if constexpr (sizeof(R) == 4) return fmaf(x, C.h[i], x * C.l[i]);
+  else return x * C.v[i];
+}}
+template <typename R>
+__device__ __forceinline__ void cfmakc(cpx<R>& acc, R s, const Consts& C, int ir, int ii) {{
+  if constexpr (sizeof(R) == 4) {{
+    acc.re = fmaf(s, C.h[ir], fmaf(s, C.l[ir], acc.re));
+    acc.im = fmaf(s, C.h[ii], fmaf(s, C.l[ii], acc.im));
+  }} else {{
+    acc.re = fma(s, C.v[ir], acc.re);
+    acc.im = fma(s, C.v[ii], acc.im);
+  }}
+}}
+template <typename R>
+__device__ __forceinline__ cpx<R> cmulkc(const Consts& C, int ir, int ii, cpx<R> z) {{
+  if constexpr (sizeof(R) == 4) {{
+    const cpx<float> a = cmul(cmk<float>(C.h[ir], C.h[ii]), z);
+    const cpx<float> b = cmul(cmk<float>(C.l[ir], C.l[ii]), z);
+    return cmk<float>(a.re + b.re, a.im + b.im);
+  }} else {{
+    return cmul(cmk<double>(C.v[ir], C.v[ii]), z);
+  }}
+}}
 """
 
 
@@ -273,7 +310,10 @@ class ModelCode:
 
     # ------------------------------------------------------------ helpers
     def _cst(self, name):
-        return f"R(C.v[{self.consts.index[name]}])"
+        return f"cR<R>(C, {self.consts.index[name]})"
+
+    def _ci(self, name):
+        return str(self.consts.index[name])
 
     def _cv(self, name):
         """The FP64 constant itself (for mulk / cfmak / cmulk, which keep
@@ -448,13 +488,13 @@ class ModelCode:
                         poly = _lit(co[0])
                         for cc_ in co[1:]:
                             poly = f"fma({poly}, {z}, {_lit(cc_)})"
-                        e(f"  R bp_{tag}_{l} = mulk<R>(R(1) / ({poly}), {self._cv(f'{d}.Pz0_{l}')});")
+                        e(f"  R bp_{tag}_{l} = mulkc<R>(R(1) / ({poly}), C, {self._ci(f'{d}.Pz0_{l}')});")
                         e(f"  bp_{tag}_{l} = bp_{tag}_{l} > R(0) ? bp_{tag}_{l} : R(1);")
                         bf = f"({ql}) * psqrt(bp_{tag}_{l})"
                     else:
                         bf = ql
                     if d.barrier_factor_norm:
-                        bf = f"mulk<R>({bf}, {self._cv(f'{d}.norm_{l}')})"
+                        bf = f"mulkc<R>({bf}, C, {self._ci(f'{d}.norm_{l}')})"
                     e(f"  const R bf_{tag}_{l} = {bf};")
             # D*^{Ja}_{la, lb-lc}(alpha, beta, 0); indices are 2m + 2J
             j2 = two(a.J)
@@ -540,11 +580,11 @@ class ModelCode:
                 poly = _lit(co[0])
                 for cc_ in co[1:]:
                     poly = f"fma({poly}, {z}, {_lit(cc_)})"
-                e(f"  const R rr_{tag} = mulk<R>(qq_{tag}, {self._cv(f'{p}.iq02')});")
+                e(f"  const R rr_{tag} = mulkc<R>(qq_{tag}, C, {self._ci(f'{p}.iq02')});")
                 ph = f"psqrt(rr_{tag} < R(0) ? -rr_{tag} : rr_{tag})"
                 for _ in range(L_):
                     ph = f"{ph} * rr_{tag}"
-                e(f"  const R ya_{tag} = mulk<R>(({ph}) / (R({m}) * ({poly})), {self._cv(f'{p}.K')});")
+                e(f"  const R ya_{tag} = mulkc<R>(({ph}) / (R({m}) * ({poly})), C, {self._ci(f'{p}.K')});")
                 e(f"  const R y_{tag} = rr_{tag} < R(0) ? R(0) : ya_{tag};")
                 e(f"  const R yi_{tag} = rr_{tag} < R(0) ? ya_{tag} : R(0);")
                 e(f"  const R dre_{tag} = xr_{tag} + yi_{tag};")
@@ -563,7 +603,7 @@ class ModelCode:
                         poly = f"fma({poly}, {z}, {_lit(cc_)})"
                     qp = "*".join([f"q_{tag}"] * (2 * L_ + 1))
                     e(f"  const R qp_{tag} = {cst(f'{p}.useq')} != R(0) ? ({qp}) : R(1);")
-                    e(f"  const R y_{tag} = mulk<R>(qp_{tag} / (R({m}) * ({poly})), {self._cv(f'{p}.K')});")
+                    e(f"  const R y_{tag} = mulkc<R>(qp_{tag} / (R({m}) * ({poly})), C, {self._ci(f'{p}.K')});")
                     e(f"  const R s_{tag} = xr_{tag} * xr_{tag} + y_{tag} * y_{tag};")
                     e(f"  const cpx<R> bw_{tag} = cmk<R>(xr_{tag} / s_{tag}, y_{tag} / s_{tag});")
                 else:
@@ -575,9 +615,9 @@ class ModelCode:
                     e(f"    bw_{tag} = cmk<R>(R(xd / sd), R(yd / sd)); }}")
             if p.width_norm_applies():
                 # the chain product takes Gamma0 R (the derivatives use R)
-                wn = self._cv(f'{p}.wn')
-                bw_names[-1] = (f"cmk<R>(mulk<R>(bw_{tag}.re, {wn}), "
-                                f"mulk<R>(bw_{tag}.im, {wn}))")
+                wn = self._ci(f'{p}.wn')
+                bw_names[-1] = (f"cmk<R>(mulkc<R>(bw_{tag}.re, C, {wn}), "
+                                f"mulkc<R>(bw_{tag}.im, C, {wn}))")
         if bw_names:
             e(f"  cpx<R> BW_c{ci} = {bw_names[0]};")
             for nm in bw_names[1:]:
@@ -645,8 +685,8 @@ class ModelCode:
                             l = ls[i][0]
                             bfv = f"bf_c{ci}v{vi}_{l} * " if d.has_barrier_factor else ""
                             g = f"{d}.g{i}"
-                            e(f"  cfmak({nm}, {self._kcoef(cgv, bfv)}, {self._cv(g + '.re')}, "
-                              f"{self._cv(g + '.im')});")
+                            e(f"  cfmakc({nm}, {self._kcoef(cgv, bfv)}, C, {self._ci(g + '.re')}, "
+                              f"{self._ci(g + '.im')});")
             pre = {}
             for facs, po, coefs in self.chain_assign[ci]:
                 if any((vi, ib, ic) not in hnames for (vi, _, _, ib, ic) in facs):
@@ -666,15 +706,19 @@ class ModelCode:
                         prod = f"cmul({prod}, {v})"
                     e(f"  cfmac({nm}, {prod}, {vs[-1]});")
             cur = self._emit_align_forward(e, ci, pre, "Aa")
-            tre, tim = self._cv(f"t{ci}.re"), self._cv(f"t{ci}.im")
             if ci in self.cp_chains and self.ncp:
-                tre = f"(cc ? {self._cv(f't{ci}m.re')} : {tre})"
-                tim = f"(cc ? {self._cv(f't{ci}m.im')} : {tim})"
-            if self._factor() == 1.0:
-                e(f"  const cpx<R> E_c{ci} = cmulk<R>({tre}, {tim}, BW_c{ci});")
+                # per-event charge selects the total: the FP64 values (a
+                # thread-dependent index into the constant block would copy it
+                # to local memory)
+                tre = f"(cc ? {self._cv(f't{ci}m.re')} : {self._cv(f't{ci}.re')})"
+                tim = f"(cc ? {self._cv(f't{ci}m.im')} : {self._cv(f't{ci}.im')})"
+                tot = f"cmulk<R>({tre}, {tim}, BW_c{ci})"
             else:
-                e(f"  const cpx<R> E_c{ci} = cscale(cmulk<R>({tre}, {tim}, BW_c{ci}), "
-                  f"{_lit(self._factor())});")
+                tot = f"cmulkc<R>(C, {self._ci(f't{ci}.re')}, {self._ci(f't{ci}.im')}, BW_c{ci})"
+            if self._factor() == 1.0:
+                e(f"  const cpx<R> E_c{ci} = {tot};")
+            else:
+                e(f"  const cpx<R> E_c{ci} = cscale({tot}, {_lit(self._factor())});")
             for o, nm in cur.items():
                 e(f"  cfmac(A{self._out(o)}, E_c{ci}, {nm});")
             e("  }")

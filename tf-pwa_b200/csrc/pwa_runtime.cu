@@ -168,6 +168,24 @@ int ensure_partials(pwa_plan* h, long long n) {
   return PWA_OK;
 }
 
+// The kernels' constant block (struct Consts of the model source): the
+// FP64 constants, then each one's FP32 rounding and the FP32 rounding of the
+// rest, so the FP32 kernels take their hi + lo parts without converting
+// per event.  consts may be null (all zero).
+std::vector<double> consts_block(const pwa_plan* h, const double* consts) {
+  const int n = h->nconst;
+  std::vector<double> b(2 * (size_t)n, 0.0);
+  if (consts) std::copy(consts, consts + n, b.begin());
+  float* f = reinterpret_cast<float*>(b.data() + n);
+  for (int i = 0; i < n; ++i) {
+    const double v = b[i];
+    const float hi = (float)v;
+    f[i] = hi;
+    f[n + i] = (float)(v - (double)hi);
+  }
+  return b;
+}
+
 void free_events(pwa_plan* h) {
   if (h->xm) cudaFree(h->xm);
   if (h->xa) cudaFree(h->xa);
@@ -536,7 +554,7 @@ int pwa_eval_enqueue(pwa_plan* h, const double* consts, int precision, int mc, v
   if (!consts || (precision != PWA_PLAIN_F64 && precision != PWA_MIXED_F32))
     return set_err(h, PWA_ERR_ARG, "invalid eval arguments");
   cudaStream_t s = (cudaStream_t)stream;
-  std::vector<double> cbuf(consts, consts + h->nconst);
+  std::vector<double> cbuf = consts_block(h, consts);
   long long n_all = mc ? h->n_data + h->n_mc : h->n_data;
   const bool f64 = precision == PWA_PLAIN_F64;
   const int nb_all = f64 ? h->nblocks : h->nblocks32;
@@ -587,7 +605,7 @@ int pwa_shape_cache(pwa_plan* h, const double* consts, void* stream) {
   h->scache_n = 0;
   if (cudaMalloc(&h->scache, sizeof(float2) * tile * h->nf * (size_t)ntiles) != cudaSuccess)
     return set_err(h, PWA_ERR_OOM, "cudaMalloc of the floating-shape column cache failed");
-  std::vector<double> cbuf(consts, consts + h->nconst);
+  std::vector<double> cbuf = consts_block(h, consts);
   long long ld = h->ld;
   void* args[] = {cbuf.data(), &h->xa, &h->xm, (void*)&n, (void*)&ntiles, &ld, &h->scache};
   long long nb = (ntiles * tile + tile - 1) / tile;
@@ -621,7 +639,7 @@ int pwa_eval_shapecache_enqueue(pwa_plan* h, const double* consts, const double*
   if (h->scache_n != h->n_data + h->n_mc || h->scache_n <= 0)
     return set_err(h, PWA_ERR_STATE, "no floating-shape column cache (call pwa_shape_cache)");
   cudaStream_t s = (cudaStream_t)stream;
-  std::vector<double> cbuf(consts, consts + h->nconst), rbuf(ratio, ratio + h->ncol);
+  std::vector<double> cbuf = consts_block(h, consts), rbuf(ratio, ratio + h->ncol);
   long long nd = h->n_data, na = h->n_data + h->n_mc, ld = h->ld;
   int bd = h->sc_blocks_data, nb = h->sc_blocks;
   void* args[] = {cbuf.data(), rbuf.data(), &h->scache, &h->xm, &h->w, &nd, &na, &ld, &bd,
@@ -655,7 +673,7 @@ int pwa_eval_pdf(pwa_plan* h, const double* consts, int precision, long long beg
     return set_err(h, PWA_ERR_ARG, "invalid pdf arguments");
   if (end == beg) return PWA_OK;
   cudaStream_t s = (cudaStream_t)stream;
-  std::vector<double> cbuf(consts, consts + h->nconst);
+  std::vector<double> cbuf = consts_block(h, consts);
   const void* xa = precision == PWA_PLAIN_F64 ? (const void*)h->xa : (const void*)h->xa32;
   long long ld = h->ld;
   void* args[] = {cbuf.data(), (void*)&xa, &h->xm, &beg, &end, &ld, &out_dev};
@@ -690,8 +708,7 @@ int pwa_toy_select(pwa_plan* h, const double* consts, unsigned long long seed, l
     return set_err(h, PWA_ERR_ARG, "invalid toy_select arguments");
   if (n == 0) return PWA_OK;
   cudaStream_t s = (cudaStream_t)stream;
-  std::vector<double> cbuf(h->nconst, 0.0);
-  if (consts) cbuf.assign(consts, consts + h->nconst);
+  std::vector<double> cbuf = consts_block(h, consts);
   void* args[] = {cbuf.data(), &seed, &first, &n, &fmax, &flat, &out};
   const size_t smem = sizeof(double) * (size_t)(h->n_mass + h->n_angle) * h->tpb;
   if (smem > 48 * 1024)
@@ -781,7 +798,7 @@ int pwa_build_gram(pwa_plan* h, const double* consts, void* stream, double* out)
   if (!consts) return set_err(h, PWA_ERR_ARG, "invalid gram arguments");
   cudaStream_t s = (cudaStream_t)stream;
   const bool tc = h->gram_method == 1 && 2 * h->ncol <= 64;
-  std::vector<double> cbuf(consts, consts + h->nconst);
+  std::vector<double> cbuf = consts_block(h, consts);
   const long long row = 2LL * h->ncol * h->nout;
   // chunked: columns of at most `chunk` events at a time
   long long chunk = (256LL << 20) / (8 * row);
@@ -874,7 +891,7 @@ int pwa_cache_data(pwa_plan* h, const double* consts, void* stream) {
     h->ntiles_cap = ntiles;
   }
   h->ntiles = ntiles;
-  std::vector<double> cbuf(consts, consts + h->nconst);
+  std::vector<double> cbuf = consts_block(h, consts);
   long long ld = h->ld, nt = ntiles;
   void* args[] = {cbuf.data(), &h->xa, &h->xm, &h->w, (void*)&n, &nt, &ld, &h->fcache,
                   &h->wcache};
@@ -1442,7 +1459,7 @@ int pwa_pool_fill(pwa_plan* h, long long first_tile, const double* consts, const
   if (ntl < 0) return set_err(h, PWA_ERR_ARG, "tile run not allocated");
   if ((n + h->tpb - 1) / h->tpb > ntl) return set_err(h, PWA_ERR_ARG, "events exceed the tile run");
   cudaStream_t s = (cudaStream_t)stream;
-  std::vector<double> cbuf(consts, consts + h->nconst);
+  std::vector<double> cbuf = consts_block(h, consts);
   float2* fdst = h->pool_f + first_tile * h->nf * (long long)h->tpb;
   double* wdst = h->pool_w + first_tile * (long long)h->tpb;
   void* args[] = {cbuf.data(), (void*)&xa, (void*)&xm, (void*)&w, &n, &ntl, &ld, &fdst, &wdst};
@@ -2113,7 +2130,7 @@ extern "C" int pwa_eval_noalloc(pwa_plan* h, const double* consts, const double*
   // nothing in the scratch must start at zero: every launched block writes
   // its whole partial row before pwa_reduce reads it
   cudaStream_t s = (cudaStream_t)stream;
-  std::vector<double> cbuf(consts, consts + h->nconst);
+  std::vector<double> cbuf = consts_block(h, consts);
   long long n_all = n;
   void* args[] = {cbuf.data(), (void*)&xa, (void*)&xm, (void*)&w, &n_data, &n_all, &ld,
                   &blocks_data, &scratch};
