@@ -382,12 +382,12 @@ NCU_F64_FLOPS_PER_EVENT = {
 # FP32 and FP64 operations per event of the FP32-amplitude kernel
 # (pwa_eval_f32), same captures: 2 * FFMA + FMUL + FADD, 2 * DFMA + DMUL + DADD
 NCU_F32_KERNEL_FLOPS = {
-    "d2kpipi_float": ((2 * 121909312 + 50303104 + 6151552) / 5e5,
-                      (2 * 47750000 + 25250000 + 27795200) / 5e5),
-    "lc2pkpi": ((2 * 658350000 + 309225000 + 22050000) / 5.25e5,
-                (2 * 94500000 + 55975000 + 99693704) / 5.25e5),
-    "b2dstkpi": ((2 * 1581000000 + 929500000 + 80000000) / 5e5,
-                 (2 * 99600000 + 57500000 + 268206080) / 5e5),
+    "d2kpipi_float": ((2 * 125378880 + 49568320 + 6189440) / 5e5,
+                      (2 * 47750000 + 25250000 + 27289040) / 5e5),
+    "lc2pkpi": ((2 * 655654656 + 305706984 + 22125776) / 5.25e5,
+                (2 * 94500000 + 55975000 + 71343704) / 5.25e5),
+    "b2dstkpi": ((2 * 1563318624 + 906727936 + 80454656) / 5e5,
+                 (2 * 99600000 + 57500000 + 136206080) / 5e5),
 }
 
 
