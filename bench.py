@@ -640,6 +640,20 @@ def measure_floating(name, args, rank, world, dist, timed, log, n_sig, n_mc):
     t_sc = timed(lambda: fcn.nll_grad(x0), args.steps)
     t_f32 = timed(lambda: fcn_r.nll_grad(x0), args.steps)
     t_p = timed(lambda: fcn_p.nll_grad(x0), args.steps)
+    # as in a fit: every evaluation at a new mass/width setting (two points
+    # alternating), so the lineshape and barrier constants are rebuilt each time
+    x1 = x0.copy()
+    for i, n in enumerate(names):
+        if n.endswith(("_mass", "_width")):
+            x1[i] *= 1.0 + 1e-6
+    pts = [x0, x1]
+    t_mv = timed(lambda: fcn.nll_grad(pts[fcn.n_call % 2]), args.steps)
+    # the same two timings with the host side in the engine's Python code
+    native = fcn.native_host
+    fcn.native_host = False
+    t_py = timed(lambda: fcn.nll_grad(x0), args.steps)
+    t_py_mv = timed(lambda: fcn.nll_grad(pts[fcn.n_call % 2]), args.steps)
+    fcn.native_host = native
     C = fcn.eng.consts(vals)
     for _ in range(3):
         fcn.eng.eval_shapecache_enqueue(C)
@@ -705,6 +719,17 @@ def measure_floating(name, args, rank, world, dist, timed, log, n_sig, n_mc):
                 "h2d_bytes_per_step": 8 * len(x0), "d2h_bytes_per_step": 8 * (1 + len(x0)),
                 "call": "FCN.nll_grad(x) with x a host numpy vector"},
         "roofline": roof,
+        "host": {"native": bool(fcn.native_host),
+                 "us_per_step": 1e6 * (t_sc - t_ks) / args.steps,
+                 "what": "FCN.nll_grad step minus the device time of its kernels: parameter "
+                         "copy, constants, Jacobian, launch, result read, chain rule",
+                 "moving_point": {"ms_per_step": 1e3 * t_mv / args.steps,
+                                  "value": world * args.steps / t_mv,
+                                  "what": "each evaluation at a new mass/width setting"},
+                 "python_host": {"ms_per_step": 1e3 * t_py / args.steps,
+                                 "moving_point_ms_per_step": 1e3 * t_py_mv / args.steps,
+                                 "what": "the same steps with the host side in the engine's "
+                                         "Python code (Engine.nll_grad)"}},
         "fma_peaks": peaks,
         "gpu_launches": 2 * args.steps,
         "hessian": {"seconds": t_hess, "n_params": len(x0), "evaluations": 4 * len(x0) + 1,

@@ -42,6 +42,7 @@ extern "C" {
 
 typedef struct pwa_plan pwa_plan;
 typedef struct pwa_server pwa_server;
+typedef struct pwa_hostprog pwa_hostprog;
 
 enum {
   PWA_OK = 0,
@@ -283,6 +284,70 @@ int pwa_pieces_points(pwa_plan* h, int n_pts, const double* vars, double sw, dou
                       void* stream, double* out);
 int pwa_nll_grad_cached(pwa_plan* h, const double* vars, double sw, void* stream,
                         double* out_nll, double* out_grad);
+
+/* ---- evaluations from the variable vector (host program) ---------------
+ * The host side of one evaluation in native code: the reference builds the
+ * couplings, lineshape and barrier constants from its variables and applies
+ * the chain rule per evaluation (tf_pwa/model/model.py:407-449,
+ * tf_pwa/amp/core.py:349-418,1072-1104, tf_pwa/variable.py:1715-1765).  A
+ * host program holds, for one model and one variable layout, what that
+ * takes; it needs no device and runs on the host alone.
+ *
+ * Format: ip (int) and dp (double) arrays read in order
+ *   ip: 0x50574850, 1, ncol, nconst, nshape, n_vars, n_train, n_coup, nfac,
+ *       coup_r[n_coup], coup_i[n_coup], coup_polar[n_coup] (the couplings'
+ *       variable indices, polar r e^{i phi} or r + i phi),
+ *       col_fac[ncol*nfac] (column k = product of couplings, -1 unused),
+ *       train_idx[n_train],
+ *       n_vg, n_vg x (coupling, re slot, im slot) (vertex couplings and
+ *       chain totals in the constant block),
+ *       n_m, m_var[n_m] (variable of each listed mass, -1 fixed),
+ *       n_vt, per vertex: ia, ib, ic (mass indices of a -> b c), no_q0,
+ *         n_e, per entry: l, has_bprime, norm, Pz0 slot, norm slot, n_coef,
+ *       n_ls, per lineshape: kind (0 BW, 1 BWR, 2 BWR2), m0, mb, mc (mass
+ *         indices), L, width variable (-1 fixed), slots m0sq, K, useq, y,
+ *         iq02, wn, kappa_m, inv_g0 (-1 absent), n_coef,
+ *       n_sel, n_sel x (variable, shape sum) (d f / d variable through
+ *         that sum of the kernels),
+ *       n_mj, per resonance mass with barrier factors: variable, mass
+ *         index, n_verts, verts[], n_c, n_c x (column, vertex, entry),
+ *       n_rt, n_rt x (column, slot, sqrt) (barrier normalisations of each
+ *         column), 0x50574850
+ *   dp: m_base[n_m] (masses of the fixed entries), per vertex d and per
+ *       entry coef[n_coef] (B' polynomial, highest power first), per
+ *       lineshape d, default width, coef[n_coef].
+ * PWA_ERR_ARG (message in pwa_last_error(NULL)) for a malformed program. */
+int pwa_hostprog_create(const int* ip, long long n_ip, const double* dp, long long n_dp,
+                        pwa_hostprog** out);
+int pwa_hostprog_destroy(pwa_hostprog* p);
+/* The constant block (nconst doubles) of the kernels at vars[n_vars]. */
+int pwa_hostprog_consts(pwa_hostprog* p, const double* vars, double* out);
+/* J[2*(t*ncol + k)] (re, im): d c_k / d vars[train_idx[t]];
+ * D[t*nshape + j]: its selector of shape sum j. */
+int pwa_hostprog_jacobian(pwa_hostprog* p, const double* vars, double* J, double* D);
+/* Piece vector (pwa_pieces_cached layout) from the kernels' data and MC
+ * sums sd, sm (1 + 2*ncol + nshape each). */
+int pwa_hostprog_pieces(pwa_hostprog* p, const double* vars, const double* sd, const double* sm,
+                        double sw, double mc_share, double* out);
+/* Each column's product of its barrier normalisations in a constant block
+ * (PWA_ERR_ARG where one is not positive). */
+int pwa_hostprog_column_rho(const pwa_hostprog* p, const double* consts, double* out);
+
+enum { PWA_FORM_PLAIN_F64 = 0, PWA_FORM_MIXED_F32 = 1, PWA_FORM_SHAPE_CACHE = 2 };
+
+/* A copy of p for this plan's evaluations (sizes must match the plan). */
+int pwa_set_host_program(pwa_plan* h, const pwa_hostprog* p);
+/* Piece vector of one evaluation at vars: constants and Jacobian from the
+ * plan's host program, the kernels of `form` (FP64, FP32 amplitudes, or the
+ * floating-shape column cache of pwa_shape_cache, which falls back to FP32
+ * amplitudes at a point where a barrier normalisation is not positive), the
+ * chain rule.  BaseModel.nll_grad_batch, tf_pwa/model/model.py:739-759. */
+int pwa_pieces_vars(pwa_plan* h, const double* vars, int form, double sw, double mc_share,
+                    void* stream, double* out);
+/* NLL and gradient of one device's events (FCN.nll_grad,
+ * tf_pwa/model/model.py:1223-1229). */
+int pwa_nll_grad_vars(pwa_plan* h, const double* vars, int form, double sw, void* stream,
+                      double* out_nll, double* out_grad);
 
 /* ---- many concurrent fits (serving) ------------------------------------
  * A pool of column-cache tiles (PWA_TPB events each) holds the data events

@@ -62,6 +62,28 @@ def host_engine(monkeypatch, tmp_path):
         x, w, nd = self._hx
         return self._host.sums(C, x, w, nd, f32=precision == E.MIXED_F32)
 
+    # the native host program runs as in the product; only the kernels'
+    # sums come from the host-compiled model code
+    def set_host_program(self, var_names, train_names):
+        self._hp = self.host_program(var_names, train_names)
+        self._hp_train = len(train_names)
+
+    def pieces_vars(self, var_values, form, mc_share=None, stream=None):
+        v = np.asarray(var_values, np.float64)
+        C = self._hp.consts(v)
+        sd, sm = self.eval_sums(C, E.PLAIN_F64 if form == E.FORM_PLAIN_F64 else E.MIXED_F32)
+        share = self.mc_share if mc_share is None else mc_share
+        return self._hp.pieces(v, sd, sm, self._sw, share)
+
+    def nll_grad_vars(self, var_values, form, stream=None):
+        vec = self.pieces_vars(var_values, form, stream=stream)
+        if self.dist_reduce is not None:
+            vec = self.dist_reduce(vec)
+        return E.combine_pieces(vec, self._hp_train)
+
+    monkeypatch.setattr(E.Engine, "set_host_program", set_host_program)
+    monkeypatch.setattr(E.Engine, "pieces_vars", pieces_vars)
+    monkeypatch.setattr(E.Engine, "nll_grad_vars", nll_grad_vars)
     monkeypatch.setattr(E.Engine, "_create", _create)
     monkeypatch.setattr(E.Engine, "upload", upload)
     monkeypatch.setattr(E.Engine, "eval_sums", eval_sums)

@@ -210,3 +210,78 @@ def test_shape_cache_fcn(name):
     np.testing.assert_allclose(g_m, g_p, rtol=0, atol=1e-5 * np.abs(g_p).max())
     fm.eng.close()
     fp.eng.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["d2kpipi_float", "d2kpipi_shapes", "lc2pkpi", "b2dstkpi",
+                                  "dp2kpipi_ident", "toy_vvp"])
+@pytest.mark.parametrize("precision", ["plain", "mixed"])
+def test_native_host_matches_python_host(name, precision):
+    """FCN's evaluations with the host side in native code (pwa_nll_grad_vars:
+    constants, Jacobian and chain rule of the host program) against the
+    engine's Python host code on the same device sums: NLL to 1e-12
+    relative, gradient to 1e-10 of its largest entry, at the golden point
+    and at a shifted shape setting; every mass and width trainable."""
+    import os
+
+    from common import CONFIGS
+    from tf_pwa_b200.api import FCN, ConfigLoader, EventData
+
+    g, meta = load_golden(name)
+    cl = ConfigLoader(os.path.join(CONFIGS, meta["config"]))
+    cl.vm.set_all(meta["variables"])
+    vm = cl.vm
+    for n in list(vm.variables):
+        if n.endswith(("_mass", "_width")) and n not in vm.trainable_vars:
+            vm.set_fix(n, unfix=True)
+    x, w = golden_data(g, meta)
+    alpha = w.sum() / (w * w).sum()
+    f = FCN(cl, EventData(x, w / alpha), EventData(g["fields_mc"]), precision=precision,
+            shape_cache=False)
+    assert f.native_host and not f.use_gram
+    names = list(vm.trainable_vars)
+    x0 = np.array(vm.get_all_val())
+    x1 = x0.copy()
+    for i, n in enumerate(names):
+        if n.endswith("_mass"):
+            x1[i] *= 1.003
+        elif n.endswith("_width"):
+            x1[i] *= 1.05
+    for xv in (x0, x1):
+        nll, grad = f.nll_grad(xv)
+        ref_n, ref_g = f.eng.nll_grad(vm.get_all_dic(), names, f.precision)
+        assert abs(nll - ref_n) <= 1e-12 * abs(ref_n)
+        np.testing.assert_allclose(grad, ref_g, rtol=0, atol=1e-10 * np.abs(ref_g).max())
+    f.eng.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["d2kpipi_float", "d2kpipi_shapes"])
+def test_native_host_shape_cache(name):
+    """The floating-shape column cache through the native host side
+    (pwa_pieces_vars with the shape-cache form) against the Python host
+    side's shape-cache evaluation: same NLL and gradient to 1e-12 / 1e-10."""
+    import os
+
+    from common import CONFIGS
+    from tf_pwa_b200.api import FCN, ConfigLoader, EventData
+
+    g, meta = load_golden(name)
+    cl = ConfigLoader(os.path.join(CONFIGS, meta["config"]))
+    cl.vm.set_all(meta["variables"])
+    x, w = golden_data(g, meta)
+    alpha = w.sum() / (w * w).sum()
+    f = FCN(cl, EventData(x, w / alpha), EventData(g["fields_mc"]), precision="mixed")
+    assert f.native_host and f.use_shape_cache
+    names = list(cl.vm.trainable_vars)
+    x1 = np.array(cl.vm.get_all_val())
+    for i, n in enumerate(names):
+        if n.endswith("_mass"):
+            x1[i] *= 1.005
+        elif n.endswith("_width"):
+            x1[i] *= 1.08
+    nll, grad = f.nll_grad(x1)
+    ref_n, ref_g = f.eng.nll_grad(cl.vm.get_all_dic(), names, f.precision)
+    assert abs(nll - ref_n) <= 1e-12 * abs(ref_n)
+    np.testing.assert_allclose(grad, ref_g, rtol=0, atol=1e-10 * np.abs(ref_g).max())
+    f.eng.close()

@@ -27,7 +27,8 @@ import warnings
 import numpy as np
 
 from .decay_config import DecayConfig, float_particles, init_params, load_yaml
-from .engine import MIXED_F32, PLAIN_F64, Engine, PWAError, read_dat
+from .engine import (FORM_MIXED_F32, FORM_PLAIN_F64, FORM_SHAPE_CACHE, MIXED_F32, PLAIN_F64,
+                     Engine, PWAError, read_dat)
 from .kinematics import event_fields, p4_dict
 from .plan import Plan
 from .variables import Bound, VarsManager
@@ -208,12 +209,25 @@ class FCN:
                     raise
                 warnings.warn(f"floating-shape column cache not used: {e}")
                 self.use_shape_cache = False
+        self._var_names = list(self.vm.variables.keys())
+        self._train = list(self.vm.trainable_vars)
+        # the host side of each evaluation (constants, Jacobian, chain rule)
+        # in native code where the host program covers the model (no
+        # CP-violating totals, no polarised parent); else the Python host code
+        self.native_host = False
+        if not self.use_gram:
+            self._form = (FORM_PLAIN_F64 if self.precision == PLAIN_F64 else
+                          FORM_SHAPE_CACHE if self.use_shape_cache else FORM_MIXED_F32)
+            try:
+                self.eng.set_host_program(self._var_names, self._train)
+                self.native_host = True
+            except PWAError:
+                pass
         if self.use_gram:
             vals = self.vm.get_all_dic()
             self.eng.set_gram(vals)
             self.eng.cache_data(vals)
-            self._var_names = list(self.vm.variables.keys())
-            self.eng.set_param_layout(self._var_names, self.vm.trainable_vars)
+            self.eng.set_param_layout(self._var_names, self._train)
             # pick the fastest configuration of the cached data-term kernel
             # for this model and event count (PWA_AUTOTUNE=0: keep the default;
             # PWA_CACHED_CONFIG="variant,ring_depth,blocks_per_sm": pin one)
@@ -269,14 +283,28 @@ class FCN:
 
     def get_nll_grad(self, x=None):
         self._set(x)
+        if self.vm.trainable_vars != self._train:
+            self._relayout()
         if self.use_gram:
             v = self.vm.variables
             nll, g = self.eng.nll_grad_cached([v[k] for k in self._var_names])
+        elif self.native_host:
+            v = self.vm.variables
+            nll, g = self.eng.nll_grad_vars([v[k] for k in self._var_names], self._form)
         else:
             nll, g = self.eng.nll_grad(self.vm.get_all_dic(), self.vm.trainable_vars,
                                        self.precision)
         self.n_call += 1
         return nll, g
+
+    def _relayout(self):
+        """The trainable set changed (set_fix after construction): new
+        gradient layout for the native chain rules."""
+        self._train = list(self.vm.trainable_vars)
+        if self.use_gram:
+            self.eng.set_param_layout(self._var_names, self._train)
+        elif self.native_host:
+            self.eng.set_host_program(self._var_names, self._train)
 
     def nll_grad(self, x=None):
         nll, g = self.get_nll_grad(x)

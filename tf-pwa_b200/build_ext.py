@@ -44,7 +44,8 @@ def build(force=False, verbose=False):
         return LIB
     cmd = [NVCC, "-O3", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
            "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
-           os.path.join(CSRC, "pwa_runtime.cu"), "-o", LIB + ".tmp",
+           os.path.join(CSRC, "pwa_runtime.cu"), os.path.join(CSRC, "pwa_hostprog.cpp"),
+           "-Xcompiler", "-ffp-contract=off", "-o", LIB + ".tmp",
            "-L" + CUDA_LIB, "-lnvrtc", "-Xlinker", "-rpath," + CUDA_LIB,
            "-cudart", "static"]
     if verbose:

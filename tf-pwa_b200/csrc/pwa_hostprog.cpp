@@ -1,0 +1,505 @@
+// Host program of one model (pwa_hostprog.h): the constant block, the
+// Jacobian of the column couplings and the chain rule in native code.
+//
+// The formulas follow the engine's Python host code line for line, with the
+// same order of operations, so that the constant block agrees with it to
+// rounding: rel_p / rel_p2 (tf_pwa/amp/core.py:311-334), the
+// Blatt-Weisskopf polynomials of tf_pwa/breit_wigner.py:319-390 evaluated by
+// Horner's rule, the lineshape constants of BW (K = m0 Gamma0), BWR
+// (K = m0^2 Gamma0 B(q0) / q0^(2L+1), q0 clamped at threshold) and BWR2
+// (K = m0^2 Gamma0 B(q0^2), q0^2 unclamped; tf_pwa/breit_wigner.py:56-91,
+// 193-265,280-306).  Derivatives in a mass are taken by a complex step of
+// 1e-20 (exact to rounding: no difference is formed).
+#include "pwa_hostprog.h"
+
+#include <cmath>
+
+namespace pwa_host {
+namespace {
+
+using cd = std::complex<double>;
+constexpr double kStep = 1e-20;
+
+inline double re(double x) { return x; }
+inline double re(const cd& x) { return x.real(); }
+inline double im(double) { return 0.0; }
+inline double im(const cd& x) { return x.imag(); }
+
+// x^n for a small integer n >= 0: the C library's pow for reals, binary
+// powering (products from the low bit up) for complex numbers
+inline double ipow(double x, int n) { return std::pow(x, (double)n); }
+inline cd ipow(const cd& x, int n) {
+  cd r(1.0, 0.0), p = x;
+  for (unsigned m = 1; m > 0 && (unsigned)n >= m; m <<= 1) {
+    if (n & m) r = r * p;
+    p = p * p;
+  }
+  return r;
+}
+
+template <class T>
+T rel_p2(T m0, T m1, T m2) {
+  const T s = m1 + m2, d = m1 - m2;
+  return (m0 - s) * (m0 + s) * (m0 - d) * (m0 + d) / ipow(2.0 * m0, 2);
+}
+
+template <class T>
+T rel_p(T m0, T m1, T m2) {
+  const T s = m1 + m2, d = m1 - m2;
+  const T me = re(m0) > re(s) ? m0 : s;
+  const T p = (me - s) * (me + s) * (me - d) * (me + d);
+  return std::sqrt(p) / (2.0 * me);
+}
+
+template <class T>
+T horner(const std::vector<double>& coef, T z) {
+  T r = T(0.0);
+  for (double c : coef) r = r * z + c;
+  return r;
+}
+
+// 1 / |q0^2|^(l/2); for a complex q0^2, 1 / sqrt(q0^2 q0^2)^(l/2)
+inline double inv_norm(double q02, int l) { return 1.0 / std::pow(std::fabs(q02), l / 2.0); }
+inline cd inv_norm(const cd& q02, int l) {
+  const cd a = std::sqrt(q02 * q02);
+  const cd p = (l % 2 == 0) ? ipow(a, l / 2) : std::pow(a, l / 2.0);
+  return 1.0 / p;
+}
+
+template <class T>
+void entry_values(T q02, double d, const pwa_hostprog::VEntry& e, T* pz, T* nrm) {
+  const T z = q02 * d * d;
+  *pz = e.bp ? horner(e.coef, z) : T(1.0);
+  *nrm = e.bn ? inv_norm(q02, e.l) : T(1.0);
+}
+
+template <class T>
+T vertex_q02(const std::vector<T>& M, const pwa_hostprog::VRow& r) {
+  if (r.noq0) return T(1.0);
+  return rel_p2(M[r.ia], M[r.ib], M[r.ic]);
+}
+
+// (K, useq, q0^2) of one lineshape at parent mass m0
+template <class T>
+void row_values(const pwa_hostprog::LRow& r, T m0, double g0, T mb, T mc, T* K, double* useq,
+                T* q02) {
+  *useq = 1.0;
+  *q02 = T(0.0);
+  if (r.kind == 0) {  // BW
+    *K = m0 * g0;
+    return;
+  }
+  if (r.kind == 2) {  // BWR2
+    *q02 = rel_p2(m0, mb, mc);
+    const T z = *q02 * r.d * r.d;
+    *K = m0 * m0 * g0 * horner(r.coef, z);
+    return;
+  }
+  const T q0 = rel_p(m0, mb, mc);  // BWR
+  const T z = ipow(q0 * r.d, 2);
+  const T b = horner(r.coef, z);
+  if (re(q0) > 1e-15) {
+    *K = m0 * m0 * g0 * b / ipow(q0, 2 * r.L + 1);
+  } else {
+    *K = m0 * m0 * g0 * b;
+    *useq = 0.0;
+  }
+}
+
+void mass_list(const pwa_hostprog* p, const double* vars, std::vector<double>* M) {
+  *M = p->m_base;
+  for (size_t i = 0; i < M->size(); ++i)
+    if (p->m_var[i] >= 0) (*M)[i] = vars[p->m_var[i]];
+}
+
+// Lineshape and barrier constants into C (the rest of C untouched) and the
+// barrier rows of every resonance mass.
+void shape_part(pwa_hostprog* p, const double* vars, double* C) {
+  std::vector<double> M;
+  mass_list(p, vars, &M);
+  for (const auto& r : p->vt) {
+    const double q02 = vertex_q02(M, r);
+    for (const auto& e : r.e) {
+      double pz, nrm;
+      entry_values(q02, r.d, e, &pz, &nrm);
+      if (e.s_pz >= 0) C[e.s_pz] = pz;
+      if (e.s_norm >= 0) C[e.s_norm] = nrm;
+    }
+  }
+  for (const auto& r : p->ls) {
+    const double m0 = M[r.im], mb = M[r.ib], mc = M[r.ic];
+    const double g0 = r.g_var >= 0 ? vars[r.g_var] : r.g_def;
+    C[r.s_m0sq] = m0 * m0;
+    double K, useq, q02;
+    row_values(r, m0, g0, mb, mc, &K, &useq, &q02);
+    if (r.kind == 1) {
+      C[r.s_k] = K;
+      C[r.s_useq] = useq;
+    } else if (r.kind == 2) {
+      C[r.s_k] = K;
+      C[r.s_iq] = 1.0 / q02;
+    } else {
+      C[r.s_y] = K;
+    }
+    if (r.s_wn >= 0) C[r.s_wn] = g0;
+    if (r.s_kap >= 0) {
+      // kappa = d ln(m0 Gamma) / d m0; for BWR2 m0 Gamma2 = K r^(L+1/2) / (m B)
+      // gives d ln K - (L + 1/2) d ln q0^2
+      cd Kc, qc;
+      double uc;
+      row_values(r, cd(m0, kStep), g0, cd(mb), cd(mc), &Kc, &uc, &qc);
+      double kap = K != 0.0 ? Kc.imag() / kStep / K : 0.0;
+      if (r.kind == 2) kap -= (r.L + 0.5) * qc.imag() / kStep / q02;
+      C[r.s_kap] = kap;
+      C[r.s_ig] = g0 != 0.0 ? 1.0 / g0 : 0.0;
+    }
+  }
+  // barrier rows: d ln(bf_l) / dm with bf_l ~ sqrt(Pz0_l) norm_l per vertex
+  // entry, summed over each column's entries
+  p->kap.assign(p->mj.size(), std::vector<double>(p->ncol, 0.0));
+  for (size_t q = 0; q < p->mj.size(); ++q) {
+    const auto& mj = p->mj[q];
+    std::vector<cd> Mc(M.begin(), M.end());
+    Mc[mj.qi] = cd(M[mj.qi], kStep);
+    std::vector<std::vector<double>> dlog(p->vt.size());
+    for (int v : mj.verts) {
+      const auto& r = p->vt[v];
+      const double q0r = vertex_q02(M, r);
+      const cd q0c = vertex_q02(Mc, r);
+      dlog[v].resize(r.e.size());
+      for (size_t j = 0; j < r.e.size(); ++j) {
+        double pz0, n0;
+        cd pzc, nc;
+        entry_values(q0r, r.d, r.e[j], &pz0, &n0);
+        entry_values(q0c, r.d, r.e[j], &pzc, &nc);
+        double t = 0.0;
+        if (r.e[j].bp) t += 0.5 * pzc.imag() / kStep / pz0;
+        if (r.e[j].bn) t += nc.imag() / kStep / n0;
+        dlog[v][j] = t;
+      }
+    }
+    for (size_t c = 0; c < mj.c_col.size(); ++c)
+      p->kap[q][mj.c_col[c]] += dlog[mj.c_row[c]][mj.c_ent[c]];
+  }
+}
+
+// the cursor of parse(): bounds-checked reads of the two arrays
+struct Reader {
+  const int* ip;
+  long long n_ip, i = 0;
+  const double* dp;
+  long long n_dp, j = 0;
+  bool ok = true;
+  int next() {
+    if (i >= n_ip) {
+      ok = false;
+      return 0;
+    }
+    return ip[i++];
+  }
+  double dnext() {
+    if (j >= n_dp) {
+      ok = false;
+      return 0.0;
+    }
+    return dp[j++];
+  }
+  int count(int cap) {  // a non-negative count of at most cap
+    const int n = next();
+    if (n < 0 || n > cap) ok = false;
+    return ok ? n : 0;
+  }
+};
+
+}  // namespace
+
+bool parse(const int* ip, long long n_ip, const double* dp, long long n_dp, pwa_hostprog* p,
+           std::string* err) {
+  Reader rd{ip, n_ip, 0, dp, n_dp};
+  constexpr int kMagic = 0x50574850, kVersion = 1, kCap = 1 << 20;
+  auto fail = [&](const std::string& m) {
+    *err = "host program: " + m;
+    return false;
+  };
+  if (!ip || n_ip <= 0 || (n_dp > 0 && !dp)) return fail("empty program");
+  if (rd.next() != kMagic || rd.next() != kVersion) return fail("bad magic or version");
+  p->ncol = rd.count(kCap);
+  p->nconst = rd.count(kCap);
+  p->nshape = rd.count(kCap);
+  p->n_vars = rd.count(kCap);
+  p->n_train = rd.count(kCap);
+  p->n_coup = rd.count(kCap);
+  p->nfac = rd.count(64);
+  if (!rd.ok || p->ncol <= 0 || p->nconst < 2 * p->ncol || p->n_coup <= 0 || p->nfac <= 0)
+    return fail("bad header");
+  auto ints = [&](std::vector<int>* v, long long n) {
+    v->resize(n);
+    for (long long q = 0; q < n; ++q) (*v)[q] = rd.next();
+  };
+  ints(&p->coup_r, p->n_coup);
+  ints(&p->coup_i, p->n_coup);
+  ints(&p->coup_polar, p->n_coup);
+  ints(&p->col_fac, (long long)p->ncol * p->nfac);
+  ints(&p->train_idx, p->n_train);
+  const int n_vg = rd.count(kCap);
+  p->vg_src.resize(n_vg);
+  p->vg_re.resize(n_vg);
+  p->vg_im.resize(n_vg);
+  for (int q = 0; q < n_vg; ++q) {
+    p->vg_src[q] = rd.next();
+    p->vg_re[q] = rd.next();
+    p->vg_im[q] = rd.next();
+  }
+  const int n_m = rd.count(kCap);
+  ints(&p->m_var, n_m);
+  p->m_base.resize(n_m);
+  for (int q = 0; q < n_m; ++q) p->m_base[q] = rd.dnext();
+  const int n_vt = rd.count(kCap);
+  p->vt.assign(n_vt, {});
+  for (auto& r : p->vt) {
+    r.ia = rd.next();
+    r.ib = rd.next();
+    r.ic = rd.next();
+    r.noq0 = rd.next();
+    r.e.resize(rd.count(64));
+    r.d = rd.dnext();
+    for (auto& e : r.e) {
+      e.l = rd.next();
+      e.bp = rd.next();
+      e.bn = rd.next();
+      e.s_pz = rd.next();
+      e.s_norm = rd.next();
+      e.coef.resize(rd.count(64));
+      for (auto& c : e.coef) c = rd.dnext();
+    }
+  }
+  const int n_ls = rd.count(kCap);
+  p->ls.assign(n_ls, {});
+  for (auto& r : p->ls) {
+    r.kind = rd.next();
+    r.im = rd.next();
+    r.ib = rd.next();
+    r.ic = rd.next();
+    r.L = rd.next();
+    r.g_var = rd.next();
+    r.s_m0sq = rd.next();
+    r.s_k = rd.next();
+    r.s_useq = rd.next();
+    r.s_y = rd.next();
+    r.s_iq = rd.next();
+    r.s_wn = rd.next();
+    r.s_kap = rd.next();
+    r.s_ig = rd.next();
+    r.coef.resize(rd.count(64));
+    r.d = rd.dnext();
+    r.g_def = rd.dnext();
+    for (auto& c : r.coef) c = rd.dnext();
+  }
+  const int n_sel = rd.count(kCap);
+  p->sel_var.resize(n_sel);
+  p->sel_slot.resize(n_sel);
+  for (int q = 0; q < n_sel; ++q) {
+    p->sel_var[q] = rd.next();
+    p->sel_slot[q] = rd.next();
+  }
+  const int n_mj = rd.count(kCap);
+  p->mj.assign(n_mj, {});
+  for (auto& m : p->mj) {
+    m.var = rd.next();
+    m.qi = rd.next();
+    ints(&m.verts, rd.count(kCap));
+    const int nc = rd.count(kCap);
+    m.c_col.resize(nc);
+    m.c_row.resize(nc);
+    m.c_ent.resize(nc);
+    for (int q = 0; q < nc; ++q) {
+      m.c_col[q] = rd.next();
+      m.c_row[q] = rd.next();
+      m.c_ent[q] = rd.next();
+    }
+  }
+  const int n_rt = rd.count(kCap);
+  p->rt_col.resize(n_rt);
+  p->rt_slot.resize(n_rt);
+  p->rt_sqrt.resize(n_rt);
+  for (int q = 0; q < n_rt; ++q) {
+    p->rt_col[q] = rd.next();
+    p->rt_slot[q] = rd.next();
+    p->rt_sqrt[q] = rd.next();
+  }
+  if (rd.next() != kMagic || !rd.ok) return fail("truncated program");
+  if (rd.i != n_ip || rd.j != n_dp) return fail("trailing entries");
+
+  // ranges of every index
+  const int V = p->n_vars, S = p->nconst, K = p->ncol;
+  auto in = [](int x, int lo, int hi) { return x >= lo && x < hi; };
+  auto slot = [&](int x) { return x == -1 || in(x, 0, S); };
+  for (int q = 0; q < p->n_coup; ++q)
+    if (!in(p->coup_r[q], 0, V) || !in(p->coup_i[q], 0, V)) return fail("coupling index");
+  for (int x : p->col_fac)
+    if (!in(x, -1, p->n_coup)) return fail("column factor index");
+  for (int x : p->train_idx)
+    if (!in(x, 0, V)) return fail("trainable index");
+  for (int q = 0; q < n_vg; ++q)
+    if (!in(p->vg_src[q], 0, p->n_coup) || !in(p->vg_re[q], 0, S) || !in(p->vg_im[q], 0, S))
+      return fail("vertex coupling slot");
+  for (int x : p->m_var)
+    if (!in(x, -1, V)) return fail("mass variable index");
+  for (const auto& r : p->vt) {
+    if (!in(r.ia, 0, n_m) || !in(r.ib, 0, n_m) || !in(r.ic, 0, n_m)) return fail("vertex mass");
+    for (const auto& e : r.e)
+      if (!slot(e.s_pz) || !slot(e.s_norm) || e.l < 0) return fail("vertex entry");
+  }
+  for (const auto& r : p->ls) {
+    if (!in(r.kind, 0, 3) || !in(r.im, 0, n_m) || !in(r.ib, 0, n_m) || !in(r.ic, 0, n_m) ||
+        !in(r.g_var, -1, V) || !in(r.s_m0sq, 0, S) || !slot(r.s_k) || !slot(r.s_useq) ||
+        !slot(r.s_y) || !slot(r.s_iq) || !slot(r.s_wn) || !slot(r.s_kap) || !slot(r.s_ig) ||
+        r.L < 0)
+      return fail("lineshape row");
+    if ((r.kind == 1 && (r.s_k < 0 || r.s_useq < 0)) || (r.kind == 2 && (r.s_k < 0 || r.s_iq < 0)) ||
+        (r.kind == 0 && r.s_y < 0) || ((r.s_kap < 0) != (r.s_ig < 0)))
+      return fail("lineshape slots");
+  }
+  for (int q = 0; q < n_sel; ++q)
+    if (!in(p->sel_var[q], 0, V) || !in(p->sel_slot[q], 0, p->nshape)) return fail("selector");
+  for (const auto& m : p->mj) {
+    if (!in(m.var, 0, V) || !in(m.qi, 0, n_m)) return fail("barrier row");
+    for (int v : m.verts)
+      if (!in(v, 0, n_vt)) return fail("barrier row vertex");
+    for (size_t q = 0; q < m.c_col.size(); ++q) {
+      if (!in(m.c_col[q], 0, K) || !in(m.c_row[q], 0, n_vt) ||
+          !in(m.c_ent[q], 0, (int)p->vt[m.c_row[q]].e.size()))
+        return fail("barrier row entry");
+      bool listed = false;
+      for (int v : m.verts) listed |= v == m.c_row[q];
+      if (!listed) return fail("barrier row entry outside its vertices");
+    }
+  }
+  for (int q = 0; q < n_rt; ++q)
+    if (!in(p->rt_col[q], 0, K) || !in(p->rt_slot[q], 0, S)) return fail("normalisation term");
+
+  // roles of the trainable variables and the inputs of the shape part
+  p->t_coup.assign(p->n_train, -1);
+  p->t_comp.assign(p->n_train, 0);
+  p->t_sel.assign(p->n_train, -1);
+  p->t_mj.assign(p->n_train, -1);
+  for (int t = 0; t < p->n_train; ++t) {
+    const int v = p->train_idx[t];
+    for (int q = 0; q < p->n_coup && p->t_coup[t] < 0; ++q) {
+      if (p->coup_r[q] == v) p->t_coup[t] = q, p->t_comp[t] = 0;
+      else if (p->coup_i[q] == v) p->t_coup[t] = q, p->t_comp[t] = 1;
+    }
+    for (int q = 0; q < n_sel; ++q)
+      if (p->sel_var[q] == v) p->t_sel[t] = p->sel_slot[q];
+    for (int q = 0; q < n_mj; ++q)
+      if (p->mj[q].var == v) p->t_mj[t] = q;
+  }
+  p->key_var.clear();
+  auto add_key = [&](int v) {
+    if (v < 0) return;
+    for (int x : p->key_var)
+      if (x == v) return;
+    p->key_var.push_back(v);
+  };
+  for (int x : p->m_var) add_key(x);
+  for (const auto& r : p->ls) add_key(r.g_var);
+  p->have_shape = false;
+  return true;
+}
+
+void consts(pwa_hostprog* p, const double* vars, double* C, std::vector<cd>* z,
+            std::vector<double>* ck) {
+  // shape part: recomputed when a mass or width it reads changed
+  bool same = p->have_shape && p->key.size() == p->key_var.size();
+  for (size_t q = 0; same && q < p->key_var.size(); ++q) same = p->key[q] == vars[p->key_var[q]];
+  if (!same) {
+    p->cshape.assign(p->nconst, 0.0);
+    shape_part(p, vars, p->cshape.data());
+    p->key.resize(p->key_var.size());
+    for (size_t q = 0; q < p->key_var.size(); ++q) p->key[q] = vars[p->key_var[q]];
+    p->have_shape = true;
+  }
+  for (int q = 0; q < p->nconst; ++q) C[q] = p->cshape[q];
+  // couplings: r e^{i phi} (polar) or r + i phi, columns their products
+  z->resize(p->n_coup);
+  for (int j = 0; j < p->n_coup; ++j) {
+    const double r = vars[p->coup_r[j]], ph = vars[p->coup_i[j]];
+    (*z)[j] = p->coup_polar[j] ? cd(r * std::cos(ph), r * std::sin(ph)) : cd(r, ph);
+  }
+  ck->resize(2 * p->ncol);
+  for (int k = 0; k < p->ncol; ++k) {
+    cd c(1.0, 0.0);
+    for (int f = 0; f < p->nfac; ++f) {
+      const int j = p->col_fac[k * p->nfac + f];
+      if (j >= 0) c = c * (*z)[j];
+    }
+    (*ck)[2 * k] = C[2 * k] = c.real();
+    (*ck)[2 * k + 1] = C[2 * k + 1] = c.imag();
+  }
+  for (size_t q = 0; q < p->vg_src.size(); ++q) {
+    C[p->vg_re[q]] = (*z)[p->vg_src[q]].real();
+    C[p->vg_im[q]] = (*z)[p->vg_src[q]].imag();
+  }
+}
+
+void jacobian(pwa_hostprog* p, const double* vars, const std::vector<cd>& z,
+              const std::vector<double>& ck, cd* J, double* D) {
+  const int K = p->ncol, P = p->n_train, NS = p->nshape;
+  for (long long q = 0; q < (long long)P * K; ++q) J[q] = cd(0.0, 0.0);
+  for (long long q = 0; q < (long long)P * NS; ++q) D[q] = 0.0;
+  for (int t = 0; t < P; ++t) {
+    cd* Jt = J + (long long)t * K;
+    const int j = p->t_coup[t];
+    if (j >= 0) {
+      const double ph = vars[p->coup_i[j]];
+      cd dz;
+      if (p->coup_polar[j])
+        dz = p->t_comp[t] == 0 ? cd(std::cos(ph), std::sin(ph)) : cd(0.0, 1.0) * z[j];
+      else
+        dz = p->t_comp[t] == 0 ? cd(1.0, 0.0) : cd(0.0, 1.0);
+      for (int k = 0; k < K; ++k) {
+        // d(prod of factors)/dz: count of z times the product of the others
+        // (further factors z included)
+        int cnt = 0;
+        cd others(1.0, 0.0);
+        for (int f = 0; f < p->nfac; ++f) {
+          const int q = p->col_fac[k * p->nfac + f];
+          if (q < 0) continue;
+          if (q == j && cnt++ == 0) continue;
+          others = others * z[q];
+        }
+        if (cnt) Jt[k] = (double)cnt * others * dz;
+      }
+    }
+    if (p->t_mj[t] >= 0) {
+      const auto& kap = p->kap[p->t_mj[t]];
+      for (int k = 0; k < K; ++k) Jt[k] += cd(ck[2 * k], ck[2 * k + 1]) * kap[k];
+    }
+    if (p->t_sel[t] >= 0) D[(long long)t * NS + p->t_sel[t]] = 1.0;
+  }
+}
+
+void grad_from_sums(const pwa_hostprog* p, const cd* J, const double* D, const double* s,
+                    double* g) {
+  const int K = p->ncol, NS = p->nshape;
+  for (int t = 0; t < p->n_train; ++t) {
+    const cd* Jt = J + (long long)t * K;
+    double acc = 0.0;
+    for (int k = 0; k < K; ++k) acc += Jt[k].real() * s[1 + 2 * k] - Jt[k].imag() * s[2 + 2 * k];
+    acc *= 2.0;
+    for (int q = 0; q < NS; ++q) acc += D[(long long)t * NS + q] * s[1 + 2 * K + q];
+    g[t] = acc;
+  }
+}
+
+bool column_rho(const pwa_hostprog* p, const double* C, double* rho) {
+  for (int k = 0; k < p->ncol; ++k) rho[k] = 1.0;
+  for (size_t q = 0; q < p->rt_col.size(); ++q) {
+    const double v = C[p->rt_slot[q]];
+    if (!(v > 0.0)) return false;
+    rho[p->rt_col[q]] *= p->rt_sqrt[q] ? std::sqrt(v) : v;
+  }
+  return true;
+}
+
+}  // namespace pwa_host

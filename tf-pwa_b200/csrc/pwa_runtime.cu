@@ -27,6 +27,7 @@
 #include <vector>
 
 #include "../../include/pwa_b200.h"
+#include "pwa_hostprog.h"
 
 namespace {
 
@@ -124,6 +125,12 @@ struct pwa_plan {
   // parameter layout for the C-side chain rule
   int n_vars = 0, n_coup = 0, nfac = 0, n_train = 0;
   std::vector<int> coup_r, coup_i, coup_polar, col_fac, train_idx;
+  // host program of the evaluations from the variable vector
+  // (pwa_set_host_program) and the constant block the floating-shape column
+  // cache was built at
+  pwa_hostprog hp;
+  bool hp_set = false;
+  std::vector<double> sc_consts;
   // scratch
   double* partials = nullptr;
   long long partials_cap = 0;
@@ -629,6 +636,7 @@ int pwa_shape_cache(pwa_plan* h, const double* consts, void* stream) {
   h->sc_blocks_data = (int)bd;
   CU(cudaStreamSynchronize(s));
   h->scache_n = n;
+  h->sc_consts.assign(consts, consts + h->nconst);
   return PWA_OK;
 }
 
@@ -1898,6 +1906,139 @@ int pwa_plan_info(pwa_plan* h, long long* info) {
   info[5] = h->blocks_data;
   info[6] = h->nacc;
   info[7] = h->tpb;
+  return PWA_OK;
+}
+
+// ------------------------------------------------------------ host program
+int pwa_hostprog_create(const int* ip, long long n_ip, const double* dp, long long n_dp,
+                        pwa_hostprog** out) {
+  if (!out) return set_err(nullptr, PWA_ERR_ARG, "null output");
+  *out = nullptr;
+  auto* p = new pwa_hostprog();
+  std::string err;
+  if (!pwa_host::parse(ip, n_ip, dp, n_dp, p, &err)) {
+    delete p;
+    return set_err(nullptr, PWA_ERR_ARG, err);
+  }
+  *out = p;
+  return PWA_OK;
+}
+
+int pwa_hostprog_destroy(pwa_hostprog* p) {
+  delete p;
+  return PWA_OK;
+}
+
+int pwa_hostprog_consts(pwa_hostprog* p, const double* vars, double* out) {
+  if (!p || !vars || !out) return set_err(nullptr, PWA_ERR_ARG, "null argument");
+  std::vector<std::complex<double>> z;
+  std::vector<double> ck;
+  pwa_host::consts(p, vars, out, &z, &ck);
+  return PWA_OK;
+}
+
+int pwa_hostprog_jacobian(pwa_hostprog* p, const double* vars, double* J, double* D) {
+  if (!p || !vars || !J || !D) return set_err(nullptr, PWA_ERR_ARG, "null argument");
+  std::vector<double> C(p->nconst), ck;
+  std::vector<std::complex<double>> z;
+  pwa_host::consts(p, vars, C.data(), &z, &ck);
+  pwa_host::jacobian(p, vars, z, ck, reinterpret_cast<std::complex<double>*>(J), D);
+  return PWA_OK;
+}
+
+namespace {
+// piece vector [S_d, S_m*share, sw, g_d, g_m*share] from the data and MC sums
+void pieces_from_hp_sums(pwa_hostprog* p, const double* vars, const std::vector<std::complex<double>>& z,
+                         const std::vector<double>& ck, const double* sd, const double* sm,
+                         double sw, double mc_share, double* out) {
+  const int P = p->n_train;
+  std::vector<std::complex<double>> J((size_t)P * p->ncol);
+  std::vector<double> D((size_t)P * p->nshape + 1);
+  pwa_host::jacobian(p, vars, z, ck, J.data(), D.data());
+  out[0] = sd[0];
+  out[1] = sm[0] * mc_share;
+  out[2] = sw;
+  pwa_host::grad_from_sums(p, J.data(), D.data(), sd, out + 3);
+  pwa_host::grad_from_sums(p, J.data(), D.data(), sm, out + 3 + P);
+  for (int t = 0; t < P; ++t) out[3 + P + t] *= mc_share;
+}
+}  // namespace
+
+int pwa_hostprog_pieces(pwa_hostprog* p, const double* vars, const double* sd, const double* sm,
+                        double sw, double mc_share, double* out) {
+  if (!p || !vars || !sd || !sm || !out) return set_err(nullptr, PWA_ERR_ARG, "null argument");
+  std::vector<double> C(p->nconst), ck;
+  std::vector<std::complex<double>> z;
+  pwa_host::consts(p, vars, C.data(), &z, &ck);
+  pieces_from_hp_sums(p, vars, z, ck, sd, sm, sw, mc_share, out);
+  return PWA_OK;
+}
+
+int pwa_hostprog_column_rho(const pwa_hostprog* p, const double* consts, double* out) {
+  if (!p || !consts || !out) return set_err(nullptr, PWA_ERR_ARG, "null argument");
+  if (!pwa_host::column_rho(p, consts, out))
+    return set_err(nullptr, PWA_ERR_ARG, "non-positive barrier normalisation");
+  return PWA_OK;
+}
+
+int pwa_set_host_program(pwa_plan* h, const pwa_hostprog* p) {
+  if (!h) return PWA_ERR_ARG;
+  if (!p) return set_err(h, PWA_ERR_ARG, "null host program");
+  if (p->ncol != h->ncol || p->nconst != h->nconst || p->nshape != h->nshape ||
+      1 + 2 * p->ncol + p->nshape != h->nacc)
+    return set_err(h, PWA_ERR_ARG, "host program does not match the plan's model sizes");
+  h->hp = *p;
+  h->hp.have_shape = false;
+  h->hp_set = true;
+  return PWA_OK;
+}
+
+int pwa_pieces_vars(pwa_plan* h, const double* vars, int form, double sw, double mc_share,
+                    void* stream, double* out) {
+  if (!h) return PWA_ERR_ARG;
+  if (!vars || !out) return set_err(h, PWA_ERR_ARG, "null argument");
+  if (!h->hp_set) return set_err(h, PWA_ERR_STATE, "host program not set");
+  if (form != PWA_FORM_PLAIN_F64 && form != PWA_FORM_MIXED_F32 && form != PWA_FORM_SHAPE_CACHE)
+    return set_err(h, PWA_ERR_ARG, "invalid evaluation form");
+  pwa_hostprog* p = &h->hp;
+  std::vector<double> C(h->nconst), ck, sums(2 * h->nacc);
+  std::vector<std::complex<double>> z;
+  pwa_host::consts(p, vars, C.data(), &z, &ck);
+  int rc;
+  if (form == PWA_FORM_SHAPE_CACHE) {
+    if (h->scache_n != h->n_data + h->n_mc || h->scache_n <= 0 ||
+        h->sc_consts.size() != (size_t)h->nconst)
+      return set_err(h, PWA_ERR_STATE, "no floating-shape column cache (call pwa_shape_cache)");
+    std::vector<double> rho(h->ncol), rho0(h->ncol);
+    if (pwa_host::column_rho(p, C.data(), rho.data()) &&
+        pwa_host::column_rho(p, h->sc_consts.data(), rho0.data())) {
+      for (int k = 0; k < h->ncol; ++k) rho[k] /= rho0[k];
+      rc = pwa_eval_shapecache(h, C.data(), rho.data(), stream, sums.data());
+    } else {
+      // a normalisation is not positive here: the columns do not factorise,
+      // so this point recomputes them (FP32 amplitudes)
+      rc = pwa_eval(h, C.data(), PWA_MIXED_F32, 1, stream, sums.data());
+    }
+  } else {
+    rc = pwa_eval(h, C.data(), form == PWA_FORM_PLAIN_F64 ? PWA_PLAIN_F64 : PWA_MIXED_F32, 1,
+                  stream, sums.data());
+  }
+  if (rc) return rc;
+  pieces_from_hp_sums(p, vars, z, ck, sums.data(), sums.data() + h->nacc, sw, mc_share, out);
+  return PWA_OK;
+}
+
+int pwa_nll_grad_vars(pwa_plan* h, const double* vars, int form, double sw, void* stream,
+                      double* out_nll, double* out_grad) {
+  if (!h) return PWA_ERR_ARG;
+  if (!out_nll || !out_grad) return set_err(h, PWA_ERR_ARG, "null output");
+  const int P = h->hp.n_train;
+  std::vector<double> v(3 + 2 * P);
+  int rc = pwa_pieces_vars(h, vars, form, sw, 1.0, stream, v.data());
+  if (rc) return rc;
+  // NLL = -S_d + sw ln S_m, grad = -g_d + sw g_m / S_m (tf_pwa/model/model.py:433-449)
+  *out_nll = -v[0] + v[2] * std::log(v[1]);
+  for (int t = 0; t < P; ++t) out_grad[t] = -v[3 + t] + v[2] * v[3 + P + t] / v[1];
   return PWA_OK;
 }
 

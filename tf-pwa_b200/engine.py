@@ -97,6 +97,15 @@ def load_library(path=LIB_PATH):
     lib.pwa_eval_shapecache.argtypes = [vp, dp, dp, vp, dp]
     lib.pwa_eval_shapecache_enqueue.argtypes = [vp, dp, dp, vp]
     lib.pwa_read_dat.argtypes = [cp, vp, ll, ctypes.POINTER(ll)]
+    lib.pwa_hostprog_create.argtypes = [ip, ll, dp, ll, ctypes.POINTER(vp)]
+    lib.pwa_hostprog_destroy.argtypes = [vp]
+    lib.pwa_hostprog_consts.argtypes = [vp, dp, dp]
+    lib.pwa_hostprog_jacobian.argtypes = [vp, dp, dp, dp]
+    lib.pwa_hostprog_pieces.argtypes = [vp, dp, dp, dp, ctypes.c_double, ctypes.c_double, dp]
+    lib.pwa_hostprog_column_rho.argtypes = [vp, dp, dp]
+    lib.pwa_set_host_program.argtypes = [vp, vp]
+    lib.pwa_pieces_vars.argtypes = [vp, vp, i, ctypes.c_double, ctypes.c_double, vp, vp]
+    lib.pwa_nll_grad_vars.argtypes = [vp, vp, i, ctypes.c_double, vp, vp, vp]
     lib.pwa_server_create.argtypes = [vp, dp, dp, i, ctypes.c_double, i, ctypes.POINTER(vp)]
     lib.pwa_server_submit.argtypes = [vp, dp, vp, vp, vp, ll, ll, ctypes.POINTER(ll)]
     ip_ = ctypes.POINTER(ctypes.c_int)
@@ -132,13 +141,88 @@ EXPORTED = ("pwa_plan_create", "pwa_plan_destroy", "pwa_compile_only", "pwa_prec
             "pwa_eval_noalloc", "pwa_fields_from_p4", "pwa_toy_select", "pwa_toy_fields",
             "pwa_hessian_cached", "pwa_hessian_cached_exact", "pwa_hess_sums_cached",
             "pwa_shape_cache", "pwa_eval_shapecache", "pwa_eval_shapecache_enqueue",
-            "pwa_read_dat", "pwa_server_create", "pwa_server_submit",
+            "pwa_read_dat", "pwa_hostprog_create", "pwa_hostprog_destroy",
+            "pwa_hostprog_consts", "pwa_hostprog_jacobian", "pwa_hostprog_pieces",
+            "pwa_hostprog_column_rho", "pwa_set_host_program", "pwa_pieces_vars",
+            "pwa_nll_grad_vars", "pwa_server_create", "pwa_server_submit",
             "pwa_server_result", "pwa_server_stats", "pwa_server_destroy",
             "pwa_plan_info", "pwa_last_error")
 
 
 class PWAError(RuntimeError):
     pass
+
+
+HOSTPROG_MAGIC = 0x50574850
+FORM_PLAIN_F64, FORM_MIXED_F32, FORM_SHAPE_CACHE = 0, 1, 2
+
+
+class HostProgram:
+    """A host program (pwa_hostprog_*): the constant block, the Jacobian of
+    the column couplings and the chain rule of one model and variable
+    layout in native code, from the flat arrays of
+    :meth:`Engine.host_program_arrays`.  Needs no device."""
+
+    def __init__(self, ip, dp, ncol, nconst, nshape, n_train):
+        self.ip = np.ascontiguousarray(ip, np.int32)
+        self.dp = np.ascontiguousarray(dp, np.float64)
+        self.ncol, self.nconst, self.nshape, self.n_train = ncol, nconst, nshape, n_train
+        lib = load_library()
+        h = ctypes.c_void_p()
+        rc = lib.pwa_hostprog_create(self.ip.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                     len(self.ip), _dptr(self.dp), len(self.dp), ctypes.byref(h))
+        if rc:
+            raise PWAError(f"pwa_hostprog_create failed ({rc}): "
+                           f"{lib.pwa_last_error(None).decode()}")
+        self.h = h
+
+    def _check(self, rc, what):
+        if rc:
+            raise PWAError(f"{what} failed ({rc}): {load_library().pwa_last_error(None).decode()}")
+
+    def consts(self, var_values):
+        v = np.ascontiguousarray(var_values, np.float64)
+        out = np.zeros(self.nconst)
+        self._check(load_library().pwa_hostprog_consts(self.h, _dptr(v), _dptr(out)),
+                    "pwa_hostprog_consts")
+        return out
+
+    def jacobian(self, var_values):
+        v = np.ascontiguousarray(var_values, np.float64)
+        J = np.zeros(2 * self.n_train * self.ncol)
+        D = np.zeros(max(self.n_train * self.nshape, 1))
+        self._check(load_library().pwa_hostprog_jacobian(self.h, _dptr(v), _dptr(J), _dptr(D)),
+                    "pwa_hostprog_jacobian")
+        J = (J[0::2] + 1j * J[1::2]).reshape(self.n_train, self.ncol)
+        return J, D[:self.n_train * self.nshape].reshape(self.n_train, self.nshape)
+
+    def pieces(self, var_values, sd, sm, sw, mc_share=1.0):
+        v = np.ascontiguousarray(var_values, np.float64)
+        sd = np.ascontiguousarray(sd, np.float64)
+        sm = np.ascontiguousarray(sm, np.float64)
+        out = np.zeros(3 + 2 * self.n_train)
+        self._check(load_library().pwa_hostprog_pieces(self.h, _dptr(v), _dptr(sd), _dptr(sm),
+                                                       float(sw), float(mc_share), _dptr(out)),
+                    "pwa_hostprog_pieces")
+        return out
+
+    def column_rho(self, C):
+        C = np.ascontiguousarray(C, np.float64)
+        out = np.zeros(self.ncol)
+        self._check(load_library().pwa_hostprog_column_rho(self.h, _dptr(C), _dptr(out)),
+                    "pwa_hostprog_column_rho")
+        return out
+
+    def close(self):
+        if getattr(self, "h", None):
+            load_library().pwa_hostprog_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def _dptr(a):
@@ -1016,6 +1100,139 @@ class Engine:
         self._check(load_library().pwa_set_param_layout(
             self.h, len(var_names), len(r), pa, pb, pc, nfac, pd, len(tr), pe),
             "pwa_set_param_layout")
+
+    # ------------------------------------- native host side (host program)
+    def host_program_arrays(self, var_names, train_names):
+        """The flat (int, double) arrays of this model's host program for
+        the variable layout ``var_names`` (all variables, in order) and the
+        gradient w.r.t. ``train_names`` (format in include/pwa_b200.h).
+        PWAError for models whose host side it does not cover (CP-violating
+        totals, a polarised parent) or a trainable name with no role."""
+        if len(self._cp_coup) or self._pol_names:
+            raise PWAError("the host program covers models without CP-violating totals or a "
+                           "polarised parent")
+        c = self.code
+        idx = {n: i for i, n in enumerate(var_names)}
+        for n in train_names:
+            ok = (n[:-1] in self._cn_index and n[-1] in "ri") or n in self._mass_names \
+                or n in self._width_names
+            if not ok or n not in idx:
+                raise PWAError(f"trainable variable {n} has no role in the host program")
+        try:
+            cr = [idx[n + "r"] for n in self.coupling_names]
+            ci = [idx[n + "i"] for n in self.coupling_names]
+        except KeyError as e:
+            raise PWAError(f"coupling variable {e} missing from the layout") from None
+        nfac = self._fac_idx.shape[1]
+        ip = [HOSTPROG_MAGIC, 1, c.ncol, len(c.consts), c.nshape, len(var_names),
+              len(train_names), len(self.coupling_names), nfac]
+        ip += cr + ci + [int(bool(x)) for x in self._cn_polar]
+        ip += [int(x) for x in self._fac_idx.reshape(-1)]
+        ip += [idx[n] for n in train_names]
+        ip += [len(self._vg_src)]
+        for a, b, d in zip(self._vg_src, self._vg_re, self._vg_im):
+            ip += [int(a), int(b), int(d)]
+        m_var = [-1] * len(self._m_base)
+        m_base = [float(x) for x in self._m_base]
+        for i, n, dflt in self._m_res:
+            if n in idx:
+                m_var[i] = idx[n]
+            elif dflt is None:
+                raise PWAError(f"resonance mass {n} has neither a variable nor a value")
+        ip += [len(m_var)] + m_var
+        dp = list(m_base)
+        ip += [len(self._vt_rows)]
+        for ia, ib, ic_, noq0, d, _, entries in self._vt_rows:
+            ip += [ia, ib, ic_, int(noq0), len(entries)]
+            dp += [float(d)]
+            for l, coef, bp, bn, s_pz, s_norm in entries:
+                ip += [int(l), int(bp), int(bn), int(s_pz), int(s_norm), len(coef)]
+                dp += [float(x) for x in coef]
+        kinds = {"BW": 0, "BWR": 1, "BWR2": 2}
+        opt = (lambda x: -1 if x is None else int(x))
+        ip += [len(self._ls_rows)]
+        for (kind, im, ib, ic_, L, d, gname, gdef, coef, s_m0sq, s_k, s_useq, s_y, s_iq, s_wn,
+             s_kap, s_ig) in self._ls_rows:
+            if kind not in kinds:
+                raise PWAError(f"lineshape kind {kind} not in the host program")
+            if gname not in idx and gdef is None:
+                raise PWAError(f"width {gname} has neither a variable nor a value")
+            ip += [kinds[kind], im, ib, ic_, int(L), idx.get(gname, -1), int(s_m0sq), opt(s_k),
+                   opt(s_useq), opt(s_y), opt(s_iq), opt(s_wn), opt(s_kap), opt(s_ig), len(coef)]
+            dp += [float(d), float(gdef or 0.0)] + [float(x) for x in coef]
+        sel = []
+        for n in var_names:
+            for names, kind in ((self._mass_names, "m"), (self._width_names, "g")):
+                if n in names and (names[n], kind) in self.shape_index:
+                    sel.append((idx[n], self.shape_index[(names[n], kind)]))
+        ip += [len(sel)]
+        for a, b in sel:
+            ip += [a, b]
+        mj = []
+        for n, p in self._mass_names.items():
+            if n in idx and p.key() in self._jac_pairs:
+                qi, verts, contrib = self._jac_pairs[p.key()]
+                trip = []
+                for k, v, l in contrib:
+                    ls_ = [e[0] for e in self._vt_rows[v][6]]
+                    trip += [k, v, ls_.index(l)]
+                mj.append([idx[n], qi, len(verts)] + list(verts) + [len(contrib)] + trip)
+        ip += [len(mj)]
+        for row in mj:
+            ip += row
+        cidx = c.consts.index
+        rt = [(k, cidx[name], int(kind == "sqrt")) for k in range(c.ncol)
+              for kind, name in c.column_barrier_consts(k)]
+        ip += [len(rt)]
+        for t in rt:
+            ip += list(t)
+        ip += [HOSTPROG_MAGIC]
+        return np.array(ip, np.int32), np.array(dp, np.float64)
+
+    def host_program(self, var_names, train_names):
+        """:class:`HostProgram` of this model for the given layout."""
+        ip, dp = self.host_program_arrays(var_names, train_names)
+        return HostProgram(ip, dp, self.code.ncol, len(self.code.consts), self.code.nshape,
+                           len(train_names))
+
+    def set_host_program(self, var_names, train_names):
+        """Give the plan its host program: evaluations from the variable
+        vector (pieces_vars / nll_grad_vars) then run the host side in
+        native code."""
+        hp = self.host_program(var_names, train_names)
+        try:
+            self._check(load_library().pwa_set_host_program(self.h, hp.h), "pwa_set_host_program")
+        finally:
+            hp.close()
+        self._hp_train = len(train_names)
+        self._hp_vbuf = np.zeros(len(var_names))
+        self._hp_gbuf = np.zeros(len(train_names))
+        self._hp_nbuf = np.zeros(1)
+        self._hp_ptrs = (self._hp_vbuf.ctypes.data, self._hp_gbuf.ctypes.data,
+                         self._hp_nbuf.ctypes.data)
+
+    def pieces_vars(self, var_values, form, mc_share=None, stream=None):
+        """This device's piece vector (layout of :meth:`local_pieces`) of
+        one evaluation at ``var_values`` (pwa_pieces_vars)."""
+        v = np.ascontiguousarray(var_values, np.float64)
+        out = np.zeros(3 + 2 * self._hp_train)
+        share = self.mc_share if mc_share is None else mc_share
+        self._check(load_library().pwa_pieces_vars(self.h, v.ctypes.data, int(form), self._sw,
+                                                   share, stream or 0, out.ctypes.data),
+                    "pwa_pieces_vars")
+        return out
+
+    def nll_grad_vars(self, var_values, form, stream=None):
+        """NLL and gradient at ``var_values`` with the host side in native
+        code (pwa_nll_grad_vars; over all devices through dist_reduce)."""
+        if self.dist_reduce is not None:
+            vec = self.dist_reduce(self.pieces_vars(var_values, form, stream=stream))
+            return combine_pieces(vec, self._hp_train)
+        self._hp_vbuf[:] = var_values
+        pv, pg, pn = self._hp_ptrs
+        self._check(load_library().pwa_nll_grad_vars(self.h, pv, int(form), self._sw,
+                                                     stream or 0, pn, pg), "pwa_nll_grad_vars")
+        return float(self._hp_nbuf[0]), self._hp_gbuf.copy()
 
     def cache_data(self, vals):
         if self.code.nrho or self.code.cp_chains:
