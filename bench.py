@@ -8,7 +8,8 @@ Prints one JSON line (rank 0).  ``value`` is device-timed evaluations/s of the
 headline (mixed) form: FP32 amplitudes, FP64 log-sum and reductions, MC
 integral from the FP64 Gram matrix (masses/widths fixed); inputs resident in
 HBM, L2 flushed before every timed step.  ``plain_f64`` is the same metric
-for the all-FP64 kernels.  ``e2e`` times the public call ``FCN.nll_grad(x)``
+for the all-FP64 kernels, through the same native host side (constants,
+chain rule in the library).  ``e2e`` times the public call ``FCN.nll_grad(x)``
 with host parameters in and host NLL/gradient out.  ``roofline`` covers the
 dominant kernel (the fused data-term kernel), timed with CUDA events on the
 stream it is launched on.  ``cpu_baseline`` times the FP64 CPU oracle on a
@@ -423,7 +424,7 @@ def measure_cached(name, args, rank, world, dist, timed, log, n_sig, n_bg, n_mc,
     import torch
 
     from tf_pwa_b200.api import FCN
-    from tf_pwa_b200.engine import MIXED_F32, PLAIN_F64
+    from tf_pwa_b200.engine import FORM_MIXED_F32, FORM_PLAIN_F64, MIXED_F32, PLAIN_F64
     from tf_pwa_b200.workload import make_dataset
 
     config, _, _, _, metric, workload = WORKLOADS[name]
@@ -464,7 +465,9 @@ def measure_cached(name, args, rank, world, dist, timed, log, n_sig, n_bg, n_mc,
     # headline: one NLL+gradient evaluation per step through the C ABI
     # (couplings -> cached-column kernel + Gram MC term -> chain rule)
     t_mixed = timed(lambda: eng.nll_grad_cached(var_vec), args.steps)
-    t_plain = timed(lambda: eng_p.nll_grad(vals, names, PLAIN_F64), args.steps)
+    # the plain FP64 form through the same native host side (host program)
+    assert fcn_plain.native_host
+    t_plain = timed(lambda: eng_p.nll_grad_vars(var_vec, FORM_PLAIN_F64), args.steps)
     # e2e through the public API with host parameters
     t_e2e = timed(lambda: fcn.nll_grad(x0), args.steps)
     # roofline: the data-term kernel (with its own ordered reduction) alone
@@ -491,7 +494,7 @@ def measure_cached(name, args, rank, world, dist, timed, log, n_sig, n_bg, n_mc,
     t_kernel_p = timed(lambda: eng_p.eval_enqueue(Cp, PLAIN_F64, mc=True), k_kernel)
     # the FP32-amplitude recompute form (what a fit with floating masses and
     # widths, where no column cache applies, uses instead of plain FP64)
-    t_f32 = timed(lambda: eng_p.nll_grad(vals, names, MIXED_F32), args.steps)
+    t_f32 = timed(lambda: eng_p.nll_grad_vars(var_vec, FORM_MIXED_F32), args.steps)
     t_kernel_f32 = timed(lambda: eng_p.eval_enqueue(Cp, MIXED_F32, mc=True), k_kernel)
     ck_clocks = clocks.stop(local)
     tuned = eng.cached_config()

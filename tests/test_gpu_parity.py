@@ -285,3 +285,35 @@ def test_native_host_shape_cache(name):
     assert abs(nll - ref_n) <= 1e-12 * abs(ref_n)
     np.testing.assert_allclose(grad, ref_g, rtol=0, atol=1e-10 * np.abs(ref_g).max())
     f.eng.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n_data,n_mc", [(1, 1), (31, 33), (129, 95), (397, 1499)])
+def test_shape_cache_ragged_sizes(n_data, n_mc):
+    """The floating-shape evaluation at set sizes that end inside a 32-event
+    segment and a 128-event tile, and a data/MC boundary inside one: NLL and
+    gradient against the plain FP64 form on the same events."""
+    import os
+
+    from common import CONFIGS
+    from tf_pwa_b200.api import FCN, ConfigLoader, EventData
+
+    g, meta = load_golden("d2kpipi_float")
+    cl = ConfigLoader(os.path.join(CONFIGS, meta["config"]))
+    cl.vm.set_all(meta["variables"])
+    xd = g["fields_data"][:, :n_data]
+    xm = g["fields_mc"][:, :n_mc]
+    assert xd.shape[1] == n_data and xm.shape[1] == n_mc
+    fm = FCN(cl, EventData(xd), EventData(xm), precision="mixed")
+    fp = FCN(cl, EventData(xd), EventData(xm), precision="plain")
+    assert fm.use_shape_cache
+    x1 = np.array(cl.vm.get_all_val())
+    for i, n in enumerate(cl.vm.trainable_vars):
+        if n.endswith(("_mass", "_width")):
+            x1[i] *= 1.01
+    n_m, g_m = fm.nll_grad(x1)
+    n_p, g_p = fp.nll_grad(x1)
+    assert abs(n_m - n_p) < 1e-6 * max(1.0, abs(n_p))
+    np.testing.assert_allclose(g_m, g_p, rtol=0, atol=1e-6 * np.abs(g_p).max())
+    fm.eng.close()
+    fp.eng.close()

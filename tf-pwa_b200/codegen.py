@@ -1010,6 +1010,11 @@ class ModelCode:
         L.append(self._pdf_source())
         fl = sorted(self._fset)
         L.append(f"#define PWA_NF {self.nf}")
+        # the floating-shape evaluation stages its next events in shared
+        # memory (two stages of pairs, masses and weight per event at 128
+        # threads) where that takes at most 150 KB per block
+        sc_bytes = 2 * (self.nf + max(len(self.mass_fields), 1) + 1) * 128 * 8
+        L.append(f"#define PWA_SC_STAGES {2 if sc_bytes <= 150 * 1024 else 0}")
         L.append("__device__ constexpr int pwa_fk[PWA_NF] = {" + ", ".join(str(k) for k, _ in fl) + "};")
         L.append("__device__ constexpr int pwa_fo[PWA_NF] = {" + ", ".join(str(o) for _, o in fl) + "};")
         # dataset step: momenta -> fields, and the phase-space generator;

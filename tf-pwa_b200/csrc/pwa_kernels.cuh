@@ -629,11 +629,40 @@ struct CRatio {
 #ifndef PWA_SC_MINB
 #define PWA_SC_MINB 2
 #endif
+// PWA_SC_STAGES 2 (set by the model source where the buffers fit): each warp
+// copies its next 32 events' cached pairs, masses and weights into shared
+// memory (16-byte cp.async, through L2) while it computes the current ones,
+// so the loads in flight do not depend on how many warps the registers
+// allow; 0: direct loads.
+#ifndef PWA_SC_STAGES
+#define PWA_SC_STAGES 0
+#endif
+#define PWA_SC_NM (PWA_NFIELD_MASS > 0 ? PWA_NFIELD_MASS : 1)
+// doubles (a float2 pair is one) of one stage: pairs, masses, weights
+#define PWA_SC_STAGE ((PWA_NF + PWA_SC_NM + 1) * PWA_TPB)
+
+// Copies of the 32 events from s (a multiple of 32, s < n_all) into stage
+// buffer d: lane l moves 16 bytes (two events) of rows l / 16, l / 16 + 2, ...
+__device__ __forceinline__ void sc_issue(double* __restrict__ d, const float2* __restrict__ Fc,
+                                         const double* __restrict__ XM,
+                                         const double* __restrict__ W, long long ld, long long s,
+                                         int warp, int lane) {
+  const long long t = s / PWA_TPB, e0 = s % PWA_TPB;
+  const int half = lane >> 4, c2 = 2 * (lane & 15), col = 32 * warp + c2;
+#pragma unroll
+  for (int j = half; j < PWA_NF; j += 2)
+    cp_async16(d + j * PWA_TPB + col, Fc + (t * PWA_NF + j) * PWA_TPB + e0 + c2);
+#pragma unroll
+  for (int m = half; m < PWA_NFIELD_MASS; m += 2)
+    cp_async16(d + (PWA_NF + m) * PWA_TPB + col, XM + (long long)m * ld + s + c2);
+  if (half == 0) cp_async16(d + (PWA_NF + PWA_SC_NM) * PWA_TPB + col, W + s + c2);
+}
+
 extern "C" __global__ void __launch_bounds__(PWA_TPB, PWA_SC_MINB)
     pwa_eval_shapecache(const Consts C, const CRatio rk, const float2* __restrict__ Fc,
                         const double* __restrict__ XM, const double* __restrict__ W,
                         long long n_data, long long n_all, long long ld, int blocks_data,
-                        double* __restrict__ partials) {
+                        double* __restrict__ partials, int smem_bytes) {
   constexpr int K = PWA_NCOL, NS = PWA_NSRES > 0 ? PWA_NSRES : 1;
   const bool is_data = (int)blockIdx.x < blocks_data;
   const long long beg = is_data ? 0 : n_data;
@@ -643,14 +672,53 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, PWA_SC_MINB)
   double acc[PWA_NACC];
 #pragma unroll
   for (int j = 0; j < PWA_NACC; ++j) acc[j] = 0.0;
+#if PWA_SC_STAGES > 0
+  extern __shared__ __align__(16) double sc_smem[];
+  if (smem_bytes < 2 * PWA_SC_STAGE * (int)sizeof(double)) {
+    // launched without the staging buffers: no event is read, the sums are NaN
+    for (int j = threadIdx.x; j < PWA_NACC; j += PWA_TPB)
+      partials[(long long)blockIdx.x * PWA_NACC + j] = __longlong_as_double(0x7ff8000000000000LL);
+    return;
+  }
+  const int lane_s = threadIdx.x & 31, warp_s = threadIdx.x >> 5;
+  const long long stride = (long long)nb * PWA_TPB;
+  // segments of 32 events from a multiple of 32 at or below beg (events
+  // outside [beg, end) are computed but not summed)
+  long long s = (beg & ~31LL) + (long long)b * PWA_TPB + 32 * warp_s;
+  if (s < end) sc_issue(sc_smem, Fc, XM, W, ld, s, warp_s, lane_s);
+  cp_async_commit();
+  for (int it = 0; s < end; s += stride, ++it) {
+    double* cur = sc_smem + (it & 1) * PWA_SC_STAGE;
+    double* nxt = sc_smem + ((it & 1) ^ 1) * PWA_SC_STAGE;
+    __syncwarp();  // every lane has read the other stage (last segment)
+    if (s + stride < end) sc_issue(nxt, Fc, XM, W, ld, s + stride, warp_s, lane_s);
+    cp_async_commit();
+    cp_async_wait_prior();  // this lane's copies of the current segment landed
+    __syncwarp();           // ... and every lane's
+    const long long i = s + lane_s;
+    const bool valid = i >= beg && i < end;
+    const int col = 32 * warp_s + lane_s;
+    // the pairs are read from shared memory where used (both passes), not
+    // held in registers
+    const float2* vs = reinterpret_cast<const float2*>(cur) + col;
+#define PWA_SC_V(j) vs[(j) * PWA_TPB]
+    cpx<double> BW[PWA_NCHAIN], DM[NS], DG[NS];
+    model_shapes<double, false>(C, cur + PWA_NF * PWA_TPB, PWA_TPB, col, BW, DM, DG);
+    const double w = valid ? cur[(PWA_NF + PWA_SC_NM) * PWA_TPB + col] : 0.0;
+#else
+  (void)smem_bytes;
   for (long long i = beg + (long long)b * PWA_TPB + threadIdx.x; i < end;
        i += (long long)nb * PWA_TPB) {
     const long long t = i / PWA_TPB, e = i % PWA_TPB;
+    constexpr bool valid = true;
     float2 v[PWA_NF];
 #pragma unroll
     for (int j = 0; j < PWA_NF; ++j) v[j] = __ldcs(Fc + (t * PWA_NF + j) * PWA_TPB + e);
+#define PWA_SC_V(j) v[j]
     cpx<double> BW[PWA_NCHAIN], DM[NS], DG[NS];
     model_shapes<double>(C, XM, ld, i, BW, DM, DG);
+    const double w = __ldg(W + i);
+#endif
     // F = s_k Fhat with s_k = r_k BW_ch(k); A_o = sum_k c_k s_k Fhat_k,o
     double ar[PWA_NOUT], ai[PWA_NOUT];
 #pragma unroll
@@ -661,22 +729,22 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, PWA_SC_MINB)
       const cpx<double> bw = BW[pwa_col_chain[k]];
       const cpx<double> cs = cmul(cmk<double>(C.v[2 * k], C.v[2 * k + 1]),
                                   cmk<double>(rk.v[k] * bw.re, rk.v[k] * bw.im));
-      const double x = (double)v[j].x, y = (double)v[j].y;
+      const float2 vj = PWA_SC_V(j);
+      const double x = (double)vj.x, y = (double)vj.y;
       ar[o] = fma(cs.re, x, fma(-cs.im, y, ar[o]));
       ai[o] = fma(cs.re, y, fma(cs.im, x, ai[o]));
     }
     double f = 0.0;
 #pragma unroll
     for (int o = 0; o < PWA_NOUT; ++o) f = fma(ar[o], ar[o], fma(ai[o], ai[o], f));
-    const double w = __ldg(W + i);
     double fac;
     if (is_data) {
       double dl;
       const double cl = clip_log(f, &dl);
-      acc[0] = fma(w, cl, acc[0]);
+      acc[0] = valid ? fma(w, cl, acc[0]) : acc[0];
       fac = w * dl;
     } else {
-      acc[0] = fma(w, f, acc[0]);
+      acc[0] = valid ? fma(w, f, acc[0]) : acc[0];
       fac = w;
     }
     // g_k = fac s_k sum_o conj(A_o) Fhat_k,o (the pairs j run column by
@@ -692,13 +760,15 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, PWA_SC_MINB)
       for (int j = 0; j < PWA_NF; ++j) {
         if (pwa_fk[j] != k) continue;
         const int o = pwa_fo[j];
-        const double x = (double)v[j].x, y = (double)v[j].y;
+        const float2 vj = PWA_SC_V(j);
+        const double x = (double)vj.x, y = (double)vj.y;
         hk.re = fma(ar[o], x, fma(ai[o], y, hk.re));
         hk.im = fma(ar[o], y, fma(-ai[o], x, hk.im));
       }
       const cpx<double> bw = BW[pwa_col_chain[k]];
-      const cpx<double> g =
-          cscale(cmul(cmk<double>(rk.v[k] * bw.re, rk.v[k] * bw.im), hk), fac);
+      cpx<double> g = cscale(cmul(cmk<double>(rk.v[k] * bw.re, rk.v[k] * bw.im), hk), fac);
+      g.re = valid ? g.re : 0.0;  // events outside the set (garbage inputs: select, not scale)
+      g.im = valid ? g.im : 0.0;
       acc[1 + 2 * k] += g.re;
       acc[2 + 2 * k] += g.im;
       const cpx<double> cg = cmul(cmk<double>(C.v[2 * k], C.v[2 * k + 1]), g);
@@ -711,10 +781,15 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, PWA_SC_MINB)
     }
 #pragma unroll
     for (int q = 0; q < PWA_NSRES; ++q) {
-      acc[1 + 2 * K + 2 * q] += 2.0 * cmul(SR[q], DM[q]).re;
-      acc[2 + 2 * K + 2 * q] += 2.0 * cmul(SR[q], DG[q]).re;
+      const double dm = 2.0 * cmul(SR[q], DM[q]).re, dg = 2.0 * cmul(SR[q], DG[q]).re;
+      acc[1 + 2 * K + 2 * q] += valid ? dm : 0.0;
+      acc[2 + 2 * K + 2 * q] += valid ? dg : 0.0;
     }
   }
+#if PWA_SC_STAGES > 0
+  cp_async_wait_all();  // (nothing is in flight here: the last group is empty)
+#endif
+#undef PWA_SC_V
   __shared__ double red[PWA_TPB / 32][PWA_NACC];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll

@@ -120,6 +120,8 @@ struct pwa_plan {
   float2* scache = nullptr;
   long long scache_n = 0;
   int sc_blocks = 0, sc_blocks_data = 0;
+  int sc_stages = 0;  // PWA_SC_STAGES of the model source
+  int sc_smem = 0;    // dynamic shared memory of pwa_eval_shapecache
   bool shape_cache_ok = false;  // the model's columns factorise (PWA_SHAPE_CACHE_OK 1)
   double* d_hsum = nullptr;
   // parameter layout for the C-side chain rule
@@ -381,6 +383,12 @@ int pwa_plan_create(const char* src, size_t src_len, int n_mass, int n_angle, in
       std::string(src, src_len).find("#define PWA_HESS_STAGE 1") != std::string::npos;
   h->shape_cache_ok =
       std::string(src, src_len).find("#define PWA_SHAPE_CACHE_OK 1") != std::string::npos;
+  {
+    const std::string key = "#define PWA_SC_STAGES ";
+    const std::string text(src, src_len);
+    const size_t at = text.find(key);
+    h->sc_stages = at == std::string::npos ? 0 : std::atoi(text.c_str() + at + key.size());
+  }
   h->n_angle = n_angle;
   h->ncol = ncol;
   h->nout = nout;
@@ -619,10 +627,18 @@ int pwa_shape_cache(pwa_plan* h, const double* consts, void* stream) {
   if (nb > 16LL * h->sms) nb = 16LL * h->sms;
   int rc = launch(h, h->k.cache_ns_f32, dim3((int)nb), dim3(h->tpb), args, s);
   if (rc) return rc;
+  // staging buffers of the evaluation: two stages of (pairs, masses,
+  // weight) per thread
+  h->sc_smem = h->sc_stages > 0
+                   ? 2 * (h->nf + (h->n_mass > 0 ? h->n_mass : 1) + 1) * h->tpb * (int)sizeof(double)
+                   : 0;
+  if (h->sc_smem > 48 * 1024)
+    CU(cudaFuncSetAttribute((const void*)h->k.eval_shapecache,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize, h->sc_smem));
   // persistent grid split between data and MC events as the plain kernels
   int per_sm = 0;
   CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)h->k.eval_shapecache,
-                                                   h->tpb, 0));
+                                                   h->tpb, h->sc_smem));
   if (per_sm < 1) per_sm = 1;
   const long long want = (long long)per_sm * h->sms;
   long long gb = want < ntiles ? want : ntiles;
@@ -649,11 +665,13 @@ int pwa_eval_shapecache_enqueue(pwa_plan* h, const double* consts, const double*
   cudaStream_t s = (cudaStream_t)stream;
   std::vector<double> cbuf = consts_block(h, consts), rbuf(ratio, ratio + h->ncol);
   long long nd = h->n_data, na = h->n_data + h->n_mc, ld = h->ld;
-  int bd = h->sc_blocks_data, nb = h->sc_blocks;
+  int bd = h->sc_blocks_data, nb = h->sc_blocks, smem = h->sc_smem;
   void* args[] = {cbuf.data(), rbuf.data(), &h->scache, &h->xm, &h->w, &nd, &na, &ld, &bd,
-                  &h->partials};
-  int rc = launch(h, h->k.eval_shapecache, dim3(nb), dim3(h->tpb), args, s);
-  if (rc) return rc;
+                  &h->partials, &smem};
+  cudaError_t e = cudaLaunchKernel((const void*)h->k.eval_shapecache, dim3(nb), dim3(h->tpb), args,
+                                   (size_t)smem, s);
+  if (e != cudaSuccess)
+    return set_err(h, PWA_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
   int nacc = h->nacc;
   void* args2[] = {&h->partials, &nacc, &bd, &nb, &h->d_out};
   return launch(h, h->k.reduce, dim3(1), dim3(1024), args2, s);
