@@ -169,3 +169,75 @@ def test_two_rank_engine_pieces(name, tmp_path):
     for rank, nll, grad, ref_nll, ref_grad in res:
         assert abs(nll - ref_nll) <= 1e-9 * abs(ref_nll)
         np.testing.assert_allclose(grad, ref_grad, rtol=1e-7, atol=1e-7 * np.abs(ref_grad).max())
+
+
+def _native_pieces(rank, world, q, name, build_dir):
+    """The native host program's piece vector (pwa_hostprog_pieces: its own
+    constant block, Jacobian and chain rule) on this rank's half of the
+    events, summed over the ranks with gloo and combined."""
+    import sys
+
+    here = os.path.dirname(os.path.abspath(__file__))
+    sys.path.insert(0, here)
+    sys.path.insert(0, os.path.dirname(here))
+    import conftest  # noqa: F401
+    import torch
+    import torch.distributed as dist
+
+    from common import golden_data, load_golden, load_model
+    from hostexec import HostModel
+    from tf_pwa_b200.engine import Engine, combine_pieces
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    g, meta = load_golden(name)
+    dc, vm, plan = load_model(meta["config"])
+    vm.set_all(meta["variables"])
+    eng = Engine(dc.decay_group, plan, vm, compile=False)
+    hm = HostModel(eng.code, build_dir)
+    names = list(vm.variables)
+    hp = eng.host_program(names, meta["trainable"])
+    v = np.array([vm.variables[k] for k in names])
+    xd, wd = golden_data(g, meta)
+    xm = g["fields_mc"]
+    wm_all = np.ones(xm.shape[1]) / xm.shape[1]
+    sd_idx = np.array_split(np.arange(xd.shape[1]), world)[rank]
+    sm_idx = np.array_split(np.arange(xm.shape[1]), world)[rank]
+    share = wm_all[sm_idx].sum()
+    x = np.concatenate([xd[:, sd_idx], xm[:, sm_idx]], 1)
+    w = np.concatenate([wd[sd_idx], wm_all[sm_idx] / share])
+    sd, sm = hm.sums(hp.consts(v), x, w, len(sd_idx))
+    vec = torch.as_tensor(hp.pieces(v, sd, sm, float(wd[sd_idx].sum()), share))
+    dist.all_reduce(vec)
+    nll, grad = combine_pieces(vec.numpy(), len(meta["trainable"]))
+    dist.destroy_process_group()
+    q.put((rank, nll, grad, float(g["nll"]), np.asarray(g["grad"])))
+
+
+@pytest.mark.parametrize("name", ["d2kpipi_float", "lc2pkpi"])
+def test_two_rank_native_host_pieces(name, tmp_path):
+    """Two gloo ranks, each with half of the data and MC events, through the
+    native host program: the reference's single-process NLL and gradient."""
+    import torch.multiprocessing as mp
+
+    from common import load_golden, load_model
+    from hostexec import HostModel
+    from tf_pwa_b200.engine import Engine
+
+    g, meta = load_golden(name)
+    dc, vm, plan = load_model(meta["config"])
+    HostModel(Engine(dc.decay_group, plan, vm, compile=False).code, str(tmp_path))  # build once
+    os.environ["MASTER_PORT"] = str(29700 + os.getpid() % 1000 + (name == "lc2pkpi"))
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_native_pieces, args=(r, 2, q, name, str(tmp_path)))
+             for r in range(2)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=300) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank, nll, grad, ref_nll, ref_grad in res:
+        assert abs(nll - ref_nll) <= 1e-9 * abs(ref_nll)
+        np.testing.assert_allclose(grad, ref_grad, rtol=1e-7, atol=1e-7 * np.abs(ref_grad).max())
