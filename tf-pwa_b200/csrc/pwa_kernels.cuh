@@ -658,11 +658,23 @@ __device__ __forceinline__ void sc_issue(double* __restrict__ d, const float2* _
   if (half == 0) cp_async16(d + (PWA_NF + PWA_SC_NM) * PWA_TPB + col, W + s + c2);
 }
 
+// Ends with the ordered two-level reduction of pwa_eval_cached (grouped_sum,
+// declared below): block rows of 2 * PWA_NACC (a data block's sums in the
+// first half, an MC block's in the second); the last block writes the data
+// and MC sums to out[0 .. 2 PWA_NACC), the error flag and the call number
+// seq (publish_result); out may be mapped host memory.
+__device__ __forceinline__ bool grouped_sum(double* __restrict__ partials,
+                                            unsigned int* __restrict__ ticket, int na,
+                                            double* __restrict__ out, int* s_flag);
+__device__ __forceinline__ void publish_result(unsigned int* __restrict__ ticket, int na,
+                                               double* __restrict__ out, double seq);
+
 extern "C" __global__ void __launch_bounds__(PWA_TPB, PWA_SC_MINB)
     pwa_eval_shapecache(const Consts C, const CRatio rk, const float2* __restrict__ Fc,
                         const double* __restrict__ XM, const double* __restrict__ W,
                         long long n_data, long long n_all, long long ld, int blocks_data,
-                        double* __restrict__ partials, int smem_bytes) {
+                        double* __restrict__ partials, int smem_bytes,
+                        unsigned int* __restrict__ ticket, double* __restrict__ out, double seq) {
   constexpr int K = PWA_NCOL, NS = PWA_NSRES > 0 ? PWA_NSRES : 1;
   const bool is_data = (int)blockIdx.x < blocks_data;
   const long long beg = is_data ? 0 : n_data;
@@ -674,17 +686,14 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, PWA_SC_MINB)
   for (int j = 0; j < PWA_NACC; ++j) acc[j] = 0.0;
 #if PWA_SC_STAGES > 0
   extern __shared__ __align__(16) double sc_smem[];
-  if (smem_bytes < 2 * PWA_SC_STAGE * (int)sizeof(double)) {
-    // launched without the staging buffers: no event is read, the sums are NaN
-    for (int j = threadIdx.x; j < PWA_NACC; j += PWA_TPB)
-      partials[(long long)blockIdx.x * PWA_NACC + j] = __longlong_as_double(0x7ff8000000000000LL);
-    return;
-  }
+  // launched without the staging buffers: no event is read, the sums are NaN
+  const bool staged = smem_bytes >= 2 * PWA_SC_STAGE * (int)sizeof(double);
+  if (!staged) acc[0] = __longlong_as_double(0x7ff8000000000000LL);
   const int lane_s = threadIdx.x & 31, warp_s = threadIdx.x >> 5;
   const long long stride = (long long)nb * PWA_TPB;
   // segments of 32 events from a multiple of 32 at or below beg (events
   // outside [beg, end) are computed but not summed)
-  long long s = (beg & ~31LL) + (long long)b * PWA_TPB + 32 * warp_s;
+  long long s = staged ? (beg & ~31LL) + (long long)b * PWA_TPB + 32 * warp_s : end;
   if (s < end) sc_issue(sc_smem, Fc, XM, W, ld, s, warp_s, lane_s);
   cp_async_commit();
   for (int it = 0; s < end; s += stride, ++it) {
@@ -791,6 +800,7 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, PWA_SC_MINB)
 #endif
 #undef PWA_SC_V
   __shared__ double red[PWA_TPB / 32][PWA_NACC];
+  __shared__ int s_last;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int j = 0; j < PWA_NACC; ++j) {
@@ -798,12 +808,20 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, PWA_SC_MINB)
     if (lane == 0) red[warp][j] = vv;
   }
   __syncthreads();
-  for (int j = threadIdx.x; j < PWA_NACC; j += PWA_TPB) {
+  constexpr int NA2 = 2 * PWA_NACC;
+  for (int j = threadIdx.x; j < NA2; j += PWA_TPB) {
+    const int jj = j - (is_data ? 0 : PWA_NACC);
     double sacc = 0.0;
+    if (jj >= 0 && jj < PWA_NACC) {
 #pragma unroll
-    for (int w2 = 0; w2 < PWA_TPB / 32; ++w2) sacc += red[w2][j];
-    partials[(long long)blockIdx.x * PWA_NACC + j] = sacc;
+      for (int w2 = 0; w2 < PWA_TPB / 32; ++w2) sacc += red[w2][jj];
+    }
+    partials[(long long)blockIdx.x * NA2 + j] = sacc;
   }
+  __threadfence();
+  __syncthreads();
+  if (!grouped_sum(partials, ticket, NA2, out, &s_last)) return;
+  publish_result(ticket, NA2, out, seq);
 }
 
 struct CCoup {

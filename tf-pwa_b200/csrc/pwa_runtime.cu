@@ -89,6 +89,8 @@ struct pwa_plan {
   unsigned int* ticket = nullptr;  // [0] finished groups, [1] error flag, [2 + g] group counts
   double* h_map = nullptr;         // mapped pinned result of the cached kernel
   double* d_map = nullptr;         // its device address
+  double* h_map_sc = nullptr;      // mapped result of pwa_eval_shapecache (2 nacc + 2)
+  double* d_map_sc = nullptr;
   double seq = 0.0;
   std::vector<double> gram;  // MC Gram matrix, (re, im) row-major ncol x ncol
   bool gram_valid = false;
@@ -463,6 +465,9 @@ int pwa_plan_create(const char* src, size_t src_len, int n_mass, int n_angle, in
   CU(cudaMemset(h->ticket, 0, kTicketWords * sizeof(unsigned int)));
   CU(cudaHostAlloc(&h->h_map, sizeof(double) * (2 * ncol + 4), cudaHostAllocMapped));
   CU(cudaHostGetDevicePointer((void**)&h->d_map, h->h_map, 0));
+  CU(cudaHostAlloc(&h->h_map_sc, sizeof(double) * (2 * h->nacc + 2), cudaHostAllocMapped));
+  CU(cudaHostGetDevicePointer((void**)&h->d_map_sc, h->h_map_sc, 0));
+  h->h_map_sc[2 * h->nacc + 1] = -1.0;
   CU(cudaMallocHost(&h->h_out, sizeof(double) * 2 * (h->nacc > ncol * ncol ? h->nacc : ncol * ncol)));
   return PWA_OK;
 }
@@ -486,6 +491,7 @@ int pwa_plan_destroy(pwa_plan* h) {
   if (h->d_hsum) cudaFree(h->d_hsum);
   if (h->scache) cudaFree(h->scache);
   if (h->h_map) cudaFreeHost(h->h_map);
+  if (h->h_map_sc) cudaFreeHost(h->h_map_sc);
   if (h->d_out) cudaFree(h->d_out);
   if (h->h_out) cudaFreeHost(h->h_out);
   if (h->lib) cudaLibraryUnload(h->lib);
@@ -646,7 +652,8 @@ int pwa_shape_cache(pwa_plan* h, const double* consts, void* stream) {
   long long bd = h->n_mc == 0 ? gb : (h->n_data == 0 ? 0 : (gb * h->n_data + n / 2) / n);
   if (h->n_data > 0 && bd < 1) bd = 1;
   if (h->n_mc > 0 && bd > gb - 1) bd = gb - 1;
-  rc = ensure_partials(h, gb * h->nacc);
+  // block rows of 2 nacc and the group rows of the in-kernel reduction
+  rc = ensure_partials(h, (gb + (gb + 15) / 16) * 2 * h->nacc);
   if (rc) return rc;
   h->sc_blocks = (int)gb;
   h->sc_blocks_data = (int)bd;
@@ -666,15 +673,15 @@ int pwa_eval_shapecache_enqueue(pwa_plan* h, const double* consts, const double*
   std::vector<double> cbuf = consts_block(h, consts), rbuf(ratio, ratio + h->ncol);
   long long nd = h->n_data, na = h->n_data + h->n_mc, ld = h->ld;
   int bd = h->sc_blocks_data, nb = h->sc_blocks, smem = h->sc_smem;
+  h->seq += 1.0;
+  double seq = h->seq;
   void* args[] = {cbuf.data(), rbuf.data(), &h->scache, &h->xm, &h->w, &nd, &na, &ld, &bd,
-                  &h->partials, &smem};
+                  &h->partials, &smem, &h->ticket, &h->d_map_sc, &seq};
   cudaError_t e = cudaLaunchKernel((const void*)h->k.eval_shapecache, dim3(nb), dim3(h->tpb), args,
                                    (size_t)smem, s);
   if (e != cudaSuccess)
     return set_err(h, PWA_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
-  int nacc = h->nacc;
-  void* args2[] = {&h->partials, &nacc, &bd, &nb, &h->d_out};
-  return launch(h, h->k.reduce, dim3(1), dim3(1024), args2, s);
+  return PWA_OK;
 }
 
 int pwa_eval_shapecache(pwa_plan* h, const double* consts, const double* ratio, void* stream,
@@ -684,10 +691,25 @@ int pwa_eval_shapecache(pwa_plan* h, const double* consts, const double* ratio, 
   int rc = pwa_eval_shapecache_enqueue(h, consts, ratio, stream);
   if (rc) return rc;
   cudaStream_t s = (cudaStream_t)stream;
-  const int nacc = h->nacc;
-  CU(cudaMemcpyAsync(h->h_out, h->d_out, sizeof(double) * 2 * nacc, cudaMemcpyDeviceToHost, s));
-  CU(cudaStreamSynchronize(s));
-  std::memcpy(out, h->h_out, sizeof(double) * 2 * nacc);
+  const int na2 = 2 * h->nacc;
+  // the kernel publishes its call number last (after a system fence) into
+  // the mapped result: poll it, with a stream synchronisation after 1 s
+  const volatile double* m = h->h_map_sc;
+  const auto t0 = std::chrono::steady_clock::now();
+  for (unsigned it = 1; m[na2 + 1] != h->seq; ++it) {
+    if ((it & 4095u) == 0 &&
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > 1.0) {
+      CU(cudaStreamSynchronize(s));
+      break;
+    }
+  }
+  std::atomic_thread_fence(std::memory_order_acquire);
+  if (m[na2 + 1] != h->seq) {
+    cudaMemset(h->ticket, 0, kTicketWords * sizeof(unsigned int));
+    return set_err(h, PWA_ERR_CUDA, "floating-shape evaluation did not complete (stale result)");
+  }
+  if (m[na2] != 0.0) return set_err(h, PWA_ERR_CUDA, "floating-shape evaluation: error flag set");
+  for (int j = 0; j < na2; ++j) out[j] = m[j];
   return PWA_OK;
 }
 
