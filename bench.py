@@ -55,6 +55,9 @@ CONFIG, N_SIG, N_BG, N_MC, METRIC, WORKLOAD = WORKLOADS["lc2pkpi"]
 # 1e6 rows); traffic grows with the rows, so a launch's traffic = this x rows
 NCU_TRAFFIC_PER_ROW = {"lc2pkpi": (290.436096e6 + 6.841088e6) / 1.1e6,
                        "b2dstkpi": (248.044032e6 + 3.609856e6) / 1e6}
+# the same for the floating-shape evaluation kernel, per event (data + MC):
+# D -> K pi pi, 80.04 + 2.29 MB for 2e6 events
+NCU_SC_TRAFFIC_PER_EVENT = {"d2kpipi_float": (80.041728e6 + 2.286848e6) / 2e6}
 
 
 def _select(name):
@@ -688,8 +691,12 @@ def measure_floating(name, args, rank, world, dist, timed, log, n_sig, n_mc):
     fl_p = NCU_F64_FLOPS_PER_EVENT[name]
     ach_p = fl_p * n_all / (t_kp / args.steps) / 1e12
     roof = {"bound": "hbm", "achieved": ach_s, "peak": hbm, "unit": "GB/s", "frac": ach_s / hbm,
-            "traffic": None, "peak_kind": peak_kind,
-            "kernel": "pwa_eval_shapecache + pwa_reduce (data + MC: FP32 shape-free columns, "
+            "traffic": (NCU_SC_TRAFFIC_PER_EVENT[name] * n_all
+                        if name in NCU_SC_TRAFFIC_PER_EVENT else None),
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch at "
+                              "the bench size, scaled by the events",
+            "peak_kind": peak_kind,
+            "kernel": "pwa_eval_shapecache with its own reduction (data + MC: FP32 shape-free columns, "
                       "FP64 masses, lineshapes recomputed)",
             "algorithmic_bytes_per_launch": bytes_sc, "launch_us": 1e6 * t_ks / args.steps,
             "plain_f64_kernel": {
@@ -753,7 +760,7 @@ def measure_floating(name, args, rank, world, dist, timed, log, n_sig, n_mc):
 def _compact(line):
     """A workload's line trimmed for the `workloads` key of the headline line."""
     keep = ("metric", "value", "unit", "ms_per_step", "config", "plain_f64", "fp32_recompute",
-            "e2e", "roofline", "autotune", "hessian", "check", "clocks", "setup_s")
+            "e2e", "roofline", "host", "autotune", "hessian", "check", "clocks", "setup_s")
     return {k: line[k] for k in keep if k in line}
 
 
