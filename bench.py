@@ -58,6 +58,8 @@ NCU_TRAFFIC_PER_ROW = {"lc2pkpi": (290.436096e6 + 6.841088e6) / 1.1e6,
 # the same for the floating-shape evaluation kernel, per event (data + MC):
 # D -> K pi pi, 80.04 + 2.29 MB for 2e6 events
 NCU_SC_TRAFFIC_PER_EVENT = {"d2kpipi_float": (80.041728e6 + 2.286848e6) / 2e6}
+# its FP64 operations per event (2 DFMA + DMUL + DADD executed, ncu, 2e6 events)
+NCU_SC_F64_FLOPS_PER_EVENT = {"d2kpipi_float": (2 * 249757760 + 131606208 + 59444606) / 2e6}
 
 
 def _select(name):
@@ -690,21 +692,35 @@ def measure_floating(name, args, rank, world, dist, timed, log, n_sig, n_mc):
                            "peak_kind": peak_kind, "algorithmic_bytes_per_launch": bytes_f32}})
     fl_p = NCU_F64_FLOPS_PER_EVENT[name]
     ach_p = fl_p * n_all / (t_kp / args.steps) / 1e12
-    roof = {"bound": "hbm", "achieved": ach_s, "peak": hbm, "unit": "GB/s", "frac": ach_s / hbm,
-            "traffic": (NCU_SC_TRAFFIC_PER_EVENT[name] * n_all
-                        if name in NCU_SC_TRAFFIC_PER_EVENT else None),
-            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch at "
-                              "the bench size, scaled by the events",
-            "peak_kind": peak_kind,
-            "kernel": "pwa_eval_shapecache with its own reduction (data + MC: FP32 shape-free columns, "
-                      "FP64 masses, lineshapes recomputed)",
-            "algorithmic_bytes_per_launch": bytes_sc, "launch_us": 1e6 * t_ks / args.steps,
-            "plain_f64_kernel": {
-                "bound": "fp64", "achieved": ach_p, "peak": peaks["f64_tflops"],
-                "unit": "TFLOP/s", "frac": ach_p / peaks["f64_tflops"], "flops_per_event": fl_p,
-                "flops_source": "ncu: 2 DFMA + DADD + DMUL executed per event (forward and "
-                                "adjoint)",
-                "launch_us": 1e6 * t_kp / args.steps, "algorithmic_bytes_per_launch": bytes_f64}}
+    hbm_roof = {"bound": "hbm", "achieved": ach_s, "peak": hbm, "unit": "GB/s",
+                "frac": ach_s / hbm,
+                "traffic": (NCU_SC_TRAFFIC_PER_EVENT[name] * n_all
+                            if name in NCU_SC_TRAFFIC_PER_EVENT else None),
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch "
+                                  "at the bench size, scaled by the events",
+                "peak_kind": peak_kind}
+    if name in NCU_SC_F64_FLOPS_PER_EVENT:
+        # the kernel is bound by its FP64 lineshape arithmetic, not by HBM
+        fl_s = NCU_SC_F64_FLOPS_PER_EVENT[name]
+        ach_f = fl_s * n_all / (t_ks / args.steps) / 1e12
+        roof = {"bound": "fp64", "achieved": ach_f, "peak": peaks["f64_tflops"],
+                "unit": "TFLOP/s", "frac": ach_f / peaks["f64_tflops"],
+                "peak_kind": "measured here (pwa_fma_peak, FP64 FMA chains)",
+                "flops_per_event": fl_s,
+                "flops_source": "ncu: 2 DFMA + DMUL + DADD executed per event",
+                "traffic": hbm_roof["traffic"], "hbm": hbm_roof}
+    else:
+        roof = dict(hbm_roof)
+    roof.update({
+        "kernel": "pwa_eval_shapecache with its own reduction (data + MC: FP32 shape-free columns, "
+                  "FP64 masses, lineshapes recomputed)",
+        "algorithmic_bytes_per_launch": bytes_sc, "launch_us": 1e6 * t_ks / args.steps,
+        "plain_f64_kernel": {
+            "bound": "fp64", "achieved": ach_p, "peak": peaks["f64_tflops"],
+            "unit": "TFLOP/s", "frac": ach_p / peaks["f64_tflops"], "flops_per_event": fl_p,
+            "flops_source": "ncu: 2 DFMA + DADD + DMUL executed per event (forward and "
+                            "adjoint)",
+            "launch_us": 1e6 * t_kp / args.steps, "algorithmic_bytes_per_launch": bytes_f64}})
     line = {
         "metric": metric, "value": world * args.steps / t_sc, "unit": "evals/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,

@@ -122,8 +122,12 @@ extern "C" __global__ void __launch_bounds__(PWA_TPB, PWA_EVAL_MINB_F32)
 
 // out[0..nacc) = data sums, out[nacc..2 nacc) = MC sums.  One warp per
 // accumulator; each lane strides over the blocks, then a fixed shuffle tree.
+// With seq_out set (out in mapped host memory), the call number seq is
+// written there last, after a system-scope fence that orders every warp's
+// out[] writes (observed through the block barrier) before it.
 extern "C" __global__ void pwa_reduce(const double* __restrict__ partials, int nacc,
-                                      int blocks_data, int nblocks, double* __restrict__ out) {
+                                      int blocks_data, int nblocks, double* __restrict__ out,
+                                      double* __restrict__ seq_out, double seq) {
   const int lane = threadIdx.x & 31;
   const int warps = blockDim.x >> 5;
   for (int j = (int)(threadIdx.x >> 5); j < 2 * nacc; j += warps) {
@@ -133,6 +137,13 @@ extern "C" __global__ void pwa_reduce(const double* __restrict__ partials, int n
     for (int b = b0 + lane; b < b1; b += 32) s += partials[(long long)b * nacc + jj];
     s = warp_sum(s);
     if (lane == 0) out[j] = s;
+  }
+  if (seq_out) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence_system();
+      *seq_out = seq;
+    }
   }
 }
 

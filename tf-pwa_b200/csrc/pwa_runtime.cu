@@ -594,19 +594,47 @@ int pwa_eval_enqueue(pwa_plan* h, const double* consts, int precision, int mc, v
   if (!mc) {
     // only data sums: the MC half of d_out is cleared by the reduction
   }
-  void* args2[] = {&h->partials, &nacc, &bd, &nblocks, &h->d_out};
+  // sums into the mapped result, the call number last
+  h->seq += 1.0;
+  double seq = h->seq;
+  double* seq_out = h->d_map_sc + 2 * nacc + 1;
+  void* args2[] = {&h->partials, &nacc, &bd, &nblocks, &h->d_map_sc, &seq_out, &seq};
   return launch(h, h->k.reduce, dim3(1), dim3(1024), args2, s);
 }
+
+namespace {
+// Wait for the sums of the last pwa_eval_enqueue / pwa_eval_shapecache_enqueue
+// in the mapped result (its call number is written last); after 1 s without
+// it, synchronise the stream (which also surfaces launch errors).
+int wait_mapped_sums(pwa_plan* h, cudaStream_t s) {
+  const int na2 = 2 * h->nacc;
+  const volatile double* m = h->h_map_sc;
+  const auto t0 = std::chrono::steady_clock::now();
+  for (unsigned it = 1; m[na2 + 1] != h->seq; ++it) {
+    if ((it & 4095u) == 0 &&
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > 1.0) {
+      CU(cudaStreamSynchronize(s));
+      break;
+    }
+  }
+  std::atomic_thread_fence(std::memory_order_acquire);
+  if (m[na2 + 1] != h->seq) {
+    cudaMemset(h->ticket, 0, kTicketWords * sizeof(unsigned int));
+    return set_err(h, PWA_ERR_CUDA, "evaluation did not complete (stale result)");
+  }
+  return PWA_OK;
+}
+}  // namespace
 
 int pwa_eval(pwa_plan* h, const double* consts, int precision, int mc, void* stream, double* out) {
   if (!out) return set_err(h, PWA_ERR_ARG, "null output");
   int rc = pwa_eval_enqueue(h, consts, precision, mc, stream);
   if (rc) return rc;
-  cudaStream_t s = (cudaStream_t)stream;
-  int nacc = h->nacc;
-  CU(cudaMemcpyAsync(h->h_out, h->d_out, sizeof(double) * 2 * nacc, cudaMemcpyDeviceToHost, s));
-  CU(cudaStreamSynchronize(s));
-  std::memcpy(out, h->h_out, sizeof(double) * 2 * nacc);
+  rc = wait_mapped_sums(h, (cudaStream_t)stream);
+  if (rc) return rc;
+  const int nacc = h->nacc;
+  const volatile double* m = h->h_map_sc;
+  for (int j = 0; j < 2 * nacc; ++j) out[j] = m[j];
   if (!mc)
     for (int j = 0; j < nacc; ++j) out[nacc + j] = 0.0;
   return PWA_OK;
@@ -690,24 +718,12 @@ int pwa_eval_shapecache(pwa_plan* h, const double* consts, const double* ratio, 
   if (!out) return set_err(h, PWA_ERR_ARG, "null output");
   int rc = pwa_eval_shapecache_enqueue(h, consts, ratio, stream);
   if (rc) return rc;
-  cudaStream_t s = (cudaStream_t)stream;
-  const int na2 = 2 * h->nacc;
   // the kernel publishes its call number last (after a system fence) into
-  // the mapped result: poll it, with a stream synchronisation after 1 s
+  // the mapped result
+  rc = wait_mapped_sums(h, (cudaStream_t)stream);
+  if (rc) return rc;
+  const int na2 = 2 * h->nacc;
   const volatile double* m = h->h_map_sc;
-  const auto t0 = std::chrono::steady_clock::now();
-  for (unsigned it = 1; m[na2 + 1] != h->seq; ++it) {
-    if ((it & 4095u) == 0 &&
-        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > 1.0) {
-      CU(cudaStreamSynchronize(s));
-      break;
-    }
-  }
-  std::atomic_thread_fence(std::memory_order_acquire);
-  if (m[na2 + 1] != h->seq) {
-    cudaMemset(h->ticket, 0, kTicketWords * sizeof(unsigned int));
-    return set_err(h, PWA_ERR_CUDA, "floating-shape evaluation did not complete (stale result)");
-  }
   if (m[na2] != 0.0) return set_err(h, PWA_ERR_CUDA, "floating-shape evaluation: error flag set");
   for (int j = 0; j < na2; ++j) out[j] = m[j];
   return PWA_OK;
@@ -2318,7 +2334,9 @@ extern "C" int pwa_eval_noalloc(pwa_plan* h, const double* consts, const double*
   rc = launch(h, h->k.eval_f64, dim3(nblocks), dim3(h->tpb), args, s);
   if (rc) return rc;
   int nacc = h->nacc;
-  void* args2[] = {&scratch, &nacc, &blocks_data, &nblocks, &out};
+  double* no_seq = nullptr;
+  double seq0 = 0.0;
+  void* args2[] = {&scratch, &nacc, &blocks_data, &nblocks, &out, &no_seq, &seq0};
   return launch(h, h->k.reduce, dim3(1), dim3(1024), args2, s);
 }
 
