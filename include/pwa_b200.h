@@ -294,7 +294,8 @@ int pwa_nll_grad_cached(pwa_plan* h, const double* vars, double sw, void* stream
  * takes; it needs no device and runs on the host alone.
  *
  * Format: ip (int) and dp (double) arrays read in order
- *   ip: 0x50574850, 1, ncol, nconst, nshape, n_vars, n_train, n_coup, nfac,
+ *   ip: 0x50574850, 2, ncol, nconst, nshape (all sums past the column
+ *       sums, as pwa_plan_create), n_vars, n_train, n_coup, nfac,
  *       coup_r[n_coup], coup_i[n_coup], coup_polar[n_coup] (the couplings'
  *       variable indices, polar r e^{i phi} or r + i phi),
  *       col_fac[ncol*nfac] (column k = product of couplings, -1 unused),
@@ -312,10 +313,19 @@ int pwa_nll_grad_cached(pwa_plan* h, const double* vars, double sw, void* stream
  *       n_mj, per resonance mass with barrier factors: variable, mass
  *         index, n_verts, verts[], n_c, n_c x (column, vertex, entry),
  *       n_rt, n_rt x (column, slot, sqrt) (barrier normalisations of each
- *         column), 0x50574850
+ *         column),
+ *       n_rho, rho_re[n_rho], rho_im[n_rho] (density matrix slots of a
+ *         polarised parent, 0 entries otherwise), pol_off (its sums after
+ *         the lineshape sums), n_pol, pol_var[n_pol],
+ *       n_cp, n_cp x (coupling, deltar variable, deltai variable, charge -1
+ *         re slot, im slot) (CP-violating totals),
+ *       n_cpc, n_cpc x (column, charge -1 coupling re slot, im slot),
+ *       cp_off (charge -1 column sums among the extra sums, -1 none),
+ *       0x50574850
  *   dp: m_base[n_m] (masses of the fixed entries), per vertex d and per
  *       entry coef[n_coef] (B' polynomial, highest power first), per
- *       lineshape d, default width, coef[n_coef].
+ *       lineshape d, default width, coef[n_coef]; rho = rho0 + sum_q p_q G_q:
+ *       rho0 and per polarisation variable G_q as n_rho (re, im) pairs.
  * PWA_ERR_ARG (message in pwa_last_error(NULL)) for a malformed program. */
 int pwa_hostprog_create(const int* ip, long long n_ip, const double* dp, long long n_dp,
                         pwa_hostprog** out);
@@ -323,8 +333,12 @@ int pwa_hostprog_destroy(pwa_hostprog* p);
 /* The constant block (nconst doubles) of the kernels at vars[n_vars]. */
 int pwa_hostprog_consts(pwa_hostprog* p, const double* vars, double* out);
 /* J[2*(t*ncol + k)] (re, im): d c_k / d vars[train_idx[t]];
- * D[t*nshape + j]: its selector of shape sum j. */
-int pwa_hostprog_jacobian(pwa_hostprog* p, const double* vars, double* J, double* D);
+ * Jm[2*(t*n_cpc + q)]: d c_q^- / d vars[train_idx[t]] of the CP columns'
+ * charge -1 couplings (may be NULL when there are none);
+ * D[t*nshape + j]: its selector of the kernels' extra sum j (lineshape
+ * sums, then the parent-helicity products of a polarised parent). */
+int pwa_hostprog_jacobian(pwa_hostprog* p, const double* vars, double* J, double* D,
+                          double* Jm);
 /* Piece vector (pwa_pieces_cached layout) from the kernels' data and MC
  * sums sd, sm (1 + 2*ncol + nshape each). */
 int pwa_hostprog_pieces(pwa_hostprog* p, const double* vars, const double* sd, const double* sm,

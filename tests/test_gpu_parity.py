@@ -214,7 +214,8 @@ def test_shape_cache_fcn(name):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", ["d2kpipi_float", "d2kpipi_shapes", "lc2pkpi", "b2dstkpi",
-                                  "dp2kpipi_ident", "toy_vvp"])
+                                  "dp2kpipi_ident", "toy_vvp", "lc2pkpi_pol", "lc2pkpi_cp",
+                                  "epem_pol"])
 @pytest.mark.parametrize("precision", ["plain", "mixed"])
 def test_native_host_matches_python_host(name, precision):
     """FCN's evaluations with the host side in native code (pwa_nll_grad_vars:

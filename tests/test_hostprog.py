@@ -1,8 +1,10 @@
 """The native host program (pwa_hostprog_*) against the engine's Python host
 code, on the host alone (no device): the constant block, the Jacobian of the
-column couplings with every mass and width trainable, the piece vector of the
-chain rule, the columns' barrier-normalisation products, the cache of the
-shape part, and malformed programs.
+column couplings with every mass and width trainable (with the charge -1
+couplings of CP-violating totals and the density matrix of a polarised
+parent), the piece vector of the chain rule, the columns'
+barrier-normalisation products, the cache of the shape part, and malformed
+programs.
 
 The Python host code is the one the parity tests pin against the oracle
 (test_oracle_golden.py, test_gpu_parity.py); here the native restatement is
@@ -15,7 +17,8 @@ import pytest
 from common import load_golden, load_model
 
 CASES = ["d2kpipi", "d2kpipi_float", "d2kpipi_shapes", "lc2pkpi", "lc2pkpi_cc", "b2dstkpi",
-         "b2dstkpi_cc", "toy_vvp", "dp2kpipi_ident", "ident_fermions", "ident3_fermions"]
+         "b2dstkpi_cc", "toy_vvp", "dp2kpipi_ident", "ident_fermions", "ident3_fermions",
+         "lc2pkpi_pol", "lc2pkpi_cp", "epem_pol", "epem_cp"]
 
 
 def _setup(name):
@@ -56,9 +59,15 @@ def test_consts_and_jacobian_match_python(name):
         C_nat = hp.consts(v)
         np.testing.assert_allclose(C_nat, C_py, rtol=1e-12, atol=0)
         J_py, D_py = eng.jacobian(vals, train)
-        J_nat, D_nat = hp.jacobian(v)
+        J_nat, D_nat, Jm_nat = hp.jacobian(v)
         _close(J_nat, J_py, 1e-12)
-        np.testing.assert_array_equal(D_nat, D_py[:, :eng.code.nshape])
+        ns = eng.code.nshape + eng.code.nrho
+        np.testing.assert_allclose(D_nat[:, :ns], D_py[:, :ns], rtol=1e-15, atol=0)
+        assert not np.any(D_nat[:, ns:])  # the charge -1 sums enter through Jm
+        if eng.code.cp_cols:
+            _close(Jm_nat, eng._Jm, 1e-12)
+        else:
+            assert Jm_nat.size == 0
 
 
 @pytest.mark.parametrize("name", CASES)
@@ -68,7 +77,7 @@ def test_pieces_match_python_chain_rule(name):
     rng = np.random.default_rng(7)
     vals = _shifted(vm)
     v = np.array([vals[k] for k in names])
-    nacc = 1 + 2 * eng.code.ncol + eng.code.nshape
+    nacc = eng.code.nacc
     sd, sm = rng.normal(size=nacc), rng.normal(size=nacc)
     sm[0] = abs(sm[0]) + 1.0
     C = eng.consts(vals)
@@ -123,17 +132,13 @@ def test_below_threshold_resonance_mass():
     v = np.array([vals[k] for k in names])
     np.testing.assert_allclose(hp.consts(v), eng.consts(vals), rtol=1e-12, atol=0)
     J_py, _ = eng.jacobian(vals, train)
-    J_nat, _ = hp.jacobian(v)
+    J_nat, _, _ = hp.jacobian(v)
     _close(J_nat, J_py, 1e-12)
 
 
-def test_models_the_program_does_not_cover():
+def test_trainable_without_a_role():
     from tf_pwa_b200.engine import PWAError
 
-    for name in ("lc2pkpi_pol", "lc2pkpi_cp"):
-        eng, vm, names, train = _setup(name)
-        with pytest.raises(PWAError, match="CP-violating totals or a polarised parent"):
-            eng.host_program(names, train)
     eng, vm, names, train = _setup("d2kpipi")
     with pytest.raises(PWAError, match="no role"):
         eng.host_program(names, train + ["not_a_variable"])
@@ -153,7 +158,7 @@ def test_malformed_programs_are_rejected():
     with pytest.raises(PWAError, match="trailing"):
         HostProgram(np.append(ip, 0), dp, *sizes)
     bad = ip.copy()
-    bad[1] = 2
+    bad[1] = 1  # the layout before polarisation and CP sections
     with pytest.raises(PWAError, match="magic or version"):
         HostProgram(bad, dp, *sizes)
     # a coupling's variable index past the variables

@@ -214,7 +214,7 @@ def _native_pieces(rank, world, q, name, build_dir):
     q.put((rank, nll, grad, float(g["nll"]), np.asarray(g["grad"])))
 
 
-@pytest.mark.parametrize("name", ["d2kpipi_float", "lc2pkpi"])
+@pytest.mark.parametrize("name", ["d2kpipi_float", "lc2pkpi", "lc2pkpi_cp", "lc2pkpi_pol"])
 def test_two_rank_native_host_pieces(name, tmp_path):
     """Two gloo ranks, each with half of the data and MC events, through the
     native host program: the reference's single-process NLL and gradient."""
@@ -227,7 +227,8 @@ def test_two_rank_native_host_pieces(name, tmp_path):
     g, meta = load_golden(name)
     dc, vm, plan = load_model(meta["config"])
     HostModel(Engine(dc.decay_group, plan, vm, compile=False).code, str(tmp_path))  # build once
-    os.environ["MASTER_PORT"] = str(29700 + os.getpid() % 1000 + (name == "lc2pkpi"))
+    os.environ["MASTER_PORT"] = str(29700 + os.getpid() % 1000 +
+                                    ["d2kpipi_float", "lc2pkpi", "lc2pkpi_cp", "lc2pkpi_pol"].index(name))
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     procs = [ctx.Process(target=_native_pieces, args=(r, 2, q, name, str(tmp_path)))

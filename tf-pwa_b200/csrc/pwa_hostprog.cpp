@@ -216,7 +216,7 @@ struct Reader {
 bool parse(const int* ip, long long n_ip, const double* dp, long long n_dp, pwa_hostprog* p,
            std::string* err) {
   Reader rd{ip, n_ip, 0, dp, n_dp};
-  constexpr int kMagic = 0x50574850, kVersion = 1, kCap = 1 << 20;
+  constexpr int kMagic = 0x50574850, kVersion = 2, kCap = 1 << 20;
   auto fail = [&](const std::string& m) {
     *err = "host program: " + m;
     return false;
@@ -327,6 +327,39 @@ bool parse(const int* ip, long long n_ip, const double* dp, long long n_dp, pwa_
     p->rt_slot[q] = rd.next();
     p->rt_sqrt[q] = rd.next();
   }
+  p->n_rho = rd.count(64 * 64);
+  ints(&p->rho_re, p->n_rho);
+  ints(&p->rho_im, p->n_rho);
+  p->pol_off = rd.next();
+  ints(&p->pol_var, rd.count(kCap));
+  p->rho0.resize(2 * p->n_rho);
+  for (auto& x : p->rho0) x = rd.dnext();
+  p->rho_g.assign(p->pol_var.size(), std::vector<double>(2 * p->n_rho));
+  for (auto& g : p->rho_g)
+    for (auto& x : g) x = rd.dnext();
+  const int n_cp = rd.count(kCap);
+  p->cp_coup.resize(n_cp);
+  p->cp_dr.resize(n_cp);
+  p->cp_di.resize(n_cp);
+  p->cp_t_re.resize(n_cp);
+  p->cp_t_im.resize(n_cp);
+  for (int q = 0; q < n_cp; ++q) {
+    p->cp_coup[q] = rd.next();
+    p->cp_dr[q] = rd.next();
+    p->cp_di[q] = rd.next();
+    p->cp_t_re[q] = rd.next();
+    p->cp_t_im[q] = rd.next();
+  }
+  const int n_cpc = rd.count(kCap);
+  p->cp_col.resize(n_cpc);
+  p->cp_c_re.resize(n_cpc);
+  p->cp_c_im.resize(n_cpc);
+  for (int q = 0; q < n_cpc; ++q) {
+    p->cp_col[q] = rd.next();
+    p->cp_c_re[q] = rd.next();
+    p->cp_c_im[q] = rd.next();
+  }
+  p->cp_off = rd.next();
   if (rd.next() != kMagic || !rd.ok) return fail("truncated program");
   if (rd.i != n_ip || rd.j != n_dp) return fail("trailing entries");
 
@@ -377,18 +410,42 @@ bool parse(const int* ip, long long n_ip, const double* dp, long long n_dp, pwa_
   }
   for (int q = 0; q < n_rt; ++q)
     if (!in(p->rt_col[q], 0, K) || !in(p->rt_slot[q], 0, S)) return fail("normalisation term");
+  for (int e = 0; e < p->n_rho; ++e)
+    if (!in(p->rho_re[e], 0, S) || !in(p->rho_im[e], 0, S)) return fail("density matrix slot");
+  if (p->n_rho && (p->pol_off < 0 || p->pol_off + 2 * p->n_rho > p->nshape))
+    return fail("polarisation sums outside the extra sums");
+  for (int v : p->pol_var)
+    if (!in(v, 0, V) || !p->n_rho) return fail("polarisation variable");
+  for (int q = 0; q < n_cp; ++q)
+    if (!in(p->cp_coup[q], 0, p->n_coup) || !in(p->cp_dr[q], 0, V) || !in(p->cp_di[q], 0, V) ||
+        !in(p->cp_t_re[q], 0, S) || !in(p->cp_t_im[q], 0, S))
+      return fail("CP total");
+  for (int q = 0; q < n_cpc; ++q)
+    if (!in(p->cp_col[q], 0, K) || !in(p->cp_c_re[q], 0, S) || !in(p->cp_c_im[q], 0, S))
+      return fail("CP column");
+  if (p->cp_off != -1 && (p->cp_off < 0 || p->cp_off + 2 * n_cpc > p->nshape))
+    return fail("charge -1 sums outside the extra sums");
 
   // roles of the trainable variables and the inputs of the shape part
+  p->coup_cp.assign(p->n_coup, -1);
+  for (int q = 0; q < n_cp; ++q) p->coup_cp[p->cp_coup[q]] = q;
   p->t_coup.assign(p->n_train, -1);
   p->t_comp.assign(p->n_train, 0);
   p->t_sel.assign(p->n_train, -1);
   p->t_mj.assign(p->n_train, -1);
+  p->t_pol.assign(p->n_train, -1);
   for (int t = 0; t < p->n_train; ++t) {
     const int v = p->train_idx[t];
     for (int q = 0; q < p->n_coup && p->t_coup[t] < 0; ++q) {
       if (p->coup_r[q] == v) p->t_coup[t] = q, p->t_comp[t] = 0;
       else if (p->coup_i[q] == v) p->t_coup[t] = q, p->t_comp[t] = 1;
     }
+    for (int q = 0; q < n_cp && p->t_coup[t] < 0; ++q) {
+      if (p->cp_dr[q] == v) p->t_coup[t] = p->cp_coup[q], p->t_comp[t] = 2;
+      else if (p->cp_di[q] == v) p->t_coup[t] = p->cp_coup[q], p->t_comp[t] = 3;
+    }
+    for (size_t q = 0; q < p->pol_var.size(); ++q)
+      if (p->pol_var[q] == v) p->t_pol[t] = (int)q;
     for (int q = 0; q < n_sel; ++q)
       if (p->sel_var[q] == v) p->t_sel[t] = p->sel_slot[q];
     for (int q = 0; q < n_mj; ++q)
@@ -420,19 +477,37 @@ void consts(pwa_hostprog* p, const double* vars, double* C, std::vector<cd>* z,
     p->have_shape = true;
   }
   for (int q = 0; q < p->nconst; ++q) C[q] = p->cshape[q];
-  // couplings: r e^{i phi} (polar) or r + i phi, columns their products
+  // couplings: r e^{i phi} (polar) or r + i phi, columns their products;
+  // a CP total at (r + dr, i + di), its charge -1 value at (r - dr, i - di)
+  auto value = [](int polar, double r, double ph) {
+    return polar ? cd(r * std::cos(ph), r * std::sin(ph)) : cd(r, ph);
+  };
   z->resize(p->n_coup);
+  p->zm.resize(p->n_coup);
   for (int j = 0; j < p->n_coup; ++j) {
-    const double r = vars[p->coup_r[j]], ph = vars[p->coup_i[j]];
-    (*z)[j] = p->coup_polar[j] ? cd(r * std::cos(ph), r * std::sin(ph)) : cd(r, ph);
+    double r = vars[p->coup_r[j]], ph = vars[p->coup_i[j]];
+    const int q = p->coup_cp[j];
+    if (q >= 0) {
+      const double dr = vars[p->cp_dr[q]], di = vars[p->cp_di[q]];
+      p->zm[j] = value(p->coup_polar[j], r - dr, ph - di);
+      r += dr;
+      ph += di;
+      (*z)[j] = value(p->coup_polar[j], r, ph);
+    } else {
+      (*z)[j] = p->zm[j] = value(p->coup_polar[j], r, ph);
+    }
   }
-  ck->resize(2 * p->ncol);
-  for (int k = 0; k < p->ncol; ++k) {
+  auto column = [&](int k, const std::vector<cd>& zz) {
     cd c(1.0, 0.0);
     for (int f = 0; f < p->nfac; ++f) {
       const int j = p->col_fac[k * p->nfac + f];
-      if (j >= 0) c = c * (*z)[j];
+      if (j >= 0) c = c * zz[j];
     }
+    return c;
+  };
+  ck->resize(2 * p->ncol);
+  for (int k = 0; k < p->ncol; ++k) {
+    const cd c = column(k, *z);
     (*ck)[2 * k] = C[2 * k] = c.real();
     (*ck)[2 * k + 1] = C[2 * k + 1] = c.imag();
   }
@@ -440,52 +515,105 @@ void consts(pwa_hostprog* p, const double* vars, double* C, std::vector<cd>* z,
     C[p->vg_re[q]] = (*z)[p->vg_src[q]].real();
     C[p->vg_im[q]] = (*z)[p->vg_src[q]].imag();
   }
+  for (size_t q = 0; q < p->cp_coup.size(); ++q) {
+    C[p->cp_t_re[q]] = p->zm[p->cp_coup[q]].real();
+    C[p->cp_t_im[q]] = p->zm[p->cp_coup[q]].imag();
+  }
+  p->ckm.resize(2 * p->cp_col.size());
+  for (size_t q = 0; q < p->cp_col.size(); ++q) {
+    const cd c = column(p->cp_col[q], p->zm);
+    p->ckm[2 * q] = C[p->cp_c_re[q]] = c.real();
+    p->ckm[2 * q + 1] = C[p->cp_c_im[q]] = c.imag();
+  }
+  // parent density matrix, linear in the polarisation variables
+  for (int e = 0; e < p->n_rho; ++e) {
+    cd r(p->rho0[2 * e], p->rho0[2 * e + 1]);
+    for (size_t q = 0; q < p->pol_var.size(); ++q)
+      r += vars[p->pol_var[q]] * cd(p->rho_g[q][2 * e], p->rho_g[q][2 * e + 1]);
+    C[p->rho_re[e]] = r.real();
+    C[p->rho_im[e]] = r.imag();
+  }
 }
 
 void jacobian(pwa_hostprog* p, const double* vars, const std::vector<cd>& z,
-              const std::vector<double>& ck, cd* J, double* D) {
-  const int K = p->ncol, P = p->n_train, NS = p->nshape;
+              const std::vector<double>& ck, cd* J, cd* Jm, double* D) {
+  const int K = p->ncol, P = p->n_train, NS = p->nshape, NC = (int)p->cp_col.size();
   for (long long q = 0; q < (long long)P * K; ++q) J[q] = cd(0.0, 0.0);
+  if (Jm)
+    for (long long q = 0; q < (long long)P * NC; ++q) Jm[q] = cd(0.0, 0.0);
   for (long long q = 0; q < (long long)P * NS; ++q) D[q] = 0.0;
+  // d(prod of column k's factors)/dz_j with the factors zz (each occurrence
+  // of j in turn, the others kept), times dz
+  auto prod_rule = [&](int k, int j, const std::vector<cd>& zz, cd dz) {
+    int cnt = 0;
+    cd others(1.0, 0.0);
+    for (int f = 0; f < p->nfac; ++f) {
+      const int q = p->col_fac[k * p->nfac + f];
+      if (q < 0) continue;
+      if (q == j && cnt++ == 0) continue;
+      others = others * zz[q];
+    }
+    return cnt ? (double)cnt * others * dz : cd(0.0, 0.0);
+  };
   for (int t = 0; t < P; ++t) {
     cd* Jt = J + (long long)t * K;
+    cd* Jmt = Jm ? Jm + (long long)t * NC : nullptr;
     const int j = p->t_coup[t];
     if (j >= 0) {
-      const double ph = vars[p->coup_i[j]];
-      cd dz;
-      if (p->coup_polar[j])
-        dz = p->t_comp[t] == 0 ? cd(std::cos(ph), std::sin(ph)) : cd(0.0, 1.0) * z[j];
-      else
-        dz = p->t_comp[t] == 0 ? cd(1.0, 0.0) : cd(0.0, 1.0);
-      for (int k = 0; k < K; ++k) {
-        // d(prod of factors)/dz: count of z times the product of the others
-        // (further factors z included)
-        int cnt = 0;
-        cd others(1.0, 0.0);
-        for (int f = 0; f < p->nfac; ++f) {
-          const int q = p->col_fac[k * p->nfac + f];
-          if (q < 0) continue;
-          if (q == j && cnt++ == 0) continue;
-          others = others * z[q];
-        }
-        if (cnt) Jt[k] = (double)cnt * others * dz;
+      // z = a e^{i phi}: dz/da = e^{i phi}, dz/dphi = i z (polar); 1, i
+      // (Cartesian); at the charge's own (a, phi); deltar / deltai enter
+      // charge -1 with a minus sign
+      const int role = p->t_comp[t], q = p->coup_cp[j];
+      const bool is_i = role == 1 || role == 3;
+      auto dz_at = [&](double ph, const cd& zv) {
+        if (p->coup_polar[j]) return is_i ? cd(0.0, 1.0) * zv : cd(std::cos(ph), std::sin(ph));
+        return is_i ? cd(0.0, 1.0) : cd(1.0, 0.0);
+      };
+      double ph_p = vars[p->coup_i[j]], ph_m = ph_p;
+      if (q >= 0) {
+        ph_p += vars[p->cp_di[q]];
+        ph_m -= vars[p->cp_di[q]];
       }
+      const cd dzp = dz_at(ph_p, z[j]);
+      const cd dzm = (role >= 2 ? -1.0 : 1.0) * dz_at(ph_m, p->zm[j]);
+      for (int k = 0; k < K; ++k) Jt[k] = prod_rule(k, j, z, dzp);
+      if (Jmt)
+        for (int c = 0; c < NC; ++c) Jmt[c] = prod_rule(p->cp_col[c], j, p->zm, dzm);
     }
     if (p->t_mj[t] >= 0) {
       const auto& kap = p->kap[p->t_mj[t]];
       for (int k = 0; k < K; ++k) Jt[k] += cd(ck[2 * k], ck[2 * k + 1]) * kap[k];
+      if (Jmt)
+        for (int c = 0; c < NC; ++c)
+          Jmt[c] += cd(p->ckm[2 * c], p->ckm[2 * c + 1]) * kap[p->cp_col[c]];
     }
-    if (p->t_sel[t] >= 0) D[(long long)t * NS + p->t_sel[t]] = 1.0;
+    double* Dt = D + (long long)t * NS;
+    if (p->t_sel[t] >= 0) Dt[p->t_sel[t]] = 1.0;
+    if (p->t_pol[t] >= 0) {
+      // d f / d p = Re sum_e T_e G_e with the kernels' T sums as (re, im):
+      // Re(T G) = T.re G.re - T.im G.im
+      const auto& g = p->rho_g[p->t_pol[t]];
+      for (int e = 0; e < p->n_rho; ++e) {
+        Dt[p->pol_off + 2 * e] = g[2 * e];
+        Dt[p->pol_off + 2 * e + 1] = -g[2 * e + 1];
+      }
+    }
   }
 }
 
-void grad_from_sums(const pwa_hostprog* p, const cd* J, const double* D, const double* s,
-                    double* g) {
-  const int K = p->ncol, NS = p->nshape;
+void grad_from_sums(const pwa_hostprog* p, const cd* J, const cd* Jm, const double* D,
+                    const double* s, double* g) {
+  const int K = p->ncol, NS = p->nshape, NC = (int)p->cp_col.size();
   for (int t = 0; t < p->n_train; ++t) {
     const cd* Jt = J + (long long)t * K;
     double acc = 0.0;
     for (int k = 0; k < K; ++k) acc += Jt[k].real() * s[1 + 2 * k] - Jt[k].imag() * s[2 + 2 * k];
+    if (Jm && p->cp_off >= 0) {
+      // charge -1 column sums of the CP columns
+      const cd* Jmt = Jm + (long long)t * NC;
+      const double* sm = s + 1 + 2 * K + p->cp_off;
+      for (int c = 0; c < NC; ++c) acc += Jmt[c].real() * sm[2 * c] - Jmt[c].imag() * sm[2 * c + 1];
+    }
     acc *= 2.0;
     for (int q = 0; q < NS; ++q) acc += D[(long long)t * NS + q] * s[1 + 2 * K + q];
     g[t] = acc;

@@ -57,10 +57,31 @@ struct pwa_hostprog {
   std::vector<int> sel_var, sel_slot;
   std::vector<MJac> mj;
   std::vector<int> rt_col, rt_slot, rt_sqrt;
+  // polarised parent: rho = rho0 + sum_q p_q G_q into the slots rho_re /
+  // rho_im (n_rho entries); p_q acts through the kernels' parent-helicity
+  // sums from pol_off on (d f / d p_q = Re sum_e T_e G_q,e)
+  int n_rho = 0, pol_off = 0;
+  std::vector<int> rho_re, rho_im, pol_var;
+  std::vector<double> rho0;                 // (re, im) per entry
+  std::vector<std::vector<double>> rho_g;   // per polarisation variable
+  // CP-violating chain totals: charge +1 takes (r + dr, i + di), charge -1
+  // (r - dr, i - di) (tf_pwa/variable.py:199-235); the minus-charge totals
+  // and the CP columns' minus-charge couplings go to their slots, the
+  // kernels' charge -1 column sums start at cp_off (-1: the data carry no
+  // charge, no such sums)
+  std::vector<int> cp_coup, cp_dr, cp_di, cp_t_re, cp_t_im;  // per CP total
+  std::vector<int> cp_col, cp_c_re, cp_c_im;                 // per CP column
+  int cp_off = -1;
   std::vector<int> key_var;
-  // per trainable variable: coupling (index, 0 = r / 1 = i) or -1, shape
-  // selector slot or -1, barrier-row entry of mj or -1
-  std::vector<int> t_coup, t_comp, t_sel, t_mj;
+  // per coupling: its CP total entry or -1
+  std::vector<int> coup_cp;
+  // per trainable variable: coupling index or -1 with its role (0 r, 1 i,
+  // 2 deltar, 3 deltai), shape selector slot or -1, barrier-row entry of mj
+  // or -1, polarisation entry or -1
+  std::vector<int> t_coup, t_comp, t_sel, t_mj, t_pol;
+  // couplings and CP columns' couplings of the last consts() call, charge -1
+  std::vector<std::complex<double>> zm;
+  std::vector<double> ckm;
   // cache of the shape part
   bool have_shape = false;
   std::vector<double> key, cshape;
@@ -77,13 +98,16 @@ bool parse(const int* ip, long long n_ip, const double* dp, long long n_dp, pwa_
 // (2*ncol, re/im) are filled on the way.
 void consts(pwa_hostprog* p, const double* vars, double* C, std::vector<std::complex<double>>* z,
             std::vector<double>* ck);
-// Jacobian of the column couplings, J[t*ncol + k] (complex), and the shape
-// selectors D[t*nshape + j] of every trainable variable (after consts()).
+// Jacobian of the column couplings, J[t*ncol + k] (complex), of the CP
+// columns' charge -1 couplings, Jm[t*ncp_col + q] (may be null without CP
+// columns), and the selectors D[t*nshape + j] of the kernels' extra sums of
+// every trainable variable (after consts()).
 void jacobian(pwa_hostprog* p, const double* vars, const std::vector<std::complex<double>>& z,
-              const std::vector<double>& ck, std::complex<double>* J, double* D);
+              const std::vector<double>& ck, std::complex<double>* J, std::complex<double>* Jm,
+              double* D);
 // d(sum)/d(trainable) of one event set's sums s (1 + 2*ncol + nshape).
-void grad_from_sums(const pwa_hostprog* p, const std::complex<double>* J, const double* D,
-                    const double* s, double* g);
+void grad_from_sums(const pwa_hostprog* p, const std::complex<double>* J,
+                    const std::complex<double>* Jm, const double* D, const double* s, double* g);
 // Barrier-normalisation product of each column (ncol) in the constant
 // block C; false where a factor is not positive (the columns do not
 // factorise at this setting).

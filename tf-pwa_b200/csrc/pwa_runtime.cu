@@ -1993,12 +1993,14 @@ int pwa_hostprog_consts(pwa_hostprog* p, const double* vars, double* out) {
   return PWA_OK;
 }
 
-int pwa_hostprog_jacobian(pwa_hostprog* p, const double* vars, double* J, double* D) {
+int pwa_hostprog_jacobian(pwa_hostprog* p, const double* vars, double* J, double* D,
+                          double* Jm) {
   if (!p || !vars || !J || !D) return set_err(nullptr, PWA_ERR_ARG, "null argument");
   std::vector<double> C(p->nconst), ck;
   std::vector<std::complex<double>> z;
   pwa_host::consts(p, vars, C.data(), &z, &ck);
-  pwa_host::jacobian(p, vars, z, ck, reinterpret_cast<std::complex<double>*>(J), D);
+  pwa_host::jacobian(p, vars, z, ck, reinterpret_cast<std::complex<double>*>(J),
+                     reinterpret_cast<std::complex<double>*>(Jm), D);
   return PWA_OK;
 }
 
@@ -2008,14 +2010,14 @@ void pieces_from_hp_sums(pwa_hostprog* p, const double* vars, const std::vector<
                          const std::vector<double>& ck, const double* sd, const double* sm,
                          double sw, double mc_share, double* out) {
   const int P = p->n_train;
-  std::vector<std::complex<double>> J((size_t)P * p->ncol);
+  std::vector<std::complex<double>> J((size_t)P * p->ncol), Jm((size_t)P * p->cp_col.size() + 1);
   std::vector<double> D((size_t)P * p->nshape + 1);
-  pwa_host::jacobian(p, vars, z, ck, J.data(), D.data());
+  pwa_host::jacobian(p, vars, z, ck, J.data(), Jm.data(), D.data());
   out[0] = sd[0];
   out[1] = sm[0] * mc_share;
   out[2] = sw;
-  pwa_host::grad_from_sums(p, J.data(), D.data(), sd, out + 3);
-  pwa_host::grad_from_sums(p, J.data(), D.data(), sm, out + 3 + P);
+  pwa_host::grad_from_sums(p, J.data(), Jm.data(), D.data(), sd, out + 3);
+  pwa_host::grad_from_sums(p, J.data(), Jm.data(), D.data(), sm, out + 3 + P);
   for (int t = 0; t < P; ++t) out[3 + P + t] *= mc_share;
 }
 }  // namespace

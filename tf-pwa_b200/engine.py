@@ -100,7 +100,7 @@ def load_library(path=LIB_PATH):
     lib.pwa_hostprog_create.argtypes = [ip, ll, dp, ll, ctypes.POINTER(vp)]
     lib.pwa_hostprog_destroy.argtypes = [vp]
     lib.pwa_hostprog_consts.argtypes = [vp, dp, dp]
-    lib.pwa_hostprog_jacobian.argtypes = [vp, dp, dp, dp]
+    lib.pwa_hostprog_jacobian.argtypes = [vp, dp, dp, dp, dp]
     lib.pwa_hostprog_pieces.argtypes = [vp, dp, dp, dp, ctypes.c_double, ctypes.c_double, dp]
     lib.pwa_hostprog_column_rho.argtypes = [vp, dp, dp]
     lib.pwa_set_host_program.argtypes = [vp, vp]
@@ -163,10 +163,11 @@ class HostProgram:
     layout in native code, from the flat arrays of
     :meth:`Engine.host_program_arrays`.  Needs no device."""
 
-    def __init__(self, ip, dp, ncol, nconst, nshape, n_train):
+    def __init__(self, ip, dp, ncol, nconst, nshape, n_train, n_cpc=0):
         self.ip = np.ascontiguousarray(ip, np.int32)
         self.dp = np.ascontiguousarray(dp, np.float64)
         self.ncol, self.nconst, self.nshape, self.n_train = ncol, nconst, nshape, n_train
+        self.n_cpc = n_cpc
         lib = load_library()
         h = ctypes.c_void_p()
         rc = lib.pwa_hostprog_create(self.ip.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
@@ -188,13 +189,19 @@ class HostProgram:
         return out
 
     def jacobian(self, var_values):
+        """(J, D, Jm): column-coupling Jacobian (n_train x ncol), selectors
+        of the extra sums (n_train x nshape), charge -1 Jacobian of the CP
+        columns (n_train x n_cpc)."""
         v = np.ascontiguousarray(var_values, np.float64)
         J = np.zeros(2 * self.n_train * self.ncol)
         D = np.zeros(max(self.n_train * self.nshape, 1))
-        self._check(load_library().pwa_hostprog_jacobian(self.h, _dptr(v), _dptr(J), _dptr(D)),
-                    "pwa_hostprog_jacobian")
+        Jm = np.zeros(max(2 * self.n_train * self.n_cpc, 1))
+        self._check(load_library().pwa_hostprog_jacobian(self.h, _dptr(v), _dptr(J), _dptr(D),
+                                                         _dptr(Jm)), "pwa_hostprog_jacobian")
         J = (J[0::2] + 1j * J[1::2]).reshape(self.n_train, self.ncol)
-        return J, D[:self.n_train * self.nshape].reshape(self.n_train, self.nshape)
+        Jm = (Jm[0::2] + 1j * Jm[1::2])[:self.n_train * self.n_cpc].reshape(self.n_train,
+                                                                            self.n_cpc)
+        return J, D[:self.n_train * self.nshape].reshape(self.n_train, self.nshape), Jm
 
     def pieces(self, var_values, sd, sm, sw, mc_share=1.0):
         v = np.ascontiguousarray(var_values, np.float64)
@@ -1106,16 +1113,13 @@ class Engine:
         """The flat (int, double) arrays of this model's host program for
         the variable layout ``var_names`` (all variables, in order) and the
         gradient w.r.t. ``train_names`` (format in include/pwa_b200.h).
-        PWAError for models whose host side it does not cover (CP-violating
-        totals, a polarised parent) or a trainable name with no role."""
-        if len(self._cp_coup) or self._pol_names:
-            raise PWAError("the host program covers models without CP-violating totals or a "
-                           "polarised parent")
+        PWAError for a trainable name with no role."""
         c = self.code
         idx = {n: i for i, n in enumerate(var_names)}
+        cp_names = set(self._cp_dr) | set(self._cp_di)
         for n in train_names:
             ok = (n[:-1] in self._cn_index and n[-1] in "ri") or n in self._mass_names \
-                or n in self._width_names
+                or n in self._width_names or n in cp_names or n in self._pol_index
             if not ok or n not in idx:
                 raise PWAError(f"trainable variable {n} has no role in the host program")
         try:
@@ -1124,7 +1128,8 @@ class Engine:
         except KeyError as e:
             raise PWAError(f"coupling variable {e} missing from the layout") from None
         nfac = self._fac_idx.shape[1]
-        ip = [HOSTPROG_MAGIC, 1, c.ncol, len(c.consts), c.nshape, len(var_names),
+        n_extra = c.nshape + c.nrho + c.ncp
+        ip = [HOSTPROG_MAGIC, 2, c.ncol, len(c.consts), n_extra, len(var_names),
               len(train_names), len(self.coupling_names), nfac]
         ip += cr + ci + [int(bool(x)) for x in self._cn_polar]
         ip += [int(x) for x in self._fac_idx.reshape(-1)]
@@ -1186,14 +1191,42 @@ class Engine:
         ip += [len(rt)]
         for t in rt:
             ip += list(t)
+        # polarised parent: rho = rho0 + sum_q p_q G_q (density_matrix is
+        # linear in the polarisation)
+        if self._pol_names:
+            try:
+                pv = [idx[n] for n in self._pol_names]
+            except KeyError as e:
+                raise PWAError(f"polarisation variable {e} missing from the layout") from None
+            rho0, G = density_matrix(self.group.top.J, np.zeros(len(self._pol_names)))
+            ne = rho0.size
+            ip += [ne] + [int(x) for x in self._rho_re] + [int(x) for x in self._rho_im]
+            ip += [c.nshape, len(pv)] + pv
+            for m in [rho0] + list(G):
+                dp += [float(x) for pair in zip(m.real.reshape(-1), m.imag.reshape(-1))
+                       for x in pair]
+        else:
+            ip += [0, 0, 0]
+        # CP-violating totals and the CP columns' charge -1 couplings
+        ip += [len(self._cp_coup)]
+        for j, ndr, ndi, sre, sim in zip(self._cp_coup, self._cp_dr, self._cp_di,
+                                         self._cp_t_re, self._cp_t_im):
+            if ndr not in idx or ndi not in idx:
+                raise PWAError(f"CP variables of {self.coupling_names[j]} missing from the layout")
+            ip += [int(j), idx[ndr], idx[ndi], int(sre), int(sim)]
+        ip += [len(self._cp_cols)]
+        for k, sre, sim in zip(self._cp_cols, self._cp_c_re, self._cp_c_im):
+            ip += [int(k), int(sre), int(sim)]
+        ip += [c.nshape + c.nrho if c.ncp else -1]
         ip += [HOSTPROG_MAGIC]
         return np.array(ip, np.int32), np.array(dp, np.float64)
 
     def host_program(self, var_names, train_names):
         """:class:`HostProgram` of this model for the given layout."""
         ip, dp = self.host_program_arrays(var_names, train_names)
-        return HostProgram(ip, dp, self.code.ncol, len(self.code.consts), self.code.nshape,
-                           len(train_names))
+        c = self.code
+        return HostProgram(ip, dp, c.ncol, len(c.consts), c.nshape + c.nrho + c.ncp,
+                           len(train_names), len(c.cp_cols))
 
     def set_host_program(self, var_names, train_names):
         """Give the plan its host program: evaluations from the variable
