@@ -19,6 +19,9 @@
  *                      (cal_angle_from_momentum at data load)
  *   pwa_toy_select /   flat phase space and toy        tf_pwa/phasespace.py:31-254,
  *   pwa_toy_fields     accept-reject on sum |A|^2      tf_pwa/applications.py:394-487
+ *   pwa_hostprog_* /   constants, Jacobian, chain rule tf_pwa/model/model.py:407-449,1223-1229
+ *   pwa_nll_grad_vars  from the variables (host side   tf_pwa/amp/core.py:349-418,1072-1104
+ *                      of FCN.nll_grad)
  *   pwa_hessian_cached Hessian (differenced adjoint)   tf_pwa/model/model.py:513-561
  *   pwa_hessian_cached_exact  (closed form, one pass)  tf_pwa/model/model.py:513-561
  *   pwa_read_dat       text momentum files             tf_pwa/data.py:300-365
