@@ -42,6 +42,11 @@ WORKLOADS = {
                       "D0 -> K pi pi (K*(892) 1-, f0(980) 0+; 2 chains), both resonance masses "
                       "and widths floating (no column cache), 1e6 accept-reject data, 1e6 flat "
                       "MC"),
+    "lc2pkpi_float": ("lc2pkpi_float.yml", 1_000_000, 100_000, 1_000_000,
+                      "NLL+grad evals/s @1M data+1M MC, masses and widths floating",
+                      "Lambda_c+ -> p K- pi+ (the headline model) with the three resonance masses "
+                      "and widths floating (no Gram matrix), 1e6 accept-reject signal + 1e5 flat "
+                      "background (w=-0.1) data rows, 1e6 flat MC"),
     "b2dstkpi": ("b2dstkpi.yml", 1_000_000, 0, 4_000_000,
                  "NLL+grad evals/s @1M data+4M MC",
                  "B -> D*(2007) (-> D pi_s) K pi, 12 resonances (J = 0..3) in the D*K, D*pi "
@@ -395,6 +400,11 @@ NCU_F32_KERNEL_FLOPS = {
     "b2dstkpi": ((2 * 1563318624 + 906727936 + 80454656) / 5e5,
                  (2 * 99600000 + 57500000 + 136206080) / 5e5),
 }
+# the Lambda_c model with floating masses and widths compiles to the same
+# plain and FP32 kernels as with fixed ones
+for _table in (FWD_FLOPS, NCU_F64_FLOPS_PER_EVENT, NCU_F32_KERNEL_FLOPS):
+    _table["lc2pkpi_float"] = _table["lc2pkpi"]
+FLOATING = ("d2kpipi_float", "lc2pkpi_float")
 
 
 def _mixed_pipe_roofline(name, n_ev, launch_s, peaks):
@@ -620,7 +630,7 @@ def measure_cached(name, args, rank, world, dist, timed, log, n_sig, n_bg, n_mc,
 
 
 # ------------------------------------------------- floating masses/widths
-def measure_floating(name, args, rank, world, dist, timed, log, n_sig, n_mc):
+def measure_floating(name, args, rank, world, dist, timed, log, n_sig, n_mc, n_bg=0):
     """Workload with floating lineshape parameters (no Gram matrix): the
     chosen form is the floating-shape column cache (shape-free columns
     cached in FP32, lineshapes recomputed from the resident masses every
@@ -635,15 +645,16 @@ def measure_floating(name, args, rank, world, dist, timed, log, n_sig, n_mc):
 
     config, _, _, _, metric, workload = WORKLOADS[name]
     t0 = time.perf_counter()
-    cl, data, bg, mc = make_dataset(config, n_sig, n_mc, seed=1 + rank)
+    cl, data, bg, mc = make_dataset(config, n_sig, n_mc, n_bg=n_bg, bg_weight=BG_WEIGHT,
+                                    seed=1 + rank)
     t_data = time.perf_counter() - t0
-    log(f"{name}: dataset {n_sig} data + {n_mc} MC events")
+    log(f"{name}: dataset {n_sig} data + {n_bg} background + {n_mc} MC events")
     t0 = time.perf_counter()
-    fcn = FCN(cl, data, mc, precision="mixed")
+    fcn = FCN(cl, data, mc, bg=bg, precision="mixed")
     t_cache = time.perf_counter() - t0
-    assert not fcn.use_gram
-    fcn_r = FCN(cl, data, mc, precision="mixed", shape_cache=False)
-    fcn_p = FCN(cl, data, mc, precision="plain")
+    assert not fcn.use_gram and fcn.use_shape_cache
+    fcn_r = FCN(cl, data, mc, bg=bg, precision="mixed", shape_cache=False)
+    fcn_p = FCN(cl, data, mc, bg=bg, precision="plain")
     for f in (fcn, fcn_r, fcn_p):
         f.eng.dist_reduce = _reduce_fn(dist)
         f.eng.mc_share = 1.0 / world  # equal MC shards
@@ -688,7 +699,7 @@ def measure_floating(name, args, rank, world, dist, timed, log, n_sig, n_mc):
     nll_f, g_f = fcn_r.nll_grad(x0)
     nll_p, g_p = fcn_p.nll_grad(x0)
     code = fcn.eng.code
-    n_all = n_sig + n_mc
+    n_all = n_sig + n_bg + n_mc
     bytes_f32 = n_all * (8 * len(code.mass_fields) + 4 * len(code.angle_fields) + 8)
     bytes_f64 = n_all * (8 * len(code.mass_fields) + 8 * len(code.angle_fields) + 8)
     bytes_sc = n_all * (8 * code.nf + 8 * len(code.mass_fields) + 8)
@@ -741,7 +752,7 @@ def measure_floating(name, args, rank, world, dist, timed, log, n_sig, n_mc):
                    "partial-wave columns without their lineshapes cached as FP32 (computed in "
                    "FP64), lineshapes and their derivatives recomputed in FP64 from the resident "
                    "masses every evaluation, FP64 amplitude, log and sums",
-                   "events_per_rank": {"data": n_sig, "mc": n_mc},
+                   "events_per_rank": {"data": n_sig, "background": n_bg, "mc": n_mc},
                    "l2": "256 MB buffer written before every timed step (L2 126 MB)",
                    "parallelism": f"dp{world}" if world > 1 else "single GPU"},
         "plain_f64": {"value": world * args.steps / t_p, "unit": "evals/s",
@@ -889,9 +900,9 @@ def main():
     def log(msg):
         print(f"[bench {time.perf_counter() - t_setup:8.1f}s] {msg}", file=sys.stderr, flush=True)
 
-    if args.workload == "d2kpipi_float":
+    if args.workload in FLOATING:
         line = measure_floating(args.workload, args, rank, world, dist, timed, log, args.n_sig,
-                                args.n_mc)
+                                args.n_mc, args.n_bg)
     else:
         line = measure_cached(args.workload, args, rank, world, dist, timed, log, args.n_sig,
                               args.n_bg, args.n_mc)
@@ -903,9 +914,10 @@ def main():
             _, s4, b4, m4, _, _ = WORKLOADS["b2dstkpi"]
             extra["b2dstkpi"] = _compact(measure_cached("b2dstkpi", args, rank, world, dist,
                                                         timed, log, s4, b4, m4, variants=False))
-            _, sf, _, mf, _, _ = WORKLOADS["d2kpipi_float"]
-            extra["d2kpipi_float"] = _compact(measure_floating("d2kpipi_float", args, rank,
-                                                               world, dist, timed, log, sf, mf))
+            for fname in FLOATING:
+                _, sf, bf, mf, _, _ = WORKLOADS[fname]
+                extra[fname] = _compact(measure_floating(fname, args, rank, world, dist, timed,
+                                                         log, sf, mf, bf))
             log("serving")
             line["serving"] = serving_summary(args.n_fits)
         except Exception as e:  # reported, never fatal to the headline

@@ -42,3 +42,19 @@ def test_default_cache_dir_is_the_package(monkeypatch):
     monkeypatch.setenv("PWA_CUBIN_CACHE", "/nonexistent-choice")
     engine._default_cubin_cache()  # an explicit setting is kept
     assert os.environ["PWA_CUBIN_CACHE"] == "/nonexistent-choice"
+
+
+def test_floating_shapes_share_the_kernels():
+    """Floating a model's masses and widths changes its trainable set, not
+    its kernels: the floating-shape Lambda_c config compiles to the same
+    source (and cubin) as the fixed one, so the plain and FP32 kernels'
+    measured operation counts apply to both."""
+    from tf_pwa_b200.engine import Engine
+
+    srcs = []
+    for cfg in ("lc2pkpi.yml", "lc2pkpi_float.yml"):
+        dc, vm, plan = load_model(cfg)
+        srcs.append(Engine(dc.decay_group, plan, vm, compile=False).src)
+        if cfg == "lc2pkpi_float.yml":
+            assert sum(n.endswith(("_mass", "_width")) for n in vm.trainable_vars) == 6
+    assert srcs[0] == srcs[1]
