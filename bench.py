@@ -62,9 +62,14 @@ NCU_TRAFFIC_PER_ROW = {"lc2pkpi": (290.436096e6 + 6.841088e6) / 1.1e6,
                        "b2dstkpi": (248.044032e6 + 3.609856e6) / 1e6}
 # the same for the floating-shape evaluation kernel, per event (data + MC):
 # D -> K pi pi, 80.04 + 2.29 MB for 2e6 events
-NCU_SC_TRAFFIC_PER_EVENT = {"d2kpipi_float": (80.041728e6 + 2.286848e6) / 2e6}
-# its FP64 operations per event (2 DFMA + DMUL + DADD executed, ncu, 2e6 events)
-NCU_SC_F64_FLOPS_PER_EVENT = {"d2kpipi_float": (2 * 249757760 + 131606208 + 59444606) / 2e6}
+# (Lambda_c: 151.30 + 5.62 MB for the 5.25e5 events of a quarter-size
+# capture, inputs larger than L2; traffic grows with the events)
+NCU_SC_TRAFFIC_PER_EVENT = {"d2kpipi_float": (80.041728e6 + 2.286848e6) / 2e6,
+                            "lc2pkpi_float": (151.29728e6 + 5.616384e6) / 5.25e5}
+# its FP64 operations per event (2 DFMA + DMUL + DADD executed, ncu; 2e6 and
+# 5.25e5 events)
+NCU_SC_F64_FLOPS_PER_EVENT = {"d2kpipi_float": (2 * 249757760 + 131606208 + 59444606) / 2e6,
+                              "lc2pkpi_float": (2 * 236845232 + 81638568 + 38105098) / 5.25e5}
 
 
 def _select(name):
