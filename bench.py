@@ -784,7 +784,9 @@ def measure_floating(name, args, rank, world, dist, timed, log, n_sig, n_mc, n_b
                                  "what": "the same steps with the host side in the engine's "
                                          "Python code (Engine.nll_grad)"}},
         "fma_peaks": peaks,
-        "gpu_launches": 2 * args.steps,
+        # one launch of pwa_eval_shapecache per timed step (its reduction is
+        # in the same launch)
+        "gpu_launches": args.steps,
         "hessian": {"seconds": t_hess, "n_params": len(x0), "evaluations": 4 * len(x0) + 1,
                     "errors": dict(zip(names, np.sqrt(np.abs(np.diag(cov))).tolist()))},
         "check": {"nll_shape_cache": nll_s, "nll_plain": nll_p, "dnll": nll_s - nll_p,
