@@ -138,8 +138,6 @@ struct pwa_plan {
   // scratch
   double* partials = nullptr;
   long long partials_cap = 0;
-  double* d_out = nullptr;
-  double* h_out = nullptr;
 };
 
 namespace {
@@ -459,7 +457,6 @@ int pwa_plan_create(const char* src, size_t src_len, int n_mass, int n_angle, in
     h->regs[p] = a.numRegs;
     h->local_bytes[p] = (long long)a.localSizeBytes;
   }
-  CU(cudaMalloc(&h->d_out, sizeof(double) * 2 * h->nacc));
   // [0] finished groups, [1] error flag, [2 + g] finished blocks of group g
   CU(cudaMalloc(&h->ticket, kTicketWords * sizeof(unsigned int)));
   CU(cudaMemset(h->ticket, 0, kTicketWords * sizeof(unsigned int)));
@@ -468,7 +465,6 @@ int pwa_plan_create(const char* src, size_t src_len, int n_mass, int n_angle, in
   CU(cudaHostAlloc(&h->h_map_sc, sizeof(double) * (2 * h->nacc + 2), cudaHostAllocMapped));
   CU(cudaHostGetDevicePointer((void**)&h->d_map_sc, h->h_map_sc, 0));
   h->h_map_sc[2 * h->nacc + 1] = -1.0;
-  CU(cudaMallocHost(&h->h_out, sizeof(double) * 2 * (h->nacc > ncol * ncol ? h->nacc : ncol * ncol)));
   return PWA_OK;
 }
 
@@ -492,8 +488,6 @@ int pwa_plan_destroy(pwa_plan* h) {
   if (h->scache) cudaFree(h->scache);
   if (h->h_map) cudaFreeHost(h->h_map);
   if (h->h_map_sc) cudaFreeHost(h->h_map_sc);
-  if (h->d_out) cudaFree(h->d_out);
-  if (h->h_out) cudaFreeHost(h->h_out);
   if (h->lib) cudaLibraryUnload(h->lib);
   delete h;
   return PWA_OK;
@@ -591,10 +585,8 @@ int pwa_eval_enqueue(pwa_plan* h, const double* consts, int precision, int mc, v
                   dim3(h->tpb), args, s);
   if (rc) return rc;
   int nacc = h->nacc;
-  if (!mc) {
-    // only data sums: the MC half of d_out is cleared by the reduction
-  }
-  // sums into the mapped result, the call number last
+  // sums into the mapped result (with mc = 0 the MC half comes out zero:
+  // no MC blocks), the call number last
   h->seq += 1.0;
   double seq = h->seq;
   double* seq_out = h->d_map_sc + 2 * nacc + 1;
