@@ -1010,6 +1010,11 @@ class ModelCode:
         L.append(self._pdf_source())
         fl = sorted(self._fset)
         L.append(f"#define PWA_NF {self.nf}")
+        # blocks per SM of the plain FP64 kernels: 4 where the accumulators
+        # are few (Lambda_c, 23: 651 vs 724 us per 2.1e6 events at 3), 3 for
+        # larger models, whose FP64 state spills more at 4 (four-body, 85:
+        # 6.77 vs 5.95 ms)
+        L.append(f"#define PWA_EVAL_MINB {4 if self.nacc <= 32 else 3}")
         # the floating-shape evaluation stages its next events in shared
         # memory (two stages of pairs, masses and weight per event at 128
         # threads) where that takes at most 150 KB per block

@@ -97,9 +97,10 @@ __device__ __forceinline__ void eval_body(const Consts& C, const R* __restrict__
 // Blocks per SM the plain kernels are compiled for (register cap 65536 /
 // (128 x MINB)).  Measured on B200 (2.1e6 events): the FP32 form runs
 // 7-13 % faster at 4 than at 3 (Lambda_c 424 vs 454 us, four-body 3.94 vs
-// 4.52 ms); the FP64 form is faster at 4 for Lambda_c (616 vs 667 us) but
+// 4.52 ms); the FP64 form is faster at 4 for Lambda_c (651 vs 724 us) but
 // slower for the four-body model, whose FP64 state already spills at 3
-// (6.77 vs 5.95 ms), so it stays at 3.
+// (6.77 vs 5.95 ms): the model source sets PWA_EVAL_MINB by its size (3
+// when it does not).
 #ifndef PWA_EVAL_MINB
 #define PWA_EVAL_MINB 3
 #endif
