@@ -58,3 +58,16 @@ def test_floating_shapes_share_the_kernels():
         if cfg == "lc2pkpi_float.yml":
             assert sum(n.endswith(("_mass", "_width")) for n in vm.trainable_vars) == 6
     assert srcs[0] == srcs[1]
+
+
+def test_plain_kernel_occupancy_by_model_size():
+    """The model source sets the plain kernels' blocks per SM: 4 for the
+    Lambda_c model (23 accumulators), 3 for the four-body model (85)."""
+    import re
+
+    from tf_pwa_b200.engine import Engine
+
+    for cfg, want in (("lc2pkpi.yml", 4), ("b2dstkpi.yml", 3)):
+        dc, vm, plan = load_model(cfg)
+        src = Engine(dc.decay_group, plan, vm, compile=False).src
+        assert re.search(r"#define PWA_EVAL_MINB (\d+)", src).group(1) == str(want)
