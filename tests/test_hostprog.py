@@ -174,3 +174,9 @@ def test_malformed_programs_are_rejected():
     bad[o + 2] = len(eng.code.consts)
     with pytest.raises(PWAError, match="vertex coupling slot"):
         HostProgram(bad, dp, *sizes)
+    # a list count larger than the program itself is refused before anything
+    # of that size is allocated
+    bad = ip.copy()
+    bad[o] = 1 << 20
+    with pytest.raises(PWAError, match="truncated"):
+        HostProgram(bad, dp, *sizes)

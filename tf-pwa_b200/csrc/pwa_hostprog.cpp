@@ -204,7 +204,15 @@ struct Reader {
     }
     return dp[j++];
   }
-  int count(int cap) {  // a non-negative count of at most cap
+  // a non-negative count of at most cap, and of at most the ints left (every
+  // counted item reads at least one), so a malformed program cannot make
+  // parse() allocate more than its own size
+  int count(int cap) {
+    const int n = next();
+    if (n < 0 || n > cap || n > n_ip - i) ok = false;
+    return ok ? n : 0;
+  }
+  int value(int cap) {  // a non-negative size of at most cap (not a list length)
     const int n = next();
     if (n < 0 || n > cap) ok = false;
     return ok ? n : 0;
@@ -223,16 +231,20 @@ bool parse(const int* ip, long long n_ip, const double* dp, long long n_dp, pwa_
   };
   if (!ip || n_ip <= 0 || (n_dp > 0 && !dp)) return fail("empty program");
   if (rd.next() != kMagic || rd.next() != kVersion) return fail("bad magic or version");
-  p->ncol = rd.count(kCap);
-  p->nconst = rd.count(kCap);
-  p->nshape = rd.count(kCap);
-  p->n_vars = rd.count(kCap);
-  p->n_train = rd.count(kCap);
-  p->n_coup = rd.count(kCap);
-  p->nfac = rd.count(64);
+  p->ncol = rd.value(kCap);
+  p->nconst = rd.value(kCap);
+  p->nshape = rd.value(kCap);
+  p->n_vars = rd.value(kCap);
+  p->n_train = rd.value(kCap);
+  p->n_coup = rd.value(kCap);
+  p->nfac = rd.value(64);
   if (!rd.ok || p->ncol <= 0 || p->nconst < 2 * p->ncol || p->n_coup <= 0 || p->nfac <= 0)
     return fail("bad header");
   auto ints = [&](std::vector<int>* v, long long n) {
+    if (n < 0 || n > rd.n_ip - rd.i) {
+      rd.ok = false;
+      n = 0;
+    }
     v->resize(n);
     for (long long q = 0; q < n; ++q) (*v)[q] = rd.next();
   };
@@ -269,7 +281,7 @@ bool parse(const int* ip, long long n_ip, const double* dp, long long n_dp, pwa_
       e.bn = rd.next();
       e.s_pz = rd.next();
       e.s_norm = rd.next();
-      e.coef.resize(rd.count(64));
+      e.coef.resize(rd.value(64));  // doubles: not a count of ints
       for (auto& c : e.coef) c = rd.dnext();
     }
   }
@@ -290,7 +302,7 @@ bool parse(const int* ip, long long n_ip, const double* dp, long long n_dp, pwa_
     r.s_wn = rd.next();
     r.s_kap = rd.next();
     r.s_ig = rd.next();
-    r.coef.resize(rd.count(64));
+    r.coef.resize(rd.value(64));
     r.d = rd.dnext();
     r.g_def = rd.dnext();
     for (auto& c : r.coef) c = rd.dnext();
