@@ -589,7 +589,9 @@ class ModelCode:
                 e(f"  const R yi_{tag} = rr_{tag} < R(0) ? ya_{tag} : R(0);")
                 e(f"  const R dre_{tag} = xr_{tag} + yi_{tag};")
                 e(f"  const R s_{tag} = dre_{tag} * dre_{tag} + y_{tag} * y_{tag};")
-                e(f"  const cpx<R> bw_{tag} = cmk<R>(dre_{tag} / s_{tag}, -y_{tag} / s_{tag});")
+                # one reciprocal for both parts (a division each would be two)
+                e(f"  const R is_{tag} = R(1) / s_{tag};")
+                e(f"  const cpx<R> bw_{tag} = cmk<R>(dre_{tag} * is_{tag}, -y_{tag} * is_{tag});")
             else:
                 if kind == "BWR":
                     dp = c.decay_of(p)
@@ -605,14 +607,16 @@ class ModelCode:
                     e(f"  const R qp_{tag} = {cst(f'{p}.useq')} != R(0) ? ({qp}) : R(1);")
                     e(f"  const R y_{tag} = mulkc<R>(qp_{tag} / (R({m}) * ({poly})), C, {self._ci(f'{p}.K')});")
                     e(f"  const R s_{tag} = xr_{tag} * xr_{tag} + y_{tag} * y_{tag};")
-                    e(f"  const cpx<R> bw_{tag} = cmk<R>(xr_{tag} / s_{tag}, y_{tag} / s_{tag});")
+                    e(f"  const R is_{tag} = R(1) / s_{tag};")
+                    e(f"  const cpx<R> bw_{tag} = cmk<R>(xr_{tag} * is_{tag}, y_{tag} * is_{tag});")
                 else:
                     # constant width: value from the FP64 m0^2 - m^2 and m0 Gamma0
                     e(f"  const R y_{tag} = {cst(f'{p}.y')};")
                     e(f"  cpx<R> bw_{tag};")
                     e(f"  {{ const double xd = {self._cv(f'{p}.m0sq')} - {m} * {m}, "
                       f"yd = {self._cv(f'{p}.y')}, sd = xd * xd + yd * yd;")
-                    e(f"    bw_{tag} = cmk<R>(R(xd / sd), R(yd / sd)); }}")
+                    e("    const double isd = 1.0 / sd;")
+                    e(f"    bw_{tag} = cmk<R>(R(xd * isd), R(yd * isd)); }}")
             if p.width_norm_applies():
                 # the chain product takes Gamma0 R (the derivatives use R)
                 wn = self._ci(f'{p}.wn')
