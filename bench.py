@@ -66,10 +66,10 @@ NCU_TRAFFIC_PER_ROW = {"lc2pkpi": (290.436096e6 + 6.841088e6) / 1.1e6,
 # capture, inputs larger than L2; traffic grows with the events)
 NCU_SC_TRAFFIC_PER_EVENT = {"d2kpipi_float": (80.041728e6 + 2.286848e6) / 2e6,
                             "lc2pkpi_float": (151.29728e6 + 5.616384e6) / 5.25e5}
-# its FP64 operations per event (2 DFMA + DMUL + DADD executed, ncu; 2e6 and
+# its FP64 operations per event (2 DFMA + DMUL + DADD executed, ncu; 5e5 and
 # 5.25e5 events)
-NCU_SC_F64_FLOPS_PER_EVENT = {"d2kpipi_float": (2 * 249757760 + 131606208 + 59444606) / 2e6,
-                              "lc2pkpi_float": (2 * 236845232 + 81638568 + 38105098) / 5.25e5}
+NCU_SC_F64_FLOPS_PER_EVENT = {"d2kpipi_float": (2 * 54011168 + 33358304 + 17445502) / 5e5,
+                              "lc2pkpi_float": (2 * 222667712 + 81638424 + 38105098) / 5.25e5}
 
 
 def _select(name):
@@ -387,22 +387,22 @@ FWD_FLOPS = {"d2kpipi_float": (318, 77), "lc2pkpi": (1614, 228), "b2dstkpi": (67
 # adjoint, data and MC alike), 2 * DFMA + DADD + DMUL executed, from an ncu
 # capture of pwa_eval_f64 (None: not captured; the forward count is used)
 NCU_F64_FLOPS_PER_EVENT = {
-    # 2 * 1.723050e9 DFMA + 7.7975e8 DMUL + 1.54827e8 DADD per launch over
-    # 5.5e5 data + 5e5 MC events of the Lambda_c model
-    "lc2pkpi": (2 * 1723050000 + 779750000 + 154826528) / 1.05e6,
-    # 2 * 2.0671e9 DFMA + 1.0715e9 DMUL + 1.35105e8 DADD over 1e5 + 4e5 events
-    "b2dstkpi": (2 * 2067100000 + 1071500000 + 135104560) / 5e5,
-    # 2 * 2.1725e8 DFMA + 9.075e7 DMUL + 2.74312e7 DADD over 2.5e5 + 2.5e5 events
-    "d2kpipi_float": (2 * 217250000 + 90750000 + 27431232) / 5e5,
+    # 2 * 8.17425e8 DFMA + 3.88825e8 DMUL + 7.97437e7 DADD per launch over
+    # 2.75e5 data + 2.5e5 MC events of the Lambda_c model
+    "lc2pkpi": (2 * 817425000 + 388825000 + 79743704) / 5.25e5,
+    # 2 * 1.9591e9 DFMA + 1.0715e9 DMUL + 1.35105e8 DADD over 1e5 + 4e5 events
+    "b2dstkpi": (2 * 1959100000 + 1071500000 + 135104560) / 5e5,
+    # 2 * 1.9925e8 DFMA + 9.075e7 DMUL + 2.74312e7 DADD over 2.5e5 + 2.5e5 events
+    "d2kpipi_float": (2 * 199250000 + 90750000 + 27431232) / 5e5,
 }
 # FP32 and FP64 operations per event of the FP32-amplitude kernel
 # (pwa_eval_f32), same captures: 2 * FFMA + FMUL + FADD, 2 * DFMA + DMUL + DADD
 NCU_F32_KERNEL_FLOPS = {
-    "d2kpipi_float": ((2 * 125378880 + 49568320 + 6189440) / 5e5,
+    "d2kpipi_float": ((2 * 109378880 + 53568320 + 8189440) / 5e5,
                       (2 * 47750000 + 25250000 + 27289040) / 5e5),
-    "lc2pkpi": ((2 * 655654656 + 305706984 + 22125776) / 5.25e5,
+    "lc2pkpi": ((2 * 630454656 + 312006984 + 25275776) / 5.25e5,
                 (2 * 94500000 + 55975000 + 71343704) / 5.25e5),
-    "b2dstkpi": ((2 * 1563318624 + 906727936 + 80454656) / 5e5,
+    "b2dstkpi": ((2 * 1467318624 + 930727936 + 92454656) / 5e5,
                  (2 * 99600000 + 57500000 + 136206080) / 5e5),
 }
 # the Lambda_c model with floating masses and widths compiles to the same
